@@ -1,0 +1,382 @@
+"""ctypes bindings for the CPU oracle (test infrastructure only).
+
+Two libraries live here:
+
+* ``_build/liboracle.so`` -- the plain-C restatement of the reference residue path
+  (``ckks_oracle.c``), always buildable with gcc.
+* ``_ref/libwalshref.so`` -- the reference itself, compiled from its own sources by
+  ``make -C oracle ref`` with a thin harness (``ref_harness.cpp``).  Present only where the
+  reference sources were available at build time.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libwalshref.so")
+
+u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+i8p = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+szp = np.ctypeslib.ndpointer(dtype=np.uintp, flags="C_CONTIGUOUS")
+
+
+def build(ref: bool = False) -> None:
+    """Compile the oracle (and, when asked and the sources exist, the reference harness)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if ref and os.path.isdir(os.environ.get("REF_ROOT", "/root/reference")):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+
+
+_lib = None
+_ref = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        L.orc_find_primes.argtypes = [u64p, C.c_size_t, u64p, C.c_size_t, C.c_uint64, u64p, u64p]
+        L.orc_ntt_tables.argtypes = [C.c_uint64, C.c_uint64, u64p, u64p, u64p, u64p, C.POINTER(C.c_uint64)]
+        L.orc_ctx_create.restype = C.c_void_p
+        L.orc_ctx_create.argtypes = [C.c_uint64, u64p, C.c_size_t, u64p, C.c_size_t, C.c_size_t]
+        L.orc_ctx_destroy.argtypes = [C.c_void_p]
+        L.orc_ctx_alpha.restype = C.c_size_t
+        L.orc_ctx_alpha.argtypes = [C.c_void_p]
+        L.orc_ntt.argtypes = [C.c_void_p, u64p, C.c_size_t, C.c_size_t, C.c_int, C.c_int, C.c_int]
+        L.orc_keyswitch.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, C.c_size_t, u64p, u64p, C.c_int, C.c_int]
+        L.orc_automorphism_map.argtypes = [C.c_uint64, C.c_uint64, u64p]
+        L.orc_rotation_galois.restype = C.c_uint64
+        L.orc_rotation_galois.argtypes = [C.c_uint64, C.c_int64]
+        L.orc_rotate.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, u64p, C.c_size_t, C.c_int64]
+        L.orc_conjugate.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, u64p, C.c_size_t]
+        L.orc_mul.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, u64p, u64p, u64p]
+        L.orc_relin.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, u64p, u64p, C.c_size_t]
+        L.orc_rescale.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, u64p]
+        L.orc_sample_ternary.argtypes = [C.c_uint64, C.c_size_t, C.c_uint64, i8p]
+        L.orc_keygen_switch.argtypes = [C.c_void_p, i8p, C.c_int, i8p, C.c_double, C.c_uint64, u64p]
+        L.orc_secret_automorphism.argtypes = [C.c_uint64, C.c_uint64, i8p, i8p]
+        L.orc_uniform_poly.argtypes = [C.c_void_p, C.c_size_t, C.c_uint64, u64p]
+        L.orc_encrypt.argtypes = [C.c_void_p, C.c_size_t, u64p, i8p, C.c_double, C.c_uint64, u64p, u64p]
+        L.orc_decrypt_coeffs.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, i8p, f64p]
+        L.orc_barrett_mul.restype = C.c_uint64
+        L.orc_barrett_mul.argtypes = [C.c_uint64] * 5
+        L.orc_batched_ops.argtypes = [C.c_void_p, C.c_size_t, szp, u64p, u64p, u64p, u64p, u64p,
+                                      C.c_void_p, i64p, C.c_size_t, C.c_size_t, C.c_int]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        R = C.CDLL(REF_SO)
+        R.ref_last_error.restype = C.c_char_p
+        R.ref_find_primes.argtypes = [u64p, C.c_size_t, u64p, C.c_size_t, C.c_uint64, u64p, u64p]
+        R.ref_ntt_tables.argtypes = [C.c_uint64, C.c_uint64, u64p, u64p, u64p, u64p, C.POINTER(C.c_uint64), u64p]
+        R.ref_ctx_create.restype = C.c_void_p
+        R.ref_ctx_create.argtypes = [C.c_uint64, u64p, C.c_size_t, u64p, C.c_size_t, C.c_size_t, C.c_size_t,
+                                     C.c_double, C.c_double, i64p, C.c_size_t]
+        R.ref_ctx_destroy.argtypes = [C.c_void_p]
+        R.ref_ctx_moduli.argtypes = [C.c_void_p, u64p, C.POINTER(C.c_size_t), u64p, C.POINTER(C.c_size_t)]
+        R.ref_ctx_ntt.argtypes = [C.c_void_p, u64p, C.c_size_t, C.c_int, C.c_int]
+        R.ref_ctx_key_shape.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+        R.ref_ctx_key.argtypes = [C.c_void_p, C.c_int, C.c_int64, u64p]
+        R.ref_ctx_map.argtypes = [C.c_void_p, C.c_int, C.c_int64, u64p]
+        R.ref_ctx_secret.argtypes = [C.c_void_p, u64p]
+        R.ref_keyswitch.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, C.c_size_t, C.c_size_t, u64p, u64p,
+                                    C.c_int, C.c_int, C.c_int]
+        R.ref_rotate.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, C.c_int64]
+        R.ref_conjugate.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
+        R.ref_mul.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, u64p, u64p, u64p]
+        R.ref_relin.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, u64p]
+        R.ref_rescale.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, u64p]
+        R.ref_hoisted_rotations.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, i64p, C.c_size_t, u64p]
+        R.ref_batched_ops.argtypes = [C.c_void_p, C.c_size_t, szp, u64p, u64p, u64p, u64p, i64p, C.c_size_t,
+                                      C.c_int, C.POINTER(C.c_double)]
+        R.ref_max_threads.restype = C.c_int
+        _ref = R
+    return _ref
+
+
+def _check(rc: int, who: str) -> None:
+    if rc != 0:
+        msg = ref().ref_last_error().decode() if who.startswith("ref") else ""
+        raise RuntimeError(f"{who} failed ({rc}) {msg}")
+
+
+# ------------------------------------------------------------------------------------------
+# Parameter helpers
+# ------------------------------------------------------------------------------------------
+def find_primes(p_bits, q_bits, N):
+    pb = np.ascontiguousarray(p_bits, dtype=np.uint64)
+    qb = np.ascontiguousarray(q_bits, dtype=np.uint64)
+    p = np.zeros(len(pb), np.uint64)
+    q = np.zeros(len(qb), np.uint64)
+    _check(lib().orc_find_primes(pb, len(pb), qb, len(qb), N, p, q), "orc_find_primes")
+    return p, q
+
+
+def ntt_tables(N, q):
+    f = np.zeros(N, np.uint64)
+    fs = np.zeros(N, np.uint64)
+    i = np.zeros(N, np.uint64)
+    is_ = np.zeros(N + 1, np.uint64)
+    ninv = C.c_uint64()
+    _check(lib().orc_ntt_tables(N, int(q), f, fs, i, is_, C.byref(ninv)), "orc_ntt_tables")
+    return f, fs, i, is_, ninv.value
+
+
+class OracleCtx:
+    """Oracle context for one parameter set (moduli Q, P, dnum)."""
+
+    def __init__(self, N, q, p, dnum):
+        self.N = int(N)
+        self.q = np.ascontiguousarray(q, dtype=np.uint64)
+        self.p = np.ascontiguousarray(p, dtype=np.uint64)
+        self.dnum = int(dnum)
+        self.h = lib().orc_ctx_create(self.N, self.q, len(self.q), self.p, len(self.p), self.dnum)
+        if not self.h:
+            raise ValueError("invalid oracle parameters")
+        self.alpha = lib().orc_ctx_alpha(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_ctx_destroy(self.h)
+            self.h = None
+
+    @property
+    def nq(self):
+        return len(self.q)
+
+    @property
+    def np_(self):
+        return len(self.p)
+
+    def parts(self, level):
+        return min(self.dnum, (level + 1 + self.alpha - 1) // self.alpha)
+
+    def key_size(self, key_level=None):
+        kl = self.nq - 1 if key_level is None else key_level
+        return self.dnum_top() * 2 * (kl + 1 + self.np_) * self.N
+
+    def dnum_top(self):
+        return self.parts(self.nq - 1)
+
+    def ntt(self, poly, first=0, which=0, inverse=False, lazy=False):
+        poly = np.ascontiguousarray(poly, dtype=np.uint64).copy()
+        limbs = poly.size // self.N
+        lib().orc_ntt(self.h, poly, first, limbs, which, int(inverse), int(lazy))
+        return poly
+
+    def uniform(self, limbs, seed):
+        out = np.zeros(limbs * self.N, np.uint64)
+        lib().orc_uniform_poly(self.h, limbs, seed, out)
+        return out
+
+    def ternary(self, h, seed):
+        s = np.zeros(self.N, np.int8)
+        lib().orc_sample_ternary(self.N, h, seed, s)
+        return s
+
+    def keygen(self, src, dst, seed, square=False, sigma=3.2):
+        key = np.zeros(self.key_size(), np.uint64)
+        _check(lib().orc_keygen_switch(self.h, src, int(square), dst, sigma, seed, key), "orc_keygen")
+        return key
+
+    def rotation_key(self, s, rotation, seed):
+        g_inv = lib().orc_rotation_galois(self.N, -rotation)
+        sd = np.zeros(self.N, np.int8)
+        lib().orc_secret_automorphism(self.N, g_inv, s, sd)
+        return self.keygen(s, sd, seed)
+
+    def conjugation_key(self, s, seed):
+        sd = np.zeros(self.N, np.int8)
+        lib().orc_secret_automorphism(self.N, 2 * self.N - 1, s, sd)
+        return self.keygen(sd, s, seed)
+
+    def relin_key(self, s, seed):
+        return self.keygen(s, s, seed, square=True)
+
+    def keyswitch(self, level, key_term, key, b, a, b_add=True, a_add=False, key_level=None):
+        kl = self.nq - 1 if key_level is None else key_level
+        b = np.ascontiguousarray(b, dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        kt = np.ascontiguousarray(key_term, dtype=np.uint64)
+        _check(lib().orc_keyswitch(self.h, level, kt, np.ascontiguousarray(key), kl, b, a,
+                                   int(b_add), int(a_add)), "orc_keyswitch")
+        return b, a
+
+    def rotate(self, level, b, a, key, rotation, key_level=None):
+        kl = self.nq - 1 if key_level is None else key_level
+        b = np.ascontiguousarray(b, dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        _check(lib().orc_rotate(self.h, level, b, a, np.ascontiguousarray(key), kl, rotation), "orc_rotate")
+        return b, a
+
+    def conjugate(self, level, b, a, key, key_level=None):
+        kl = self.nq - 1 if key_level is None else key_level
+        b = np.ascontiguousarray(b, dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        _check(lib().orc_conjugate(self.h, level, b, a, np.ascontiguousarray(key), kl), "orc_conjugate")
+        return b, a
+
+    def mul(self, level, b1, a1, b2, a2):
+        b1 = np.ascontiguousarray(b1, dtype=np.uint64).copy()
+        a1 = np.ascontiguousarray(a1, dtype=np.uint64).copy()
+        c2 = np.zeros_like(b1)
+        _check(lib().orc_mul(self.h, level, b1, a1, np.ascontiguousarray(b2), np.ascontiguousarray(a2), c2),
+               "orc_mul")
+        return b1, a1, c2
+
+    def relin(self, level, c0, c1, c2, key, key_level=None):
+        kl = self.nq - 1 if key_level is None else key_level
+        c0 = np.ascontiguousarray(c0, dtype=np.uint64).copy()
+        c1 = np.ascontiguousarray(c1, dtype=np.uint64).copy()
+        _check(lib().orc_relin(self.h, level, c0, c1, np.ascontiguousarray(c2), np.ascontiguousarray(key), kl),
+               "orc_relin")
+        return c0, c1
+
+    def rescale(self, level, polys):
+        """polys: list of (level+1)*N arrays; returns list of level*N arrays."""
+        n = (level + 1) * self.N
+        flat = np.concatenate([np.ascontiguousarray(p, dtype=np.uint64) for p in polys])
+        _check(lib().orc_rescale(self.h, level, len(polys), flat), "orc_rescale")
+        return [flat[k * n:k * n + level * self.N].copy() for k in range(len(polys))]
+
+    def automorphism_map(self, g):
+        m = np.zeros(self.N, np.uint64)
+        lib().orc_automorphism_map(self.N, g, m)
+        return m
+
+    def galois(self, rotation):
+        return lib().orc_rotation_galois(self.N, rotation)
+
+    def encrypt(self, level, m_ntt, s, seed, sigma=3.2):
+        n = (level + 1) * self.N
+        b = np.zeros(n, np.uint64)
+        a = np.zeros(n, np.uint64)
+        _check(lib().orc_encrypt(self.h, level, np.ascontiguousarray(m_ntt, dtype=np.uint64), s, sigma, seed, b, a),
+               "orc_encrypt")
+        return b, a
+
+    def decrypt_coeffs(self, level, b, a, s):
+        out = np.zeros(self.N, np.float64)
+        _check(lib().orc_decrypt_coeffs(self.h, level, np.ascontiguousarray(b), np.ascontiguousarray(a), s, out),
+               "orc_decrypt")
+        return out
+
+    def batched_ops(self, levels, x_b, x_a, y_b, y_a, relin_key, rot_keys, rots, stride, threads):
+        """CPU timing baseline: x_* updated in place.  rot_keys: list of key arrays."""
+        levels = np.ascontiguousarray(levels, dtype=np.uintp)
+        ptrs = (C.c_void_p * len(rot_keys))(*[k.ctypes.data for k in rot_keys])
+        rc = lib().orc_batched_ops(self.h, len(levels), levels, x_b, x_a, y_b, y_a, relin_key,
+                                   C.cast(ptrs, C.c_void_p), np.ascontiguousarray(rots, dtype=np.int64),
+                                   self.nq - 1, stride, threads)
+        _check(rc, "orc_batched_ops")
+
+
+class RefCtx:
+    """The reference's own CKKSContext (custom moduli schedule, no bootstrapping keys)."""
+
+    def __init__(self, N, q_bits, p_bits, dnum, h=192, sigma=3.2, scale=2.0 ** 40, rotations=(1,)):
+        R = ref()
+        qb = np.ascontiguousarray(q_bits, dtype=np.uint64)
+        pb = np.ascontiguousarray(p_bits, dtype=np.uint64)
+        rots = np.ascontiguousarray(rotations, dtype=np.int64)
+        self.N = int(N)
+        self.h = R.ref_ctx_create(self.N, qb, len(qb), pb, len(pb), dnum, h, sigma, scale, rots, len(rots))
+        if not self.h:
+            raise RuntimeError("ref_ctx_create: " + R.ref_last_error().decode())
+        nq, np_ = C.c_size_t(), C.c_size_t()
+        _check(R.ref_ctx_moduli(self.h, np.zeros(64, np.uint64), C.byref(nq), np.zeros(64, np.uint64),
+                                C.byref(np_)), "ref_ctx_moduli")
+        self.q = np.zeros(nq.value, np.uint64)
+        self.p = np.zeros(np_.value, np.uint64)
+        _check(R.ref_ctx_moduli(self.h, self.q, C.byref(nq), self.p, C.byref(np_)), "ref_ctx_moduli")
+        self.dnum = dnum
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().ref_ctx_destroy(self.h)
+            self.h = None
+
+    def ntt(self, poly, inverse=False, lazy=False):
+        poly = np.ascontiguousarray(poly, dtype=np.uint64).copy()
+        _check(ref().ref_ctx_ntt(self.h, poly, poly.size // self.N, int(inverse), int(lazy)), "ref_ctx_ntt")
+        return poly
+
+    def key(self, kind, rot=0):
+        parts, kl = C.c_size_t(), C.c_size_t()
+        _check(ref().ref_ctx_key_shape(self.h, kind, rot, C.byref(parts), C.byref(kl)), "ref_ctx_key_shape")
+        size = parts.value * 2 * (kl.value + 1 + len(self.p)) * self.N
+        out = np.zeros(size, np.uint64)
+        _check(ref().ref_ctx_key(self.h, kind, rot, out), "ref_ctx_key")
+        return out, parts.value, kl.value
+
+    def map(self, kind, rot=0):
+        out = np.zeros(self.N, np.uint64)
+        _check(ref().ref_ctx_map(self.h, kind, rot, out), "ref_ctx_map")
+        return out
+
+    def keyswitch(self, level, key_term, key, parts, key_level, b, a, b_add=True, a_add=False):
+        b = np.ascontiguousarray(b, dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        kt = np.ascontiguousarray(key_term, dtype=np.uint64).copy()
+        _check(ref().ref_keyswitch(self.h, level, kt, np.ascontiguousarray(key), parts, key_level, b, a,
+                                   int(b_add), int(a_add), 1), "ref_keyswitch")
+        return b, a
+
+    def rotate(self, level, b, a, rot):
+        b = np.ascontiguousarray(b, dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        _check(ref().ref_rotate(self.h, level, b, a, rot), "ref_rotate")
+        return b, a
+
+    def conjugate(self, level, b, a):
+        b = np.ascontiguousarray(b, dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        _check(ref().ref_conjugate(self.h, level, b, a), "ref_conjugate")
+        return b, a
+
+    def mul(self, level, b1, a1, b2, a2):
+        b1 = np.ascontiguousarray(b1, dtype=np.uint64).copy()
+        a1 = np.ascontiguousarray(a1, dtype=np.uint64).copy()
+        c2 = np.zeros_like(b1)
+        _check(ref().ref_mul(self.h, level, b1, a1, np.ascontiguousarray(b2), np.ascontiguousarray(a2), c2),
+               "ref_mul")
+        return b1, a1, c2
+
+    def relin(self, level, c0, c1, c2):
+        c0 = np.ascontiguousarray(c0, dtype=np.uint64).copy()
+        c1 = np.ascontiguousarray(c1, dtype=np.uint64).copy()
+        _check(ref().ref_relin(self.h, level, c0, c1, np.ascontiguousarray(c2)), "ref_relin")
+        return c0, c1
+
+    def rescale(self, level, polys):
+        n = (level + 1) * self.N
+        flat = np.concatenate([np.ascontiguousarray(p, dtype=np.uint64) for p in polys])
+        _check(ref().ref_rescale(self.h, level, len(polys), flat), "ref_rescale")
+        return [flat[k * n:k * n + level * self.N].copy() for k in range(len(polys))]
+
+    def hoisted_rotations(self, level, b, a, rots):
+        n = (level + 1) * self.N
+        out = np.zeros(len(rots) * 2 * n, np.uint64)
+        _check(ref().ref_hoisted_rotations(self.h, level, np.ascontiguousarray(b), np.ascontiguousarray(a),
+                                           np.ascontiguousarray(rots, dtype=np.int64), len(rots), out),
+               "ref_hoisted_rotations")
+        return out.reshape(len(rots), 2, n)

@@ -1,0 +1,381 @@
+// Test-infrastructure harness around the reference library compiled from its own sources.
+//
+// It exposes the reference's own functions through plain C entry points so the Python tests
+// can (1) pin the C restatement in ckks_oracle.c against the real thing and (2) write golden
+// fixtures.  Nothing in the product links this file.  Every entry point returns 0 on success
+// and a negative value when the reference threw (the message is kept for ref_last_error()).
+//
+// Reference entry points wrapped here:
+//   find_p_and_q_primes                src/util/random.cpp:115
+//   generate_negacyclic_ntt_twiddles   src/math/ntt/ntt.cpp:54
+//   ntt_{forward,inverse}_rns_flat_inplace  src/math/ntt/ntt.cpp:416,433
+//   CKKSContext::CKKSContext           src/ckks/context/ckks_context.cpp:603
+//   ckks_hybrid_key_switch_inplace     src/ckks/operations/keyswitch/ckks_keyswitch.cpp:1330
+//   ckks_rotate_inplace                src/ckks/operations/keyswitch/ckks_rotation.cpp:41
+//   ckks_conjugate_inplace             src/ckks/operations/keyswitch/ckks_conjugate.cpp:112
+//   ckks_relin_hybrid_inplace          src/ckks/operations/keyswitch/ckks_relin.cpp:8
+//   ckks_mul_inplace (ct x ct)         src/ckks/operations/arith/ckks_mul.cpp:90
+//   ckks_rescale                       src/ckks/operations/arith/ckks_rescale.cpp:68
+//   ckks_hoist_ciphertext_a_qp_eval / ckks_hybrid_key_switch_hoisted_inplace
+//                                      src/ckks/operations/keyswitch/ckks_keyswitch.cpp:344,1072
+
+#include <algorithm>
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+#include <omp.h>
+
+#include "ckks_ciphertext.hpp"
+#include "ckks_context.hpp"
+#include "ckks_conjugate.hpp"
+#include "ckks_keyswitch.hpp"
+#include "ckks_mul.hpp"
+#include "ckks_params.hpp"
+#include "ckks_relin.hpp"
+#include "ckks_rescale.hpp"
+#include "ckks_rotation.hpp"
+#include "ntt.hpp"
+#include "random.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    } catch (...) {
+        g_last_error = "unknown exception";
+        return -2;
+    }
+}
+
+MyVector<uint64_t> copy_in(const uint64_t* src, size_t n) {
+    return MyVector<uint64_t>(src, src + n);
+}
+
+void copy_out(const MyVector<uint64_t>& src, uint64_t* dst) {
+    std::memcpy(dst, src.data(), src.size() * sizeof(uint64_t));
+}
+
+// Key layout shared with the oracle and the device library:
+// [part][poly: 0 = a, 1 = b][limb: key_level+1 Q limbs then K P limbs][N]
+std::vector<CKKSCiphertext> keys_from_flat(const uint64_t* flat, size_t parts, size_t key_level,
+                                           size_t p_count, size_t N) {
+    const size_t limbs = key_level + 1 + p_count;
+    std::vector<CKKSCiphertext> out;
+    out.reserve(parts);
+    for (size_t part = 0; part < parts; ++part) {
+        const uint64_t* a = flat + (part * 2 + 0) * limbs * N;
+        const uint64_t* b = flat + (part * 2 + 1) * limbs * N;
+        out.emplace_back(N, copy_in(a, limbs * N), copy_in(b, limbs * N), 1.0L, key_level);
+    }
+    return out;
+}
+
+void keys_to_flat(std::span<const CKKSCiphertext> keys, uint64_t* flat) {
+    size_t off = 0;
+    for (const auto& k : keys) {
+        std::memcpy(flat + off, k.getA().data(), k.getA().size() * sizeof(uint64_t));
+        off += k.getA().size();
+        std::memcpy(flat + off, k.getB().data(), k.getB().size() * sizeof(uint64_t));
+        off += k.getB().size();
+    }
+}
+
+struct RefCtx {
+    CKKSContext ctx;
+    explicit RefCtx(CKKSParams p) : ctx(std::move(p)) {}
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_last_error.c_str(); }
+
+int ref_find_primes(const uint64_t* p_bits, size_t np, const uint64_t* q_bits, size_t nq,
+                    uint64_t N, uint64_t* p_out, uint64_t* q_out) {
+    return guarded([&] {
+        std::vector<uint64_t> pb(p_bits, p_bits + np), qb(q_bits, q_bits + nq);
+        auto [p, q] = find_p_and_q_primes(pb, qb, N);
+        std::copy(p.begin(), p.end(), p_out);
+        std::copy(q.begin(), q.end(), q_out);
+    });
+}
+
+int ref_ntt_tables(uint64_t N, uint64_t q, uint64_t* fwd, uint64_t* fwd_shoup, uint64_t* inv,
+                   uint64_t* inv_shoup_np1, uint64_t* n_inv, uint64_t* barrett_lo_hi) {
+    return guarded([&] {
+        auto t = generate_negacyclic_ntt_twiddles(N, q);
+        copy_out(t.forward_ntt, fwd);
+        copy_out(t.forward_shoup, fwd_shoup);
+        copy_out(t.inverse_ntt, inv);
+        copy_out(t.inverse_shoup, inv_shoup_np1);
+        *n_inv = t.N_inv;
+        barrett_lo_hi[0] = t.barrett_const.low;
+        barrett_lo_hi[1] = t.barrett_const.high;
+    });
+}
+
+// Context with custom moduli schedule and no bootstrapping keys.
+void* ref_ctx_create(uint64_t N, const uint64_t* q_bits, size_t nq, const uint64_t* p_bits,
+                     size_t np, size_t dnum, size_t hamming_weight, double sigma, double scale,
+                     const int64_t* rotations, size_t nrot) {
+    RefCtx* out = nullptr;
+    const int rc = guarded([&] {
+        CKKSParamsConfig cfg;
+        cfg.secure = false;
+        cfg.bts_keys = false;
+        cfg.N = N;
+        cfg.q_bits.assign(q_bits, q_bits + nq);
+        cfg.mult_depth = nq - 1;
+        cfg.q0_bit = q_bits[0];
+        cfg.q_bit = nq > 1 ? q_bits[1] : q_bits[0];
+        cfg.p_bits.assign(p_bits, p_bits + np);
+        cfg.pmoduli_count = np;
+        cfg.dnum = dnum;
+        cfg.secret_key_hamming_weight = hamming_weight;
+        cfg.sigma = sigma;
+        cfg.scale = scale;
+        cfg.rotate_values.assign(rotations, rotations + nrot);
+        out = new RefCtx(CKKSParams(std::move(cfg)));
+    });
+    return rc == 0 ? out : nullptr;
+}
+
+void ref_ctx_destroy(void* h) { delete static_cast<RefCtx*>(h); }
+
+int ref_ctx_moduli(void* h, uint64_t* q_out, size_t* nq, uint64_t* p_out, size_t* np) {
+    return guarded([&] {
+        const auto& p = static_cast<RefCtx*>(h)->ctx.getParams();
+        *nq = p.getModuli().size();
+        *np = p.getPModuli().size();
+        if (q_out) std::copy(p.getModuli().begin(), p.getModuli().end(), q_out);
+        if (p_out) std::copy(p.getPModuli().begin(), p.getPModuli().end(), p_out);
+    });
+}
+
+// Forward/inverse NTT of `limbs` consecutive Q limbs (limb-major, N each).
+int ref_ctx_ntt(void* h, uint64_t* poly, size_t limbs, int inverse, int lazy) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const auto& p = c.getParams();
+        if (inverse)
+            ntt_inverse_rns_flat_inplace(poly, p.getN(), limbs, p.getModuli(), c.getTwiddleNtt(), lazy != 0);
+        else
+            ntt_forward_rns_flat_inplace(poly, p.getN(), limbs, p.getModuli(), c.getTwiddleNtt(), lazy != 0);
+    });
+}
+
+// kind: 0 = rotation (by `rot`), 1 = conjugation, 2 = relinearization.
+int ref_ctx_key_shape(void* h, int kind, int64_t rot, size_t* parts, size_t* key_level) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        std::span<const CKKSCiphertext> k =
+            kind == 0 ? c.getRotationKey(rot)
+                      : (kind == 1 ? c.getConjugationKey() : c.getRelinHybrid(c.getParams().getMaxLevel()));
+        *parts = k.size();
+        *key_level = k.empty() ? 0 : k.front().getLevel();
+    });
+}
+
+int ref_ctx_key(void* h, int kind, int64_t rot, uint64_t* flat) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        std::span<const CKKSCiphertext> k =
+            kind == 0 ? c.getRotationKey(rot)
+                      : (kind == 1 ? c.getConjugationKey() : c.getRelinHybrid(c.getParams().getMaxLevel()));
+        keys_to_flat(k, flat);
+    });
+}
+
+// NTT-domain automorphism map (dst -> src) used by rotation (kind 0) or conjugation (kind 1).
+int ref_ctx_map(void* h, int kind, int64_t rot, uint64_t* map_out) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const auto& m = kind == 0 ? c.getRotationNttMap(rot) : c.getConjugationNttMap();
+        for (size_t i = 0; i < m.size(); ++i) map_out[i] = m[i];
+    });
+}
+
+// Secret key in NTT form for every Q limb: [limb][N].
+int ref_ctx_secret(void* h, uint64_t* out) {
+    return guarded([&] {
+        const auto& sk = static_cast<RefCtx*>(h)->ctx.getSecretKey();
+        size_t off = 0;
+        for (const auto& limb : sk) {
+            std::memcpy(out + off, limb.data(), limb.size() * sizeof(uint64_t));
+            off += limb.size();
+        }
+    });
+}
+
+// Hybrid key switch with caller-supplied key material (flat layout as above).
+int ref_keyswitch(void* h, size_t level, uint64_t* key_term, const uint64_t* key_flat, size_t parts,
+                  size_t key_level, uint64_t* b, uint64_t* a, int b_add, int a_add, int montgomery) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t L = level + 1;
+        auto keys = keys_from_flat(key_flat, parts, key_level, c.getParams().getPModuli().size(), N);
+        auto kt = copy_in(key_term, L * N);
+        auto bv = copy_in(b, L * N);
+        auto av = copy_in(a, L * N);
+        ckks_hybrid_key_switch_inplace(
+            c, level, kt, std::span<const CKKSCiphertext>(keys.data(), keys.size()), bv, av,
+            b_add ? CKKSHybridKeySwitchCombine::Add : CKKSHybridKeySwitchCombine::Assign,
+            a_add ? CKKSHybridKeySwitchCombine::Add : CKKSHybridKeySwitchCombine::Assign,
+            montgomery != 0);
+        copy_out(bv, b);
+        copy_out(av, a);
+    });
+}
+
+// In-place ciphertext ops on (b, a) buffers of (level+1)*N residues each.
+int ref_rotate(void* h, size_t level, uint64_t* b, uint64_t* a, int64_t rot) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t n = (level + 1) * c.getParams().getN();
+        CKKSCiphertext ct(c.getParams().getN(), copy_in(a, n), copy_in(b, n), 1.0L, level);
+        ckks_rotate_inplace(c, ct, rot);
+        copy_out(ct.getB(), b);
+        copy_out(ct.getA(), a);
+    });
+}
+
+int ref_conjugate(void* h, size_t level, uint64_t* b, uint64_t* a) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t n = (level + 1) * c.getParams().getN();
+        CKKSCiphertext ct(c.getParams().getN(), copy_in(a, n), copy_in(b, n), 1.0L, level);
+        ckks_conjugate_inplace(c, ct);
+        copy_out(ct.getB(), b);
+        copy_out(ct.getA(), a);
+    });
+}
+
+// (b1,a1) <- tensor with (b2,a2); writes c0 -> b1, c1 -> a1, c2 -> c2_out.
+int ref_mul(void* h, size_t level, uint64_t* b1, uint64_t* a1, const uint64_t* b2, const uint64_t* a2,
+            uint64_t* c2_out) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        CKKSCiphertext x(N, copy_in(a1, n), copy_in(b1, n), 1.0L, level);
+        CKKSCiphertext y(N, copy_in(a2, n), copy_in(b2, n), 1.0L, level);
+        ckks_mul_inplace(c, x, y);
+        copy_out(x.getB(), b1);
+        copy_out(x.getA(), a1);
+        copy_out(x.getPoly(2), c2_out);
+    });
+}
+
+int ref_relin(void* h, size_t level, uint64_t* c0, uint64_t* c1, const uint64_t* c2) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        MyVector<MyVector<uint64_t>> polys;
+        polys.emplace_back(copy_in(c0, n));
+        polys.emplace_back(copy_in(c1, n));
+        polys.emplace_back(copy_in(c2, n));
+        CKKSCiphertext ct(N, std::move(polys), 1.0L, level);
+        ckks_relin_hybrid_inplace(c, ct);
+        copy_out(ct.getB(), c0);
+        copy_out(ct.getA(), c1);
+    });
+}
+
+// Rescale `npolys` polynomials stored back to back ((level+1)*N each); the output keeps the
+// same stride but only the first level*N residues of each polynomial are meaningful.
+int ref_rescale(void* h, size_t level, size_t npolys, uint64_t* polys_flat) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        MyVector<MyVector<uint64_t>> polys;
+        for (size_t i = 0; i < npolys; ++i) polys.emplace_back(copy_in(polys_flat + i * n, n));
+        CKKSCiphertext ct(N, std::move(polys), 1.0L, level);
+        ckks_rescale(c, ct);
+        for (size_t i = 0; i < npolys; ++i)
+            std::memcpy(polys_flat + i * n, ct.getPoly(i).data(), level * N * sizeof(uint64_t));
+    });
+}
+
+// Hoisted rotations: one hoist of `a`, then one switch per rotation (rotation-key maps applied).
+// out layout: [rot][poly: b then a][limb][N].
+int ref_hoisted_rotations(void* h, size_t level, const uint64_t* b, const uint64_t* a,
+                          const int64_t* rots, size_t nrot, uint64_t* out) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        CKKSCiphertext ct(N, copy_in(a, n), copy_in(b, n), 1.0L, level);
+        CKKSHoistWorkspace ws;
+        CKKSEvalHoistedCiphertextQP hoisted;
+        ckks_hoist_ciphertext_a_qp_eval(c, ct, ws, hoisted);
+        for (size_t r = 0; r < nrot; ++r) {
+            MyVector<uint64_t> bo = copy_in(b, n);
+            MyVector<uint64_t> ao(n, 0);
+            const auto& map = c.getRotationNttMap(rots[r]);
+            ckks_hybrid_key_switch_hoisted_inplace(
+                c, hoisted, c.getRotationKey(rots[r]), bo, ao, CKKSHybridKeySwitchCombine::Add,
+                CKKSHybridKeySwitchCombine::Assign, c.getParams().montgomery,
+                std::span<const size_t>(map.data(), map.size()));
+            copy_out(bo, out + (r * 2 + 0) * n);
+            copy_out(ao, out + (r * 2 + 1) * n);
+        }
+    });
+}
+
+// The batched-ops workload on the reference CPU path: for each ciphertext i at level[i],
+// multiply by its partner, relinearize, rescale and rotate by rots[i], with OpenMP over
+// ciphertexts (the way the reference parallelizes independent ciphertexts).  Buffers hold
+// (level_max+1)*N residues per polynomial; x_b/x_a are updated in place (rescaled level).
+// Returns the wall time in seconds through *seconds.
+int ref_batched_ops(void* h, size_t count, const size_t* levels, uint64_t* x_b, uint64_t* x_a,
+                    const uint64_t* y_b, const uint64_t* y_a, const int64_t* rots, size_t stride,
+                    int threads, double* seconds) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        std::string err;
+        const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic) num_threads(threads)
+        for (std::ptrdiff_t i = 0; i < static_cast<std::ptrdiff_t>(count); ++i) {
+            try {
+                const size_t level = levels[i];
+                const size_t n = (level + 1) * N;
+                const size_t off = static_cast<size_t>(i) * stride;
+                CKKSCiphertext x(N, copy_in(x_a + off, n), copy_in(x_b + off, n), 1.0L, level);
+                CKKSCiphertext y(N, copy_in(y_a + off, n), copy_in(y_b + off, n), 1.0L, level);
+                ckks_mul_inplace(c, x, y);
+                ckks_relin_hybrid_inplace(c, x);
+                ckks_rescale(c, x);
+                ckks_rotate_inplace(c, x, rots[i]);
+                std::memcpy(x_b + off, x.getB().data(), x.getB().size() * sizeof(uint64_t));
+                std::memcpy(x_a + off, x.getA().data(), x.getA().size() * sizeof(uint64_t));
+            } catch (const std::exception& e) {
+#pragma omp critical
+                err = e.what();
+            }
+        }
+        const auto t1 = std::chrono::steady_clock::now();
+        *seconds = std::chrono::duration<double>(t1 - t0).count();
+        if (!err.empty()) throw std::runtime_error(err);
+    });
+}
+
+int ref_max_threads(void) { return omp_get_max_threads(); }
+
+}  // extern "C"
