@@ -1,0 +1,354 @@
+// C ABI (include/walsh_gpu.h): argument checks, key registry, workspace routing and the
+// operation sequences of rotation, conjugation, relinearization and the batched workload.
+#include <cstring>
+#include <string>
+
+#include "../../include/walsh_gpu.h"
+#include "wg_internal.hpp"
+
+namespace wg {
+Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t* p, size_t np, size_t dnum,
+                        int device);
+}
+
+struct wg_context {
+    wg::Context* c;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        g_err.clear();
+        return WG_OK;
+    } catch (const wg::Error& e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return WG_ERR_RUNTIME;
+    } catch (...) {
+        g_err = "unknown error";
+        return WG_ERR_RUNTIME;
+    }
+}
+
+wg::Context& C(wg_context* h) {
+    if (!h || !h->c) wg::fail(wg::kInvalid, "null context");
+    return *h->c;
+}
+
+cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int64_t normalize_rotation(const wg::Context& c, int64_t r) {
+    const int64_t slots = (int64_t)(c.N / 2);
+    r %= slots;
+    if (r < 0) r += slots;
+    return r;
+}
+
+uint64_t rotation_galois(const wg::Context& c, int64_t r) { return wg::host::powmod(5, (uint64_t)r, 2 * c.N); }
+
+void check_level(const wg::Context& c, size_t level, const char* who) {
+    if (level >= c.nq) wg::fail(wg::kInvalid, std::string(who) + ": invalid ciphertext level");
+}
+void check_ptr(const void* p, const char* who) {
+    if (!p) wg::fail(wg::kInvalid, std::string(who) + ": null buffer");
+}
+
+void do_rotate(wg::Context& c, size_t level, uint64_t* b, uint64_t* a, int64_t rotation, cudaStream_t s) {
+    const int64_t r = normalize_rotation(c, rotation);
+    if (r == 0) return;
+    const wg::KeyEntry& k = c.key(WG_KEY_ROTATION, r);
+    wg::keyswitch(c, level, a, k, b, a, b, a, true, false, rotation_galois(c, r), c.workspace(s), s);
+}
+
+void do_relin(wg::Context& c, size_t level, uint64_t* c0, uint64_t* c1, const uint64_t* c2, cudaStream_t s) {
+    const wg::KeyEntry& k = c.key(WG_KEY_RELIN, 0);
+    wg::keyswitch(c, level, c2, k, c0, c1, c0, c1, true, true, 0, c.workspace(s), s);
+}
+
+uint64_t* scratch_after_switch(wg::Context& c, cudaStream_t s) {
+    return c.workspace(s) + wg::keyswitch_workspace_words(c, c.nq - 1);
+}
+
+void do_rescale(wg::Context& c, size_t level, uint64_t* polys, size_t npolys, size_t stride, cudaStream_t s) {
+    uint64_t* ws = scratch_after_switch(c, s);
+    for (size_t k = 0; k < npolys; k += 2) {
+        const int n = (int)std::min<size_t>(2, npolys - k);
+        wg::rescale(c, level, polys + k * stride, n, stride, ws, s);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* wg_last_error(void) { return g_err.c_str(); }
+int wg_version(void) { return 100; }
+
+int wg_find_primes(const uint64_t* p_bits, size_t np, const uint64_t* q_bits, size_t nq, uint64_t N,
+                   uint64_t* p_out, uint64_t* q_out) {
+    return guard([&] {
+        if (!N || (N & (N - 1))) wg::fail(wg::kInvalid, "N must be a power of two");
+        std::vector<uint64_t> pb(p_bits, p_bits + np), qb(q_bits, q_bits + nq), p, q;
+        wg::host::find_primes(pb, qb, N, p, q);
+        std::memcpy(p_out, p.data(), np * 8);
+        std::memcpy(q_out, q.data(), nq * 8);
+    });
+}
+
+int wg_ctx_create(uint64_t N, const uint64_t* q, size_t nq, const uint64_t* p, size_t np, size_t dnum, int device,
+                  wg_context** out) {
+    return guard([&] {
+        if (!out || !q || !p) wg::fail(wg::kInvalid, "wg_ctx_create: null argument");
+        *out = nullptr;
+        wg::Context* c = wg::create_context(N, q, nq, p, np, dnum, device);
+        *out = new wg_context{c};
+    });
+}
+
+void wg_ctx_destroy(wg_context* ctx) {
+    if (!ctx) return;
+    delete ctx->c;
+    delete ctx;
+}
+
+int wg_ctx_set_key(wg_context* ctx, int kind, int64_t rotation, const uint64_t* host_key, size_t parts,
+                   size_t key_level) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(host_key, "wg_ctx_set_key");
+        if (kind != WG_KEY_RELIN && kind != WG_KEY_CONJ && kind != WG_KEY_ROTATION)
+            wg::fail(wg::kInvalid, "wg_ctx_set_key: unknown key kind");
+        if (key_level >= c.nq) wg::fail(wg::kInvalid, "wg_ctx_set_key: key level out of range");
+        if (parts < c.parts_at(key_level) || parts > 16) wg::fail(wg::kInvalid, "wg_ctx_set_key: invalid part count");
+        const int64_t r = kind == WG_KEY_ROTATION ? normalize_rotation(c, rotation) : 0;
+        if (kind == WG_KEY_ROTATION && r == 0) wg::fail(wg::kInvalid, "wg_ctx_set_key: zero rotation needs no key");
+        const size_t words = parts * 2 * (key_level + 1 + c.np) * c.N;
+        wg::KeyEntry e;
+        e.parts = parts;
+        e.key_level = key_level;
+        wg::check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+        if (cudaMalloc(&e.d_data, words * 8) != cudaSuccess) {
+            cudaGetLastError();
+            wg::fail(wg::kNoMemory, "wg_ctx_set_key: device allocation failed");
+        }
+        if (cudaMemcpy(e.d_data, host_key, words * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFree(e.d_data);
+            wg::fail(wg::kCuda, "wg_ctx_set_key: upload failed");
+        }
+        auto it = c.keys.find({kind, r});
+        if (it != c.keys.end()) {
+            cudaFree(it->second.d_data);
+            it->second = e;
+        } else {
+            c.keys.emplace(std::make_pair(kind, r), e);
+        }
+    });
+}
+
+int wg_ctx_has_key(const wg_context* ctx, int kind, int64_t rotation) {
+    if (!ctx || !ctx->c) return 0;
+    const int64_t r = kind == WG_KEY_ROTATION ? normalize_rotation(*ctx->c, rotation) : 0;
+    if (kind == WG_KEY_ROTATION && r == 0) return 1;
+    return ctx->c->keys.count({kind, r}) ? 1 : 0;
+}
+
+int wg_ctx_reserve(wg_context* ctx, void* stream) {
+    return guard([&] { C(ctx).workspace(S(stream)); });
+}
+
+size_t wg_ctx_workspace_words(const wg_context* ctx) { return ctx && ctx->c ? ctx->c->workspace_words() : 0; }
+
+static int ntt_call(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, int basis, size_t polys,
+                    size_t stride, void* stream, bool fwd) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(poly, "ntt");
+        const size_t avail = basis ? c.np : c.nq;
+        if (basis != 0 && basis != 1) wg::fail(wg::kInvalid, "ntt: basis must be 0 (Q) or 1 (P)");
+        if (first + limbs > avail) wg::fail(wg::kInvalid, "ntt: limb range exceeds the modulus chain");
+        if (polys > 1 && stride < limbs * c.N) wg::fail(wg::kInvalid, "ntt: polynomial stride too small");
+        const wg::LimbMap map = basis ? wg::LimbMap{0, 0, (int)(c.nq + first)} : wg::LimbMap{(int)limbs, (int)first, 0};
+        if (fwd)
+            wg::ntt_forward(c, poly, (int)limbs, (int)polys, stride, map, S(stream));
+        else
+            wg::ntt_inverse(c, poly, (int)limbs, (int)polys, stride, map, S(stream));
+    });
+}
+
+int wg_ntt_forward(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, int basis, size_t polys,
+                   size_t poly_stride, void* stream) {
+    return ntt_call(ctx, poly, limbs, first, basis, polys, poly_stride, stream, true);
+}
+int wg_ntt_inverse(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, int basis, size_t polys,
+                   size_t poly_stride, void* stream) {
+    return ntt_call(ctx, poly, limbs, first, basis, polys, poly_stride, stream, false);
+}
+
+int wg_keyswitch(wg_context* ctx, size_t level, const uint64_t* key_term, int kind, int64_t rotation, uint64_t* b,
+                 uint64_t* a, int b_add, int a_add, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_level(c, level, "ckks_hybrid_keyswitch");
+        check_ptr(key_term, "ckks_hybrid_keyswitch");
+        check_ptr(b, "ckks_hybrid_keyswitch");
+        check_ptr(a, "ckks_hybrid_keyswitch");
+        const int64_t r = kind == WG_KEY_ROTATION ? normalize_rotation(c, rotation) : 0;
+        const wg::KeyEntry& k = c.key(kind, r);
+        wg::keyswitch(c, level, key_term, k, b, a, b, a, b_add != 0, a_add != 0, 0, c.workspace(S(stream)),
+                      S(stream));
+    });
+}
+
+int wg_rotate(wg_context* ctx, size_t level, uint64_t* b, uint64_t* a, int64_t rotation, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_level(c, level, "ckks_rotate");
+        check_ptr(b, "ckks_rotate");
+        check_ptr(a, "ckks_rotate");
+        do_rotate(c, level, b, a, rotation, S(stream));
+    });
+}
+
+int wg_conjugate(wg_context* ctx, size_t level, uint64_t* b, uint64_t* a, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_level(c, level, "ckks_conjugate");
+        check_ptr(b, "ckks_conjugate");
+        check_ptr(a, "ckks_conjugate");
+        const wg::KeyEntry& k = c.key(WG_KEY_CONJ, 0);
+        const size_t n = (level + 1) * c.N;
+        uint64_t* pb = scratch_after_switch(c, S(stream));
+        uint64_t* pa = pb + n;
+        const uint64_t g = 2 * c.N - 1;
+        wg::automorphism(c, b, pb, (int)(level + 1), 1, 0, g, S(stream));
+        wg::automorphism(c, a, pa, (int)(level + 1), 1, 0, g, S(stream));
+        wg::keyswitch(c, level, pa, k, pb, pa, b, a, true, false, 0, c.workspace(S(stream)), S(stream));
+    });
+}
+
+int wg_rotate_many(wg_context* ctx, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rotations,
+                   size_t nrot, uint64_t* out, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_level(c, level, "ckks_rotate");
+        check_ptr(b, "ckks_rotate");
+        check_ptr(a, "ckks_rotate");
+        check_ptr(out, "ckks_rotate");
+        const size_t n = (level + 1) * c.N;
+        for (size_t r = 0; r < nrot; ++r) c.key(WG_KEY_ROTATION, normalize_rotation(c, rotations[r]));
+        for (size_t r = 0; r < nrot; ++r) {
+            uint64_t* ob = out + (2 * r) * n;
+            uint64_t* oa = ob + n;
+            wg::check_cuda(cudaMemcpyAsync(ob, b, n * 8, cudaMemcpyDeviceToDevice, S(stream)), "copy");
+            wg::check_cuda(cudaMemcpyAsync(oa, a, n * 8, cudaMemcpyDeviceToDevice, S(stream)), "copy");
+            do_rotate(c, level, ob, oa, rotations[r], S(stream));
+        }
+    });
+}
+
+int wg_mul(wg_context* ctx, size_t level, uint64_t* b1, uint64_t* a1, const uint64_t* b2, const uint64_t* a2,
+           uint64_t* c2, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_level(c, level, "ckks_mul_inplace(ct,ct)");
+        for (const void* p : {(const void*)b1, (const void*)a1, (const void*)b2, (const void*)a2, (const void*)c2})
+            check_ptr(p, "ckks_mul_inplace(ct,ct)");
+        wg::tensor(c, level, b1, a1, b2, a2, c2, S(stream));
+    });
+}
+
+int wg_relin(wg_context* ctx, size_t level, uint64_t* c0, uint64_t* c1, const uint64_t* c2, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_level(c, level, "ckks_relin");
+        check_ptr(c0, "ckks_relin");
+        check_ptr(c1, "ckks_relin");
+        check_ptr(c2, "ckks_relin");
+        do_relin(c, level, c0, c1, c2, S(stream));
+    });
+}
+
+int wg_rescale(wg_context* ctx, size_t level, uint64_t* polys, size_t npolys, size_t poly_stride, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        if (level == 0 || level >= c.nq) wg::fail(wg::kInvalid, "ckks_rescale: invalid level");
+        check_ptr(polys, "ckks_rescale");
+        if (npolys == 0) wg::fail(wg::kInvalid, "ckks_rescale: empty ciphertext");
+        if (npolys > 1 && poly_stride < (level + 1) * c.N) wg::fail(wg::kInvalid, "ckks_rescale: stride too small");
+        do_rescale(c, level, polys, npolys, poly_stride, S(stream));
+    });
+}
+
+static int add_sub_call(wg_context* ctx, size_t level, uint64_t* x, const uint64_t* y, size_t npolys, size_t stride,
+                        void* stream, bool sub) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_level(c, level, sub ? "ckks_sub_inplace" : "ckks_add_inplace");
+        check_ptr(x, "ckks_add_inplace");
+        check_ptr(y, "ckks_add_inplace");
+        if (npolys > 1 && stride < (level + 1) * c.N) wg::fail(wg::kInvalid, "ckks_add_inplace: stride too small");
+        wg::add_sub(c, level, x, y, (int)npolys, stride, sub, S(stream));
+    });
+}
+int wg_add(wg_context* ctx, size_t level, uint64_t* x, const uint64_t* y, size_t npolys, size_t poly_stride,
+           void* stream) {
+    return add_sub_call(ctx, level, x, y, npolys, poly_stride, stream, false);
+}
+int wg_sub(wg_context* ctx, size_t level, uint64_t* x, const uint64_t* y, size_t npolys, size_t poly_stride,
+           void* stream) {
+    return add_sub_call(ctx, level, x, y, npolys, poly_stride, stream, true);
+}
+
+int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_t* levels, uint64_t* const* xb,
+                                      uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                                      const int64_t* rots, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        cudaStream_t s = S(stream);
+        for (size_t i = 0; i < count; ++i) {
+            if (levels[i] == 0 || levels[i] >= c.nq) wg::fail(wg::kInvalid, "batch: ciphertext level must be in [1, L)");
+            const int64_t r = normalize_rotation(c, rots[i]);
+            if (r) c.key(WG_KEY_ROTATION, r);
+        }
+        c.key(WG_KEY_RELIN, 0);
+        uint64_t* c2 = scratch_after_switch(c, s) + 2 * c.nq * c.N;
+        for (size_t i = 0; i < count; ++i) {
+            const size_t lv = levels[i];
+            wg::tensor(c, lv, xb[i], xa[i], yb[i], ya[i], c2, s);
+            do_relin(c, lv, xb[i], xa[i], c2, s);
+            do_rescale(c, lv, xb[i], 1, 0, s);
+            do_rescale(c, lv, xa[i], 1, 0, s);
+            do_rotate(c, lv - 1, xb[i], xa[i], rots[i], s);
+        }
+    });
+}
+
+int wg_malloc(void** ptr, size_t bytes) {
+    return guard([&] {
+        if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            wg::fail(wg::kNoMemory, "cudaMalloc failed");
+        }
+    });
+}
+int wg_free(void* ptr) {
+    return guard([&] { wg::check_cuda(cudaFree(ptr), "cudaFree"); });
+}
+int wg_memcpy_htod(void* dst, const void* src, size_t bytes, void* stream) {
+    return guard([&] { wg::check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, S(stream)), "memcpy"); });
+}
+int wg_memcpy_dtoh(void* dst, const void* src, size_t bytes, void* stream) {
+    return guard([&] { wg::check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, S(stream)), "memcpy"); });
+}
+int wg_stream_synchronize(void* stream) {
+    return guard([&] { wg::check_cuda(cudaStreamSynchronize(S(stream)), "cudaStreamSynchronize"); });
+}
+
+}  // extern "C"

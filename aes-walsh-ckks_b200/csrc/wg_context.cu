@@ -1,0 +1,131 @@
+// Context construction: the host tables (wg_tables.cpp) uploaded once into device-resident
+// buffers, per-stream scratch and the switching-key registry.
+#include <algorithm>
+#include <cstring>
+
+#include "wg_internal.hpp"
+#include "wg_tables.hpp"
+
+namespace wg {
+
+Context::~Context() {
+    for (auto& kv : keys) cudaFree(kv.second.d_data);
+    for (auto& kv : workspaces) cudaFree(kv.second.base);
+    cudaFree(d_mod);
+    cudaFree(d_tw);
+    cudaFree(d_tables);
+}
+
+size_t Context::workspace_words() const {
+    // the largest switch plus room for a permuted copy of a ciphertext (conjugation) and the
+    // rescale remainders
+    return keyswitch_workspace_words(*this, nq - 1) + 4 * nq * N;
+}
+
+uint64_t* Context::workspace(cudaStream_t s) {
+    std::lock_guard<std::mutex> g(ws_mutex);
+    auto it = workspaces.find(s);
+    if (it != workspaces.end()) return it->second.base;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (s) cudaStreamIsCapturing(s, &cs);
+    if (cs != cudaStreamCaptureStatusNone)
+        fail(kRuntime, "workspace for this stream must be reserved (wg_ctx_reserve) before graph capture");
+    Workspace w;
+    w.words = workspace_words();
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    if (cudaMalloc(&w.base, w.words * 8) != cudaSuccess) {
+        cudaGetLastError();
+        fail(kNoMemory, "workspace allocation failed");
+    }
+    workspaces.emplace(s, w);
+    return w.base;
+}
+
+const KeyEntry& Context::key(int kind, int64_t rotation) const {
+    auto it = keys.find({kind, rotation});
+    if (it == keys.end()) fail(kRuntime, "switching key is unavailable");
+    return it->second;
+}
+
+Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t* p, size_t np, size_t dnum,
+                        int device) {
+    if (N < 1024 || N > 65536 || (N & (N - 1))) fail(kInvalid, "ring degree must be a power of two in [2^10, 2^16]");
+    if (nq == 0 || np == 0) fail(kInvalid, "hybrid key switching needs at least one Q and one P modulus");
+    if (np > (size_t)16) fail(kInvalid, "at most 16 P moduli are supported");
+    if (dnum == 0 || dnum > nq) fail(kInvalid, "invalid hybrid key-switch partition count");
+    for (size_t i = 0; i < nq + np; ++i) {
+        const uint64_t m = i < nq ? q[i] : p[i - nq];
+        if (m >= (uint64_t{1} << 62) || m < 3 || (m - 1) % (2 * N)) fail(kInvalid, "moduli must be primes 1 mod 2N below 2^62");
+    }
+    if ((nq + dnum - 1) / dnum > 16) fail(kInvalid, "digit width above 16 limbs is not supported");
+    auto c = std::make_unique<Context>();
+    c->device = device;
+    c->N = N;
+    c->logN = __builtin_ctzll(N);
+    c->nq = nq;
+    c->np = np;
+    c->dnum = dnum;
+    c->alpha = (nq + dnum - 1) / dnum;
+    c->q.assign(q, q + nq);
+    c->p.assign(p, p + np);
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    HostTables H = build_tables(N, q, nq, p, np, dnum);
+    c->mods = H.mods;
+    const size_t nm = nq + np;
+
+    // Upload.
+    auto dev_alloc = [&](void** ptr, size_t bytes) {
+        if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            fail(kNoMemory, "device allocation failed while building the context");
+        }
+    };
+    dev_alloc((void**)&c->d_mod, nm * sizeof(Modulus));
+    dev_alloc((void**)&c->d_tw, H.tw.size() * 8);
+    c->tables_words = H.words.size() + 1;
+    dev_alloc((void**)&c->d_tables, c->tables_words * 8);
+    check_cuda(cudaMemcpy(c->d_mod, c->mods.data(), nm * sizeof(Modulus), cudaMemcpyHostToDevice), "upload moduli");
+    check_cuda(cudaMemcpy(c->d_tw, H.tw.data(), H.tw.size() * 8, cudaMemcpyHostToDevice), "upload twiddles");
+    check_cuda(cudaMemcpy(c->d_tables, H.words.data(), H.words.size() * 8, cudaMemcpyHostToDevice),
+               "upload tables");
+    const uint64_t* T = c->d_tables;
+    c->modup.resize(nq);
+    for (size_t level = 0; level < nq; ++level) {
+        for (size_t part = 0; part < H.modup[level].size(); ++part) {
+            const ModUpOffsets& o = H.modup[level][part];
+            ModUpDesc d;
+            d.src_count = o.src_count;
+            d.dst_count = o.dst_count;
+            d.src_first = o.src_first;
+            d.pad = 0;
+            d.qhat_inv = T + o.qhat_inv;
+            d.qhat_inv_s = T + o.qhat_inv_s;
+            d.src_inv = reinterpret_cast<const double*>(T + o.src_inv);
+            d.qhat = T + o.qhat;
+            d.qhat_s = T + o.qhat_s;
+            d.corr = T + o.corr;
+            d.dst_limb = reinterpret_cast<const int*>(T + o.dst_limb);
+            d.dst_mod = reinterpret_cast<const int*>(T + o.dst_mod);
+            c->modup[level].push_back(d);
+        }
+    }
+    c->fold_inv.resize(nq);
+    c->fold_inv_s.resize(nq);
+    for (size_t level = 0; level < nq; ++level) {
+        c->fold_inv[level] = T + H.fold_inv[level];
+        c->fold_inv_s[level] = T + H.fold_inv_s[level];
+    }
+    c->rs_one_s.assign(nq, nullptr);
+    c->rs_inv_p.assign(nq, nullptr);
+    c->rs_inv_p_s.assign(nq, nullptr);
+    c->rs_half.assign(nq, nullptr);
+    for (size_t d = 1; d < nq; ++d) {
+        c->rs_one_s[d] = T + H.rescale[d];
+        c->rs_inv_p[d] = T + H.rescale[d] + d;
+        c->rs_inv_p_s[d] = T + H.rescale[d] + 2 * d;
+        c->rs_half[d] = T + H.rescale[d] + 3 * d;
+    }
+    return c.release();
+}
+
+}  // namespace wg

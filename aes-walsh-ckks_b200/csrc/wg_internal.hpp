@@ -1,0 +1,178 @@
+// Internal declarations shared by the device library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "wg_arith.cuh"
+
+namespace wg {
+
+// Status codes of the C ABI (walsh_gpu.h): invalid arguments mirror the reference's
+// std::invalid_argument, missing keys or precomputed material its std::runtime_error.
+enum Status : int { kOk = 0, kInvalid = -1, kRuntime = -2, kCuda = -3, kNoMemory = -4 };
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+[[noreturn]] inline void fail(int code, const std::string& m) { throw Error(code, m); }
+inline void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) fail(kCuda, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------------------
+// Host-side precomputation (wg_host.cpp).  Restates the reference's context-build math.
+// ---------------------------------------------------------------------------------------
+namespace host {
+uint64_t mulmod(uint64_t a, uint64_t b, uint64_t m);
+uint64_t powmod(uint64_t a, uint64_t e, uint64_t m);
+uint64_t inverse(uint64_t a, uint64_t m);
+uint64_t shoup(uint64_t w, uint64_t q);
+void barrett_const(uint64_t q, uint64_t& lo, uint64_t& hi);
+uint64_t barrett_mul(uint64_t a, uint64_t b, uint64_t q, uint64_t lo, uint64_t hi);
+uint64_t mont_neg_inv(uint64_t q);
+void find_primes(const std::vector<uint64_t>& p_bits, const std::vector<uint64_t>& q_bits,
+                 uint64_t N, std::vector<uint64_t>& p, std::vector<uint64_t>& q);
+// Twiddles: fwd, fwd_shoup, inv, inv_shoup (N entries each), N^-1.
+void ntt_tables(uint64_t N, uint64_t q, uint64_t* fwd, uint64_t* fwd_s, uint64_t* inv,
+                uint64_t* inv_s, uint64_t& n_inv);
+}  // namespace host
+
+// ---------------------------------------------------------------------------------------
+// Device-side descriptors.
+// ---------------------------------------------------------------------------------------
+
+// Base change Q-digit -> (other Q limbs, P limbs) for one (level, digit); arrays in device
+// memory, row-major [dst][src] like the reference's ApproxCrtModUpPrecomp.
+struct ModUpDesc {
+    int src_count;
+    int dst_count;
+    int src_first;             // first Q limb of the digit
+    int pad;
+    const uint64_t* qhat_inv;  // [src]
+    const uint64_t* qhat_inv_s;
+    const double* src_inv;     // [src]
+    const uint64_t* qhat;      // [dst][src]
+    const uint64_t* qhat_s;
+    const uint64_t* corr;      // [dst][src+1]
+    const int* dst_limb;       // QP limb index written for each dst
+    const int* dst_mod;        // modulus index (into Context::d_mod) for each dst
+};
+
+struct KeyEntry {
+    uint64_t* d_data = nullptr;  // [part][a|b][key_level+1+K][N], Montgomery, folded
+    size_t parts = 0;
+    size_t key_level = 0;
+};
+
+struct Workspace {
+    uint64_t* base = nullptr;
+    size_t words = 0;
+};
+
+struct Context {
+    int device = 0;
+    uint64_t N = 0;
+    int logN = 0;
+    size_t nq = 0, np = 0, dnum = 0, alpha = 0;
+    std::vector<uint64_t> q, p;
+    std::vector<Modulus> mods;       // nq + np entries (P after Q)
+    Modulus* d_mod = nullptr;
+    uint64_t* d_tw = nullptr;        // [mod][4][N]: fwd, fwd_shoup, inv, inv_shoup
+    // ModUp descriptors, host copies holding device pointers: [level][part]
+    std::vector<std::vector<ModUpDesc>> modup;
+    uint64_t* d_tables = nullptr;    // backing store for all small tables
+    size_t tables_words = 0;
+    // folded ModDown constants per level: [qi][pi] inverse and Shoup
+    std::vector<const uint64_t*> fold_inv, fold_inv_s;
+    const double* d_p_inv = nullptr; // [pi] 1.0 / p
+    // rescale constants per dropped limb d: arrays of d entries (Shoup of 1, p^-1 and its
+    // Shoup companion, floor(p/2) mod q_i)
+    std::vector<const uint64_t*> rs_one_s, rs_inv_p, rs_inv_p_s, rs_half;
+    std::map<std::pair<int, int64_t>, KeyEntry> keys;
+    std::mutex ws_mutex;
+    std::map<cudaStream_t, Workspace> workspaces;  // one per stream, allocated on first use
+
+    ~Context();
+    uint64_t* workspace(cudaStream_t s);   // scratch for one in-flight operation on stream s
+    size_t workspace_words() const;
+    const KeyEntry& key(int kind, int64_t rotation) const;
+
+    size_t parts_at(size_t level) const {
+        if (level >= nq) return 0;
+        const size_t L = level + 1;
+        const size_t p_ = (L + alpha - 1) / alpha;
+        return p_ < dnum ? p_ : dnum;
+    }
+    const uint64_t* tw(int mod) const { return d_tw + (size_t)mod * 4 * N; }
+};
+
+// Modulus-index rule for a batch of limbs: limb l of a polynomial uses modulus
+// (l < nA ? firstA + l : firstB + l - nA).  Q moduli occupy [0, nq), P moduli [nq, nq+np).
+struct LimbMap {
+    int nA;
+    int firstA;
+    int firstB;
+    __host__ __device__ int operator()(int l) const { return l < nA ? firstA + l : firstB + (l - nA); }
+};
+
+// ---------------------------------------------------------------------------------------
+// Launch accounting.  Every kernel launch of the library goes through a Probe: it counts
+// launches and, when event timing is enabled for the launch's class, brackets it with a pair
+// of CUDA events on the launching stream and books its algorithmic bytes.
+// ---------------------------------------------------------------------------------------
+enum KernelClass : int {
+    kClsNtt = 0,       // NTT / inverse NTT phases
+    kClsModUp = 1,     // HPS base extension
+    kClsKeyMac = 2,    // key inner product
+    kClsModDown = 3,   // folded HPS ModDown
+    kClsCombine = 4,   // combine / automorphism gathers
+    kClsElementwise = 5,  // tensor, add/sub, rescale steps
+    kClsCount = 6
+};
+struct Probe {
+    Probe(int cls, double bytes, cudaStream_t s);
+    ~Probe();
+    Probe(const Probe&) = delete;
+    Probe& operator=(const Probe&) = delete;
+    int slot = -1;
+    cudaStream_t stream;
+};
+
+// ---------------------------------------------------------------------------------------
+// Kernel launchers.
+// ---------------------------------------------------------------------------------------
+// NTT over `polys` polynomials of `limbs` limbs each, `poly_stride` words apart.
+void ntt_forward(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride,
+                 LimbMap map, cudaStream_t s);
+void ntt_inverse(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride,
+                 LimbMap map, cudaStream_t s);
+
+// Key switch of key_term (level) with key `k`; b/a combine modes; optional automorphism
+// (galois != 0) applied to the outputs.  `ws` must hold keyswitch_workspace_words(level).
+size_t keyswitch_workspace_words(const Context& c, size_t level);
+// b = (b_add ? b_in + ks_b : ks_b), a likewise; b_in/a_in may alias b/a.
+void keyswitch(const Context& c, size_t level, const uint64_t* key_term, const KeyEntry& k,
+               const uint64_t* b_in, const uint64_t* a_in, uint64_t* b, uint64_t* a, bool b_add,
+               bool a_add, uint64_t galois, uint64_t* ws, cudaStream_t s);
+
+// Elementwise and structural kernels (wg_ops.cu).
+void automorphism(const Context& c, const uint64_t* src, uint64_t* dst, int limbs, int polys,
+                  size_t poly_stride, uint64_t galois, cudaStream_t s);
+void tensor(const Context& c, size_t level, uint64_t* b1, uint64_t* a1, const uint64_t* b2,
+            const uint64_t* a2, uint64_t* c2, cudaStream_t s);
+// Divide by the last active Q limb with rounding; ws holds npolys*level*N words.
+void rescale(const Context& c, size_t level, uint64_t* polys, int npolys, size_t poly_stride,
+             uint64_t* ws, cudaStream_t s);
+void add_sub(const Context& c, size_t level, uint64_t* x, const uint64_t* y, int npolys,
+             size_t poly_stride, bool subtract, cudaStream_t s);
+
+}  // namespace wg

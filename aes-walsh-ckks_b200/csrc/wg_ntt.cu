@@ -1,0 +1,129 @@
+// Negacyclic NTT / inverse NTT over batches of RNS limbs.
+//
+// Same transform as the reference's ntt_forward_dit2 / ntt_inverse_dif2 (src/math/ntt/ntt.cpp:
+// 235-386): forward Cooley-Tukey with psi-folded bit-reversed twiddles (natural order in,
+// bit-reversed out), inverse Gentleman-Sande with the mirrored table followed by N^-1.
+// Outputs are canonical ([0, q)).
+//
+// Device organisation (N = 2^n, n = n1 + n2, n1 = floor(n/2)):
+//   * the transform runs as two phases; the "column" phase owns the n1 high index bits, the
+//     "row" phase the n2 low bits.  Forward = columns then rows, inverse = rows then columns.
+//   * a CTA stages a 2048-element tile (or the whole limb for N < 2048) in shared memory with
+//     one pad word every 16 words, so strided 64-bit accesses stay at two wavefronts per warp;
+//   * each thread carries 8 elements through up to three radix-2 stages in registers per
+//     round (one shared-memory round trip per three stages);
+//   * grid.y indexes limbs and grid.z polynomials, so one launch covers a whole ciphertext
+//     batch; each limb picks its modulus through a LimbMap (Q limbs, P limbs or a mix).
+// Butterflies are Harvey/Shoup with lazy ranges: forward values stay in [0, 4q), inverse in
+// [0, 2q); the last phase canonicalises (forward) or scales by N^-1 with Shoup (inverse).
+#include <utility>
+
+#include "wg_internal.hpp"
+#include "wg_ntt.cuh"
+
+namespace wg {
+namespace {
+using namespace ntt;
+
+template <int LOGN, bool FWD, bool COLS, int... RD>
+__device__ __forceinline__ void ntt_rounds(std::integer_sequence<int, RD...>, uint64_t* sm, int sub,
+                                           int o, int tile, uint64_t q, const uint64_t* tw,
+                                           const uint64_t* tws) {
+    ((ntt_round<LOGN, FWD, COLS, RD>(sm, sub, o, tile, q, tw, tws), __syncthreads()), ...);
+}
+
+template <int LOGN, bool FWD, bool COLS>
+__global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS)
+    k_ntt_phase(uint64_t* __restrict__ data, size_t poly_stride, LimbMap map,
+                const Modulus* __restrict__ mods, const uint64_t* __restrict__ tw_base) {
+    using P = Phase<LOGN, FWD, COLS>;
+    constexpr int N = P::N;
+    __shared__ uint64_t sm[P::TILE + P::TILE / 16];
+
+    const int limb = blockIdx.y;
+    uint64_t* __restrict__ x = data + (size_t)blockIdx.z * poly_stride + (size_t)limb * N;
+    const int mi = map(limb);
+    const uint64_t q = mods[mi].q;
+    const uint64_t* tw = tw_base + (size_t)mi * 4 * N + (FWD ? 0 : 2 * N);
+    const uint64_t* tws = tw + N;
+    const int tile = blockIdx.x;
+    const int t = threadIdx.x;
+
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int e = t + k * P::THREADS;
+        sm[pad16(e)] = x[tile_offset<LOGN, FWD, COLS>(tile, e)];
+    }
+    __syncthreads();
+
+    const int sub = COLS ? t % P::SUBS : t >> P::OB;
+    const int o = COLS ? t / P::SUBS : t & ((1 << P::OB) - 1);
+    ntt_rounds<LOGN, FWD, COLS>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, tile, q,
+                                tw, tws);
+
+    uint64_t n_inv = 0, n_inv_s = 0;
+    if (P::LAST && !FWD) {
+        n_inv = mods[mi].n_inv;
+        n_inv_s = mods[mi].n_inv_shoup;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int e = t + k * P::THREADS;
+        uint64_t val = sm[pad16(e)];
+        if (P::LAST) val = FWD ? red4q(val, q) : mul_shoup(val, n_inv, n_inv_s, q);
+        x[tile_offset<LOGN, FWD, COLS>(tile, e)] = val;
+    }
+}
+
+template <int LOGN, bool FWD, bool COLS>
+void launch_phase(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map,
+                  cudaStream_t s) {
+    using P = Phase<LOGN, FWD, COLS>;
+    const dim3 grid(P::N / P::TILE, limbs, polys);
+    // algorithmic bytes: every residue read once and written once
+    Probe probe(kClsNtt, 16.0 * P::N * limbs * polys, s);
+    k_ntt_phase<LOGN, FWD, COLS><<<grid, P::THREADS, 0, s>>>(data, stride, map, c.d_mod, c.d_tw);
+}
+
+template <int LOGN>
+void run(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map, bool fwd,
+         cudaStream_t s) {
+    if (fwd) {
+        launch_phase<LOGN, true, true>(c, data, limbs, polys, stride, map, s);
+        launch_phase<LOGN, true, false>(c, data, limbs, polys, stride, map, s);
+    } else {
+        launch_phase<LOGN, false, false>(c, data, limbs, polys, stride, map, s);
+        launch_phase<LOGN, false, true>(c, data, limbs, polys, stride, map, s);
+    }
+}
+
+void dispatch(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map, bool fwd,
+              cudaStream_t s) {
+    if (limbs <= 0 || polys <= 0) return;
+    if (polys > 65535 || limbs > 65535) fail(kInvalid, "ntt: too many limbs or polynomials in one batch");
+    switch (c.logN) {
+        case 10: run<10>(c, data, limbs, polys, stride, map, fwd, s); break;
+        case 11: run<11>(c, data, limbs, polys, stride, map, fwd, s); break;
+        case 12: run<12>(c, data, limbs, polys, stride, map, fwd, s); break;
+        case 13: run<13>(c, data, limbs, polys, stride, map, fwd, s); break;
+        case 14: run<14>(c, data, limbs, polys, stride, map, fwd, s); break;
+        case 15: run<15>(c, data, limbs, polys, stride, map, fwd, s); break;
+        case 16: run<16>(c, data, limbs, polys, stride, map, fwd, s); break;
+        default: fail(kInvalid, "ntt: ring degree must be 2^10 .. 2^16");
+    }
+    check_cuda(cudaGetLastError(), "ntt launch");
+}
+
+}  // namespace
+
+void ntt_forward(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride, LimbMap map,
+                 cudaStream_t s) {
+    dispatch(c, data, limbs, polys, poly_stride, map, true, s);
+}
+
+void ntt_inverse(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride, LimbMap map,
+                 cudaStream_t s) {
+    dispatch(c, data, limbs, polys, poly_stride, map, false, s);
+}
+
+}  // namespace wg

@@ -1,0 +1,138 @@
+// Index logic and butterflies of the two-phase NTT (see wg_ntt.cu), shared by the device
+// kernels and the CPU emulation test.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <utility>
+
+#include "wg_arith.cuh"
+
+namespace wg {
+namespace ntt {
+
+constexpr int kMaxTile = 2048;
+
+WG_HD int pad16(int e) { return e + (e >> 4); }
+WG_HD int insert_zero(int v, int g) {
+    return ((v >> g) << (g + 1)) | (v & ((1 << g) - 1));
+}
+
+// Bits handled by one round: up to three stage bits (in processing order) plus filler bits
+// (the lowest free bits) so every thread always owns 8 elements.
+struct RoundPlan {
+    int ns;
+    int sb[3];  // stage bits, processing order
+    int jb[3];  // position of each stage bit inside the 3-bit element index j
+    int g[3];   // group bits ascending
+};
+
+template <int MB, bool FWD>
+WG_HDC constexpr RoundPlan make_plan(int rd) {
+    RoundPlan p{0, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int k = 0; k < 3; ++k) {
+        const int b = FWD ? MB - 1 - 3 * rd - k : 3 * rd + k;
+        if (b >= 0 && b < MB) p.sb[p.ns++] = b;
+    }
+    int mask = 0;
+    for (int k = 0; k < p.ns; ++k) mask |= 1 << p.sb[k];
+    int filled = p.ns;
+    for (int b = 0; filled < 3; ++b)
+        if (!((mask >> b) & 1)) {
+            mask |= 1 << b;
+            ++filled;
+        }
+    int k = 0;
+    for (int b = 0; b < 32 && k < 3; ++b)
+        if ((mask >> b) & 1) p.g[k++] = b;
+    for (int s = 0; s < p.ns; ++s) p.jb[s] = p.sb[s] == p.g[0] ? 0 : (p.sb[s] == p.g[1] ? 1 : 2);
+    return p;
+}
+
+template <int LOGN, bool FWD, bool COLS>
+struct Phase {
+    static constexpr int N = 1 << LOGN;
+    static constexpr int NB1 = LOGN / 2;
+    static constexpr int NB2 = LOGN - NB1;
+    static constexpr int MB = COLS ? NB1 : NB2;
+    static constexpr int TILE = N < kMaxTile ? N : kMaxTile;
+    static constexpr int THREADS = TILE / 8;
+    static constexpr int SUBS = TILE >> MB;  // sub-transforms per tile
+    static constexpr int OB = MB - 3;
+    static constexpr int ROUNDS = (MB + 2) / 3;
+    static constexpr bool LAST = FWD ? !COLS : COLS;
+    static_assert(MB >= 3, "transform too small");
+};
+
+template <int LOGN, bool FWD, bool COLS, int RD>
+WG_HD void ntt_round(uint64_t* sm, int sub, int o, int tile, uint64_t q,
+                                          const uint64_t* __restrict__ tw,
+                                          const uint64_t* __restrict__ tws) {
+    using P = Phase<LOGN, FWD, COLS>;
+    constexpr RoundPlan plan = make_plan<P::MB, FWD>(RD);
+    const uint64_t two_q = q << 1;
+    int base = o;
+    base = insert_zero(base, plan.g[0]);
+    base = insert_zero(base, plan.g[1]);
+    base = insert_zero(base, plan.g[2]);
+    int h[8];
+    uint64_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        h[j] = base | ((j & 1) << plan.g[0]) | (((j >> 1) & 1) << plan.g[1]) | (((j >> 2) & 1) << plan.g[2]);
+        const int e = COLS ? h[j] * P::SUBS + sub : (sub << P::MB) | h[j];
+        v[j] = sm[pad16(e)];
+    }
+#pragma unroll
+    for (int s = 0; s < plan.ns; ++s) {
+        const int b = plan.sb[s];
+        const int jb = plan.jb[s];
+        const int gb = COLS ? P::NB2 + b : b;  // global index bit of this stage
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if ((j >> jb) & 1) continue;
+            const int j1 = j | (1 << jb);
+            // Twiddle index (1 << (n-1-gb)) + (x >> (gb+1)) for the pair's global index x.
+            size_t hi;
+            if (COLS) {
+                hi = (size_t)(h[j] >> (b + 1));
+            } else {
+                const size_t row = (size_t)tile * P::SUBS + sub;
+                hi = (row << (P::NB2 - b - 1)) + (size_t)(h[j] >> (b + 1));
+            }
+            const size_t idx = ((size_t)1 << (LOGN - 1 - gb)) + hi;
+            const uint64_t w = WG_LDG(tw + idx), ws = WG_LDG(tws + idx);
+            if (FWD) {
+                uint64_t t = v[j];
+                if (t >= two_q) t -= two_q;
+                const uint64_t u = mul_shoup_lazy(v[j1], w, ws, q);
+                v[j] = t + u;
+                v[j1] = t + two_q - u;
+            } else {
+                const uint64_t t = v[j], u = v[j1];
+                uint64_t sum = t + u;
+                if (sum >= two_q) sum -= two_q;
+                v[j] = sum;
+                v[j1] = mul_shoup_lazy(t - u + two_q, w, ws, q);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int e = COLS ? h[j] * P::SUBS + sub : (sub << P::MB) | h[j];
+        sm[pad16(e)] = v[j];
+    }
+}
+
+// Global offset (within one limb) of tile element e.
+template <int LOGN, bool FWD, bool COLS>
+WG_HD size_t tile_offset(int tile, int e) {
+    using P = Phase<LOGN, FWD, COLS>;
+    if (COLS) {
+        const int hh = e / P::SUBS, c = e % P::SUBS;
+        return ((size_t)hh << P::NB2) + (size_t)tile * P::SUBS + c;
+    }
+    return (size_t)tile * P::TILE + e;
+}
+
+}  // namespace ntt
+}  // namespace wg

@@ -1,0 +1,268 @@
+"""Python binding of libwalshgpu.so (include/walsh_gpu.h) over ctypes.
+
+The library is the product: every operation here is one C-ABI call that launches sm_100a
+kernels.  There is no CPU fallback -- importing this module fails loudly when the library is
+missing, and every call raises when the library reports an error.
+
+Device buffers are torch tensors (dtype int64 holding the uint64 residues bit for bit);
+torch only provides memory and the current CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "libwalshgpu.so")
+
+WG_KEY_RELIN = 0
+WG_KEY_CONJ = 1
+WG_KEY_ROTATION = 2
+
+
+class WalshGpuError(RuntimeError):
+    """Raised for a non-zero status of the C ABI; `code` is the WG_ERR_* value."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class InvalidArgument(WalshGpuError, ValueError):
+    """WG_ERR_INVALID -- the reference raises std::invalid_argument here."""
+
+
+def build(force: bool = False) -> str:
+    """Compile libwalshgpu.so in-tree for sm_100a (nvcc cross-compiles without a GPU)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-j8", "-C", PKG], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libwalshgpu.so is not built ({LIB_PATH}); run walshgpu.build()")
+        L = C.CDLL(LIB_PATH)
+        vp, sz, u64 = C.c_void_p, C.c_size_t, C.c_uint64
+        L.wg_last_error.restype = C.c_char_p
+        L.wg_version.restype = C.c_int
+        L.wg_find_primes.argtypes = [vp, sz, vp, sz, u64, vp, vp]
+        L.wg_ctx_create.argtypes = [u64, vp, sz, vp, sz, sz, C.c_int, C.POINTER(vp)]
+        L.wg_ctx_destroy.argtypes = [vp]
+        L.wg_ctx_destroy.restype = None
+        L.wg_ctx_set_key.argtypes = [vp, C.c_int, C.c_int64, vp, sz, sz]
+        L.wg_ctx_has_key.argtypes = [vp, C.c_int, C.c_int64]
+        L.wg_ctx_reserve.argtypes = [vp, vp]
+        L.wg_ctx_workspace_words.argtypes = [vp]
+        L.wg_ctx_workspace_words.restype = sz
+        for f in (L.wg_ntt_forward, L.wg_ntt_inverse):
+            f.argtypes = [vp, vp, sz, sz, C.c_int, sz, sz, vp]
+        L.wg_keyswitch.argtypes = [vp, sz, vp, C.c_int, C.c_int64, vp, vp, C.c_int, C.c_int, vp]
+        L.wg_rotate.argtypes = [vp, sz, vp, vp, C.c_int64, vp]
+        L.wg_conjugate.argtypes = [vp, sz, vp, vp, vp]
+        L.wg_rotate_many.argtypes = [vp, sz, vp, vp, vp, sz, vp, vp]
+        L.wg_mul.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp]
+        L.wg_relin.argtypes = [vp, sz, vp, vp, vp, vp]
+        L.wg_rescale.argtypes = [vp, sz, vp, sz, sz, vp]
+        L.wg_add.argtypes = [vp, sz, vp, vp, sz, sz, vp]
+        L.wg_sub.argtypes = [vp, sz, vp, vp, sz, sz, vp]
+        L.wg_batch_mul_relin_rescale_rotate.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp]
+        L.wg_launch_count.argtypes = [C.c_int]
+        L.wg_launch_count.restype = C.c_uint64
+        L.wg_probe_begin.argtypes = [C.c_int, C.c_int]
+        L.wg_probe_end.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.wg_malloc.argtypes = [C.POINTER(vp), sz]
+        L.wg_free.argtypes = [vp]
+        L.wg_memcpy_htod.argtypes = [vp, vp, sz, vp]
+        L.wg_memcpy_dtoh.argtypes = [vp, vp, sz, vp]
+        L.wg_stream_synchronize.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        msg = lib().wg_last_error().decode()
+        if rc == -1:
+            raise InvalidArgument(rc, msg)
+        raise WalshGpuError(rc, msg)
+
+
+def _ptr(t) -> int:
+    """Device pointer of a torch tensor (or an int already holding one)."""
+    if t is None:
+        return 0
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def _stream(stream=None) -> int:
+    if stream is not None:
+        return stream if isinstance(stream, int) else stream.cuda_stream
+    import torch
+
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _u64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
+
+
+KCLASS = {"ntt": 0, "modup": 1, "keymac": 2, "moddown": 3, "combine": 4, "elementwise": 5}
+
+
+def launch_count(kernel_class=-1) -> int:
+    """Kernel launches the library issued so far (all classes by default)."""
+    return int(lib().wg_launch_count(kernel_class))
+
+
+def probe_begin(kernel_class, max_launches=60000):
+    """Start CUDA-event timing of every launch of one kernel class."""
+    _check(lib().wg_probe_begin(kernel_class, max_launches))
+
+
+def probe_end():
+    """Stop timing; returns (launches, total_ms, total_algorithmic_bytes)."""
+    n, ms, by = C.c_uint64(), C.c_double(), C.c_double()
+    _check(lib().wg_probe_end(C.byref(n), C.byref(ms), C.byref(by)))
+    return n.value, ms.value, by.value
+
+
+def memcpy_htod(dst, src_ptr, nbytes, stream=None):
+    _check(lib().wg_memcpy_htod(_ptr(dst), src_ptr, nbytes, _stream(stream)))
+
+
+def memcpy_dtoh(dst_ptr, src, nbytes, stream=None):
+    _check(lib().wg_memcpy_dtoh(dst_ptr, _ptr(src), nbytes, _stream(stream)))
+
+
+def find_primes(p_bits, q_bits, N):
+    """Reference prime chain (find_p_and_q_primes): returns (p, q) as uint64 arrays."""
+    pb, qb = _u64(p_bits), _u64(q_bits)
+    p = np.zeros(len(pb), np.uint64)
+    q = np.zeros(len(qb), np.uint64)
+    _check(lib().wg_find_primes(pb.ctypes.data, len(pb), qb.ctypes.data, len(qb), int(N), p.ctypes.data,
+                                q.ctypes.data))
+    return p, q
+
+
+def to_device(arr, device="cuda"):
+    """uint64 numpy array -> int64 torch tensor on the GPU (bit-identical)."""
+    import torch
+
+    return torch.from_numpy(_u64(arr).view(np.int64).copy()).to(device)
+
+
+def to_host(t) -> np.ndarray:
+    """int64 torch tensor -> uint64 numpy array (bit-identical)."""
+    return t.detach().cpu().numpy().view(np.uint64).copy()
+
+
+class Context:
+    """Device-resident CKKS context (moduli, twiddles, base-change tables, keys)."""
+
+    def __init__(self, N, q, p, dnum, device: int = 0):
+        self.N = int(N)
+        self.q = _u64(q)
+        self.p = _u64(p)
+        self.dnum = int(dnum)
+        self.device = device
+        self.alpha = (len(self.q) + self.dnum - 1) // self.dnum
+        h = C.c_void_p()
+        _check(lib().wg_ctx_create(self.N, self.q.ctypes.data, len(self.q), self.p.ctypes.data, len(self.p),
+                                   self.dnum, device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nq(self):
+        return len(self.q)
+
+    @property
+    def np_(self):
+        return len(self.p)
+
+    def parts(self, level):
+        return min(self.dnum, (level + self.alpha) // self.alpha)
+
+    def set_key(self, kind, key, rotation=0, parts=None, key_level=None):
+        kl = self.nq - 1 if key_level is None else key_level
+        parts = self.parts(kl) if parts is None else parts
+        k = _u64(key)
+        expect = parts * 2 * (kl + 1 + self.np_) * self.N
+        if k.size != expect:
+            raise ValueError(f"key has {k.size} words, expected {expect}")
+        _check(lib().wg_ctx_set_key(self.h, kind, int(rotation), k.ctypes.data, parts, kl))
+
+    def has_key(self, kind, rotation=0):
+        return bool(lib().wg_ctx_has_key(self.h, kind, int(rotation)))
+
+    def reserve(self, stream=None):
+        _check(lib().wg_ctx_reserve(self.h, _stream(stream)))
+
+    # --- operations on device buffers -------------------------------------------------
+    def ntt_forward(self, poly, limbs, first=0, basis=0, polys=1, stride=0, stream=None):
+        _check(lib().wg_ntt_forward(self.h, _ptr(poly), limbs, first, basis, polys, stride, _stream(stream)))
+
+    def ntt_inverse(self, poly, limbs, first=0, basis=0, polys=1, stride=0, stream=None):
+        _check(lib().wg_ntt_inverse(self.h, _ptr(poly), limbs, first, basis, polys, stride, _stream(stream)))
+
+    def keyswitch(self, level, key_term, kind, b, a, b_add=True, a_add=False, rotation=0, stream=None):
+        _check(lib().wg_keyswitch(self.h, level, _ptr(key_term), kind, int(rotation), _ptr(b), _ptr(a),
+                                  int(b_add), int(a_add), _stream(stream)))
+
+    def rotate(self, level, b, a, rotation, stream=None):
+        _check(lib().wg_rotate(self.h, level, _ptr(b), _ptr(a), int(rotation), _stream(stream)))
+
+    def conjugate(self, level, b, a, stream=None):
+        _check(lib().wg_conjugate(self.h, level, _ptr(b), _ptr(a), _stream(stream)))
+
+    def rotate_many(self, level, b, a, rotations, out, stream=None):
+        r = np.ascontiguousarray(rotations, dtype=np.int64)
+        _check(lib().wg_rotate_many(self.h, level, _ptr(b), _ptr(a), r.ctypes.data, len(r), _ptr(out),
+                                    _stream(stream)))
+
+    def mul(self, level, b1, a1, b2, a2, c2, stream=None):
+        _check(lib().wg_mul(self.h, level, _ptr(b1), _ptr(a1), _ptr(b2), _ptr(a2), _ptr(c2), _stream(stream)))
+
+    def relin(self, level, c0, c1, c2, stream=None):
+        _check(lib().wg_relin(self.h, level, _ptr(c0), _ptr(c1), _ptr(c2), _stream(stream)))
+
+    def rescale(self, level, polys, npolys=1, stride=0, stream=None):
+        _check(lib().wg_rescale(self.h, level, _ptr(polys), npolys, stride, _stream(stream)))
+
+    def add(self, level, x, y, npolys=1, stride=0, stream=None):
+        _check(lib().wg_add(self.h, level, _ptr(x), _ptr(y), npolys, stride, _stream(stream)))
+
+    def sub(self, level, x, y, npolys=1, stride=0, stream=None):
+        _check(lib().wg_sub(self.h, level, _ptr(x), _ptr(y), npolys, stride, _stream(stream)))
+
+    def batch_mul_relin_rescale_rotate(self, levels, xb, xa, yb, ya, rots, stream=None):
+        n = len(levels)
+        lv = np.ascontiguousarray(levels, dtype=np.uintp)
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        pxb, pxa, pyb, pya = arr(xb), arr(xa), arr(yb), arr(ya)
+        r = np.ascontiguousarray(rots, dtype=np.int64)
+        _check(lib().wg_batch_mul_relin_rescale_rotate(self.h, n, lv.ctypes.data, pxb.ctypes.data, pxa.ctypes.data,
+                                                       pyb.ctypes.data, pya.ctypes.data, r.ctypes.data,
+                                                       _stream(stream)))

@@ -1,0 +1,173 @@
+/* walsh_gpu.h -- C ABI of the B200 CKKS residue engine (libwalshgpu.so).
+ *
+ * The engine replaces the CPU residue path of TrustworthyComputing/aes-walsh-ckks.  Every
+ * entry point below names the reference interface it stands in for (path:line inside that
+ * project).  Conventions shared by all calls:
+ *
+ *   - Polynomials are limb-major arrays of uint64 residues in DEVICE memory, limb l of a
+ *     polynomial at poly + l*N, in the evaluation (NTT, bit-reversed) domain, exactly the
+ *     reference's CKKSCiphertext poly layout (src/ckks/ciphertext/ckks_ciphertext.hpp:18-74).
+ *     A ciphertext at level l has (l+1) Q limbs per polynomial; "b" is polynomial 0 and "a"
+ *     polynomial 1 (src/ckks/ciphertext/ckks_ciphertext.cpp:20).
+ *   - Switching keys are given in HOST memory in the layout
+ *     [part][0 = a, 1 = b][key_level+1 Q limbs then K P limbs][N], folded and in Montgomery
+ *     form as the reference stores them (hybrid_key_folding.hpp:50-77,
+ *     hybrid_key_montgomery.hpp:12-36 under src/ckks/context/).
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls enqueue work and
+ *     return; results are ready when the stream is synchronised.
+ *   - Return 0 on success or a negative WG_ERR_* code; wg_last_error() describes the last
+ *     failure of the calling thread.  WG_ERR_INVALID corresponds to the reference's
+ *     std::invalid_argument, WG_ERR_RUNTIME to its std::runtime_error (missing key or table).
+ *   - One context serves one stream per in-flight operation: each stream gets its own
+ *     scratch on first use (wg_ctx_reserve allocates it ahead, e.g. before graph capture).
+ */
+#ifndef WALSH_GPU_H
+#define WALSH_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WG_OK 0
+#define WG_ERR_INVALID (-1)
+#define WG_ERR_RUNTIME (-2)
+#define WG_ERR_CUDA (-3)
+#define WG_ERR_NOMEM (-4)
+
+/* Switching-key kinds for wg_ctx_set_key / wg_keyswitch. */
+#define WG_KEY_RELIN 0       /* s^2 -> s           (relinearization_key_generation.cpp:130-199) */
+#define WG_KEY_CONJ 1        /* conj(s) -> s       (conjugation_key_generation.cpp:63-167) */
+#define WG_KEY_ROTATION 2    /* s -> pi^-1(s)      (rotation_key_generation.cpp:92-199) */
+
+typedef struct wg_context wg_context;
+
+/* Last error message of the calling thread ("" when none). */
+const char* wg_last_error(void);
+/* ABI version (major * 100 + minor). */
+int wg_version(void);
+
+/* Prime chain: P primes for p_bits then Q primes for q_bits, each k*2N+1 searched downward
+ * from 2^bits.  Replaces find_p_and_q_primes, src/util/random.cpp:115-131. */
+int wg_find_primes(const uint64_t* p_bits, size_t np, const uint64_t* q_bits, size_t nq,
+                   uint64_t N, uint64_t* p_out, uint64_t* q_out);
+
+/* Device-resident context for one parameter set: Q moduli q[0..nq), P moduli p[0..np), dnum
+ * digits.  Builds twiddles, ModUp/ModDown and rescale tables on `device`.
+ * Replaces the table-building part of CKKSContext::CKKSContext,
+ * src/ckks/context/ckks_context.cpp:603-705 (keys are installed with wg_ctx_set_key). */
+int wg_ctx_create(uint64_t N, const uint64_t* q, size_t nq, const uint64_t* p, size_t np,
+                  size_t dnum, int device, wg_context** out);
+void wg_ctx_destroy(wg_context* ctx);
+
+/* Install a switching key (copied to the device).  `rotation` is used for WG_KEY_ROTATION
+ * only and is normalised modulo N/2.  Replaces the key storage behind
+ * CKKSContext::getRelinHybrid / getConjugationKey / getRotationKey,
+ * src/ckks/context/ckks_context.cpp:720-814. */
+int wg_ctx_set_key(wg_context* ctx, int kind, int64_t rotation, const uint64_t* host_key,
+                   size_t parts, size_t key_level);
+/* 1 if the key is installed, else 0.  CKKSContext::hasRotationKey, ckks_context.cpp:769-775. */
+int wg_ctx_has_key(const wg_context* ctx, int kind, int64_t rotation);
+/* Allocate the scratch of `stream` now (required before capturing the stream in a graph). */
+int wg_ctx_reserve(wg_context* ctx, void* stream);
+/* Scratch words one in-flight operation uses (informational). */
+size_t wg_ctx_workspace_words(const wg_context* ctx);
+
+/* In-place negacyclic NTT of `polys` polynomials of `limbs` limbs, `poly_stride` words
+ * apart; limb l uses Q modulus first+l (basis 0) or P modulus first+l (basis 1).  Output is
+ * canonical.  Replaces ntt_forward_rns_flat_inplace / ntt_inverse_rns_flat_inplace,
+ * src/math/ntt/ntt.cpp:416-447. */
+int wg_ntt_forward(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, int basis,
+                   size_t polys, size_t poly_stride, void* stream);
+int wg_ntt_inverse(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, int basis,
+                   size_t polys, size_t poly_stride, void* stream);
+
+/* Hybrid key switch of key_term at `level` with the installed key (kind, rotation):
+ * b = (b_add ? b + ks_b : ks_b), a = (a_add ? a + ks_a : ks_a).  key_term may alias a.
+ * Replaces ckks_hybrid_key_switch_inplace (Montgomery, folded keys),
+ * src/ckks/operations/keyswitch/ckks_keyswitch.cpp:1330-1641. */
+int wg_keyswitch(wg_context* ctx, size_t level, const uint64_t* key_term, int kind,
+                 int64_t rotation, uint64_t* b, uint64_t* a, int b_add, int a_add, void* stream);
+
+/* Rotation by `rotation` slots (key switch to pi^-1(s), then the automorphism).
+ * Replaces ckks_rotate_inplace, src/ckks/operations/keyswitch/ckks_rotation.cpp:41-96. */
+int wg_rotate(wg_context* ctx, size_t level, uint64_t* b, uint64_t* a, int64_t rotation,
+              void* stream);
+
+/* Complex conjugation (automorphism X -> X^(2N-1), then the switch).
+ * Replaces ckks_conjugate_inplace, src/ckks/operations/keyswitch/ckks_conjugate.cpp:16-61. */
+int wg_conjugate(wg_context* ctx, size_t level, uint64_t* b, uint64_t* a, void* stream);
+
+/* Several rotations of one ciphertext; out holds nrot ciphertexts laid out
+ * [rot][b, a][level+1][N].  Replaces the hoisted path ckks_hoist_ciphertext_a_qp_eval +
+ * ckks_hybrid_key_switch_hoisted_inplace, ckks_keyswitch.cpp:344-373 and 1072-1328. */
+int wg_rotate_many(wg_context* ctx, size_t level, const uint64_t* b, const uint64_t* a,
+                   const int64_t* rotations, size_t nrot, uint64_t* out, void* stream);
+
+/* Tensor product: (b1, a1) <- (b1 b2, a1 b2 + b1 a2), c2 <- a1 a2 (Barrett products).
+ * Replaces ckks_mul_inplace(ct, ct), src/ckks/operations/arith/ckks_mul.cpp:90-157. */
+int wg_mul(wg_context* ctx, size_t level, uint64_t* b1, uint64_t* a1, const uint64_t* b2,
+           const uint64_t* a2, uint64_t* c2, void* stream);
+
+/* Relinearization of (c0, c1, c2) into (c0, c1).
+ * Replaces ckks_relin_hybrid_inplace, src/ckks/operations/keyswitch/ckks_relin.cpp:8-44. */
+int wg_relin(wg_context* ctx, size_t level, uint64_t* c0, uint64_t* c1, const uint64_t* c2,
+             void* stream);
+
+/* Rescale `npolys` polynomials (poly_stride words apart) from `level` to level-1; the first
+ * level*N words of each polynomial hold the result.
+ * Replaces ckks_rescale, src/ckks/operations/arith/ckks_rescale.cpp:68-148. */
+int wg_rescale(wg_context* ctx, size_t level, uint64_t* polys, size_t npolys,
+               size_t poly_stride, void* stream);
+
+/* x <- x + y / x <- x - y over npolys polynomials at `level`.
+ * Replaces ckks_add_inplace / ckks_sub_inplace (ct, ct),
+ * src/ckks/operations/arith/ckks_addition.cpp:62-139. */
+int wg_add(wg_context* ctx, size_t level, uint64_t* x, const uint64_t* y, size_t npolys,
+           size_t poly_stride, void* stream);
+int wg_sub(wg_context* ctx, size_t level, uint64_t* x, const uint64_t* y, size_t npolys,
+           size_t poly_stride, void* stream);
+
+/* Batched multiply + relinearize + rescale + rotate over `count` ciphertexts at arbitrary
+ * levels: for ciphertext i, (xb[i], xa[i]) <- rotate(rescale(relin(x_i * y_i)), rots[i]).
+ * Pointer arrays are host arrays of device pointers; each x buffer must hold
+ * (levels[i]+1)*N words per polynomial and receives levels[i]*N words.  The workload the
+ * reference runs as ckks_mul_inplace, ckks_relin_hybrid_inplace, ckks_rescale,
+ * ckks_rotate_inplace per ciphertext with OpenMP over ciphertexts. */
+int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_t* levels,
+                                      uint64_t* const* xb, uint64_t* const* xa,
+                                      const uint64_t* const* yb, const uint64_t* const* ya,
+                                      const int64_t* rots, void* stream);
+
+/* Instrumentation (no counterpart in the reference, which has only one wall-clock span
+ * around the AES evaluation, bench/aes_bench.cpp:264-271).  Kernel classes:
+ * 0 NTT phases, 1 ModUp, 2 key inner product, 3 ModDown, 4 combine/automorphism,
+ * 5 elementwise (tensor, add/sub, rescale steps). */
+#define WG_KCLASS_NTT 0
+#define WG_KCLASS_MODUP 1
+#define WG_KCLASS_KEYMAC 2
+#define WG_KCLASS_MODDOWN 3
+#define WG_KCLASS_COMBINE 4
+#define WG_KCLASS_ELEMENTWISE 5
+/* Kernel launches issued so far for a class (kernel_class < 0: all classes). */
+uint64_t wg_launch_count(int kernel_class);
+/* Bracket each following launch of `kernel_class` (up to max_launches) with CUDA events on
+ * its stream; wg_probe_end synchronises them and returns the launch count, the summed
+ * device time in ms and the summed algorithmic bytes (each input residue read once, each
+ * output written once). */
+int wg_probe_begin(int kernel_class, int max_launches);
+int wg_probe_end(uint64_t* launches, double* total_ms, double* total_bytes);
+
+/* Plain device-memory helpers for C callers without another allocator. */
+int wg_malloc(void** ptr, size_t bytes);
+int wg_free(void* ptr);
+int wg_memcpy_htod(void* dst, const void* src, size_t bytes, void* stream);
+int wg_memcpy_dtoh(void* dst, const void* src, size_t bytes, void* stream);
+int wg_stream_synchronize(void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WALSH_GPU_H */

@@ -180,7 +180,7 @@ class OracleCtx:
     def ntt(self, poly, first=0, which=0, inverse=False, lazy=False):
         poly = np.ascontiguousarray(poly, dtype=np.uint64).copy()
         limbs = poly.size // self.N
-        lib().orc_ntt(self.h, poly, first, limbs, which, int(inverse), int(lazy))
+        lib().orc_ntt(self.h, poly, first, limbs, int(which), int(inverse), int(lazy))
         return poly
 
     def uniform(self, limbs, seed):

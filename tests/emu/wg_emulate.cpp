@@ -1,0 +1,188 @@
+// CPU emulation of the device kernels (test infrastructure).
+//
+// Compiles the product's kernel bodies (wg_ntt.cuh, wg_keyswitch.cuh) and host table builder
+// (wg_tables.cpp, wg_host.cpp) with the host compiler and runs them CTA by CTA and thread by
+// thread, so the index logic, butterflies, HPS base changes and tables can be checked against
+// the oracle without a GPU.  Shared-memory rounds are separated exactly where the kernels put
+// __syncthreads().  Not part of the product library.
+#include <cstring>
+#include <utility>
+#include <vector>
+
+#include "wg_keyswitch.cuh"
+#include "wg_ntt.cuh"
+#include "wg_tables.hpp"
+
+using namespace wg;
+
+namespace {
+
+struct HostModUp {
+    int src_count, dst_count, src_first, pad;
+    const uint64_t *qhat_inv, *qhat_inv_s;
+    const double* src_inv;
+    const uint64_t *qhat, *qhat_s, *corr;
+    const int *dst_limb, *dst_mod;
+};
+
+struct Emu {
+    HostTables H;
+    int logN;
+    std::vector<std::vector<HostModUp>> modup;
+};
+
+template <int LOGN, bool FWD, bool COLS, int... RD>
+void rounds(std::integer_sequence<int, RD...>, uint64_t* sm, int tile, uint64_t q, const uint64_t* tw,
+            const uint64_t* tws) {
+    using P = ntt::Phase<LOGN, FWD, COLS>;
+    auto one = [&](auto rd_const) {
+        constexpr int R = decltype(rd_const)::value;
+        for (int t = 0; t < P::THREADS; ++t) {
+            const int sub = COLS ? t % P::SUBS : t >> P::OB;
+            const int o = COLS ? t / P::SUBS : t & ((1 << P::OB) - 1);
+            ntt::ntt_round<LOGN, FWD, COLS, R>(sm, sub, o, tile, q, tw, tws);
+        }
+    };
+    (one(std::integral_constant<int, RD>{}), ...);
+}
+
+template <int LOGN, bool FWD, bool COLS>
+void phase(const Emu& E, uint64_t* x, int mi) {
+    using P = ntt::Phase<LOGN, FWD, COLS>;
+    const size_t N = P::N;
+    const uint64_t* tw = E.H.tw.data() + (size_t)mi * 4 * N + (FWD ? 0 : 2 * N);
+    const uint64_t* tws = tw + N;
+    const Modulus& md = E.H.mods[mi];
+    std::vector<uint64_t> sm(P::TILE + P::TILE / 16);
+    for (int tile = 0; tile < (int)(N / P::TILE); ++tile) {
+        for (int e = 0; e < P::TILE; ++e) sm[ntt::pad16(e)] = x[ntt::tile_offset<LOGN, FWD, COLS>(tile, e)];
+        rounds<LOGN, FWD, COLS>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), tile, md.q, tw, tws);
+        for (int e = 0; e < P::TILE; ++e) {
+            uint64_t v = sm[ntt::pad16(e)];
+            if (P::LAST) v = FWD ? red4q(v, md.q) : mul_shoup(v, md.n_inv, md.n_inv_shoup, md.q);
+            x[ntt::tile_offset<LOGN, FWD, COLS>(tile, e)] = v;
+        }
+    }
+}
+
+template <int LOGN>
+void ntt_limb(const Emu& E, uint64_t* x, int mi, bool fwd) {
+    if (fwd) {
+        phase<LOGN, true, true>(E, x, mi);
+        phase<LOGN, true, false>(E, x, mi);
+    } else {
+        phase<LOGN, false, false>(E, x, mi);
+        phase<LOGN, false, true>(E, x, mi);
+    }
+}
+
+void ntt_one(const Emu& E, uint64_t* x, int mi, bool fwd) {
+    switch (E.logN) {
+        case 10: ntt_limb<10>(E, x, mi, fwd); break;
+        case 11: ntt_limb<11>(E, x, mi, fwd); break;
+        case 12: ntt_limb<12>(E, x, mi, fwd); break;
+        case 13: ntt_limb<13>(E, x, mi, fwd); break;
+        case 14: ntt_limb<14>(E, x, mi, fwd); break;
+        case 15: ntt_limb<15>(E, x, mi, fwd); break;
+        default: break;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void* emu_create(uint64_t N, const uint64_t* q, size_t nq, const uint64_t* p, size_t np, size_t dnum) {
+    Emu* E = new Emu;
+    E->H = build_tables(N, q, nq, p, np, dnum);
+    E->logN = __builtin_ctzll(N);
+    const uint64_t* T = E->H.words.data();
+    E->modup.resize(nq);
+    for (size_t l = 0; l < nq; ++l)
+        for (const auto& o : E->H.modup[l]) {
+            HostModUp d;
+            d.src_count = o.src_count;
+            d.dst_count = o.dst_count;
+            d.src_first = o.src_first;
+            d.pad = 0;
+            d.qhat_inv = T + o.qhat_inv;
+            d.qhat_inv_s = T + o.qhat_inv_s;
+            d.src_inv = reinterpret_cast<const double*>(T + o.src_inv);
+            d.qhat = T + o.qhat;
+            d.qhat_s = T + o.qhat_s;
+            d.corr = T + o.corr;
+            d.dst_limb = reinterpret_cast<const int*>(T + o.dst_limb);
+            d.dst_mod = reinterpret_cast<const int*>(T + o.dst_mod);
+            E->modup[l].push_back(d);
+        }
+    return E;
+}
+
+void emu_destroy(void* h) { delete static_cast<Emu*>(h); }
+
+// limbs consecutive limbs using modulus index first.. (basis 0 = Q, 1 = P)
+void emu_ntt(void* h, uint64_t* poly, size_t limbs, size_t first, int basis, int inverse) {
+    const Emu& E = *static_cast<Emu*>(h);
+    for (size_t l = 0; l < limbs; ++l)
+        ntt_one(E, poly + l * E.H.N, (int)((basis ? E.H.nq : 0) + first + l), !inverse);
+}
+
+// The device keyswitch() sequence, stage by stage, with the same buffers.
+void emu_keyswitch(void* h, size_t level, const uint64_t* key_term, const uint64_t* key, size_t key_level,
+                   uint64_t* b, uint64_t* a, int b_add, int a_add, uint64_t galois) {
+    const Emu& E = *static_cast<Emu*>(h);
+    const size_t N = E.H.N, L = level + 1, K = E.H.np, T = L + K, nq = E.H.nq;
+    const size_t alpha = E.H.alpha;
+    const size_t B = parts_at(level, nq, alpha, E.H.dnum);
+    std::vector<uint64_t> ws(N * (L + B * T + 2 * T + 2 * L));
+    uint64_t* coeff = ws.data();
+    uint64_t* digits = coeff + L * N;
+    uint64_t* acc = digits + B * T * N;
+    uint64_t* contrib = acc + 2 * T * N;
+    const Modulus* mods = E.H.mods.data();
+    std::memcpy(coeff, key_term, L * N * 8);
+    for (size_t l = 0; l < L; ++l) ntt_one(E, coeff + l * N, (int)l, false);
+    for (size_t j = 0; j < B; ++j)
+        for (size_t c = 0; c < N; ++c) modup_coeff(E.modup[level][j], mods, coeff, digits + j * T * N, N, c);
+    for (size_t j = 0; j < B; ++j) {
+        const size_t s0 = j * alpha, s1 = std::min(s0 + alpha, L);
+        for (size_t l = 0; l < T; ++l) {
+            if (l >= s0 && l < s1) continue;
+            ntt_one(E, digits + j * T * N + l * N, (int)(l < L ? l : nq + (l - L)), true);
+        }
+    }
+    for (size_t i = 0; i < T; ++i)
+        for (size_t c = 0; c < N; ++c)
+            mac_coeff(mods, (int)nq, (int)L, (int)K, (int)B, (int)alpha, key, (int)key_level, key_term, digits, T * N,
+                      acc, N, (int)i, c);
+    for (int poly = 0; poly < 2; ++poly)
+        for (size_t pi = 0; pi < K; ++pi) ntt_one(E, acc + (poly * T + L + pi) * N, (int)(nq + pi), false);
+    const uint64_t* W = E.H.words.data();
+    for (int poly = 0; poly < 2; ++poly)
+        for (size_t qi = 0; qi < L; ++qi)
+            for (size_t c = 0; c < N; ++c)
+                contrib[(poly * L + qi) * N + c] =
+                    moddown_coeff(mods[qi], mods + nq, (int)K, acc + (poly * T + L) * N, N, c,
+                                  W + E.H.fold_inv[level] + qi * K, W + E.H.fold_inv_s[level] + qi * K);
+    for (int poly = 0; poly < 2; ++poly)
+        for (size_t qi = 0; qi < L; ++qi) ntt_one(E, contrib + (poly * L + qi) * N, (int)qi, true);
+    if (galois == 0) {
+        for (size_t qi = 0; qi < L; ++qi)
+            for (size_t c = 0; c < N; ++c)
+                combine_coeff(mods[qi].q, (int)L, (int)K, acc, contrib, b, a, b, a, b_add, a_add, N, (int)qi, c);
+    } else {
+        uint64_t* tb = acc + T * N;
+        uint64_t* ta = acc;
+        for (size_t qi = 0; qi < L; ++qi)
+            for (size_t c = 0; c < N; ++c)
+                combine_coeff(mods[qi].q, (int)L, (int)K, acc, contrib, b, a, tb, ta, b_add, a_add, N, (int)qi, c);
+        for (size_t qi = 0; qi < L; ++qi)
+            for (uint32_t i = 0; i < N; ++i) {
+                const uint32_t s = automorphism_src(i, galois, E.logN);
+                b[qi * N + i] = tb[qi * N + s];
+                a[qi * N + i] = ta[qi * N + s];
+            }
+    }
+}
+
+}  // extern "C"
