@@ -1,0 +1,446 @@
+// Batched execution: one launch per pipeline stage over every ciphertext, limb and digit of a
+// batch, whatever their levels.
+//
+// Each stage reads a table of small jobs (pointers, modulus index, constants) from device
+// memory; block (x, y + 65535 z) runs tile x of job y.  All tables of a call are built on the
+// host, staged in pinned memory and uploaded with one copy, so a batched key switch over 64
+// ciphertexts is ~13 launches instead of ~13 per ciphertext.  Arithmetic is shared with the
+// single-ciphertext path (wg_keyswitch.cuh, wg_arith.cuh), so results are identical.
+#include <algorithm>
+#include <cstring>
+
+#include "wg_batch.hpp"
+#include "wg_internal.hpp"
+#include "wg_keyswitch.cuh"
+
+namespace wg {
+namespace {
+
+constexpr int kT = 256;
+
+struct ModUpJob {
+    const ModUpDesc* desc;
+    const uint64_t* src;
+    uint64_t* digit;
+};
+struct MacJob {
+    const uint64_t* key;
+    const uint64_t* key_term;
+    const uint64_t* digits;
+    uint64_t* acc;
+    size_t part_stride;
+    int L, K, parts, alpha, key_level, i;
+};
+struct ModDownJob {
+    const uint64_t* src_p;
+    uint64_t* out;
+    const uint64_t* inv;
+    const uint64_t* inv_s;
+    int qmod;
+    int pad;
+};
+struct CombineJob {
+    const uint64_t* acc;
+    const uint64_t* contrib;
+    const uint64_t* b_in;
+    const uint64_t* a_in;
+    uint64_t* b_out;
+    uint64_t* a_out;
+    int L, K, qi, b_add, a_add, pad;
+};
+struct GatherJob {
+    const uint64_t* src_b;
+    const uint64_t* src_a;
+    uint64_t* b;
+    uint64_t* a;
+    uint64_t galois;
+};
+struct TensorJob {
+    uint64_t* b1;
+    uint64_t* a1;
+    const uint64_t* b2;
+    const uint64_t* a2;
+    uint64_t* c2;
+    int mod;
+    int pad;
+};
+struct RescalePrepJob {
+    const uint64_t* drop;
+    uint64_t* rem;
+    uint64_t one_s, half;
+    int pmod, qmod;
+};
+struct RescaleFinishJob {
+    uint64_t* x;
+    const uint64_t* rem;
+    uint64_t inv_p, inv_p_s;
+    int mod, pad;
+};
+
+template <class J>
+__device__ __forceinline__ const J* job_of(const J* jobs, int n) {
+    const int j = blockIdx.y + 65535 * blockIdx.z;
+    return j < n ? jobs + j : nullptr;
+}
+
+__global__ void __launch_bounds__(kT) kb_modup(const ModUpJob* jobs, int n, const Modulus* mods, size_t N) {
+    const ModUpJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    modup_coeff(*j->desc, mods, j->src, j->digit, N, coeff);
+}
+
+__global__ void __launch_bounds__(kT) kb_mac(const MacJob* jobs, int n, const Modulus* mods, int nq, size_t N) {
+    const MacJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    mac_coeff(mods, nq, j->L, j->K, j->parts, j->alpha, j->key, j->key_level, j->key_term, j->digits, j->part_stride,
+              j->acc, N, j->i, coeff);
+}
+
+__global__ void __launch_bounds__(kT) kb_moddown(const ModDownJob* jobs, int n, const Modulus* mods, int nq, int K,
+                                                 size_t N) {
+    const ModDownJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    j->out[coeff] = moddown_coeff(mods[j->qmod], mods + nq, K, j->src_p, N, coeff, j->inv, j->inv_s);
+}
+
+__global__ void __launch_bounds__(kT) kb_combine(const CombineJob* jobs, int n, const Modulus* mods, size_t N) {
+    const CombineJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    combine_coeff(mods[j->qi].q, j->L, j->K, j->acc, j->contrib, j->b_in, j->a_in, j->b_out, j->a_out, j->b_add,
+                  j->a_add, N, j->qi, coeff);
+}
+
+__global__ void __launch_bounds__(kT) kb_gather(const GatherJob* jobs, int n, int logN) {
+    const GatherJob* j = job_of(jobs, n);
+    if (!j) return;
+    const uint32_t i = blockIdx.x * kT + threadIdx.x;
+    const uint32_t s = automorphism_src(i, j->galois, logN);
+    j->b[i] = j->src_b[s];
+    j->a[i] = j->src_a[s];
+}
+
+__global__ void __launch_bounds__(kT) kb_tensor(const TensorJob* jobs, int n, const Modulus* mods) {
+    const TensorJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const Modulus m = mods[j->mod];
+    const uint64_t xa = j->a1[k], xb = j->b1[k], ya = j->a2[k], yb = j->b2[k];
+    j->c2[k] = barrett_mul(xa, ya, m);
+    const uint64_t tmp = barrett_mul(xb, ya, m);
+    j->b1[k] = barrett_mul(xb, yb, m);
+    j->a1[k] = add_mod(barrett_mul(xa, yb, m), tmp, m.q);
+}
+
+// Same two steps as k_rescale_prep / k_rescale_finish in wg_ops.cu.
+__global__ void __launch_bounds__(kT) kb_rescale_prep(const RescalePrepJob* jobs, int n, const Modulus* mods) {
+    const RescalePrepJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const uint64_t p = mods[j->pmod].q, q = mods[j->qmod].q;
+    uint64_t shift = j->drop[k] + (p >> 1);
+    if (shift >= p) shift -= p;
+    j->rem[k] = sub_mod(reduce_shoup(shift, q, j->one_s), j->half, q);
+}
+
+__global__ void __launch_bounds__(kT) kb_rescale_finish(const RescaleFinishJob* jobs, int n, const Modulus* mods) {
+    const RescaleFinishJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const uint64_t q = mods[j->mod].q;
+    uint64_t x = j->x[k];
+    if (x >= q) x -= q;
+    j->x[k] = mul_shoup(sub_mod(x, j->rem[k], q), j->inv_p, j->inv_p_s, q);
+}
+
+dim3 grid_for(const Context& c, size_t njobs) {
+    return dim3((unsigned)(c.N / kT), (unsigned)std::min<size_t>(njobs, 65535), (unsigned)((njobs + 65534) / 65535));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// Job-table staging
+// ------------------------------------------------------------------------------------------
+template <class J>
+const J* JobTable::add(const std::vector<J>& v) {
+    size_t off = (bytes.size() + 15) & ~size_t{15};
+    bytes.resize(off + v.size() * sizeof(J));
+    if (!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(J));
+    offsets.push_back(off);
+    return reinterpret_cast<const J*>(off);  // resolved against the device base by at()
+}
+
+void JobTable::upload(Context& c, cudaStream_t s) {
+    BatchBuffers& bb = c.batch_buffers(s);
+    bb.ensure_jobs(c, bytes.size(), s);
+    if (bb.staged_event) cudaEventSynchronize(bb.staged_event);  // previous upload left the pinned stage
+    std::memcpy(bb.h_jobs, bytes.data(), bytes.size());
+    check_cuda(cudaMemcpyAsync(bb.d_jobs, bb.h_jobs, bytes.size(), cudaMemcpyHostToDevice, s), "job upload");
+    check_cuda(cudaEventRecord(bb.staged_event, s), "job event");
+    base = bb.d_jobs;
+}
+
+// ------------------------------------------------------------------------------------------
+// Batched key switch
+// ------------------------------------------------------------------------------------------
+struct KsPlan {
+    const NttJob* intt_in;
+    int n_intt_in;
+    const ModUpJob* modup;
+    int n_modup;
+    const NttJob* ntt_digits;
+    int n_ntt_digits;
+    const MacJob* mac;
+    int n_mac;
+    const NttJob* intt_p;
+    int n_intt_p;
+    const ModDownJob* moddown;
+    int n_moddown;
+    const NttJob* ntt_contrib;
+    int n_ntt_contrib;
+    const CombineJob* combine;
+    int n_combine;
+    const GatherJob* gather;
+    int n_gather;
+    double mac_bytes, modup_bytes, moddown_bytes, combine_bytes;
+};
+
+size_t batch_keyswitch_words(const Context& c, const KsItem* items, size_t n) {
+    size_t w = 0;
+    for (size_t i = 0; i < n; ++i) w += keyswitch_workspace_words(c, items[i].level);
+    return w;
+}
+
+static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, uint64_t* ws, JobTable& t) {
+    const size_t N = c.N, K = c.np, nq = c.nq;
+    std::vector<NttJob> intt_in, ntt_digits, intt_p, ntt_contrib;
+    std::vector<ModUpJob> modup;
+    std::vector<MacJob> mac;
+    std::vector<ModDownJob> moddown;
+    std::vector<CombineJob> combine;
+    std::vector<GatherJob> gather;
+    KsPlan p{};
+    for (size_t it = 0; it < n; ++it) {
+        const KsItem& x = items[it];
+        const size_t level = x.level, L = level + 1, T = L + K, B = c.parts_at(level);
+        if (level >= nq) fail(kInvalid, "batched keyswitch: invalid ciphertext level");
+        if (x.key->key_level < level) fail(kRuntime, "keyswitch: switch key level is below ciphertext level");
+        if (x.key->parts < B) fail(kRuntime, "keyswitch: insufficient key partitions");
+        uint64_t* coeff = ws;
+        uint64_t* digits = coeff + L * N;
+        uint64_t* acc = digits + B * T * N;
+        uint64_t* contrib = acc + 2 * T * N;
+        ws += keyswitch_workspace_words(c, level);
+        for (size_t l = 0; l < L; ++l) intt_in.push_back({x.key_term + l * N, coeff + l * N, (int)l, 0});
+        for (size_t j = 0; j < B; ++j) {
+            modup.push_back({c.d_modup + level * c.dnum + j, coeff, digits + j * T * N});
+            const ModUpDesc& d = c.modup[level][j];
+            p.modup_bytes += 8.0 * N * (d.src_count + d.dst_count);
+            const size_t s0 = j * c.alpha, s1 = std::min(s0 + c.alpha, L);
+            for (size_t l = 0; l < T; ++l) {
+                if (l >= s0 && l < s1) continue;
+                uint64_t* ptr = digits + j * T * N + l * N;
+                ntt_digits.push_back({ptr, ptr, (int)(l < L ? l : nq + (l - L)), 0});
+            }
+        }
+        for (size_t i = 0; i < T; ++i)
+            mac.push_back({x.key->d_data, x.key_term, digits, acc, T * N, (int)L, (int)K, (int)B, (int)c.alpha,
+                           (int)x.key->key_level, (int)i});
+        p.mac_bytes += 8.0 * N * T * (3.0 * B + 2.0);
+        for (int poly = 0; poly < 2; ++poly)
+            for (size_t pi = 0; pi < K; ++pi) {
+                uint64_t* ptr = acc + (poly * T + L + pi) * N;
+                intt_p.push_back({ptr, ptr, (int)(nq + pi), 0});
+            }
+        for (int poly = 0; poly < 2; ++poly)
+            for (size_t qi = 0; qi < L; ++qi) {
+                moddown.push_back({acc + (poly * T + L) * N, contrib + (poly * L + qi) * N,
+                                   c.fold_inv[level] + qi * K, c.fold_inv_s[level] + qi * K, (int)qi, 0});
+                uint64_t* ptr = contrib + (poly * L + qi) * N;
+                ntt_contrib.push_back({ptr, ptr, (int)qi, 0});
+            }
+        p.moddown_bytes += 8.0 * N * 2.0 * (K + L);
+        const bool gal = x.galois != 0;
+        for (size_t qi = 0; qi < L; ++qi) {
+            uint64_t* bo = gal ? acc + T * N : x.b;
+            uint64_t* ao = gal ? acc : x.a;
+            combine.push_back({acc, contrib, x.b_in, x.a_in, bo, ao, (int)L, (int)K, (int)qi, x.b_add, x.a_add, 0});
+            if (gal)
+                gather.push_back({acc + T * N + qi * N, acc + qi * N, x.b + qi * N, x.a + qi * N, x.galois});
+        }
+        p.combine_bytes += 8.0 * N * L * (x.b_add + x.a_add + 6.0) + (gal ? 8.0 * N * L * 4.0 : 0.0);
+    }
+    p.intt_in = t.add(intt_in);
+    p.n_intt_in = (int)intt_in.size();
+    p.modup = t.add(modup);
+    p.n_modup = (int)modup.size();
+    p.ntt_digits = t.add(ntt_digits);
+    p.n_ntt_digits = (int)ntt_digits.size();
+    p.mac = t.add(mac);
+    p.n_mac = (int)mac.size();
+    p.intt_p = t.add(intt_p);
+    p.n_intt_p = (int)intt_p.size();
+    p.moddown = t.add(moddown);
+    p.n_moddown = (int)moddown.size();
+    p.ntt_contrib = t.add(ntt_contrib);
+    p.n_ntt_contrib = (int)ntt_contrib.size();
+    p.combine = t.add(combine);
+    p.n_combine = (int)combine.size();
+    p.gather = t.add(gather);
+    p.n_gather = (int)gather.size();
+    return p;
+}
+
+static void run_keyswitch(const Context& c, const KsPlan& p, const JobTable& t, cudaStream_t s) {
+    const size_t N = c.N;
+    ntt_jobs(c, t.at(p.intt_in), p.n_intt_in, false, s);
+    {
+        Probe probe(kClsModUp, p.modup_bytes, s);
+        kb_modup<<<grid_for(c, p.n_modup), kT, 0, s>>>(t.at(p.modup), p.n_modup, c.d_mod, N);
+    }
+    ntt_jobs(c, t.at(p.ntt_digits), p.n_ntt_digits, true, s);
+    {
+        Probe probe(kClsKeyMac, p.mac_bytes, s);
+        kb_mac<<<grid_for(c, p.n_mac), kT, 0, s>>>(t.at(p.mac), p.n_mac, c.d_mod, (int)c.nq, N);
+    }
+    ntt_jobs(c, t.at(p.intt_p), p.n_intt_p, false, s);
+    {
+        Probe probe(kClsModDown, p.moddown_bytes, s);
+        kb_moddown<<<grid_for(c, p.n_moddown), kT, 0, s>>>(t.at(p.moddown), p.n_moddown, c.d_mod, (int)c.nq,
+                                                            (int)c.np, N);
+    }
+    ntt_jobs(c, t.at(p.ntt_contrib), p.n_ntt_contrib, true, s);
+    {
+        Probe probe(kClsCombine, p.combine_bytes, s);
+        kb_combine<<<grid_for(c, p.n_combine), kT, 0, s>>>(t.at(p.combine), p.n_combine, c.d_mod, N);
+        if (p.n_gather) kb_gather<<<grid_for(c, p.n_gather), kT, 0, s>>>(t.at(p.gather), p.n_gather, c.logN);
+    }
+    check_cuda(cudaGetLastError(), "batched keyswitch launch");
+}
+
+void batch_keyswitch(Context& c, const KsItem* items, size_t n, cudaStream_t s) {
+    if (n == 0) return;
+    uint64_t* ws = c.batch_buffers(s).arena(c, batch_keyswitch_words(c, items, n), s);
+    JobTable t;
+    KsPlan p = plan_keyswitch(c, items, n, ws, t);
+    t.upload(c, s);
+    run_keyswitch(c, p, t, s);
+}
+
+// ------------------------------------------------------------------------------------------
+// Batched mul + relin + rescale + rotate
+// ------------------------------------------------------------------------------------------
+void batch_mul_relin_rescale_rotate(Context& c, size_t count, const size_t* levels, uint64_t* const* xb,
+                                    uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                                    const int64_t* rots, const uint64_t* galois, const KeyEntry* relin,
+                                    const KeyEntry* const* rot_keys, cudaStream_t s) {
+    if (count == 0) return;
+    const size_t N = c.N;
+    // Arena: c2 per ciphertext, the relin key switches, rescale remainders, rotate switches.
+    std::vector<KsItem> relin_items(count), rot_items;
+    size_t c2_words = 0, rem_words = 0;
+    for (size_t i = 0; i < count; ++i) {
+        c2_words += (levels[i] + 1) * N;
+        rem_words += 2 * levels[i] * N;
+    }
+    for (size_t i = 0; i < count; ++i) relin_items[i].level = levels[i];
+    for (size_t i = 0; i < count; ++i)
+        if (galois[i]) {
+            KsItem it;
+            it.level = levels[i] - 1;
+            rot_items.push_back(it);
+        }
+    const size_t ks1 = batch_keyswitch_words(c, relin_items.data(), count);
+    const size_t ks2 = batch_keyswitch_words(c, rot_items.data(), rot_items.size());
+    uint64_t* arena = c.batch_buffers(s).arena(c, c2_words + rem_words + std::max(ks1, ks2), s);
+    uint64_t* c2base = arena;
+    uint64_t* rembase = c2base + c2_words;
+    uint64_t* ksbase = rembase + rem_words;
+
+    JobTable t;
+    std::vector<TensorJob> tensor;
+    std::vector<NttJob> drop_intt, rem_ntt;
+    std::vector<RescalePrepJob> prep;
+    std::vector<RescaleFinishJob> fin;
+    uint64_t* c2p = c2base;
+    uint64_t* remp = rembase;
+    size_t r = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const size_t lv = levels[i], L = lv + 1;
+        for (size_t l = 0; l < L; ++l)
+            tensor.push_back({xb[i] + l * N, xa[i] + l * N, yb[i] + l * N, ya[i] + l * N, c2p + l * N, (int)l, 0});
+        KsItem& ri = relin_items[i];
+        ri.key_term = c2p;
+        ri.key = relin;
+        ri.b_in = xb[i];
+        ri.a_in = xa[i];
+        ri.b = xb[i];
+        ri.a = xa[i];
+        ri.b_add = 1;
+        ri.a_add = 1;
+        ri.galois = 0;
+        c2p += L * N;
+        const uint64_t* rc = c.rs_host.data() + c.rs_host_off[lv];
+        for (int poly = 0; poly < 2; ++poly) {
+            uint64_t* x = poly ? xa[i] : xb[i];
+            uint64_t* drop = x + lv * N;
+            drop_intt.push_back({drop, drop, (int)lv, 0});
+            for (size_t q = 0; q < lv; ++q) {
+                prep.push_back({drop, remp + q * N, rc[q], rc[3 * lv + q], (int)lv, (int)q});
+                rem_ntt.push_back({remp + q * N, remp + q * N, (int)q, 0});
+                fin.push_back({x + q * N, remp + q * N, rc[lv + q], rc[2 * lv + q], (int)q, 0});
+            }
+            remp += lv * N;
+        }
+        if (galois[i]) {
+            KsItem& it = rot_items[r++];
+            it.key_term = xa[i];
+            it.key = rot_keys[i];
+            it.b_in = xb[i];
+            it.a_in = xa[i];
+            it.b = xb[i];
+            it.a = xa[i];
+            it.b_add = 1;
+            it.a_add = 0;
+            it.galois = galois[i];
+        }
+    }
+    const TensorJob* jt = t.add(tensor);
+    const NttJob* jd = t.add(drop_intt);
+    const RescalePrepJob* jp = t.add(prep);
+    const NttJob* jr = t.add(rem_ntt);
+    const RescaleFinishJob* jf = t.add(fin);
+    KsPlan p1 = plan_keyswitch(c, relin_items.data(), count, ksbase, t);
+    KsPlan p2 = plan_keyswitch(c, rot_items.data(), rot_items.size(), ksbase, t);
+    t.upload(c, s);
+
+    double tb = 0, pb = 0, fb = 0;
+    for (size_t i = 0; i < count; ++i) {
+        tb += 8.0 * N * (levels[i] + 1) * 7.0;
+        pb += 8.0 * N * 2.0 * (1.0 + levels[i]);
+        fb += 8.0 * N * 2.0 * 3.0 * levels[i];
+    }
+    {
+        Probe probe(kClsElementwise, tb, s);
+        kb_tensor<<<grid_for(c, tensor.size()), kT, 0, s>>>(t.at(jt), (int)tensor.size(), c.d_mod);
+    }
+    run_keyswitch(c, p1, t, s);
+    ntt_jobs(c, t.at(jd), (int)drop_intt.size(), false, s);
+    {
+        Probe probe(kClsElementwise, pb, s);
+        kb_rescale_prep<<<grid_for(c, prep.size()), kT, 0, s>>>(t.at(jp), (int)prep.size(), c.d_mod);
+    }
+    ntt_jobs(c, t.at(jr), (int)rem_ntt.size(), true, s);
+    {
+        Probe probe(kClsElementwise, fb, s);
+        kb_rescale_finish<<<grid_for(c, fin.size()), kT, 0, s>>>(t.at(jf), (int)fin.size(), c.d_mod);
+    }
+    if (!rot_items.empty()) run_keyswitch(c, p2, t, s);
+    check_cuda(cudaGetLastError(), "batched pipeline launch");
+}
+
+}  // namespace wg

@@ -1,0 +1,48 @@
+// Batched execution over many ciphertexts (wg_batch.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "wg_internal.hpp"
+
+namespace wg {
+
+// One key switch of a batch: b = (b_add ? b_in + ks_b : ks_b), a likewise, then the
+// automorphism `galois` (0 = none) on both outputs.
+struct KsItem {
+    size_t level = 0;
+    const uint64_t* key_term = nullptr;
+    const KeyEntry* key = nullptr;
+    const uint64_t* b_in = nullptr;
+    const uint64_t* a_in = nullptr;
+    uint64_t* b = nullptr;
+    uint64_t* a = nullptr;
+    int b_add = 1;
+    int a_add = 0;
+    uint64_t galois = 0;
+};
+
+// Host image of the job tables of one call; pointers returned by add() are byte offsets
+// until upload() places the image in device memory, at() turns them into device pointers.
+struct JobTable {
+    std::vector<unsigned char> bytes;
+    std::vector<size_t> offsets;
+    void* base = nullptr;
+    template <class J>
+    const J* add(const std::vector<J>& v);
+    template <class J>
+    const J* at(const J* off) const {
+        return reinterpret_cast<const J*>(static_cast<unsigned char*>(base) + reinterpret_cast<size_t>(off));
+    }
+    void upload(Context& c, cudaStream_t s);
+};
+
+size_t batch_keyswitch_words(const Context& c, const KsItem* items, size_t n);
+void batch_keyswitch(Context& c, const KsItem* items, size_t n, cudaStream_t s);
+void batch_mul_relin_rescale_rotate(Context& c, size_t count, const size_t* levels, uint64_t* const* xb,
+                                    uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                                    const int64_t* rots, const uint64_t* galois, const KeyEntry* relin,
+                                    const KeyEntry* const* rot_keys, cudaStream_t s);
+
+}  // namespace wg

@@ -4,6 +4,7 @@
 #include <string>
 
 #include "../../include/walsh_gpu.h"
+#include "wg_batch.hpp"
 #include "wg_internal.hpp"
 
 namespace wg {
@@ -306,18 +307,45 @@ int wg_sub(wg_context* ctx, size_t level, uint64_t* x, const uint64_t* y, size_t
     return add_sub_call(ctx, level, x, y, npolys, poly_stride, stream, true);
 }
 
+static void check_batch(wg::Context& c, size_t count, const size_t* levels, uint64_t* const* xb,
+                        uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                        const int64_t* rots) {
+    if (count && (!levels || !xb || !xa || !yb || !ya || !rots)) wg::fail(wg::kInvalid, "batch: null array");
+    for (size_t i = 0; i < count; ++i) {
+        if (levels[i] == 0 || levels[i] >= c.nq) wg::fail(wg::kInvalid, "batch: ciphertext level must be in [1, L)");
+        for (const void* p : {(const void*)xb[i], (const void*)xa[i], (const void*)yb[i], (const void*)ya[i]})
+            check_ptr(p, "batch");
+        const int64_t r = normalize_rotation(c, rots[i]);
+        if (r) c.key(WG_KEY_ROTATION, r);
+    }
+    c.key(WG_KEY_RELIN, 0);
+}
+
 int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_t* levels, uint64_t* const* xb,
                                       uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
                                       const int64_t* rots, void* stream) {
     return guard([&] {
         wg::Context& c = C(ctx);
-        cudaStream_t s = S(stream);
+        check_batch(c, count, levels, xb, xa, yb, ya, rots);
+        std::vector<uint64_t> galois(count);
+        std::vector<const wg::KeyEntry*> keys(count, nullptr);
         for (size_t i = 0; i < count; ++i) {
-            if (levels[i] == 0 || levels[i] >= c.nq) wg::fail(wg::kInvalid, "batch: ciphertext level must be in [1, L)");
             const int64_t r = normalize_rotation(c, rots[i]);
-            if (r) c.key(WG_KEY_ROTATION, r);
+            galois[i] = r ? rotation_galois(c, r) : 0;
+            if (r) keys[i] = &c.key(WG_KEY_ROTATION, r);
         }
-        c.key(WG_KEY_RELIN, 0);
+        wg::batch_mul_relin_rescale_rotate(c, count, levels, xb, xa, yb, ya, rots, galois.data(),
+                                           &c.key(WG_KEY_RELIN, 0), keys.data(), S(stream));
+    });
+}
+
+int wg_sequence_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_t* levels, uint64_t* const* xb,
+                                         uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                                         const int64_t* rots, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        cudaStream_t s = S(stream);
+        check_batch(c, count, levels, xb, xa, yb, ya, rots);
         uint64_t* c2 = scratch_after_switch(c, s) + 2 * c.nq * c.N;
         for (size_t i = 0; i < count; ++i) {
             const size_t lv = levels[i];

@@ -8,9 +8,70 @@
 
 namespace wg {
 
+static bool capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (s) cudaStreamIsCapturing(s, &cs);
+    return cs != cudaStreamCaptureStatusNone;
+}
+
+void BatchBuffers::ensure_jobs(const Context& c, size_t bytes, cudaStream_t s) {
+    if (bytes <= jobs_bytes) return;
+    if (capturing(s)) fail(kRuntime, "batched job tables must be sized (one uncaptured call) before graph capture");
+    if (staged_event) cudaEventSynchronize(staged_event);
+    check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+    cudaFree(d_jobs);
+    cudaFreeHost(h_jobs);
+    d_jobs = h_jobs = nullptr;
+    jobs_bytes = 0;
+    const size_t cap = bytes + bytes / 2 + 4096;
+    if (cudaMalloc(&d_jobs, cap) != cudaSuccess || cudaMallocHost(&h_jobs, cap) != cudaSuccess) {
+        cudaGetLastError();
+        fail(kNoMemory, "batched job-table allocation failed");
+    }
+    jobs_bytes = cap;
+    if (!staged_event) check_cuda(cudaEventCreateWithFlags(&staged_event, cudaEventDisableTiming), "event");
+}
+
+uint64_t* BatchBuffers::arena(const Context& c, size_t words, cudaStream_t s) {
+    if (words <= arena_words) return d_arena;
+    if (capturing(s)) fail(kRuntime, "batched scratch must be sized (one uncaptured call) before graph capture");
+    check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+    cudaDeviceSynchronize();  // a smaller arena may still be in use by queued work
+    cudaFree(d_arena);
+    d_arena = nullptr;
+    arena_words = 0;
+    if (cudaMalloc(&d_arena, words * 8) != cudaSuccess) {
+        cudaGetLastError();
+        fail(kNoMemory, "batched scratch allocation failed");
+    }
+    arena_words = words;
+    return d_arena;
+}
+
+void BatchBuffers::release() {
+    if (staged_event) cudaEventSynchronize(staged_event);
+    cudaFree(d_jobs);
+    cudaFreeHost(h_jobs);
+    cudaFree(d_arena);
+    if (staged_event) cudaEventDestroy(staged_event);
+    d_jobs = h_jobs = nullptr;
+    d_arena = nullptr;
+    staged_event = nullptr;
+}
+
+BatchBuffers& Context::batch_buffers(cudaStream_t s) {
+    std::lock_guard<std::mutex> g(ws_mutex);
+    auto it = batches.find(s);
+    if (it != batches.end()) return it->second;
+    if (capturing(s)) fail(kRuntime, "batched buffers for this stream must be reserved before graph capture");
+    return batches[s];
+}
+
 Context::~Context() {
     for (auto& kv : keys) cudaFree(kv.second.d_data);
     for (auto& kv : workspaces) cudaFree(kv.second.base);
+    for (auto& kv : batches) kv.second.release();
+    cudaFree(d_modup);
     cudaFree(d_mod);
     cudaFree(d_tw);
     cudaFree(d_tables);
@@ -114,6 +175,19 @@ Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t
     for (size_t level = 0; level < nq; ++level) {
         c->fold_inv[level] = T + H.fold_inv[level];
         c->fold_inv_s[level] = T + H.fold_inv_s[level];
+    }
+    {
+        std::vector<ModUpDesc> flat(nq * dnum);
+        for (size_t level = 0; level < nq; ++level)
+            for (size_t part = 0; part < c->modup[level].size(); ++part) flat[level * dnum + part] = c->modup[level][part];
+        dev_alloc((void**)&c->d_modup, flat.size() * sizeof(ModUpDesc));
+        check_cuda(cudaMemcpy(c->d_modup, flat.data(), flat.size() * sizeof(ModUpDesc), cudaMemcpyHostToDevice),
+                   "upload ModUp descriptors");
+    }
+    c->rs_host_off.assign(nq, 0);
+    for (size_t d = 1; d < nq; ++d) {
+        c->rs_host_off[d] = c->rs_host.size();
+        c->rs_host.insert(c->rs_host.end(), H.words.begin() + H.rescale[d], H.words.begin() + H.rescale[d] + 4 * d);
     }
     c->rs_one_s.assign(nq, nullptr);
     c->rs_inv_p.assign(nq, nullptr);

@@ -78,6 +78,21 @@ struct Workspace {
     size_t words = 0;
 };
 
+struct Context;
+// Per-stream buffers of the batched path: the job-table image (pinned stage + device copy)
+// and a scratch arena, both grown on demand outside stream capture.
+struct BatchBuffers {
+    void* d_jobs = nullptr;
+    void* h_jobs = nullptr;
+    size_t jobs_bytes = 0;
+    cudaEvent_t staged_event = nullptr;
+    uint64_t* d_arena = nullptr;
+    size_t arena_words = 0;
+    void ensure_jobs(const Context& c, size_t bytes, cudaStream_t s);
+    uint64_t* arena(const Context& c, size_t words, cudaStream_t s);
+    void release();
+};
+
 struct Context {
     int device = 0;
     uint64_t N = 0;
@@ -100,6 +115,13 @@ struct Context {
     std::map<std::pair<int, int64_t>, KeyEntry> keys;
     std::mutex ws_mutex;
     std::map<cudaStream_t, Workspace> workspaces;  // one per stream, allocated on first use
+    std::map<cudaStream_t, BatchBuffers> batches;   // batched-path buffers per stream
+    ModUpDesc* d_modup = nullptr;                  // device copy of modup, [level * dnum + part]
+    // host copy of the rescale constants: for dropped limb d at rs_host_off[d]:
+    // one_s[d], inv_p[d], inv_p_s[d], half[d]
+    std::vector<uint64_t> rs_host;
+    std::vector<size_t> rs_host_off;
+    BatchBuffers& batch_buffers(cudaStream_t s);
 
     ~Context();
     uint64_t* workspace(cudaStream_t s);   // scratch for one in-flight operation on stream s
@@ -150,6 +172,16 @@ struct Probe {
 // ---------------------------------------------------------------------------------------
 // Kernel launchers.
 // ---------------------------------------------------------------------------------------
+// One limb of a job-table NTT: the first phase reads src and writes dst, the second phase
+// works in place on dst (src == dst for an in-place transform).
+struct NttJob {
+    const uint64_t* src;
+    uint64_t* dst;
+    int mod;
+    int pad;
+};
+void ntt_jobs(const Context& c, const NttJob* d_jobs, int njobs, bool forward, cudaStream_t s);
+
 // NTT over `polys` polynomials of `limbs` limbs each, `poly_stride` words apart.
 void ntt_forward(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride,
                  LimbMap map, cudaStream_t s);

@@ -32,17 +32,35 @@ __device__ __forceinline__ void ntt_rounds(std::integer_sequence<int, RD...>, ui
     ((ntt_round<LOGN, FWD, COLS, RD>(sm, sub, o, tile, q, tw, tws), __syncthreads()), ...);
 }
 
-template <int LOGN, bool FWD, bool COLS>
+// Addressing of one limb: either a strided batch (blockIdx.y = limb, blockIdx.z = polynomial,
+// modulus from a LimbMap) or an entry of a job table (blockIdx.y + 65535 * blockIdx.z).  The
+// first phase may read from a different buffer than it writes (src -> dst); the second phase
+// works in place on dst.
+template <int LOGN, bool FWD, bool COLS, bool TABLE>
 __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS)
-    k_ntt_phase(uint64_t* __restrict__ data, size_t poly_stride, LimbMap map,
-                const Modulus* __restrict__ mods, const uint64_t* __restrict__ tw_base) {
+    k_ntt_phase(uint64_t* __restrict__ data, size_t poly_stride, LimbMap map, const NttJob* __restrict__ jobs,
+                int njobs, const Modulus* __restrict__ mods, const uint64_t* __restrict__ tw_base) {
     using P = Phase<LOGN, FWD, COLS>;
     constexpr int N = P::N;
+    constexpr bool FIRST = FWD ? COLS : !COLS;
     __shared__ uint64_t sm[P::TILE + P::TILE / 16];
 
-    const int limb = blockIdx.y;
-    uint64_t* __restrict__ x = data + (size_t)blockIdx.z * poly_stride + (size_t)limb * N;
-    const int mi = map(limb);
+    const uint64_t* __restrict__ xin;
+    uint64_t* __restrict__ x;
+    int mi;
+    if (TABLE) {
+        const int j = blockIdx.y + 65535 * blockIdx.z;
+        if (j >= njobs) return;
+        const NttJob job = jobs[j];
+        x = job.dst;
+        xin = FIRST ? job.src : job.dst;
+        mi = job.mod;
+    } else {
+        const int limb = blockIdx.y;
+        x = data + (size_t)blockIdx.z * poly_stride + (size_t)limb * N;
+        xin = x;
+        mi = map(limb);
+    }
     const uint64_t q = mods[mi].q;
     const uint64_t* tw = tw_base + (size_t)mi * 4 * N + (FWD ? 0 : 2 * N);
     const uint64_t* tws = tw + N;
@@ -52,7 +70,7 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS)
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int e = t + k * P::THREADS;
-        sm[pad16(e)] = x[tile_offset<LOGN, FWD, COLS>(tile, e)];
+        sm[pad16(e)] = xin[tile_offset<LOGN, FWD, COLS>(tile, e)];
     }
     __syncthreads();
 
@@ -77,38 +95,45 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS)
 
 template <int LOGN, bool FWD, bool COLS>
 void launch_phase(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map,
-                  cudaStream_t s) {
+                  const NttJob* jobs, int njobs, cudaStream_t s) {
     using P = Phase<LOGN, FWD, COLS>;
-    const dim3 grid(P::N / P::TILE, limbs, polys);
-    // algorithmic bytes: every residue read once and written once
-    Probe probe(kClsNtt, 16.0 * P::N * limbs * polys, s);
-    k_ntt_phase<LOGN, FWD, COLS><<<grid, P::THREADS, 0, s>>>(data, stride, map, c.d_mod, c.d_tw);
-}
-
-template <int LOGN>
-void run(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map, bool fwd,
-         cudaStream_t s) {
-    if (fwd) {
-        launch_phase<LOGN, true, true>(c, data, limbs, polys, stride, map, s);
-        launch_phase<LOGN, true, false>(c, data, limbs, polys, stride, map, s);
+    if (jobs) {
+        const dim3 grid(P::N / P::TILE, njobs < 65535 ? njobs : 65535, (njobs + 65534) / 65535);
+        Probe probe(kClsNtt, 16.0 * P::N * njobs, s);
+        k_ntt_phase<LOGN, FWD, COLS, true><<<grid, P::THREADS, 0, s>>>(nullptr, 0, map, jobs, njobs, c.d_mod, c.d_tw);
     } else {
-        launch_phase<LOGN, false, false>(c, data, limbs, polys, stride, map, s);
-        launch_phase<LOGN, false, true>(c, data, limbs, polys, stride, map, s);
+        const dim3 grid(P::N / P::TILE, limbs, polys);
+        // algorithmic bytes: every residue read once and written once
+        Probe probe(kClsNtt, 16.0 * P::N * limbs * polys, s);
+        k_ntt_phase<LOGN, FWD, COLS, false><<<grid, P::THREADS, 0, s>>>(data, stride, map, nullptr, 0, c.d_mod,
+                                                                        c.d_tw);
     }
 }
 
-void dispatch(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map, bool fwd,
-              cudaStream_t s) {
-    if (limbs <= 0 || polys <= 0) return;
-    if (polys > 65535 || limbs > 65535) fail(kInvalid, "ntt: too many limbs or polynomials in one batch");
+template <int LOGN>
+void run(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map, const NttJob* jobs,
+         int njobs, bool fwd, cudaStream_t s) {
+    if (fwd) {
+        launch_phase<LOGN, true, true>(c, data, limbs, polys, stride, map, jobs, njobs, s);
+        launch_phase<LOGN, true, false>(c, data, limbs, polys, stride, map, jobs, njobs, s);
+    } else {
+        launch_phase<LOGN, false, false>(c, data, limbs, polys, stride, map, jobs, njobs, s);
+        launch_phase<LOGN, false, true>(c, data, limbs, polys, stride, map, jobs, njobs, s);
+    }
+}
+
+void dispatch(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map,
+              const NttJob* jobs, int njobs, bool fwd, cudaStream_t s) {
+    if (jobs ? njobs <= 0 : (limbs <= 0 || polys <= 0)) return;
+    if (!jobs && (polys > 65535 || limbs > 65535)) fail(kInvalid, "ntt: too many limbs or polynomials in one batch");
     switch (c.logN) {
-        case 10: run<10>(c, data, limbs, polys, stride, map, fwd, s); break;
-        case 11: run<11>(c, data, limbs, polys, stride, map, fwd, s); break;
-        case 12: run<12>(c, data, limbs, polys, stride, map, fwd, s); break;
-        case 13: run<13>(c, data, limbs, polys, stride, map, fwd, s); break;
-        case 14: run<14>(c, data, limbs, polys, stride, map, fwd, s); break;
-        case 15: run<15>(c, data, limbs, polys, stride, map, fwd, s); break;
-        case 16: run<16>(c, data, limbs, polys, stride, map, fwd, s); break;
+        case 10: run<10>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
+        case 11: run<11>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
+        case 12: run<12>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
+        case 13: run<13>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
+        case 14: run<14>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
+        case 15: run<15>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
+        case 16: run<16>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
         default: fail(kInvalid, "ntt: ring degree must be 2^10 .. 2^16");
     }
     check_cuda(cudaGetLastError(), "ntt launch");
@@ -118,12 +143,16 @@ void dispatch(const Context& c, uint64_t* data, int limbs, int polys, size_t str
 
 void ntt_forward(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride, LimbMap map,
                  cudaStream_t s) {
-    dispatch(c, data, limbs, polys, poly_stride, map, true, s);
+    dispatch(c, data, limbs, polys, poly_stride, map, nullptr, 0, true, s);
 }
 
 void ntt_inverse(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride, LimbMap map,
                  cudaStream_t s) {
-    dispatch(c, data, limbs, polys, poly_stride, map, false, s);
+    dispatch(c, data, limbs, polys, poly_stride, map, nullptr, 0, false, s);
+}
+
+void ntt_jobs(const Context& c, const NttJob* d_jobs, int njobs, bool forward, cudaStream_t s) {
+    dispatch(c, nullptr, 0, 0, 0, LimbMap{0, 0, 0}, d_jobs, njobs, forward, s);
 }
 
 }  // namespace wg

@@ -76,6 +76,7 @@ def lib() -> C.CDLL:
         L.wg_add.argtypes = [vp, sz, vp, vp, sz, sz, vp]
         L.wg_sub.argtypes = [vp, sz, vp, vp, sz, sz, vp]
         L.wg_batch_mul_relin_rescale_rotate.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp]
+        L.wg_sequence_mul_relin_rescale_rotate.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp]
         L.wg_launch_count.argtypes = [C.c_int]
         L.wg_launch_count.restype = C.c_uint64
         L.wg_probe_begin.argtypes = [C.c_int, C.c_int]
@@ -257,12 +258,14 @@ class Context:
     def sub(self, level, x, y, npolys=1, stride=0, stream=None):
         _check(lib().wg_sub(self.h, level, _ptr(x), _ptr(y), npolys, stride, _stream(stream)))
 
-    def batch_mul_relin_rescale_rotate(self, levels, xb, xa, yb, ya, rots, stream=None):
+    def batch_mul_relin_rescale_rotate(self, levels, xb, xa, yb, ya, rots, stream=None, plain=False):
+        """mul + relin + rescale + rotate per ciphertext; batched launches, or op by op with
+        plain=True (the per-operation path)."""
         n = len(levels)
         lv = np.ascontiguousarray(levels, dtype=np.uintp)
         arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
         pxb, pxa, pyb, pya = arr(xb), arr(xa), arr(yb), arr(ya)
         r = np.ascontiguousarray(rots, dtype=np.int64)
-        _check(lib().wg_batch_mul_relin_rescale_rotate(self.h, n, lv.ctypes.data, pxb.ctypes.data, pxa.ctypes.data,
-                                                       pyb.ctypes.data, pya.ctypes.data, r.ctypes.data,
-                                                       _stream(stream)))
+        fn = lib().wg_sequence_mul_relin_rescale_rotate if plain else lib().wg_batch_mul_relin_rescale_rotate
+        _check(fn(self.h, n, lv.ctypes.data, pxb.ctypes.data, pxa.ctypes.data, pyb.ctypes.data, pya.ctypes.data,
+                  r.ctypes.data, _stream(stream)))

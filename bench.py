@@ -297,6 +297,16 @@ def main():
                 "avg_launch_us": 1000 * dom["ms"] / max(1, dom["launches"]),
                 "bytes_per_launch": dom["bytes"] / max(1, dom["launches"])}
 
+    # the same workload op by op (the plain per-operation GPU path)
+    def plain_step():
+        work.copy_(pristine)
+        ctx.batch_mul_relin_rescale_rotate(levels, xb, xa, yb, ya, rots, stream=stream, plain=True)
+
+    plain_step()
+    plain_launches0 = wg.launch_count()
+    plain_ms = timed(plain_step, max(1, args.steps // 2))
+    plain_launches = (wg.launch_count() - plain_launches0) / max(1, args.steps // 2)
+
     # end to end through the C ABI with host buffers: H2D of each ciphertext's active limbs
     # (x and y), the batched call, D2H of the rescaled and rotated results.
     pin_x = torch.from_numpy(host_x.view(np.int64)).pin_memory()
@@ -347,6 +357,8 @@ def main():
         "e2e": {"value": count * world / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "gpu_launches": int(launches),
+        "plain_per_op": {"value": count * world / (plain_ms / 1000.0), "unit": UNIT, "ms_per_step": plain_ms,
+                         "launches_per_step": plain_launches},
         "roofline": roofline,
         "kernels": kernels,
         "cpu_baseline": cpu,

@@ -135,11 +135,20 @@ int wg_sub(wg_context* ctx, size_t level, uint64_t* x, const uint64_t* y, size_t
  * Pointer arrays are host arrays of device pointers; each x buffer must hold
  * (levels[i]+1)*N words per polynomial and receives levels[i]*N words.  The workload the
  * reference runs as ckks_mul_inplace, ckks_relin_hybrid_inplace, ckks_rescale,
- * ckks_rotate_inplace per ciphertext with OpenMP over ciphertexts. */
+ * ckks_rotate_inplace per ciphertext with OpenMP over ciphertexts.  Every stage is one launch
+ * over all ciphertexts, limbs and digits (job tables uploaded once per call). */
 int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_t* levels,
                                       uint64_t* const* xb, uint64_t* const* xa,
                                       const uint64_t* const* yb, const uint64_t* const* ya,
                                       const int64_t* rots, void* stream);
+
+/* The same workload issued op by op (one ciphertext after another, a few launches per op):
+ * the plain per-operation GPU path the batched entry point is measured against.  Results
+ * are identical to wg_batch_mul_relin_rescale_rotate. */
+int wg_sequence_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_t* levels,
+                                         uint64_t* const* xb, uint64_t* const* xa,
+                                         const uint64_t* const* yb, const uint64_t* const* ya,
+                                         const int64_t* rots, void* stream);
 
 /* Instrumentation (no counterpart in the reference, which has only one wall-clock span
  * around the AES evaluation, bench/aes_bench.cpp:264-271).  Kernel classes:

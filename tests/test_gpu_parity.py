@@ -204,6 +204,12 @@ def test_walsh15_batched_ops(wg, oracle_mod):
     ctx.batch_mul_relin_rescale_rotate(levels, [sl(dxb, i) for i in range(count)], [sl(dxa, i) for i in range(count)],
                                        [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots)
     gb, ga = _host(wg, dxb), _host(wg, dxa)
+    # the plain per-operation path gives the same residues
+    pxb, pxa = _dev(wg, xb), _dev(wg, xa)
+    ctx.batch_mul_relin_rescale_rotate(levels, [sl(pxb, i) for i in range(count)], [sl(pxa, i) for i in range(count)],
+                                       [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots,
+                                       plain=True)
+    assert (_host(wg, pxb) == gb).all() and (_host(wg, pxa) == ga).all()
     ob, oa = xb.copy(), xa.copy()
     o.batched_ops(levels, ob, oa, yb, ya, relin, [keys[r] for r in ct_rots], ct_rots, stride, 8)
     for i in range(count):
