@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--count", type=int, default=COUNT)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the op-by-op comparison pass")
+    ap.add_argument("--no-probe", action="store_true", help="skip the per-kernel event-timing passes")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass")
     return ap.parse_args()
 
 
@@ -274,7 +277,7 @@ def main():
 
     # per-kernel-class device time over the same K steps (CUDA events on the launch stream)
     kernels = {}
-    for name, cls in wg.KCLASS.items():
+    for name, cls in ([] if args.no_probe else wg.KCLASS.items()):
         wg.probe_begin(cls, 60000)
         timed(step, args.steps)
         n, kms, kbytes = wg.probe_end()
@@ -283,8 +286,8 @@ def main():
     for v in kernels.values():
         v["share"] = v["ms"] / probed_total if probed_total else None
         v["gbs"] = v["bytes"] / (v["ms"] * 1e6) if v["ms"] else None
-    dom_name = max(kernels, key=lambda k: kernels[k]["ms"])
-    dom = kernels[dom_name]
+    dom_name = max(kernels, key=lambda k: kernels[k]["ms"]) if kernels else "ntt"
+    dom = kernels.get(dom_name, {"ms": 0.0, "launches": 0, "bytes": 0.0, "gbs": None})
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -302,10 +305,12 @@ def main():
         work.copy_(pristine)
         ctx.batch_mul_relin_rescale_rotate(levels, xb, xa, yb, ya, rots, stream=stream, plain=True)
 
-    plain_step()
-    plain_launches0 = wg.launch_count()
-    plain_ms = timed(plain_step, max(1, args.steps // 2))
-    plain_launches = (wg.launch_count() - plain_launches0) / max(1, args.steps // 2)
+    plain_ms, plain_launches = None, None
+    if not args.no_plain:
+        plain_step()
+        plain_launches0 = wg.launch_count()
+        plain_ms = timed(plain_step, max(1, args.steps // 2))
+        plain_launches = (wg.launch_count() - plain_launches0) / max(1, args.steps // 2)
 
     # end to end through the C ABI with host buffers: H2D of each ciphertext's active limbs
     # (x and y), the batched call, D2H of the rescaled and rotated results.
@@ -327,9 +332,11 @@ def main():
             for j in range(2):
                 wg.memcpy_dtoh(pin_out[i, j].data_ptr(), work[i, j], nb, stream=stream)
 
-    for _ in range(args.warmup):
-        e2e_step()
-    e2e_ms = timed(e2e_step, args.steps)
+    e2e_ms = None
+    if not args.no_e2e:
+        for _ in range(args.warmup):
+            e2e_step()
+        e2e_ms = timed(e2e_step, args.steps)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -354,11 +361,11 @@ def main():
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2: ~0.9 GB of ciphertexts plus ~1.1 GB of keys per step"},
         "clocks": clk.summary(),
-        "e2e": {"value": count * world / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "e2e": {"value": count * world / (e2e_ms / 1000.0) if e2e_ms else None, "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "gpu_launches": int(launches),
-        "plain_per_op": {"value": count * world / (plain_ms / 1000.0), "unit": UNIT, "ms_per_step": plain_ms,
-                         "launches_per_step": plain_launches},
+        "plain_per_op": {"value": count * world / (plain_ms / 1000.0) if plain_ms else None, "unit": UNIT,
+                         "ms_per_step": plain_ms, "launches_per_step": plain_launches},
         "roofline": roofline,
         "kernels": kernels,
         "cpu_baseline": cpu,
