@@ -87,6 +87,10 @@ void do_rescale(wg::Context& c, size_t level, uint64_t* polys, size_t npolys, si
 
 }  // namespace
 
+namespace wg {
+void set_last_error(const std::string& m) { g_err = m; }
+}  // namespace wg
+
 extern "C" {
 
 const char* wg_last_error(void) { return g_err.c_str(); }

@@ -24,6 +24,8 @@ struct Error : std::runtime_error {
     Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 [[noreturn]] inline void fail(int code, const std::string& m) { throw Error(code, m); }
+// Message returned by wg_last_error() for the calling thread (wg_capi.cu).
+void set_last_error(const std::string& m);
 inline void check_cuda(cudaError_t e, const char* what) {
     if (e != cudaSuccess) fail(kCuda, std::string(what) + ": " + cudaGetErrorString(e));
 }

@@ -68,6 +68,7 @@ def lib() -> C.CDLL:
             f.argtypes = [vp, vp, sz, sz, C.c_int, sz, sz, vp]
         L.wg_keyswitch.argtypes = [vp, sz, vp, C.c_int, C.c_int64, vp, vp, C.c_int, C.c_int, vp]
         L.wg_rotate.argtypes = [vp, sz, vp, vp, C.c_int64, vp]
+        L.wg_rotate_noalloc.argtypes = [vp, sz, vp, vp, C.c_int64, vp]
         L.wg_conjugate.argtypes = [vp, sz, vp, vp, vp]
         L.wg_rotate_many.argtypes = [vp, sz, vp, vp, vp, sz, vp, vp]
         L.wg_mul.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp]
@@ -234,6 +235,11 @@ class Context:
 
     def rotate(self, level, b, a, rotation, stream=None):
         _check(lib().wg_rotate(self.h, level, _ptr(b), _ptr(a), int(rotation), _stream(stream)))
+
+    def rotate_noalloc(self, level, b, a, rotation, stream=None):
+        """Rotation whose scratch is the library's fixed 32 MiB static device array: no device
+        allocation happens in the call (see wg_rotate_noalloc in include/walsh_gpu.h)."""
+        _check(lib().wg_rotate_noalloc(self.h, level, _ptr(b), _ptr(a), int(rotation), _stream(stream)))
 
     def conjugate(self, level, b, a, stream=None):
         _check(lib().wg_conjugate(self.h, level, _ptr(b), _ptr(a), _stream(stream)))

@@ -142,6 +142,18 @@ int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_
                                       const uint64_t* const* yb, const uint64_t* const* ya,
                                       const int64_t* rots, void* stream);
 
+/* Rotation that allocates no device memory (no counterpart in the reference, whose
+ * operations all allocate host vectors).  For callers that cannot call cudaMalloc when they
+ * rotate: memory reserved up front by another allocator, work issued while a stream is being
+ * captured into a CUDA graph, or loops that must not trigger the synchronisation allocation
+ * can cause.  Same result as wg_rotate.  The key-switch scratch is a file-scope static device
+ * array of 32 MiB that every GPU loading the library holds until exit; a level needing more
+ * returns WG_ERR_INVALID.  All calls share that array (nothing in it needs clearing between
+ * calls), so calls that overlap on the GPU race: serialise them.  The first call on a device
+ * looks up the array's address; make it before any stream capture. */
+int wg_rotate_noalloc(wg_context* ctx, size_t level, uint64_t* b, uint64_t* a, int64_t rotation,
+                      void* stream);
+
 /* The same workload issued op by op (one ciphertext after another, a few launches per op):
  * the plain per-operation GPU path the batched entry point is measured against.  Results
  * are identical to wg_batch_mul_relin_rescale_rotate. */
