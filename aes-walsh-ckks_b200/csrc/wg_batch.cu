@@ -32,11 +32,11 @@ struct MacJob {
     int L, K, parts, alpha, key_level, i;
 };
 struct ModDownJob {
-    const uint64_t* src_p;
-    uint64_t* out;
-    const uint64_t* inv;
+    const uint64_t* src_p;  // P limbs of one accumulator (coefficient form)
+    uint64_t* out;          // L contribution limbs
+    const uint64_t* inv;    // folded P^-1 table of the level, [qi][pi]
     const uint64_t* inv_s;
-    int qmod;
+    int L;
     int pad;
 };
 struct CombineJob {
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kT) kb_moddown(const ModDownJob* jobs, int n, 
     const ModDownJob* j = job_of(jobs, n);
     if (!j) return;
     const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
-    j->out[coeff] = moddown_coeff(mods[j->qmod], mods + nq, K, j->src_p, N, coeff, j->inv, j->inv_s);
+    moddown_all_limbs(mods, nq, j->L, K, j->src_p, N, coeff, j->inv, j->inv_s, j->out);
 }
 
 __global__ void __launch_bounds__(kT) kb_combine(const CombineJob* jobs, int n, const Modulus* mods, size_t N) {
@@ -256,13 +256,14 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
                 uint64_t* ptr = acc + (poly * T + L + pi) * N;
                 intt_p.push_back({ptr, ptr, (int)(nq + pi), 0});
             }
-        for (int poly = 0; poly < 2; ++poly)
+        for (int poly = 0; poly < 2; ++poly) {
+            moddown.push_back({acc + (poly * T + L) * N, contrib + poly * L * N, c.fold_inv[level],
+                               c.fold_inv_s[level], (int)L, 0});
             for (size_t qi = 0; qi < L; ++qi) {
-                moddown.push_back({acc + (poly * T + L) * N, contrib + (poly * L + qi) * N,
-                                   c.fold_inv[level] + qi * K, c.fold_inv_s[level] + qi * K, (int)qi, 0});
                 uint64_t* ptr = contrib + (poly * L + qi) * N;
                 ntt_contrib.push_back({ptr, ptr, (int)qi, 0});
             }
+        }
         p.moddown_bytes += 8.0 * N * 2.0 * (K + L);
         const bool gal = x.galois != 0;
         for (size_t qi = 0; qi < L; ++qi) {

@@ -47,11 +47,10 @@ __global__ void __launch_bounds__(kThreads)
               const uint64_t* __restrict__ inv, const uint64_t* __restrict__ inv_s,
               uint64_t* __restrict__ contrib, size_t N) {
     const size_t coeff = (size_t)blockIdx.x * kThreads + threadIdx.x;
-    const int qi = blockIdx.y, poly = blockIdx.z;
+    const int poly = blockIdx.y;
     const int T = L + K;
     const uint64_t* src_p = acc + ((size_t)poly * T + L) * N;
-    contrib[((size_t)poly * L + qi) * N + coeff] =
-        moddown_coeff(mods[qi], mods + nq, K, src_p, N, coeff, inv + (size_t)qi * K, inv_s + (size_t)qi * K);
+    moddown_all_limbs(mods, nq, L, K, src_p, N, coeff, inv, inv_s, contrib + (size_t)poly * L * N);
 }
 
 // Combine; written in place of acc when an automorphism follows (so the gather reads a
@@ -138,7 +137,7 @@ void keyswitch(const Context& c, size_t level, const uint64_t* key_term, const K
     // 6. Folded ModDown contributions, then to evaluation form.
     {
         Probe probe(kClsModDown, 8.0 * N * 2.0 * (K + L), s);
-        k_moddown<<<dim3(gx, (unsigned)L, 2), blk, 0, s>>>(c.d_mod, (int)c.nq, (int)L, (int)K, acc,
+        k_moddown<<<dim3(gx, 2), blk, 0, s>>>(c.d_mod, (int)c.nq, (int)L, (int)K, acc,
                                                             c.fold_inv[level], c.fold_inv_s[level], contrib, N);
     }
     ntt_forward(c, contrib, (int)L, 2, L * N, LimbMap{(int)L, 0, 0}, s);

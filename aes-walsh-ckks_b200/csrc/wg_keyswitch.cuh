@@ -87,6 +87,34 @@ WG_HD uint64_t moddown_coeff(const Modulus& mq, const Modulus* __restrict__ pmod
     return sub_mod(acc, hps, q);
 }
 
+// Folded ModDown of one coefficient for Q limbs [0, L): the P residues are read and the FP64
+// alpha estimate formed once, then each limb gets its Shoup dot product (same arithmetic as
+// moddown_coeff, which recomputes both per limb).  out[qi * N + coeff] = contribution.
+WG_HD void moddown_all_limbs(const Modulus* __restrict__ mods, int nq, int L, int K,
+                             const uint64_t* __restrict__ src_p, size_t N, size_t coeff,
+                             const uint64_t* __restrict__ inv, const uint64_t* __restrict__ inv_s,
+                             uint64_t* __restrict__ out) {
+    uint64_t s[kMaxPLimbs];
+    double alpha = 0.0;
+    for (int pi = 0; pi < K; ++pi) {
+        const Modulus& mp = mods[nq + pi];
+        s[pi] = red4q(src_p[(size_t)pi * N + coeff], mp.q);
+        alpha = dfma(u2d(s[pi]), mp.inv_q, alpha);
+    }
+    uint64_t hps = round_half_up(alpha);
+    if (hps > (uint64_t)K) hps = (uint64_t)K;
+    for (int qi = 0; qi < L; ++qi) {
+        const Modulus& mq = mods[qi];
+        const uint64_t q = mq.q;
+        const uint64_t* iv = inv + (size_t)qi * K;
+        const uint64_t* ivs = inv_s + (size_t)qi * K;
+        uint64_t acc = 0;
+        for (int pi = 0; pi < K; ++pi)
+            acc = add_mod(acc, mul_shoup(barrett_u64(s[pi], q, mq.mu_hi), WG_LDG(iv + pi), WG_LDG(ivs + pi), q), q);
+        out[(size_t)qi * N + coeff] = sub_mod(acc, hps, q);
+    }
+}
+
 // Key inner product for QP limb i at one coefficient:
 //   acc_{a,b}[i] = sum_parts REDC(digit_part[i] * key_part_{a,b}[i]).
 // Source limbs of a digit use the evaluation-form key term itself (as the reference does).
@@ -101,6 +129,7 @@ WG_HD void mac_coeff(const Modulus* __restrict__ mods, int nq, int L, int K, int
     const size_t key_limbs = (size_t)key_level + 1 + K;
     const size_t klimb = is_p ? (size_t)key_level + 1 + (i - L) : (size_t)i;
     uint64_t acc_a = 0, acc_b = 0;
+#pragma unroll 4
     for (int j = 0; j < parts; ++j) {
         const int s0 = j * alpha, s1 = s0 + alpha < L ? s0 + alpha : L;
         const uint64_t d = (!is_p && i >= s0 && i < s1) ? key_term[(size_t)i * N + coeff]

@@ -27,9 +27,14 @@ using namespace ntt;
 
 template <int LOGN, bool FWD, bool COLS, int... RD>
 __device__ __forceinline__ void ntt_rounds(std::integer_sequence<int, RD...>, uint64_t* sm, int sub,
-                                           int o, int tile, uint64_t q, const uint64_t* tw,
-                                           const uint64_t* tws) {
-    ((ntt_round<LOGN, FWD, COLS, RD>(sm, sub, o, tile, q, tw, tws), __syncthreads()), ...);
+                                           int o, uint64_t q, const uint64_t* tw, const uint64_t* tws) {
+    ((ntt_round<LOGN, FWD, COLS, RD>(sm, sub, o, q, tw, tws), __syncthreads()), ...);
+}
+
+template <int LOGN, bool FWD, bool COLS>
+constexpr size_t smem_bytes() {
+    using P = Phase<LOGN, FWD, COLS>;
+    return 8 * (size_t)(P::TILE + P::TILE / 16 + 2 * P::TW);
 }
 
 // Addressing of one limb: either a strided batch (blockIdx.y = limb, blockIdx.z = polynomial,
@@ -37,13 +42,16 @@ __device__ __forceinline__ void ntt_rounds(std::integer_sequence<int, RD...>, ui
 // first phase may read from a different buffer than it writes (src -> dst); the second phase
 // works in place on dst.
 template <int LOGN, bool FWD, bool COLS, bool TABLE>
-__global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS)
+__global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS, 4)
     k_ntt_phase(uint64_t* __restrict__ data, size_t poly_stride, LimbMap map, const NttJob* __restrict__ jobs,
                 int njobs, const Modulus* __restrict__ mods, const uint64_t* __restrict__ tw_base) {
     using P = Phase<LOGN, FWD, COLS>;
     constexpr int N = P::N;
     constexpr bool FIRST = FWD ? COLS : !COLS;
-    __shared__ uint64_t sm[P::TILE + P::TILE / 16];
+    extern __shared__ uint64_t smem[];
+    uint64_t* sm = smem;                                  // data tile, padded
+    uint64_t* tw_s = smem + P::TILE + P::TILE / 16;       // staged twiddles
+    uint64_t* tws_s = tw_s + P::TW;
 
     const uint64_t* __restrict__ xin;
     uint64_t* __restrict__ x;
@@ -72,12 +80,16 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS)
         const int e = t + k * P::THREADS;
         sm[pad16(e)] = xin[tile_offset<LOGN, FWD, COLS>(tile, e)];
     }
+    for (int e = t; e < P::TW; e += P::THREADS) {
+        const size_t src = twiddle_src<LOGN, FWD, COLS>(tile, e);
+        tw_s[e] = __ldg(tw + src);
+        tws_s[e] = __ldg(tws + src);
+    }
     __syncthreads();
 
     const int sub = COLS ? t % P::SUBS : t >> P::OB;
     const int o = COLS ? t / P::SUBS : t & ((1 << P::OB) - 1);
-    ntt_rounds<LOGN, FWD, COLS>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, tile, q,
-                                tw, tws);
+    ntt_rounds<LOGN, FWD, COLS>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, q, tw_s, tws_s);
 
     uint64_t n_inv = 0, n_inv_s = 0;
     if (P::LAST && !FWD) {
@@ -93,20 +105,34 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS)
     }
 }
 
+template <int LOGN, bool FWD, bool COLS, bool TABLE>
+void enable_smem() {
+    // opt in to more than 48 KiB of dynamic shared memory once per kernel instance
+    static const bool done = [] {
+        cudaFuncSetAttribute(k_ntt_phase<LOGN, FWD, COLS, TABLE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_bytes<LOGN, FWD, COLS>());
+        return true;
+    }();
+    (void)done;
+}
+
 template <int LOGN, bool FWD, bool COLS>
 void launch_phase(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map,
                   const NttJob* jobs, int njobs, cudaStream_t s) {
     using P = Phase<LOGN, FWD, COLS>;
+    constexpr size_t sm = smem_bytes<LOGN, FWD, COLS>();
     if (jobs) {
+        enable_smem<LOGN, FWD, COLS, true>();
         const dim3 grid(P::N / P::TILE, njobs < 65535 ? njobs : 65535, (njobs + 65534) / 65535);
         Probe probe(kClsNtt, 16.0 * P::N * njobs, s);
-        k_ntt_phase<LOGN, FWD, COLS, true><<<grid, P::THREADS, 0, s>>>(nullptr, 0, map, jobs, njobs, c.d_mod, c.d_tw);
+        k_ntt_phase<LOGN, FWD, COLS, true><<<grid, P::THREADS, sm, s>>>(nullptr, 0, map, jobs, njobs, c.d_mod, c.d_tw);
     } else {
+        enable_smem<LOGN, FWD, COLS, false>();
         const dim3 grid(P::N / P::TILE, limbs, polys);
         // algorithmic bytes: every residue read once and written once
         Probe probe(kClsNtt, 16.0 * P::N * limbs * polys, s);
-        k_ntt_phase<LOGN, FWD, COLS, false><<<grid, P::THREADS, 0, s>>>(data, stride, map, nullptr, 0, c.d_mod,
-                                                                        c.d_tw);
+        k_ntt_phase<LOGN, FWD, COLS, false><<<grid, P::THREADS, sm, s>>>(data, stride, map, nullptr, 0, c.d_mod,
+                                                                         c.d_tw);
     }
 }
 

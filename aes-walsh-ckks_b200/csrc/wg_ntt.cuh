@@ -13,6 +13,13 @@ namespace ntt {
 constexpr int kMaxTile = 2048;
 
 WG_HD int pad16(int e) { return e + (e >> 4); }
+WG_HD int floor_log2(unsigned x) {
+#if defined(__CUDA_ARCH__)
+    return 31 - __clz(x);
+#else
+    return 31 - __builtin_clz(x);
+#endif
+}
 WG_HD int insert_zero(int v, int g) {
     return ((v >> g) << (g + 1)) | (v & ((1 << g) - 1));
 }
@@ -60,13 +67,29 @@ struct Phase {
     static constexpr int OB = MB - 3;
     static constexpr int ROUNDS = (MB + 2) / 3;
     static constexpr bool LAST = FWD ? !COLS : COLS;
+    // Twiddles one CTA reads, staged in shared memory: the column phase reads table entries
+    // [0, 2^NB1); the row phase reads, for row-stage k, SUBS * 2^k contiguous entries.
+    static constexpr int TW = COLS ? (1 << NB1) : (TILE - SUBS);
     static_assert(MB >= 3, "transform too small");
 };
 
+// Table index of staged twiddle t (see Phase::TW).  Row-stage k occupies staged entries
+// [SUBS (2^k - 1), SUBS (2^(k+1) - 1)) and maps to table entries starting at
+// 2^(NB1 + k) + tile * SUBS * 2^k.
+template <int LOGN, bool FWD, bool COLS>
+WG_HD size_t twiddle_src(int tile, int t) {
+    using P = Phase<LOGN, FWD, COLS>;
+    if (COLS) return (size_t)t;
+    const int k = floor_log2((unsigned)(t / P::SUBS + 1));
+    const int off = P::SUBS * ((1 << k) - 1);
+    return ((size_t)1 << (P::NB1 + k)) + (size_t)tile * P::SUBS * ((size_t)1 << k) + (size_t)(t - off);
+}
+
+// One round (up to three radix-2 stages) for thread (sub, o); tw / tws are the staged
+// twiddles of this CTA (twiddle_src order).
 template <int LOGN, bool FWD, bool COLS, int RD>
-WG_HD void ntt_round(uint64_t* sm, int sub, int o, int tile, uint64_t q,
-                                          const uint64_t* __restrict__ tw,
-                                          const uint64_t* __restrict__ tws) {
+WG_HD void ntt_round(uint64_t* sm, int sub, int o, uint64_t q, const uint64_t* __restrict__ tw,
+                     const uint64_t* __restrict__ tws) {
     using P = Phase<LOGN, FWD, COLS>;
     constexpr RoundPlan plan = make_plan<P::MB, FWD>(RD);
     const uint64_t two_q = q << 1;
@@ -86,21 +109,15 @@ WG_HD void ntt_round(uint64_t* sm, int sub, int o, int tile, uint64_t q,
     for (int s = 0; s < plan.ns; ++s) {
         const int b = plan.sb[s];
         const int jb = plan.jb[s];
-        const int gb = COLS ? P::NB2 + b : b;  // global index bit of this stage
+        // The table index of a pair is (1 << (n-1-gb)) + (x >> (gb+1)) for its global index x
+        // and stage bit gb; relative to the staged block it is:
+        const int base_idx = COLS ? (1 << (P::NB1 - 1 - b)) : P::SUBS * ((1 << (P::NB2 - 1 - b)) - 1) + (sub << (P::NB2 - 1 - b));
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             if ((j >> jb) & 1) continue;
             const int j1 = j | (1 << jb);
-            // Twiddle index (1 << (n-1-gb)) + (x >> (gb+1)) for the pair's global index x.
-            size_t hi;
-            if (COLS) {
-                hi = (size_t)(h[j] >> (b + 1));
-            } else {
-                const size_t row = (size_t)tile * P::SUBS + sub;
-                hi = (row << (P::NB2 - b - 1)) + (size_t)(h[j] >> (b + 1));
-            }
-            const size_t idx = ((size_t)1 << (LOGN - 1 - gb)) + hi;
-            const uint64_t w = WG_LDG(tw + idx), ws = WG_LDG(tws + idx);
+            const int idx = base_idx + (h[j] >> (b + 1));
+            const uint64_t w = tw[idx], ws = tws[idx];
             if (FWD) {
                 uint64_t t = v[j];
                 if (t >= two_q) t -= two_q;

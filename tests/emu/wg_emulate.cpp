@@ -32,15 +32,14 @@ struct Emu {
 };
 
 template <int LOGN, bool FWD, bool COLS, int... RD>
-void rounds(std::integer_sequence<int, RD...>, uint64_t* sm, int tile, uint64_t q, const uint64_t* tw,
-            const uint64_t* tws) {
+void rounds(std::integer_sequence<int, RD...>, uint64_t* sm, uint64_t q, const uint64_t* tw, const uint64_t* tws) {
     using P = ntt::Phase<LOGN, FWD, COLS>;
     auto one = [&](auto rd_const) {
         constexpr int R = decltype(rd_const)::value;
         for (int t = 0; t < P::THREADS; ++t) {
             const int sub = COLS ? t % P::SUBS : t >> P::OB;
             const int o = COLS ? t / P::SUBS : t & ((1 << P::OB) - 1);
-            ntt::ntt_round<LOGN, FWD, COLS, R>(sm, sub, o, tile, q, tw, tws);
+            ntt::ntt_round<LOGN, FWD, COLS, R>(sm, sub, o, q, tw, tws);
         }
     };
     (one(std::integral_constant<int, RD>{}), ...);
@@ -53,10 +52,15 @@ void phase(const Emu& E, uint64_t* x, int mi) {
     const uint64_t* tw = E.H.tw.data() + (size_t)mi * 4 * N + (FWD ? 0 : 2 * N);
     const uint64_t* tws = tw + N;
     const Modulus& md = E.H.mods[mi];
-    std::vector<uint64_t> sm(P::TILE + P::TILE / 16);
+    std::vector<uint64_t> sm(P::TILE + P::TILE / 16), tw_s(P::TW), tws_s(P::TW);
     for (int tile = 0; tile < (int)(N / P::TILE); ++tile) {
         for (int e = 0; e < P::TILE; ++e) sm[ntt::pad16(e)] = x[ntt::tile_offset<LOGN, FWD, COLS>(tile, e)];
-        rounds<LOGN, FWD, COLS>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), tile, md.q, tw, tws);
+        for (int e = 0; e < P::TW; ++e) {
+            const size_t src = ntt::twiddle_src<LOGN, FWD, COLS>(tile, e);
+            tw_s[e] = tw[src];
+            tws_s[e] = tws[src];
+        }
+        rounds<LOGN, FWD, COLS>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), md.q, tw_s.data(), tws_s.data());
         for (int e = 0; e < P::TILE; ++e) {
             uint64_t v = sm[ntt::pad16(e)];
             if (P::LAST) v = FWD ? red4q(v, md.q) : mul_shoup(v, md.n_inv, md.n_inv_shoup, md.q);
@@ -159,11 +163,9 @@ void emu_keyswitch(void* h, size_t level, const uint64_t* key_term, const uint64
         for (size_t pi = 0; pi < K; ++pi) ntt_one(E, acc + (poly * T + L + pi) * N, (int)(nq + pi), false);
     const uint64_t* W = E.H.words.data();
     for (int poly = 0; poly < 2; ++poly)
-        for (size_t qi = 0; qi < L; ++qi)
-            for (size_t c = 0; c < N; ++c)
-                contrib[(poly * L + qi) * N + c] =
-                    moddown_coeff(mods[qi], mods + nq, (int)K, acc + (poly * T + L) * N, N, c,
-                                  W + E.H.fold_inv[level] + qi * K, W + E.H.fold_inv_s[level] + qi * K);
+        for (size_t c = 0; c < N; ++c)
+            moddown_all_limbs(mods, (int)nq, (int)L, (int)K, acc + (poly * T + L) * N, N, c, W + E.H.fold_inv[level],
+                              W + E.H.fold_inv_s[level], contrib + poly * L * N);
     for (int poly = 0; poly < 2; ++poly)
         for (size_t qi = 0; qi < L; ++qi) ntt_one(E, contrib + (poly * L + qi) * N, (int)qi, true);
     if (galois == 0) {
