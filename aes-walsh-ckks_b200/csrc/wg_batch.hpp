@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "wg_internal.hpp"
@@ -30,7 +31,13 @@ struct JobTable {
     std::vector<size_t> offsets;
     void* base = nullptr;
     template <class J>
-    const J* add(const std::vector<J>& v);
+    const J* add(const std::vector<J>& v) {
+        const size_t off = (bytes.size() + 15) & ~size_t{15};
+        bytes.resize(off + v.size() * sizeof(J));
+        if (!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(J));
+        offsets.push_back(off);
+        return reinterpret_cast<const J*>(off);  // resolved against the device base by at()
+    }
     template <class J>
     const J* at(const J* off) const {
         return reinterpret_cast<const J*>(static_cast<unsigned char*>(base) + reinterpret_cast<size_t>(off));
@@ -44,5 +51,13 @@ void batch_mul_relin_rescale_rotate(Context& c, size_t count, const size_t* leve
                                     uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
                                     const int64_t* rots, const uint64_t* galois, const KeyEntry* relin,
                                     const KeyEntry* const* rot_keys, cudaStream_t s);
+
+// One baby-step / giant-step linear-transform stage (wg_bsgs.cu).
+struct LtStage;
+LtStage* lt_stage_create(Context& c, size_t level, size_t nterms, const uint64_t* indices, const uint64_t* diags,
+                         size_t baby, size_t slots, bool rescale);
+void lt_stage_destroy(LtStage* st);
+void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const* b, uint64_t* const* a,
+                    cudaStream_t s);
 
 }  // namespace wg

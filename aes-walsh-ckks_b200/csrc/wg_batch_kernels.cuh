@@ -1,0 +1,160 @@
+// Job structures and kernels of the batched path, shared by wg_batch.cu and wg_bsgs.cu.
+//
+// Block (x, y + 65535 z) runs tile x (256 coefficients) of job y of a device job table.
+#pragma once
+#include <algorithm>
+
+#include "wg_internal.hpp"
+#include "wg_keyswitch.cuh"
+
+namespace wg {
+namespace bk {
+namespace {  // each translation unit gets its own copy of the kernels
+
+constexpr int kT = 256;
+
+struct ModUpJob {
+    const ModUpDesc* desc;
+    const uint64_t* src;
+    uint64_t* digit;
+};
+struct MacJob {
+    const uint64_t* key;
+    const uint64_t* key_term;
+    const uint64_t* digits;
+    uint64_t* acc;
+    size_t part_stride;
+    int L, K, parts, alpha, key_level, i;
+};
+struct ModDownJob {
+    const uint64_t* src_p;  // P limbs of one accumulator (coefficient form)
+    uint64_t* out;          // L contribution limbs
+    const uint64_t* inv;    // folded P^-1 table of the level, [qi][pi]
+    const uint64_t* inv_s;
+    int L;
+    int pad;
+};
+struct CombineJob {
+    const uint64_t* acc;
+    const uint64_t* contrib;
+    const uint64_t* b_in;
+    const uint64_t* a_in;
+    uint64_t* b_out;
+    uint64_t* a_out;
+    int L, K, qi, b_add, a_add, pad;
+};
+struct GatherJob {
+    const uint64_t* src_b;
+    const uint64_t* src_a;
+    uint64_t* b;
+    uint64_t* a;
+    uint64_t galois;
+};
+struct TensorJob {
+    uint64_t* b1;
+    uint64_t* a1;
+    const uint64_t* b2;
+    const uint64_t* a2;
+    uint64_t* c2;
+    int mod;
+    int pad;
+};
+struct RescalePrepJob {
+    const uint64_t* drop;
+    uint64_t* rem;
+    uint64_t one_s, half;
+    int pmod, qmod;
+};
+struct RescaleFinishJob {
+    uint64_t* x;
+    const uint64_t* rem;
+    uint64_t inv_p, inv_p_s;
+    int mod, pad;
+};
+
+template <class J>
+__device__ __forceinline__ const J* job_of(const J* jobs, int n) {
+    const int j = blockIdx.y + 65535 * blockIdx.z;
+    return j < n ? jobs + j : nullptr;
+}
+
+__global__ void __launch_bounds__(kT) kb_modup(const ModUpJob* jobs, int n, const Modulus* mods, size_t N) {
+    const ModUpJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    modup_coeff(*j->desc, mods, j->src, j->digit, N, coeff);
+}
+
+__global__ void __launch_bounds__(kT) kb_mac(const MacJob* jobs, int n, const Modulus* mods, int nq, size_t N) {
+    const MacJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    mac_coeff(mods, nq, j->L, j->K, j->parts, j->alpha, j->key, j->key_level, j->key_term, j->digits, j->part_stride,
+              j->acc, N, j->i, coeff);
+}
+
+__global__ void __launch_bounds__(kT) kb_moddown(const ModDownJob* jobs, int n, const Modulus* mods, int nq, int K,
+                                                 size_t N) {
+    const ModDownJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    moddown_all_limbs(mods, nq, j->L, K, j->src_p, N, coeff, j->inv, j->inv_s, j->out);
+}
+
+__global__ void __launch_bounds__(kT) kb_combine(const CombineJob* jobs, int n, const Modulus* mods, size_t N) {
+    const CombineJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    combine_coeff(mods[j->qi].q, j->L, j->K, j->acc, j->contrib, j->b_in, j->a_in, j->b_out, j->a_out, j->b_add,
+                  j->a_add, N, j->qi, coeff);
+}
+
+__global__ void __launch_bounds__(kT) kb_gather(const GatherJob* jobs, int n, int logN) {
+    const GatherJob* j = job_of(jobs, n);
+    if (!j) return;
+    const uint32_t i = blockIdx.x * kT + threadIdx.x;
+    const uint32_t s = automorphism_src(i, j->galois, logN);
+    j->b[i] = j->src_b[s];
+    j->a[i] = j->src_a[s];
+}
+
+__global__ void __launch_bounds__(kT) kb_tensor(const TensorJob* jobs, int n, const Modulus* mods) {
+    const TensorJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const Modulus m = mods[j->mod];
+    const uint64_t xa = j->a1[k], xb = j->b1[k], ya = j->a2[k], yb = j->b2[k];
+    j->c2[k] = barrett_mul(xa, ya, m);
+    const uint64_t tmp = barrett_mul(xb, ya, m);
+    j->b1[k] = barrett_mul(xb, yb, m);
+    j->a1[k] = add_mod(barrett_mul(xa, yb, m), tmp, m.q);
+}
+
+// Same two steps as k_rescale_prep / k_rescale_finish in wg_ops.cu.
+__global__ void __launch_bounds__(kT) kb_rescale_prep(const RescalePrepJob* jobs, int n, const Modulus* mods) {
+    const RescalePrepJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const uint64_t p = mods[j->pmod].q, q = mods[j->qmod].q;
+    uint64_t shift = j->drop[k] + (p >> 1);
+    if (shift >= p) shift -= p;
+    j->rem[k] = sub_mod(reduce_shoup(shift, q, j->one_s), j->half, q);
+}
+
+__global__ void __launch_bounds__(kT) kb_rescale_finish(const RescaleFinishJob* jobs, int n, const Modulus* mods) {
+    const RescaleFinishJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const uint64_t q = mods[j->mod].q;
+    uint64_t x = j->x[k];
+    if (x >= q) x -= q;
+    j->x[k] = mul_shoup(sub_mod(x, j->rem[k], q), j->inv_p, j->inv_p_s, q);
+}
+
+dim3 grid_for(const Context& c, size_t njobs) {
+    return dim3((unsigned)(c.N / kT), (unsigned)std::min<size_t>(njobs, 65535), (unsigned)((njobs + 65534) / 65535));
+}
+
+}  // namespace
+}  // namespace bk
+}  // namespace wg

@@ -1,0 +1,496 @@
+// Baby-step / giant-step linear transform in the QP domain (one CoeffToSlot or SlotToCoeff
+// stage), batched over ciphertexts that share the stage's diagonals.
+//
+// Reference: ckks_apply_linear_transform_owned_stage_qp,
+// src/ckks/operations/bootstrap/ckks_linear_transform.cpp:1174-1407, with its helpers
+// make_direct_input_qp :487, ckks_hybrid_key_switch_hoisted_qp_rotated (ckks_keyswitch.cpp:675),
+// multiply_qp_plaintext_accumulate_pair :418, moddown_qp_poly_to_q_eval :581,
+// ckks_hybrid_key_switch_qp_from_key_term (ckks_keyswitch.cpp:854),
+// automorphism_qp_pair_accumulate :373 and moddown_qp_pair_to_q_eval :641.
+//
+// Per stage, for a batch of C ciphertexts at level l (L = l+1 Q limbs, T = L+K QP limbs):
+//   1. hoist a: iNTT, HPS ModUp per digit, NTT                       (one launch per step)
+//   2. baby steps in QP: baby 0 = (a, b) with zero P limbs; baby r = key inner product of the
+//      hoisted digits with the rotation-r key, b added on the Q limbs, automorphism applied
+//      by scattering each coefficient to its rotated slot                (one launch)
+//   3. giant inner sums: sum over the giant's diagonals of REDC(baby * diagonal), all
+//      ciphertexts in the same thread so each diagonal word is read once per batch
+//   4. giants g >= 1: single ModDown of the inner a (alpha as multiply + add, like the
+//      reference's single-polynomial ModDown), then a QP key switch of that key term with
+//      the rotation-(g * baby) key (no ModDown)
+//   5. accumulate: out = inner_0 + sum_g automorphism_g(switch_g + (0, inner_g.b))
+//   6. pair ModDown of out (alpha fused), optional rescale.
+// Every addition is an exact modular addition of canonical residues, so the order of
+// accumulation (raw sums with periodic reduction in the reference) does not change any word.
+#include <algorithm>
+#include <map>
+
+#include "../../include/walsh_gpu.h"
+#include "wg_batch.hpp"
+#include "wg_batch_kernels.cuh"
+#include "wg_internal.hpp"
+#include "wg_keyswitch.cuh"
+
+namespace wg {
+using namespace bk;
+
+struct LtStage {
+    size_t level = 0;
+    size_t nterms = 0;
+    size_t baby = 0;
+    size_t slots = 0;
+    bool rescale = false;
+    std::vector<size_t> indices;
+    uint64_t* d_diag = nullptr;  // [term][QP limbs][N], Montgomery form
+    ~LtStage() { cudaFree(d_diag); }
+};
+
+namespace {
+
+constexpr int kGiantBatch = 8;  // ciphertexts summed per thread in the giant-step kernel
+
+struct BabyJob {
+    const uint64_t* key;
+    const uint64_t* key_term;
+    const uint64_t* digits;
+    const uint64_t* b_init;  // b limb (Q limbs) or null (P limbs)
+    uint64_t* out_a;
+    uint64_t* out_b;
+    size_t part_stride;
+    uint64_t galois_inv;
+    int L, K, parts, alpha, key_level, i;
+};
+
+struct TermRef {
+    const uint64_t* diag;  // QP plaintext of the term (limb 0)
+    int slot;              // baby slot
+    int pad;
+};
+
+struct GiantJob {
+    const uint64_t* babies;  // batch base: [C][slots][2][T][N]
+    uint64_t* inner;         // batch base: [C][giants][2][T][N]
+    int term0, nterms, i, g, c0, nc;  // terms [term0, term0 + nterms) of the term table
+};
+
+struct SubJob {
+    const uint64_t* x;
+    const uint64_t* y;
+    uint64_t* out;
+    int mod;
+    int pad;
+};
+
+struct GiantInfo {
+    uint64_t galois;  // automorphism of the giant rotation (0 for giant 0)
+    int g;
+    int pad;
+};
+
+struct AccumJob {
+    const uint64_t* inner;   // this ciphertext's [giants][2][T][N]
+    const uint64_t* sw;      // this ciphertext's switch outputs [giants][2][T][N] (g >= 1 used)
+    uint64_t* out;           // [2][T][N]
+    int ngiants, i, pad0, pad1;
+};
+
+__global__ void __launch_bounds__(kT) kb_baby(const BabyJob* jobs, int n, const Modulus* mods, int nq, int logN) {
+    const BabyJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t N = size_t{1} << logN;
+    const uint32_t x = blockIdx.x * kT + threadIdx.x;
+    const Modulus& m = mods[j->i >= j->L ? nq + (j->i - j->L) : j->i];
+    uint64_t acc_a = 0, acc_b = j->b_init ? j->b_init[x] : 0;
+    mac_accumulate(m, j->L, j->K, j->parts, j->alpha, j->key, j->key_level, j->key_term, j->digits, j->part_stride,
+                   N, j->i, x, acc_a, acc_b);
+    const uint32_t dst = automorphism_src(x, j->galois_inv, logN);
+    j->out_a[dst] = acc_a;
+    j->out_b[dst] = acc_b;
+}
+
+__global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, const TermRef* __restrict__ term_table,
+                                               const Modulus* mods, int nq, int L, int T, int nslots, int ngiants,
+                                               size_t N) {
+    const GiantJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t x = (size_t)blockIdx.x * kT + threadIdx.x;
+    const int i = j->i;
+    const Modulus& m = mods[i < L ? i : nq + (i - L)];
+    const uint64_t q = m.q, qninv = m.qninv;
+    const size_t limb = (size_t)i * N + x;
+    const size_t slot_words = 2 * (size_t)T * N;
+    uint64_t acc_a[kGiantBatch], acc_b[kGiantBatch];
+#pragma unroll
+    for (int c = 0; c < kGiantBatch; ++c) acc_a[c] = acc_b[c] = 0;
+    for (int t = 0; t < j->nterms; ++t) {
+        const TermRef tr = term_table[j->term0 + t];
+        const uint64_t d = tr.diag[limb];
+#pragma unroll
+        for (int c = 0; c < kGiantBatch; ++c) {
+            if (c >= j->nc) break;
+            const uint64_t* bs = j->babies + ((size_t)(j->c0 + c) * nslots + tr.slot) * slot_words;
+            acc_a[c] = add_mod(acc_a[c], mont_mul(bs[limb], d, q, qninv), q);
+            acc_b[c] = add_mod(acc_b[c], mont_mul(bs[(size_t)T * N + limb], d, q, qninv), q);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kGiantBatch; ++c) {
+        if (c >= j->nc) break;
+        uint64_t* o = j->inner + ((size_t)(j->c0 + c) * ngiants + j->g) * slot_words;
+        o[limb] = acc_a[c];
+        o[(size_t)T * N + limb] = acc_b[c];
+    }
+}
+
+__global__ void __launch_bounds__(kT) kb_moddown_single(const ModDownJob* jobs, int n, const Modulus* mods, int nq,
+                                                        int K, size_t N) {
+    const ModDownJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    moddown_all_limbs<false>(mods, nq, j->L, K, j->src_p, N, coeff, j->inv, j->inv_s, j->out);
+}
+
+__global__ void __launch_bounds__(kT) kb_sub(const SubJob* jobs, int n, const Modulus* mods) {
+    const SubJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    j->out[k] = sub_mod(j->x[k], j->y[k], mods[j->mod].q);
+}
+
+__global__ void __launch_bounds__(kT) kb_accumulate(const AccumJob* jobs, int n, const GiantInfo* __restrict__ giants,
+                                                    const Modulus* mods, int nq, int L, int T, int logN) {
+    const AccumJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t N = size_t{1} << logN;
+    const uint32_t x = blockIdx.x * kT + threadIdx.x;
+    const int i = j->i;
+    const uint64_t q = mods[i < L ? i : nq + (i - L)].q;
+    const size_t slot_words = 2 * (size_t)T * N;
+    const size_t limb = (size_t)i * N;
+    uint64_t oa = 0, ob = 0;
+    for (int k = 0; k < j->ngiants; ++k) {
+        const GiantInfo gi = giants[k];
+        const uint64_t* in = j->inner + (size_t)gi.g * slot_words;
+        if (gi.galois == 0) {
+            oa = add_mod(oa, in[limb + x], q);
+            ob = add_mod(ob, in[(size_t)T * N + limb + x], q);
+        } else {
+            const uint32_t s = automorphism_src(x, gi.galois, logN);
+            const uint64_t* sw = j->sw + (size_t)gi.g * slot_words;
+            oa = add_mod(oa, sw[limb + s], q);
+            ob = add_mod(ob, add_mod(sw[(size_t)T * N + limb + s], in[(size_t)T * N + limb + s], q), q);
+        }
+    }
+    j->out[limb + x] = oa;
+    j->out[(size_t)T * N + limb + x] = ob;
+}
+
+}  // namespace
+
+LtStage* lt_stage_create(Context& c, size_t level, size_t nterms, const uint64_t* indices, const uint64_t* diags,
+                         size_t baby, size_t slots, bool rescale) {
+    if (level >= c.nq) fail(kInvalid, "ckks_linear_transform: invalid stage level");
+    if (nterms == 0) fail(kInvalid, "ckks_linear_transform: empty stage");
+    const size_t full = c.N / 2;
+    if (slots == 0) slots = full;
+    if (slots > full || full % slots || (slots & (slots - 1)))
+        fail(kInvalid, "ckks_linear_transform: invalid logical stage slot count");
+    if (baby == 0 || baby > slots) fail(kInvalid, "ckks_linear_transform: invalid compiled stage input");
+    for (size_t t = 0; t < nterms; ++t)
+        if (indices[t] >= slots) fail(kInvalid, "ckks_linear_transform: diagonal index out of range");
+    auto st = std::make_unique<LtStage>();
+    st->level = level;
+    st->nterms = nterms;
+    st->baby = baby;
+    st->slots = slots;
+    st->rescale = rescale;
+    st->indices.assign(indices, indices + nterms);
+    const size_t words = nterms * (level + 1 + c.np) * c.N;
+    check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+    if (cudaMalloc(&st->d_diag, words * 8) != cudaSuccess) {
+        cudaGetLastError();
+        fail(kNoMemory, "linear transform: diagonal allocation failed");
+    }
+    check_cuda(cudaMemcpy(st->d_diag, diags, words * 8, cudaMemcpyHostToDevice), "upload diagonals");
+    return st.release();
+}
+
+void lt_stage_destroy(LtStage* st) { delete st; }
+
+// Rotation keys a stage needs: baby rotations 1..baby-1 and giant rotations g * baby.
+static void stage_rotations(const LtStage& st, std::vector<size_t>& babies, std::vector<size_t>& giants,
+                            std::vector<std::vector<size_t>>& terms_by_giant) {
+    std::vector<char> baby_needed(st.baby, 0);
+    const size_t ngiants = (st.slots + st.baby - 1) / st.baby;
+    terms_by_giant.assign(ngiants, {});
+    for (size_t t = 0; t < st.nterms; ++t) {
+        baby_needed[st.indices[t] % st.baby] = 1;
+        terms_by_giant[st.indices[t] / st.baby].push_back(t);
+    }
+    babies.clear();
+    giants.clear();
+    for (size_t r = 0; r < st.baby; ++r)
+        if (baby_needed[r]) babies.push_back(r);
+    for (size_t g = 0; g < ngiants; ++g)
+        if (!terms_by_giant[g].empty()) giants.push_back(g);
+}
+
+void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const* b, uint64_t* const* a,
+                    cudaStream_t s) {
+    if (count == 0) return;
+    const size_t N = c.N, level = st.level, L = level + 1, K = c.np, T = L + K, nq = c.nq;
+    const size_t B = c.parts_at(level);
+    const size_t slots_full = N / 2;
+    std::vector<size_t> babies, giants;
+    std::vector<std::vector<size_t>> terms_by_giant;
+    stage_rotations(st, babies, giants, terms_by_giant);
+    auto rot_key = [&](size_t r) -> const KeyEntry& {
+        const int64_t rr = (int64_t)(r % slots_full);
+        if (rr == 0) fail(kInvalid, "ckks_linear_transform: zero rotation");
+        auto it = c.keys.find({WG_KEY_ROTATION, rr});
+        if (it == c.keys.end()) fail(kInvalid, "ckks_linear_transform: missing baby-step or giant-step rotation key");
+        if (it->second.key_level < level || it->second.parts < B) fail(kRuntime, "keyswitch: unusable rotation key");
+        return it->second;
+    };
+    auto galois_of = [&](size_t r) { return host::powmod(5, (uint64_t)(r % slots_full), 2 * N); };
+    // Slot of each needed baby value and the giants with terms.
+    std::map<size_t, int> slot_of;
+    for (size_t k = 0; k < babies.size(); ++k) slot_of[babies[k]] = (int)k;
+    const size_t ns = babies.size(), ng = giants.size();
+    std::map<size_t, int> gidx;
+    for (size_t k = 0; k < ng; ++k) gidx[giants[k]] = (int)k;
+
+    // Arena layout.
+    const size_t w_coeff = count * L * N;
+    const size_t w_digits = count * B * T * N;
+    const size_t w_babies = count * ns * 2 * T * N;
+    const size_t w_inner = count * ng * 2 * T * N;
+    const size_t w_csingle = count * ng * L * N;
+    const size_t w_coeff2 = count * ng * L * N;
+    const size_t w_digits2 = count * ng * B * T * N;
+    const size_t w_switch = count * ng * 2 * T * N;
+    const size_t w_out = count * 2 * T * N;
+    const size_t w_cfinal = count * 2 * L * N;
+    const size_t w_rem = count * 2 * L * N;
+    uint64_t* base = c.batch_buffers(s).arena(c, w_coeff + w_digits + w_babies + w_inner + w_csingle + w_coeff2 +
+                                                     w_digits2 + w_switch + w_out + w_cfinal + w_rem, s);
+    uint64_t* coeff = base;
+    uint64_t* digits = coeff + w_coeff;
+    uint64_t* babybuf = digits + w_digits;
+    uint64_t* inner = babybuf + w_babies;
+    uint64_t* csingle = inner + w_inner;
+    uint64_t* coeff2 = csingle + w_csingle;
+    uint64_t* digits2 = coeff2 + w_coeff2;
+    uint64_t* sw = digits2 + w_digits2;
+    uint64_t* out = sw + w_switch;
+    uint64_t* cfinal = out + w_out;
+    uint64_t* rem = cfinal + w_cfinal;
+    const size_t slotw = 2 * T * N;
+    auto modq = [&](size_t limb) { return (int)(limb < L ? limb : nq + (limb - L)); };
+
+    JobTable t;
+    // 1. hoist
+    std::vector<NttJob> intt_a, ntt_dig;
+    std::vector<ModUpJob> modup;
+    for (size_t ci = 0; ci < count; ++ci) {
+        uint64_t* cf = coeff + ci * L * N;
+        uint64_t* dg = digits + ci * B * T * N;
+        for (size_t l = 0; l < L; ++l) intt_a.push_back({a[ci] + l * N, cf + l * N, (int)l, 0});
+        for (size_t j = 0; j < B; ++j) {
+            modup.push_back({c.d_modup + level * c.dnum + j, cf, dg + j * T * N});
+            const size_t s0 = j * c.alpha, s1 = std::min(s0 + c.alpha, L);
+            for (size_t l = 0; l < T; ++l)
+                if (l < s0 || l >= s1) ntt_dig.push_back({dg + j * T * N + l * N, dg + j * T * N + l * N, modq(l), 0});
+        }
+    }
+    // 2. babies: baby 0 as a copy (P limbs zeroed below), others by MAC + scatter
+    std::vector<BabyJob> baby_jobs;
+    const bool baby0 = !babies.empty() && babies[0] == 0;
+    for (size_t ci = 0; ci < count; ++ci) {
+        for (size_t k = 0; k < ns; ++k) {
+            uint64_t* slot = babybuf + (ci * ns + k) * slotw;
+            if (babies[k] == 0) continue;
+            const KeyEntry& key = rot_key(babies[k]);
+            const uint64_t ginv = host::powmod(galois_of(babies[k]), N - 1, 2 * N);
+            for (size_t i = 0; i < T; ++i)
+                baby_jobs.push_back({key.d_data, a[ci], digits + ci * B * T * N, i < L ? b[ci] + i * N : nullptr,
+                                     slot + i * N, slot + T * N + i * N, T * N, ginv, (int)L, (int)K, (int)B,
+                                     (int)c.alpha, (int)key.key_level, (int)i});
+        }
+    }
+    // 3. giant sums
+    std::vector<TermRef> terms;
+    std::vector<GiantJob> giant_jobs;
+    const size_t qp_words = T * N;
+    for (size_t gk = 0; gk < ng; ++gk) {
+        const auto& tl = terms_by_giant[giants[gk]];
+        const size_t off = terms.size();
+        for (size_t term : tl)
+            terms.push_back({st.d_diag + term * qp_words, slot_of[st.indices[term] % st.baby], 0});
+        for (size_t c0 = 0; c0 < count; c0 += kGiantBatch)
+            for (size_t i = 0; i < T; ++i)
+                giant_jobs.push_back({babybuf, inner, (int)off, (int)tl.size(), (int)i, (int)gk, (int)c0,
+                                      (int)std::min<size_t>(kGiantBatch, count - c0)});
+    }
+    // 4. giants >= 1: single ModDown of inner a, then QP key switch from that key term
+    std::vector<NttJob> intt_pg, ntt_cs, intt_kt, ntt_dig2;
+    std::vector<ModDownJob> md_single;
+    std::vector<SubJob> kt_sub;
+    std::vector<ModUpJob> modup2;
+    std::vector<MacJob> mac2;
+    for (size_t ci = 0; ci < count; ++ci)
+        for (size_t gk = 0; gk < ng; ++gk) {
+            if (giants[gk] == 0) continue;
+            const KeyEntry& key = rot_key(giants[gk] * st.baby);
+            uint64_t* in_a = inner + (ci * ng + gk) * slotw;
+            uint64_t* cs = csingle + (ci * ng + gk) * L * N;
+            for (size_t pi = 0; pi < K; ++pi) {
+                uint64_t* p = in_a + (L + pi) * N;
+                intt_pg.push_back({p, p, (int)(nq + pi), 0});
+            }
+            md_single.push_back({in_a + L * N, cs, c.fold_inv[level], c.fold_inv_s[level], (int)L, 0});
+            for (size_t qi = 0; qi < L; ++qi) {
+                ntt_cs.push_back({cs + qi * N, cs + qi * N, (int)qi, 0});
+                kt_sub.push_back({in_a + qi * N, cs + qi * N, in_a + qi * N, (int)qi, 0});
+            }
+            uint64_t* cf2 = coeff2 + (ci * ng + gk) * L * N;
+            uint64_t* dg2 = digits2 + (ci * ng + gk) * B * T * N;
+            uint64_t* acc = sw + (ci * ng + gk) * slotw;
+            for (size_t l = 0; l < L; ++l) intt_kt.push_back({in_a + l * N, cf2 + l * N, (int)l, 0});
+            for (size_t j = 0; j < B; ++j) {
+                modup2.push_back({c.d_modup + level * c.dnum + j, cf2, dg2 + j * T * N});
+                const size_t s0 = j * c.alpha, s1 = std::min(s0 + c.alpha, L);
+                for (size_t l = 0; l < T; ++l)
+                    if (l < s0 || l >= s1)
+                        ntt_dig2.push_back({dg2 + j * T * N + l * N, dg2 + j * T * N + l * N, modq(l), 0});
+            }
+            for (size_t i = 0; i < T; ++i)
+                mac2.push_back({key.d_data, in_a, dg2, acc, T * N, (int)L, (int)K, (int)B, (int)c.alpha,
+                                (int)key.key_level, (int)i});
+        }
+    // 5. accumulation
+    std::vector<GiantInfo> ginfo;
+    for (size_t gk = 0; gk < ng; ++gk)
+        ginfo.push_back({giants[gk] == 0 ? 0 : galois_of(giants[gk] * st.baby), (int)gk, 0});
+    std::vector<AccumJob> accum;
+    for (size_t ci = 0; ci < count; ++ci)
+        for (size_t i = 0; i < T; ++i)
+            accum.push_back({inner + ci * ng * slotw, sw + ci * ng * slotw, out + ci * slotw, (int)ng, (int)i, 0, 0});
+    // 6. pair ModDown, then into the ciphertext (and rescale)
+    std::vector<NttJob> intt_po, ntt_cf;
+    std::vector<ModDownJob> md_pair;
+    std::vector<SubJob> final_sub;
+    for (size_t ci = 0; ci < count; ++ci) {
+        for (int poly = 0; poly < 2; ++poly) {
+            uint64_t* o = out + ci * slotw + poly * T * N;
+            uint64_t* cf = cfinal + (ci * 2 + poly) * L * N;
+            for (size_t pi = 0; pi < K; ++pi) intt_po.push_back({o + (L + pi) * N, o + (L + pi) * N, (int)(nq + pi), 0});
+            md_pair.push_back({o + L * N, cf, c.fold_inv[level], c.fold_inv_s[level], (int)L, 0});
+            uint64_t* dst = poly ? a[ci] : b[ci];
+            for (size_t qi = 0; qi < L; ++qi) {
+                ntt_cf.push_back({cf + qi * N, cf + qi * N, (int)qi, 0});
+                final_sub.push_back({o + qi * N, cf + qi * N, dst + qi * N, (int)qi, 0});
+            }
+        }
+    }
+    std::vector<NttJob> drop_intt, rem_ntt;
+    std::vector<RescalePrepJob> prep;
+    std::vector<RescaleFinishJob> fin;
+    if (st.rescale) {
+        if (level == 0) fail(kInvalid, "ckks_rescale: invalid level");
+        const uint64_t* rc = c.rs_host.data() + c.rs_host_off[level];
+        for (size_t ci = 0; ci < count; ++ci)
+            for (int poly = 0; poly < 2; ++poly) {
+                uint64_t* x = poly ? a[ci] : b[ci];
+                uint64_t* drop = x + level * N;
+                uint64_t* r = rem + (ci * 2 + poly) * level * N;
+                drop_intt.push_back({drop, drop, (int)level, 0});
+                for (size_t q = 0; q < level; ++q) {
+                    prep.push_back({drop, r + q * N, rc[q], rc[3 * level + q], (int)level, (int)q});
+                    rem_ntt.push_back({r + q * N, r + q * N, (int)q, 0});
+                    fin.push_back({x + q * N, r + q * N, rc[level + q], rc[2 * level + q], (int)q, 0});
+                }
+            }
+    }
+
+    // Baby slot 0 holds (a, b) with zero P limbs: copy Q limbs, clear P limbs.
+    for (size_t ci = 0; ci < count && baby0; ++ci) {
+        uint64_t* slot = babybuf + (ci * ns + 0) * slotw;
+        check_cuda(cudaMemcpyAsync(slot, a[ci], L * N * 8, cudaMemcpyDeviceToDevice, s), "baby 0");
+        check_cuda(cudaMemcpyAsync(slot + T * N, b[ci], L * N * 8, cudaMemcpyDeviceToDevice, s), "baby 0");
+        check_cuda(cudaMemsetAsync(slot + L * N, 0, K * N * 8, s), "baby 0");
+        check_cuda(cudaMemsetAsync(slot + T * N + L * N, 0, K * N * 8, s), "baby 0");
+    }
+
+    const NttJob* j_intt_a = t.add(intt_a);
+    const ModUpJob* j_modup = t.add(modup);
+    const NttJob* j_ntt_dig = t.add(ntt_dig);
+    const BabyJob* j_baby = t.add(baby_jobs);
+    const TermRef* j_terms = t.add(terms);
+    const GiantJob* j_giant = t.add(giant_jobs);
+    const NttJob* j_intt_pg = t.add(intt_pg);
+    const ModDownJob* j_mds = t.add(md_single);
+    const NttJob* j_ntt_cs = t.add(ntt_cs);
+    const SubJob* j_kt_sub = t.add(kt_sub);
+    const NttJob* j_intt_kt = t.add(intt_kt);
+    const ModUpJob* j_modup2 = t.add(modup2);
+    const NttJob* j_ntt_dig2 = t.add(ntt_dig2);
+    const MacJob* j_mac2 = t.add(mac2);
+    const GiantInfo* j_ginfo = t.add(ginfo);
+    const AccumJob* j_accum = t.add(accum);
+    const NttJob* j_intt_po = t.add(intt_po);
+    const ModDownJob* j_mdp = t.add(md_pair);
+    const NttJob* j_ntt_cf = t.add(ntt_cf);
+    const SubJob* j_final = t.add(final_sub);
+    const NttJob* j_drop = t.add(drop_intt);
+    const RescalePrepJob* j_prep = t.add(prep);
+    const NttJob* j_rem = t.add(rem_ntt);
+    const RescaleFinishJob* j_fin = t.add(fin);
+    t.upload(c, s);
+    // 1.
+    ntt_jobs(c, t.at(j_intt_a), (int)intt_a.size(), false, s);
+    kb_modup<<<grid_for(c, modup.size()), kT, 0, s>>>(t.at(j_modup), (int)modup.size(), c.d_mod, N);
+    ntt_jobs(c, t.at(j_ntt_dig), (int)ntt_dig.size(), true, s);
+    // 2.
+    if (!baby_jobs.empty()) {
+        Probe probe(kClsKeyMac, 8.0 * N * baby_jobs.size() * (3.0 * B + 3.0), s);
+        kb_baby<<<grid_for(c, baby_jobs.size()), kT, 0, s>>>(t.at(j_baby), (int)baby_jobs.size(), c.d_mod, (int)nq,
+                                                             c.logN);
+    }
+    // 3.
+    {
+        Probe probe(kClsElementwise, 8.0 * N * (double)(st.nterms * T + count * (ns + ng) * 2 * T), s);
+        kb_giant<<<grid_for(c, giant_jobs.size()), kT, 0, s>>>(t.at(j_giant), (int)giant_jobs.size(), t.at(j_terms),
+                                                               c.d_mod, (int)nq, (int)L, (int)T, (int)ns, (int)ng, N);
+    }
+    // 4.
+    if (!md_single.empty()) {
+        ntt_jobs(c, t.at(j_intt_pg), (int)intt_pg.size(), false, s);
+        kb_moddown_single<<<grid_for(c, md_single.size()), kT, 0, s>>>(t.at(j_mds), (int)md_single.size(), c.d_mod,
+                                                                       (int)nq, (int)K, N);
+        ntt_jobs(c, t.at(j_ntt_cs), (int)ntt_cs.size(), true, s);
+        kb_sub<<<grid_for(c, kt_sub.size()), kT, 0, s>>>(t.at(j_kt_sub), (int)kt_sub.size(), c.d_mod);
+        ntt_jobs(c, t.at(j_intt_kt), (int)intt_kt.size(), false, s);
+        kb_modup<<<grid_for(c, modup2.size()), kT, 0, s>>>(t.at(j_modup2), (int)modup2.size(), c.d_mod, N);
+        ntt_jobs(c, t.at(j_ntt_dig2), (int)ntt_dig2.size(), true, s);
+        Probe probe(kClsKeyMac, 8.0 * N * mac2.size() * (3.0 * B + 2.0), s);
+        kb_mac<<<grid_for(c, mac2.size()), kT, 0, s>>>(t.at(j_mac2), (int)mac2.size(), c.d_mod, (int)nq, N);
+    }
+    // 5.
+    kb_accumulate<<<grid_for(c, accum.size()), kT, 0, s>>>(t.at(j_accum), (int)accum.size(), t.at(j_ginfo), c.d_mod,
+                                                           (int)nq, (int)L, (int)T, c.logN);
+    // 6.
+    ntt_jobs(c, t.at(j_intt_po), (int)intt_po.size(), false, s);
+    kb_moddown<<<grid_for(c, md_pair.size()), kT, 0, s>>>(t.at(j_mdp), (int)md_pair.size(), c.d_mod, (int)nq, (int)K, N);
+    ntt_jobs(c, t.at(j_ntt_cf), (int)ntt_cf.size(), true, s);
+    kb_sub<<<grid_for(c, final_sub.size()), kT, 0, s>>>(t.at(j_final), (int)final_sub.size(), c.d_mod);
+    if (st.rescale) {
+        ntt_jobs(c, t.at(j_drop), (int)drop_intt.size(), false, s);
+        kb_rescale_prep<<<grid_for(c, prep.size()), kT, 0, s>>>(t.at(j_prep), (int)prep.size(), c.d_mod);
+        ntt_jobs(c, t.at(j_rem), (int)rem_ntt.size(), true, s);
+        kb_rescale_finish<<<grid_for(c, fin.size()), kT, 0, s>>>(t.at(j_fin), (int)fin.size(), c.d_mod);
+    }
+    check_cuda(cudaGetLastError(), "linear transform launch");
+}
+
+}  // namespace wg

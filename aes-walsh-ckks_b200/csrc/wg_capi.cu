@@ -15,6 +15,9 @@ Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t
 struct wg_context {
     wg::Context* c;
 };
+struct wg_lt_stage {
+    wg::LtStage* s;
+};
 
 namespace {
 
@@ -359,6 +362,39 @@ int wg_sequence_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const si
             do_rescale(c, lv, xa[i], 1, 0, s);
             do_rotate(c, lv - 1, xb[i], xa[i], rots[i], s);
         }
+    });
+}
+
+int wg_lt_stage_create(wg_context* ctx, size_t level, size_t nterms, const uint64_t* indices,
+                       const uint64_t* diagonals, size_t baby_step_count, size_t slot_count, int rescale_after,
+                       wg_lt_stage** out) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        if (!out || !indices || !diagonals) wg::fail(wg::kInvalid, "ckks_linear_transform: null argument");
+        *out = nullptr;
+        wg::LtStage* st = wg::lt_stage_create(c, level, nterms, indices, diagonals, baby_step_count, slot_count,
+                                              rescale_after != 0);
+        *out = new wg_lt_stage{st};
+    });
+}
+
+void wg_lt_stage_destroy(wg_lt_stage* st) {
+    if (!st) return;
+    wg::lt_stage_destroy(st->s);
+    delete st;
+}
+
+int wg_lt_stage_apply(wg_context* ctx, const wg_lt_stage* st, size_t count, uint64_t* const* b, uint64_t* const* a,
+                      void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        if (!st || !st->s) wg::fail(wg::kInvalid, "ckks_linear_transform: null stage");
+        if (count && (!b || !a)) wg::fail(wg::kInvalid, "ckks_linear_transform: null ciphertext array");
+        for (size_t i = 0; i < count; ++i) {
+            check_ptr(b[i], "ckks_linear_transform");
+            check_ptr(a[i], "ckks_linear_transform");
+        }
+        wg::lt_stage_apply(c, *st->s, count, b, a, S(stream));
     });
 }
 

@@ -90,6 +90,10 @@ WG_HD uint64_t moddown_coeff(const Modulus& mq, const Modulus* __restrict__ pmod
 // Folded ModDown of one coefficient for Q limbs [0, L): the P residues are read and the FP64
 // alpha estimate formed once, then each limb gets its Shoup dot product (same arithmetic as
 // moddown_coeff, which recomputes both per limb).  out[qi * N + coeff] = contribution.
+// FUSED selects how the alpha sum is rounded: the reference's pair ModDown
+// (ckks_keyswitch.cpp:521-607) is compiled into an FMA, its single-polynomial ModDown
+// (ckks_keyswitch.cpp:609-673, used by the QP linear transform) into a multiply and an add.
+template <bool FUSED = true>
 WG_HD void moddown_all_limbs(const Modulus* __restrict__ mods, int nq, int L, int K,
                              const uint64_t* __restrict__ src_p, size_t N, size_t coeff,
                              const uint64_t* __restrict__ inv, const uint64_t* __restrict__ inv_s,
@@ -99,7 +103,7 @@ WG_HD void moddown_all_limbs(const Modulus* __restrict__ mods, int nq, int L, in
     for (int pi = 0; pi < K; ++pi) {
         const Modulus& mp = mods[nq + pi];
         s[pi] = red4q(src_p[(size_t)pi * N + coeff], mp.q);
-        alpha = dfma(u2d(s[pi]), mp.inv_q, alpha);
+        alpha = FUSED ? dfma(u2d(s[pi]), mp.inv_q, alpha) : dadd(alpha, dmul(u2d(s[pi]), mp.inv_q));
     }
     uint64_t hps = round_half_up(alpha);
     if (hps > (uint64_t)K) hps = (uint64_t)K;
@@ -115,20 +119,16 @@ WG_HD void moddown_all_limbs(const Modulus* __restrict__ mods, int nq, int L, in
     }
 }
 
-// Key inner product for QP limb i at one coefficient:
-//   acc_{a,b}[i] = sum_parts REDC(digit_part[i] * key_part_{a,b}[i]).
-// Source limbs of a digit use the evaluation-form key term itself (as the reference does).
-WG_HD void mac_coeff(const Modulus* __restrict__ mods, int nq, int L, int K, int parts, int alpha,
-                     const uint64_t* __restrict__ key, int key_level, const uint64_t* __restrict__ key_term,
-                     const uint64_t* __restrict__ digits, size_t part_stride, uint64_t* __restrict__ acc,
-                     size_t N, int i, size_t coeff) {
-    const int T = L + K;
+// Key inner product for QP limb i at one coefficient, added digit by digit onto (acc_a,
+// acc_b) with canonical modular additions (ckks_pointwise_multiply_accumulate_montgomery_key_lazy,
+// ckks_keyswitch.cpp:445-463).  Source limbs of a digit use the evaluation-form key term itself.
+WG_HD void mac_accumulate(const Modulus& m, int L, int K, int parts, int alpha, const uint64_t* __restrict__ key,
+                          int key_level, const uint64_t* __restrict__ key_term, const uint64_t* __restrict__ digits,
+                          size_t part_stride, size_t N, int i, size_t coeff, uint64_t& acc_a, uint64_t& acc_b) {
     const bool is_p = i >= L;
-    const Modulus& m = mods[is_p ? nq + (i - L) : i];
     const uint64_t q = m.q, qninv = m.qninv;
     const size_t key_limbs = (size_t)key_level + 1 + K;
     const size_t klimb = is_p ? (size_t)key_level + 1 + (i - L) : (size_t)i;
-    uint64_t acc_a = 0, acc_b = 0;
 #pragma unroll 4
     for (int j = 0; j < parts; ++j) {
         const int s0 = j * alpha, s1 = s0 + alpha < L ? s0 + alpha : L;
@@ -139,6 +139,19 @@ WG_HD void mac_coeff(const Modulus* __restrict__ mods, int nq, int L, int K, int
         acc_a = add_mod(acc_a, mont_mul(d, ka, q, qninv), q);
         acc_b = add_mod(acc_b, mont_mul(d, kb, q, qninv), q);
     }
+}
+
+// Key inner product for QP limb i at one coefficient:
+//   acc_{a,b}[i] = sum_parts REDC(digit_part[i] * key_part_{a,b}[i]).
+// Source limbs of a digit use the evaluation-form key term itself (as the reference does).
+WG_HD void mac_coeff(const Modulus* __restrict__ mods, int nq, int L, int K, int parts, int alpha,
+                     const uint64_t* __restrict__ key, int key_level, const uint64_t* __restrict__ key_term,
+                     const uint64_t* __restrict__ digits, size_t part_stride, uint64_t* __restrict__ acc,
+                     size_t N, int i, size_t coeff) {
+    const int T = L + K;
+    const Modulus& m = mods[i >= L ? nq + (i - L) : i];
+    uint64_t acc_a = 0, acc_b = 0;
+    mac_accumulate(m, L, K, parts, alpha, key, key_level, key_term, digits, part_stride, N, i, coeff, acc_a, acc_b);
     acc[(size_t)i * N + coeff] = acc_a;
     acc[(size_t)(T + i) * N + coeff] = acc_b;
 }

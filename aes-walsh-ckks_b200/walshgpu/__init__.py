@@ -78,6 +78,10 @@ def lib() -> C.CDLL:
         L.wg_sub.argtypes = [vp, sz, vp, vp, sz, sz, vp]
         L.wg_batch_mul_relin_rescale_rotate.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp]
         L.wg_sequence_mul_relin_rescale_rotate.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp]
+        L.wg_lt_stage_create.argtypes = [vp, sz, sz, vp, vp, sz, sz, C.c_int, C.POINTER(vp)]
+        L.wg_lt_stage_destroy.argtypes = [vp]
+        L.wg_lt_stage_destroy.restype = None
+        L.wg_lt_stage_apply.argtypes = [vp, vp, sz, vp, vp, vp]
         L.wg_launch_count.argtypes = [C.c_int]
         L.wg_launch_count.restype = C.c_uint64
         L.wg_probe_begin.argtypes = [C.c_int, C.c_int]
@@ -168,6 +172,38 @@ def to_device(arr, device="cuda"):
 def to_host(t) -> np.ndarray:
     """int64 torch tensor -> uint64 numpy array (bit-identical)."""
     return t.detach().cpu().numpy().view(np.uint64).copy()
+
+
+class LtStage:
+    """One baby-step / giant-step linear-transform stage (diagonals device-resident)."""
+
+    def __init__(self, ctx, level, indices, diagonals, baby_step_count, slot_count=0, rescale=False):
+        self.ctx = ctx
+        idx = _u64(indices)
+        d = _u64(diagonals)
+        h = C.c_void_p()
+        _check(lib().wg_lt_stage_create(ctx.h, level, len(idx), idx.ctypes.data, d.ctypes.data, baby_step_count,
+                                        slot_count, int(rescale), C.byref(h)))
+        self.h = h
+        self.level = level
+        self.rescale = rescale
+
+    def apply(self, bs, as_, stream=None):
+        """Apply to a batch of ciphertexts (lists of device tensors), in place."""
+        pb = np.ascontiguousarray([_ptr(t) for t in bs], dtype=np.uint64)
+        pa = np.ascontiguousarray([_ptr(t) for t in as_], dtype=np.uint64)
+        _check(lib().wg_lt_stage_apply(self.ctx.h, self.h, len(pb), pb.ctypes.data, pa.ctypes.data, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wg_lt_stage_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:

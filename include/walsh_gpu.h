@@ -142,6 +142,24 @@ int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_
                                       const uint64_t* const* yb, const uint64_t* const* ya,
                                       const int64_t* rots, void* stream);
 
+/* One CoeffToSlot / SlotToCoeff stage: a baby-step / giant-step linear transform evaluated in
+ * the QP basis (hoisted baby rotations without ModDown, one ModDown per giant step).
+ * `diagonals` (host) holds the stage's nterms plaintexts [term][level+1+K limbs][N] in
+ * Montgomery form, `indices` their diagonal indices, exactly as the reference's plan stores
+ * them (CKKSLinearTransformOwnedStage, src/ckks/operations/bootstrap/
+ * ckks_linear_transform_plan.hpp:29-44).  Rotation keys for the baby steps 1..baby-1 and giant
+ * steps g*baby must be installed.  Apply replaces ckks_apply_linear_transform_owned_stage_qp
+ * (src/ckks/operations/bootstrap/ckks_linear_transform.cpp:1174-1407) on `count` ciphertexts
+ * at the stage's level at once (the diagonals are read once per batch); the result overwrites
+ * (b[i], a[i]), one level lower when the stage rescales. */
+typedef struct wg_lt_stage wg_lt_stage;
+int wg_lt_stage_create(wg_context* ctx, size_t level, size_t nterms, const uint64_t* indices,
+                       const uint64_t* diagonals, size_t baby_step_count, size_t slot_count,
+                       int rescale_after, wg_lt_stage** out);
+void wg_lt_stage_destroy(wg_lt_stage* stage);
+int wg_lt_stage_apply(wg_context* ctx, const wg_lt_stage* stage, size_t count, uint64_t* const* b,
+                      uint64_t* const* a, void* stream);
+
 /* Rotation that allocates no device memory (no counterpart in the reference, whose
  * operations all allocate host vectors).  For callers that cannot call cudaMalloc when they
  * rotate: memory reserved up front by another allocator, work issued while a stream is being

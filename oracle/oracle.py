@@ -380,3 +380,74 @@ class RefCtx:
                                            np.ascontiguousarray(rots, dtype=np.int64), len(rots), out),
                "ref_hoisted_rotations")
         return out.reshape(len(rots), 2, n)
+
+
+class RefPlans:
+    """The reference's walsh15 S2C / C2S plans and rotation keys (ref_walsh15_plans_create)."""
+
+    def __init__(self):
+        R = ref()
+        R.ref_walsh15_plans_create.restype = C.c_void_p
+        R.ref_plan_stage_count.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+        R.ref_plan_stage_info.argtypes = [C.c_void_p, C.c_int, C.c_size_t] + [C.POINTER(C.c_size_t)] * 2 + \
+            [C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]
+        R.ref_plan_stage_data.argtypes = [C.c_void_p, C.c_int, C.c_size_t, u64p, C.c_void_p]
+        R.ref_lt_stage.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, u64p, u64p, u64p, u64p,
+                                   C.POINTER(C.c_size_t)]
+        R.ref_ctx_rotations.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_size_t)]
+        self.h = R.ref_walsh15_plans_create()
+        if not self.h:
+            raise RuntimeError("ref_walsh15_plans_create: " + R.ref_last_error().decode())
+        nq, np_ = C.c_size_t(), C.c_size_t()
+        _check(R.ref_ctx_moduli(self.h, np.zeros(64, np.uint64), C.byref(nq), np.zeros(64, np.uint64), C.byref(np_)),
+               "ref_ctx_moduli")
+        self.q = np.zeros(nq.value, np.uint64)
+        self.p = np.zeros(np_.value, np.uint64)
+        _check(R.ref_ctx_moduli(self.h, self.q, C.byref(nq), self.p, C.byref(np_)), "ref_ctx_moduli")
+        self.N = 1 << 15
+        self.dnum = 3
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().ref_ctx_destroy(self.h)
+            self.h = None
+
+    def stages(self, which):
+        n, qp = C.c_size_t(), C.c_int()
+        _check(ref().ref_plan_stage_count(self.h, which, C.byref(n), C.byref(qp)), "ref_plan_stage_count")
+        return n.value
+
+    def stage(self, which, stage, with_diagonals=True):
+        nt, baby, qpl, slots = C.c_size_t(), C.c_size_t(), C.c_size_t(), C.c_size_t()
+        resc, mont = C.c_int(), C.c_int()
+        _check(ref().ref_plan_stage_info(self.h, which, stage, C.byref(nt), C.byref(baby), C.byref(resc),
+                                         C.byref(qpl), C.byref(mont), C.byref(slots)), "ref_plan_stage_info")
+        idx = np.zeros(nt.value, np.uint64)
+        diags = np.zeros(nt.value * qpl.value * self.N, np.uint64) if with_diagonals else None
+        _check(ref().ref_plan_stage_data(self.h, which, stage, idx, diags.ctypes.data if with_diagonals else None),
+               "ref_plan_stage_data")
+        return dict(nterms=nt.value, baby=baby.value, rescale=bool(resc.value), qp_limbs=qpl.value,
+                    montgomery=bool(mont.value), slot_count=slots.value, indices=idx, diagonals=diags)
+
+    def apply_stage(self, which, stage, level, b, a):
+        n = (level + 1) * self.N
+        ob = np.zeros(n, np.uint64)
+        oa = np.zeros(n, np.uint64)
+        lv = C.c_size_t()
+        _check(ref().ref_lt_stage(self.h, which, stage, level, np.ascontiguousarray(b), np.ascontiguousarray(a),
+                                  ob, oa, C.byref(lv)), "ref_lt_stage")
+        return ob[:(lv.value + 1) * self.N], oa[:(lv.value + 1) * self.N], lv.value
+
+    def rotations(self):
+        n = C.c_size_t()
+        _check(ref().ref_ctx_rotations(self.h, None, C.byref(n)), "ref_ctx_rotations")
+        out = np.zeros(n.value, np.int64)
+        _check(ref().ref_ctx_rotations(self.h, out.ctypes.data, C.byref(n)), "ref_ctx_rotations")
+        return out
+
+    def key(self, rot):
+        parts, kl = C.c_size_t(), C.c_size_t()
+        _check(ref().ref_ctx_key_shape(self.h, 0, rot, C.byref(parts), C.byref(kl)), "ref_ctx_key_shape")
+        out = np.zeros(parts.value * 2 * (kl.value + 1 + len(self.p)) * self.N, np.uint64)
+        _check(ref().ref_ctx_key(self.h, 0, rot, out), "ref_ctx_key")
+        return out, parts.value, kl.value

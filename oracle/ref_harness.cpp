@@ -29,7 +29,9 @@
 
 #include <omp.h>
 
+#include "ckks_aes_params.hpp"
 #include "ckks_ciphertext.hpp"
+#include "ckks_linear_transform.hpp"
 #include "ckks_context.hpp"
 #include "ckks_conjugate.hpp"
 #include "ckks_keyswitch.hpp"
@@ -91,6 +93,15 @@ void keys_to_flat(std::span<const CKKSCiphertext> keys, uint64_t* flat) {
         off += k.getB().size();
     }
 }
+
+}  // namespace
+
+// Defined with external linkage in src/ckks/operations/bootstrap/ckks_linear_transform.cpp:1174
+// but not declared in its header.
+CKKSCiphertext ckks_apply_linear_transform_owned_stage_qp(const CKKSContext& context, const CKKSCiphertext& ct,
+                                                          const CKKSLinearTransformOwnedStage& owned_stage);
+
+namespace {
 
 struct RefCtx {
     CKKSContext ctx;
@@ -377,5 +388,101 @@ int ref_batched_ops(void* h, size_t count, const size_t* levels, uint64_t* x_b, 
 }
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
+
+// The AESWalsh15 modulus chain and bootstrapping DFT parameters with CoeffToSlot / SlotToCoeff
+// plaintext plans but no bootstrapping keys (the EvalMod fit needs MPFR): the context builds
+// the reference's own S2C and C2S plans and the rotation keys they need.  The chain is the
+// preset's (36 | 61 | 42 42 | 38 x7 | 50 50); mult_depth absorbs the EvalMod levels so the
+// depth check holds with the explicit chain.
+void* ref_walsh15_plans_create(void) {
+    RefCtx* out = nullptr;
+    const int rc = guarded([&] {
+        CKKSParamsConfig cfg = ckks_aes_params_detail::AESWalsh15Config();
+        cfg.secure = false;
+        cfg.bts_keys = false;
+        cfg.s2c_ptxt = true;
+        cfg.c2s_ptxt = true;
+        cfg.aes_walsh_params.enabled = false;
+        cfg.q_mult_bits.clear();
+        cfg.q_bits = {36, 61, 42, 42, 38, 38, 38, 38, 38, 38, 38, 50, 50};
+        cfg.mult_depth = 9;
+        out = new RefCtx(CKKSParams(std::move(cfg)));
+    });
+    return rc == 0 ? out : nullptr;
+}
+
+static const CKKSLinearTransformPlan& plan_of(void* h, int which) {
+    const auto& c = static_cast<RefCtx*>(h)->ctx;
+    return which == 0 ? c.getEvalModS2CPlan() : c.getEvalModScaledC2SPlan();
+}
+
+int ref_plan_stage_count(void* h, int which, size_t* stages, int* use_qp) {
+    return guarded([&] {
+        const auto& p = plan_of(h, which);
+        *stages = p.stages.size();
+        *use_qp = p.use_qp_evaluator ? 1 : 0;
+    });
+}
+
+// Stage metadata: number of diagonals, baby-step count, rescale flag, QP limb count of the
+// stored plaintexts, Montgomery flag, logical slot count.
+int ref_plan_stage_info(void* h, int which, size_t stage, size_t* nterms, size_t* baby, int* rescale,
+                        size_t* qp_limbs, int* montgomery, size_t* slot_count) {
+    return guarded([&] {
+        const auto& st = plan_of(h, which).stages.at(stage);
+        *nterms = st.diagonal_qp_plaintexts.size();
+        *baby = st.baby_step_count;
+        *rescale = st.rescale_after ? 1 : 0;
+        *qp_limbs = st.qp_limb_count;
+        *montgomery = st.diagonal_qp_plaintexts_montgomery ? 1 : 0;
+        *slot_count = st.slot_count;
+    });
+}
+
+// Diagonal indices of a stage (one per term) and all QP plaintexts [term][qp_limbs][N].
+int ref_plan_stage_data(void* h, int which, size_t stage, uint64_t* indices, uint64_t* diagonals) {
+    return guarded([&] {
+        const auto& st = plan_of(h, which).stages.at(stage);
+        for (size_t t = 0; t < st.diagonal_qp_plaintexts.size(); ++t) {
+            indices[t] = st.diagonal_indices.empty() ? t : st.diagonal_indices[t];
+            if (diagonals) {
+                const auto& d = st.diagonal_qp_plaintexts[t];
+                std::memcpy(diagonals + t * d.size(), d.data(), d.size() * sizeof(uint64_t));
+            }
+        }
+    });
+}
+
+// One stage of the reference's linear transform on (b, a) at `level`, through its QP
+// evaluator (ckks_apply_linear_transform_owned_stage_qp).  Outputs (out_level+1)*N residues.
+int ref_lt_stage(void* h, int which, size_t stage, size_t level, const uint64_t* b, const uint64_t* a,
+                 uint64_t* out_b, uint64_t* out_a, size_t* out_level) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        CKKSCiphertext ct(N, copy_in(a, n), copy_in(b, n), c.getParams().getScale(), level);
+        const auto& st = plan_of(h, which).stages.at(stage);
+        CKKSCiphertext r = ckks_apply_linear_transform_owned_stage_qp(c, ct, st);
+        copy_out(r.getB(), out_b);
+        copy_out(r.getA(), out_a);
+        *out_level = r.getLevel();
+    });
+}
+
+// Every rotation value with a key in the context.
+int ref_ctx_rotations(void* h, int64_t* out, size_t* n) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t slots = c.getParams().getSlots();
+        size_t k = 0;
+        for (size_t r = 1; r < slots; ++r)
+            if (c.hasRotationKey((int64_t)r)) {
+                if (out) out[k] = (int64_t)r;
+                ++k;
+            }
+        *n = k;
+    });
+}
 
 }  // extern "C"
