@@ -386,7 +386,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
             uint64_t* cf = cfinal + (ci * 2 + poly) * L * N;
             for (size_t pi = 0; pi < K; ++pi) intt_po.push_back({o + (L + pi) * N, o + (L + pi) * N, (int)(nq + pi), 0});
             md_pair.push_back({o + L * N, cf, c.fold_inv[level], c.fold_inv_s[level], (int)L, 0});
-            uint64_t* dst = poly ? a[ci] : b[ci];
+            uint64_t* dst = poly ? b[ci] : a[ci];  // out holds a at offset 0, b at T*N
             for (size_t qi = 0; qi < L; ++qi) {
                 ntt_cf.push_back({cf + qi * N, cf + qi * N, (int)qi, 0});
                 final_sub.push_back({o + qi * N, cf + qi * N, dst + qi * N, (int)qi, 0});

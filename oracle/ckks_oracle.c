@@ -1047,3 +1047,234 @@ int orc_batched_ops(const orc_ctx* c, size_t count, const size_t* levels, uint64
     }
     return err;
 }
+
+/* ------------------------------------------------------------------------------------------
+ * QP-domain baby-step / giant-step linear-transform stage:
+ * ckks_apply_linear_transform_owned_stage_qp
+ * (src/ckks/operations/bootstrap/ckks_linear_transform.cpp:1174-1407).
+ * ---------------------------------------------------------------------------------------- */
+
+/* single-polynomial folded ModDown (ckks_keyswitch.cpp:609-673): alpha as multiply + add */
+static void folded_moddown_single(const orc_ctx* c, size_t level, const uint64_t* src_p, uint64_t* dst_q) {
+    const uint64_t N = c->N;
+    const size_t np = c->np;
+    const uint64_t* invs = c->fold_inv[level];
+    const uint64_t* inv_s = c->fold_inv_s[level];
+    double p_inv[16];
+    for (size_t pi = 0; pi < np; ++pi) p_inv[pi] = 1.0 / (double)c->pm[pi].q;
+    uint64_t* contrib = malloc(N * 8);
+    for (size_t qi = 0; qi <= level; ++qi) {
+        const modulus_t* m = &c->qm[qi];
+        const uint64_t q = m->q;
+        for (uint64_t coeff = 0; coeff < N; ++coeff) {
+            uint64_t acc = 0;
+            double alpha_est = 0.0;
+            for (size_t pi = 0; pi < np; ++pi) {
+                const uint64_t s = red4q(src_p[pi * N + coeff], c->pm[pi].q);
+                alpha_est = alpha_est + (double)s * p_inv[pi];
+                acc = add_mod(acc, mul_shoup(barrett_u64(s, q, m->mu_hi), invs[qi * np + pi], inv_s[qi * np + pi], q), q);
+            }
+            uint64_t hps_alpha = (uint64_t)(alpha_est + 0.5);
+            if (hps_alpha > np) hps_alpha = np;
+            contrib[coeff] = sub_mod(acc, hps_alpha, q);
+        }
+        fwd_limb(m, contrib, N, 0);
+        uint64_t* d = dst_q + qi * N;
+        for (uint64_t coeff = 0; coeff < N; ++coeff) d[coeff] = sub_mod(d[coeff], contrib[coeff], q);
+    }
+    free(contrib);
+}
+
+static const modulus_t* qp_mod(const orc_ctx* c, size_t L, size_t i) { return i < L ? &c->qm[i] : &c->pm[i - L]; }
+
+/* Digits of a QP key switch of `key_term` (Q eval, level): digit[part] holds every QP limb in
+ * evaluation form (source limbs: the key term itself). */
+static uint64_t* qp_digits(const orc_ctx* c, size_t level, const uint64_t* key_term) {
+    const uint64_t N = c->N;
+    const size_t L = level + 1, K = c->np, T = L + K;
+    const size_t parts = c->parts[level];
+    uint64_t* coeff = malloc(L * N * 8);
+    uint64_t* digits = malloc(parts * T * N * 8);
+    memcpy(coeff, key_term, L * N * 8);
+    for (size_t i = 0; i < L; ++i) inv_limb(&c->qm[i], coeff + i * N, N, 1);
+    for (size_t part = 0; part < parts; ++part) {
+        const size_t s0 = part * c->alpha, s1 = s0 + c->alpha < L ? s0 + c->alpha : L;
+        uint64_t* dg = digits + part * T * N;
+        const uint64_t* srcp[64];
+        uint64_t* dstp[128];
+        size_t dc = 0;
+        for (size_t s = s0; s < s1; ++s) srcp[s - s0] = coeff + s * N;
+        for (size_t i = 0; i < s0; ++i) dstp[dc++] = dg + i * N;
+        for (size_t i = s1; i < L; ++i) dstp[dc++] = dg + i * N;
+        for (size_t i = 0; i < K; ++i) dstp[dc++] = dg + (L + i) * N;
+        if (dc) hps_modup(&c->modup[level][part], srcp, dstp, N);
+        for (size_t i = 0; i < T; ++i) {
+            if (i >= s0 && i < s1) {
+                memcpy(dg + i * N, key_term + i * N, N * 8);
+            } else {
+                fwd_limb(qp_mod(c, L, i), dg + i * N, N, 1);
+            }
+        }
+    }
+    free(coeff);
+    return digits;
+}
+
+/* acc_{a,b} (+)= sum_parts REDC(digit * key) over all QP limbs. */
+static void qp_mac(const orc_ctx* c, size_t level, const uint64_t* digits, const uint64_t* key, size_t key_level,
+                   uint64_t* acc_a, uint64_t* acc_b) {
+    const uint64_t N = c->N;
+    const size_t L = level + 1, K = c->np, T = L + K;
+    const size_t key_limbs = key_level + 1 + K;
+    for (size_t part = 0; part < c->parts[level]; ++part) {
+        const uint64_t* ka = key + (part * 2 + 0) * key_limbs * N;
+        const uint64_t* kb = key + (part * 2 + 1) * key_limbs * N;
+        for (size_t i = 0; i < T; ++i) {
+            const modulus_t* m = qp_mod(c, L, i);
+            const size_t kl = i < L ? i : key_level + 1 + (i - L);
+            const uint64_t* d = digits + (part * T + i) * N;
+            for (uint64_t j = 0; j < N; ++j) {
+                acc_a[i * N + j] = add_mod(acc_a[i * N + j], mont_mul(d[j], ka[kl * N + j], m->q, m->qninv), m->q);
+                acc_b[i * N + j] = add_mod(acc_b[i * N + j], mont_mul(d[j], kb[kl * N + j], m->q, m->qninv), m->q);
+            }
+        }
+    }
+}
+
+static void apply_map_qp(uint64_t* poly, uint64_t N, size_t limbs, const uint64_t* map) { apply_map(poly, N, limbs, map); }
+
+int orc_lt_stage(const orc_ctx* c, size_t level, size_t nterms, const uint64_t* indices, const uint64_t* diags,
+                 size_t baby, size_t slots, int rescale, const uint64_t* const* keys, const int64_t* key_rots,
+                 size_t nkeys, size_t key_level, uint64_t* b, uint64_t* a) {
+    const uint64_t N = c->N;
+    const size_t L = level + 1, K = c->np, T = L + K;
+    const size_t full = N / 2;
+    if (!slots) slots = full;
+    const size_t ngiant = (slots + baby - 1) / baby;
+    /* key lookup by normalized rotation */
+#define FIND_KEY(rot, out)                                                   \
+    do {                                                                     \
+        out = NULL;                                                          \
+        for (size_t kk = 0; kk < nkeys; ++kk)                                \
+            if ((uint64_t)(((key_rots[kk] % (int64_t)full) + full) % full) == (uint64_t)((rot) % full)) out = keys[kk]; \
+    } while (0)
+    /* babies */
+    char* need = calloc(baby, 1);
+    for (size_t t = 0; t < nterms; ++t) need[indices[t] % baby] = 1;
+    uint64_t** ba = calloc(baby, sizeof(uint64_t*));
+    uint64_t** bb = calloc(baby, sizeof(uint64_t*));
+    uint64_t* digits = NULL;
+    uint64_t* map = malloc(N * 8);
+    for (size_t r = 0; r < baby; ++r) {
+        if (!need[r]) continue;
+        ba[r] = calloc(T * N, 8);
+        bb[r] = calloc(T * N, 8);
+        if (r == 0) {
+            memcpy(ba[r], a, L * N * 8);
+            memcpy(bb[r], b, L * N * 8);
+            continue;
+        }
+        if (!digits) digits = qp_digits(c, level, a);
+        const uint64_t* key;
+        FIND_KEY(r, key);
+        if (!key) return -3;
+        memcpy(bb[r], b, L * N * 8);
+        qp_mac(c, level, digits, key, key_level, ba[r], bb[r]);
+        orc_automorphism_map(N, orc_rotation_galois(N, (int64_t)r), map);
+        apply_map_qp(ba[r], N, T, map);
+        apply_map_qp(bb[r], N, T, map);
+    }
+    uint64_t* out_a = calloc(T * N, 8);
+    uint64_t* out_b = calloc(T * N, 8);
+    uint64_t* in_a = malloc(T * N * 8);
+    uint64_t* in_b = malloc(T * N * 8);
+    uint64_t* sw_a = malloc(T * N * 8);
+    uint64_t* sw_b = malloc(T * N * 8);
+    for (size_t g = 0; g < ngiant; ++g) {
+        int have = 0;
+        memset(in_a, 0, T * N * 8);
+        memset(in_b, 0, T * N * 8);
+        for (size_t t = 0; t < nterms; ++t) {
+            if (indices[t] / baby != g) continue;
+            have = 1;
+            const size_t r = indices[t] % baby;
+            const uint64_t* d = diags + t * T * N;
+            for (size_t i = 0; i < T; ++i) {
+                const modulus_t* m = qp_mod(c, L, i);
+                for (uint64_t j = 0; j < N; ++j) {
+                    const size_t k = i * N + j;
+                    in_a[k] = add_mod(in_a[k], mont_mul(ba[r][k], d[k], m->q, m->qninv), m->q);
+                    in_b[k] = add_mod(in_b[k], mont_mul(bb[r][k], d[k], m->q, m->qninv), m->q);
+                }
+            }
+        }
+        if (!have) continue;
+        if (g == 0) {
+            for (size_t i = 0; i < T; ++i) {
+                const modulus_t* m = qp_mod(c, L, i);
+                for (uint64_t j = 0; j < N; ++j) {
+                    const size_t k = i * N + j;
+                    out_a[k] = add_mod(out_a[k], in_a[k], m->q);
+                    out_b[k] = add_mod(out_b[k], in_b[k], m->q);
+                }
+            }
+            continue;
+        }
+        /* single ModDown of the inner a, then a QP key switch of that key term */
+        for (size_t pi = 0; pi < K; ++pi) inv_limb(&c->pm[pi], in_a + (L + pi) * N, N, 1);
+        folded_moddown_single(c, level, in_a + L * N, in_a);
+        uint64_t* dg = qp_digits(c, level, in_a);
+        const uint64_t* key;
+        FIND_KEY(g * baby, key);
+        if (!key) return -3;
+        memset(sw_a, 0, T * N * 8);
+        memset(sw_b, 0, T * N * 8);
+        qp_mac(c, level, dg, key, key_level, sw_a, sw_b);
+        free(dg);
+        orc_automorphism_map(N, orc_rotation_galois(N, (int64_t)(g * baby)), map);
+        for (size_t i = 0; i < T; ++i) {
+            const modulus_t* m = qp_mod(c, L, i);
+            for (uint64_t j = 0; j < N; ++j) {
+                const size_t k = i * N + j, s = i * N + map[j];
+                out_a[k] = add_mod(out_a[k], sw_a[s], m->q);
+                out_b[k] = add_mod(out_b[k], add_mod(sw_b[s], in_b[s], m->q), m->q);
+            }
+        }
+    }
+#undef FIND_KEY
+    /* pair ModDown */
+    for (size_t pi = 0; pi < K; ++pi) {
+        inv_limb(&c->pm[pi], out_a + (L + pi) * N, N, 1);
+        inv_limb(&c->pm[pi], out_b + (L + pi) * N, N, 1);
+    }
+    folded_moddown(c, level, out_a + L * N, out_a);
+    folded_moddown(c, level, out_b + L * N, out_b);
+    memcpy(b, out_b, L * N * 8);
+    memcpy(a, out_a, L * N * 8);
+    int rc = 0;
+    if (rescale) {
+        uint64_t* buf = malloc(2 * L * N * 8);
+        memcpy(buf, b, L * N * 8);
+        memcpy(buf + L * N, a, L * N * 8);
+        rc = orc_rescale(c, level, 2, buf);
+        memcpy(b, buf, level * N * 8);
+        memcpy(a, buf + L * N, level * N * 8);
+        free(buf);
+    }
+    for (size_t r = 0; r < baby; ++r) {
+        free(ba[r]);
+        free(bb[r]);
+    }
+    free(ba);
+    free(bb);
+    free(need);
+    free(digits);
+    free(map);
+    free(out_a);
+    free(out_b);
+    free(in_a);
+    free(in_b);
+    free(sw_a);
+    free(sw_b);
+    return rc;
+}

@@ -69,6 +69,13 @@ int orc_hoisted_rotations(const orc_ctx* c, size_t level, const uint64_t* b, con
                           const uint64_t* const* keys, size_t key_level, const int64_t* rots,
                           size_t nrot, uint64_t* out);
 
+/* One QP baby-step / giant-step linear-transform stage (reference
+ * ckks_apply_linear_transform_owned_stage_qp); diags [term][level+1+K][N] Montgomery; keys:
+ * nkeys rotation keys with their rotations.  (b, a) updated in place (level-1 when rescale). */
+int orc_lt_stage(const orc_ctx* c, size_t level, size_t nterms, const uint64_t* indices, const uint64_t* diags,
+                 size_t baby, size_t slots, int rescale, const uint64_t* const* keys, const int64_t* key_rots,
+                 size_t nkeys, size_t key_level, uint64_t* b, uint64_t* a);
+
 /* --- seeded key material and encryption (test data generation) --- */
 void orc_sample_ternary(uint64_t N, size_t hamming_weight, uint64_t seed, int8_t* out);
 /* Switch key from secret `src` (squared when src_square, for relinearization) to secret

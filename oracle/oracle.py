@@ -71,6 +71,8 @@ def lib() -> C.CDLL:
         L.orc_decrypt_coeffs.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, i8p, f64p]
         L.orc_barrett_mul.restype = C.c_uint64
         L.orc_barrett_mul.argtypes = [C.c_uint64] * 5
+        L.orc_lt_stage.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, u64p, u64p, C.c_size_t, C.c_size_t, C.c_int,
+                                   C.c_void_p, i64p, C.c_size_t, C.c_size_t, u64p, u64p]
         L.orc_batched_ops.argtypes = [C.c_void_p, C.c_size_t, szp, u64p, u64p, u64p, u64p, u64p,
                                       C.c_void_p, i64p, C.c_size_t, C.c_size_t, C.c_int]
         _lib = L
@@ -279,6 +281,20 @@ class OracleCtx:
         _check(lib().orc_decrypt_coeffs(self.h, level, np.ascontiguousarray(b), np.ascontiguousarray(a), s, out),
                "orc_decrypt")
         return out
+
+    def lt_stage(self, level, indices, diags, baby, slots, rescale, keys, b, a, key_level=None):
+        """keys: dict rotation -> flat key array."""
+        kl = self.nq - 1 if key_level is None else key_level
+        rots = np.ascontiguousarray(list(keys.keys()), dtype=np.int64)
+        arrs = [np.ascontiguousarray(keys[int(r)], dtype=np.uint64) for r in rots]
+        ptrs = (C.c_void_p * len(arrs))(*[x.ctypes.data for x in arrs])
+        b = np.ascontiguousarray(b, dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        _check(lib().orc_lt_stage(self.h, level, len(indices), np.ascontiguousarray(indices, dtype=np.uint64),
+                                  np.ascontiguousarray(diags, dtype=np.uint64), baby, slots, int(rescale),
+                                  C.cast(ptrs, C.c_void_p), rots, len(rots), kl, b, a), "orc_lt_stage")
+        n = (level if rescale else level + 1) * self.N
+        return b[:n], a[:n]
 
     def batched_ops(self, levels, x_b, x_a, y_b, y_a, relin_key, rot_keys, rots, stride, threads):
         """CPU timing baseline: x_* updated in place.  rot_keys: list of key arrays."""

@@ -59,3 +59,44 @@ def test_bsgs_stage_matches_reference(wg, plans, gpu_ctx, which, stage, level):
         assert (gb == rb).all(), (which, stage, k, int((gb != rb).sum()))
         assert (ga == ra).all(), (which, stage, k, int((ga != ra).sum()))
     st.close()
+
+
+# Synthetic stage shapes at N = 2^12 against the oracle's restatement of the same evaluator:
+# each shape isolates one part (baby 0 only, one baby rotation, one giant rotation, a mix).
+SYN = [([0], 4, False), ([1], 4, False), ([4], 4, False), ([0, 1, 2, 5, 9, 12], 4, False),
+       ([0, 1, 2, 5, 9, 12], 4, True), ([3, 2047, 2040], 8, False)]
+
+
+@pytest.mark.parametrize("indices,baby,rescale", SYN)
+def test_bsgs_synthetic_shapes_match_oracle(wg, oracle_mod, indices, baby, rescale):
+    import torch
+
+    O = oracle_mod
+    N = 1 << 12
+    p, q = O.find_primes([50, 50], [40, 45, 45, 45], N)
+    o = O.OracleCtx(N, q, p, 2)
+    ctx = wg.Context(N, q, p, 2)
+    s = o.ternary(64, 9)
+    slots = N // 2
+    rots = sorted({i % baby for i in indices if i % baby} | {(i // baby) * baby for i in indices if i // baby})
+    keys = {}
+    for r in rots:
+        keys[r] = o.rotation_key(s, r, 500 + r)
+        ctx.set_key(wg.WG_KEY_ROTATION, keys[r], rotation=r)
+    level = 3
+    T = level + 1 + 2
+    rng = np.random.default_rng(len(indices) + baby)
+    mods = np.concatenate([q[: level + 1], p])
+    diags = np.concatenate([(rng.integers(0, 1 << 62, T * N, dtype=np.uint64) % np.repeat(mods, N)).astype(np.uint64)
+                            for _ in indices])
+    st = wg.LtStage(ctx, level, indices, diags, baby, slots, rescale)
+    ins = [(o.uniform(level + 1, 10 + k), o.uniform(level + 1, 20 + k)) for k in range(2)]
+    db = [wg.to_device(b) for b, _ in ins]
+    da = [wg.to_device(a) for _, a in ins]
+    st.apply(db, da)
+    torch.cuda.synchronize()
+    for k, (b, a) in enumerate(ins):
+        ob, oa = o.lt_stage(level, indices, diags, baby, slots, rescale, keys, b, a)
+        n = ob.size
+        gb, ga = wg.to_host(db[k])[:n], wg.to_host(da[k])[:n]
+        assert (gb == ob).all() and (ga == oa).all(), (indices, baby, k, int((gb != ob).sum()), int((ga != oa).sum()))

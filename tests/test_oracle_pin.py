@@ -134,3 +134,18 @@ def test_walsh15_chain_ops(ref_mod):
         rb, ra = R.rotate(level - 1, rs[0], rs[1], r)
         ob, oa = o.rotate(level - 1, os_[0], os_[1], rk[r], r, key_level=kl)
         assert (rb == ob).all() and (ra == oa).all()
+
+
+def test_bsgs_stages_match_reference(ref_mod):
+    """The oracle's QP BSGS stage against the reference's own walsh15 S2C / C2S plans."""
+    P = ref_mod.RefPlans()
+    o = ref_mod.OracleCtx(P.N, P.q, P.p, P.dnum)
+    keys = {int(r): P.key(int(r))[0] for r in P.rotations()}
+    rng = np.random.default_rng(3)
+    for which, stage, level in ((0, 0, 1), (0, 2, 1), (1, 1, 12), (1, 3, 11)):
+        info = P.stage(which, stage)
+        b, a = _uniform(rng, P.q, P.N, level + 1), _uniform(rng, P.q, P.N, level + 1)
+        rb, ra, _ = P.apply_stage(which, stage, level, b, a)
+        ob, oa = o.lt_stage(level, info["indices"], info["diagonals"], info["baby"], info["slot_count"],
+                            info["rescale"], keys, b, a)
+        assert (rb == ob).all() and (ra == oa).all(), (which, stage)
