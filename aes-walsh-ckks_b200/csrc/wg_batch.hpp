@@ -60,4 +60,8 @@ void lt_stage_destroy(LtStage* st);
 void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const* b, uint64_t* const* a,
                     cudaStream_t s);
 
+// Hoisted rotations of one ciphertext; out [rotation][b, a][level+1][N] (wg_bsgs.cu).
+void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rots, size_t nrot,
+                 uint64_t* out, cudaStream_t s);
+
 }  // namespace wg

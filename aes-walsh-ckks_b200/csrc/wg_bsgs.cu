@@ -493,4 +493,111 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     check_cuda(cudaGetLastError(), "linear transform launch");
 }
 
+// Hoisted rotations of one ciphertext (ckks_hoist_ciphertext_a_qp_eval + per rotation
+// ckks_hybrid_key_switch_hoisted_inplace, ckks_keyswitch.cpp:344-373 and 1072-1328): the
+// iNTT / ModUp / NTT of `a` is done once; each rotation then costs a key inner product, a
+// pair ModDown, the combine and the automorphism, all rotations batched per step.
+// out: [rotation][b, a][level+1][N].
+void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rots, size_t nrot,
+                 uint64_t* out, cudaStream_t s) {
+    if (nrot == 0) return;
+    const size_t N = c.N, L = level + 1, K = c.np, T = L + K, nq = c.nq;
+    const size_t B = c.parts_at(level);
+    const size_t slots = N / 2;
+    std::vector<const KeyEntry*> keys(nrot, nullptr);
+    std::vector<uint64_t> gal(nrot, 0);
+    for (size_t r = 0; r < nrot; ++r) {
+        int64_t rr = rots[r] % (int64_t)slots;
+        if (rr < 0) rr += (int64_t)slots;
+        if (rr == 0) continue;
+        const KeyEntry& k = c.key(WG_KEY_ROTATION, rr);
+        if (k.key_level < level) fail(kRuntime, "keyswitch: switch key level is below ciphertext level");
+        if (k.parts < B) fail(kRuntime, "keyswitch: insufficient key partitions");
+        keys[r] = &k;
+        gal[r] = host::powmod(5, (uint64_t)rr, 2 * N);
+    }
+    const size_t w_coeff = L * N, w_digits = B * T * N, w_acc = nrot * 2 * T * N, w_contrib = nrot * 2 * L * N;
+    uint64_t* coeff = c.batch_buffers(s).arena(c, w_coeff + w_digits + w_acc + w_contrib, s);
+    uint64_t* digits = coeff + w_coeff;
+    uint64_t* accb = digits + w_digits;
+    uint64_t* contrib = accb + w_acc;
+    auto modq = [&](size_t limb) { return (int)(limb < L ? limb : nq + (limb - L)); };
+
+    std::vector<NttJob> intt_a, ntt_dig, intt_p, ntt_c;
+    std::vector<ModUpJob> modup;
+    std::vector<MacJob> mac;
+    std::vector<ModDownJob> md;
+    std::vector<CombineJob> comb;
+    std::vector<GatherJob> gath;
+    for (size_t l = 0; l < L; ++l) intt_a.push_back({a + l * N, coeff + l * N, (int)l, 0});
+    for (size_t j = 0; j < B; ++j) {
+        modup.push_back({c.d_modup + level * c.dnum + j, coeff, digits + j * T * N});
+        const size_t s0 = j * c.alpha, s1 = std::min(s0 + c.alpha, L);
+        for (size_t l = 0; l < T; ++l)
+            if (l < s0 || l >= s1) ntt_dig.push_back({digits + j * T * N + l * N, digits + j * T * N + l * N, modq(l), 0});
+    }
+    for (size_t r = 0; r < nrot; ++r) {
+        uint64_t* ob = out + (2 * r) * L * N;
+        uint64_t* oa = ob + L * N;
+        if (!keys[r]) {  // rotation by a multiple of the slot count: the ciphertext itself
+            check_cuda(cudaMemcpyAsync(ob, b, L * N * 8, cudaMemcpyDeviceToDevice, s), "rotate_many copy");
+            check_cuda(cudaMemcpyAsync(oa, a, L * N * 8, cudaMemcpyDeviceToDevice, s), "rotate_many copy");
+            continue;
+        }
+        uint64_t* acc = accb + r * 2 * T * N;
+        uint64_t* cr = contrib + r * 2 * L * N;
+        for (size_t i = 0; i < T; ++i)
+            mac.push_back({keys[r]->d_data, a, digits, acc, T * N, (int)L, (int)K, (int)B, (int)c.alpha,
+                           (int)keys[r]->key_level, (int)i});
+        for (int poly = 0; poly < 2; ++poly) {
+            for (size_t pi = 0; pi < K; ++pi) {
+                uint64_t* p = acc + (poly * T + L + pi) * N;
+                intt_p.push_back({p, p, (int)(nq + pi), 0});
+            }
+            md.push_back({acc + (poly * T + L) * N, cr + poly * L * N, c.fold_inv[level], c.fold_inv_s[level], (int)L, 0});
+            for (size_t qi = 0; qi < L; ++qi) ntt_c.push_back({cr + (poly * L + qi) * N, cr + (poly * L + qi) * N, (int)qi, 0});
+        }
+        for (size_t qi = 0; qi < L; ++qi) {
+            // combine in place of the accumulators, then gather into the output slot
+            comb.push_back({acc, cr, b, a, acc + T * N, acc, (int)L, (int)K, (int)qi, 1, 0, 0});
+            gath.push_back({acc + T * N + qi * N, acc + qi * N, ob + qi * N, oa + qi * N, gal[r]});
+        }
+    }
+    JobTable t;
+    const NttJob* j1 = t.add(intt_a);
+    const ModUpJob* j2 = t.add(modup);
+    const NttJob* j3 = t.add(ntt_dig);
+    const MacJob* j4 = t.add(mac);
+    const NttJob* j5 = t.add(intt_p);
+    const ModDownJob* j6 = t.add(md);
+    const NttJob* j7 = t.add(ntt_c);
+    const CombineJob* j8 = t.add(comb);
+    const GatherJob* j9 = t.add(gath);
+    t.upload(c, s);
+    ntt_jobs(c, t.at(j1), (int)intt_a.size(), false, s);
+    {
+        double bytes = 0;
+        for (size_t j = 0; j < B; ++j) bytes += 8.0 * N * (c.modup[level][j].src_count + c.modup[level][j].dst_count);
+        Probe probe(kClsModUp, bytes, s);
+        kb_modup<<<grid_for(c, modup.size()), kT, 0, s>>>(t.at(j2), (int)modup.size(), c.d_mod, N);
+    }
+    ntt_jobs(c, t.at(j3), (int)ntt_dig.size(), true, s);
+    if (!mac.empty()) {
+        {
+            Probe probe(kClsKeyMac, 8.0 * N * mac.size() * (3.0 * B + 2.0), s);
+            kb_mac<<<grid_for(c, mac.size()), kT, 0, s>>>(t.at(j4), (int)mac.size(), c.d_mod, (int)nq, N);
+        }
+        ntt_jobs(c, t.at(j5), (int)intt_p.size(), false, s);
+        {
+            Probe probe(kClsModDown, 8.0 * N * (K + L) * md.size(), s);
+            kb_moddown<<<grid_for(c, md.size()), kT, 0, s>>>(t.at(j6), (int)md.size(), c.d_mod, (int)nq, (int)K, N);
+        }
+        ntt_jobs(c, t.at(j7), (int)ntt_c.size(), true, s);
+        Probe probe(kClsCombine, 8.0 * N * L * 12.0 * (mac.size() / T), s);
+        kb_combine<<<grid_for(c, comb.size()), kT, 0, s>>>(t.at(j8), (int)comb.size(), c.d_mod, N);
+        kb_gather<<<grid_for(c, gath.size()), kT, 0, s>>>(t.at(j9), (int)gath.size(), c.logN);
+    }
+    check_cuda(cudaGetLastError(), "rotate_many launch");
+}
+
 }  // namespace wg

@@ -249,15 +249,8 @@ int wg_rotate_many(wg_context* ctx, size_t level, const uint64_t* b, const uint6
         check_ptr(b, "ckks_rotate");
         check_ptr(a, "ckks_rotate");
         check_ptr(out, "ckks_rotate");
-        const size_t n = (level + 1) * c.N;
-        for (size_t r = 0; r < nrot; ++r) c.key(WG_KEY_ROTATION, normalize_rotation(c, rotations[r]));
-        for (size_t r = 0; r < nrot; ++r) {
-            uint64_t* ob = out + (2 * r) * n;
-            uint64_t* oa = ob + n;
-            wg::check_cuda(cudaMemcpyAsync(ob, b, n * 8, cudaMemcpyDeviceToDevice, S(stream)), "copy");
-            wg::check_cuda(cudaMemcpyAsync(oa, a, n * 8, cudaMemcpyDeviceToDevice, S(stream)), "copy");
-            do_rotate(c, level, ob, oa, rotations[r], S(stream));
-        }
+        if (nrot && !rotations) wg::fail(wg::kInvalid, "ckks_rotate: null rotation list");
+        wg::rotate_many(c, level, b, a, rotations, nrot, out, S(stream));
     });
 }
 
