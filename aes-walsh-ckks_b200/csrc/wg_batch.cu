@@ -8,6 +8,7 @@
 // single-ciphertext path (wg_keyswitch.cuh, wg_arith.cuh), so results are identical.
 #include <algorithm>
 #include <cstring>
+#include <memory>
 
 #include "wg_batch.hpp"
 #include "wg_batch_kernels.cuh"
@@ -180,46 +181,66 @@ void batch_keyswitch(Context& c, const KsItem* items, size_t n, cudaStream_t s) 
 // ------------------------------------------------------------------------------------------
 // Batched mul + relin + rescale + rotate
 // ------------------------------------------------------------------------------------------
-void batch_mul_relin_rescale_rotate(Context& c, size_t count, const size_t* levels, uint64_t* const* xb,
-                                    uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
-                                    const int64_t* rots, const uint64_t* galois, const KeyEntry* relin,
-                                    const KeyEntry* const* rot_keys, cudaStream_t s) {
-    if (count == 0) return;
+// A planned pipeline: the job-table image and the launch sequence that reads it.
+struct PipelinePlan {
+    JobTable t;
+    const TensorJob* jt = nullptr;
+    const NttJob* jd = nullptr;
+    const RescalePrepJob* jp = nullptr;
+    const NttJob* jr = nullptr;
+    const RescaleFinishJob* jf = nullptr;
+    int nt = 0, nd = 0, np = 0, nr = 0, nf = 0;
+    KsPlan p1{}, p2{};
+    bool rotate = false;
+    double tb = 0, pb = 0, fb = 0;
+};
+
+// Arena: c2 per ciphertext, rescale remainders, then the larger of the two key-switch batches.
+static size_t pipeline_words(const Context& c, size_t count, const size_t* levels, const uint64_t* galois,
+                             size_t* c2_out, size_t* rem_out) {
     const size_t N = c.N;
-    // Arena: c2 per ciphertext, the relin key switches, rescale remainders, rotate switches.
     std::vector<KsItem> relin_items(count), rot_items;
     size_t c2_words = 0, rem_words = 0;
     for (size_t i = 0; i < count; ++i) {
         c2_words += (levels[i] + 1) * N;
         rem_words += 2 * levels[i] * N;
-    }
-    for (size_t i = 0; i < count; ++i) relin_items[i].level = levels[i];
-    for (size_t i = 0; i < count; ++i)
+        relin_items[i].level = levels[i];
         if (galois[i]) {
             KsItem it;
             it.level = levels[i] - 1;
             rot_items.push_back(it);
         }
+    }
     const size_t ks1 = batch_keyswitch_words(c, relin_items.data(), count);
     const size_t ks2 = batch_keyswitch_words(c, rot_items.data(), rot_items.size());
-    uint64_t* arena = c.batch_buffers(s).arena(c, c2_words + rem_words + std::max(ks1, ks2), s);
+    if (c2_out) *c2_out = c2_words;
+    if (rem_out) *rem_out = rem_words;
+    return c2_words + rem_words + std::max(ks1, ks2);
+}
+
+static void plan_pipeline(const Context& c, PipelinePlan& P, size_t count, const size_t* levels,
+                          uint64_t* const* xb, uint64_t* const* xa, const uint64_t* const* yb,
+                          const uint64_t* const* ya, const uint64_t* galois, const KeyEntry* relin,
+                          const KeyEntry* const* rot_keys, uint64_t* arena) {
+    const size_t N = c.N;
+    size_t c2_words = 0, rem_words = 0;
+    pipeline_words(c, count, levels, galois, &c2_words, &rem_words);
     uint64_t* c2base = arena;
     uint64_t* rembase = c2base + c2_words;
     uint64_t* ksbase = rembase + rem_words;
-
-    JobTable t;
+    std::vector<KsItem> relin_items(count), rot_items;
     std::vector<TensorJob> tensor;
     std::vector<NttJob> drop_intt, rem_ntt;
     std::vector<RescalePrepJob> prep;
     std::vector<RescaleFinishJob> fin;
     uint64_t* c2p = c2base;
     uint64_t* remp = rembase;
-    size_t r = 0;
     for (size_t i = 0; i < count; ++i) {
         const size_t lv = levels[i], L = lv + 1;
         for (size_t l = 0; l < L; ++l)
             tensor.push_back({xb[i] + l * N, xa[i] + l * N, yb[i] + l * N, ya[i] + l * N, c2p + l * N, (int)l, 0});
         KsItem& ri = relin_items[i];
+        ri.level = lv;
         ri.key_term = c2p;
         ri.key = relin;
         ri.b_in = xb[i];
@@ -243,7 +264,8 @@ void batch_mul_relin_rescale_rotate(Context& c, size_t count, const size_t* leve
             remp += lv * N;
         }
         if (galois[i]) {
-            KsItem& it = rot_items[r++];
+            KsItem it;
+            it.level = lv - 1;
             it.key_term = xa[i];
             it.key = rot_keys[i];
             it.b_in = xb[i];
@@ -253,40 +275,117 @@ void batch_mul_relin_rescale_rotate(Context& c, size_t count, const size_t* leve
             it.b_add = 1;
             it.a_add = 0;
             it.galois = galois[i];
+            rot_items.push_back(it);
         }
+        P.tb += 8.0 * N * (lv + 1) * 7.0;
+        P.pb += 8.0 * N * 2.0 * (1.0 + lv);
+        P.fb += 8.0 * N * 2.0 * 3.0 * lv;
     }
-    const TensorJob* jt = t.add(tensor);
-    const NttJob* jd = t.add(drop_intt);
-    const RescalePrepJob* jp = t.add(prep);
-    const NttJob* jr = t.add(rem_ntt);
-    const RescaleFinishJob* jf = t.add(fin);
-    KsPlan p1 = plan_keyswitch(c, relin_items.data(), count, ksbase, t);
-    KsPlan p2 = plan_keyswitch(c, rot_items.data(), rot_items.size(), ksbase, t);
-    t.upload(c, s);
+    P.jt = P.t.add(tensor);
+    P.nt = (int)tensor.size();
+    P.jd = P.t.add(drop_intt);
+    P.nd = (int)drop_intt.size();
+    P.jp = P.t.add(prep);
+    P.np = (int)prep.size();
+    P.jr = P.t.add(rem_ntt);
+    P.nr = (int)rem_ntt.size();
+    P.jf = P.t.add(fin);
+    P.nf = (int)fin.size();
+    P.p1 = plan_keyswitch(c, relin_items.data(), count, ksbase, P.t);
+    P.p2 = plan_keyswitch(c, rot_items.data(), rot_items.size(), ksbase, P.t);
+    P.rotate = !rot_items.empty();
+}
 
-    double tb = 0, pb = 0, fb = 0;
-    for (size_t i = 0; i < count; ++i) {
-        tb += 8.0 * N * (levels[i] + 1) * 7.0;
-        pb += 8.0 * N * 2.0 * (1.0 + levels[i]);
-        fb += 8.0 * N * 2.0 * 3.0 * levels[i];
-    }
+static void launch_pipeline(const Context& c, const PipelinePlan& P, cudaStream_t s) {
+    const JobTable& t = P.t;
     {
-        Probe probe(kClsElementwise, tb, s);
-        kb_tensor<<<grid_for(c, tensor.size()), kT, 0, s>>>(t.at(jt), (int)tensor.size(), c.d_mod);
+        Probe probe(kClsElementwise, P.tb, s);
+        kb_tensor<<<grid_for(c, P.nt), kT, 0, s>>>(t.at(P.jt), P.nt, c.d_mod);
     }
-    run_keyswitch(c, p1, t, s);
-    ntt_jobs(c, t.at(jd), (int)drop_intt.size(), false, s);
+    run_keyswitch(c, P.p1, t, s);
+    ntt_jobs(c, t.at(P.jd), P.nd, false, s);
     {
-        Probe probe(kClsElementwise, pb, s);
-        kb_rescale_prep<<<grid_for(c, prep.size()), kT, 0, s>>>(t.at(jp), (int)prep.size(), c.d_mod);
+        Probe probe(kClsElementwise, P.pb, s);
+        kb_rescale_prep<<<grid_for(c, P.np), kT, 0, s>>>(t.at(P.jp), P.np, c.d_mod);
     }
-    ntt_jobs(c, t.at(jr), (int)rem_ntt.size(), true, s);
+    ntt_jobs(c, t.at(P.jr), P.nr, true, s);
     {
-        Probe probe(kClsElementwise, fb, s);
-        kb_rescale_finish<<<grid_for(c, fin.size()), kT, 0, s>>>(t.at(jf), (int)fin.size(), c.d_mod);
+        Probe probe(kClsElementwise, P.fb, s);
+        kb_rescale_finish<<<grid_for(c, P.nf), kT, 0, s>>>(t.at(P.jf), P.nf, c.d_mod);
     }
-    if (!rot_items.empty()) run_keyswitch(c, p2, t, s);
+    if (P.rotate) run_keyswitch(c, P.p2, t, s);
     check_cuda(cudaGetLastError(), "batched pipeline launch");
+}
+
+void batch_mul_relin_rescale_rotate(Context& c, size_t count, const size_t* levels, uint64_t* const* xb,
+                                    uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                                    const int64_t* rots, const uint64_t* galois, const KeyEntry* relin,
+                                    const KeyEntry* const* rot_keys, cudaStream_t s) {
+    (void)rots;
+    if (count == 0) return;
+    uint64_t* arena = c.batch_buffers(s).arena(c, pipeline_words(c, count, levels, galois, nullptr, nullptr), s);
+    PipelinePlan P;
+    plan_pipeline(c, P, count, levels, xb, xa, yb, ya, galois, relin, rot_keys, arena);
+    P.t.upload(c, s);
+    launch_pipeline(c, P, s);
+}
+
+// ------------------------------------------------------------------------------------------
+// Graph-captured batch plan
+// ------------------------------------------------------------------------------------------
+BatchGraph::~BatchGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaFree(d_jobs);
+    cudaFree(d_arena);
+}
+
+BatchGraph* batch_graph_create(Context& c, size_t count, const size_t* levels, uint64_t* const* xb,
+                               uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                               const uint64_t* galois, const KeyEntry* relin, const KeyEntry* const* rot_keys) {
+    if (count == 0) fail(kInvalid, "batch plan: empty batch");
+    check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+    std::unique_ptr<BatchGraph> g(new BatchGraph);
+    const size_t words = pipeline_words(c, count, levels, galois, nullptr, nullptr);
+    if (cudaMalloc(&g->d_arena, words * 8) != cudaSuccess) {
+        cudaGetLastError();
+        fail(kNoMemory, "batch plan: scratch allocation failed");
+    }
+    PipelinePlan P;
+    plan_pipeline(c, P, count, levels, xb, xa, yb, ya, galois, relin, rot_keys, g->d_arena);
+    if (cudaMalloc(&g->d_jobs, std::max<size_t>(P.t.bytes.size(), 16)) != cudaSuccess) {
+        cudaGetLastError();
+        fail(kNoMemory, "batch plan: job-table allocation failed");
+    }
+    check_cuda(cudaMemcpy(g->d_jobs, P.t.bytes.data(), P.t.bytes.size(), cudaMemcpyHostToDevice), "job upload");
+    P.t.base = g->d_jobs;
+    cudaStream_t ps = nullptr;
+    check_cuda(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking), "stream");
+    uint64_t before[kClsCount], after[kClsCount];
+    probe_counts(before);
+    check_cuda(cudaStreamBeginCapture(ps, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        launch_pipeline(c, P, ps);
+    } catch (...) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(ps, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        cudaStreamDestroy(ps);
+        cudaGetLastError();
+        throw;
+    }
+    const cudaError_t ec = cudaStreamEndCapture(ps, &g->graph);
+    probe_counts(after);
+    cudaStreamDestroy(ps);
+    check_cuda(ec, "end capture");
+    check_cuda(cudaGraphInstantiate(&g->exec, g->graph, 0), "graph instantiate");
+    for (int k = 0; k < kClsCount; ++k) g->launches[k] = after[k] - before[k];
+    return g.release();
+}
+
+void batch_graph_launch(BatchGraph& g, cudaStream_t s) {
+    check_cuda(cudaGraphLaunch(g.exec, s), "graph launch");
+    probe_add(g.launches);
 }
 
 }  // namespace wg

@@ -52,6 +52,22 @@ void batch_mul_relin_rescale_rotate(Context& c, size_t count, const size_t* leve
                                     const int64_t* rots, const uint64_t* galois, const KeyEntry* relin,
                                     const KeyEntry* const* rot_keys, cudaStream_t s);
 
+// A batched mul + relin + rescale + rotate pipeline planned once for fixed buffers and captured
+// as a CUDA graph: launching it replays every stage with no host-side planning or upload.  It
+// owns its job table and scratch; the ciphertext buffers stay the caller's.
+struct BatchGraph {
+    uint64_t* d_jobs = nullptr;
+    uint64_t* d_arena = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches[kClsCount] = {};
+    ~BatchGraph();
+};
+BatchGraph* batch_graph_create(Context& c, size_t count, const size_t* levels, uint64_t* const* xb,
+                               uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                               const uint64_t* galois, const KeyEntry* relin, const KeyEntry* const* rot_keys);
+void batch_graph_launch(BatchGraph& g, cudaStream_t s);
+
 // One baby-step / giant-step linear-transform stage (wg_bsgs.cu).
 struct LtStage;
 LtStage* lt_stage_create(Context& c, size_t level, size_t nterms, const uint64_t* indices, const uint64_t* diags,

@@ -449,7 +449,10 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     t.upload(c, s);
     // 1.
     ntt_jobs(c, t.at(j_intt_a), (int)intt_a.size(), false, s);
-    kb_modup<<<grid_for(c, modup.size()), kT, 0, s>>>(t.at(j_modup), (int)modup.size(), c.d_mod, N);
+    {
+        Probe probe(kClsModUp, 8.0 * N * (double)(count * B * T), s);
+        kb_modup<<<grid_for(c, modup.size()), kT, 0, s>>>(t.at(j_modup), (int)modup.size(), c.d_mod, N);
+    }
     ntt_jobs(c, t.at(j_ntt_dig), (int)ntt_dig.size(), true, s);
     // 2.
     if (!baby_jobs.empty()) {
@@ -466,28 +469,51 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     // 4.
     if (!md_single.empty()) {
         ntt_jobs(c, t.at(j_intt_pg), (int)intt_pg.size(), false, s);
-        kb_moddown_single<<<grid_for(c, md_single.size()), kT, 0, s>>>(t.at(j_mds), (int)md_single.size(), c.d_mod,
-                                                                       (int)nq, (int)K, N);
+        {
+            Probe probe(kClsModDown, 8.0 * N * (K + L) * md_single.size(), s);
+            kb_moddown_single<<<grid_for(c, md_single.size()), kT, 0, s>>>(t.at(j_mds), (int)md_single.size(),
+                                                                           c.d_mod, (int)nq, (int)K, N);
+        }
         ntt_jobs(c, t.at(j_ntt_cs), (int)ntt_cs.size(), true, s);
-        kb_sub<<<grid_for(c, kt_sub.size()), kT, 0, s>>>(t.at(j_kt_sub), (int)kt_sub.size(), c.d_mod);
+        {
+            Probe probe(kClsElementwise, 8.0 * N * 3.0 * kt_sub.size(), s);
+            kb_sub<<<grid_for(c, kt_sub.size()), kT, 0, s>>>(t.at(j_kt_sub), (int)kt_sub.size(), c.d_mod);
+        }
         ntt_jobs(c, t.at(j_intt_kt), (int)intt_kt.size(), false, s);
-        kb_modup<<<grid_for(c, modup2.size()), kT, 0, s>>>(t.at(j_modup2), (int)modup2.size(), c.d_mod, N);
+        {
+            Probe probe(kClsModUp, 8.0 * N * (double)(md_single.size() * B * T), s);
+            kb_modup<<<grid_for(c, modup2.size()), kT, 0, s>>>(t.at(j_modup2), (int)modup2.size(), c.d_mod, N);
+        }
         ntt_jobs(c, t.at(j_ntt_dig2), (int)ntt_dig2.size(), true, s);
         Probe probe(kClsKeyMac, 8.0 * N * mac2.size() * (3.0 * B + 2.0), s);
         kb_mac<<<grid_for(c, mac2.size()), kT, 0, s>>>(t.at(j_mac2), (int)mac2.size(), c.d_mod, (int)nq, N);
     }
     // 5.
-    kb_accumulate<<<grid_for(c, accum.size()), kT, 0, s>>>(t.at(j_accum), (int)accum.size(), t.at(j_ginfo), c.d_mod,
-                                                           (int)nq, (int)L, (int)T, c.logN);
+    {
+        Probe probe(kClsCombine, 8.0 * N * (double)(count * (2 * ng + 1) * 2 * T), s);
+        kb_accumulate<<<grid_for(c, accum.size()), kT, 0, s>>>(t.at(j_accum), (int)accum.size(), t.at(j_ginfo),
+                                                               c.d_mod, (int)nq, (int)L, (int)T, c.logN);
+    }
     // 6.
     ntt_jobs(c, t.at(j_intt_po), (int)intt_po.size(), false, s);
-    kb_moddown<<<grid_for(c, md_pair.size()), kT, 0, s>>>(t.at(j_mdp), (int)md_pair.size(), c.d_mod, (int)nq, (int)K, N);
+    {
+        Probe probe(kClsModDown, 8.0 * N * (K + L) * md_pair.size(), s);
+        kb_moddown<<<grid_for(c, md_pair.size()), kT, 0, s>>>(t.at(j_mdp), (int)md_pair.size(), c.d_mod, (int)nq,
+                                                              (int)K, N);
+    }
     ntt_jobs(c, t.at(j_ntt_cf), (int)ntt_cf.size(), true, s);
-    kb_sub<<<grid_for(c, final_sub.size()), kT, 0, s>>>(t.at(j_final), (int)final_sub.size(), c.d_mod);
+    {
+        Probe probe(kClsElementwise, 8.0 * N * 3.0 * final_sub.size(), s);
+        kb_sub<<<grid_for(c, final_sub.size()), kT, 0, s>>>(t.at(j_final), (int)final_sub.size(), c.d_mod);
+    }
     if (st.rescale) {
         ntt_jobs(c, t.at(j_drop), (int)drop_intt.size(), false, s);
-        kb_rescale_prep<<<grid_for(c, prep.size()), kT, 0, s>>>(t.at(j_prep), (int)prep.size(), c.d_mod);
+        {
+            Probe probe(kClsElementwise, 8.0 * N * 2.0 * prep.size(), s);
+            kb_rescale_prep<<<grid_for(c, prep.size()), kT, 0, s>>>(t.at(j_prep), (int)prep.size(), c.d_mod);
+        }
         ntt_jobs(c, t.at(j_rem), (int)rem_ntt.size(), true, s);
+        Probe probe(kClsElementwise, 8.0 * N * 3.0 * fin.size(), s);
         kb_rescale_finish<<<grid_for(c, fin.size()), kT, 0, s>>>(t.at(j_fin), (int)fin.size(), c.d_mod);
     }
     check_cuda(cudaGetLastError(), "linear transform launch");

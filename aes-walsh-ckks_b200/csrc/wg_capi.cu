@@ -339,6 +339,47 @@ int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_
     });
 }
 
+struct wg_batch_plan {
+    wg::Context* c;
+    wg::BatchGraph* g;
+};
+
+int wg_batch_plan_create(wg_context* ctx, size_t count, const size_t* levels, uint64_t* const* xb,
+                         uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                         const int64_t* rots, wg_batch_plan** out) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(out, "wg_batch_plan_create");
+        *out = nullptr;
+        check_batch(c, count, levels, xb, xa, yb, ya, rots);
+        std::vector<uint64_t> galois(count);
+        std::vector<const wg::KeyEntry*> keys(count, nullptr);
+        for (size_t i = 0; i < count; ++i) {
+            const int64_t r = normalize_rotation(c, rots[i]);
+            galois[i] = r ? rotation_galois(c, r) : 0;
+            if (r) keys[i] = &c.key(WG_KEY_ROTATION, r);
+        }
+        wg::BatchGraph* g = wg::batch_graph_create(c, count, levels, xb, xa, yb, ya, galois.data(),
+                                                   &c.key(WG_KEY_RELIN, 0), keys.data());
+        *out = new wg_batch_plan{&c, g};
+    });
+}
+
+int wg_batch_plan_launch(wg_batch_plan* plan, void* stream) {
+    return guard([&] {
+        check_ptr(plan, "wg_batch_plan_launch");
+        wg::check_cuda(cudaSetDevice(plan->c->device), "cudaSetDevice");
+        wg::batch_graph_launch(*plan->g, S(stream));
+    });
+}
+
+void wg_batch_plan_destroy(wg_batch_plan* plan) {
+    if (!plan) return;
+    cudaSetDevice(plan->c->device);
+    delete plan->g;
+    delete plan;
+}
+
 int wg_sequence_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_t* levels, uint64_t* const* xb,
                                          uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
                                          const int64_t* rots, void* stream) {

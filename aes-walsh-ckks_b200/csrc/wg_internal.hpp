@@ -162,6 +162,9 @@ enum KernelClass : int {
     kClsElementwise = 5,  // tensor, add/sub, rescale steps
     kClsCount = 6
 };
+// Per-class launch counters: snapshot, and credit of the kernels a graph replay runs.
+void probe_counts(uint64_t* out);
+void probe_add(const uint64_t* counts);
 struct Probe {
     Probe(int cls, double bytes, cudaStream_t s);
     ~Probe();

@@ -43,6 +43,14 @@ Probe::~Probe() {
     if (slot >= 0) cudaEventRecord(state().end[slot], stream);
 }
 
+void probe_counts(uint64_t* out) {
+    for (int i = 0; i < kClsCount; ++i) out[i] = state().launches[i].load();
+}
+
+void probe_add(const uint64_t* counts) {
+    for (int i = 0; i < kClsCount; ++i) state().launches[i].fetch_add(counts[i], std::memory_order_relaxed);
+}
+
 }  // namespace wg
 
 extern "C" {

@@ -78,6 +78,10 @@ def lib() -> C.CDLL:
         L.wg_sub.argtypes = [vp, sz, vp, vp, sz, sz, vp]
         L.wg_batch_mul_relin_rescale_rotate.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp]
         L.wg_sequence_mul_relin_rescale_rotate.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp]
+        L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
+        L.wg_batch_plan_launch.argtypes = [vp, vp]
+        L.wg_batch_plan_destroy.argtypes = [vp]
+        L.wg_batch_plan_destroy.restype = None
         L.wg_lt_stage_create.argtypes = [vp, sz, sz, vp, vp, sz, sz, C.c_int, C.POINTER(vp)]
         L.wg_lt_stage_destroy.argtypes = [vp]
         L.wg_lt_stage_destroy.restype = None
@@ -197,6 +201,37 @@ class LtStage:
     def close(self):
         if getattr(self, "h", None):
             lib().wg_lt_stage_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchPlan:
+    """The batched mul + relin + rescale + rotate pipeline planned once for fixed device buffers
+    and captured as a CUDA graph (wg_batch_plan_*); launch() replays it on a stream."""
+
+    def __init__(self, ctx, levels, xb, xa, yb, ya, rots):
+        self.ctx = ctx
+        lv = np.ascontiguousarray(levels, dtype=np.uintp)
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        pxb, pxa, pyb, pya = arr(xb), arr(xa), arr(yb), arr(ya)
+        r = np.ascontiguousarray(rots, dtype=np.int64)
+        h = C.c_void_p()
+        _check(lib().wg_batch_plan_create(ctx.h, len(lv), lv.ctypes.data, pxb.ctypes.data, pxa.ctypes.data,
+                                          pyb.ctypes.data, pya.ctypes.data, r.ctypes.data, C.byref(h)))
+        self.h = h
+        self._keep = (xb, xa, yb, ya)  # the graph reads and writes these buffers
+
+    def launch(self, stream=None):
+        _check(lib().wg_batch_plan_launch(self.h, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wg_batch_plan_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -40,7 +40,7 @@ WORKLOAD = ("walsh15 batched ops: 64 ciphertexts at seeded levels 1..12, each ct
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="walsh", choices=["walsh", "reference"])
     ap.add_argument("--count", type=int, default=COUNT)
@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the op-by-op comparison pass")
     ap.add_argument("--no-probe", action="store_true", help="skip the per-kernel event-timing passes")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass")
+    ap.add_argument("--no-bsgs", action="store_true", help="skip the CoeffToSlot / SlotToCoeff section")
+    ap.add_argument("--e2e-chunk", type=int, default=16, help="ciphertexts per overlapped chunk (e2e)")
     return ap.parse_args()
 
 
@@ -67,18 +69,22 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device):
+    def __init__(self, device, period_ms=50):
         self.device = device
+        self.period_ms = period_ms
         self.rows = []
         self.proc = None
+        self.first = threading.Event()
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
-                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms",
+                 str(self.period_ms), "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.first.wait(timeout=15.0)  # the timed region starts once sampling runs
         except OSError:
             self.proc = None
         return self
@@ -88,6 +94,7 @@ class ClockSampler:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
                 self.rows.append(parts)
+                self.first.set()
 
     def __exit__(self, *a):
         if self.proc:
@@ -183,6 +190,96 @@ def reference_arm(args):
 
 
 # ------------------------------------------------------------------------------------------
+# CoeffToSlot / SlotToCoeff (BSGS linear-transform stages)
+# ------------------------------------------------------------------------------------------
+SLOTS = 1 << (LOGN - 1)
+
+
+def _two_sided(step, count):
+    return [step * k for k in range(count)] + [SLOTS - step * k for k in range(1, count)]
+
+
+# The walsh15 plans' stage shapes (level, diagonal indices, baby-step count, rescale), as the
+# reference's plan builder lays them out for this parameter set.
+S2C_STAGES = [(1, list(range(16)) + [SLOTS - k for k in range(1, 16)], 8, False),
+              (1, _two_sided(16, 32), 256, False),
+              (1, [512 * k for k in range(32)], 4096, True)]
+C2S_STAGES = [(12, [1024 * k for k in range(16)], 8192, False),
+              (12, _two_sided(64, 16), 512, True),
+              (11, _two_sided(8, 8), 64, False),
+              (11, list(range(8)) + [SLOTS - k for k in range(1, 8)], 8, True)]
+BSGS_BATCH = 8
+
+
+def bsgs_bench(wg, ctx, q, p, stream, timed, steps, warmup):
+    """Config 3: CoeffToSlot (4 stages from level 12) and SlotToCoeff (3 stages at level 1) over
+    a batch of 8 ciphertexts, diagonals with the plans' index sets (uniform residues), keys of
+    the walsh15 key shape (uniform residues)."""
+    import torch
+
+    N = 1 << LOGN
+    K = len(P_BITS)
+    L = len(Q_BITS)
+    mods = np.concatenate([q, p]).astype(np.uint64)
+    rng = np.random.default_rng(31)
+    need = set()
+    for _, idx, baby, _ in S2C_STAGES + C2S_STAGES:
+        need |= {i % baby for i in idx if i % baby} | {(i // baby) * baby for i in idx if i // baby}
+    parts = ctx.parts(L - 1)
+    for r in sorted(need):
+        if not ctx.has_key(wg.WG_KEY_ROTATION, r):
+            limb_mod = np.tile(np.repeat(mods, N), 2 * parts)
+            ctx.set_key(wg.WG_KEY_ROTATION, (rng.integers(0, 1 << 62, limb_mod.size, dtype=np.uint64) % limb_mod)
+                        .astype(np.uint64), rotation=r)
+
+    def stages(spec):
+        out = []
+        for level, idx, baby, resc in spec:
+            qp = np.concatenate([q[: level + 1], p])
+            col = np.tile(np.repeat(qp, N), len(idx))
+            d = (rng.integers(0, 1 << 62, col.size, dtype=np.uint64) % col).astype(np.uint64)
+            out.append((wg.LtStage(ctx, level, idx, d, baby, SLOTS, resc), level, len(idx), baby))
+        return out
+
+    res = {}
+    qcol = np.repeat(q, N)
+    cts = torch.from_numpy(np.stack([(rng.integers(0, 1 << 62, L * N, dtype=np.uint64) % qcol).astype(np.uint64)
+                                     for _ in range(2 * BSGS_BATCH)]).view(np.int64)).cuda()
+    bs = [cts[2 * i] for i in range(BSGS_BATCH)]
+    as_ = [cts[2 * i + 1] for i in range(BSGS_BATCH)]
+    for name, spec in (("coeff_to_slot", C2S_STAGES), ("slot_to_coeff", S2C_STAGES)):
+        sts = stages(spec)
+
+        def run():
+            for st, _, _, _ in sts:
+                st.apply(bs, as_, stream)
+
+        for _ in range(warmup):
+            run()
+        ms = timed(run, steps)
+        per_stage = []
+        for st, level, d, baby in sts:
+            sms = timed(lambda: st.apply(bs, as_, stream), steps)
+            per_stage.append({"level": level, "diagonals": d, "baby": baby, "ms": sms})
+        # algorithmic bytes: each diagonal read once per batch, each rotation key once, each
+        # ciphertext read and written once
+        total_bytes = 0.0
+        for (level, idx, baby, _), ps in zip(spec, per_stage):
+            Lq, beta = level + 1, ctx.parts(level)
+            R = len({i % baby for i in idx if i % baby} | {(i // baby) * baby for i in idx if i // baby})
+            sb = 8.0 * N * (len(idx) * (Lq + K) + R * beta * 2 * (Lq + K) + BSGS_BATCH * 4 * Lq)
+            ps["gbs"] = sb / (ps["ms"] * 1e6)
+            total_bytes += sb
+        res[name] = {"ciphertexts_per_s": BSGS_BATCH / (ms / 1000.0), "ms_per_batch": ms,
+                     "algorithmic_gbs": total_bytes / (ms * 1e6), "stages": per_stage}
+        for st, _, _, _ in sts:
+            st.close()
+    res["batch"] = BSGS_BATCH
+    res["data"] = "diagonals with the walsh15 plans' index sets, uniform residues; uniform keys"
+    return res
+
+
+# ------------------------------------------------------------------------------------------
 # device arm
 # ------------------------------------------------------------------------------------------
 def main():
@@ -244,8 +341,15 @@ def main():
     yb = [dy[i, 0] for i in range(count)]
     ya = [dy[i, 1] for i in range(count)]
 
+    work.copy_(pristine)
+    plan = wg.BatchPlan(ctx, levels, xb, xa, yb, ya, rots)
+
     def step():
-        work.copy_(pristine)
+        # one graph replay of the whole batched pipeline; every step runs on the previous
+        # step's outputs (same levels and shapes: the work does not depend on residue values)
+        plan.launch(stream)
+
+    def step_nograph():
         ctx.batch_mul_relin_rescale_rotate(levels, xb, xa, yb, ya, rots, stream=stream)
 
     def barrier():
@@ -275,11 +379,16 @@ def main():
         ms = timed(step, args.steps)
     launches = wg.launch_count() - launches0
 
-    # per-kernel-class device time over the same K steps (CUDA events on the launch stream)
+    for _ in range(args.warmup):
+        step_nograph()
+    nograph_ms = timed(step_nograph, args.steps)
+
+    # per-kernel-class device time over the same K steps (CUDA events on the launch stream,
+    # so the un-captured batched call is used)
     kernels = {}
     for name, cls in ([] if args.no_probe else wg.KCLASS.items()):
         wg.probe_begin(cls, 60000)
-        timed(step, args.steps)
+        timed(step_nograph, args.steps)
         n, kms, kbytes = wg.probe_end()
         kernels[name] = {"launches": n, "ms": kms, "bytes": kbytes}
     probed_total = sum(v["ms"] for v in kernels.values())
@@ -302,7 +411,6 @@ def main():
 
     # the same workload op by op (the plain per-operation GPU path)
     def plain_step():
-        work.copy_(pristine)
         ctx.batch_mul_relin_rescale_rotate(levels, xb, xa, yb, ya, rots, stream=stream, plain=True)
 
     plain_ms, plain_launches = None, None
@@ -312,31 +420,64 @@ def main():
         plain_ms = timed(plain_step, max(1, args.steps // 2))
         plain_launches = (wg.launch_count() - plain_launches0) / max(1, args.steps // 2)
 
-    # end to end through the C ABI with host buffers: H2D of each ciphertext's active limbs
-    # (x and y), the batched call, D2H of the rescaled and rotated results.
+    # End to end through the C ABI with host buffers: H2D of each ciphertext's active limbs
+    # (x and y), the batched pipeline, D2H of the rescaled and rotated results.  The batch is
+    # cut into chunks, each with its own graph plan; chunk k's compute overlaps chunk k+1's
+    # upload and chunk k-1's download (copy-in, compute and copy-out streams).
     pin_x = torch.from_numpy(host_x.view(np.int64)).pin_memory()
     pin_y = torch.from_numpy(host_y.view(np.int64)).pin_memory()
     pin_out = torch.empty((count, 2, stride), dtype=torch.int64).pin_memory()
     h2d = int(sum(4 * (int(lv) + 1) * N * 8 for lv in levels))
     d2h = int(sum(2 * int(lv) * N * 8 for lv in levels))
-
-    def e2e_step():
-        for i in range(count):
-            nb = (int(levels[i]) + 1) * N * 8
-            for j in range(2):
-                wg.memcpy_htod(work[i, j], pin_x[i, j].data_ptr(), nb, stream=stream)
-                wg.memcpy_htod(dy[i, j], pin_y[i, j].data_ptr(), nb, stream=stream)
-        ctx.batch_mul_relin_rescale_rotate(levels, xb, xa, yb, ya, rots, stream=stream)
-        for i in range(count):
-            nb = int(levels[i]) * N * 8
-            for j in range(2):
-                wg.memcpy_dtoh(pin_out[i, j].data_ptr(), work[i, j], nb, stream=stream)
-
+    chunk = max(1, min(args.e2e_chunk, count))
+    bounds = [(i, min(count, i + chunk)) for i in range(0, count, chunk)]
     e2e_ms = None
     if not args.no_e2e:
+        cplans = [wg.BatchPlan(ctx, levels[a:b], xb[a:b], xa[a:b], yb[a:b], ya[a:b], rots[a:b]) for a, b in bounds]
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+        ev = lambda: torch.cuda.Event()
+        in_done = [ev() for _ in bounds]
+        comp_done = [ev() for _ in bounds]
+        out_done = [ev() for _ in bounds]
+        for e in out_done:
+            e.record(s_out)
+
+        def e2e_step():
+            start = ev()
+            start.record(stream)
+            s_in.wait_event(start)
+            for k, (a, b) in enumerate(bounds):
+                s_in.wait_event(out_done[k])  # the chunk's buffers are free again
+                for i in range(a, b):
+                    nb = (int(levels[i]) + 1) * N * 8
+                    for j in range(2):
+                        wg.memcpy_htod(work[i, j], pin_x[i, j].data_ptr(), nb, stream=s_in)
+                        wg.memcpy_htod(dy[i, j], pin_y[i, j].data_ptr(), nb, stream=s_in)
+                in_done[k].record(s_in)
+                stream.wait_event(in_done[k])
+                cplans[k].launch(stream)
+                comp_done[k].record(stream)
+                s_out.wait_event(comp_done[k])
+                for i in range(a, b):
+                    nb = int(levels[i]) * N * 8
+                    for j in range(2):
+                        wg.memcpy_dtoh(pin_out[i, j].data_ptr(), work[i, j], nb, stream=s_out)
+                out_done[k].record(s_out)
+            stream.wait_stream(s_out)
+
         for _ in range(args.warmup):
             e2e_step()
         e2e_ms = timed(e2e_step, args.steps)
+        # the last chunk's results are back in pinned host memory and match the device copy
+        torch.cuda.synchronize()
+        i = count - 1
+        nb = int(levels[i]) * N
+        assert torch.equal(pin_out[i, 0, :nb], work[i, 0, :nb].cpu())
+        for cp in cplans:
+            cp.close()
+
+    bsgs = None if args.no_bsgs else bsgs_bench(wg, ctx, q, p, stream, timed, max(1, args.steps // 2),
+                                                args.warmup)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -359,15 +500,19 @@ def main():
                    "ciphertexts_per_gpu": count, "levels": [int(x) for x in levels],
                    "rotation_keys": len(set(rots)), "keys": "uniform residues of the walsh15 key shape",
                    "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2: ~0.9 GB of ciphertexts plus ~1.1 GB of keys per step"},
+                   "l2": "inputs larger than L2: ~0.9 GB of ciphertexts plus ~1.1 GB of keys per step",
+                   "step": "one CUDA-graph replay of the batched pipeline on the previous step's outputs",
+                   "e2e_chunk": chunk},
         "clocks": clk.summary(),
         "e2e": {"value": count * world / (e2e_ms / 1000.0) if e2e_ms else None, "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "gpu_launches": int(launches),
+        "batched_nograph": {"value": count * world / (nograph_ms / 1000.0), "unit": UNIT, "ms_per_step": nograph_ms},
         "plain_per_op": {"value": count * world / (plain_ms / 1000.0) if plain_ms else None, "unit": UNIT,
                          "ms_per_step": plain_ms, "launches_per_step": plain_launches},
         "roofline": roofline,
         "kernels": kernels,
+        "bsgs": bsgs,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)

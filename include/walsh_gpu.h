@@ -142,6 +142,23 @@ int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_
                                       const uint64_t* const* yb, const uint64_t* const* ya,
                                       const int64_t* rots, void* stream);
 
+/* The same batched pipeline planned once for fixed buffers and captured as a CUDA graph
+ * (no counterpart in the reference, which plans nothing ahead).  Create takes the arguments
+ * of wg_batch_mul_relin_rescale_rotate minus the stream, builds the job tables, uploads them
+ * into memory the plan owns (with its own scratch) and captures the launch sequence; launch
+ * replays it on `stream`, with no host planning or upload, reading and writing the buffers
+ * given at creation, whose current contents are used.  Results equal those of
+ * wg_batch_mul_relin_rescale_rotate.  Launches of one plan must not overlap (they share its
+ * scratch); different plans are independent.  The plan refers to the context's tables and
+ * to the switching keys installed at creation: destroy it before the context, and do not
+ * replace those keys while it exists. */
+typedef struct wg_batch_plan wg_batch_plan;
+int wg_batch_plan_create(wg_context* ctx, size_t count, const size_t* levels, uint64_t* const* xb,
+                         uint64_t* const* xa, const uint64_t* const* yb, const uint64_t* const* ya,
+                         const int64_t* rots, wg_batch_plan** out);
+int wg_batch_plan_launch(wg_batch_plan* plan, void* stream);
+void wg_batch_plan_destroy(wg_batch_plan* plan);
+
 /* One CoeffToSlot / SlotToCoeff stage: a baby-step / giant-step linear transform evaluated in
  * the QP basis (hoisted baby rotations without ModDown, one ModDown per giant step).
  * `diagonals` (host) holds the stage's nterms plaintexts [term][level+1+K limbs][N] in

@@ -210,6 +210,18 @@ def test_walsh15_batched_ops(wg, oracle_mod):
                                        [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots,
                                        plain=True)
     assert (_host(wg, pxb) == gb).all() and (_host(wg, pxa) == ga).all()
+    # the graph-captured plan over its own buffers: same residues, replayable
+    gxb, gxa = _dev(wg, xb), _dev(wg, xa)
+    plan = wg.BatchPlan(ctx, levels, [sl(gxb, i) for i in range(count)], [sl(gxa, i) for i in range(count)],
+                        [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots)
+    n0 = wg.launch_count()
+    for _ in range(2):
+        gxb.copy_(_dev(wg, xb))
+        gxa.copy_(_dev(wg, xa))
+        plan.launch()
+        assert (_host(wg, gxb) == gb).all() and (_host(wg, gxa) == ga).all()
+    assert wg.launch_count() - n0 >= 2 * 20
+    plan.close()
     ob, oa = xb.copy(), xa.copy()
     o.batched_ops(levels, ob, oa, yb, ya, relin, [keys[r] for r in ct_rots], ct_rots, stride, 8)
     for i in range(count):
