@@ -49,16 +49,17 @@ namespace {
 
 constexpr int kGiantBatch = 8;  // ciphertexts summed per thread in the giant-step kernel
 
+// Baby rotation `slot` of QP limb i for ciphertexts [c0, c0 + nc) of the batch: the key words
+// of a coefficient are loaded once and used for every ciphertext of the group.
 struct BabyJob {
     const uint64_t* key;
-    const uint64_t* key_term;
-    const uint64_t* digits;
-    const uint64_t* b_init;  // b limb (Q limbs) or null (P limbs)
-    uint64_t* out_a;
-    uint64_t* out_b;
-    size_t part_stride;
     uint64_t galois_inv;
-    int L, K, parts, alpha, key_level, i;
+    int key_level, i, slot, c0, nc, pad;
+};
+
+struct CtRef {
+    const uint64_t* a;
+    const uint64_t* b;
 };
 
 struct TermRef {
@@ -94,18 +95,52 @@ struct AccumJob {
     int ngiants, i, pad0, pad1;
 };
 
-__global__ void __launch_bounds__(kT) kb_baby(const BabyJob* jobs, int n, const Modulus* mods, int nq, int logN) {
+__global__ void __launch_bounds__(kT) kb_baby(const BabyJob* jobs, int n, const CtRef* __restrict__ cts,
+                                              const uint64_t* __restrict__ digits, uint64_t* __restrict__ babies,
+                                              const Modulus* mods, int nq, int L, int K, int parts, int alpha,
+                                              int nslots, int logN) {
     const BabyJob* j = job_of(jobs, n);
     if (!j) return;
     const size_t N = size_t{1} << logN;
     const uint32_t x = blockIdx.x * kT + threadIdx.x;
-    const Modulus& m = mods[j->i >= j->L ? nq + (j->i - j->L) : j->i];
-    uint64_t acc_a = 0, acc_b = j->b_init ? j->b_init[x] : 0;
-    mac_accumulate(m, j->L, j->K, j->parts, j->alpha, j->key, j->key_level, j->key_term, j->digits, j->part_stride,
-                   N, j->i, x, acc_a, acc_b);
+    const int i = j->i;
+    const int T = L + K;
+    const bool is_p = i >= L;
+    const Modulus& m = mods[is_p ? nq + (i - L) : i];
+    const uint64_t q = m.q, qninv = m.qninv;
+    const size_t key_limbs = (size_t)j->key_level + 1 + K;
+    const size_t klimb = is_p ? (size_t)j->key_level + 1 + (i - L) : (size_t)i;
+    const size_t part_stride = (size_t)T * N;
+    const size_t limb = (size_t)i * N + x;
+    uint64_t acc_a[kGiantBatch], acc_b[kGiantBatch];
+#pragma unroll
+    for (int c = 0; c < kGiantBatch; ++c) {
+        acc_a[c] = 0;
+        acc_b[c] = (c < j->nc && !is_p) ? cts[j->c0 + c].b[limb] : 0;
+    }
+    for (int p = 0; p < parts; ++p) {
+        const int s0 = p * alpha, s1 = s0 + alpha < L ? s0 + alpha : L;
+        const bool own = !is_p && i >= s0 && i < s1;  // source limb: the key term itself
+        const uint64_t ka = j->key[(((size_t)p * 2 + 0) * key_limbs + klimb) * N + x];
+        const uint64_t kb = j->key[(((size_t)p * 2 + 1) * key_limbs + klimb) * N + x];
+#pragma unroll
+        for (int c = 0; c < kGiantBatch; ++c) {
+            if (c >= j->nc) break;
+            const int ci = j->c0 + c;
+            const uint64_t d = own ? cts[ci].a[limb] : digits[((size_t)ci * parts + p) * part_stride + limb];
+            acc_a[c] = add_mod(acc_a[c], mont_mul(d, ka, q, qninv), q);
+            acc_b[c] = add_mod(acc_b[c], mont_mul(d, kb, q, qninv), q);
+        }
+    }
     const uint32_t dst = automorphism_src(x, j->galois_inv, logN);
-    j->out_a[dst] = acc_a;
-    j->out_b[dst] = acc_b;
+    const size_t slot_words = 2 * (size_t)T * N;
+#pragma unroll
+    for (int c = 0; c < kGiantBatch; ++c) {
+        if (c >= j->nc) break;
+        uint64_t* o = babies + ((size_t)(j->c0 + c) * nslots + j->slot) * slot_words + (size_t)i * N;
+        o[dst] = acc_a[c];
+        o[(size_t)T * N + dst] = acc_b[c];
+    }
 }
 
 __global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, const TermRef* __restrict__ term_table,
@@ -305,18 +340,17 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     }
     // 2. babies: baby 0 as a copy (P limbs zeroed below), others by MAC + scatter
     std::vector<BabyJob> baby_jobs;
+    std::vector<CtRef> ct_refs;
+    for (size_t ci = 0; ci < count; ++ci) ct_refs.push_back({a[ci], b[ci]});
     const bool baby0 = !babies.empty() && babies[0] == 0;
-    for (size_t ci = 0; ci < count; ++ci) {
-        for (size_t k = 0; k < ns; ++k) {
-            uint64_t* slot = babybuf + (ci * ns + k) * slotw;
-            if (babies[k] == 0) continue;
-            const KeyEntry& key = rot_key(babies[k]);
-            const uint64_t ginv = host::powmod(galois_of(babies[k]), N - 1, 2 * N);
+    for (size_t k = 0; k < ns; ++k) {
+        if (babies[k] == 0) continue;
+        const KeyEntry& key = rot_key(babies[k]);
+        const uint64_t ginv = host::powmod(galois_of(babies[k]), N - 1, 2 * N);
+        for (size_t c0 = 0; c0 < count; c0 += kGiantBatch)
             for (size_t i = 0; i < T; ++i)
-                baby_jobs.push_back({key.d_data, a[ci], digits + ci * B * T * N, i < L ? b[ci] + i * N : nullptr,
-                                     slot + i * N, slot + T * N + i * N, T * N, ginv, (int)L, (int)K, (int)B,
-                                     (int)c.alpha, (int)key.key_level, (int)i});
-        }
+                baby_jobs.push_back({key.d_data, ginv, (int)key.key_level, (int)i, (int)k, (int)c0,
+                                     (int)std::min<size_t>(kGiantBatch, count - c0), 0});
     }
     // 3. giant sums
     std::vector<TermRef> terms;
@@ -426,6 +460,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     const ModUpJob* j_modup = t.add(modup);
     const NttJob* j_ntt_dig = t.add(ntt_dig);
     const BabyJob* j_baby = t.add(baby_jobs);
+    const CtRef* j_cts = t.add(ct_refs);
     const TermRef* j_terms = t.add(terms);
     const GiantJob* j_giant = t.add(giant_jobs);
     const NttJob* j_intt_pg = t.add(intt_pg);
@@ -456,9 +491,12 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     ntt_jobs(c, t.at(j_ntt_dig), (int)ntt_dig.size(), true, s);
     // 2.
     if (!baby_jobs.empty()) {
-        Probe probe(kClsKeyMac, 8.0 * N * baby_jobs.size() * (3.0 * B + 3.0), s);
-        kb_baby<<<grid_for(c, baby_jobs.size()), kT, 0, s>>>(t.at(j_baby), (int)baby_jobs.size(), c.d_mod, (int)nq,
-                                                             c.logN);
+        double bytes = 0;
+        for (const BabyJob& bj : baby_jobs) bytes += 8.0 * N * (2.0 * B + bj.nc * (B + 3.0));
+        Probe probe(kClsKeyMac, bytes, s);
+        kb_baby<<<grid_for(c, baby_jobs.size()), kT, 0, s>>>(t.at(j_baby), (int)baby_jobs.size(), t.at(j_cts), digits,
+                                                             babybuf, c.d_mod, (int)nq, (int)L, (int)K, (int)B,
+                                                             (int)c.alpha, (int)ns, c.logN);
     }
     // 3.
     {

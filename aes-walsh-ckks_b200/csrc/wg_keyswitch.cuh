@@ -39,33 +39,51 @@ WG_HD uint32_t automorphism_src(uint32_t i, uint64_t galois, int logN) {
     return bitrev32((uint32_t)((src_exp - 1) >> 1), logN);
 }
 
-// HPS ModUp of one coefficient for one digit.
+// HPS ModUp of one coefficient for one digit, digit width at most W (the scaled residues stay
+// in registers: every index below is a compile-time constant after unrolling).
 //   src:   coefficient-domain key term, limb-major (Q limb k at src + k*N)
 //   digit: QP digit buffer of this part (limb t at digit + t*N)
+template <int W, class Desc>
+WG_HD void modup_coeff_w(const Desc& d, const Modulus* __restrict__ mods, const uint64_t* __restrict__ src,
+                         uint64_t* __restrict__ digit, size_t N, size_t coeff) {
+    uint64_t scaled[W];
+    double alpha = 0.0;
+    const int n = d.src_count;
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+        scaled[i] = 0;
+        if (i < n) {
+            const uint64_t qi = mods[d.src_first + i].q;
+            const uint64_t x = red4q(src[(size_t)(d.src_first + i) * N + coeff], qi);
+            const uint64_t s = mul_shoup(x, WG_LDG(d.qhat_inv + i), WG_LDG(d.qhat_inv_s + i), qi);
+            scaled[i] = s;
+            alpha = dadd(alpha, dmul(u2d(s), WG_LDG(d.src_inv + i)));
+        }
+    }
+    uint64_t hps = round_half_up(alpha);
+    if (hps > (uint64_t)n) hps = (uint64_t)n;
+    for (int t = 0; t < d.dst_count; ++t) {
+        const uint64_t m = mods[WG_LDG(d.dst_mod + t)].q;
+        const uint64_t* row = d.qhat + (size_t)t * n;
+        const uint64_t* row_s = d.qhat_s + (size_t)t * n;
+        uint64_t acc = 0;
+#pragma unroll
+        for (int i = 0; i < W; ++i)
+            if (i < n) acc = add_mod(acc, mul_shoup(scaled[i], WG_LDG(row + i), WG_LDG(row_s + i), m), m);
+        const uint64_t corr = WG_LDG(d.corr + (size_t)t * (n + 1) + hps);
+        digit[(size_t)WG_LDG(d.dst_limb + t) * N + coeff] = sub_mod(acc, corr, m);
+    }
+}
+
 template <class Desc>
 WG_HD void modup_coeff(const Desc& d, const Modulus* __restrict__ mods, const uint64_t* __restrict__ src,
                        uint64_t* __restrict__ digit, size_t N, size_t coeff) {
-    uint64_t scaled[kMaxDigitWidth];
-    double alpha = 0.0;
-    for (int i = 0; i < d.src_count; ++i) {
-        const uint64_t qi = mods[d.src_first + i].q;
-        const uint64_t x = red4q(src[(size_t)(d.src_first + i) * N + coeff], qi);
-        const uint64_t s = mul_shoup(x, WG_LDG(d.qhat_inv + i), WG_LDG(d.qhat_inv_s + i), qi);
-        scaled[i] = s;
-        alpha = dadd(alpha, dmul(u2d(s), WG_LDG(d.src_inv + i)));
-    }
-    uint64_t hps = round_half_up(alpha);
-    if (hps > (uint64_t)d.src_count) hps = (uint64_t)d.src_count;
-    for (int t = 0; t < d.dst_count; ++t) {
-        const uint64_t m = mods[WG_LDG(d.dst_mod + t)].q;
-        const uint64_t* row = d.qhat + (size_t)t * d.src_count;
-        const uint64_t* row_s = d.qhat_s + (size_t)t * d.src_count;
-        uint64_t acc = 0;
-        for (int i = 0; i < d.src_count; ++i)
-            acc = add_mod(acc, mul_shoup(scaled[i], WG_LDG(row + i), WG_LDG(row_s + i), m), m);
-        const uint64_t corr = WG_LDG(d.corr + (size_t)t * (d.src_count + 1) + hps);
-        digit[(size_t)WG_LDG(d.dst_limb + t) * N + coeff] = sub_mod(acc, corr, m);
-    }
+    if (d.src_count <= 4)
+        modup_coeff_w<4>(d, mods, src, digit, N, coeff);
+    else if (d.src_count <= 8)
+        modup_coeff_w<8>(d, mods, src, digit, N, coeff);
+    else
+        modup_coeff_w<kMaxDigitWidth>(d, mods, src, digit, N, coeff);
 }
 
 // Folded ModDown contribution of one coefficient for Q limb qi:
@@ -87,6 +105,39 @@ WG_HD uint64_t moddown_coeff(const Modulus& mq, const Modulus* __restrict__ pmod
     return sub_mod(acc, hps, q);
 }
 
+// moddown_all_limbs for at most KW P limbs (the P residues stay in registers).
+template <bool FUSED, int KW>
+WG_HD void moddown_all_limbs_k(const Modulus* __restrict__ mods, int nq, int L, int K,
+                               const uint64_t* __restrict__ src_p, size_t N, size_t coeff,
+                               const uint64_t* __restrict__ inv, const uint64_t* __restrict__ inv_s,
+                               uint64_t* __restrict__ out) {
+    uint64_t s[KW];
+    double alpha = 0.0;
+#pragma unroll
+    for (int pi = 0; pi < KW; ++pi) {
+        s[pi] = 0;
+        if (pi < K) {
+            const Modulus& mp = mods[nq + pi];
+            s[pi] = red4q(src_p[(size_t)pi * N + coeff], mp.q);
+            alpha = FUSED ? dfma(u2d(s[pi]), mp.inv_q, alpha) : dadd(alpha, dmul(u2d(s[pi]), mp.inv_q));
+        }
+    }
+    uint64_t hps = round_half_up(alpha);
+    if (hps > (uint64_t)K) hps = (uint64_t)K;
+    for (int qi = 0; qi < L; ++qi) {
+        const Modulus& mq = mods[qi];
+        const uint64_t q = mq.q;
+        const uint64_t* iv = inv + (size_t)qi * K;
+        const uint64_t* ivs = inv_s + (size_t)qi * K;
+        uint64_t acc = 0;
+#pragma unroll
+        for (int pi = 0; pi < KW; ++pi)
+            if (pi < K)
+                acc = add_mod(acc, mul_shoup(barrett_u64(s[pi], q, mq.mu_hi), WG_LDG(iv + pi), WG_LDG(ivs + pi), q), q);
+        out[(size_t)qi * N + coeff] = sub_mod(acc, hps, q);
+    }
+}
+
 // Folded ModDown of one coefficient for Q limbs [0, L): the P residues are read and the FP64
 // alpha estimate formed once, then each limb gets its Shoup dot product (same arithmetic as
 // moddown_coeff, which recomputes both per limb).  out[qi * N + coeff] = contribution.
@@ -98,25 +149,12 @@ WG_HD void moddown_all_limbs(const Modulus* __restrict__ mods, int nq, int L, in
                              const uint64_t* __restrict__ src_p, size_t N, size_t coeff,
                              const uint64_t* __restrict__ inv, const uint64_t* __restrict__ inv_s,
                              uint64_t* __restrict__ out) {
-    uint64_t s[kMaxPLimbs];
-    double alpha = 0.0;
-    for (int pi = 0; pi < K; ++pi) {
-        const Modulus& mp = mods[nq + pi];
-        s[pi] = red4q(src_p[(size_t)pi * N + coeff], mp.q);
-        alpha = FUSED ? dfma(u2d(s[pi]), mp.inv_q, alpha) : dadd(alpha, dmul(u2d(s[pi]), mp.inv_q));
-    }
-    uint64_t hps = round_half_up(alpha);
-    if (hps > (uint64_t)K) hps = (uint64_t)K;
-    for (int qi = 0; qi < L; ++qi) {
-        const Modulus& mq = mods[qi];
-        const uint64_t q = mq.q;
-        const uint64_t* iv = inv + (size_t)qi * K;
-        const uint64_t* ivs = inv_s + (size_t)qi * K;
-        uint64_t acc = 0;
-        for (int pi = 0; pi < K; ++pi)
-            acc = add_mod(acc, mul_shoup(barrett_u64(s[pi], q, mq.mu_hi), WG_LDG(iv + pi), WG_LDG(ivs + pi), q), q);
-        out[(size_t)qi * N + coeff] = sub_mod(acc, hps, q);
-    }
+    if (K <= 4)
+        moddown_all_limbs_k<FUSED, 4>(mods, nq, L, K, src_p, N, coeff, inv, inv_s, out);
+    else if (K <= 8)
+        moddown_all_limbs_k<FUSED, 8>(mods, nq, L, K, src_p, N, coeff, inv, inv_s, out);
+    else
+        moddown_all_limbs_k<FUSED, kMaxPLimbs>(mods, nq, L, K, src_p, N, coeff, inv, inv_s, out);
 }
 
 // Key inner product for QP limb i at one coefficient, added digit by digit onto (acc_a,

@@ -80,10 +80,23 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS, 4)
         const int e = t + k * P::THREADS;
         sm[pad16(e)] = xin[tile_offset<LOGN, FWD, COLS>(tile, e)];
     }
-    for (int e = t; e < P::TW; e += P::THREADS) {
-        const size_t src = twiddle_src<LOGN, FWD, COLS>(tile, e);
-        tw_s[e] = __ldg(tw + src);
-        tws_s[e] = __ldg(tws + src);
+    if (COLS) {
+        for (int e = t; e < P::TW; e += P::THREADS) {
+            tw_s[e] = __ldg(tw + e);
+            tws_s[e] = __ldg(tws + e);
+        }
+    } else {
+        // row-stage k: SUBS * 2^k contiguous table entries (twiddle_src order)
+#pragma unroll
+        for (int k = 0; k < P::MB; ++k) {
+            const int cnt = P::SUBS << k;
+            const int dst = P::SUBS * ((1 << k) - 1);
+            const size_t src = ((size_t)1 << (P::NB1 + k)) + (size_t)tile * cnt;
+            for (int e = t; e < cnt; e += P::THREADS) {
+                tw_s[dst + e] = __ldg(tw + src + e);
+                tws_s[dst + e] = __ldg(tws + src + e);
+            }
+        }
     }
     __syncthreads();
 

@@ -85,8 +85,19 @@ WG_HD size_t twiddle_src(int tile, int t) {
     return ((size_t)1 << (P::NB1 + k)) + (size_t)tile * P::SUBS * ((size_t)1 << k) + (size_t)(t - off);
 }
 
+// Bits of element j (0..7) of a round placed at the plan's group positions.
+WG_HDC int round_bits(const RoundPlan& p, int j) {
+    return ((j & 1) << p.g[0]) | (((j >> 1) & 1) << p.g[1]) | (((j >> 2) & 1) << p.g[2]);
+}
+
 // One round (up to three radix-2 stages) for thread (sub, o); tw / tws are the staged
 // twiddles of this CTA (twiddle_src order).
+//
+// The thread's 8 elements are base | round_bits(j), with base's bits disjoint from the group
+// positions, so every index splits into a runtime part (one per round, or one per stage for
+// twiddles) plus a compile-time offset: pad16 and shifts distribute over disjoint bit sets.
+// Loads then use immediate offsets, and butterflies of a stage that share a twiddle load it
+// once (same address).
 template <int LOGN, bool FWD, bool COLS, int RD>
 WG_HD void ntt_round(uint64_t* sm, int sub, int o, uint64_t q, const uint64_t* __restrict__ tw,
                      const uint64_t* __restrict__ tws) {
@@ -97,13 +108,14 @@ WG_HD void ntt_round(uint64_t* sm, int sub, int o, uint64_t q, const uint64_t* _
     base = insert_zero(base, plan.g[0]);
     base = insert_zero(base, plan.g[1]);
     base = insert_zero(base, plan.g[2]);
-    int h[8];
+    // element index e = COLS ? h * SUBS + sub : (sub << MB) | h, with h = base | round_bits(j)
+    const int e_base = COLS ? base * P::SUBS + sub : (sub << P::MB) | base;
+    uint64_t* row = sm + pad16(e_base);
     uint64_t v[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        h[j] = base | ((j & 1) << plan.g[0]) | (((j >> 1) & 1) << plan.g[1]) | (((j >> 2) & 1) << plan.g[2]);
-        const int e = COLS ? h[j] * P::SUBS + sub : (sub << P::MB) | h[j];
-        v[j] = sm[pad16(e)];
+        const int c = COLS ? round_bits(plan, j) * P::SUBS : round_bits(plan, j);
+        v[j] = row[pad16(c)];
     }
 #pragma unroll
     for (int s = 0; s < plan.ns; ++s) {
@@ -112,12 +124,14 @@ WG_HD void ntt_round(uint64_t* sm, int sub, int o, uint64_t q, const uint64_t* _
         // The table index of a pair is (1 << (n-1-gb)) + (x >> (gb+1)) for its global index x
         // and stage bit gb; relative to the staged block it is:
         const int base_idx = COLS ? (1 << (P::NB1 - 1 - b)) : P::SUBS * ((1 << (P::NB2 - 1 - b)) - 1) + (sub << (P::NB2 - 1 - b));
+        const uint64_t* tw_st = tw + base_idx + (base >> (b + 1));
+        const uint64_t* tws_st = tws + base_idx + (base >> (b + 1));
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             if ((j >> jb) & 1) continue;
             const int j1 = j | (1 << jb);
-            const int idx = base_idx + (h[j] >> (b + 1));
-            const uint64_t w = tw[idx], ws = tws[idx];
+            const int k = round_bits(plan, j) >> (b + 1);
+            const uint64_t w = tw_st[k], ws = tws_st[k];
             if (FWD) {
                 uint64_t t = v[j];
                 if (t >= two_q) t -= two_q;
@@ -135,8 +149,8 @@ WG_HD void ntt_round(uint64_t* sm, int sub, int o, uint64_t q, const uint64_t* _
     }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        const int e = COLS ? h[j] * P::SUBS + sub : (sub << P::MB) | h[j];
-        sm[pad16(e)] = v[j];
+        const int c = COLS ? round_bits(plan, j) * P::SUBS : round_bits(plan, j);
+        row[pad16(c)] = v[j];
     }
 }
 

@@ -32,6 +32,7 @@
 #include "ckks_aes_params.hpp"
 #include "ckks_ciphertext.hpp"
 #include "ckks_linear_transform.hpp"
+#include "ckks_modraise.hpp"
 #include "ckks_context.hpp"
 #include "ckks_conjugate.hpp"
 #include "ckks_keyswitch.hpp"
@@ -189,25 +190,39 @@ int ref_ctx_ntt(void* h, uint64_t* poly, size_t limbs, int inverse, int lazy) {
 }
 
 // kind: 0 = rotation (by `rot`), 1 = conjugation, 2 = relinearization.
+// Switching keys by kind: 0 rotation, 1 conjugation, 2 relinearization, 3 dense-to-sparse
+// (compact q0/p0 key: one level-0 part whose a and b hold the q0 limb then the p0 limb),
+// 4 sparse-to-dense (hybrid key at the top level).  Kinds 3 and 4 exist in bootstrapping
+// contexts only.
+static std::span<const CKKSCiphertext> key_span(const CKKSContext& c, int kind, int64_t rot) {
+    switch (kind) {
+        case 0: return c.getRotationKey(rot);
+        case 1: return c.getConjugationKey();
+        case 2: return c.getRelinHybrid(c.getParams().getMaxLevel());
+        case 3: return c.getDenseToSparseSwitchKey();
+        case 4: return c.getSparseToDenseSwitchKey();
+        default: throw std::invalid_argument("ref_ctx_key: unknown key kind");
+    }
+}
+
 int ref_ctx_key_shape(void* h, int kind, int64_t rot, size_t* parts, size_t* key_level) {
     return guarded([&] {
-        const auto& c = static_cast<RefCtx*>(h)->ctx;
-        std::span<const CKKSCiphertext> k =
-            kind == 0 ? c.getRotationKey(rot)
-                      : (kind == 1 ? c.getConjugationKey() : c.getRelinHybrid(c.getParams().getMaxLevel()));
+        std::span<const CKKSCiphertext> k = key_span(static_cast<RefCtx*>(h)->ctx, kind, rot);
         *parts = k.size();
         *key_level = k.empty() ? 0 : k.front().getLevel();
     });
 }
 
-int ref_ctx_key(void* h, int kind, int64_t rot, uint64_t* flat) {
+// Words of one part's a (or b) polynomial of a key (kind 3 keys are compact).
+int ref_ctx_key_words(void* h, int kind, int64_t rot, size_t* words) {
     return guarded([&] {
-        const auto& c = static_cast<RefCtx*>(h)->ctx;
-        std::span<const CKKSCiphertext> k =
-            kind == 0 ? c.getRotationKey(rot)
-                      : (kind == 1 ? c.getConjugationKey() : c.getRelinHybrid(c.getParams().getMaxLevel()));
-        keys_to_flat(k, flat);
+        std::span<const CKKSCiphertext> k = key_span(static_cast<RefCtx*>(h)->ctx, kind, rot);
+        *words = k.empty() ? 0 : k.front().getA().size();
     });
+}
+
+int ref_ctx_key(void* h, int kind, int64_t rot, uint64_t* flat) {
+    return guarded([&] { keys_to_flat(key_span(static_cast<RefCtx*>(h)->ctx, kind, rot), flat); });
 }
 
 // NTT-domain automorphism map (dst -> src) used by rotation (kind 0) or conjugation (kind 1).
@@ -409,6 +424,65 @@ void* ref_walsh15_plans_create(void) {
         out = new RefCtx(CKKSParams(std::move(cfg)));
     });
     return rc == 0 ? out : nullptr;
+}
+
+// The same chain with bootstrapping keys (dense-to-sparse, sparse-to-dense, EvalMod
+// polynomial).  The EvalMod fit comes from the stand-in in ref_evalmod_stub.cpp, so the
+// polynomial is not the reference's MPFR fit; nothing built from this context is compared
+// on EvalMod coefficients other than those it reports itself.
+void* ref_walsh15_bts_create(void) {
+    RefCtx* out = nullptr;
+    const int rc = guarded([&] {
+        CKKSParamsConfig cfg = ckks_aes_params_detail::AESWalsh15Config();
+        cfg.secure = false;
+        cfg.bts_keys = true;
+        cfg.s2c_ptxt = true;
+        cfg.c2s_ptxt = true;
+        cfg.aes_walsh_params.enabled = false;
+        cfg.q_mult_bits.clear();
+        cfg.q_bits = {36, 61, 42, 42, 38, 38, 38, 38, 38, 38, 38, 50, 50};
+        cfg.mult_depth = 9;
+        out = new RefCtx(CKKSParams(std::move(cfg)));
+    });
+    return rc == 0 ? out : nullptr;
+}
+
+// ckks_modraise_inplace (src/ckks/operations/bootstrap/ckks_modraise.cpp:103) on a level-0
+// sparse-secret ciphertext: limb 0 of b and a in, target_level+1 limbs out (in place).
+int ref_modraise(void* h, size_t target_level, uint64_t* b, uint64_t* a) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        CKKSCiphertext ct(N, copy_in(a, N), copy_in(b, N), 1.0L, 0, CKKSSecretOwner::BootstrapSparse);
+        ckks_modraise_inplace(c, ct, target_level);
+        copy_out(ct.getB(), b);
+        copy_out(ct.getA(), a);
+    });
+}
+
+// ckks_key_switch_dense_to_sparse_inplace (ckks_keyswitch.cpp:1844) on a level-0 ciphertext.
+int ref_dense_to_sparse(void* h, uint64_t* b, uint64_t* a) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        CKKSCiphertext ct(N, copy_in(a, N), copy_in(b, N), 1.0L, 0, CKKSSecretOwner::Dense);
+        ckks_key_switch_dense_to_sparse_inplace(c, ct);
+        copy_out(ct.getB(), b);
+        copy_out(ct.getA(), a);
+    });
+}
+
+// ckks_key_switch_sparse_to_dense_inplace (ckks_keyswitch.cpp:1858) at `level`.
+int ref_sparse_to_dense(void* h, size_t level, uint64_t* b, uint64_t* a) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t n = (level + 1) * c.getParams().getN();
+        CKKSCiphertext ct(c.getParams().getN(), copy_in(a, n), copy_in(b, n), 1.0L, level,
+                          CKKSSecretOwner::BootstrapSparse);
+        ckks_key_switch_sparse_to_dense_inplace(c, ct);
+        copy_out(ct.getB(), b);
+        copy_out(ct.getA(), a);
+    });
 }
 
 static const CKKSLinearTransformPlan& plan_of(void* h, int which) {

@@ -7,6 +7,7 @@
 // __syncthreads().  Not part of the product library.
 #include <cstring>
 #include <utility>
+#include <stdexcept>
 #include <vector>
 
 #include "wg_keyswitch.cuh"
@@ -88,7 +89,8 @@ void ntt_one(const Emu& E, uint64_t* x, int mi, bool fwd) {
         case 13: ntt_limb<13>(E, x, mi, fwd); break;
         case 14: ntt_limb<14>(E, x, mi, fwd); break;
         case 15: ntt_limb<15>(E, x, mi, fwd); break;
-        default: break;
+        case 16: ntt_limb<16>(E, x, mi, fwd); break;
+        default: throw std::invalid_argument("emu: unsupported ring degree");
     }
 }
 

@@ -72,3 +72,22 @@ def test_emulated_kernels_match_oracle(oracle_mod, emu, prm):
             assert (e0 == r0).all() and (e1 == r1).all()
     finally:
         emu.emu_destroy(h)
+
+
+@pytest.mark.parametrize("logN", [13, 14, 15, 16])
+def test_emulated_ntt_large_rings(oracle_mod, emu, logN):
+    """Round plans of the larger rings (column / row phases of 6..8 bits)."""
+    O = oracle_mod
+    N = 1 << logN
+    p, q = O.find_primes([61], [36, 61], N)
+    o = O.OracleCtx(N, q, p, 1)
+    h = emu.emu_create(N, q, len(q), p, len(p), 1)
+    try:
+        x = o.uniform(len(q), 17)
+        y = x.copy()
+        emu.emu_ntt(h, y, len(q), 0, 0, 0)
+        assert (y == o.ntt(x)).all()
+        emu.emu_ntt(h, y, len(q), 0, 0, 1)
+        assert (y == x).all()
+    finally:
+        emu.emu_destroy(h)
