@@ -76,6 +76,13 @@ void lt_stage_destroy(LtStage* st);
 void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const* b, uint64_t* const* a,
                     cudaStream_t s);
 
+// Bootstrapping boundary steps (wg_boot.cu): ModRaise of level-0 ciphertexts to target_level,
+// and the level-0 dense-to-sparse switch through q0 and p0 with the compact key.
+void modraise(Context& c, size_t count, size_t target_level, uint64_t* const* b, uint64_t* const* a,
+              cudaStream_t s);
+void q0p0_switch(Context& c, size_t count, uint64_t* const* b, uint64_t* const* a, const KeyEntry& key,
+                 cudaStream_t s);
+
 // Hoisted rotations of one ciphertext; out [rotation][b, a][level+1][N] (wg_bsgs.cu).
 void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rots, size_t nrot,
                  uint64_t* out, cudaStream_t s);

@@ -131,13 +131,16 @@ int wg_ctx_set_key(wg_context* ctx, int kind, int64_t rotation, const uint64_t* 
     return guard([&] {
         wg::Context& c = C(ctx);
         check_ptr(host_key, "wg_ctx_set_key");
-        if (kind != WG_KEY_RELIN && kind != WG_KEY_CONJ && kind != WG_KEY_ROTATION)
-            wg::fail(wg::kInvalid, "wg_ctx_set_key: unknown key kind");
+        if (kind < WG_KEY_RELIN || kind > WG_KEY_SPARSE_TO_DENSE) wg::fail(wg::kInvalid, "wg_ctx_set_key: unknown key kind");
         if (key_level >= c.nq) wg::fail(wg::kInvalid, "wg_ctx_set_key: key level out of range");
-        if (parts < c.parts_at(key_level) || parts > 16) wg::fail(wg::kInvalid, "wg_ctx_set_key: invalid part count");
+        const bool compact = kind == WG_KEY_DENSE_TO_SPARSE;
+        if (compact && (parts != 1 || key_level != 0))
+            wg::fail(wg::kInvalid, "wg_ctx_set_key: the dense-to-sparse key is one level-0 part");
+        if (!compact && (parts < c.parts_at(key_level) || parts > 16))
+            wg::fail(wg::kInvalid, "wg_ctx_set_key: invalid part count");
         const int64_t r = kind == WG_KEY_ROTATION ? normalize_rotation(c, rotation) : 0;
         if (kind == WG_KEY_ROTATION && r == 0) wg::fail(wg::kInvalid, "wg_ctx_set_key: zero rotation needs no key");
-        const size_t words = parts * 2 * (key_level + 1 + c.np) * c.N;
+        const size_t words = compact ? 4 * c.N : parts * 2 * (key_level + 1 + c.np) * c.N;
         wg::KeyEntry e;
         e.parts = parts;
         e.key_level = key_level;
@@ -336,6 +339,60 @@ int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_
         }
         wg::batch_mul_relin_rescale_rotate(c, count, levels, xb, xa, yb, ya, rots, galois.data(),
                                            &c.key(WG_KEY_RELIN, 0), keys.data(), S(stream));
+    });
+}
+
+static void check_cts(wg::Context& c, size_t count, uint64_t* const* b, uint64_t* const* a, const char* who) {
+    if (count && (!b || !a)) wg::fail(wg::kInvalid, std::string(who) + ": null array");
+    for (size_t i = 0; i < count; ++i) {
+        check_ptr(b[i], who);
+        check_ptr(a[i], who);
+    }
+}
+
+int wg_modraise(wg_context* ctx, size_t count, size_t target_level, uint64_t* const* b, uint64_t* const* a,
+                void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        if (target_level == 0 || target_level >= c.nq)
+            wg::fail(wg::kInvalid, "ckks_modraise: target level must be in [1, max_level]");
+        check_cts(c, count, b, a, "ckks_modraise");
+        wg::modraise(c, count, target_level, b, a, S(stream));
+    });
+}
+
+int wg_dense_to_sparse(wg_context* ctx, size_t count, uint64_t* const* b, uint64_t* const* a, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_cts(c, count, b, a, "ckks_key_switch");
+        const wg::KeyEntry& k = c.key(WG_KEY_DENSE_TO_SPARSE, 0);
+        wg::q0p0_switch(c, count, b, a, k, S(stream));
+    });
+}
+
+int wg_sparse_to_dense(wg_context* ctx, size_t count, const size_t* levels, uint64_t* const* b,
+                       uint64_t* const* a, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_cts(c, count, b, a, "ckks_key_switch");
+        if (count && !levels) wg::fail(wg::kInvalid, "ckks_key_switch: null levels");
+        const wg::KeyEntry& k = c.key(WG_KEY_SPARSE_TO_DENSE, 0);
+        std::vector<wg::KsItem> items(count);
+        for (size_t i = 0; i < count; ++i) {
+            check_level(c, levels[i], "ckks_key_switch");
+            wg::KsItem& it = items[i];
+            it.level = levels[i];
+            it.key_term = a[i];
+            it.key = &k;
+            it.b_in = b[i];
+            it.a_in = a[i];
+            it.b = b[i];
+            it.a = a[i];
+            it.b_add = 1;
+            it.a_add = 0;
+            it.galois = 0;
+        }
+        wg::batch_keyswitch(c, items.data(), count, S(stream));
     });
 }
 

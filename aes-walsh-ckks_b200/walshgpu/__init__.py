@@ -22,6 +22,8 @@ LIB_PATH = os.path.join(PKG, "libwalshgpu.so")
 WG_KEY_RELIN = 0
 WG_KEY_CONJ = 1
 WG_KEY_ROTATION = 2
+WG_KEY_DENSE_TO_SPARSE = 3
+WG_KEY_SPARSE_TO_DENSE = 4
 
 
 class WalshGpuError(RuntimeError):
@@ -78,6 +80,9 @@ def lib() -> C.CDLL:
         L.wg_sub.argtypes = [vp, sz, vp, vp, sz, sz, vp]
         L.wg_batch_mul_relin_rescale_rotate.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp]
         L.wg_sequence_mul_relin_rescale_rotate.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp]
+        L.wg_modraise.argtypes = [vp, sz, sz, vp, vp, vp]
+        L.wg_dense_to_sparse.argtypes = [vp, sz, vp, vp, vp]
+        L.wg_sparse_to_dense.argtypes = [vp, sz, vp, vp, vp, vp]
         L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_batch_plan_launch.argtypes = [vp, vp]
         L.wg_batch_plan_destroy.argtypes = [vp]
@@ -279,10 +284,12 @@ class Context:
         return min(self.dnum, (level + self.alpha) // self.alpha)
 
     def set_key(self, kind, key, rotation=0, parts=None, key_level=None):
+        if kind == WG_KEY_DENSE_TO_SPARSE:  # compact q0/p0 key: one level-0 part
+            key_level, parts = 0, 1
         kl = self.nq - 1 if key_level is None else key_level
         parts = self.parts(kl) if parts is None else parts
         k = _u64(key)
-        expect = parts * 2 * (kl + 1 + self.np_) * self.N
+        expect = 4 * self.N if kind == WG_KEY_DENSE_TO_SPARSE else parts * 2 * (kl + 1 + self.np_) * self.N
         if k.size != expect:
             raise ValueError(f"key has {k.size} words, expected {expect}")
         _check(lib().wg_ctx_set_key(self.h, kind, int(rotation), k.ctypes.data, parts, kl))
@@ -319,6 +326,27 @@ class Context:
         r = np.ascontiguousarray(rotations, dtype=np.int64)
         _check(lib().wg_rotate_many(self.h, level, _ptr(b), _ptr(a), r.ctypes.data, len(r), _ptr(out),
                                     _stream(stream)))
+
+    def modraise(self, target_level, bs, as_, stream=None):
+        """Raise level-0 ciphertexts (lists of device tensors holding target_level+1 limbs,
+        limb 0 = q0 input) to target_level, in place."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        pb, pa = arr(bs), arr(as_)
+        _check(lib().wg_modraise(self.h, len(pb), target_level, pb.ctypes.data, pa.ctypes.data, _stream(stream)))
+
+    def dense_to_sparse(self, bs, as_, stream=None):
+        """Level-0 dense-to-sparse switch (q0/p0 key), in place."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        pb, pa = arr(bs), arr(as_)
+        _check(lib().wg_dense_to_sparse(self.h, len(pb), pb.ctypes.data, pa.ctypes.data, _stream(stream)))
+
+    def sparse_to_dense(self, levels, bs, as_, stream=None):
+        """Sparse-to-dense hybrid switch of ciphertext i at levels[i], in place."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        pb, pa = arr(bs), arr(as_)
+        lv = np.ascontiguousarray(levels, dtype=np.uintp)
+        _check(lib().wg_sparse_to_dense(self.h, len(pb), lv.ctypes.data, pb.ctypes.data, pa.ctypes.data,
+                                        _stream(stream)))
 
     def mul(self, level, b1, a1, b2, a2, c2, stream=None):
         _check(lib().wg_mul(self.h, level, _ptr(b1), _ptr(a1), _ptr(b2), _ptr(a2), _ptr(c2), _stream(stream)))

@@ -41,6 +41,12 @@ extern "C" {
 #define WG_KEY_RELIN 0       /* s^2 -> s           (relinearization_key_generation.cpp:130-199) */
 #define WG_KEY_CONJ 1        /* conj(s) -> s       (conjugation_key_generation.cpp:63-167) */
 #define WG_KEY_ROTATION 2    /* s -> pi^-1(s)      (rotation_key_generation.cpp:92-199) */
+/* dense s -> sparse s' at q0 * p0 only: compact key, one level-0 part whose a and b hold the
+ * q0 limb then the p0 limb (2 x 2 x N words; parts = 1, key_level = 0).
+ * generate_secret_key_switch_key_q0p0_hybrid, ckks_context.cpp:453. */
+#define WG_KEY_DENSE_TO_SPARSE 3
+/* sparse s' -> dense s, hybrid key (generate_secret_key_switch_key_hybrid, ckks_context.cpp:458) */
+#define WG_KEY_SPARSE_TO_DENSE 4
 
 typedef struct wg_context wg_context;
 
@@ -141,6 +147,24 @@ int wg_batch_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const size_
                                       uint64_t* const* xb, uint64_t* const* xa,
                                       const uint64_t* const* yb, const uint64_t* const* ya,
                                       const int64_t* rots, void* stream);
+
+/* Bootstrapping boundary steps, batched over `count` ciphertexts (host arrays of device
+ * pointers).
+ * ModRaise: limb 0 (q0, evaluation form) of each b[i] / a[i] is lifted to target_level+1 limbs
+ * in place (centered lift, then NTT); buffers hold (target_level+1)*N words.  Replaces
+ * ckks_modraise_inplace, src/ckks/operations/bootstrap/ckks_modraise.cpp:103-110 (the caller
+ * tracks the secret owner, which the reference checks).
+ * Dense-to-sparse: level-0 key switch through q0 and p0 only with the WG_KEY_DENSE_TO_SPARSE
+ * key (folded, Montgomery).  Replaces ckks_key_switch_dense_to_sparse_inplace /
+ * ckks_q0p0_key_switch_level0_inplace, src/ckks/operations/keyswitch/ckks_keyswitch.cpp:1661-1856.
+ * Sparse-to-dense: hybrid key switch of ciphertext i at levels[i] with the
+ * WG_KEY_SPARSE_TO_DENSE key.  Replaces ckks_key_switch_sparse_to_dense_inplace,
+ * ckks_keyswitch.cpp:1858-1869. */
+int wg_modraise(wg_context* ctx, size_t count, size_t target_level, uint64_t* const* b, uint64_t* const* a,
+                void* stream);
+int wg_dense_to_sparse(wg_context* ctx, size_t count, uint64_t* const* b, uint64_t* const* a, void* stream);
+int wg_sparse_to_dense(wg_context* ctx, size_t count, const size_t* levels, uint64_t* const* b,
+                       uint64_t* const* a, void* stream);
 
 /* The same batched pipeline planned once for fixed buffers and captured as a CUDA graph
  * (no counterpart in the reference, which plans nothing ahead).  Create takes the arguments

@@ -1278,3 +1278,97 @@ int orc_lt_stage(const orc_ctx* c, size_t level, size_t nterms, const uint64_t* 
     free(sw_b);
     return rc;
 }
+
+/* ------------------------------------------------------------------------------------------
+ * Bootstrapping boundary steps
+ * ------------------------------------------------------------------------------------------ */
+
+/* center_lift_mod_q / signed_to_mod_q (src/ckks/operations/bootstrap/ckks_modraise.cpp:12-29). */
+static int64_t center_lift(uint64_t v, uint64_t q) {
+    const uint64_t half = q >> 1;
+    return v > half ? -(int64_t)(q - v) : (int64_t)v;
+}
+static uint64_t signed_mod(int64_t v, uint64_t q) {
+    if (v >= 0) return (uint64_t)v % q;
+    const uint64_t m = (uint64_t)(-v) % q;
+    return m == 0 ? 0 : q - m;
+}
+
+/* ckks_modraise_inplace / modraise_eval_poly_from_q0 (ckks_modraise.cpp:31-110): the q0 limb
+ * of b and a (limb 0 of each buffer) is lifted to target_level+1 limbs, in place. */
+int orc_modraise(const orc_ctx* c, size_t target_level, uint64_t* b, uint64_t* a) {
+    const uint64_t N = c->N;
+    if (target_level == 0 || target_level >= c->nq) return -1;
+    uint64_t* coeff = malloc(N * 8);
+    uint64_t* polys[2] = {b, a};
+    for (int k = 0; k < 2; ++k) {
+        uint64_t* x = polys[k];
+        memcpy(coeff, x, N * 8);
+        inv_limb(&c->qm[0], coeff, N, 0);
+        for (size_t l = 0; l <= target_level; ++l) {
+            const uint64_t q = c->qm[l].q;
+            for (uint64_t i = 0; i < N; ++i) x[l * N + i] = signed_mod(center_lift(coeff[i], c->qm[0].q), q);
+        }
+        for (size_t l = 0; l <= target_level; ++l) fwd_limb(&c->qm[l], x + l * N, N, 0);
+    }
+    free(coeff);
+    return 0;
+}
+
+/* hps_base_change_single_limb (src/ckks/operations/keyswitch/ckks_keyswitch.cpp:1645-1659). */
+static uint64_t base_change_single(uint64_t v, uint64_t src, const modulus_t* dst) {
+    const uint64_t reduced = red4q(v, src);
+    const uint64_t r = barrett_u64(reduced, dst->q, dst->mu_hi);
+    const uint64_t s = barrett_u64(src, dst->q, dst->mu_hi);
+    return reduced >= (src >> 1) + 1 ? sub_mod(r, s, dst->q) : r;
+}
+
+/* ckks_q0p0_key_switch_level0_inplace (ckks_keyswitch.cpp:1661-1816), folded Montgomery key
+ * (the reference defaults): key = [a: q0 limb, p0 limb][b: q0 limb, p0 limb].  Level-0
+ * (b, a) updated in place. */
+int orc_q0p0_switch(const orc_ctx* c, const uint64_t* key, uint64_t* b, uint64_t* a) {
+    const uint64_t N = c->N;
+    const modulus_t* q0 = &c->qm[0];
+    const modulus_t* p0 = &c->pm[0];
+    uint64_t* dc = malloc(N * 8);
+    uint64_t* dp = malloc(N * 8);
+    uint64_t* acc = calloc(4 * N, 8); /* a_q0, a_p0, b_q0, b_p0 */
+    memcpy(dc, a, N * 8);
+    inv_limb(q0, dc, N, 1);
+    for (uint64_t i = 0; i < N; ++i) dp[i] = base_change_single(dc[i], q0->q, p0);
+    fwd_limb(p0, dp, N, 1);
+    for (uint64_t i = 0; i < N; ++i) {
+        acc[i] = add_mod(0, mont_mul(a[i], key[i], q0->q, q0->qninv), q0->q);
+        acc[2 * N + i] = add_mod(0, mont_mul(a[i], key[2 * N + i], q0->q, q0->qninv), q0->q);
+        acc[N + i] = add_mod(0, mont_mul(dp[i], key[N + i], p0->q, p0->qninv), p0->q);
+        acc[3 * N + i] = add_mod(0, mont_mul(dp[i], key[3 * N + i], p0->q, p0->qninv), p0->q);
+    }
+    inv_limb(p0, acc + N, N, 1);
+    inv_limb(p0, acc + 3 * N, N, 1);
+    /* ckks_apply_folded_approx_crt_moddown_pair_eval_q with P = {p0}, Q = {q0}, inverse p0^-1 */
+    const uint64_t inv = mod_inverse(p0->q % q0->q, q0->q);
+    const uint64_t inv_s = orc_shoup_const(inv, q0->q);
+    const double p_inv = 1.0 / (double)p0->q;
+    for (int poly = 0; poly < 2; ++poly) {
+        const uint64_t* src = acc + (2 * poly + 1) * N;
+        uint64_t* dst = acc + 2 * poly * N;
+        for (uint64_t i = 0; i < N; ++i) {
+            const uint64_t s = red4q(src[i], p0->q);
+            const double alpha = fma((double)s, p_inv, 0.0);
+            const uint64_t term = mul_shoup(barrett_u64(s, q0->q, q0->mu_hi), inv, inv_s, q0->q);
+            uint64_t hps = (uint64_t)(alpha + 0.5);
+            if (hps > 1) hps = 1;
+            dc[i] = sub_mod(add_mod(0, term, q0->q), hps, q0->q);
+        }
+        fwd_limb(q0, dc, N, 0);
+        for (uint64_t i = 0; i < N; ++i) dst[i] = sub_mod(dst[i], dc[i], q0->q);
+    }
+    for (uint64_t i = 0; i < N; ++i) {
+        b[i] = add_mod(b[i], acc[2 * N + i], q0->q);
+        a[i] = acc[i];
+    }
+    free(dc);
+    free(dp);
+    free(acc);
+    return 0;
+}

@@ -76,6 +76,14 @@ int orc_lt_stage(const orc_ctx* c, size_t level, size_t nterms, const uint64_t* 
                  size_t baby, size_t slots, int rescale, const uint64_t* const* keys, const int64_t* key_rots,
                  size_t nkeys, size_t key_level, uint64_t* b, uint64_t* a);
 
+/* --- bootstrapping boundary steps --- */
+/* ModRaise (reference ckks_modraise_inplace): limb 0 of b and a lifted to target_level+1 limbs
+ * in place (buffers hold (target_level+1)*N words). */
+int orc_modraise(const orc_ctx* c, size_t target_level, uint64_t* b, uint64_t* a);
+/* Level-0 dense-to-sparse switch through q0 and p0 only (reference
+ * ckks_q0p0_key_switch_level0_inplace); key [a: q0, p0][b: q0, p0] x N, folded Montgomery. */
+int orc_q0p0_switch(const orc_ctx* c, const uint64_t* key, uint64_t* b, uint64_t* a);
+
 /* --- seeded key material and encryption (test data generation) --- */
 void orc_sample_ternary(uint64_t N, size_t hamming_weight, uint64_t seed, int8_t* out);
 /* Switch key from secret `src` (squared when src_square, for relinearization) to secret

@@ -75,6 +75,8 @@ def lib() -> C.CDLL:
                                    C.c_void_p, i64p, C.c_size_t, C.c_size_t, u64p, u64p]
         L.orc_batched_ops.argtypes = [C.c_void_p, C.c_size_t, szp, u64p, u64p, u64p, u64p, u64p,
                                       C.c_void_p, i64p, C.c_size_t, C.c_size_t, C.c_int]
+        L.orc_modraise.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
+        L.orc_q0p0_switch.argtypes = [C.c_void_p, u64p, u64p, u64p]
         _lib = L
     return _lib
 
@@ -228,6 +230,23 @@ class OracleCtx:
         b = np.ascontiguousarray(b, dtype=np.uint64).copy()
         a = np.ascontiguousarray(a, dtype=np.uint64).copy()
         _check(lib().orc_rotate(self.h, level, b, a, np.ascontiguousarray(key), kl, rotation), "orc_rotate")
+        return b, a
+
+    def modraise(self, target_level, b, a):
+        """Limb 0 of (b, a) raised to target_level+1 limbs (ModRaise)."""
+        n = (target_level + 1) * self.N
+        bo = np.zeros(n, np.uint64)
+        ao = np.zeros(n, np.uint64)
+        bo[: self.N] = np.asarray(b, dtype=np.uint64)[: self.N]
+        ao[: self.N] = np.asarray(a, dtype=np.uint64)[: self.N]
+        _check(lib().orc_modraise(self.h, target_level, bo, ao), "orc_modraise")
+        return bo, ao
+
+    def q0p0_switch(self, key, b, a):
+        """Level-0 dense-to-sparse switch with the compact q0/p0 key."""
+        b = np.ascontiguousarray(b[: self.N], dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a[: self.N], dtype=np.uint64).copy()
+        _check(lib().orc_q0p0_switch(self.h, np.ascontiguousarray(key, dtype=np.uint64), b, a), "orc_q0p0_switch")
         return b, a
 
     def conjugate(self, level, b, a, key, key_level=None):
@@ -401,9 +420,14 @@ class RefCtx:
 class RefPlans:
     """The reference's walsh15 S2C / C2S plans and rotation keys (ref_walsh15_plans_create)."""
 
-    def __init__(self):
+    def __init__(self, bootstrap_keys=False):
         R = ref()
         R.ref_walsh15_plans_create.restype = C.c_void_p
+        R.ref_walsh15_bts_create.restype = C.c_void_p
+        R.ref_ctx_key_words.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.POINTER(C.c_size_t)]
+        R.ref_modraise.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
+        R.ref_dense_to_sparse.argtypes = [C.c_void_p, u64p, u64p]
+        R.ref_sparse_to_dense.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
         R.ref_plan_stage_count.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
         R.ref_plan_stage_info.argtypes = [C.c_void_p, C.c_int, C.c_size_t] + [C.POINTER(C.c_size_t)] * 2 + \
             [C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]
@@ -411,9 +435,9 @@ class RefPlans:
         R.ref_lt_stage.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, u64p, u64p, u64p, u64p,
                                    C.POINTER(C.c_size_t)]
         R.ref_ctx_rotations.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_size_t)]
-        self.h = R.ref_walsh15_plans_create()
+        self.h = R.ref_walsh15_bts_create() if bootstrap_keys else R.ref_walsh15_plans_create()
         if not self.h:
-            raise RuntimeError("ref_walsh15_plans_create: " + R.ref_last_error().decode())
+            raise RuntimeError("ref_walsh15 context: " + R.ref_last_error().decode())
         nq, np_ = C.c_size_t(), C.c_size_t()
         _check(R.ref_ctx_moduli(self.h, np.zeros(64, np.uint64), C.byref(nq), np.zeros(64, np.uint64), C.byref(np_)),
                "ref_ctx_moduli")
@@ -461,9 +485,35 @@ class RefPlans:
         _check(ref().ref_ctx_rotations(self.h, out.ctypes.data, C.byref(n)), "ref_ctx_rotations")
         return out
 
-    def key(self, rot):
-        parts, kl = C.c_size_t(), C.c_size_t()
-        _check(ref().ref_ctx_key_shape(self.h, 0, rot, C.byref(parts), C.byref(kl)), "ref_ctx_key_shape")
-        out = np.zeros(parts.value * 2 * (kl.value + 1 + len(self.p)) * self.N, np.uint64)
-        _check(ref().ref_ctx_key(self.h, 0, rot, out), "ref_ctx_key")
+    def key(self, rot, kind=0):
+        """Switching key as stored: (flat [part][a|b][limbs][N], parts, key level).  kind 0
+        rotation, 1 conjugation, 2 relinearization, 3 dense-to-sparse (compact q0/p0 key),
+        4 sparse-to-dense."""
+        parts, kl, words = C.c_size_t(), C.c_size_t(), C.c_size_t()
+        _check(ref().ref_ctx_key_shape(self.h, kind, rot, C.byref(parts), C.byref(kl)), "ref_ctx_key_shape")
+        _check(ref().ref_ctx_key_words(self.h, kind, rot, C.byref(words)), "ref_ctx_key_words")
+        out = np.zeros(parts.value * 2 * words.value, np.uint64)
+        _check(ref().ref_ctx_key(self.h, kind, rot, out), "ref_ctx_key")
         return out, parts.value, kl.value
+
+    def modraise(self, target_level, b, a):
+        n = (target_level + 1) * self.N
+        bo = np.zeros(n, np.uint64)
+        ao = np.zeros(n, np.uint64)
+        bo[: self.N] = np.asarray(b, dtype=np.uint64)[: self.N]
+        ao[: self.N] = np.asarray(a, dtype=np.uint64)[: self.N]
+        _check(ref().ref_modraise(self.h, target_level, bo, ao), "ref_modraise")
+        return bo, ao
+
+    def dense_to_sparse(self, b, a):
+        b = np.ascontiguousarray(b[: self.N], dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a[: self.N], dtype=np.uint64).copy()
+        _check(ref().ref_dense_to_sparse(self.h, b, a), "ref_dense_to_sparse")
+        return b, a
+
+    def sparse_to_dense(self, level, b, a):
+        n = (level + 1) * self.N
+        b = np.ascontiguousarray(b[:n], dtype=np.uint64).copy()
+        a = np.ascontiguousarray(a[:n], dtype=np.uint64).copy()
+        _check(ref().ref_sparse_to_dense(self.h, level, b, a), "ref_sparse_to_dense")
+        return b, a

@@ -441,7 +441,7 @@ void* ref_walsh15_bts_create(void) {
         cfg.aes_walsh_params.enabled = false;
         cfg.q_mult_bits.clear();
         cfg.q_bits = {36, 61, 42, 42, 38, 38, 38, 38, 38, 38, 38, 50, 50};
-        cfg.mult_depth = 9;
+        cfg.mult_depth = 2;  // the EvalMod, S2C and C2S levels are the bootstrap depths here
         out = new RefCtx(CKKSParams(std::move(cfg)));
     });
     return rc == 0 ? out : nullptr;

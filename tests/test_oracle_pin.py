@@ -149,3 +149,30 @@ def test_bsgs_stages_match_reference(ref_mod):
         ob, oa = o.lt_stage(level, info["indices"], info["diagonals"], info["baby"], info["slot_count"],
                             info["rescale"], keys, b, a)
         assert (rb == ob).all() and (ra == oa).all(), (which, stage)
+
+
+def test_bootstrap_boundary_steps_match_reference(oracle_mod, ref_mod):
+    """ModRaise, the q0/p0 dense-to-sparse switch and the sparse-to-dense switch of the oracle
+    against the reference's walsh15 bootstrapping context (its own keys)."""
+    R = ref_mod.RefPlans(bootstrap_keys=True)
+    N = R.N
+    o = oracle_mod.OracleCtx(N, R.q, R.p, R.dnum)
+    rng = np.random.default_rng(1)
+    b = (rng.integers(0, 1 << 62, N, dtype=np.uint64) % R.q[0]).astype(np.uint64)
+    a = (rng.integers(0, 1 << 62, N, dtype=np.uint64) % R.q[0]).astype(np.uint64)
+    for tl in (12, 1):
+        rb, ra = R.modraise(tl, b, a)
+        ob, oa = o.modraise(tl, b, a)
+        assert (rb == ob).all() and (ra == oa).all(), tl
+    k3, _, _ = R.key(0, kind=3)
+    rb, ra = R.dense_to_sparse(b, a)
+    ob, oa = o.q0p0_switch(k3, b, a)
+    assert (rb == ob).all() and (ra == oa).all()
+    k4, _, kl = R.key(0, kind=4)
+    lv = 5
+    qc = np.repeat(R.q[: lv + 1], N)
+    bb = (rng.integers(0, 1 << 62, (lv + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
+    aa = (rng.integers(0, 1 << 62, (lv + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
+    rb, ra = R.sparse_to_dense(lv, bb, aa)
+    ob, oa = o.keyswitch(lv, aa, k4, bb, aa, True, False, key_level=kl)
+    assert (rb == ob).all() and (ra == oa).all()
