@@ -83,6 +83,12 @@ void modraise(Context& c, size_t count, size_t target_level, uint64_t* const* b,
 void q0p0_switch(Context& c, size_t count, uint64_t* const* b, uint64_t* const* a, const KeyEntry& key,
                  cudaStream_t s);
 
+// Chebyshev evaluation (wg_evalpoly.cu) of `count` ciphertexts sharing level and scale.
+void evalchebyshev(Context& c, size_t count, size_t level, double scale, const double* coeffs, size_t ncoeffs,
+                   double target_scale, double default_scale, uint64_t* const* b, uint64_t* const* a,
+                   uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                   cudaStream_t s);
+
 // Hoisted rotations of one ciphertext; out [rotation][b, a][level+1][N] (wg_bsgs.cu).
 void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rots, size_t nrot,
                  uint64_t* out, cudaStream_t s);

@@ -1,6 +1,7 @@
 // C ABI (include/walsh_gpu.h): argument checks, key registry, workspace routing and the
 // operation sequences of rotation, conjugation, relinearization and the batched workload.
 #include <cstring>
+#include <stdexcept>
 #include <string>
 
 #include "../../include/walsh_gpu.h"
@@ -32,6 +33,9 @@ int guard(F&& f) {
     } catch (const wg::Error& e) {
         g_err = e.what();
         return e.code;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return WG_ERR_INVALID;
     } catch (const std::exception& e) {
         g_err = e.what();
         return WG_ERR_RUNTIME;
@@ -393,6 +397,22 @@ int wg_sparse_to_dense(wg_context* ctx, size_t count, const size_t* levels, uint
             it.galois = 0;
         }
         wg::batch_keyswitch(c, items.data(), count, S(stream));
+    });
+}
+
+int wg_evalchebyshev(wg_context* ctx, size_t count, size_t level, double scale, const double* coeffs,
+                     size_t ncoeffs, double target_scale, double default_scale, uint64_t* const* b,
+                     uint64_t* const* a, uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level,
+                     double* out_scale, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_cts(c, count, b, a, "ckks_evalchebyshev");
+        check_cts(c, count, out_b, out_a, "ckks_evalchebyshev");
+        check_ptr(coeffs, "ckks_evalchebyshev");
+        check_ptr(out_level, "ckks_evalchebyshev");
+        check_ptr(out_scale, "ckks_evalchebyshev");
+        wg::evalchebyshev(c, count, level, scale, coeffs, ncoeffs, target_scale, default_scale, b, a, out_b, out_a,
+                          out_level, out_scale, S(stream));
     });
 }
 

@@ -1,0 +1,766 @@
+// Chebyshev polynomial evaluation (the EvalMod / LUT polynomial step) over a batch of
+// ciphertexts that share level and scale: every homomorphic operation of the evaluation is one
+// set of batched launches for the whole batch.
+//
+// Reference: ckks_evalchebyshev_preconditioned, src/ckks/operations/evalpoly/ckks_evalpoly.cpp
+// (1221-1256), with its power basis (:834-938), scale-aware Paterson-Stockmeyer plan (:548-836,
+// the strategy of Bossuat et al., EUROCRYPT 2021, Section 3) and plan evaluation (:940-1219).
+// The residues the evaluation produces depend on the exact order of operations and on every
+// scalar it rounds, so the host side follows the reference's steps one for one: the same power
+// generation order, the same long-double scale bookkeeping (exact scales as seed powers over
+// moduli), the same constant rounding (round, then fmod by q, in long double), the same
+// baby-step / giant-step schedule.  The device side supplies the operations (tensor product,
+// relinearisation, rescale, scalar multiply / multiply-add / add, add, subtract).
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <limits>
+#include <map>
+#include <optional>
+#include <stdexcept>
+#include <utility>
+#include <vector>
+
+#include "../../include/walsh_gpu.h"
+#include "wg_batch.hpp"
+#include "wg_batch_kernels.cuh"
+#include "wg_internal.hpp"
+
+namespace wg {
+using namespace bk;
+
+namespace {
+
+// ------------------------------------------------------------------------------------------
+// Device side
+// ------------------------------------------------------------------------------------------
+enum ScalarOp : int { kScalarMul = 0, kScalarMulAdd = 1, kScalarAdd = 2 };
+
+struct ScalarJob {
+    uint64_t* x;
+    const uint64_t* y;
+    uint64_t s, s_shoup;
+    int mod, op;
+};
+
+// x = x * s, x = x + y * s or x = x + s (mod q), s < q; canonical in, canonical out.
+__global__ void __launch_bounds__(kT) kb_scalar(const ScalarJob* jobs, int n, const Modulus* mods) {
+    const ScalarJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const uint64_t q = mods[j->mod].q;
+    if (j->op == kScalarMul)
+        j->x[k] = mul_shoup(j->x[k], j->s, j->s_shoup, q);
+    else if (j->op == kScalarMulAdd)
+        j->x[k] = add_mod(j->x[k], mul_shoup(j->y[k], j->s, j->s_shoup, q), q);
+    else
+        j->x[k] = add_mod(j->x[k], j->s, q);
+}
+
+// A batch of ciphertexts with common metadata.  Polynomial k of ciphertext i lives at p[i][k]
+// with room for `cap` limbs; limbs [0, level] are live.
+struct CtBatch {
+    std::vector<std::array<uint64_t*, 3>> p;
+    int np = 2;
+    size_t level = 0;
+    size_t cap = 0;
+    long double scale = 0.0L;
+};
+
+class DeviceOps {
+public:
+    DeviceOps(Context& c, size_t count, cudaStream_t s) : c_(c), count_(count), s_(s) {}
+    ~DeviceOps() {
+        for (uint64_t* p : owned_) cudaFreeAsync(p, s_);
+    }
+    DeviceOps(const DeviceOps&) = delete;
+    DeviceOps& operator=(const DeviceOps&) = delete;
+
+    size_t count() const { return count_; }
+
+    CtBatch wrap(uint64_t* const* b, uint64_t* const* a, size_t level, long double scale) {
+        CtBatch x;
+        x.p.resize(count_);
+        for (size_t i = 0; i < count_; ++i) x.p[i] = {b[i], a[i], nullptr};
+        x.np = 2;
+        x.level = level;
+        x.cap = level + 1;
+        x.scale = scale;
+        return x;
+    }
+
+    CtBatch zeros(size_t level, long double scale) {
+        CtBatch x;
+        x.p.resize(count_);
+        for (size_t i = 0; i < count_; ++i) x.p[i] = {buffer(level + 1, true), buffer(level + 1, true), nullptr};
+        x.np = 2;
+        x.level = level;
+        x.cap = level + 1;
+        x.scale = scale;
+        return x;
+    }
+
+    CtBatch clone(const CtBatch& x) {
+        CtBatch y = x;
+        y.cap = x.level + 1;
+        for (size_t i = 0; i < count_; ++i)
+            for (int k = 0; k < x.np; ++k) {
+                y.p[i][k] = buffer(y.cap, false);
+                check_cuda(cudaMemcpyAsync(y.p[i][k], x.p[i][k], y.cap * c_.N * 8, cudaMemcpyDeviceToDevice, s_),
+                           "evalpoly copy");
+            }
+        return y;
+    }
+
+    void pad(CtBatch& x, int np) {
+        if (np < x.np) throw std::invalid_argument("ckks_evalchebyshev: cannot shrink ciphertext degree by padding");
+        while (x.np < np) {
+            for (size_t i = 0; i < count_; ++i) x.p[i][x.np] = buffer(x.cap, true);
+            ++x.np;
+        }
+    }
+
+    // (b, a) x (b', a') -> (b b', a b' + b a', a a'); y must not alias x.
+    void tensor(CtBatch& x, const CtBatch& y) {
+        const size_t N = c_.N;
+        pad(x, 3);
+        std::vector<TensorJob> jobs;
+        for (size_t i = 0; i < count_; ++i)
+            for (size_t l = 0; l <= x.level; ++l)
+                jobs.push_back({x.p[i][0] + l * N, x.p[i][1] + l * N, y.p[i][0] + l * N, y.p[i][1] + l * N,
+                                x.p[i][2] + l * N, (int)l, 0});
+        JobTable t;
+        const TensorJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 7.0, s_);
+        kb_tensor<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        check_cuda(cudaGetLastError(), "evalpoly tensor");
+    }
+
+    void relin(CtBatch& x) {
+        if (x.np != 3) return;
+        const KeyEntry& k = c_.key(WG_KEY_RELIN, 0);
+        std::vector<KsItem> items(count_);
+        for (size_t i = 0; i < count_; ++i) {
+            KsItem& it = items[i];
+            it.level = x.level;
+            it.key_term = x.p[i][2];
+            it.key = &k;
+            it.b_in = x.p[i][0];
+            it.a_in = x.p[i][1];
+            it.b = x.p[i][0];
+            it.a = x.p[i][1];
+            it.b_add = 1;
+            it.a_add = 1;
+            it.galois = 0;
+        }
+        batch_keyswitch(c_, items.data(), count_, s_);
+        x.np = 2;
+    }
+
+    // ckks_rescale on every polynomial; scale /= q_level.
+    void rescale(CtBatch& x) {
+        const size_t N = c_.N, lv = x.level;
+        if (lv == 0) throw std::invalid_argument("ckks_rescale: invalid level");
+        uint64_t* rem = scratch(count_ * x.np * lv);
+        const uint64_t* rc = c_.rs_host.data() + c_.rs_host_off[lv];
+        std::vector<NttJob> drop_intt, rem_ntt;
+        std::vector<RescalePrepJob> prep;
+        std::vector<RescaleFinishJob> fin;
+        uint64_t* r = rem;
+        for (size_t i = 0; i < count_; ++i)
+            for (int k = 0; k < x.np; ++k) {
+                uint64_t* poly = x.p[i][k];
+                uint64_t* drop = poly + lv * N;
+                drop_intt.push_back({drop, drop, (int)lv, 0});
+                for (size_t q = 0; q < lv; ++q) {
+                    prep.push_back({drop, r + q * N, rc[q], rc[3 * lv + q], (int)lv, (int)q});
+                    rem_ntt.push_back({r + q * N, r + q * N, (int)q, 0});
+                    fin.push_back({poly + q * N, r + q * N, rc[lv + q], rc[2 * lv + q], (int)q, 0});
+                }
+                r += lv * N;
+            }
+        JobTable t;
+        const NttJob* jd = t.add(drop_intt);
+        const RescalePrepJob* jp = t.add(prep);
+        const NttJob* jr = t.add(rem_ntt);
+        const RescaleFinishJob* jf = t.add(fin);
+        t.upload(c_, s_);
+        ntt_jobs(c_, t.at(jd), (int)drop_intt.size(), false, s_);
+        {
+            Probe probe(kClsElementwise, 8.0 * N * prep.size() * 2.0, s_);
+            kb_rescale_prep<<<grid_for(c_, prep.size()), kT, 0, s_>>>(t.at(jp), (int)prep.size(), c_.d_mod);
+        }
+        ntt_jobs(c_, t.at(jr), (int)rem_ntt.size(), true, s_);
+        {
+            Probe probe(kClsElementwise, 8.0 * N * fin.size() * 3.0, s_);
+            kb_rescale_finish<<<grid_for(c_, fin.size()), kT, 0, s_>>>(t.at(jf), (int)fin.size(), c_.d_mod);
+        }
+        check_cuda(cudaGetLastError(), "evalpoly rescale");
+        x.scale = x.scale / static_cast<long double>(c_.q[lv]);
+        x.level = lv - 1;
+    }
+
+    void add(CtBatch& x, const CtBatch& y, bool subtract) {
+        for (size_t i = 0; i < count_; ++i)
+            for (int k = 0; k < x.np; ++k) add_sub(c_, x.level, x.p[i][k], y.p[i][k], 1, 0, subtract, s_);
+    }
+
+    // op per limb: scalars[l] < q_l.  kScalarMul / kScalarMulAdd touch every polynomial,
+    // kScalarAdd the b polynomial only; zero scalars of a multiply-add are skipped.
+    void scalar(CtBatch& x, const CtBatch* y, const std::vector<uint64_t>& scalars, int op) {
+        const size_t N = c_.N;
+        std::vector<ScalarJob> jobs;
+        for (size_t l = 0; l <= x.level; ++l) {
+            const uint64_t q = c_.q[l], sv = scalars[l];
+            if (op == kScalarMulAdd && sv == 0) continue;
+            const uint64_t ss = host::shoup(sv, q);
+            for (size_t i = 0; i < count_; ++i) {
+                const int polys = op == kScalarAdd ? 1 : (op == kScalarMulAdd ? y->np : x.np);
+                for (int k = 0; k < polys; ++k)
+                    jobs.push_back({x.p[i][k] + l * N, y ? y->p[i][k] + l * N : nullptr, sv, ss, (int)l, op});
+            }
+        }
+        if (jobs.empty()) return;
+        JobTable t;
+        const ScalarJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 8.0 * N * jobs.size() * (op == kScalarMulAdd ? 3.0 : 2.0), s_);
+        kb_scalar<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        check_cuda(cudaGetLastError(), "evalpoly scalar");
+    }
+
+    void copy_out(const CtBatch& x, uint64_t* const* b, uint64_t* const* a) {
+        for (size_t i = 0; i < count_; ++i) {
+            if (x.p[i][0] != b[i])
+                check_cuda(cudaMemcpyAsync(b[i], x.p[i][0], (x.level + 1) * c_.N * 8, cudaMemcpyDeviceToDevice, s_),
+                           "evalpoly output");
+            if (x.p[i][1] != a[i])
+                check_cuda(cudaMemcpyAsync(a[i], x.p[i][1], (x.level + 1) * c_.N * 8, cudaMemcpyDeviceToDevice, s_),
+                           "evalpoly output");
+        }
+    }
+
+private:
+    uint64_t* buffer(size_t limbs, bool zero) {
+        uint64_t* p = nullptr;
+        const size_t bytes = std::max<size_t>(limbs, 1) * c_.N * 8;
+        if (cudaMallocAsync((void**)&p, bytes, s_) != cudaSuccess) {
+            cudaGetLastError();
+            fail(kNoMemory, "ckks_evalchebyshev: device allocation failed");
+        }
+        owned_.push_back(p);
+        if (zero) check_cuda(cudaMemsetAsync(p, 0, bytes, s_), "evalpoly zero");
+        return p;
+    }
+    uint64_t* scratch(size_t limbs) { return buffer(limbs, false); }
+
+    Context& c_;
+    size_t count_;
+    cudaStream_t s_;
+    std::vector<uint64_t*> owned_;
+};
+
+// ------------------------------------------------------------------------------------------
+// Host side: scalars, exact scales and the Paterson-Stockmeyer schedule
+// ------------------------------------------------------------------------------------------
+size_t bit_length(size_t v) { return v == 0 ? 0 : (size_t)(std::numeric_limits<size_t>::digits - __builtin_clzl(v)); }
+
+size_t ceil_log2(size_t degree) { return degree <= 1 ? 0 : bit_length(degree - 1); }
+
+size_t eval_depth(size_t degree) { return degree <= 1 ? 0 : bit_length(degree) - 1; }
+
+size_t split_log(size_t log_degree) {
+    size_t ls = log_degree >> 1;
+    const size_t a = (size_t{1} << ls) + (size_t{1} << (log_degree - ls)) + log_degree - ls - 3;
+    const size_t b = (size_t{1} << (ls + 1)) + (size_t{1} << (log_degree - ls - 1)) + log_degree - ls - 4;
+    if (a > b) ++ls;
+    return ls;
+}
+
+std::pair<size_t, size_t> split_degree(size_t degree) {
+    if (degree == 0) throw std::invalid_argument("ckks_evalchebyshev: cannot split degree zero");
+    if ((degree & (degree - 1)) == 0) return {degree >> 1, degree >> 1};
+    const size_t k = bit_length(degree - 1) - 1;
+    return {(size_t{1} << k) - 1, degree + 1 - (size_t{1} << k)};
+}
+
+// round(value * scale) mod q, in long double.
+uint64_t scaled_constant_mod(double value, long double scale, uint64_t q) {
+    const long double scaled = static_cast<long double>(value) * scale;
+    if (!std::isfinite(scaled)) throw std::invalid_argument("ckks_evalpoly: non-finite scaled constant");
+    long double residue = std::fmod(std::round(scaled), static_cast<long double>(q));
+    if (residue < 0.0L) residue += static_cast<long double>(q);
+    uint64_t out = static_cast<uint64_t>(residue);
+    if (out >= q) out %= q;
+    return out;
+}
+
+bool scales_close(double lhs, double rhs, double rel_tol = 0x1p-45) {
+    if (!std::isfinite(lhs) || !std::isfinite(rhs)) return false;
+    const long double l = lhs, r = rhs;
+    const long double m = std::max<long double>({1.0L, std::abs(l), std::abs(r)});
+    return std::abs(l - r) <= static_cast<long double>(rel_tol) * m;
+}
+
+bool is_integer(double v, double rel_tol = 0x1p-20) {
+    if (!std::isfinite(v)) return false;
+    return std::abs(v - std::round(v)) <= rel_tol * std::max(1.0, std::abs(v));
+}
+
+// A scale seed^seed_exp / prod q_i^den[i], kept exactly.
+struct ExactScale {
+    uint64_t seed = 1;
+    int seed_exp = 0;
+    std::vector<int> den;
+
+    static ExactScale of(double value, size_t nmod) {
+        if (!std::isfinite(value) || value < 0.0) throw std::invalid_argument("ckks_evalchebyshev: invalid exact scale seed");
+        const long double r = std::round(static_cast<long double>(value));
+        const long double tol = std::max<long double>(1.0L, std::abs(static_cast<long double>(value))) * 0x1p-20L;
+        if (std::abs(static_cast<long double>(value) - r) > tol)
+            throw std::invalid_argument("ckks_evalchebyshev: non-integral initial scale is unsupported");
+        if (r > static_cast<long double>(std::numeric_limits<uint64_t>::max()))
+            throw std::invalid_argument("ckks_evalchebyshev: initial scale exceeds uint64_t");
+        ExactScale e;
+        e.seed = static_cast<uint64_t>(r);
+        e.seed_exp = 1;
+        e.den.assign(nmod, 0);
+        return e;
+    }
+    long double value(const std::vector<uint64_t>& q) const {
+        long double v = 1.0L;
+        for (int i = 0; i < seed_exp; ++i) v *= static_cast<long double>(seed);
+        for (size_t i = 0; i < den.size(); ++i)
+            for (int e = 0; e < den[i]; ++e) v /= static_cast<long double>(q[i]);
+        return v;
+    }
+    double value_d(const std::vector<uint64_t>& q) const { return static_cast<double>(value(q)); }
+};
+
+ExactScale times(const ExactScale& x, const ExactScale& y) {
+    ExactScale o;
+    o.seed = x.seed;
+    o.seed_exp = x.seed_exp + y.seed_exp;
+    o.den = x.den;
+    if (o.den.size() < y.den.size()) o.den.resize(y.den.size(), 0);
+    for (size_t i = 0; i < y.den.size(); ++i) o.den[i] += y.den[i];
+    return o;
+}
+
+uint64_t ratio_u64(const ExactScale& num, const ExactScale& den, const std::vector<uint64_t>& q) {
+    if (num.seed != den.seed) throw std::invalid_argument("ckks_evalchebyshev: mixed exact-scale seeds are unsupported");
+    long double r = 1.0L;
+    const int d = num.seed_exp - den.seed_exp;
+    for (int i = 0; i < d; ++i) r *= static_cast<long double>(num.seed);
+    for (int i = 0; i < -std::min(d, 0); ++i) r /= static_cast<long double>(num.seed);
+    for (size_t i = 0; i < q.size(); ++i) {
+        const int ne = i < num.den.size() ? num.den[i] : 0;
+        const int de = i < den.den.size() ? den.den[i] : 0;
+        const int diff = de - ne;
+        for (int e = 0; e < diff; ++e) r *= static_cast<long double>(q[i]);
+        for (int e = 0; e < -diff; ++e) r /= static_cast<long double>(q[i]);
+    }
+    const long double f = std::floor(r);
+    if (!std::isfinite(f) || f < 0.0L || f > static_cast<long double>(std::numeric_limits<uint64_t>::max()))
+        throw std::runtime_error("ckks_evalchebyshev: exact-scale ratio exceeds uint64_t");
+    return static_cast<uint64_t>(f);
+}
+
+struct SimOperand {
+    size_t level = 0;
+    long double scale = 0.0L;
+};
+
+struct Poly {
+    std::vector<double> coeffs;
+    size_t max_degree = 0;
+    bool lead = true;
+    size_t level = 0;
+    long double scale = 0.0L;
+    bool even = false, odd = false;
+    size_t degree() const { return coeffs.empty() ? 0 : coeffs.size() - 1; }
+};
+
+// Scale / level simulation and the recursive plan (leaves in evaluation order).
+class Planner {
+public:
+    explicit Planner(const std::vector<uint64_t>& q) : q_(q) {}
+
+    void rescale(SimOperand& o) const {
+        o.scale /= static_cast<long double>(q_[o.level]);
+        --o.level;
+    }
+    SimOperand mul(const SimOperand& x, const SimOperand& y) const {
+        return SimOperand{std::min(x.level, y.level), x.scale * y.scale};
+    }
+    void powers(size_t n, std::map<size_t, SimOperand>& pb) const {
+        if (n < 2 || pb.count(n)) return;
+        const auto [a, b] = split_degree(n);
+        powers(a, pb);
+        powers(b, pb);
+        pb[n] = mul(pb.at(a), pb.at(b));
+        rescale(pb.at(n));
+    }
+
+    std::pair<std::vector<Poly>, SimOperand> plan(size_t log_split, size_t target_level, const Poly& poly,
+                                                  const std::map<size_t, SimOperand>& pb, long double out_scale) const {
+        const size_t degree = poly.degree();
+        const size_t base = size_t{1} << log_split;
+        if (degree < base) {
+            if (poly.lead && log_split > 1 &&
+                poly.max_degree > ((size_t{1} << bit_length(poly.max_degree)) - (size_t{1} << (log_split - 1))))
+                return plan(split_log(bit_length(degree)), target_level, poly, pb, out_scale);
+            Poly leaf = poly;
+            leaf.level = target_level;
+            leaf.scale = poly.lead ? out_scale * static_cast<long double>(q_[target_level]) : out_scale;
+            return {std::vector<Poly>{leaf}, SimOperand{leaf.level, leaf.scale}};
+        }
+        size_t next = base;
+        while (next < (degree >> 1) + 1) next <<= 1;
+        const SimOperand& xpow = pb.at(next);
+        const auto [quot, rem] = factorize(poly, next);
+        const uint64_t qi = poly.lead ? q_[target_level] : q_[target_level + 1];
+        const long double qscale = out_scale * static_cast<long double>(qi) / xpow.scale;
+        auto [qv, res] = plan(log_split, target_level + 1, quot, pb, qscale);
+        rescale(res);
+        res = mul(res, xpow);
+        auto [rv, tmp] = plan(log_split, target_level, rem, pb, res.scale);
+        if (!scales_close(static_cast<double>(res.scale), static_cast<double>(tmp.scale)))
+            throw std::runtime_error("ckks_evalchebyshev: simulated PS scale mismatch");
+        qv.insert(qv.end(), rv.begin(), rv.end());
+        return {std::move(qv), res};
+    }
+
+private:
+    static std::pair<Poly, Poly> factorize(const Poly& p, size_t split) {
+        const size_t degree = p.degree();
+        if (split < (degree >> 1)) throw std::invalid_argument("ckks_evalchebyshev: invalid recursive PS split");
+        Poly quot, rem;
+        quot.coeffs.assign(degree - split + 1, 0.0);
+        rem.coeffs.assign(split, 0.0);
+        for (size_t i = 0; i < split && i < p.coeffs.size(); ++i) rem.coeffs[i] = p.coeffs[i];
+        if (split < p.coeffs.size()) quot.coeffs[0] = p.coeffs[split];
+        for (size_t i = split + 1, j = 1; i <= degree; ++i, ++j) {
+            const double c = p.coeffs[i];
+            if (c == 0.0) continue;
+            quot.coeffs[i - split] += 2.0 * c;
+            rem.coeffs[split - j] -= c;
+        }
+        quot.max_degree = p.max_degree;
+        quot.lead = p.lead;
+        quot.even = p.even;
+        quot.odd = p.odd;
+        rem.max_degree = p.max_degree == degree ? (split == 0 ? 0 : split - 1) : p.max_degree - (degree - split + 1);
+        rem.lead = false;
+        rem.even = p.even;
+        rem.odd = p.odd;
+        return {std::move(quot), std::move(rem)};
+    }
+
+    const std::vector<uint64_t>& q_;
+};
+
+// ------------------------------------------------------------------------------------------
+// The evaluation
+// ------------------------------------------------------------------------------------------
+class ChebyshevEval {
+public:
+    ChebyshevEval(Context& c, DeviceOps& ops, long double default_scale)
+        : c_(c), ops_(ops), default_scale_(default_scale) {}
+
+    CtBatch run(const CtBatch& x, const std::vector<double>& coeffs, size_t degree, double target_scale) {
+        Poly poly;
+        poly.coeffs.assign(coeffs.begin(), coeffs.begin() + degree + 1);
+        poly.max_degree = degree;
+        poly.lead = true;
+        poly.even = parity(coeffs, 1);
+        poly.odd = parity(coeffs, 0);
+        const size_t log_degree = bit_length(degree);
+        const size_t log_split = split_log(log_degree);
+
+        values_.emplace(1, ops_.clone(x));
+        exact_.emplace(1, ExactScale::of(static_cast<double>(x.scale), c_.q.size()));
+        gen_power(size_t{1} << (log_degree - 1));
+        for (size_t i = (size_t{1} << log_split) - 1; i > 2; --i)
+            if ((!poly.even && !poly.odd) || ((i & 1U) == 0U && poly.even) || ((i & 1U) == 1U && poly.odd))
+                gen_power(i);
+
+        // plan
+        Planner pl(c_.q);
+        std::map<size_t, SimOperand> sim;
+        sim[1] = SimOperand{x.level, x.scale};
+        pl.powers(size_t{1} << log_degree, sim);
+        auto leaves = pl.plan(log_split, x.level - eval_depth(degree), poly, sim,
+                              static_cast<long double>(target_scale)).first;
+
+        // baby steps (stored in reverse order), then giant-step merges
+        struct Step {
+            size_t degree;
+            std::optional<CtBatch> value;
+        };
+        const size_t split = leaves.size();
+        std::vector<std::optional<Step>> steps(split);
+        for (size_t i = 0; i < split; ++i)
+            steps[split - i - 1] = Step{leaves[i].degree(), eval_leaf(leaves[i].level, leaves[i])};
+        while (steps.size() != 1) {
+            std::vector<int> kind(steps.size(), 0);
+            for (size_t i = 0; i < steps.size(); ++i) {
+                if (i == steps.size() - 1) {
+                    kind[i] = 2;
+                } else if (steps[i]->degree == steps[i + 1]->degree) {
+                    kind[i] = 1;
+                    ++i;
+                }
+            }
+            for (size_t i = 0; i < steps.size(); ++i) {
+                if (kind[i] == 2) {
+                    steps[i]->degree = steps[i - 1]->degree;
+                } else if (kind[i] == 1) {
+                    Step& even = *steps[i];
+                    Step& odd = *steps[i + 1];
+                    const size_t deg = size_t{1} << bit_length(even.degree);
+                    monomial(*even.value, *odd.value, values_.at(deg));
+                    odd.degree = 2 * deg - 1;
+                    steps[i].reset();
+                    ++i;
+                }
+            }
+            size_t w = 0;
+            for (size_t i = 0; i < steps.size(); ++i)
+                if (steps[i].has_value()) {
+                    if (w != i) steps[w] = std::move(steps[i]);
+                    ++w;
+                }
+            steps.resize(w);
+        }
+        CtBatch out = std::move(*steps.front()->value);
+        if (out.np == 3) ops_.relin(out);
+        ops_.rescale(out);
+        out.scale = static_cast<long double>(target_scale);
+        return out;
+    }
+
+private:
+    static bool parity(const std::vector<double>& coeffs, size_t first) {
+        for (size_t i = first; i < coeffs.size(); i += 2)
+            if (coeffs[i] != 0.0) return false;
+        return true;
+    }
+
+    std::vector<uint64_t> constants(double value, long double scale, size_t level) const {
+        std::vector<uint64_t> v(level + 1);
+        for (size_t l = 0; l <= level; ++l) v[l] = scaled_constant_mod(value, scale, c_.q[l]);
+        return v;
+    }
+
+    void add_constant(CtBatch& x, double value, long double scale) {
+        if (value == 0.0) return;
+        ops_.scalar(x, nullptr, constants(value, scale, x.level), kScalarAdd);
+    }
+
+    // multiply_by_integer_scalar_inplace
+    void mul_integer(CtBatch& x, long double scalar, long double out_scale) {
+        if (!std::isfinite(scalar) || scalar < 0.0L) throw std::invalid_argument("ckks_evalchebyshev: invalid scalar scale-up");
+        const long double r = std::round(scalar);
+        if (r < 1.0L || std::abs(scalar - r) > std::max<long double>(1.0L, std::abs(scalar)) * 0x1p-20L)
+            throw std::invalid_argument("ckks_evalchebyshev: non-integral scalar scale-up");
+        if (r > static_cast<long double>(std::numeric_limits<uint64_t>::max()))
+            throw std::invalid_argument("ckks_evalchebyshev: scalar scale-up is too large");
+        const uint64_t s = static_cast<uint64_t>(r);
+        if (s != 1) {
+            std::vector<uint64_t> v(x.level + 1);
+            for (size_t l = 0; l <= x.level; ++l) v[l] = s % c_.q[l];
+            ops_.scalar(x, nullptr, v, kScalarMul);
+        }
+        x.scale = static_cast<double>(out_scale);
+    }
+
+    void scale_up_to(CtBatch& x, long double target) {
+        const double cur = static_cast<double>(x.scale), tgt = static_cast<double>(target);
+        const double m = std::max({1.0, std::abs(cur), std::abs(tgt)});
+        if (std::isfinite(cur) && std::isfinite(tgt) && std::abs(cur - tgt) <= 0x1p-45 * m) {
+            x.scale = static_cast<double>(target);
+            return;
+        }
+        if (x.scale > target) throw std::invalid_argument("ckks_evalchebyshev: cannot scale down ciphertext during scale alignment");
+        mul_integer(x, target / x.scale, target);
+    }
+
+    long double rescale_product(size_t level) const {
+        const size_t levels = std::log2(default_scale_) <= 64.0 ? 1 : 2;
+        if (level + 1 < levels) throw std::invalid_argument("ckks_evalchebyshev: insufficient level for rescale modulus product");
+        long double s = 1.0L;
+        for (size_t i = 0; i < levels; ++i) s *= static_cast<long double>(c_.q[level - i]);
+        return s;
+    }
+
+    void align(CtBatch& x, size_t level, double scale, int np) {
+        if (level > x.level) throw std::invalid_argument("ckks_drop_to_level_inplace: cannot raise ciphertext level");
+        x.level = level;
+        x.scale = scale;
+        ops_.pad(x, np);
+    }
+
+    // multhenadd_real_scalar_scale_aware_inplace: out += scalar * x, scales reconciled.
+    void mul_then_add(const CtBatch& x, double scalar, CtBatch& out) {
+        if (scalar == 0.0) return;
+        const size_t level = std::min(x.level, out.level);
+        const double out_scale = static_cast<double>(out.scale);
+        const int np = std::max(x.np, out.np);
+        align(out, level, out_scale, np);
+        CtBatch xa = ops_.clone(x);
+        align(xa, level, static_cast<double>(x.scale), np);
+        long double scale_rlwe = 0.0L;
+        if (scales_close(static_cast<double>(xa.scale), static_cast<double>(out.scale))) {
+            if (is_integer(scalar)) {
+                scale_rlwe = 1.0L;
+            } else {
+                scale_rlwe = rescale_product(level);
+                scale_up_to(out, out.scale * scale_rlwe);
+            }
+        } else if (xa.scale < out.scale) {
+            scale_rlwe = out.scale / xa.scale;
+        } else {
+            throw std::invalid_argument("ckks_evalchebyshev: MulThenAdd requires op0.Scale <= opOut.Scale");
+        }
+        const long double term_scale = xa.scale * scale_rlwe;
+        if (!scales_close(static_cast<double>(term_scale), static_cast<double>(out.scale)))
+            throw std::runtime_error("ckks_evalchebyshev: MulThenAdd scale mismatch");
+        ops_.scalar(out, &xa, constants(scalar, scale_rlwe, out.level), kScalarMulAdd);
+    }
+
+    CtBatch eval_leaf(size_t target_level, const Poly& p) {
+        const size_t degree = p.degree();
+        CtBatch r = ops_.zeros(target_level, static_cast<double>(p.scale));
+        if (p.even && p.coeffs[0] != 0.0) add_constant(r, p.coeffs[0], p.scale);
+        if (degree == 0) return r;
+        for (size_t e = degree; e > 0; --e) {
+            const double cf = p.coeffs[e];
+            if (cf == 0.0) continue;
+            if (!((!p.even && !p.odd) || ((e & 1U) == 0U && p.even) || ((e & 1U) == 1U && p.odd))) continue;
+            align(r, target_level, static_cast<double>(p.scale), r.np);
+            mul_then_add(values_.at(e), cf, r);
+        }
+        return r;
+    }
+
+    // evaluate_monomial: odd <- even + rescale(relin(odd)) * xpow
+    void monomial(CtBatch& even, CtBatch& odd, const CtBatch& xpow) {
+        if (odd.np == 3) ops_.relin(odd);
+        ops_.rescale(odd);
+        CtBatch xp = ops_.clone(xpow);
+        if (odd.level > xp.level) throw std::invalid_argument("ckks_drop_to_level_inplace: cannot raise ciphertext level");
+        xp.level = odd.level;
+        const long double prod = odd.scale * xp.scale;
+        ops_.tensor(odd, xp);
+        odd.scale = prod;
+        align(even, odd.level, static_cast<double>(even.scale), odd.np);
+        if (!scales_close(static_cast<double>(even.scale), static_cast<double>(odd.scale)))
+            throw std::runtime_error("ckks_evalchebyshev: EvaluateMonomial scale mismatch");
+        const double common = static_cast<double>(std::max(even.scale, odd.scale));
+        even.scale = common;
+        odd.scale = common;
+        ops_.add(odd, even, false);
+    }
+
+    void rescale_power(size_t n) {
+        CtBatch& v = values_.at(n);
+        const size_t before = v.level;
+        ops_.rescale(v);
+        ExactScale& e = exact_.at(n);
+        if (e.den.size() < before + 1) e.den.resize(before + 1, 0);
+        e.den[before] += 1;
+        v.scale = e.value_d(c_.q);
+    }
+
+    void gen_power(size_t n) {
+        if (n < 2 || values_.count(n)) return;
+        if (gen_power_rec(n)) rescale_power(n);
+    }
+
+    bool gen_power_rec(size_t n) {
+        if (values_.count(n)) return false;
+        const auto [a, b] = split_degree(n);
+        const bool ra = gen_power_rec(a);
+        const bool rb = gen_power_rec(b);
+        if (ra) rescale_power(a);
+        if (rb) rescale_power(b);
+        CtBatch out = ops_.clone(values_.at(a));
+        const size_t level = a == b ? out.level : std::min(out.level, values_.at(b).level);
+        out.level = level;
+        const ExactScale prod = times(exact_.at(a), exact_.at(b));
+        CtBatch rhs = ops_.clone(values_.at(b));  // the square uses a second copy (no aliasing)
+        rhs.level = level;
+        ops_.tensor(out, rhs);
+        ops_.relin(out);
+        out.scale = prod.value_d(c_.q);
+        mul_integer(out, 2.0L, prod.value(c_.q));
+        const size_t cdeg = a > b ? a - b : b - a;
+        if (cdeg == 0) {
+            add_constant(out, -1.0, prod.value(c_.q));
+        } else {
+            gen_power(cdeg);
+            CtBatch corr = ops_.clone(values_.at(cdeg));
+            const uint64_t ratio = ratio_u64(prod, exact_.at(cdeg), c_.q);
+            corr.scale = exact_.at(cdeg).value_d(c_.q);
+            align(corr, out.level, static_cast<double>(corr.scale), out.np);
+            mul_integer(corr, static_cast<long double>(ratio), prod.value(c_.q));
+            ops_.add(out, corr, true);
+        }
+        values_.insert_or_assign(n, std::move(out));
+        exact_.insert_or_assign(n, prod);
+        return true;
+    }
+
+    Context& c_;
+    DeviceOps& ops_;
+    long double default_scale_;
+    std::map<size_t, CtBatch> values_;
+    std::map<size_t, ExactScale> exact_;
+};
+
+}  // namespace
+
+void evalchebyshev(Context& c, size_t count, size_t level, double scale, const double* coeffs, size_t ncoeffs,
+                   double target_scale, double default_scale, uint64_t* const* b, uint64_t* const* a,
+                   uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                   cudaStream_t s) {
+    if (ncoeffs == 0) throw std::invalid_argument("ckks_evalpoly: polynomial must have at least one coefficient");
+    std::vector<double> cf(coeffs, coeffs + ncoeffs);
+    for (double v : cf)
+        if (!std::isfinite(v)) throw std::invalid_argument("ckks_evalpoly: polynomial coefficients must be finite");
+    size_t degree = 0;
+    for (size_t i = cf.size(); i > 0; --i)
+        if (cf[i - 1] != 0.0) {
+            degree = i - 1;
+            break;
+        }
+    const double tgt = target_scale > 0.0 ? target_scale : scale;
+    if (!std::isfinite(tgt) || tgt <= 0.0) throw std::invalid_argument("ckks_evalpoly: invalid scale");
+    if (level >= c.nq) throw std::invalid_argument("ckks_evalpoly: invalid ciphertext level");
+    if (level < ceil_log2(degree))
+        throw std::invalid_argument(
+            "ckks_evalchebyshev_preconditioned: ciphertext level is too small for Chebyshev evaluation depth");
+    if (count == 0) return;
+    DeviceOps ops(c, count, s);
+    CtBatch x = ops.wrap(b, a, level, static_cast<long double>(scale));
+    CtBatch out;
+    if (degree == 0) {
+        out = ops.zeros(level, tgt);
+        if (cf[0] != 0.0) {
+            std::vector<uint64_t> v(level + 1);
+            for (size_t l = 0; l <= level; ++l) v[l] = scaled_constant_mod(cf[0], static_cast<long double>(tgt), c.q[l]);
+            ops.scalar(out, nullptr, v, kScalarAdd);
+        }
+    } else {
+        if (level < eval_depth(degree)) throw std::invalid_argument("ckks_evalchebyshev: insufficient level for polynomial depth");
+        ChebyshevEval ev(c, ops, static_cast<long double>(default_scale));
+        out = ev.run(x, cf, degree, tgt);
+    }
+    ops.copy_out(out, out_b, out_a);
+    *out_level = out.level;
+    *out_scale = static_cast<double>(out.scale);
+}
+
+}  // namespace wg

@@ -83,6 +83,8 @@ def lib() -> C.CDLL:
         L.wg_modraise.argtypes = [vp, sz, sz, vp, vp, vp]
         L.wg_dense_to_sparse.argtypes = [vp, sz, vp, vp, vp]
         L.wg_sparse_to_dense.argtypes = [vp, sz, vp, vp, vp, vp]
+        L.wg_evalchebyshev.argtypes = [vp, sz, sz, C.c_double, vp, sz, C.c_double, C.c_double, vp, vp, vp, vp,
+                                       C.POINTER(C.c_size_t), C.POINTER(C.c_double), vp]
         L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_batch_plan_launch.argtypes = [vp, vp]
         L.wg_batch_plan_destroy.argtypes = [vp]
@@ -347,6 +349,20 @@ class Context:
         lv = np.ascontiguousarray(levels, dtype=np.uintp)
         _check(lib().wg_sparse_to_dense(self.h, len(pb), lv.ctypes.data, pb.ctypes.data, pa.ctypes.data,
                                         _stream(stream)))
+
+    def evalchebyshev(self, level, scale, coeffs, bs, as_, out_bs, out_as, target_scale=0.0, default_scale=None,
+                      stream=None):
+        """Chebyshev series sum_k coeffs[k] T_k(x) of ciphertexts sharing level and scale (lists of
+        device tensors); results into out_bs / out_as.  Returns (out_level, out_scale)."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        pb, pa, ob, oa = arr(bs), arr(as_), arr(out_bs), arr(out_as)
+        cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        lvl, sc = C.c_size_t(), C.c_double()
+        _check(lib().wg_evalchebyshev(self.h, len(pb), level, float(scale), cf.ctypes.data, len(cf), float(target_scale),
+                                      float(scale if default_scale is None else default_scale), pb.ctypes.data,
+                                      pa.ctypes.data, ob.ctypes.data, oa.ctypes.data, C.byref(lvl), C.byref(sc),
+                                      _stream(stream)))
+        return lvl.value, sc.value
 
     def mul(self, level, b1, a1, b2, a2, c2, stream=None):
         _check(lib().wg_mul(self.h, level, _ptr(b1), _ptr(a1), _ptr(b2), _ptr(a2), _ptr(c2), _stream(stream)))

@@ -166,6 +166,20 @@ int wg_dense_to_sparse(wg_context* ctx, size_t count, uint64_t* const* b, uint64
 int wg_sparse_to_dense(wg_context* ctx, size_t count, const size_t* levels, uint64_t* const* b,
                        uint64_t* const* a, void* stream);
 
+/* Chebyshev polynomial evaluation of `count` ciphertexts that share `level` and `scale`
+ * (device pointers b[i], a[i]; the inputs are read only): sum_k coeffs[k] T_k(x) with the
+ * reference's power basis, scale-aware Paterson-Stockmeyer schedule and constant rounding, so
+ * the residues equal those of ckks_evalchebyshev_preconditioned
+ * (src/ckks/operations/evalpoly/ckks_evalpoly.cpp:1221-1256) for the same inputs.
+ * target_scale <= 0 keeps `scale`; default_scale is the parameter set's scale
+ * (CKKSParams::getScale, which decides how many moduli one rescale consumes).  The results go
+ * to out_b[i], out_a[i] (room for level+1 limbs) at *out_level with scale *out_scale.  Needs
+ * the relinearisation key.  Temporary ciphertexts come from the stream-ordered allocator. */
+int wg_evalchebyshev(wg_context* ctx, size_t count, size_t level, double scale, const double* coeffs,
+                     size_t ncoeffs, double target_scale, double default_scale, uint64_t* const* b,
+                     uint64_t* const* a, uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level,
+                     double* out_scale, void* stream);
+
 /* The same batched pipeline planned once for fixed buffers and captured as a CUDA graph
  * (no counterpart in the reference, which plans nothing ahead).  Create takes the arguments
  * of wg_batch_mul_relin_rescale_rotate minus the stream, builds the job tables, uploads them

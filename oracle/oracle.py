@@ -428,6 +428,9 @@ class RefPlans:
         R.ref_modraise.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
         R.ref_dense_to_sparse.argtypes = [C.c_void_p, u64p, u64p]
         R.ref_sparse_to_dense.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
+        R.ref_ctx_scale.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        R.ref_evalchebyshev.argtypes = [C.c_void_p, C.c_size_t, C.c_double, f64p, C.c_size_t, C.c_double, u64p, u64p,
+                                        C.POINTER(C.c_size_t), C.POINTER(C.c_double), u64p, u64p]
         R.ref_plan_stage_count.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
         R.ref_plan_stage_info.argtypes = [C.c_void_p, C.c_int, C.c_size_t] + [C.POINTER(C.c_size_t)] * 2 + \
             [C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]
@@ -446,6 +449,9 @@ class RefPlans:
         _check(R.ref_ctx_moduli(self.h, self.q, C.byref(nq), self.p, C.byref(np_)), "ref_ctx_moduli")
         self.N = 1 << 15
         self.dnum = 3
+        sc = C.c_double()
+        _check(R.ref_ctx_scale(self.h, C.byref(sc)), "ref_ctx_scale")
+        self.scale = sc.value
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -504,6 +510,19 @@ class RefPlans:
         ao[: self.N] = np.asarray(a, dtype=np.uint64)[: self.N]
         _check(ref().ref_modraise(self.h, target_level, bo, ao), "ref_modraise")
         return bo, ao
+
+    def evalchebyshev(self, level, scale, coeffs, b, a, target_scale=0.0):
+        """The reference's ckks_evalchebyshev_preconditioned: (b, a, out_level, out_scale)."""
+        n = (level + 1) * self.N
+        ob = np.zeros(n, np.uint64)
+        oa = np.zeros(n, np.uint64)
+        lvl, sc = C.c_size_t(), C.c_double()
+        _check(ref().ref_evalchebyshev(self.h, level, float(scale), np.ascontiguousarray(coeffs, dtype=np.float64),
+                                       len(coeffs), float(target_scale), np.ascontiguousarray(b[:n], dtype=np.uint64),
+                                       np.ascontiguousarray(a[:n], dtype=np.uint64), C.byref(lvl), C.byref(sc), ob, oa),
+               "ref_evalchebyshev")
+        m = (lvl.value + 1) * self.N
+        return ob[:m].copy(), oa[:m].copy(), lvl.value, sc.value
 
     def dense_to_sparse(self, b, a):
         b = np.ascontiguousarray(b[: self.N], dtype=np.uint64).copy()

@@ -33,6 +33,7 @@
 #include "ckks_ciphertext.hpp"
 #include "ckks_linear_transform.hpp"
 #include "ckks_modraise.hpp"
+#include "ckks_evalpoly.hpp"
 #include "ckks_context.hpp"
 #include "ckks_conjugate.hpp"
 #include "ckks_keyswitch.hpp"
@@ -483,6 +484,34 @@ int ref_sparse_to_dense(void* h, size_t level, uint64_t* b, uint64_t* a) {
         copy_out(ct.getB(), b);
         copy_out(ct.getA(), a);
     });
+}
+
+// ckks_evalchebyshev_preconditioned (src/ckks/operations/evalpoly/ckks_evalpoly.cpp:1221-1256)
+// on a ciphertext at `level` with scale `scale`; target_scale 0 keeps the input scale.  The
+// output (b, a) has (*out_level + 1) * N residues; *out_scale is its scale.
+int ref_evalchebyshev(void* h, size_t level, double scale, const double* coeffs, size_t ncoeffs,
+                      double target_scale, const uint64_t* b, const uint64_t* a, size_t* out_level,
+                      double* out_scale, uint64_t* out_b, uint64_t* out_a) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        CKKSCiphertext ct(N, copy_in(a, n), copy_in(b, n), (long double)scale, level);
+        CKKSEvalPolyOptions opt;
+        opt.target_scale = target_scale;
+        CKKSCiphertext out = ckks_evalchebyshev_preconditioned(c, ct, std::span<const double>(coeffs, ncoeffs), opt);
+        if (out.getNumPolys() != 2) throw std::runtime_error("ref_evalchebyshev: unexpected polynomial count");
+        *out_level = out.getLevel();
+        *out_scale = (double)out.getScale();
+        copy_out(out.getB(), out_b);
+        copy_out(out.getA(), out_a);
+    });
+}
+
+// The context's default scale and the EvalMod polynomial it built (Chebyshev coefficients on
+// [interval_min, interval_max]).
+int ref_ctx_scale(void* h, double* scale) {
+    return guarded([&] { *scale = (double)static_cast<RefCtx*>(h)->ctx.getParams().getScale(); });
 }
 
 static const CKKSLinearTransformPlan& plan_of(void* h, int which) {
