@@ -89,6 +89,19 @@ void evalchebyshev(Context& c, size_t count, size_t level, double scale, const d
                    uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
                    cudaStream_t s);
 
+// EvalMod bootstrap of packed ciphertexts (wg_evalpoly.cu).
+struct BootstrapParams {
+    size_t s2c_depth = 0, depth = 0, evalmod_log_scale = 0, double_angle = 0, active_slots = 0, slots = 0;
+    double scale = 0.0;
+};
+size_t lt_stage_level(const LtStage& st);
+bool lt_stage_rescales(const LtStage& st);
+void bootstrap_evalmod(Context& c, const BootstrapParams& p, const LtStage* const* s2c, size_t ns2c,
+                       const LtStage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs, size_t count,
+                       uint64_t* const* b, uint64_t* const* a, uint64_t* const* out0_b, uint64_t* const* out0_a,
+                       uint64_t* const* out1_b, uint64_t* const* out1_a, size_t* out_level, double* out_scale,
+                       cudaStream_t s);
+
 // Hoisted rotations of one ciphertext; out [rotation][b, a][level+1][N] (wg_bsgs.cu).
 void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rots, size_t nrot,
                  uint64_t* out, cudaStream_t s);

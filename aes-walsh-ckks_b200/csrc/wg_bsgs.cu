@@ -222,6 +222,9 @@ __global__ void __launch_bounds__(kT) kb_accumulate(const AccumJob* jobs, int n,
 
 }  // namespace
 
+size_t lt_stage_level(const LtStage& st) { return st.level; }
+bool lt_stage_rescales(const LtStage& st) { return st.rescale; }
+
 LtStage* lt_stage_create(Context& c, size_t level, size_t nterms, const uint64_t* indices, const uint64_t* diags,
                          size_t baby, size_t slots, bool rescale) {
     if (level >= c.nq) fail(kInvalid, "ckks_linear_transform: invalid stage level");

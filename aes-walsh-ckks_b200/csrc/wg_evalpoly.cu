@@ -57,6 +57,20 @@ __global__ void __launch_bounds__(kT) kb_scalar(const ScalarJob* jobs, int n, co
         j->x[k] = add_mod(j->x[k], j->s, q);
 }
 
+struct PmulJob {
+    uint64_t* x;
+    const uint64_t* p;
+    int mod, pad;
+};
+
+// x = x * p (mod q), pointwise (Barrett product of canonical residues)
+__global__ void __launch_bounds__(kT) kb_pmul(const PmulJob* jobs, int n, const Modulus* mods) {
+    const PmulJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    j->x[k] = barrett_mul(j->x[k], j->p[k], mods[j->mod]);
+}
+
 // A batch of ciphertexts with common metadata.  Polynomial k of ciphertext i lives at p[i][k]
 // with room for `cap` limbs; limbs [0, level] are live.
 struct CtBatch {
@@ -228,6 +242,77 @@ public:
         Probe probe(kClsElementwise, 8.0 * N * jobs.size() * (op == kScalarMulAdd ? 3.0 : 2.0), s_);
         kb_scalar<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
         check_cuda(cudaGetLastError(), "evalpoly scalar");
+    }
+
+    // ckks_conjugate: automorphism X -> X^(2N-1) of (b, a), then key switch of the permuted a.
+    CtBatch conjugate(const CtBatch& x) {
+        const size_t N = c_.N, L = x.level + 1;
+        const KeyEntry& k = c_.key(WG_KEY_CONJ, 0);
+        CtBatch perm = alloc(x.level, 2);
+        CtBatch out = alloc(x.level, 2);
+        out.scale = x.scale;
+        std::vector<KsItem> items(count_);
+        for (size_t i = 0; i < count_; ++i) {
+            for (int poly = 0; poly < 2; ++poly)
+                automorphism(c_, x.p[i][poly], perm.p[i][poly], (int)L, 1, 0, 2 * N - 1, s_);
+            KsItem& it = items[i];
+            it.level = x.level;
+            it.key_term = perm.p[i][1];
+            it.key = &k;
+            it.b_in = perm.p[i][0];
+            it.a_in = perm.p[i][1];
+            it.b = out.p[i][0];
+            it.a = out.p[i][1];
+            it.b_add = 1;
+            it.a_add = 0;
+            it.galois = 0;
+        }
+        batch_keyswitch(c_, items.data(), count_, s_);
+        return out;
+    }
+
+    // ckks_mul_inplace(ct, Complex, scale): the slot-constant re + i im encodes (at scale
+    // `scale`) to round(scale re) + round(scale im) X^(N/2); multiply every polynomial by it.
+    void mul_complex_constant(CtBatch& x, double re, double im, double scale) {
+        const size_t N = c_.N, L = x.level + 1;
+        const long long r0 = std::llround(scale * re), r1 = std::llround(scale * im);
+        std::vector<uint64_t> host(L * N, 0);
+        for (size_t l = 0; l < L; ++l) {
+            const uint64_t q = c_.q[l];
+            auto modq = [q](long long v) {
+                const uint64_t m = (uint64_t)(v < 0 ? -v : v) % q;
+                return v < 0 && m ? q - m : m;
+            };
+            host[l * N] = modq(r0);
+            host[l * N + N / 2] = modq(r1);
+        }
+        uint64_t* pt = buffer(L, false);
+        check_cuda(cudaMemcpyAsync(pt, host.data(), L * N * 8, cudaMemcpyHostToDevice, s_), "constant plaintext");
+        check_cuda(cudaStreamSynchronize(s_), "constant plaintext");
+        ntt_forward(c_, pt, (int)L, 1, 0, LimbMap{0, 0, 0}, s_);
+        std::vector<PmulJob> jobs;
+        for (size_t i = 0; i < count_; ++i)
+            for (int k = 0; k < x.np; ++k)
+                for (size_t l = 0; l < L; ++l) jobs.push_back({x.p[i][k] + l * N, pt + l * N, (int)l, 0});
+        JobTable t;
+        const PmulJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 3.0, s_);
+        kb_pmul<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        check_cuda(cudaGetLastError(), "evalpoly plaintext multiply");
+    }
+
+    CtBatch alloc(size_t level, int np) {
+        CtBatch x;
+        x.p.resize(count_);
+        for (size_t i = 0; i < count_; ++i) {
+            x.p[i] = {nullptr, nullptr, nullptr};
+            for (int k = 0; k < np; ++k) x.p[i][k] = buffer(level + 1, false);
+        }
+        x.np = np;
+        x.level = level;
+        x.cap = level + 1;
+        return x;
     }
 
     void copy_out(const CtBatch& x, uint64_t* const* b, uint64_t* const* a) {
@@ -720,12 +805,9 @@ private:
     std::map<size_t, ExactScale> exact_;
 };
 
-}  // namespace
-
-void evalchebyshev(Context& c, size_t count, size_t level, double scale, const double* coeffs, size_t ncoeffs,
-                   double target_scale, double default_scale, uint64_t* const* b, uint64_t* const* a,
-                   uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
-                   cudaStream_t s) {
+// ckks_evalchebyshev_preconditioned on a batch (the input is read only).
+CtBatch chebyshev(Context& c, DeviceOps& ops, const CtBatch& x, const double* coeffs, size_t ncoeffs,
+                  double target_scale, double default_scale) {
     if (ncoeffs == 0) throw std::invalid_argument("ckks_evalpoly: polynomial must have at least one coefficient");
     std::vector<double> cf(coeffs, coeffs + ncoeffs);
     for (double v : cf)
@@ -736,28 +818,173 @@ void evalchebyshev(Context& c, size_t count, size_t level, double scale, const d
             degree = i - 1;
             break;
         }
-    const double tgt = target_scale > 0.0 ? target_scale : scale;
+    const double tgt = target_scale > 0.0 ? target_scale : static_cast<double>(x.scale);
     if (!std::isfinite(tgt) || tgt <= 0.0) throw std::invalid_argument("ckks_evalpoly: invalid scale");
-    if (level >= c.nq) throw std::invalid_argument("ckks_evalpoly: invalid ciphertext level");
-    if (level < ceil_log2(degree))
+    if (x.level >= c.nq) throw std::invalid_argument("ckks_evalpoly: invalid ciphertext level");
+    if (x.level < ceil_log2(degree))
         throw std::invalid_argument(
             "ckks_evalchebyshev_preconditioned: ciphertext level is too small for Chebyshev evaluation depth");
+    if (degree == 0) {
+        CtBatch out = ops.zeros(x.level, tgt);
+        if (cf[0] != 0.0) {
+            std::vector<uint64_t> v(x.level + 1);
+            for (size_t l = 0; l <= x.level; ++l)
+                v[l] = scaled_constant_mod(cf[0], static_cast<long double>(tgt), c.q[l]);
+            ops.scalar(out, nullptr, v, kScalarAdd);
+        }
+        return out;
+    }
+    if (x.level < eval_depth(degree)) throw std::invalid_argument("ckks_evalchebyshev: insufficient level for polynomial depth");
+    ChebyshevEval ev(c, ops, static_cast<long double>(default_scale));
+    return ev.run(x, cf, degree, tgt);
+}
+
+// multiply_by_real_scalar_to_scale_inplace (ckks_bootstrap_evalmod_inplace.cpp:220-263)
+void mul_real_to_scale(Context& c, DeviceOps& ops, CtBatch& x, double scalar, long double out_scale) {
+    if (!std::isfinite(scalar) || !std::isfinite(out_scale) || out_scale <= 0.0L || x.scale <= 0.0L)
+        throw std::invalid_argument("evalmod_binary_inplace: invalid double-angle scalar scaling");
+    const long double ss = out_scale / x.scale;
+    std::vector<uint64_t> v(x.level + 1);
+    for (size_t l = 0; l <= x.level; ++l) v[l] = scaled_constant_mod(scalar, ss, c.q[l]);
+    ops.scalar(x, nullptr, v, kScalarMul);
+    x.scale = static_cast<double>(out_scale);
+}
+
+}  // namespace
+
+// ckks_batch_bootstrap_evalmod_from_complex_packed (ckks_bootstrap_evalmod_inplace.cpp:265-434)
+// for a batch of packed ciphertexts at level p.s2c_depth whose scale equals p.scale:
+// SlotToCoeff, dense-to-sparse switch, ModRaise to p.depth, sparse-to-dense switch, sparse-slot
+// trace, CoeffToSlot, conjugate split into (ct + conj) and -i (ct - conj), then EvalMod (the
+// Chebyshev series at scale 2^evalmod_log_scale, then the double-angle steps) on both halves
+// as one batch of 2 x count.  b[i] / a[i] need room for depth+1 limbs and are overwritten.
+void bootstrap_evalmod(Context& c, const BootstrapParams& p, const LtStage* const* s2c, size_t ns2c,
+                       const LtStage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs, size_t count,
+                       uint64_t* const* b, uint64_t* const* a, uint64_t* const* out0_b, uint64_t* const* out0_a,
+                       uint64_t* const* out1_b, uint64_t* const* out1_a, size_t* out_level, double* out_scale,
+                       cudaStream_t s) {
+    if (count == 0) return;
+    if (p.s2c_depth == 0 || p.depth >= c.nq || p.depth < p.s2c_depth)
+        throw std::invalid_argument("ckks EvalMod: invalid bootstrap depths");
+    const size_t N = c.N;
+    size_t level = p.s2c_depth;
+    // SlotToCoeff
+    for (size_t k = 0; k < ns2c; ++k) {
+        if (lt_stage_level(*s2c[k]) != level) throw std::invalid_argument("ckks_linear_transform: stage level mismatch");
+        lt_stage_apply(c, *s2c[k], count, b, a, s);
+        if (lt_stage_rescales(*s2c[k])) --level;
+    }
+    if (level != 0) throw std::invalid_argument("ckks EvalMod: SlotToCoeff must end at level 0");
+    // secret switch, ModRaise, switch back
+    q0p0_switch(c, count, b, a, c.key(WG_KEY_DENSE_TO_SPARSE, 0), s);
+    modraise(c, count, p.depth, b, a, s);
+    level = p.depth;
+    {
+        const KeyEntry& k = c.key(WG_KEY_SPARSE_TO_DENSE, 0);
+        std::vector<KsItem> items(count);
+        for (size_t i = 0; i < count; ++i) {
+            KsItem& it = items[i];
+            it.level = level;
+            it.key_term = a[i];
+            it.key = &k;
+            it.b_in = b[i];
+            it.a_in = a[i];
+            it.b = b[i];
+            it.a = a[i];
+            it.b_add = 1;
+            it.a_add = 0;
+            it.galois = 0;
+        }
+        batch_keyswitch(c, items.data(), count, s);
+    }
+    DeviceOps ops(c, count, s);
+    // sparse-slot trace: ct += rotate(ct, r) for r = active, 2 active, ... < slots
+    for (size_t r = p.active_slots; r < p.slots; r <<= 1) {
+        CtBatch x = ops.wrap(b, a, level, 0.0L);
+        CtBatch rot = ops.clone(x);
+        const KeyEntry& k = c.key(WG_KEY_ROTATION, (int64_t)r);
+        std::vector<KsItem> items(count);
+        for (size_t i = 0; i < count; ++i) {
+            KsItem& it = items[i];
+            it.level = level;
+            it.key_term = rot.p[i][1];
+            it.key = &k;
+            it.b_in = rot.p[i][0];
+            it.a_in = rot.p[i][1];
+            it.b = rot.p[i][0];
+            it.a = rot.p[i][1];
+            it.b_add = 1;
+            it.a_add = 0;
+            it.galois = host::powmod(5, r, 2 * N);
+        }
+        batch_keyswitch(c, items.data(), count, s);
+        ops.add(x, rot, false);
+    }
+    // CoeffToSlot
+    for (size_t k = 0; k < nc2s; ++k) {
+        if (lt_stage_level(*c2s[k]) != level) throw std::invalid_argument("ckks_linear_transform: stage level mismatch");
+        lt_stage_apply(c, *c2s[k], count, b, a, s);
+        if (lt_stage_rescales(*c2s[k])) --level;
+    }
+    // conjugate split into the 2 x count EvalMod batch (out0 rows, then out1 rows)
+    CtBatch packed = ops.wrap(b, a, level, 0.0L);
+    CtBatch conj = ops.conjugate(packed);
+    std::vector<uint64_t*> eb(2 * count), ea(2 * count);
+    for (size_t i = 0; i < count; ++i) {
+        eb[i] = out0_b[i];
+        ea[i] = out0_a[i];
+        eb[count + i] = out1_b[i];
+        ea[count + i] = out1_a[i];
+        for (int poly = 0; poly < 2; ++poly) {
+            uint64_t* dst0 = poly ? out0_a[i] : out0_b[i];
+            uint64_t* dst1 = poly ? out1_a[i] : out1_b[i];
+            check_cuda(cudaMemcpyAsync(dst0, packed.p[i][poly], (level + 1) * N * 8, cudaMemcpyDeviceToDevice, s), "split");
+            check_cuda(cudaMemcpyAsync(dst1, packed.p[i][poly], (level + 1) * N * 8, cudaMemcpyDeviceToDevice, s), "split");
+        }
+    }
+    {
+        CtBatch o0 = ops.wrap(out0_b, out0_a, level, 0.0L);
+        CtBatch o1 = ops.wrap(out1_b, out1_a, level, 0.0L);
+        ops.add(o0, conj, false);
+        ops.add(o1, conj, true);
+        ops.mul_complex_constant(o1, 0.0, -1.0, 1.0);
+    }
+    // EvalMod on both halves at once
+    DeviceOps ops2(c, 2 * count, s);
+    CtBatch x = ops2.wrap(eb.data(), ea.data(), level, static_cast<long double>(std::exp2((double)p.evalmod_log_scale)));
+    CtBatch y = chebyshev(c, ops2, x, coeffs, ncoeffs, p.scale, p.scale);
+    y.scale = p.scale;
+    const long double target = y.scale;
+    for (size_t i = 0; i < p.double_angle; ++i) {
+        if (y.level == 0) throw std::invalid_argument("evalmod_binary_inplace: insufficient level for BinBoot double-angle");
+        CtBatch sq = ops2.clone(y);
+        CtBatch sq2 = ops2.clone(y);
+        const long double prod = sq.scale * sq.scale;
+        ops2.tensor(sq, sq2);
+        sq.scale = prod;
+        ops2.relin(sq);
+        ops2.rescale(sq);
+        mul_real_to_scale(c, ops2, sq, -4.0, target);
+        y.level = sq.level;
+        mul_real_to_scale(c, ops2, y, 4.0, target);
+        ops2.add(y, sq, false);
+        y.scale = target;
+    }
+    y.scale = p.scale;
+    ops2.copy_out(y, eb.data(), ea.data());
+    *out_level = y.level;
+    *out_scale = static_cast<double>(y.scale);
+}
+
+void evalchebyshev(Context& c, size_t count, size_t level, double scale, const double* coeffs, size_t ncoeffs,
+                   double target_scale, double default_scale, uint64_t* const* b, uint64_t* const* a,
+                   uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                   cudaStream_t s) {
+    if (level >= c.nq) throw std::invalid_argument("ckks_evalpoly: invalid ciphertext level");
     if (count == 0) return;
     DeviceOps ops(c, count, s);
     CtBatch x = ops.wrap(b, a, level, static_cast<long double>(scale));
-    CtBatch out;
-    if (degree == 0) {
-        out = ops.zeros(level, tgt);
-        if (cf[0] != 0.0) {
-            std::vector<uint64_t> v(level + 1);
-            for (size_t l = 0; l <= level; ++l) v[l] = scaled_constant_mod(cf[0], static_cast<long double>(tgt), c.q[l]);
-            ops.scalar(out, nullptr, v, kScalarAdd);
-        }
-    } else {
-        if (level < eval_depth(degree)) throw std::invalid_argument("ckks_evalchebyshev: insufficient level for polynomial depth");
-        ChebyshevEval ev(c, ops, static_cast<long double>(default_scale));
-        out = ev.run(x, cf, degree, tgt);
-    }
+    CtBatch out = chebyshev(c, ops, x, coeffs, ncoeffs, target_scale, default_scale);
     ops.copy_out(out, out_b, out_a);
     *out_level = out.level;
     *out_scale = static_cast<double>(out.scale);

@@ -85,6 +85,8 @@ def lib() -> C.CDLL:
         L.wg_sparse_to_dense.argtypes = [vp, sz, vp, vp, vp, vp]
         L.wg_evalchebyshev.argtypes = [vp, sz, sz, C.c_double, vp, sz, C.c_double, C.c_double, vp, vp, vp, vp,
                                        C.POINTER(C.c_size_t), C.POINTER(C.c_double), vp]
+        L.wg_bootstrap_evalmod.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, sz, vp, vp, vp, vp, vp, vp,
+                                           C.POINTER(C.c_size_t), C.POINTER(C.c_double), vp]
         L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_batch_plan_launch.argtypes = [vp, vp]
         L.wg_batch_plan_destroy.argtypes = [vp]
@@ -215,6 +217,13 @@ class LtStage:
             self.close()
         except Exception:
             pass
+
+
+class BootstrapParams(C.Structure):
+    """wg_bootstrap_params."""
+    _fields_ = [("s2c_depth", C.c_size_t), ("depth", C.c_size_t), ("evalmod_log_scale", C.c_size_t),
+                ("double_angle", C.c_size_t), ("active_slots", C.c_size_t), ("slots", C.c_size_t),
+                ("scale", C.c_double)]
 
 
 class BatchPlan:
@@ -362,6 +371,24 @@ class Context:
                                       float(scale if default_scale is None else default_scale), pb.ctypes.data,
                                       pa.ctypes.data, ob.ctypes.data, oa.ctypes.data, C.byref(lvl), C.byref(sc),
                                       _stream(stream)))
+        return lvl.value, sc.value
+
+    def bootstrap_evalmod(self, params, s2c, c2s, coeffs, bs, as_, out0, out1, stream=None):
+        """EvalMod bootstrap of packed ciphertexts (device tensors with room for depth+1 limbs):
+        params a BootstrapParams, s2c / c2s lists of LtStage, out0 / out1 lists of (b, a) device
+        tensors.  Returns (out_level, out_scale)."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        hs = lambda sts: np.ascontiguousarray([st.h.value for st in sts], dtype=np.uint64)
+        ps, pc = hs(s2c), hs(c2s)
+        pb, pa = arr(bs), arr(as_)
+        o0b, o0a = arr([x[0] for x in out0]), arr([x[1] for x in out0])
+        o1b, o1a = arr([x[0] for x in out1]), arr([x[1] for x in out1])
+        cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        lvl, sc = C.c_size_t(), C.c_double()
+        _check(lib().wg_bootstrap_evalmod(self.h, C.byref(params), ps.ctypes.data, len(ps), pc.ctypes.data, len(pc),
+                                          cf.ctypes.data, len(cf), len(pb), pb.ctypes.data, pa.ctypes.data,
+                                          o0b.ctypes.data, o0a.ctypes.data, o1b.ctypes.data, o1a.ctypes.data,
+                                          C.byref(lvl), C.byref(sc), _stream(stream)))
         return lvl.value, sc.value
 
     def mul(self, level, b1, a1, b2, a2, c2, stream=None):

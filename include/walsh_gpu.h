@@ -215,6 +215,28 @@ void wg_lt_stage_destroy(wg_lt_stage* stage);
 int wg_lt_stage_apply(wg_context* ctx, const wg_lt_stage* stage, size_t count, uint64_t* const* b,
                       uint64_t* const* a, void* stream);
 
+/* EvalMod bootstrap of `count` packed ciphertexts (no counterpart as a batch: the reference
+ * boots one packed ciphertext per call): replaces ckks_batch_bootstrap_evalmod_from_complex_packed
+ * (src/ckks/operations/bootstrap/ckks_bootstrap_evalmod_inplace.cpp:416-434) -- SlotToCoeff
+ * with the `s2c` stages, dense-to-sparse switch, ModRaise to params->depth, sparse-to-dense
+ * switch, sparse-slot trace when active_slots < slots, CoeffToSlot with the `c2s` stages, the
+ * conjugate split (ct + conj, -i (ct - conj)), and EvalMod on both halves (Chebyshev series
+ * `coeffs` at scale 2^evalmod_log_scale, then double_angle doubling steps).  Inputs at level
+ * s2c_depth with scale params->scale; b[i] / a[i] need room for depth+1 limbs and are
+ * overwritten; the two results go to out0_* / out1_* (room for depth+1 limbs) at *out_level
+ * with scale *out_scale.  Needs the relinearisation, conjugation, both secret-switch keys and
+ * the stages' rotation keys. */
+typedef struct wg_bootstrap_params {
+    size_t s2c_depth, depth, evalmod_log_scale, double_angle, active_slots, slots;
+    double scale;
+} wg_bootstrap_params;
+int wg_bootstrap_evalmod(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
+                         size_t ns2c, const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs,
+                         size_t ncoeffs, size_t count, uint64_t* const* b, uint64_t* const* a,
+                         uint64_t* const* out0_b, uint64_t* const* out0_a, uint64_t* const* out1_b,
+                         uint64_t* const* out1_a, size_t* out_level, double* out_scale, void* stream);
+
+
 /* Rotation that allocates no device memory (no counterpart in the reference, whose
  * operations all allocate host vectors).  For callers that cannot call cudaMalloc when they
  * rotate: memory reserved up front by another allocator, work issued while a stream is being

@@ -429,6 +429,11 @@ class RefPlans:
         R.ref_dense_to_sparse.argtypes = [C.c_void_p, u64p, u64p]
         R.ref_sparse_to_dense.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
         R.ref_ctx_scale.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        R.ref_bts_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_size_t)] * 6 + [C.POINTER(C.c_double),
+                                                                               C.POINTER(C.c_size_t)]
+        R.ref_bts_evalmod_coeffs.argtypes = [C.c_void_p, f64p]
+        R.ref_bootstrap_evalmod.argtypes = [C.c_void_p, C.c_size_t, C.c_double, u64p, u64p, u64p, u64p, u64p, u64p,
+                                            C.POINTER(C.c_size_t), C.POINTER(C.c_double)]
         R.ref_evalchebyshev.argtypes = [C.c_void_p, C.c_size_t, C.c_double, f64p, C.c_size_t, C.c_double, u64p, u64p,
                                         C.POINTER(C.c_size_t), C.POINTER(C.c_double), u64p, u64p]
         R.ref_plan_stage_count.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
@@ -523,6 +528,31 @@ class RefPlans:
                "ref_evalchebyshev")
         m = (lvl.value + 1) * self.N
         return ob[:m].copy(), oa[:m].copy(), lvl.value, sc.value
+
+    def bts_info(self):
+        """EvalMod bootstrap parameters of a bootstrapping context, with its EvalMod series."""
+        v = [C.c_size_t() for _ in range(6)]
+        sc, nc = C.c_double(), C.c_size_t()
+        _check(ref().ref_bts_info(self.h, *[C.byref(x) for x in v], C.byref(sc), C.byref(nc)), "ref_bts_info")
+        coeffs = np.zeros(nc.value, np.float64)
+        _check(ref().ref_bts_evalmod_coeffs(self.h, coeffs), "ref_bts_evalmod_coeffs")
+        keys = ("s2c_depth", "depth", "evalmod_log_scale", "double_angle", "active_slots", "slots")
+        out = {k: x.value for k, x in zip(keys, v)}
+        out["scale"] = sc.value
+        out["coeffs"] = coeffs
+        return out
+
+    def bootstrap_evalmod(self, level, scale, b, a):
+        """The reference's EvalMod bootstrap of one packed ciphertext: (out0, out1, level, scale)."""
+        n = (self.N) * len(self.q)
+        bufs = [np.zeros(n, np.uint64) for _ in range(4)]
+        lvl, sc = C.c_size_t(), C.c_double()
+        m = (level + 1) * self.N
+        _check(ref().ref_bootstrap_evalmod(self.h, level, float(scale), np.ascontiguousarray(b[:m], dtype=np.uint64),
+                                           np.ascontiguousarray(a[:m], dtype=np.uint64), *bufs, C.byref(lvl),
+                                           C.byref(sc)), "ref_bootstrap_evalmod")
+        k = (lvl.value + 1) * self.N
+        return (bufs[0][:k].copy(), bufs[1][:k].copy()), (bufs[2][:k].copy(), bufs[3][:k].copy()), lvl.value, sc.value
 
     def dense_to_sparse(self, b, a):
         b = np.ascontiguousarray(b[: self.N], dtype=np.uint64).copy()

@@ -34,6 +34,9 @@
 #include "ckks_linear_transform.hpp"
 #include "ckks_modraise.hpp"
 #include "ckks_evalpoly.hpp"
+#include "ckks_encoding.hpp"
+#include "ckks_bootstrap_evalmod_inplace.hpp"
+#include "ckks_evalmod_scale_plan.hpp"
 #include "ckks_context.hpp"
 #include "ckks_conjugate.hpp"
 #include "ckks_keyswitch.hpp"
@@ -512,6 +515,65 @@ int ref_evalchebyshev(void* h, size_t level, double scale, const double* coeffs,
 // [interval_min, interval_max]).
 int ref_ctx_scale(void* h, double* scale) {
     return guarded([&] { *scale = (double)static_cast<RefCtx*>(h)->ctx.getParams().getScale(); });
+}
+
+// Parameters the EvalMod bootstrap reads (ckks_bootstrap_evalmod_inplace.cpp:246-416) and the
+// size of the EvalMod polynomial the context built.
+int ref_bts_info(void* h, size_t* s2c_depth, size_t* depth, size_t* evalmod_log_scale, size_t* double_angle,
+                 size_t* active_slots, size_t* slots, double* scale, size_t* ncoeffs) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const auto& p = c.getParams();
+        *s2c_depth = p.getBootstrapS2CDepth();
+        *depth = p.getDepth();
+        *evalmod_log_scale = ckks_evalmod_log_scale_bits(p);
+        *double_angle = p.getBootstrapEvalModDoubleAngle();
+        *active_slots = p.getBootstrapActiveSlotCount();
+        *slots = p.getSlots();
+        *scale = (double)p.getScale();
+        *ncoeffs = c.getEvalModPolynomial().chebyshev_coeffs.size();
+    });
+}
+
+int ref_bts_evalmod_coeffs(void* h, double* out) {
+    return guarded([&] {
+        const auto& v = static_cast<RefCtx*>(h)->ctx.getEvalModPolynomial().chebyshev_coeffs;
+        std::memcpy(out, v.data(), v.size() * sizeof(double));
+    });
+}
+
+// ckks_batch_bootstrap_evalmod_from_complex_packed (ckks_bootstrap_evalmod_inplace.cpp:416-434)
+// on a packed ciphertext at level `level` with scale `scale`: both outputs (b, a) with
+// (*out_level + 1) * N residues each.
+int ref_bootstrap_evalmod(void* h, size_t level, double scale, const uint64_t* b, const uint64_t* a,
+                          uint64_t* out0_b, uint64_t* out0_a, uint64_t* out1_b, uint64_t* out1_a, size_t* out_level,
+                          double* out_scale) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        CKKSCiphertext ct(N, copy_in(a, n), copy_in(b, n), (long double)scale, level);
+        auto outs = ckks_batch_bootstrap_evalmod_from_complex_packed(c, std::move(ct));
+        if (outs.first.getLevel() != outs.second.getLevel()) throw std::runtime_error("ref_bootstrap_evalmod: level mismatch");
+        *out_level = outs.first.getLevel();
+        *out_scale = (double)outs.first.getScale();
+        copy_out(outs.first.getB(), out0_b);
+        copy_out(outs.first.getA(), out0_a);
+        copy_out(outs.second.getB(), out1_b);
+        copy_out(outs.second.getA(), out1_a);
+    });
+}
+
+// ckks_encode of a constant slot vector (coefficient form, eval = false): the plaintext's
+// (level+1)*N residues and its Montgomery flag.
+int ref_encode_constant(void* h, double re, double im, double scale, size_t level, uint64_t* out, int* montgomery) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        MyVector<Complex> slots(c.getParams().getSlots(), Complex(re, im));
+        CKKSEncoding pt = ckks_encode(c, slots, scale, level, /*eval=*/false);
+        copy_out(pt.getPlaintext(), out);
+        *montgomery = pt.isMontgomeryForm() ? 1 : 0;
+    });
 }
 
 static const CKKSLinearTransformPlan& plan_of(void* h, int which) {
