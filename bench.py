@@ -403,8 +403,17 @@ def main():
     except (OSError, ValueError):
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
+    # DRAM traffic of the dominant kernel from the committed ncu capture summary (ratio of
+    # dram__bytes to algorithmic bytes, scaled to this launch size)
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "ntt_phase_traffic.json")))
+        if dom_name == "ntt" and dom["launches"]:
+            traffic = tr["dram_traffic_over_algorithmic"] * dom["bytes"] / dom["launches"]
+    except (OSError, ValueError, KeyError):
+        pass
     roofline = {"kernel": dom_name, "bound": "hbm", "achieved": dom["gbs"], "peak": hbm, "unit": "GB/s",
-                "frac": dom["gbs"] / hbm if dom["gbs"] else None, "traffic": None,
+                "frac": dom["gbs"] / hbm if dom["gbs"] else None, "traffic": traffic,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "avg_launch_us": 1000 * dom["ms"] / max(1, dom["launches"]),
                 "bytes_per_launch": dom["bytes"] / max(1, dom["launches"])}
