@@ -102,6 +102,13 @@ void bootstrap_evalmod(Context& c, const BootstrapParams& p, const LtStage* cons
                        uint64_t* const* out1_b, uint64_t* const* out1_a, size_t* out_level, double* out_scale,
                        cudaStream_t s);
 
+// Mask-packed Walsh S-box over `count` instances (wg_sbox.cu); in/out are bit-major arrays of
+// 8 * count ciphertext pointers.
+void walsh_sbox(Context& c, const BootstrapParams& p, const LtStage* const* s2c, size_t ns2c, const LtStage* const* c2s,
+                size_t nc2s, const double* coeffs, size_t ncoeffs, size_t block_count, size_t count, size_t level,
+                double scale, uint64_t* const* in_b, uint64_t* const* in_a, uint64_t* const* out_b,
+                uint64_t* const* out_a, size_t* out_level, double* out_scale, cudaStream_t s);
+
 // Hoisted rotations of one ciphertext; out [rotation][b, a][level+1][N] (wg_bsgs.cu).
 void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rots, size_t nrot,
                  uint64_t* out, cudaStream_t s);

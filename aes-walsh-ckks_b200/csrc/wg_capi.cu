@@ -416,6 +416,35 @@ int wg_evalchebyshev(wg_context* ctx, size_t count, size_t level, double scale, 
     });
 }
 
+static wg::BootstrapParams boot_args(const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
+                                     const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs,
+                                     std::vector<const wg::LtStage*>& vs, std::vector<const wg::LtStage*>& vc) {
+    check_ptr(params, "ckks EvalMod");
+    check_ptr(coeffs, "ckks EvalMod");
+    if ((ns2c && !s2c) || (nc2s && !c2s)) wg::fail(wg::kInvalid, "ckks EvalMod: null stage list");
+    vs.resize(ns2c);
+    vc.resize(nc2s);
+    for (size_t k = 0; k < ns2c; ++k) {
+        check_ptr(s2c[k], "ckks EvalMod");
+        vs[k] = s2c[k]->s;
+    }
+    for (size_t k = 0; k < nc2s; ++k) {
+        check_ptr(c2s[k], "ckks EvalMod");
+        vc[k] = c2s[k]->s;
+    }
+    wg::BootstrapParams bp;
+    bp.s2c_depth = params->s2c_depth;
+    bp.depth = params->depth;
+    bp.evalmod_log_scale = params->evalmod_log_scale;
+    bp.double_angle = params->double_angle;
+    bp.active_slots = params->active_slots;
+    bp.slots = params->slots;
+    bp.scale = params->scale;
+    if (bp.active_slots == 0 || bp.slots == 0 || bp.active_slots > bp.slots)
+        wg::fail(wg::kInvalid, "ckks EvalMod: invalid slot counts");
+    return bp;
+}
+
 int wg_bootstrap_evalmod(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
                          size_t ns2c, const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs,
                          size_t ncoeffs, size_t count, uint64_t* const* b, uint64_t* const* a,
@@ -423,35 +452,33 @@ int wg_bootstrap_evalmod(wg_context* ctx, const wg_bootstrap_params* params, con
                          uint64_t* const* out1_a, size_t* out_level, double* out_scale, void* stream) {
     return guard([&] {
         wg::Context& c = C(ctx);
-        check_ptr(params, "ckks EvalMod");
-        check_ptr(coeffs, "ckks EvalMod");
         check_ptr(out_level, "ckks EvalMod");
         check_ptr(out_scale, "ckks EvalMod");
         check_cts(c, count, b, a, "ckks EvalMod");
         check_cts(c, count, out0_b, out0_a, "ckks EvalMod");
         check_cts(c, count, out1_b, out1_a, "ckks EvalMod");
-        if ((ns2c && !s2c) || (nc2s && !c2s)) wg::fail(wg::kInvalid, "ckks EvalMod: null stage list");
-        std::vector<const wg::LtStage*> vs(ns2c), vc(nc2s);
-        for (size_t k = 0; k < ns2c; ++k) {
-            check_ptr(s2c[k], "ckks EvalMod");
-            vs[k] = s2c[k]->s;
-        }
-        for (size_t k = 0; k < nc2s; ++k) {
-            check_ptr(c2s[k], "ckks EvalMod");
-            vc[k] = c2s[k]->s;
-        }
-        wg::BootstrapParams bp;
-        bp.s2c_depth = params->s2c_depth;
-        bp.depth = params->depth;
-        bp.evalmod_log_scale = params->evalmod_log_scale;
-        bp.double_angle = params->double_angle;
-        bp.active_slots = params->active_slots;
-        bp.slots = params->slots;
-        bp.scale = params->scale;
-        if (bp.active_slots == 0 || bp.slots == 0 || bp.active_slots > bp.slots)
-            wg::fail(wg::kInvalid, "ckks EvalMod: invalid slot counts");
+        std::vector<const wg::LtStage*> vs, vc;
+        const wg::BootstrapParams bp = boot_args(params, s2c, ns2c, c2s, nc2s, coeffs, vs, vc);
         wg::bootstrap_evalmod(c, bp, vs.data(), ns2c, vc.data(), nc2s, coeffs, ncoeffs, count, b, a, out0_b, out0_a,
                               out1_b, out1_a, out_level, out_scale, S(stream));
+    });
+}
+
+int wg_walsh_sbox(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
+                  const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                  size_t block_count, size_t count, size_t level, double scale, uint64_t* const* in_b,
+                  uint64_t* const* in_a, uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level,
+                  double* out_scale, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(out_level, "ckks_walsh_sbox");
+        check_ptr(out_scale, "ckks_walsh_sbox");
+        check_cts(c, 8 * count, in_b, in_a, "ckks_walsh_sbox");
+        check_cts(c, 8 * count, out_b, out_a, "ckks_walsh_sbox");
+        std::vector<const wg::LtStage*> vs, vc;
+        const wg::BootstrapParams bp = boot_args(params, s2c, ns2c, c2s, nc2s, coeffs, vs, vc);
+        wg::walsh_sbox(c, bp, vs.data(), ns2c, vc.data(), nc2s, coeffs, ncoeffs, block_count, count, level, scale, in_b,
+                       in_a, out_b, out_a, out_level, out_scale, S(stream));
     });
 }
 

@@ -257,15 +257,20 @@ public:
 
     // ckks_mul_inplace(ct, Complex, scale): the slot-constant re + i im encodes (at scale
     // `scale`) to round(scale re) + round(scale im) X^(N/2); multiply every polynomial by it.
-    void mul_complex_constant(CtBatch& x, double re, double im, double scale) {
-        const size_t N = c_.N, L = x.level + 1;
-        const long long r0 = std::llround(scale * re), r1 = std::llround(scale * im);
+    // Evaluation-form plaintext of the slot constant re + i im at `scale`:
+    // round(scale re) + round(scale im) X^(N/2), reduced per limb, then NTT.
+    uint64_t* constant_plaintext(size_t L, double re, double im, double scale) {
+        const size_t N = c_.N;
+        const long double r0 = std::round(static_cast<long double>(scale) * re);
+        const long double r1 = std::round(static_cast<long double>(scale) * im);
         std::vector<uint64_t> host(L * N, 0);
         for (size_t l = 0; l < L; ++l) {
             const uint64_t q = c_.q[l];
-            auto modq = [q](long long v) {
-                const uint64_t m = (uint64_t)(v < 0 ? -v : v) % q;
-                return v < 0 && m ? q - m : m;
+            auto modq = [q](long double v) {
+                long double m = std::fmod(v, static_cast<long double>(q));
+                if (m < 0.0L) m += static_cast<long double>(q);
+                uint64_t r = static_cast<uint64_t>(m);
+                return r >= q ? r % q : r;
             };
             host[l * N] = modq(r0);
             host[l * N + N / 2] = modq(r1);
@@ -274,6 +279,12 @@ public:
         check_cuda(cudaMemcpyAsync(pt, host.data(), L * N * 8, cudaMemcpyHostToDevice, s_), "constant plaintext");
         check_cuda(cudaStreamSynchronize(s_), "constant plaintext");
         ntt_forward(c_, pt, (int)L, 1, 0, LimbMap{0, 0, 0}, s_);
+        return pt;
+    }
+
+    void mul_complex_constant(CtBatch& x, double re, double im, double scale) {
+        const size_t N = c_.N, L = x.level + 1;
+        uint64_t* pt = constant_plaintext(L, re, im, scale);
         std::vector<PmulJob> jobs;
         for (size_t i = 0; i < count_; ++i)
             for (int k = 0; k < x.np; ++k)
@@ -285,6 +296,35 @@ public:
         kb_pmul<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
         check_cuda(cudaGetLastError(), "evalpoly plaintext multiply");
     }
+
+    // b += the encoding of the slot constant re + i im at `scale` (closed form, as in
+    // mul_complex_constant), on every ciphertext of the batch.
+    void add_complex_constant(CtBatch& x, double re, double im, double scale) {
+        const size_t N = c_.N, L = x.level + 1;
+        uint64_t* pt = constant_plaintext(L, re, im, scale);
+        for (size_t i = 0; i < count_; ++i) add_sub(c_, x.level, x.p[i][0], pt, 1, 0, false, s_);
+    }
+
+    // x *= k (mod q) on every polynomial (ckks_mul_inplace(ct, int64_t)); scale unchanged.
+    void mul_int(CtBatch& x, int64_t k) {
+        if (k == 1) return;
+        if (k == 0) {
+            for (size_t i = 0; i < count_; ++i)
+                for (int j = 0; j < x.np; ++j)
+                    check_cuda(cudaMemsetAsync(x.p[i][j], 0, (x.level + 1) * c_.N * 8, s_), "zero");
+            return;
+        }
+        std::vector<uint64_t> v(x.level + 1);
+        for (size_t l = 0; l <= x.level; ++l) {
+            const int64_t q = (int64_t)c_.q[l];
+            int64_t r = k % q;
+            if (r < 0) r += q;
+            v[l] = (uint64_t)r;
+        }
+        scalar(x, nullptr, v, kScalarMul);
+    }
+
+    uint64_t* raw(size_t limbs) { return buffer(limbs, false); }
 
     CtBatch alloc(size_t level, int np) {
         CtBatch x;

@@ -87,6 +87,7 @@ def lib() -> C.CDLL:
                                        C.POINTER(C.c_size_t), C.POINTER(C.c_double), vp]
         L.wg_bootstrap_evalmod.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, sz, vp, vp, vp, vp, vp, vp,
                                            C.POINTER(C.c_size_t), C.POINTER(C.c_double), vp]
+        L.wg_walsh_sbox.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, sz, sz, sz, C.c_double, vp, vp, vp, vp, vp, vp, vp]
         L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_batch_plan_launch.argtypes = [vp, vp]
         L.wg_batch_plan_destroy.argtypes = [vp]
@@ -390,6 +391,27 @@ class Context:
                                           o0b.ctypes.data, o0a.ctypes.data, o1b.ctypes.data, o1a.ctypes.data,
                                           C.byref(lvl), C.byref(sc), _stream(stream)))
         return lvl.value, sc.value
+
+    def walsh_sbox(self, params, s2c, c2s, coeffs, block_count, level, scale, bits, out_bits, stream=None):
+        """Mask-packed Walsh S-box of len(bits) instances: bits[i] = 8 (b, a) device tensors of
+        instance i; out_bits likewise (room for depth+1 limbs).  Returns per-output-bit
+        (levels, scales)."""
+        count = len(bits)
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        hs = lambda sts: np.ascontiguousarray([st.h.value for st in sts], dtype=np.uint64)
+        ib = arr([bits[i][k][0] for k in range(8) for i in range(count)])
+        ia = arr([bits[i][k][1] for k in range(8) for i in range(count)])
+        ob = arr([out_bits[i][k][0] for k in range(8) for i in range(count)])
+        oa = arr([out_bits[i][k][1] for k in range(8) for i in range(count)])
+        ps, pc = hs(s2c), hs(c2s)
+        cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        lv = np.zeros(8, np.uintp)
+        sc = np.zeros(8, np.float64)
+        _check(lib().wg_walsh_sbox(self.h, C.byref(params), ps.ctypes.data, len(ps), pc.ctypes.data, len(pc),
+                                   cf.ctypes.data, len(cf), block_count, count, level, float(scale), ib.ctypes.data,
+                                   ia.ctypes.data, ob.ctypes.data, oa.ctypes.data, lv.ctypes.data, sc.ctypes.data,
+                                   _stream(stream)))
+        return [int(x) for x in lv], [float(x) for x in sc]
 
     def mul(self, level, b1, a1, b2, a2, c2, stream=None):
         _check(lib().wg_mul(self.h, level, _ptr(b1), _ptr(a1), _ptr(b2), _ptr(a2), _ptr(c2), _stream(stream)))

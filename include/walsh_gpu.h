@@ -236,6 +236,22 @@ int wg_bootstrap_evalmod(wg_context* ctx, const wg_bootstrap_params* params, con
                          uint64_t* const* out0_b, uint64_t* const* out0_a, uint64_t* const* out1_b,
                          uint64_t* const* out1_a, size_t* out_level, double* out_scale, void* stream);
 
+/* The AES S-box on lazy bits through its Walsh expansion, mask-packed, for `count` S-box
+ * instances at once (the reference runs one per call): replaces
+ * ckks_walsh_sbox_complex_blocks_mask_packed (src/ckks/operations/circuits/
+ * ckks_walsh_sbox.cpp:1286-1323).  in_b / in_a hold 8 * count device pointers, bit-major
+ * (bit k of instance i at [k * count + i]), each a ciphertext at `level` (= s2c_depth) with
+ * scale `scale` (= params->scale) and room for level+1 limbs; outputs likewise into out_b /
+ * out_a (room for depth+1 limbs), with each output bit's level and scale in out_level[8] /
+ * out_scale[8].  The bootstrap arguments are those of wg_bootstrap_evalmod; the rotation keys
+ * +-k * block_count (k = 1..29) must be installed besides the bootstrap's keys. */
+int wg_walsh_sbox(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
+                  const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                  size_t block_count, size_t count, size_t level, double scale, uint64_t* const* in_b,
+                  uint64_t* const* in_a, uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level,
+                  double* out_scale, void* stream);
+
+
 
 /* Rotation that allocates no device memory (no counterpart in the reference, whose
  * operations all allocate host vectors).  For callers that cannot call cudaMalloc when they

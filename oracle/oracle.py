@@ -429,6 +429,7 @@ class RefPlans:
         R.ref_dense_to_sparse.argtypes = [C.c_void_p, u64p, u64p]
         R.ref_sparse_to_dense.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
         R.ref_ctx_scale.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        R.ref_walsh_sbox.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_double, u64p, u64p, szp, f64p]
         R.ref_bts_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_size_t)] * 6 + [C.POINTER(C.c_double),
                                                                                C.POINTER(C.c_size_t)]
         R.ref_bts_evalmod_coeffs.argtypes = [C.c_void_p, f64p]
@@ -553,6 +554,23 @@ class RefPlans:
                                            C.byref(sc)), "ref_bootstrap_evalmod")
         k = (lvl.value + 1) * self.N
         return (bufs[0][:k].copy(), bufs[1][:k].copy()), (bufs[2][:k].copy(), bufs[3][:k].copy()), lvl.value, sc.value
+
+    def walsh_sbox(self, block_count, level, scale, bits):
+        """The reference's mask-packed Walsh S-box on 8 bit ciphertexts [(b, a)] x 8:
+        returns [(b, a, level, scale)] x 8."""
+        n = (level + 1) * self.N
+        flat = np.concatenate([np.concatenate([np.asarray(b[:n], np.uint64), np.asarray(a[:n], np.uint64)])
+                               for b, a in bits])
+        out = np.zeros(16 * len(self.q) * self.N, np.uint64)
+        lv = np.zeros(8, np.uintp)
+        sc = np.zeros(8, np.float64)
+        _check(ref().ref_walsh_sbox(self.h, block_count, level, float(scale), flat, out, lv, sc), "ref_walsh_sbox")
+        res, off = [], 0
+        for k in range(8):
+            m = (int(lv[k]) + 1) * self.N
+            res.append((out[off:off + m].copy(), out[off + m:off + 2 * m].copy(), int(lv[k]), float(sc[k])))
+            off += 2 * m
+        return res
 
     def dense_to_sparse(self, b, a):
         b = np.ascontiguousarray(b[: self.N], dtype=np.uint64).copy()

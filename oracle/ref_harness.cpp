@@ -34,6 +34,7 @@
 #include "ckks_linear_transform.hpp"
 #include "ckks_modraise.hpp"
 #include "ckks_evalpoly.hpp"
+#include "ckks_walsh_sbox.hpp"
 #include "ckks_encoding.hpp"
 #include "ckks_bootstrap_evalmod_inplace.hpp"
 #include "ckks_evalmod_scale_plan.hpp"
@@ -445,6 +446,11 @@ void* ref_walsh15_bts_create(void) {
         cfg.aes_walsh_params.enabled = false;
         cfg.q_mult_bits.clear();
         cfg.q_bits = {36, 61, 42, 42, 38, 38, 38, 38, 38, 38, 38, 50, 50};
+        // the mask-packed S-box's segment rotations (+-512 k) as the AES parameter set adds them
+        for (int64_t k = 1; k <= 31; ++k) {
+            cfg.rotate_values.push_back(512 * k);
+            cfg.rotate_values.push_back(-512 * k);
+        }
         cfg.mult_depth = 2;  // the EvalMod, S2C and C2S levels are the bootstrap depths here
         out = new RefCtx(CKKSParams(std::move(cfg)));
     });
@@ -573,6 +579,36 @@ int ref_encode_constant(void* h, double re, double im, double scale, size_t leve
         CKKSEncoding pt = ckks_encode(c, slots, scale, level, /*eval=*/false);
         copy_out(pt.getPlaintext(), out);
         *montgomery = pt.isMontgomeryForm() ? 1 : 0;
+    });
+}
+
+// ckks_walsh_sbox_complex_blocks_mask_packed (src/ckks/operations/circuits/ckks_walsh_sbox.cpp:
+// 1286-1323) on 8 bit ciphertexts at `level` with scale `scale`: in holds, per bit, b then a
+// ((level+1)*N words each); out receives, per output bit, b then a with
+// (out_levels[bit]+1)*N words each, packed back to back.
+int ref_walsh_sbox(void* h, size_t block_count, size_t level, double scale, const uint64_t* in, uint64_t* out,
+                   size_t* out_levels, double* out_scales) {
+    return guarded([&] {
+        auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        MyVector<CKKSCiphertext> bits;
+        for (size_t k = 0; k < 8; ++k)
+            bits.emplace_back(N, copy_in(in + (2 * k + 1) * n, n), copy_in(in + 2 * k * n, n), (long double)scale,
+                              level);
+        CKKSWalshSboxScratch scratch;
+        auto res = ckks_walsh_sbox_complex_blocks_mask_packed(c, std::move(bits), block_count, scratch);
+        if (res.size() != 8) throw std::runtime_error("ref_walsh_sbox: expected 8 output bits");
+        size_t off = 0;
+        for (size_t k = 0; k < 8; ++k) {
+            if (res[k].getNumPolys() != 2) throw std::runtime_error("ref_walsh_sbox: unexpected polynomial count");
+            out_levels[k] = res[k].getLevel();
+            out_scales[k] = (double)res[k].getScale();
+            copy_out(res[k].getB(), out + off);
+            off += res[k].getB().size();
+            copy_out(res[k].getA(), out + off);
+            off += res[k].getA().size();
+        }
     });
 }
 
