@@ -6,6 +6,7 @@
 
 #include "../../include/walsh_gpu.h"
 #include "wg_batch.hpp"
+#include "wg_encode.hpp"
 #include "wg_internal.hpp"
 
 namespace wg {
@@ -111,6 +112,14 @@ int wg_find_primes(const uint64_t* p_bits, size_t np, const uint64_t* q_bits, si
         wg::host::find_primes(pb, qb, N, p, q);
         std::memcpy(p_out, p.data(), np * 8);
         std::memcpy(q_out, q.data(), nq * 8);
+    });
+}
+
+int wg_encode_slots(uint64_t N, const double* re, const double* im, double scale, const uint64_t* moduli,
+                    size_t limbs, uint64_t* out) {
+    return guard([&] {
+        if (!re || !im || !moduli || !out) wg::fail(wg::kInvalid, "ckks_encode: null argument");
+        wg::host::encode_slots(N, re, im, scale, moduli, limbs, out);
     });
 }
 

@@ -1,0 +1,15 @@
+// Host-side CKKS slot encoding (wg_encode.cpp).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace wg {
+namespace host {
+
+// Coefficient-form plaintext of the N/2 slot values re[i] + i im[i] at `scale`, one limb per
+// modulus: out[l * N + k].
+void encode_slots(size_t N, const double* re, const double* im, double scale, const uint64_t* moduli, size_t limbs,
+                  uint64_t* out);
+
+}  // namespace host
+}  // namespace wg

@@ -57,6 +57,7 @@ def lib() -> C.CDLL:
         vp, sz, u64 = C.c_void_p, C.c_size_t, C.c_uint64
         L.wg_last_error.restype = C.c_char_p
         L.wg_version.restype = C.c_int
+        L.wg_encode_slots.argtypes = [u64, vp, vp, C.c_double, vp, sz, vp]
         L.wg_find_primes.argtypes = [vp, sz, vp, sz, u64, vp, vp]
         L.wg_ctx_create.argtypes = [u64, vp, sz, vp, sz, sz, C.c_int, C.POINTER(vp)]
         L.wg_ctx_destroy.argtypes = [vp]
@@ -181,6 +182,17 @@ def to_device(arr, device="cuda"):
     import torch
 
     return torch.from_numpy(_u64(arr).view(np.int64).copy()).to(device)
+
+
+def encode_slots(N, re, im, scale, moduli) -> np.ndarray:
+    """Host CKKS encoding of N/2 complex slots at `scale`: coefficient-form residues per modulus."""
+    r = np.ascontiguousarray(re, dtype=np.float64)
+    i = np.ascontiguousarray(im, dtype=np.float64)
+    m = _u64(moduli)
+    out = np.zeros(len(m) * int(N), np.uint64)
+    _check(lib().wg_encode_slots(int(N), r.ctypes.data, i.ctypes.data, float(scale), m.ctypes.data, len(m),
+                                 out.ctypes.data))
+    return out
 
 
 def to_host(t) -> np.ndarray:

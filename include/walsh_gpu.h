@@ -60,6 +60,12 @@ int wg_version(void);
 int wg_find_primes(const uint64_t* p_bits, size_t np, const uint64_t* q_bits, size_t nq,
                    uint64_t N, uint64_t* p_out, uint64_t* q_out);
 
+/* Host-side CKKS slot encoding (no GPU needed): the coefficient-form plaintext of the N/2 slot
+ * values re[i] + i im[i] at `scale`, reduced modulo each of moduli[0..limbs), out[l*N + k].
+ * Same residues as ckks_encode(..., eval = false), src/ckks/encoding/ckks_encoding.cpp:332-414. */
+int wg_encode_slots(uint64_t N, const double* re, const double* im, double scale, const uint64_t* moduli,
+                    size_t limbs, uint64_t* out);
+
 /* Device-resident context for one parameter set: Q moduli q[0..nq), P moduli p[0..np), dnum
  * digits.  Builds twiddles, ModUp/ModDown and rescale tables on `device`.
  * Replaces the table-building part of CKKSContext::CKKSContext,

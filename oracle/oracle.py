@@ -429,6 +429,7 @@ class RefPlans:
         R.ref_dense_to_sparse.argtypes = [C.c_void_p, u64p, u64p]
         R.ref_sparse_to_dense.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
         R.ref_ctx_scale.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        R.ref_encode.argtypes = [C.c_void_p, f64p, f64p, C.c_double, C.c_size_t, u64p]
         R.ref_walsh_sbox.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_double, u64p, u64p, szp, f64p]
         R.ref_bts_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_size_t)] * 6 + [C.POINTER(C.c_double),
                                                                                C.POINTER(C.c_size_t)]
@@ -554,6 +555,13 @@ class RefPlans:
                                            C.byref(sc)), "ref_bootstrap_evalmod")
         k = (lvl.value + 1) * self.N
         return (bufs[0][:k].copy(), bufs[1][:k].copy()), (bufs[2][:k].copy(), bufs[3][:k].copy()), lvl.value, sc.value
+
+    def encode(self, re, im, scale, level):
+        """The reference's ckks_encode, coefficient form, (level+1)*N residues."""
+        out = np.zeros((level + 1) * self.N, np.uint64)
+        _check(ref().ref_encode(self.h, np.ascontiguousarray(re, np.float64), np.ascontiguousarray(im, np.float64),
+                                float(scale), level, out), "ref_encode")
+        return out
 
     def walsh_sbox(self, block_count, level, scale, bits):
         """The reference's mask-packed Walsh S-box on 8 bit ciphertexts [(b, a)] x 8:

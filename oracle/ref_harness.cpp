@@ -47,6 +47,7 @@
 #include "ckks_rescale.hpp"
 #include "ckks_rotation.hpp"
 #include "ntt.hpp"
+#include "fft.hpp"
 #include "random.hpp"
 
 namespace {
@@ -608,6 +609,39 @@ int ref_walsh_sbox(void* h, size_t block_count, size_t level, double scale, cons
             off += res[k].getB().size();
             copy_out(res[k].getA(), out + off);
             off += res[k].getA().size();
+        }
+    });
+}
+
+// ckks_encode (coefficient form, eval = false) of N/2 slot values re[i] + i im[i].
+int ref_encode(void* h, const double* re, const double* im, double scale, size_t level, uint64_t* out) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t slots = c.getParams().getSlots();
+        MyVector<Complex> v(slots);
+        for (size_t i = 0; i < slots; ++i) v[i] = Complex(re[i], im[i]);
+        CKKSEncoding pt = ckks_encode(c, v, scale, level, /*eval=*/false);
+        if (pt.isMontgomeryForm()) throw std::runtime_error("ref_encode: unexpected Montgomery plaintext");
+        copy_out(pt.getPlaintext(), out);
+    });
+}
+
+// The context's FFT twiddles (interleaved re, im) and one fft_dif of `data` (in place).
+int ref_fft_probe(void* h, double* twiddles, double* data) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const auto& tw = c.getTwiddleFft();
+        const size_t N = c.getParams().getN();
+        for (size_t i = 0; i < N; ++i) {
+            twiddles[2 * i] = tw[i].real();
+            twiddles[2 * i + 1] = tw[i].imag();
+        }
+        MyVector<Complex> v(N);
+        for (size_t i = 0; i < N; ++i) v[i] = Complex(data[2 * i], data[2 * i + 1]);
+        fft_dif(v, tw, N);
+        for (size_t i = 0; i < N; ++i) {
+            data[2 * i] = v[i].real();
+            data[2 * i + 1] = v[i].imag();
         }
     });
 }
