@@ -94,20 +94,41 @@ struct BootstrapParams {
     size_t s2c_depth = 0, depth = 0, evalmod_log_scale = 0, double_angle = 0, active_slots = 0, slots = 0;
     double scale = 0.0;
 };
+// A SlotToCoeff plan for inputs whose scale is `ratio` times the parameter scale.
+struct S2cPlan {
+    uint64_t ratio = 1;
+    const LtStage* const* stages = nullptr;
+    size_t n = 0;
+};
 size_t lt_stage_level(const LtStage& st);
 bool lt_stage_rescales(const LtStage& st);
-void bootstrap_evalmod(Context& c, const BootstrapParams& p, const LtStage* const* s2c, size_t ns2c,
+void bootstrap_evalmod(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans,
                        const LtStage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs, size_t count,
-                       uint64_t* const* b, uint64_t* const* a, uint64_t* const* out0_b, uint64_t* const* out0_a,
-                       uint64_t* const* out1_b, uint64_t* const* out1_a, size_t* out_level, double* out_scale,
-                       cudaStream_t s);
+                       double in_scale, uint64_t* const* b, uint64_t* const* a, uint64_t* const* out0_b,
+                       uint64_t* const* out0_a, uint64_t* const* out1_b, uint64_t* const* out1_a, size_t* out_level,
+                       double* out_scale, cudaStream_t s);
 
 // Mask-packed Walsh S-box over `count` instances (wg_sbox.cu); in/out are bit-major arrays of
 // 8 * count ciphertext pointers.
-void walsh_sbox(Context& c, const BootstrapParams& p, const LtStage* const* s2c, size_t ns2c, const LtStage* const* c2s,
+void walsh_sbox(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
                 size_t nc2s, const double* coeffs, size_t ncoeffs, size_t block_count, size_t count, size_t level,
                 double scale, uint64_t* const* in_b, uint64_t* const* in_a, uint64_t* const* out_b,
                 uint64_t* const* out_a, size_t* out_level, double* out_scale, cudaStream_t s);
+
+// AES-128-CTR on lazy bits with the mask-packed Walsh S-box (wg_aes.cu).
+struct AesArgs {
+    const uint64_t* const* key_b = nullptr;  // 1408 round-key bit ciphertexts at key_level
+    const uint64_t* const* key_a = nullptr;
+    const double* key_scales = nullptr;
+    size_t key_level = 0;
+    const uint8_t* counters = nullptr;       // 2 * active_blocks blocks of 16 bytes
+    const uint8_t* ciphertexts = nullptr;
+    size_t active_blocks = 0;
+    size_t packing_block_count = 0, packed_segment_count = 0;
+};
+void aes_ctr_walsh(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
+                   size_t nc2s, const double* coeffs, size_t ncoeffs, const AesArgs& args, uint64_t* const* out_b,
+                   uint64_t* const* out_a, size_t* out_level, double* out_scale, cudaStream_t s);
 
 // Hoisted rotations of one ciphertext; out [rotation][b, a][level+1][N] (wg_bsgs.cu).
 void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rots, size_t nrot,

@@ -468,7 +468,8 @@ int wg_bootstrap_evalmod(wg_context* ctx, const wg_bootstrap_params* params, con
         check_cts(c, count, out1_b, out1_a, "ckks EvalMod");
         std::vector<const wg::LtStage*> vs, vc;
         const wg::BootstrapParams bp = boot_args(params, s2c, ns2c, c2s, nc2s, coeffs, vs, vc);
-        wg::bootstrap_evalmod(c, bp, vs.data(), ns2c, vc.data(), nc2s, coeffs, ncoeffs, count, b, a, out0_b, out0_a,
+        const wg::S2cPlan plan{1, vs.data(), ns2c};
+        wg::bootstrap_evalmod(c, bp, &plan, 1, vc.data(), nc2s, coeffs, ncoeffs, count, bp.scale, b, a, out0_b, out0_a,
                               out1_b, out1_a, out_level, out_scale, S(stream));
     });
 }
@@ -486,8 +487,50 @@ int wg_walsh_sbox(wg_context* ctx, const wg_bootstrap_params* params, const wg_l
         check_cts(c, 8 * count, out_b, out_a, "ckks_walsh_sbox");
         std::vector<const wg::LtStage*> vs, vc;
         const wg::BootstrapParams bp = boot_args(params, s2c, ns2c, c2s, nc2s, coeffs, vs, vc);
-        wg::walsh_sbox(c, bp, vs.data(), ns2c, vc.data(), nc2s, coeffs, ncoeffs, block_count, count, level, scale, in_b,
-                       in_a, out_b, out_a, out_level, out_scale, S(stream));
+        const wg::S2cPlan plan{1, vs.data(), ns2c};
+        wg::walsh_sbox(c, bp, &plan, 1, vc.data(), nc2s, coeffs, ncoeffs, block_count, count, level, scale, in_b, in_a,
+                       out_b, out_a, out_level, out_scale, S(stream));
+    });
+}
+
+int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
+                     size_t ns2c, const wg_lt_stage* const* s2c_x2, size_t ns2c_x2,
+                     const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                     size_t packing_block_count, size_t packed_segment_count, const uint64_t* const* key_b,
+                     const uint64_t* const* key_a, const double* key_scales, size_t key_level,
+                     const uint8_t* counters, const uint8_t* ciphertexts, size_t active_blocks,
+                     uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                     void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(out_level, "ckks_aes_walsh");
+        check_ptr(out_scale, "ckks_aes_walsh");
+        check_cts(c, 128, out_b, out_a, "ckks_aes_walsh");
+        if (!key_b || !key_a) wg::fail(wg::kInvalid, "ckks_aes_walsh: null key bits");
+        for (size_t k = 0; k < 1408; ++k) {
+            check_ptr(key_b[k], "ckks_aes_walsh");
+            check_ptr(key_a[k], "ckks_aes_walsh");
+        }
+        std::vector<const wg::LtStage*> vs, vc, vs2(ns2c_x2);
+        const wg::BootstrapParams bp = boot_args(params, s2c, ns2c, c2s, nc2s, coeffs, vs, vc);
+        if (ns2c_x2 && !s2c_x2) wg::fail(wg::kInvalid, "ckks_aes_walsh: null stage list");
+        for (size_t k = 0; k < ns2c_x2; ++k) {
+            check_ptr(s2c_x2[k], "ckks_aes_walsh");
+            vs2[k] = s2c_x2[k]->s;
+        }
+        const wg::S2cPlan plans[2] = {{1, vs.data(), ns2c}, {2, vs2.data(), ns2c_x2}};
+        wg::AesArgs a;
+        a.key_b = key_b;
+        a.key_a = key_a;
+        a.key_scales = key_scales;
+        a.key_level = key_level;
+        a.counters = counters;
+        a.ciphertexts = ciphertexts;
+        a.active_blocks = active_blocks;
+        a.packing_block_count = packing_block_count;
+        a.packed_segment_count = packed_segment_count;
+        wg::aes_ctr_walsh(c, bp, plans, ns2c_x2 ? 2 : 1, vc.data(), nc2s, coeffs, ncoeffs, a, out_b, out_a, out_level,
+                          out_scale, S(stream));
     });
 }
 

@@ -282,6 +282,35 @@ public:
         return pt;
     }
 
+    // Evaluation-form plaintext from coefficient-form residues (L limbs): upload, then NTT.
+    uint64_t* upload_plain(const uint64_t* coeff, size_t L) {
+        uint64_t* pt = buffer(L, false);
+        check_cuda(cudaMemcpyAsync(pt, coeff, L * c_.N * 8, cudaMemcpyHostToDevice, s_), "plaintext upload");
+        check_cuda(cudaStreamSynchronize(s_), "plaintext upload");
+        ntt_forward(c_, pt, (int)L, 1, 0, LimbMap{0, 0, 0}, s_);
+        return pt;
+    }
+
+    // b += pt (evaluation form, x.level+1 limbs) on every ciphertext (ckks_add_inplace(ct, pt))
+    void add_plain(CtBatch& x, const uint64_t* pt) {
+        for (size_t i = 0; i < count_; ++i) add_sub(c_, x.level, x.p[i][0], pt, 1, 0, false, s_);
+    }
+
+    // every polynomial *= pt pointwise (ckks_mul_inplace(ct, pt)); scale left to the caller
+    void mul_plain(CtBatch& x, const uint64_t* pt) {
+        const size_t N = c_.N, L = x.level + 1;
+        std::vector<PmulJob> jobs;
+        for (size_t i = 0; i < count_; ++i)
+            for (int k = 0; k < x.np; ++k)
+                for (size_t l = 0; l < L; ++l) jobs.push_back({x.p[i][k] + l * N, pt + l * N, (int)l, 0});
+        JobTable t;
+        const PmulJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 3.0, s_);
+        kb_pmul<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        check_cuda(cudaGetLastError(), "plaintext multiply");
+    }
+
     void mul_complex_constant(CtBatch& x, double re, double im, double scale) {
         const size_t N = c_.N, L = x.level + 1;
         uint64_t* pt = constant_plaintext(L, re, im, scale);
@@ -325,6 +354,30 @@ public:
     }
 
     uint64_t* raw(size_t limbs) { return buffer(limbs, false); }
+
+    // ckks_rotate_inplace by r on every ciphertext of the batch (key switch, then automorphism)
+    void rotate(CtBatch& x, int64_t r) {
+        const int64_t slots = (int64_t)(c_.N / 2);
+        int64_t n = r % slots;
+        if (n < 0) n += slots;
+        if (n == 0) return;
+        const KeyEntry& k = c_.key(WG_KEY_ROTATION, n);
+        std::vector<KsItem> items(count_);
+        for (size_t i = 0; i < count_; ++i) {
+            KsItem& it = items[i];
+            it.level = x.level;
+            it.key_term = x.p[i][1];
+            it.key = &k;
+            it.b_in = x.p[i][0];
+            it.a_in = x.p[i][1];
+            it.b = x.p[i][0];
+            it.a = x.p[i][1];
+            it.b_add = 1;
+            it.a_add = 0;
+            it.galois = host::powmod(5, (uint64_t)n, 2 * c_.N);
+        }
+        batch_keyswitch(c_, items.data(), count_, s_);
+    }
 
     CtBatch alloc(size_t level, int np) {
         CtBatch x;

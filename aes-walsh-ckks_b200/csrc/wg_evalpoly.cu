@@ -544,14 +544,28 @@ void mul_real_to_scale(Context& c, DeviceOps& ops, CtBatch& x, double scalar, lo
 // trace, CoeffToSlot, conjugate split into (ct + conj) and -i (ct - conj), then EvalMod (the
 // Chebyshev series at scale 2^evalmod_log_scale, then the double-angle steps) on both halves
 // as one batch of 2 x count.  b[i] / a[i] need room for depth+1 limbs and are overwritten.
-void bootstrap_evalmod(Context& c, const BootstrapParams& p, const LtStage* const* s2c, size_t ns2c,
+void bootstrap_evalmod(Context& c, const BootstrapParams& p, const S2cPlan* plans, size_t nplans,
                        const LtStage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs, size_t count,
-                       uint64_t* const* b, uint64_t* const* a, uint64_t* const* out0_b, uint64_t* const* out0_a,
-                       uint64_t* const* out1_b, uint64_t* const* out1_a, size_t* out_level, double* out_scale,
-                       cudaStream_t s) {
+                       double in_scale, uint64_t* const* b, uint64_t* const* a, uint64_t* const* out0_b,
+                       uint64_t* const* out0_a, uint64_t* const* out1_b, uint64_t* const* out1_a, size_t* out_level,
+                       double* out_scale, cudaStream_t s) {
     if (count == 0) return;
     if (p.s2c_depth == 0 || p.depth >= c.nq || p.depth < p.s2c_depth)
         throw std::invalid_argument("ckks EvalMod: invalid bootstrap depths");
+    // evalmod_input_scale_ratio: the SlotToCoeff plan depends on input scale / parameter scale
+    const long double s2c_target = p.scale, input = in_scale;
+    if (!std::isfinite(input) || input <= 0.0L) throw std::invalid_argument("ckks EvalMod: invalid ciphertext scale");
+    if (input < s2c_target) throw std::invalid_argument("ckks EvalMod: EvalMod input scale is below the S2C target scale");
+    const long double ratio = input / s2c_target, rounded = std::round(ratio);
+    if (rounded < 1.0L || rounded > static_cast<long double>(std::numeric_limits<uint64_t>::max()) ||
+        std::abs(ratio - rounded) > std::max<long double>(1.0L, std::abs(ratio)) * 1e-3L)
+        throw std::invalid_argument("ckks EvalMod: EvalMod entry scale ratio is not an exact integer");
+    const S2cPlan* plan = nullptr;
+    for (size_t k = 0; k < nplans; ++k)
+        if (plans[k].ratio == static_cast<uint64_t>(rounded)) plan = &plans[k];
+    if (!plan) throw std::invalid_argument("ckks EvalMod: no SlotToCoeff plan for this input scale ratio");
+    const LtStage* const* s2c = plan->stages;
+    const size_t ns2c = plan->n;
     const size_t N = c.N;
     size_t level = p.s2c_depth;
     // SlotToCoeff

@@ -401,7 +401,7 @@ private:
 
 }  // namespace
 
-void walsh_sbox(Context& c, const BootstrapParams& p, const LtStage* const* s2c, size_t ns2c, const LtStage* const* c2s,
+void walsh_sbox(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
                 size_t nc2s, const double* coeffs, size_t ncoeffs, size_t block_count, size_t count, size_t level,
                 double scale, uint64_t* const* in_b, uint64_t* const* in_a, uint64_t* const* out_b,
                 uint64_t* const* out_a, size_t* out_level, double* out_scale, cudaStream_t s) {
@@ -433,10 +433,8 @@ void walsh_sbox(Context& c, const BootstrapParams& p, const LtStage* const* s2c,
     }
     size_t blv = 0;
     double bsc = 0.0;
-    if (!close_ld(static_cast<long double>(scale), static_cast<long double>(p.scale), 1e-3L))
-        throw std::invalid_argument("ckks_walsh_sbox: bootstrap entry scale must equal the parameter scale");
-    bootstrap_evalmod(c, p, s2c, ns2c, c2s, nc2s, coeffs, ncoeffs, count, pb.data(), pa.data(), o0b.data(), o0a.data(),
-                      o1b.data(), o1a.data(), &blv, &bsc, s);
+    bootstrap_evalmod(c, p, s2c, nplans, c2s, nc2s, coeffs, ncoeffs, count, static_cast<double>(packed.scale),
+                      pb.data(), pa.data(), o0b.data(), o0a.data(), o1b.data(), o1a.data(), &blv, &bsc, s);
     CtBatch lane0 = ops.wrap(o0b.data(), o0a.data(), blv, bsc);
     CtBatch lane1 = ops.wrap(o1b.data(), o1a.data(), blv, bsc);
     lane0.cap = lane1.cap = full;

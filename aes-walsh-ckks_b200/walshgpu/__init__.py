@@ -89,6 +89,8 @@ def lib() -> C.CDLL:
         L.wg_bootstrap_evalmod.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, sz, vp, vp, vp, vp, vp, vp,
                                            C.POINTER(C.c_size_t), C.POINTER(C.c_double), vp]
         L.wg_walsh_sbox.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, sz, sz, sz, C.c_double, vp, vp, vp, vp, vp, vp, vp]
+        L.wg_aes_ctr_walsh.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, C.c_char_p,
+                                       C.c_char_p, sz, vp, vp, vp, vp, vp]
         L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_batch_plan_launch.argtypes = [vp, vp]
         L.wg_batch_plan_destroy.argtypes = [vp]
@@ -423,6 +425,27 @@ class Context:
                                    cf.ctypes.data, len(cf), block_count, count, level, float(scale), ib.ctypes.data,
                                    ia.ctypes.data, ob.ctypes.data, oa.ctypes.data, lv.ctypes.data, sc.ctypes.data,
                                    _stream(stream)))
+        return [int(x) for x in lv], [float(x) for x in sc]
+
+    def aes_ctr_walsh(self, params, s2c, s2c_x2, c2s, coeffs, packing_block_count, packed_segment_count, key_bits,
+                      key_scales, key_level, counters, ciphertexts, active_blocks, out_bits, stream=None):
+        """Homomorphic AES-128-CTR on lazy bits: key_bits = 1408 (b, a) device tensors, counters /
+        ciphertexts = bytes of 2 * active_blocks blocks, out_bits = 128 (b, a) device tensors.
+        Returns (levels, scales) of the 128 output bits."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        hs = lambda sts: np.ascontiguousarray([st.h.value for st in sts], dtype=np.uint64)
+        kb, ka = arr([x[0] for x in key_bits]), arr([x[1] for x in key_bits])
+        ob, oa = arr([x[0] for x in out_bits]), arr([x[1] for x in out_bits])
+        ps, ps2, pc = hs(s2c), hs(s2c_x2), hs(c2s)
+        cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        ks = np.ascontiguousarray(key_scales, dtype=np.float64)
+        lv = np.zeros(128, np.uintp)
+        sc = np.zeros(128, np.float64)
+        _check(lib().wg_aes_ctr_walsh(self.h, C.byref(params), ps.ctypes.data, len(ps), ps2.ctypes.data, len(ps2),
+                                      pc.ctypes.data, len(pc), cf.ctypes.data, len(cf), packing_block_count,
+                                      packed_segment_count, kb.ctypes.data, ka.ctypes.data, ks.ctypes.data, key_level,
+                                      bytes(counters), bytes(ciphertexts), active_blocks, ob.ctypes.data,
+                                      oa.ctypes.data, lv.ctypes.data, sc.ctypes.data, _stream(stream)))
         return [int(x) for x in lv], [float(x) for x in sc]
 
     def mul(self, level, b1, a1, b2, a2, c2, stream=None):

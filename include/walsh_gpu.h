@@ -257,6 +257,31 @@ int wg_walsh_sbox(wg_context* ctx, const wg_bootstrap_params* params, const wg_l
                   uint64_t* const* in_a, uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level,
                   double* out_scale, void* stream);
 
+/* AES-128 in CTR mode on lazy bits, evaluated on the device: replaces
+ * ckks_aes_ctr_walsh_sbox_complex_blocks (src/ckks/operations/circuits/aes/
+ * ckks_aes_ctr_walsh_sbox.cpp:1037-1051).  Each of the 128 state-bit ciphertexts carries, in
+ * slot s < active_blocks, block s in its real part and block active_blocks + s in its
+ * imaginary part.  key_b / key_a: the 1408 encrypted expanded-key bits (device pointers, level
+ * key_level = s2c_depth + 1) with their scales; counters / ciphertexts: 2 * active_blocks public
+ * 16-byte blocks (host memory).  Rounds 1..10 (active-slot mask, SubBytes by the mask-packed
+ * Walsh S-box on all 16 bytes at once, ShiftRows, MixColumns except in round 10,
+ * AddRoundKey), the public ciphertext XOR and the final binary refresh (packed bootstraps);
+ * the 128 results go to out_b / out_a (room for depth+1 limbs) with levels and scales.
+ * SlotToCoeff needs a plan per bootstrap input scale: s2c for inputs at the parameter scale,
+ * s2c_x2 for inputs at twice it (the state after the first S-box); packing_block_count and
+ * packed_segment_count are the parameter set's AES-Walsh packing (512 and 32 for walsh15).
+ * Keys: relinearisation, conjugation, both secret switches, all plan rotations and
+ * +-k * packing_block_count. */
+int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
+                     size_t ns2c, const wg_lt_stage* const* s2c_x2, size_t ns2c_x2,
+                     const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                     size_t packing_block_count, size_t packed_segment_count, const uint64_t* const* key_b,
+                     const uint64_t* const* key_a, const double* key_scales, size_t key_level,
+                     const uint8_t* counters, const uint8_t* ciphertexts, size_t active_blocks,
+                     uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                     void* stream);
+
+
 
 
 /* Rotation that allocates no device memory (no counterpart in the reference, whose

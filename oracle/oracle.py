@@ -429,6 +429,11 @@ class RefPlans:
         R.ref_dense_to_sparse.argtypes = [C.c_void_p, u64p, u64p]
         R.ref_sparse_to_dense.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
         R.ref_ctx_scale.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        R.ref_build_scaled_s2c.argtypes = [C.c_void_p, C.c_uint64]
+        R.ref_aes_key_bits.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, u64p, f64p, C.POINTER(C.c_size_t)]
+        R.ref_aes_ctr.argtypes = [C.c_void_p, u64p, f64p, C.c_size_t, C.c_char_p, C.c_char_p, C.c_size_t, u64p, szp,
+                                  f64p]
+        R.ref_decrypt.argtypes = [C.c_void_p, C.c_size_t, C.c_double, u64p, u64p, f64p, f64p]
         R.ref_encode.argtypes = [C.c_void_p, f64p, f64p, C.c_double, C.c_size_t, u64p]
         R.ref_walsh_sbox.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_double, u64p, u64p, szp, f64p]
         R.ref_bts_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_size_t)] * 6 + [C.POINTER(C.c_double),
@@ -555,6 +560,46 @@ class RefPlans:
                                            C.byref(sc)), "ref_bootstrap_evalmod")
         k = (lvl.value + 1) * self.N
         return (bufs[0][:k].copy(), bufs[1][:k].copy()), (bufs[2][:k].copy(), bufs[3][:k].copy()), lvl.value, sc.value
+
+    def build_scaled_s2c(self, ratio):
+        """Build the SlotToCoeff plan for inputs at `ratio` x the parameter scale; its stages are
+        then plan 100 + ratio for stages() / stage()."""
+        _check(ref().ref_build_scaled_s2c(self.h, int(ratio)), "ref_build_scaled_s2c")
+        return 100 + int(ratio)
+
+    def aes_key_bits(self, expanded_key, active_blocks):
+        """The reference's encrypted expanded-key bits: (flat [bit][b, a][limbs][N], scales, key level)."""
+        kl = 2
+        out = np.zeros(1408 * 2 * (kl + 1) * self.N, np.uint64)
+        scales = np.zeros(1408, np.float64)
+        lv = C.c_size_t()
+        _check(ref().ref_aes_key_bits(self.h, bytes(expanded_key), active_blocks, out, scales, C.byref(lv)),
+               "ref_aes_key_bits")
+        assert lv.value == kl
+        return out, scales, lv.value
+
+    def aes_ctr(self, key_flat, key_scales, key_level, counters, ciphertexts, active_blocks):
+        """The reference's AES-CTR on lazy bits: 128 x (b, a, level, scale)."""
+        out = np.zeros(128 * 2 * len(self.q) * self.N, np.uint64)
+        lv = np.zeros(128, np.uintp)
+        sc = np.zeros(128, np.float64)
+        _check(ref().ref_aes_ctr(self.h, key_flat, np.ascontiguousarray(key_scales, np.float64), key_level,
+                                 bytes(counters), bytes(ciphertexts), active_blocks, out, lv, sc), "ref_aes_ctr")
+        res, off = [], 0
+        for k in range(128):
+            m = (int(lv[k]) + 1) * self.N
+            res.append((out[off:off + m].copy(), out[off + m:off + 2 * m].copy(), int(lv[k]), float(sc[k])))
+            off += 2 * m
+        return res
+
+    def decrypt(self, level, scale, b, a):
+        """The reference's ckks_decrypt: complex slot values."""
+        re = np.zeros(self.N // 2)
+        im = np.zeros(self.N // 2)
+        n = (level + 1) * self.N
+        _check(ref().ref_decrypt(self.h, level, float(scale), np.ascontiguousarray(b[:n], np.uint64),
+                                 np.ascontiguousarray(a[:n], np.uint64), re, im), "ref_decrypt")
+        return re + 1j * im
 
     def encode(self, re, im, scale, level):
         """The reference's ckks_encode, coefficient form, (level+1)*N residues."""

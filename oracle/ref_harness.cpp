@@ -20,6 +20,8 @@
 //                                      src/ckks/operations/keyswitch/ckks_keyswitch.cpp:344,1072
 
 #include <algorithm>
+#include <map>
+#include <array>
 #include <chrono>
 #include <cstdint>
 #include <cstring>
@@ -34,6 +36,8 @@
 #include "ckks_linear_transform.hpp"
 #include "ckks_modraise.hpp"
 #include "ckks_evalpoly.hpp"
+#include "ckks_bootstrap_dft.hpp"
+#include "ckks_aes_ctr_walsh_sbox.hpp"
 #include "ckks_walsh_sbox.hpp"
 #include "ckks_encoding.hpp"
 #include "ckks_bootstrap_evalmod_inplace.hpp"
@@ -112,6 +116,7 @@ namespace {
 
 struct RefCtx {
     CKKSContext ctx;
+    std::map<uint64_t, CKKSLinearTransformPlan> scaled_s2c;  // SlotToCoeff plans by input scale ratio
     explicit RefCtx(CKKSParams p) : ctx(std::move(p)) {}
 };
 
@@ -444,7 +449,7 @@ void* ref_walsh15_bts_create(void) {
         cfg.bts_keys = true;
         cfg.s2c_ptxt = true;
         cfg.c2s_ptxt = true;
-        cfg.aes_walsh_params.enabled = false;
+        cfg.aes_walsh_params.enabled = true;
         cfg.q_mult_bits.clear();
         cfg.q_bits = {36, 61, 42, 42, 38, 38, 38, 38, 38, 38, 38, 50, 50};
         // the mask-packed S-box's segment rotations (+-512 k) as the AES parameter set adds them
@@ -646,9 +651,103 @@ int ref_fft_probe(void* h, double* twiddles, double* data) {
     });
 }
 
+// ckks_aes128_encrypt_expanded_round_key_bits_walsh_complex_blocks (ckks_aes_ctr_walsh_sbox.cpp:
+// 981-1035): the 1408 encrypted round-key bits, each (b, a) at *key_level, back to back, with
+// their scales.
+int ref_aes_key_bits(void* h, const uint8_t* expanded_key, size_t active_blocks, uint64_t* out, double* scales,
+                     size_t* key_level) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        std::array<uint8_t, 176> ek{};
+        std::memcpy(ek.data(), expanded_key, 176);
+        auto bits = ckks_aes128_encrypt_expanded_round_key_bits_walsh_complex_blocks(c, ek, active_blocks);
+        size_t off = 0;
+        for (size_t k = 0; k < bits.size(); ++k) {
+            copy_out(bits[k].getB(), out + off);
+            off += bits[k].getB().size();
+            copy_out(bits[k].getA(), out + off);
+            off += bits[k].getA().size();
+            scales[k] = (double)bits[k].getScale();
+        }
+        *key_level = bits.front().getLevel();
+    });
+}
+
+// ckks_aes_ctr_walsh_sbox_complex_blocks (ckks_aes_ctr_walsh_sbox.cpp:1037-1051) on the given
+// key-bit ciphertexts; the 128 output bits (b, a) back to back with their levels and scales.
+int ref_aes_ctr(void* h, const uint64_t* key, const double* key_scales, size_t key_level, const uint8_t* counters,
+                const uint8_t* ciphertexts, size_t active_blocks, uint64_t* out, size_t* out_levels,
+                double* out_scales) {
+    return guarded([&] {
+        auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (key_level + 1) * N;
+        MyVector<CKKSCiphertext> kb;
+        for (size_t k = 0; k < 1408; ++k)
+            kb.emplace_back(N, copy_in(key + (2 * k + 1) * n, n), copy_in(key + 2 * k * n, n),
+                            (long double)key_scales[k], key_level);
+        std::vector<std::array<uint8_t, 16>> ctr(2 * active_blocks), ctx(2 * active_blocks);
+        for (size_t i = 0; i < 2 * active_blocks; ++i) {
+            std::memcpy(ctr[i].data(), counters + 16 * i, 16);
+            std::memcpy(ctx[i].data(), ciphertexts + 16 * i, 16);
+        }
+        auto res = ckks_aes_ctr_walsh_sbox_complex_blocks(c, kb, std::span<const std::array<uint8_t, 16>>(ctr),
+                                                          std::span<const std::array<uint8_t, 16>>(ctx));
+        size_t off = 0;
+        for (size_t k = 0; k < res.size(); ++k) {
+            out_levels[k] = res[k].getLevel();
+            out_scales[k] = (double)res[k].getScale();
+            copy_out(res[k].getB(), out + off);
+            off += res[k].getB().size();
+            copy_out(res[k].getA(), out + off);
+            off += res[k].getA().size();
+        }
+    });
+}
+
+// ckks_decrypt (slots) of a 2-polynomial ciphertext: re / im of the N/2 slots.
+int ref_decrypt(void* h, size_t level, double scale, const uint64_t* b, const uint64_t* a, double* re, double* im) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        CKKSCiphertext ct(N, copy_in(a, n), copy_in(b, n), (long double)scale, level);
+        auto v = ckks_decrypt(c, ct);
+        for (size_t i = 0; i < v.size(); ++i) {
+            re[i] = v[i].real();
+            im[i] = v[i].imag();
+        }
+    });
+}
+
+// The SlotToCoeff plan the EvalMod bootstrap uses for an input whose scale is `ratio` times the
+// parameter scale, built from the same literal as get_scaled_s2c_plan
+// (ckks_bootstrap_evalmod_inplace.cpp:115-154); afterwards plan index 100 + ratio selects it.
+int ref_build_scaled_s2c(void* h, uint64_t ratio) {
+    return guarded([&] {
+        auto* r = static_cast<RefCtx*>(h);
+        const auto& p = r->ctx.getParams();
+        const size_t d = p.getBootstrapS2CDepth();
+        CKKSBootstrapDftMatrixLiteral lit;
+        lit.type = CKKSBootstrapDftType::SlotsToCoeffs;
+        lit.level = d;
+        lit.baby_step_count = p.getBootstrapLinearTransformBsgsBabyStepCounts()[0];
+        lit.log_bsgs_ratio = p.getBootstrapS2CLogBsgsRatio();
+        lit.stage_count = d;
+        lit.log_plaintext_scale_groups = p.getBootstrapS2CLogPlaintextScales();
+        lit.merge_depths = p.getBootstrapS2CMergeDepths();
+        lit.active_slots = p.getBootstrapActiveSlotCount();
+        lit.transform_scale = (static_cast<double>(p.getModuli()[0]) * 0.5) / (p.getScale() * static_cast<double>(ratio));
+        lit.plaintext_scale = static_cast<double>(p.getModuli()[d]);
+        lit.rescale_after_each_stage = true;
+        r->scaled_s2c.insert_or_assign(ratio, ckks_generate_bootstrap_dft_plan(r->ctx, lit));
+    });
+}
+
 static const CKKSLinearTransformPlan& plan_of(void* h, int which) {
-    const auto& c = static_cast<RefCtx*>(h)->ctx;
-    return which == 0 ? c.getEvalModS2CPlan() : c.getEvalModScaledC2SPlan();
+    auto* r = static_cast<RefCtx*>(h);
+    if (which >= 100) return r->scaled_s2c.at((uint64_t)(which - 100));
+    return which == 0 ? r->ctx.getEvalModS2CPlan() : r->ctx.getEvalModScaledC2SPlan();
 }
 
 int ref_plan_stage_count(void* h, int which, size_t* stages, int* use_qp) {

@@ -1,0 +1,78 @@
+"""Homomorphic AES-128-CTR (walsh15, 1024 blocks: 512 complex slots x 2 lanes) on the device
+against the reference's ckks_aes_ctr_walsh_sbox_complex_blocks on the same encrypted key bits
+(the reference encrypts them on its bootstrapping context): all 128 output bit ciphertexts
+must match residue for residue with the same levels and scales, and decrypting them must give
+the CTR plaintext with 0 mismatched bits against plain AES-128."""
+import time
+
+import numpy as np
+import pytest
+
+from aes_util import encrypt_block, expand_key
+
+pytestmark = pytest.mark.gpu
+
+
+def test_aes_ctr_matches_reference_and_plain_aes(wg, ref_mod):
+    import torch
+
+    R = ref_mod.RefPlans(bootstrap_keys=True)
+    info = R.bts_info()
+    N, K = R.N, len(R.p)
+    acb = 512
+    rng = np.random.default_rng(2026)
+    key = bytes(rng.integers(0, 256, 16, dtype=np.uint8))
+    ek = expand_key(key)
+    counters = bytes(rng.integers(0, 256, 32 * acb, dtype=np.uint8))
+    plain = bytes(rng.integers(0, 256, 32 * acb, dtype=np.uint8))
+    stream = b"".join(encrypt_block(ek, counters[16 * i:16 * i + 16]) for i in range(2 * acb))
+    cts = bytes(x ^ y for x, y in zip(plain, stream))
+    kflat, kscales, kl = R.aes_key_bits(ek, acb)
+
+    ctx = wg.Context(N, R.q, R.p, R.dnum)
+    for kind, wkind in ((2, wg.WG_KEY_RELIN), (1, wg.WG_KEY_CONJ), (4, wg.WG_KEY_SPARSE_TO_DENSE)):
+        k, parts, lv = R.key(0, kind=kind)
+        ctx.set_key(wkind, k, parts=parts, key_level=lv)
+    ctx.set_key(wg.WG_KEY_DENSE_TO_SPARSE, R.key(0, kind=3)[0])
+    for r in R.rotations():
+        k, parts, lv = R.key(int(r))
+        ctx.set_key(wg.WG_KEY_ROTATION, k, rotation=int(r), parts=parts, key_level=lv)
+    x2 = R.build_scaled_s2c(2)
+
+    def stages(which):
+        out = []
+        for k in range(R.stages(which)):
+            st = R.stage(which, k)
+            out.append(wg.LtStage(ctx, st["qp_limbs"] - 1 - K, st["indices"], st["diagonals"], st["baby"],
+                                  st["slot_count"], st["rescale"]))
+        return out
+
+    s2c, s2c2, c2s = stages(0), stages(x2), stages(1)
+    params = wg.BootstrapParams(info["s2c_depth"], info["depth"], info["evalmod_log_scale"], info["double_angle"],
+                                info["active_slots"], info["slots"], info["scale"])
+    n = (kl + 1) * N
+    dev = torch.from_numpy(kflat.view(np.int64)).cuda().view(1408, 2, n)
+    key_bits = [(dev[k, 0], dev[k, 1]) for k in range(1408)]
+    full = (info["depth"] + 1) * N
+    outs = [(torch.zeros(full, dtype=torch.int64, device="cuda"), torch.zeros(full, dtype=torch.int64, device="cuda"))
+            for _ in range(128)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lvls, scs = ctx.aes_ctr_walsh(params, s2c, s2c2, c2s, info["coeffs"], 512, 32, key_bits, kscales, kl, counters,
+                                  cts, acb, outs)
+    torch.cuda.synchronize()
+    print(f"device AES-CTR (1024 blocks): {time.perf_counter() - t0:.2f} s")
+    want = R.aes_ctr(kflat, kscales, kl, counters, cts, acb)
+    mism = 0
+    for bit in range(128):
+        rb, ra, rl, rs = want[bit]
+        assert (lvls[bit], scs[bit]) == (rl, rs), bit
+        m = (rl + 1) * N
+        gb, ga = wg.to_host(outs[bit][0])[:m], wg.to_host(outs[bit][1])[:m]
+        assert (gb == rb).all() and (ga == ra).all(), (bit, int((gb != rb).sum()), int((ga != ra).sum()))
+        z = R.decrypt(rl, rs, gb, ga)
+        for s in range(acb):
+            for lane, val in ((0, z[s].real), (1, z[s].imag)):
+                blk = s + lane * acb
+                mism += int(round(val)) != (plain[16 * blk + bit // 8] >> (bit % 8)) & 1
+    assert mism == 0
