@@ -13,6 +13,8 @@
 #include <cstdint>
 #include <limits>
 #include <stdexcept>
+#include <exception>
+#include <thread>
 #include <vector>
 
 #include "wg_ctops.cuh"
@@ -33,6 +35,78 @@ bool aes_close(long double l, long double r, long double tol = 0x1p-45L) {
 }
 
 using Bits = std::vector<CtBatch>;  // one ciphertext per entry (batch count 1)
+
+constexpr int kMaxLinTerms = 8;
+
+// One output limb of the fused linear layer: sum_t cnt[t] * src[t] + kfac * key (mod q).
+struct LinearJob {
+    uint64_t* out;
+    const uint64_t* src[kMaxLinTerms];
+    const uint64_t* key;
+    uint64_t kfac;
+    uint8_t cnt[kMaxLinTerms];
+    int n, mod;
+};
+
+__global__ void __launch_bounds__(kT) kb_linear(const LinearJob* jobs, int njobs, const Modulus* mods) {
+    const LinearJob* j = job_of(jobs, njobs);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const Modulus m = mods[j->mod];
+    const uint64_t q = m.q;
+    uint64_t acc = 0;
+    for (int t = 0; t < j->n; ++t) {
+        const uint64_t x = j->src[t][k];
+        for (int r = 0; r < j->cnt[t]; ++r) acc = add_mod(acc, x, q);
+    }
+    if (j->key) acc = add_mod(acc, barrett_mul(j->key[k], j->kfac, m), q);
+    j->out[k] = acc;
+}
+
+// The reference's MixColumns on lazy bits (clone, add_bits, xtime, fmix_column_byte) replayed on
+// symbolic bits: out[o][j] = how many times state bit j enters output bit o.
+using SymBit = std::array<uint8_t, 128>;
+
+std::vector<SymBit> mix_symbolic() {
+    using SymByte = std::array<SymBit, 8>;
+    auto unit = [](size_t j) {
+        SymBit b{};
+        b[j] = 1;
+        return b;
+    };
+    auto add = [](const SymBit& x, const SymBit& y) {
+        SymBit r{};
+        for (size_t j = 0; j < 128; ++j) r[j] = (uint8_t)(x[j] + y[j]);
+        return r;
+    };
+    auto byte_of = [&](size_t b) {
+        SymByte o;
+        for (size_t k = 0; k < 8; ++k) o[k] = unit(b * 8 + k);
+        return o;
+    };
+    auto add_bytes = [&](const SymByte& l, const SymByte& r) {
+        SymByte o;
+        for (size_t k = 0; k < 8; ++k) o[k] = add(l[k], r[k]);
+        return o;
+    };
+    auto xtime = [&](const SymByte& b) {
+        return SymByte{b[7], add(b[0], b[7]), b[1], add(b[2], b[7]), add(b[3], b[7]), b[4], b[5], b[6]};
+    };
+    auto mix = [&](const SymByte& b0, const SymByte& b1, const SymByte& b2, const SymByte& b3) {
+        SymByte d = xtime(add_bytes(b0, b1));
+        d = add_bytes(d, b1);
+        d = add_bytes(d, b2);
+        return add_bytes(d, b3);
+    };
+    std::vector<SymBit> out(128);
+    for (size_t col = 0; col < 4; ++col) {
+        const SymByte b0 = byte_of(4 * col), b1 = byte_of(4 * col + 1), b2 = byte_of(4 * col + 2), b3 = byte_of(4 * col + 3);
+        const SymByte o[4] = {mix(b0, b1, b2, b3), mix(b1, b2, b3, b0), mix(b2, b3, b0, b1), mix(b3, b0, b1, b2)};
+        for (size_t r = 0; r < 4; ++r)
+            for (size_t k = 0; k < 8; ++k) out[(4 * col + r) * 8 + k] = o[r][k];
+    }
+    return out;
+}
 
 class Aes {
 public:
@@ -127,6 +201,7 @@ public:
     // mask_inactive_slots_inplace: x <- rescale(x * mask), mask = 1 on the packing slots at
     // scale q_level; the scale is then reset to the state's
     void mask_inactive(Bits& st, size_t pack_count) {
+        WG_SPAN("aes.mask");
         const size_t level = st[0].level;
         if (level <= p_.s2c_depth)
             throw std::invalid_argument("ckks_aes_walsh: active slot mask requires a selection limb above S2C input level");
@@ -159,6 +234,7 @@ public:
 
     // SubBytes: the 16 byte positions as one batch of 16 Walsh S-box instances
     Bits sub_bytes(const Bits& st, size_t pack_count) {
+        WG_SPAN("aes.sub_bytes");
         const size_t level = st[0].level;
         const size_t full = p_.depth + 1;
         std::vector<uint64_t*> ib(kBlockBits), ia(kBlockBits), ob(kBlockBits), oa(kBlockBits);
@@ -259,6 +335,166 @@ public:
             ops_.add_plain(st[bit], public_bit(blocks, bit, acb, st[bit].level, st[bit].scale));
     }
 
+    // MixColumns (when `mix`) and AddRoundKey as one launch: every output bit is a sum of state
+    // bits with small multiplicities plus the round-key bit scaled up to the state scale.
+    // Taken when the state bits share level and scale and the round-key bits are not above the
+    // state scale (the reference then adds without re-aligning the state); otherwise the
+    // operation-by-operation path.
+    void linear_layer(Bits& st, const AesArgs& a, size_t round, bool mix) {
+        WG_SPAN("aes.linear");
+        const size_t level = st[0].level, L = level + 1, N = c_.N;
+        const long double S = st[0].scale;
+        bool uniform = a.key_level >= level;
+        for (const auto& b : st) uniform = uniform && b.level == level && b.scale == S && b.np == 2;
+        for (size_t bit = 0; bit < kBlockBits; ++bit) {
+            const long double ks = a.key_scales[round * kBlockBits + bit];
+            uniform = uniform && std::isfinite(ks) && !(ks > S && !aes_close(ks, S));
+        }
+        if (!uniform) {
+            if (mix) mix_columns(st);
+            add_round_key(st, a, round);
+            return;
+        }
+        std::vector<SymBit> sym;
+        if (mix) {
+            sym = mix_symbolic();
+        } else {
+            sym.assign(128, SymBit{});
+            for (size_t j = 0; j < 128; ++j) sym[j][j] = 1;
+        }
+        Bits out(kBlockBits);
+        std::vector<LinearJob> jobs;
+        for (size_t o = 0; o < kBlockBits; ++o) {
+            // the key bit's scale-up factor (multiply_by_integer_scalar_inplace on the key clone);
+            // a key bit within tolerance of the state scale only relabels the sum's scale
+            const long double ks = a.key_scales[round * kBlockBits + o];
+            uint64_t k = 1;
+            out[o] = ops_.alloc(level, 2);
+            out[o].scale = S;
+            if (aes_close(ks, S)) {
+                out[o].scale = std::max(S, ks);
+            } else {
+                const long double ratio = S / ks, r = std::round(ratio);
+                if (r < 1.0L || std::abs(ratio - r) > std::max<long double>(1.0L, std::abs(ratio)) * 1e-3L)
+                    throw std::invalid_argument("ckks_aes_walsh: non-integral scalar scale-up");
+                if (r > static_cast<long double>(std::numeric_limits<int64_t>::max()))
+                    throw std::invalid_argument("ckks_aes_walsh: scalar scale-up is too large");
+                k = (uint64_t)r;
+            }
+            CtBatch key = key_bit(a, round * kBlockBits + o);
+            for (int poly = 0; poly < 2; ++poly)
+                for (size_t l = 0; l < L; ++l) {
+                    LinearJob jb{};
+                    jb.out = out[o].p[0][poly] + l * N;
+                    for (size_t j = 0; j < 128; ++j)
+                        if (sym[o][j]) {
+                            if (jb.n == kMaxLinTerms) throw std::runtime_error("ckks_aes_walsh: linear layer too wide");
+                            jb.src[jb.n] = st[j].p[0][poly] + l * N;
+                            jb.cnt[jb.n++] = sym[o][j];
+                        }
+                    jb.key = key.p[0][poly] + l * N;
+                    jb.kfac = k % c_.q[l];
+                    jb.mod = (int)l;
+                    jobs.push_back(jb);
+                }
+        }
+        launch_linear(jobs);
+        st = out;
+    }
+
+    void launch_linear(const std::vector<LinearJob>& jobs) {
+        size_t words = 0;
+        for (const auto& jb : jobs) words += jb.n + 1 + (jb.key ? 1 : 0);
+        JobTable t;
+        const LinearJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 8.0 * c_.N * words, s_);
+        kb_linear<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        check_cuda(cudaGetLastError(), "aes linear layer");
+    }
+
+    // public bit patterns of all 128 state bits at the bits' level and scale, added in one
+    // launch (encodings on host threads, one staged upload)
+    void add_public_all(Bits& st, const uint8_t* blocks, size_t acb) {
+        WG_SPAN("aes.add_public");
+        const size_t level = st[0].level, L = level + 1, N = c_.N;
+        bool uniform = true;
+        for (const auto& b : st) uniform = uniform && b.level == level;
+        if (!uniform) {
+            add_public(st, blocks, acb);
+            return;
+        }
+        std::vector<std::vector<uint64_t>> coeff(kBlockBits, std::vector<uint64_t>(L * N));
+        std::vector<double> scale(kBlockBits);
+        for (size_t bit = 0; bit < kBlockBits; ++bit) scale[bit] = static_cast<double>(st[bit].scale);
+        encode_bits_parallel(blocks, acb, scale, L, coeff);
+        std::vector<uint64_t*> pts = ops_.upload_plains(coeff, L);
+        DeviceOps all(c_, kBlockBits, s_);
+        std::vector<AddJob> jobs;
+        for (size_t bit = 0; bit < kBlockBits; ++bit)
+            for (size_t l = 0; l < L; ++l) jobs.push_back({st[bit].p[0][0] + l * N, pts[bit] + l * N, (int)l, 0});
+        all.add_jobs(jobs);
+    }
+
+    void encode_bits_parallel(const uint8_t* blocks, size_t acb, const std::vector<double>& scale, size_t L,
+                              std::vector<std::vector<uint64_t>>& coeff) {
+        const size_t nthreads = std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        std::vector<std::exception_ptr> errs(nthreads);
+        for (size_t w = 0; w < nthreads; ++w)
+            pool.emplace_back([&, w] {
+                try {
+                    std::vector<double> re(c_.N / 2), im(c_.N / 2);
+                    for (size_t bit = w; bit < kBlockBits; bit += nthreads) {
+                        std::fill(re.begin(), re.end(), 0.0);
+                        std::fill(im.begin(), im.end(), 0.0);
+                        for (size_t s = 0; s < acb; ++s) {
+                            re[s] = (double)((blocks[16 * s + bit / 8] >> (bit % 8)) & 1);
+                            im[s] = (double)((blocks[16 * (acb + s) + bit / 8] >> (bit % 8)) & 1);
+                        }
+                        host::encode_slots(c_.N, re.data(), im.data(), scale[bit], c_.q.data(), L, coeff[bit].data());
+                    }
+                } catch (...) {
+                    errs[w] = std::current_exception();
+                }
+            });
+        for (auto& th : pool) th.join();
+        for (auto& e : errs)
+            if (e) std::rethrow_exception(e);
+    }
+
+    // initial state: key bit + counter bit pattern, all 128 bits at once
+    Bits initial_state_fast(const AesArgs& a) {
+        WG_SPAN("aes.initial");
+        const size_t level = a.key_level, L = level + 1, N = c_.N;
+        std::vector<std::vector<uint64_t>> coeff(kBlockBits, std::vector<uint64_t>(L * N));
+        std::vector<double> scale(kBlockBits);
+        for (size_t bit = 0; bit < kBlockBits; ++bit) scale[bit] = a.key_scales[bit];
+        encode_bits_parallel(a.counters, a.active_blocks, scale, L, coeff);
+        std::vector<uint64_t*> pts = ops_.upload_plains(coeff, L);
+        Bits st(kBlockBits);
+        std::vector<LinearJob> jobs;
+        for (size_t bit = 0; bit < kBlockBits; ++bit) {
+            st[bit] = ops_.alloc(level, 2);
+            st[bit].scale = a.key_scales[bit];
+            const CtBatch key = key_bit(a, bit);
+            for (int poly = 0; poly < 2; ++poly)
+                for (size_t l = 0; l < L; ++l) {
+                    LinearJob jb{};
+                    jb.out = st[bit].p[0][poly] + l * N;
+                    jb.src[0] = key.p[0][poly] + l * N;
+                    jb.cnt[0] = 1;
+                    jb.n = 1;
+                    jb.key = poly == 0 ? pts[bit] + l * N : nullptr;
+                    jb.kfac = 1;
+                    jb.mod = (int)l;
+                    jobs.push_back(jb);
+                }
+        }
+        launch_linear(jobs);
+        return st;
+    }
+
     // mask_final_refresh_slots_inplace
     void refresh_mask(Bits& st, size_t active, size_t min_keep) {
         const size_t level = st[0].level;
@@ -279,6 +515,7 @@ public:
     }
 
     void final_refresh(Bits& st, size_t acb, DeviceOps& bops) {
+        WG_SPAN("aes.final_refresh");
         const size_t slots = c_.N / 2;
         const size_t stride = acb, per = slots / stride;
         const size_t batches = refresh_batches(slots, acb);
@@ -389,15 +626,14 @@ void aes_ctr_walsh(Context& c, const BootstrapParams& p, const S2cPlan* s2c, siz
         throw std::invalid_argument("ckks_aes_walsh: null argument");
     DeviceOps ops(c, 1, s);
     Aes aes(c, ops, p, s2c, nplans, c2s, nc2s, coeffs, ncoeffs, s);
-    Bits st = aes.initial_state(a);
+    Bits st = aes.initial_state_fast(a);
     for (size_t round = 1; round <= kRounds; ++round) {
         aes.mask_inactive(st, pack);
         st = aes.sub_bytes(st, pack);
         Aes::shift_rows(st);
-        if (round < kRounds) aes.mix_columns(st);
-        aes.add_round_key(st, a, round);
+        aes.linear_layer(st, a, round, round < kRounds);
     }
-    aes.add_public(st, a.ciphertexts, a.active_blocks);
+    aes.add_public_all(st, a.ciphertexts, a.active_blocks);
     DeviceOps bops(c, Aes::refresh_batches(slots, a.active_blocks), s);
     aes.final_refresh(st, a.active_blocks, bops);
     for (size_t bit = 0; bit < kBlockBits; ++bit) {

@@ -111,6 +111,22 @@ WG_HD uint64_t barrett_mul(uint64_t a, uint64_t b, const Modulus& m) {
     return r >= m.q ? r - m.q : r;
 }
 
+// Canonical residue of a 128-bit value z = z_hi 2^64 + z_lo.  The quotient estimate is the one
+// barrett_mul forms; for any z < 2^128 it is at most two below floor(z / q) (mu = floor((2^128-1)/q)
+// costs less than one, the middle carry left out at most one) and never above it, so z - q_hat q
+// lies in [0, 3q) and two corrections make it canonical.  Requires q < 2^62.
+WG_HD uint64_t reduce128(uint64_t z_hi, uint64_t z_lo, const Modulus& m) {
+    const uint64_t t_lo = z_hi * m.mu_lo;
+    const uint64_t t_hi = umulhi(z_hi, m.mu_lo);
+    const uint64_t c = umulhi(z_lo, m.mu_lo);
+    const uint64_t s_lo = t_lo + c;
+    const uint64_t carry = t_hi + (s_lo < t_lo ? 1ull : 0ull);
+    const uint64_t q_hat = z_hi * m.mu_hi + umulhi(z_lo, m.mu_hi) + carry;
+    uint64_t r = z_lo - q_hat * m.q;
+    if (r >= m.q) r -= m.q;
+    return r >= m.q ? r - m.q : r;
+}
+
 // barrett_reduce_u64 (modarith.hpp:53-58).
 WG_HD uint64_t barrett_u64(uint64_t a, uint64_t q, uint64_t mu_hi) {
     const uint64_t q_hat = umulhi(a, mu_hi);

@@ -21,13 +21,8 @@ using namespace bk;
 // Job-table staging
 // ------------------------------------------------------------------------------------------
 void JobTable::upload(Context& c, cudaStream_t s) {
-    BatchBuffers& bb = c.batch_buffers(s);
-    bb.ensure_jobs(c, bytes.size(), s);
-    if (bb.staged_event) cudaEventSynchronize(bb.staged_event);  // previous upload left the pinned stage
-    std::memcpy(bb.h_jobs, bytes.data(), bytes.size());
-    check_cuda(cudaMemcpyAsync(bb.d_jobs, bb.h_jobs, bytes.size(), cudaMemcpyHostToDevice, s), "job upload");
-    check_cuda(cudaEventRecord(bb.staged_event, s), "job event");
-    base = bb.d_jobs;
+    WG_SPAN("upload");
+    base = c.batch_buffers(s).stage(c, bytes.data(), bytes.size(), s);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -170,6 +165,7 @@ static void run_keyswitch(const Context& c, const KsPlan& p, const JobTable& t, 
 }
 
 void batch_keyswitch(Context& c, const KsItem* items, size_t n, cudaStream_t s) {
+    WG_SPAN("keyswitch");
     if (n == 0) return;
     uint64_t* ws = c.batch_buffers(s).arena(c, batch_keyswitch_words(c, items, n), s);
     JobTable t;

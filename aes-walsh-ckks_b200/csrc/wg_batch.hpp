@@ -133,5 +133,8 @@ void aes_ctr_walsh(Context& c, const BootstrapParams& p, const S2cPlan* s2c, siz
 // Hoisted rotations of one ciphertext; out [rotation][b, a][level+1][N] (wg_bsgs.cu).
 void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rots, size_t nrot,
                  uint64_t* out, cudaStream_t s);
+// ... for `count` ciphertexts at once; outs[i] as `out` above for ciphertext i.
+void rotate_many_batch(Context& c, size_t level, size_t count, const uint64_t* const* bs, const uint64_t* const* as,
+                       const int64_t* rots, size_t nrot, uint64_t* const* outs, cudaStream_t s);
 
 }  // namespace wg

@@ -62,6 +62,11 @@ struct CtRef {
     const uint64_t* b;
 };
 
+struct CopyPair {
+    uint64_t* dst;
+    const uint64_t* src;
+};
+
 struct TermRef {
     const uint64_t* diag;  // QP plaintext of the term (limb 0)
     int slot;              // baby slot
@@ -567,7 +572,14 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
 // out: [rotation][b, a][level+1][N].
 void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a, const int64_t* rots, size_t nrot,
                  uint64_t* out, cudaStream_t s) {
-    if (nrot == 0) return;
+    rotate_many_batch(c, level, 1, &b, &a, rots, nrot, &out, s);
+}
+
+// The same for `count` ciphertexts at one level, every step one launch over all of them:
+// out[i] receives ciphertext i's rotations, [rotation][b, a][level+1][N].
+void rotate_many_batch(Context& c, size_t level, size_t count, const uint64_t* const* bs, const uint64_t* const* as,
+                       const int64_t* rots, size_t nrot, uint64_t* const* outs, cudaStream_t s) {
+    if (nrot == 0 || count == 0) return;
     const size_t N = c.N, L = level + 1, K = c.np, T = L + K, nq = c.nq;
     const size_t B = c.parts_at(level);
     const size_t slots = N / 2;
@@ -584,10 +596,8 @@ void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a,
         gal[r] = host::powmod(5, (uint64_t)rr, 2 * N);
     }
     const size_t w_coeff = L * N, w_digits = B * T * N, w_acc = nrot * 2 * T * N, w_contrib = nrot * 2 * L * N;
-    uint64_t* coeff = c.batch_buffers(s).arena(c, w_coeff + w_digits + w_acc + w_contrib, s);
-    uint64_t* digits = coeff + w_coeff;
-    uint64_t* accb = digits + w_digits;
-    uint64_t* contrib = accb + w_acc;
+    const size_t per_ct = w_coeff + w_digits + w_acc + w_contrib;
+    uint64_t* arena = c.batch_buffers(s).arena(c, count * per_ct, s);
     auto modq = [&](size_t limb) { return (int)(limb < L ? limb : nq + (limb - L)); };
 
     std::vector<NttJob> intt_a, ntt_dig, intt_p, ntt_c;
@@ -596,40 +606,55 @@ void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a,
     std::vector<ModDownJob> md;
     std::vector<CombineJob> comb;
     std::vector<GatherJob> gath;
-    for (size_t l = 0; l < L; ++l) intt_a.push_back({a + l * N, coeff + l * N, (int)l, 0});
-    for (size_t j = 0; j < B; ++j) {
-        modup.push_back({c.d_modup + level * c.dnum + j, coeff, digits + j * T * N});
-        const size_t s0 = j * c.alpha, s1 = std::min(s0 + c.alpha, L);
-        for (size_t l = 0; l < T; ++l)
-            if (l < s0 || l >= s1) ntt_dig.push_back({digits + j * T * N + l * N, digits + j * T * N + l * N, modq(l), 0});
-    }
-    for (size_t r = 0; r < nrot; ++r) {
-        uint64_t* ob = out + (2 * r) * L * N;
-        uint64_t* oa = ob + L * N;
-        if (!keys[r]) {  // rotation by a multiple of the slot count: the ciphertext itself
-            check_cuda(cudaMemcpyAsync(ob, b, L * N * 8, cudaMemcpyDeviceToDevice, s), "rotate_many copy");
-            check_cuda(cudaMemcpyAsync(oa, a, L * N * 8, cudaMemcpyDeviceToDevice, s), "rotate_many copy");
-            continue;
+    std::vector<CopyPair> copies;
+    for (size_t ci = 0; ci < count; ++ci) {
+        const uint64_t* b = bs[ci];
+        const uint64_t* a = as[ci];
+        uint64_t* out = outs[ci];
+        uint64_t* coeff = arena + ci * per_ct;
+        uint64_t* digits = coeff + w_coeff;
+        uint64_t* accb = digits + w_digits;
+        uint64_t* contrib = accb + w_acc;
+        for (size_t l = 0; l < L; ++l) intt_a.push_back({a + l * N, coeff + l * N, (int)l, 0});
+        for (size_t j = 0; j < B; ++j) {
+            modup.push_back({c.d_modup + level * c.dnum + j, coeff, digits + j * T * N});
+            const size_t s0 = j * c.alpha, s1 = std::min(s0 + c.alpha, L);
+            for (size_t l = 0; l < T; ++l)
+                if (l < s0 || l >= s1)
+                    ntt_dig.push_back({digits + j * T * N + l * N, digits + j * T * N + l * N, modq(l), 0});
         }
-        uint64_t* acc = accb + r * 2 * T * N;
-        uint64_t* cr = contrib + r * 2 * L * N;
-        for (size_t i = 0; i < T; ++i)
-            mac.push_back({keys[r]->d_data, a, digits, acc, T * N, (int)L, (int)K, (int)B, (int)c.alpha,
-                           (int)keys[r]->key_level, (int)i});
-        for (int poly = 0; poly < 2; ++poly) {
-            for (size_t pi = 0; pi < K; ++pi) {
-                uint64_t* p = acc + (poly * T + L + pi) * N;
-                intt_p.push_back({p, p, (int)(nq + pi), 0});
+        for (size_t r = 0; r < nrot; ++r) {
+            uint64_t* ob = out + (2 * r) * L * N;
+            uint64_t* oa = ob + L * N;
+            if (!keys[r]) {  // rotation by a multiple of the slot count: the ciphertext itself
+                copies.push_back({ob, b});
+                copies.push_back({oa, a});
+                continue;
             }
-            md.push_back({acc + (poly * T + L) * N, cr + poly * L * N, c.fold_inv[level], c.fold_inv_s[level], (int)L, 0});
-            for (size_t qi = 0; qi < L; ++qi) ntt_c.push_back({cr + (poly * L + qi) * N, cr + (poly * L + qi) * N, (int)qi, 0});
-        }
-        for (size_t qi = 0; qi < L; ++qi) {
-            // combine in place of the accumulators, then gather into the output slot
-            comb.push_back({acc, cr, b, a, acc + T * N, acc, (int)L, (int)K, (int)qi, 1, 0, 0});
-            gath.push_back({acc + T * N + qi * N, acc + qi * N, ob + qi * N, oa + qi * N, gal[r]});
+            uint64_t* acc = accb + r * 2 * T * N;
+            uint64_t* cr = contrib + r * 2 * L * N;
+            for (size_t i = 0; i < T; ++i)
+                mac.push_back({keys[r]->d_data, a, digits, acc, T * N, (int)L, (int)K, (int)B, (int)c.alpha,
+                               (int)keys[r]->key_level, (int)i});
+            for (int poly = 0; poly < 2; ++poly) {
+                for (size_t pi = 0; pi < K; ++pi) {
+                    uint64_t* p = acc + (poly * T + L + pi) * N;
+                    intt_p.push_back({p, p, (int)(nq + pi), 0});
+                }
+                md.push_back({acc + (poly * T + L) * N, cr + poly * L * N, c.fold_inv[level], c.fold_inv_s[level],
+                              (int)L, 0});
+                for (size_t qi = 0; qi < L; ++qi)
+                    ntt_c.push_back({cr + (poly * L + qi) * N, cr + (poly * L + qi) * N, (int)qi, 0});
+            }
+            for (size_t qi = 0; qi < L; ++qi) {
+                // combine in place of the accumulators, then gather into the output slot
+                comb.push_back({acc, cr, b, a, acc + T * N, acc, (int)L, (int)K, (int)qi, 1, 0, 0});
+                gath.push_back({acc + T * N + qi * N, acc + qi * N, ob + qi * N, oa + qi * N, gal[r]});
+            }
         }
     }
+    for (const CopyPair& cp : copies)
+        check_cuda(cudaMemcpyAsync(cp.dst, cp.src, L * N * 8, cudaMemcpyDeviceToDevice, s), "rotate_many copy");
     JobTable t;
     const NttJob* j1 = t.add(intt_a);
     const ModUpJob* j2 = t.add(modup);
@@ -645,7 +670,7 @@ void rotate_many(Context& c, size_t level, const uint64_t* b, const uint64_t* a,
     {
         double bytes = 0;
         for (size_t j = 0; j < B; ++j) bytes += 8.0 * N * (c.modup[level][j].src_count + c.modup[level][j].dst_count);
-        Probe probe(kClsModUp, bytes, s);
+        Probe probe(kClsModUp, bytes * count, s);
         kb_modup<<<grid_for(c, modup.size()), kT, 0, s>>>(t.at(j2), (int)modup.size(), c.d_mod, N);
     }
     ntt_jobs(c, t.at(j3), (int)ntt_dig.size(), true, s);

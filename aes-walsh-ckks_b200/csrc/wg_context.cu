@@ -1,6 +1,8 @@
 // Context construction: the host tables (wg_tables.cpp) uploaded once into device-resident
 // buffers, per-stream scratch and the switching-key registry.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstring>
 
 #include "wg_internal.hpp"
@@ -14,22 +16,66 @@ static bool capturing(cudaStream_t s) {
     return cs != cudaStreamCaptureStatusNone;
 }
 
-void BatchBuffers::ensure_jobs(const Context& c, size_t bytes, cudaStream_t s) {
-    if (bytes <= jobs_bytes) return;
-    if (capturing(s)) fail(kRuntime, "batched job tables must be sized (one uncaptured call) before graph capture");
-    if (staged_event) cudaEventSynchronize(staged_event);
-    check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
-    cudaFree(d_jobs);
-    cudaFreeHost(h_jobs);
-    d_jobs = h_jobs = nullptr;
-    jobs_bytes = 0;
-    const size_t cap = bytes + bytes / 2 + 4096;
-    if (cudaMalloc(&d_jobs, cap) != cudaSuccess || cudaMallocHost(&h_jobs, cap) != cudaSuccess) {
-        cudaGetLastError();
-        fail(kNoMemory, "batched job-table allocation failed");
+std::atomic<uint64_t> g_stage_calls{0}, g_stage_bytes{0}, g_stage_wait_ns{0};
+
+void stage_stats(uint64_t* calls, uint64_t* bytes, uint64_t* wait_ns) {
+    *calls = g_stage_calls.load();
+    *bytes = g_stage_bytes.load();
+    *wait_ns = g_stage_wait_ns.load();
+}
+
+void* BatchBuffers::stage(const Context& c, const void* data, size_t bytes, cudaStream_t s) {
+    g_stage_calls.fetch_add(1, std::memory_order_relaxed);
+    g_stage_bytes.fetch_add(bytes, std::memory_order_relaxed);
+    if (capturing(s))
+        fail(kRuntime, "batched calls cannot be captured into a graph (their staging is reused); use wg_batch_plan_*");
+    const size_t need = (std::max<size_t>(bytes, 1) + 255) & ~size_t{255};
+    if (need > ring_bytes) {
+        // grow: everything queued on the stream may still read the old device ring
+        check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+        check_cuda(cudaStreamSynchronize(s), "staging ring resize");
+        for (Flight& f : flights) spare_events.push_back(f.done);
+        flights.clear();
+        cudaFree(d_ring);
+        cudaFreeHost(h_ring);
+        d_ring = h_ring = nullptr;
+        ring_bytes = 0;
+        const size_t cap = std::max<size_t>(need * 2, size_t{64} << 20);
+        if (cudaMalloc((void**)&d_ring, cap) != cudaSuccess || cudaMallocHost((void**)&h_ring, cap) != cudaSuccess) {
+            cudaGetLastError();
+            fail(kNoMemory, "staging ring allocation failed");
+        }
+        ring_bytes = cap;
+        head = 0;
     }
-    jobs_bytes = cap;
-    if (!staged_event) check_cuda(cudaEventCreateWithFlags(&staged_event, cudaEventDisableTiming), "event");
+    if (head + need > ring_bytes) head = 0;
+    const size_t begin = head, end = head + need;
+    // wait for the uploads whose host bytes this region still holds
+    while (!flights.empty()) {
+        const Flight& f = flights.front();
+        const bool overlap = f.begin < end && begin < f.end;
+        if (!overlap) break;
+        const auto t0 = std::chrono::steady_clock::now();
+        check_cuda(cudaEventSynchronize(f.done), "staging ring wait");
+        g_stage_wait_ns.fetch_add(
+            (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count(),
+            std::memory_order_relaxed);
+        spare_events.push_back(f.done);
+        flights.pop_front();
+    }
+    std::memcpy(h_ring + begin, data, bytes);
+    check_cuda(cudaMemcpyAsync(d_ring + begin, h_ring + begin, bytes, cudaMemcpyHostToDevice, s), "staging upload");
+    cudaEvent_t ev = nullptr;
+    if (!spare_events.empty()) {
+        ev = spare_events.back();
+        spare_events.pop_back();
+    } else {
+        check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+    }
+    check_cuda(cudaEventRecord(ev, s), "staging event");
+    flights.push_back({begin, end, ev});
+    head = end;
+    return d_ring + begin;
 }
 
 uint64_t* BatchBuffers::arena(const Context& c, size_t words, cudaStream_t s) {
@@ -49,14 +95,19 @@ uint64_t* BatchBuffers::arena(const Context& c, size_t words, cudaStream_t s) {
 }
 
 void BatchBuffers::release() {
-    if (staged_event) cudaEventSynchronize(staged_event);
-    cudaFree(d_jobs);
-    cudaFreeHost(h_jobs);
+    for (Flight& f : flights) {
+        cudaEventSynchronize(f.done);
+        cudaEventDestroy(f.done);
+    }
+    flights.clear();
+    for (cudaEvent_t e : spare_events) cudaEventDestroy(e);
+    spare_events.clear();
+    cudaFree(d_ring);
+    cudaFreeHost(h_ring);
     cudaFree(d_arena);
-    if (staged_event) cudaEventDestroy(staged_event);
-    d_jobs = h_jobs = nullptr;
+    d_ring = h_ring = nullptr;
     d_arena = nullptr;
-    staged_event = nullptr;
+    ring_bytes = 0;
 }
 
 BatchBuffers& Context::batch_buffers(cudaStream_t s) {
@@ -68,6 +119,10 @@ BatchBuffers& Context::batch_buffers(cudaStream_t s) {
 }
 
 Context::~Context() {
+    for (auto& kv : consts) {
+        cudaFree(kv.second.d);
+        cudaEventDestroy(kv.second.ready);
+    }
     for (auto& kv : keys) cudaFree(kv.second.d_data);
     for (auto& kv : workspaces) cudaFree(kv.second.base);
     for (auto& kv : batches) kv.second.release();
@@ -130,6 +185,19 @@ Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t
     c->q.assign(q, q + nq);
     c->p.assign(p, p + np);
     check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    {
+        // The batched operations draw their temporaries from this process's stream-ordered
+        // pool; let it keep up to 8 GiB across synchronisations instead of unmapping and
+        // remapping it around every event wait.
+        cudaMemPool_t pool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t cur = 0;
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur);
+            uint64_t want = uint64_t{8} << 30;
+            if (cur < want) cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &want);
+        }
+        cudaGetLastError();
+    }
     HostTables H = build_tables(N, q, nq, p, np, dnum);
     c->mods = H.mods;
     const size_t nm = nq + np;

@@ -6,6 +6,9 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstring>
+#include <map>
+#include <tuple>
 #include <stdexcept>
 #include <vector>
 
@@ -13,6 +16,7 @@
 #include "wg_batch.hpp"
 #include "wg_batch_kernels.cuh"
 #include "wg_internal.hpp"
+#include "wg_encode.hpp"
 
 namespace wg {
 namespace {
@@ -55,6 +59,33 @@ __global__ void __launch_bounds__(kT) kb_pmul(const PmulJob* jobs, int n, const 
     j->x[k] = barrett_mul(j->x[k], j->p[k], mods[j->mod]);
 }
 
+struct CopyJob {
+    uint64_t* dst;
+    const uint64_t* src;
+};
+
+__global__ void __launch_bounds__(kT) kb_copy(const CopyJob* jobs, int n) {
+    const CopyJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    j->dst[k] = j->src[k];
+}
+
+struct AddJob {
+    uint64_t* x;
+    const uint64_t* y;
+    int mod, sub;
+};
+
+// x = x +- y (mod q), canonical
+__global__ void __launch_bounds__(kT) kb_add(const AddJob* jobs, int n, const Modulus* mods) {
+    const AddJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const uint64_t q = mods[j->mod].q;
+    j->x[k] = j->sub ? sub_mod(j->x[k], j->y[k], q) : add_mod(j->x[k], j->y[k], q);
+}
+
 // A batch of ciphertexts with common metadata.  Polynomial k of ciphertext i lives at p[i][k]
 // with room for `cap` limbs; limbs [0, level] are live.
 struct CtBatch {
@@ -69,6 +100,7 @@ class DeviceOps {
 public:
     DeviceOps(Context& c, size_t count, cudaStream_t s) : c_(c), count_(count), s_(s) {}
     ~DeviceOps() {
+        WG_SPAN("free");
         for (uint64_t* p : owned_) cudaFreeAsync(p, s_);
     }
     DeviceOps(const DeviceOps&) = delete;
@@ -90,7 +122,8 @@ public:
     CtBatch zeros(size_t level, long double scale) {
         CtBatch x;
         x.p.resize(count_);
-        for (size_t i = 0; i < count_; ++i) x.p[i] = {buffer(level + 1, true), buffer(level + 1, true), nullptr};
+        const std::vector<uint64_t*> bufs = buffers(2 * count_, level + 1, true);
+        for (size_t i = 0; i < count_; ++i) x.p[i] = {bufs[2 * i], bufs[2 * i + 1], nullptr};
         x.np = 2;
         x.level = level;
         x.cap = level + 1;
@@ -98,22 +131,33 @@ public:
         return x;
     }
 
+    // fresh copy of limbs [0, level] of every polynomial (one launch)
     CtBatch clone(const CtBatch& x) {
+        const size_t N = c_.N;
         CtBatch y = x;
         y.cap = x.level + 1;
+        std::vector<CopyJob> jobs;
+        jobs.reserve(count_ * x.np * y.cap);
+        const std::vector<uint64_t*> bufs = buffers(count_ * x.np, y.cap, false);
         for (size_t i = 0; i < count_; ++i)
             for (int k = 0; k < x.np; ++k) {
-                y.p[i][k] = buffer(y.cap, false);
-                check_cuda(cudaMemcpyAsync(y.p[i][k], x.p[i][k], y.cap * c_.N * 8, cudaMemcpyDeviceToDevice, s_),
-                           "evalpoly copy");
+                y.p[i][k] = bufs[i * x.np + k];
+                for (size_t l = 0; l < y.cap; ++l) jobs.push_back({y.p[i][k] + l * N, x.p[i][k] + l * N});
             }
+        JobTable t;
+        const CopyJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 16.0 * N * jobs.size(), s_);
+        kb_copy<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size());
+        check_cuda(cudaGetLastError(), "batched copy");
         return y;
     }
 
     void pad(CtBatch& x, int np) {
         if (np < x.np) throw std::invalid_argument("ckks_evalchebyshev: cannot shrink ciphertext degree by padding");
         while (x.np < np) {
-            for (size_t i = 0; i < count_; ++i) x.p[i][x.np] = buffer(x.cap, true);
+            const std::vector<uint64_t*> bufs = buffers(count_, x.cap, true);
+            for (size_t i = 0; i < count_; ++i) x.p[i][x.np] = bufs[i];
             ++x.np;
         }
     }
@@ -121,7 +165,10 @@ public:
     // (b, a) x (b', a') -> (b b', a b' + b a', a a'); y must not alias x.
     void tensor(CtBatch& x, const CtBatch& y) {
         const size_t N = c_.N;
-        pad(x, 3);
+        if (x.np != 2) throw std::invalid_argument("ckks_mul_inplace(ct,ct): expected 2-component inputs");
+        const std::vector<uint64_t*> bufs = buffers(count_, x.cap, false);  // fully written below
+        for (size_t i = 0; i < count_; ++i) x.p[i][2] = bufs[i];
+        x.np = 3;
         std::vector<TensorJob> jobs;
         for (size_t i = 0; i < count_; ++i)
             for (size_t l = 0; l <= x.level; ++l)
@@ -199,9 +246,26 @@ public:
         x.level = lv - 1;
     }
 
+    // x +-= y on every polynomial and limb of the batch: one launch
     void add(CtBatch& x, const CtBatch& y, bool subtract) {
+        const size_t N = c_.N;
+        std::vector<AddJob> jobs;
+        jobs.reserve(count_ * x.np * (x.level + 1));
         for (size_t i = 0; i < count_; ++i)
-            for (int k = 0; k < x.np; ++k) add_sub(c_, x.level, x.p[i][k], y.p[i][k], 1, 0, subtract, s_);
+            for (int k = 0; k < x.np; ++k)
+                for (size_t l = 0; l <= x.level; ++l)
+                    jobs.push_back({x.p[i][k] + l * N, y.p[i][k] + l * N, (int)l, subtract ? 1 : 0});
+        add_jobs(jobs);
+    }
+
+    void add_jobs(const std::vector<AddJob>& jobs) {
+        if (jobs.empty()) return;
+        JobTable t;
+        const AddJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 8.0 * c_.N * jobs.size() * 3.0, s_);
+        kb_add<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        check_cuda(cudaGetLastError(), "batched add");
     }
 
     // op per limb: scalars[l] < q_l.  kScalarMul / kScalarMulAdd touch every polynomial,
@@ -257,43 +321,114 @@ public:
 
     // ckks_mul_inplace(ct, Complex, scale): the slot-constant re + i im encodes (at scale
     // `scale`) to round(scale re) + round(scale im) X^(N/2); multiply every polynomial by it.
-    // Evaluation-form plaintext of the slot constant re + i im at `scale`:
-    // round(scale re) + round(scale im) X^(N/2), reduced per limb, then NTT.
+    // Evaluation-form plaintext of the slot constant re + i im at `scale` (the host encoder,
+    // the same residues as the reference's ckks_encode; for a constant they are
+    // round(scale re) + round(scale im) X^(N/2) up to the FFT's rounding), then NTT.  Cached per
+    // (value, scale, limbs) for the lifetime of this object.
+    // Constants are shared through the context (up to kConstCacheBytes), else kept for the life
+    // of this operation set.
     uint64_t* constant_plaintext(size_t L, double re, double im, double scale) {
-        const size_t N = c_.N;
-        const long double r0 = std::round(static_cast<long double>(scale) * re);
-        const long double r1 = std::round(static_cast<long double>(scale) * im);
-        std::vector<uint64_t> host(L * N, 0);
-        for (size_t l = 0; l < L; ++l) {
-            const uint64_t q = c_.q[l];
-            auto modq = [q](long double v) {
-                long double m = std::fmod(v, static_cast<long double>(q));
-                if (m < 0.0L) m += static_cast<long double>(q);
-                uint64_t r = static_cast<uint64_t>(m);
-                return r >= q ? r % q : r;
-            };
-            host[l * N] = modq(r0);
-            host[l * N + N / 2] = modq(r1);
-        }
-        uint64_t* pt = buffer(L, false);
-        check_cuda(cudaMemcpyAsync(pt, host.data(), L * N * 8, cudaMemcpyHostToDevice, s_), "constant plaintext");
-        check_cuda(cudaStreamSynchronize(s_), "constant plaintext");
-        ntt_forward(c_, pt, (int)L, 1, 0, LimbMap{0, 0, 0}, s_);
+        const auto key = std::make_tuple(re, im, scale, L);
+        auto it = const_cache_.find(key);
+        if (it != const_cache_.end()) return it->second;
+        uint64_t* pt = shared_constant(key);
+        if (!pt) pt = constant_plaintext_new(L, re, im, scale);
+        const_cache_.emplace(key, pt);
         return pt;
+    }
+
+    static constexpr size_t kConstCacheBytes = size_t{2} << 30;
+
+    uint64_t* shared_constant(const std::tuple<double, double, double, size_t>& key) {
+        const auto [re, im, scale, L] = key;
+        std::lock_guard<std::mutex> g(c_.const_mutex);
+        auto ct = c_.consts.find(key);
+        if (ct != c_.consts.end()) {
+            if (ct->second.stream != s_) check_cuda(cudaStreamWaitEvent(s_, ct->second.ready, 0), "constant wait");
+            return ct->second.d;
+        }
+        const size_t bytes = L * c_.N * 8;
+        if (c_.const_bytes + bytes > kConstCacheBytes) return nullptr;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (s_) cudaStreamIsCapturing(s_, &cs);
+        if (cs != cudaStreamCaptureStatusNone) return nullptr;
+        Context::ConstPlain cp{nullptr, nullptr, s_, bytes};
+        check_cuda(cudaMalloc((void**)&cp.d, bytes), "constant plaintext");
+        if (cudaEventCreateWithFlags(&cp.ready, cudaEventDisableTiming) != cudaSuccess) {
+            cudaFree(cp.d);
+            fail(kRuntime, "constant plaintext event");
+        }
+        try {
+            const size_t N = c_.N;
+            std::vector<double> vr(N / 2, re), vi(N / 2, im);
+            std::vector<uint64_t> host(L * N);
+            host::encode_slots(N, vr.data(), vi.data(), scale, c_.q.data(), L, host.data());
+            upload_plain_into(host.data(), L, cp.d);
+            check_cuda(cudaEventRecord(cp.ready, s_), "constant plaintext event");
+        } catch (...) {
+            cudaFree(cp.d);
+            cudaEventDestroy(cp.ready);
+            throw;
+        }
+        c_.consts.emplace(key, cp);
+        c_.const_bytes += bytes;
+        return cp.d;
+    }
+
+    uint64_t* constant_plaintext_new(size_t L, double re, double im, double scale) {
+        const size_t N = c_.N;
+        std::vector<double> vr(N / 2, re), vi(N / 2, im);
+        std::vector<uint64_t> host(L * N);
+        host::encode_slots(N, vr.data(), vi.data(), scale, c_.q.data(), L, host.data());
+        return upload_plain(host.data(), L);
     }
 
     // Evaluation-form plaintext from coefficient-form residues (L limbs): upload, then NTT.
     uint64_t* upload_plain(const uint64_t* coeff, size_t L) {
         uint64_t* pt = buffer(L, false);
-        check_cuda(cudaMemcpyAsync(pt, coeff, L * c_.N * 8, cudaMemcpyHostToDevice, s_), "plaintext upload");
-        check_cuda(cudaStreamSynchronize(s_), "plaintext upload");
-        ntt_forward(c_, pt, (int)L, 1, 0, LimbMap{0, 0, 0}, s_);
+        upload_plain_into(coeff, L, pt);
         return pt;
+    }
+
+    void upload_plain_into(const uint64_t* coeff, size_t L, uint64_t* pt) {
+        const size_t N = c_.N;
+        // staged copy of the coefficients; the forward NTT reads it and writes the plaintext
+        auto* staged = static_cast<uint64_t*>(c_.batch_buffers(s_).stage(c_, coeff, L * N * 8, s_));
+        std::vector<NttJob> jobs;
+        for (size_t l = 0; l < L; ++l) jobs.push_back({staged + l * N, pt + l * N, (int)l, 0});
+        JobTable t;
+        const NttJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        ntt_jobs(c_, t.at(j), (int)jobs.size(), true, s_);
+    }
+
+    // Many plaintexts at once: coeff[k] holds L limbs of plaintext k (coefficient form); one
+    // staged upload and one NTT launch for all of them.
+    std::vector<uint64_t*> upload_plains(const std::vector<std::vector<uint64_t>>& coeff, size_t L) {
+        const size_t N = c_.N, words = L * N;
+        std::vector<uint64_t> flat(coeff.size() * words);
+        for (size_t k = 0; k < coeff.size(); ++k) std::memcpy(flat.data() + k * words, coeff[k].data(), words * 8);
+        auto* staged = static_cast<uint64_t*>(c_.batch_buffers(s_).stage(c_, flat.data(), flat.size() * 8, s_));
+        std::vector<uint64_t*> out(coeff.size());
+        std::vector<NttJob> jobs;
+        for (size_t k = 0; k < coeff.size(); ++k) {
+            out[k] = buffer(L, false);
+            for (size_t l = 0; l < L; ++l) jobs.push_back({staged + k * words + l * N, out[k] + l * N, (int)l, 0});
+        }
+        JobTable t;
+        const NttJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        ntt_jobs(c_, t.at(j), (int)jobs.size(), true, s_);
+        return out;
     }
 
     // b += pt (evaluation form, x.level+1 limbs) on every ciphertext (ckks_add_inplace(ct, pt))
     void add_plain(CtBatch& x, const uint64_t* pt) {
-        for (size_t i = 0; i < count_; ++i) add_sub(c_, x.level, x.p[i][0], pt, 1, 0, false, s_);
+        const size_t N = c_.N;
+        std::vector<AddJob> jobs;
+        for (size_t i = 0; i < count_; ++i)
+            for (size_t l = 0; l <= x.level; ++l) jobs.push_back({x.p[i][0] + l * N, pt + l * N, (int)l, 0});
+        add_jobs(jobs);
     }
 
     // every polynomial *= pt pointwise (ckks_mul_inplace(ct, pt)); scale left to the caller
@@ -329,9 +464,7 @@ public:
     // b += the encoding of the slot constant re + i im at `scale` (closed form, as in
     // mul_complex_constant), on every ciphertext of the batch.
     void add_complex_constant(CtBatch& x, double re, double im, double scale) {
-        const size_t N = c_.N, L = x.level + 1;
-        uint64_t* pt = constant_plaintext(L, re, im, scale);
-        for (size_t i = 0; i < count_; ++i) add_sub(c_, x.level, x.p[i][0], pt, 1, 0, false, s_);
+        add_plain(x, constant_plaintext(x.level + 1, re, im, scale));
     }
 
     // x *= k (mod q) on every polynomial (ckks_mul_inplace(ct, int64_t)); scale unchanged.
@@ -382,9 +515,10 @@ public:
     CtBatch alloc(size_t level, int np) {
         CtBatch x;
         x.p.resize(count_);
+        const std::vector<uint64_t*> bufs = buffers(count_ * np, level + 1, false);
         for (size_t i = 0; i < count_; ++i) {
             x.p[i] = {nullptr, nullptr, nullptr};
-            for (int k = 0; k < np; ++k) x.p[i][k] = buffer(level + 1, false);
+            for (int k = 0; k < np; ++k) x.p[i][k] = bufs[i * np + k];
         }
         x.np = np;
         x.level = level;
@@ -404,16 +538,47 @@ public:
     }
 
 private:
-    uint64_t* buffer(size_t limbs, bool zero) {
-        uint64_t* p = nullptr;
-        const size_t bytes = std::max<size_t>(limbs, 1) * c_.N * 8;
-        if (cudaMallocAsync((void**)&p, bytes, s_) != cudaSuccess) {
-            cudaGetLastError();
-            fail(kNoMemory, "ckks_evalchebyshev: device allocation failed");
+    // Buffers are carved from chunks of stream-ordered memory and all released together when
+    // the operation set ends (none is freed earlier), so one allocation serves many buffers.
+    static constexpr size_t kFirstChunkWords = size_t{1} << 20;   // 8 MiB
+    static constexpr size_t kMaxChunkWords = size_t{1} << 26;     // 512 MiB
+
+    uint64_t* carve(size_t words) {
+        words = (words + 31) & ~size_t{31};  // 256-byte alignment
+        if (words > left_) {
+            WG_SPAN("alloc");
+            const size_t chunk = std::max(words, next_chunk_);
+            next_chunk_ = std::min(next_chunk_ * 2, kMaxChunkWords);
+            uint64_t* p = nullptr;
+            if (cudaMallocAsync((void**)&p, chunk * 8, s_) != cudaSuccess) {
+                cudaGetLastError();
+                fail(kNoMemory, "ckks_evalchebyshev: device allocation failed");
+            }
+            owned_.push_back(p);
+            cur_ = p;
+            left_ = chunk;
         }
-        owned_.push_back(p);
-        if (zero) check_cuda(cudaMemsetAsync(p, 0, bytes, s_), "evalpoly zero");
+        uint64_t* p = cur_;
+        cur_ += words;
+        left_ -= words;
         return p;
+    }
+
+    uint64_t* buffer(size_t limbs, bool zero) {
+        const size_t words = std::max<size_t>(limbs, 1) * c_.N;
+        uint64_t* p = carve(words);
+        if (zero) check_cuda(cudaMemsetAsync(p, 0, words * 8, s_), "evalpoly zero");
+        return p;
+    }
+
+    // n contiguous buffers of `limbs` limbs each, zeroed by one memset when asked
+    std::vector<uint64_t*> buffers(size_t n, size_t limbs, bool zero) {
+        const size_t words = std::max<size_t>(limbs, 1) * c_.N;
+        uint64_t* base = carve(words * std::max<size_t>(n, 1));
+        if (zero && n) check_cuda(cudaMemsetAsync(base, 0, words * n * 8, s_), "evalpoly zero");
+        std::vector<uint64_t*> out(n);
+        for (size_t i = 0; i < n; ++i) out[i] = base + i * words;
+        return out;
     }
     uint64_t* scratch(size_t limbs) { return buffer(limbs, false); }
 
@@ -421,6 +586,9 @@ private:
     size_t count_;
     cudaStream_t s_;
     std::vector<uint64_t*> owned_;
+    uint64_t* cur_ = nullptr;
+    size_t left_ = 0, next_chunk_ = kFirstChunkWords;
+    std::map<std::tuple<double, double, double, size_t>, uint64_t*> const_cache_;
 };
 
 }  // namespace

@@ -10,7 +10,9 @@
 // the scalar product (re = fma(a, c, -(b d)), im = fma(a, d, b c)) for the twiddle recurrences
 // and the butterflies, the vectorised one (re = fma(a, c, -(b d)), im = fma(b, c, a d)) for the
 // twist loop.  The file is compiled with -ffp-contract=off so nothing else is fused.
+#include <atomic>
 #include <bit>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstddef>
@@ -117,12 +119,20 @@ void fft_dif(std::vector<Cplx>& x, const std::vector<Cplx>& tw, size_t N) {
     }
 }
 
+std::atomic<uint64_t> g_encode_calls{0}, g_encode_ns{0};
+
 }  // namespace
+
+void encode_stats(uint64_t* calls, uint64_t* ns) {
+    *calls = g_encode_calls.load();
+    *ns = g_encode_ns.load();
+}
 
 void encode_slots(size_t N, const double* re, const double* im, double scale, const uint64_t* moduli, size_t limbs,
                   uint64_t* out) {
     if (!(scale > 0.0)) throw std::invalid_argument("ckks_encode: scale must be positive");
     if (N < 2 || (N & (N - 1))) throw std::invalid_argument("ckks_encode: ring degree must be a power of two");
+    const auto t0 = std::chrono::steady_clock::now();
     const FftTables& t = tables(N);
     const size_t half = N >> 1;
     std::vector<Cplx> ev(N);
@@ -143,6 +153,9 @@ void encode_slots(size_t N, const double* re, const double* im, double scale, co
             o[i] = static_cast<uint64_t>(r + (q & (r >> 63)));
         }
     }
+    g_encode_calls.fetch_add(1, std::memory_order_relaxed);
+    g_encode_ns.fetch_add((uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count(),
+                          std::memory_order_relaxed);
 }
 
 }  // namespace host

@@ -11,5 +11,8 @@ namespace host {
 void encode_slots(size_t N, const double* re, const double* im, double scale, const uint64_t* moduli, size_t limbs,
                   uint64_t* out);
 
+// Calls of encode_slots so far and their summed wall time (ns).
+void encode_stats(uint64_t* calls, uint64_t* ns);
+
 }  // namespace host
 }  // namespace wg

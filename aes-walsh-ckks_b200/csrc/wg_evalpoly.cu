@@ -570,6 +570,7 @@ void bootstrap_evalmod(Context& c, const BootstrapParams& p, const S2cPlan* plan
     size_t level = p.s2c_depth;
     // SlotToCoeff
     for (size_t k = 0; k < ns2c; ++k) {
+        WG_SPAN("boot.s2c");
         if (lt_stage_level(*s2c[k]) != level) throw std::invalid_argument("ckks_linear_transform: stage level mismatch");
         lt_stage_apply(c, *s2c[k], count, b, a, s);
         if (lt_stage_rescales(*s2c[k])) --level;
@@ -600,6 +601,7 @@ void bootstrap_evalmod(Context& c, const BootstrapParams& p, const S2cPlan* plan
     DeviceOps ops(c, count, s);
     // sparse-slot trace: ct += rotate(ct, r) for r = active, 2 active, ... < slots
     for (size_t r = p.active_slots; r < p.slots; r <<= 1) {
+        WG_SPAN("boot.trace");
         CtBatch x = ops.wrap(b, a, level, 0.0L);
         CtBatch rot = ops.clone(x);
         const KeyEntry& k = c.key(WG_KEY_ROTATION, (int64_t)r);
@@ -622,6 +624,7 @@ void bootstrap_evalmod(Context& c, const BootstrapParams& p, const S2cPlan* plan
     }
     // CoeffToSlot
     for (size_t k = 0; k < nc2s; ++k) {
+        WG_SPAN("boot.c2s");
         if (lt_stage_level(*c2s[k]) != level) throw std::invalid_argument("ckks_linear_transform: stage level mismatch");
         lt_stage_apply(c, *c2s[k], count, b, a, s);
         if (lt_stage_rescales(*c2s[k])) --level;
@@ -652,7 +655,10 @@ void bootstrap_evalmod(Context& c, const BootstrapParams& p, const S2cPlan* plan
     // EvalMod on both halves at once
     DeviceOps ops2(c, 2 * count, s);
     CtBatch x = ops2.wrap(eb.data(), ea.data(), level, static_cast<long double>(std::exp2((double)p.evalmod_log_scale)));
-    CtBatch y = chebyshev(c, ops2, x, coeffs, ncoeffs, p.scale, p.scale);
+    CtBatch y = [&] {
+        WG_SPAN("boot.evalmod");
+        return chebyshev(c, ops2, x, coeffs, ncoeffs, p.scale, p.scale);
+    }();
     y.scale = p.scale;
     const long double target = y.scale;
     for (size_t i = 0; i < p.double_angle; ++i) {

@@ -4,11 +4,15 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <deque>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
+
+#include "wg_hostspan.hpp"
 #include <vector>
 
 #include "wg_arith.cuh"
@@ -81,16 +85,33 @@ struct Workspace {
 };
 
 struct Context;
+// Staging uploads so far: calls, bytes and the time spent waiting for ring space.
+void stage_stats(uint64_t* calls, uint64_t* bytes, uint64_t* wait_ns);
+
 // Per-stream buffers of the batched path: the job-table image (pinned stage + device copy)
 // and a scratch arena, both grown on demand outside stream capture.
+// Per-stream buffers of the batched paths.  Host-to-device staging (job tables, public
+// plaintexts) goes through a ring: a pinned host buffer mirrored by a device buffer, filled
+// front to back; each upload records an event, and a region is rewritten only after the
+// upload that last used it has completed, so the host runs ahead of the device instead of
+// waiting for every copy.  Device-side reuse is safe in stream order: a later copy into a
+// region executes after every kernel queued before it on the same stream.
 struct BatchBuffers {
-    void* d_jobs = nullptr;
-    void* h_jobs = nullptr;
-    size_t jobs_bytes = 0;
-    cudaEvent_t staged_event = nullptr;
+    struct Flight {
+        size_t begin, end;
+        cudaEvent_t done;
+    };
+    unsigned char* d_ring = nullptr;
+    unsigned char* h_ring = nullptr;
+    size_t ring_bytes = 0;
+    size_t head = 0;
+    std::deque<Flight> flights;
+    std::vector<cudaEvent_t> spare_events;
     uint64_t* d_arena = nullptr;
     size_t arena_words = 0;
-    void ensure_jobs(const Context& c, size_t bytes, cudaStream_t s);
+    // Copy `bytes` of host data into the ring and onto the device (stream order); returns the
+    // device address, valid for kernels queued on `s` before the ring wraps back over it.
+    void* stage(const Context& c, const void* data, size_t bytes, cudaStream_t s);
     uint64_t* arena(const Context& c, size_t words, cudaStream_t s);
     void release();
 };
@@ -124,6 +145,18 @@ struct Context {
     std::vector<uint64_t> rs_host;
     std::vector<size_t> rs_host_off;
     BatchBuffers& batch_buffers(cudaStream_t s);
+    // Evaluation-form plaintexts of slot-constant values, kept for the context's lifetime
+    // (keyed by value, scale and limb count); `ready` follows the NTT that filled them on
+    // `stream`, for users on other streams.
+    struct ConstPlain {
+        uint64_t* d;
+        cudaEvent_t ready;
+        cudaStream_t stream;
+        size_t bytes;
+    };
+    std::mutex const_mutex;
+    std::map<std::tuple<double, double, double, size_t>, ConstPlain> consts;
+    size_t const_bytes = 0;
 
     ~Context();
     uint64_t* workspace(cudaStream_t s);   // scratch for one in-flight operation on stream s
@@ -172,6 +205,9 @@ struct Probe {
     Probe& operator=(const Probe&) = delete;
     int slot = -1;
     cudaStream_t stream;
+#ifdef WG_HOST_SPANS
+    HostSpan span{"launch"};
+#endif
 };
 
 // ---------------------------------------------------------------------------------------

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "../../include/walsh_gpu.h"
+#include "wg_encode.hpp"
 #include "wg_internal.hpp"
 
 namespace wg {
@@ -53,7 +54,47 @@ void probe_add(const uint64_t* counts) {
 
 }  // namespace wg
 
+#ifdef WG_HOST_SPANS
+#include <cstdio>
+#include <map>
+#include <string>
+namespace wg {
+namespace {
+std::mutex g_span_mu;
+std::map<std::string, std::pair<uint64_t, uint64_t>> g_spans;  // name -> (count, ns)
+}  // namespace
+void host_span_add(const char* name, uint64_t ns) {
+    std::lock_guard<std::mutex> g(g_span_mu);
+    auto& e = g_spans[name];
+    e.first += 1;
+    e.second += ns;
+}
+}  // namespace wg
+extern "C" int wg_host_spans(char* buf, size_t n) {
+    std::lock_guard<std::mutex> g(wg::g_span_mu);
+    std::string out;
+    for (const auto& kv : wg::g_spans) {
+        char line[256];
+        std::snprintf(line, sizeof line, "%s %llu %.3f\n", kv.first.c_str(), (unsigned long long)kv.second.first,
+                      kv.second.second / 1e6);
+        out += line;
+    }
+    wg::g_spans.clear();
+    std::snprintf(buf, n, "%s", out.c_str());
+    return 0;
+}
+#endif
+
 extern "C" {
+
+int wg_host_stats(uint64_t* out, size_t n) {
+    if (!out) return WG_ERR_INVALID;
+    uint64_t v[5] = {};
+    wg::host::encode_stats(&v[0], &v[1]);
+    wg::stage_stats(&v[2], &v[3], &v[4]);
+    for (size_t i = 0; i < n && i < 5; ++i) out[i] = v[i];
+    return WG_OK;
+}
 
 uint64_t wg_launch_count(int kernel_class) {
     auto& st = wg::state();

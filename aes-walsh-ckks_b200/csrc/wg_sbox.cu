@@ -20,11 +20,13 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <optional>
 #include <stdexcept>
 #include <vector>
 
 #include "wg_ctops.cuh"
+#include "wg_walsh.cuh"
 
 namespace wg {
 namespace {
@@ -97,6 +99,97 @@ bool close_ld(long double l, long double r, long double tol = 0x1p-45L) {
     return std::abs(l - r) <= tol * m;
 }
 
+constexpr int kMaxLinLimbs = 16;
+
+struct SumJob {
+    uint64_t* out;
+    const uint64_t* src[kSegments];
+    int n, mod;
+};
+
+// out = sum of n residues (mod q): exact, so independent of the order the reference adds in
+__global__ void __launch_bounds__(kT) kb_sum(const SumJob* jobs, int njobs, const Modulus* mods) {
+    const SumJob* j = job_of(jobs, njobs);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const uint64_t q = mods[j->mod].q;
+    uint64_t acc = j->src[0][k];
+    for (int t = 1; t < j->n; ++t) acc = add_mod(acc, j->src[t][k], q);
+    j->out[k] = acc;
+}
+
+// Coefficients of one paired linear combination real + i imag over the 15 nonzero nibble masks.
+struct LinCoefs {
+    int8_t cr[kNibble], ci[kNibble];
+    uint64_t c0r[kMaxLinLimbs], c0i[kMaxLinLimbs];  // integer constants (b polynomial), per limb
+};
+
+// One limb of one instance for the fused Walsh products (masks 1..15 at their own index).
+struct WalshJob {
+    const uint64_t* low[2][kNibble];    // [b|a][mask]
+    const uint64_t* high[2][kNibble];
+    const uint64_t* pt_i;
+    uint64_t* out[5];                   // acc b, acc a, raw b, raw a, raw c2
+    int limb, pad;
+};
+
+__global__ void __launch_bounds__(kT, 2) kb_walsh_products(const WalshJob* jobs, int n, const WalshCoefs* cf,
+                                                           const Modulus* mods) {
+    const WalshJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const Modulus m = mods[j->limb];
+    const uint64_t pt_i = j->pt_i[k];
+    uint64_t lb[kNibble], la[kNibble];
+    lb[0] = la[0] = 0;
+#pragma unroll
+    for (int t = 1; t < (int)kNibble; ++t) {
+        lb[t] = j->low[0][t][k];
+        la[t] = j->low[1][t][k];
+    }
+    WalshLow w;
+    walsh_load_low(lb, la, w);
+    uint64_t acc_b, acc_a;
+    walsh_constant_pair(w, *cf, j->limb, pt_i, m, &acc_b, &acc_a);
+    j->out[0][k] = acc_b;
+    j->out[1][k] = acc_a;
+    uint64_t rb = 0, ra = 0, rc = 0;
+#pragma unroll 1
+    for (int hm = 1; hm < (int)kNibble; ++hm)
+        walsh_product(w, *cf, hm, j->limb, pt_i, m, j->high[0][hm][k], j->high[1][hm][k], &rb, &ra, &rc);
+    j->out[2][k] = rb;
+    j->out[3][k] = ra;
+    j->out[4][k] = rc;
+}
+
+struct LinJob {
+    uint64_t* out;
+    const uint64_t* terms[kNibble - 1];  // sign ciphertext of mask m at terms[m - 1]
+    const uint64_t* pt_i;                // evaluation form of the slot constant i, this limb
+    int limb, poly;
+};
+
+// out = (c0r + sum_m cr[m] s_m) + pt_i * (c0i + sum_m ci[m] s_m) (mod q), one limb of one
+// polynomial.  Exact modular sums, so equal to the reference's sequence of additions of
+// precomputed multiples; pt_i times x by a Barrett product of canonical residues.
+__global__ void __launch_bounds__(kT) kb_lin_pair(const LinJob* jobs, int n, LinCoefs cf, const Modulus* mods) {
+    const LinJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const Modulus m = mods[j->limb];
+    const uint64_t q = m.q;
+    uint64_t r = j->poly == 0 ? cf.c0r[j->limb] : 0, im = j->poly == 0 ? cf.c0i[j->limb] : 0;
+#pragma unroll
+    for (int t = 1; t < (int)kNibble; ++t) {
+        const int a = cf.cr[t], b = cf.ci[t];
+        if (a == 0 && b == 0) continue;
+        const uint64_t x = j->terms[t - 1][k];
+        if (a) r = add_mod(r, barrett_mul(x, a > 0 ? (uint64_t)a : q - (uint64_t)(-a), m), q);
+        if (b) im = add_mod(im, barrett_mul(x, b > 0 ? (uint64_t)b : q - (uint64_t)(-b), m), q);
+    }
+    j->out[k] = add_mod(r, barrett_mul(im, j->pt_i[k], m), q);
+}
+
 class Sbox {
 public:
     Sbox(Context& c, DeviceOps& ops, cudaStream_t s) : c_(c), ops_(ops), s_(s), table_(walsh_table()) {}
@@ -141,30 +234,89 @@ public:
         batch_keyswitch(c_, items.data(), items.size(), s_);
     }
 
-    // 1. build_mask_packed_parity_input
+    // 1. build_mask_packed_parity_input: the 30 nibble parities (one launch), their segment
+    // rotations (one batched key switch), and their sum (one launch)
     CtBatch pack(const std::vector<CtBatch>& in, size_t bc) {
-        std::optional<CtBatch> packed;
+        WG_SPAN("sbox.pack");
+        const size_t N = c_.N, level = in[0].level, L = level + 1, cnt = ops_.count();
+        std::vector<CtBatch> terms(kSegments);
+        std::vector<SumJob> par;
         for (size_t mask = 1; mask < kNibble; ++mask)
             for (int high = 0; high < 2; ++high) {
-                CtBatch t = parity(in, high ? 4 : 0, mask);
                 const size_t seg = (high ? kNibble - 1 : 0) + (mask - 1);
-                if (seg) rotate(t, (int64_t)(seg * bc));
-                if (!packed)
-                    packed = t;
-                else
-                    ops_.add(*packed, t, false);
+                CtBatch t = ops_.alloc(level, 2);
+                t.scale = in[0].scale;
+                for (size_t i = 0; i < cnt; ++i)
+                    for (int poly = 0; poly < 2; ++poly)
+                        for (size_t l = 0; l < L; ++l) {
+                            SumJob jb{};
+                            jb.out = t.p[i][poly] + l * N;
+                            for (size_t bit = 0; bit < 4; ++bit)
+                                if ((mask >> bit) & 1) jb.src[jb.n++] = in[(high ? 4 : 0) + bit].p[i][poly] + l * N;
+                            jb.mod = (int)l;
+                            par.push_back(jb);
+                        }
+                terms[seg] = t;
             }
-        return *packed;
+        run_sums(par);
+        std::vector<KsItem> items;
+        for (size_t seg = 1; seg < kSegments; ++seg) {
+            const int64_t slots = (int64_t)(N / 2);
+            int64_t r = (int64_t)(seg * bc) % slots;
+            if (r == 0) continue;
+            const KeyEntry& k = c_.key(WG_KEY_ROTATION, r);
+            for (size_t i = 0; i < cnt; ++i) {
+                KsItem it;
+                it.level = level;
+                it.key_term = terms[seg].p[i][1];
+                it.key = &k;
+                it.b_in = terms[seg].p[i][0];
+                it.a_in = terms[seg].p[i][1];
+                it.b = terms[seg].p[i][0];
+                it.a = terms[seg].p[i][1];
+                it.b_add = 1;
+                it.a_add = 0;
+                it.galois = host::powmod(5, (uint64_t)r, 2 * N);
+                items.push_back(it);
+            }
+        }
+        batch_keyswitch(c_, items.data(), items.size(), s_);
+        CtBatch packed = ops_.alloc(level, 2);
+        packed.scale = in[0].scale;
+        std::vector<SumJob> tot;
+        for (size_t i = 0; i < cnt; ++i)
+            for (int poly = 0; poly < 2; ++poly)
+                for (size_t l = 0; l < L; ++l) {
+                    SumJob jb{};
+                    jb.out = packed.p[i][poly] + l * N;
+                    for (size_t seg = 0; seg < kSegments; ++seg) jb.src[jb.n++] = terms[seg].p[i][poly] + l * N;
+                    jb.mod = (int)l;
+                    tot.push_back(jb);
+                }
+        run_sums(tot);
+        return packed;
+    }
+
+    void run_sums(const std::vector<SumJob>& jobs) {
+        if (jobs.empty()) return;
+        JobTable t;
+        const SumJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 8.0 * c_.N * jobs.size() * 5.0, s_);
+        kb_sum<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        check_cuda(cudaGetLastError(), "walsh parity sums");
     }
 
     // 2. parities -> signs: x <- -2 x + 1
     void to_sign(CtBatch& x) {
+        WG_SPAN("sbox.to_sign");
         ops_.mul_int(x, -2);
         add_int(x, 1);
     }
 
     // 3. unpack_mask_packed_signs: low[0] = high[0] = constant 1, low[m] / high[m] rotated back
     void unpack(const CtBatch& lane, size_t bc, std::vector<CtBatch>& low, std::vector<CtBatch>& high) {
+        WG_SPAN("sbox.unpack");
         const size_t N = c_.N, L = lane.level + 1;
         low.assign(kNibble, CtBatch{});
         high.assign(kNibble, CtBatch{});
@@ -182,9 +334,16 @@ public:
             low[mask] = lane;
             high[mask] = lane;
         }
+        std::vector<const uint64_t*> lb(ops_.count()), la(ops_.count());
+        std::vector<uint64_t*> outs(ops_.count());
         for (size_t i = 0; i < ops_.count(); ++i) {
-            uint64_t* out = ops_.raw(rots.size() * 2 * L);
-            rotate_many(c_, lane.level, lane.p[i][0], lane.p[i][1], rots.data(), rots.size(), out, s_);
+            lb[i] = lane.p[i][0];
+            la[i] = lane.p[i][1];
+            outs[i] = ops_.raw(rots.size() * 2 * L);
+        }
+        rotate_many_batch(c_, lane.level, ops_.count(), lb.data(), la.data(), rots.data(), rots.size(), outs.data(), s_);
+        for (size_t i = 0; i < ops_.count(); ++i) {
+            uint64_t* out = outs[i];
             for (size_t mask = 1; mask < kNibble; ++mask) {
                 const size_t kl = 2 * (mask - 1), kh = kl + 1;
                 low[mask].p[i] = {out + (2 * kl) * L * N, out + (2 * kl + 1) * L * N, nullptr};
@@ -199,20 +358,14 @@ public:
 
     // 4. recombine_mask_packed_signs_to_paired_outputs
     std::vector<CtBatch> recombine(const std::vector<CtBatch>& low, const std::vector<CtBatch>& high) {
+        WG_SPAN("sbox.recombine");
         if (low[1].level == 0) throw std::runtime_error("ckks_walsh_sbox: sign output level is too low for 4+4 products");
-        // multiples[m][k] = k * low[m], k = 1..8
-        std::array<std::array<std::optional<CtBatch>, kMaxAbsCoeff + 1>, kNibble> mult;
-        for (size_t m = 1; m < kNibble; ++m) {
-            mult[m][1] = ops_.clone(low[m]);
-            for (size_t k = 2; k <= kMaxAbsCoeff; ++k) {
-                CtBatch v = ops_.clone(*mult[m][k - 1]);
-                ops_.add(v, low[m], false);
-                mult[m][k] = v;
-            }
-        }
+        for (size_t m = 1; m < kNibble; ++m)
+            if (low[m].level != low[0].level || !close_ld(low[m].scale, low[0].scale))
+                throw std::invalid_argument("ckks_walsh_sbox: same-metadata addition mismatch");
         std::vector<CtBatch> out;
         for (size_t pair = 0; pair < kBits / 2; ++pair) {
-            CtBatch ws = walsh_sum(low, high, pair, pair + kBits / 2, mult);
+            CtBatch ws = walsh_sum(low, high, pair, pair + kBits / 2);
             out.push_back(to_bit_pair(ws));
         }
         return out;
@@ -220,6 +373,7 @@ public:
 
     // 5. combine_paired_lane_outputs_as_complex_bits
     std::vector<CtBatch> combine_lanes(const std::vector<CtBatch>& lane0, const std::vector<CtBatch>& lane1) {
+        WG_SPAN("sbox.combine_lanes");
         std::vector<CtBatch> bits(kBits);
         for (size_t pair = 0; pair < kBits / 2; ++pair) {
             auto [rl, rh] = split(lane0[pair]);
@@ -243,21 +397,60 @@ private:
         return *out;
     }
 
-    using Multiples = std::array<std::array<std::optional<CtBatch>, kMaxAbsCoeff + 1>, kNibble>;
-
-    // linear_combination_with_constant: c0 + sum_m c_m s_m with precomputed multiples
-    CtBatch lin(const std::vector<CtBatch>& signs, const std::array<int16_t, kNibble>& coeffs, const Multiples& mult) {
-        CtBatch out = ops_.zeros(signs[0].level, signs[0].scale);
-        if (coeffs[0] != 0) add_int(out, coeffs[0]);
-        for (size_t m = 1; m < kNibble; ++m) {
-            const int16_t cf = coeffs[m];
-            if (cf == 0) continue;
-            const int a = cf < 0 ? -cf : cf;
-            if (a > (int)kMaxAbsCoeff) throw std::runtime_error("ckks_walsh_sbox: missing low-sign multiple");
-            if (!close_ld(out.scale, mult[m][a]->scale)) throw std::invalid_argument("ckks_walsh_sbox: same-metadata addition mismatch");
-            ops_.add(out, *mult[m][a], cf < 0);
+    // linear_combination_pair_with_constant: (c0 + sum_m c_m s_m) for the real and imaginary
+    // coefficient sets, combined as real + i imag (combine_real_imag), in one launch.  The
+    // reference adds precomputed multiples |c| s_m one by one; the modular sum is the same.
+    CtBatch lin_pair(const std::vector<CtBatch>& signs, const std::array<int16_t, kNibble>& rc,
+                     const std::array<int16_t, kNibble>& ic) {
+        const size_t N = c_.N, level = signs[0].level, L = level + 1;
+        if (L > (size_t)kMaxLinLimbs) throw std::invalid_argument("ckks_walsh_sbox: too many limbs");
+        LinCoefs cf{};
+        for (size_t m = 0; m < kNibble; ++m) {
+            if (rc[m] < -(int)kMaxAbsCoeff || rc[m] > (int)kMaxAbsCoeff || ic[m] < -(int)kMaxAbsCoeff ||
+                ic[m] > (int)kMaxAbsCoeff)
+                throw std::runtime_error("ckks_walsh_sbox: missing low-sign multiple");
+            cf.cr[m] = (int8_t)rc[m];
+            cf.ci[m] = (int8_t)ic[m];
         }
+        const long double scale = signs[0].scale;
+        for (size_t l = 0; l < L; ++l) {
+            cf.c0r[l] = int_const(rc[0], scale, c_.q[l]);
+            cf.c0i[l] = int_const(ic[0], scale, c_.q[l]);
+        }
+        const uint64_t* pti = ops_.constant_plaintext(L, 0.0, 1.0, 1.0);
+        CtBatch out = ops_.alloc(level, 2);
+        out.scale = scale;
+        std::vector<LinJob> jobs;
+        for (size_t i = 0; i < ops_.count(); ++i)
+            for (int poly = 0; poly < 2; ++poly)
+                for (size_t l = 0; l < L; ++l) {
+                    LinJob jb{};
+                    jb.out = out.p[i][poly] + l * N;
+                    for (size_t m = 1; m < kNibble; ++m) jb.terms[m - 1] = signs[m].p[i][poly] + l * N;
+                    jb.pt_i = pti + l * N;
+                    jb.limb = (int)l;
+                    jb.poly = poly;
+                    jobs.push_back(jb);
+                }
+        JobTable t;
+        const LinJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 17.0, s_);
+        kb_lin_pair<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), cf, c_.d_mod);
+        check_cuda(cudaGetLastError(), "walsh linear combination");
         return out;
+    }
+
+    // rounded_scaled_integer_mod_q
+    static uint64_t int_const(int64_t k, long double scale, uint64_t q) {
+        if (k == 0) return 0;
+        const long double scaled = static_cast<long double>(k) * scale;
+        if (!std::isfinite(scaled)) throw std::invalid_argument("ckks_add_integer_constant_inplace: non-finite scaled constant");
+        long double r = std::fmod(std::round(scaled), static_cast<long double>(q));
+        if (r < 0.0L) r += static_cast<long double>(q);
+        uint64_t u = static_cast<uint64_t>(r);
+        if (u >= q) u %= q;
+        return u;
     }
 
     bool same_storage(const CtBatch& x, const CtBatch& y) const {
@@ -273,13 +466,6 @@ private:
             add_term(real, imag);
         }
         return real;
-    }
-
-    CtBatch lin_pair(const std::vector<CtBatch>& signs, const std::array<int16_t, kNibble>& rc,
-                     const std::array<int16_t, kNibble>& ic, const Multiples& mult) {
-        CtBatch real = lin(signs, rc, mult);
-        CtBatch imag = lin(signs, ic, mult);
-        return combine_ri(real, imag);
     }
 
     // multiply_by_integer_scalar_inplace (the S-box's own: int64 multiply, then scale)
@@ -338,23 +524,91 @@ private:
         return lhs;
     }
 
+    // The constant-term combination and the 15 unrelinearised products of one output pair in
+    // one launch (the high signs share level and scale with the low ones, so the reference's
+    // mul_raw multiplies without re-aligning and every step is an exact modular operation).
+    std::pair<CtBatch, CtBatch> walsh_fused(const std::vector<CtBatch>& low, const std::vector<CtBatch>& high, size_t rb,
+                                            size_t ib, long double target) {
+        const size_t N = c_.N, level = low[0].level, L = level + 1, cnt = ops_.count();
+        if (L > (size_t)kWalshLimbs) throw std::invalid_argument("ckks_walsh_sbox: too many limbs");
+        std::vector<WalshCoefs> cf(1);
+        std::memset(cf.data(), 0, sizeof(WalshCoefs));
+        const long double scale = low[0].scale;
+        for (size_t hm = 0; hm < kNibble; ++hm) {
+            for (size_t lm = 0; lm < kNibble; ++lm) {
+                const int rcm = table_[rb][lm][hm], icm = table_[ib][lm][hm];
+                if (lm > 0 && (rcm < -(int)kMaxAbsCoeff || rcm > (int)kMaxAbsCoeff || icm < -(int)kMaxAbsCoeff ||
+                               icm > (int)kMaxAbsCoeff))
+                    throw std::runtime_error("ckks_walsh_sbox: missing low-sign multiple");
+                reinterpret_cast<int8_t*>(cf[0].cw[0][hm])[lm] = (int8_t)(lm ? rcm : 0);
+                reinterpret_cast<int8_t*>(cf[0].cw[1][hm])[lm] = (int8_t)(lm ? icm : 0);
+            }
+            for (size_t l = 0; l < L; ++l) {
+                cf[0].c0[0][hm][l] = int_const(table_[rb][0][hm], scale, c_.q[l]);
+                cf[0].c0[1][hm][l] = int_const(table_[ib][0][hm], scale, c_.q[l]);
+            }
+        }
+        const uint64_t* pti = ops_.constant_plaintext(L, 0.0, 1.0, 1.0);
+        CtBatch acc = ops_.alloc(level, 2);
+        acc.scale = scale;
+        CtBatch raw = ops_.alloc(level, 3);
+        raw.scale = target * high[1].scale;
+        std::vector<WalshJob> jobs;
+        for (size_t i = 0; i < cnt; ++i)
+            for (size_t l = 0; l < L; ++l) {
+                WalshJob jb{};
+                for (size_t m = 1; m < kNibble; ++m)
+                    for (int poly = 0; poly < 2; ++poly) {
+                        jb.low[poly][m] = low[m].p[i][poly] + l * N;
+                        jb.high[poly][m] = high[m].p[i][poly] + l * N;
+                    }
+                jb.pt_i = pti + l * N;
+                jb.out[0] = acc.p[i][0] + l * N;
+                jb.out[1] = acc.p[i][1] + l * N;
+                for (int poly = 0; poly < 3; ++poly) jb.out[2 + poly] = raw.p[i][poly] + l * N;
+                jb.limb = (int)l;
+                jobs.push_back(jb);
+            }
+        JobTable t;
+        const WalshCoefs* cfd = t.add(cf);
+        const WalshJob* j = t.add(jobs);
+        t.upload(c_, s_);
+        Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 66.0, s_);
+        kb_walsh_products<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), t.at(cfd), c_.d_mod);
+        check_cuda(cudaGetLastError(), "walsh products");
+        return {acc, raw};
+    }
+
     // walsh_sum_for_output_pair
-    CtBatch walsh_sum(const std::vector<CtBatch>& low, const std::vector<CtBatch>& high, size_t rb, size_t ib,
-                      const Multiples& mult) {
+    CtBatch walsh_sum(const std::vector<CtBatch>& low, const std::vector<CtBatch>& high, size_t rb, size_t ib) {
+        WG_SPAN("sbox.walsh_sum");
         const long double target = low[0].scale;
         std::array<int16_t, kNibble> rc{}, ic{};
         for (size_t lm = 0; lm < kNibble; ++lm) {
             rc[lm] = table_[rb][lm][0];
             ic[lm] = table_[ib][lm][0];
         }
-        CtBatch acc = lin_pair(low, rc, ic, mult);
+        // the constant term and the 15 raw products in one pass when the signs share level and
+        // scale (the reference's mul_raw then multiplies without re-aligning)
+        bool uniform = true;
+        for (size_t m = 1; m < kNibble; ++m)
+            uniform = uniform && high[m].level == low[0].level && close_ld(high[m].scale, target) &&
+                      high[m].level > 0 && low[0].level > 0 && low[m].level == low[0].level &&
+                      close_ld(low[m].scale, target) && low[m].np == 2 && high[m].np == 2;
+        if (uniform) {
+            auto [acc, raw] = walsh_fused(low, high, rb, ib, target);
+            ops_.relin(raw);
+            add_term(acc, raw);
+            return acc;
+        }
+        CtBatch acc = lin_pair(low, rc, ic);
         std::optional<CtBatch> raw;
         for (size_t hm = 1; hm < kNibble; ++hm) {
             for (size_t lm = 0; lm < kNibble; ++lm) {
                 rc[lm] = table_[rb][lm][hm];
                 ic[lm] = table_[ib][lm][hm];
             }
-            CtBatch ls = lin_pair(low, rc, ic, mult);
+            CtBatch ls = lin_pair(low, rc, ic);
             CtBatch prod = mul_raw(ls, high[hm], target);
             if (!raw)
                 raw = prod;

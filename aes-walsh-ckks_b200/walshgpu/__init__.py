@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
         L.wg_launch_count.restype = C.c_uint64
         L.wg_probe_begin.argtypes = [C.c_int, C.c_int]
         L.wg_probe_end.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.wg_host_stats.argtypes = [C.POINTER(C.c_uint64), C.c_size_t]
         L.wg_malloc.argtypes = [C.POINTER(vp), sz]
         L.wg_free.argtypes = [vp]
         L.wg_memcpy_htod.argtypes = [vp, vp, sz, vp]
@@ -152,6 +153,14 @@ def launch_count(kernel_class=-1) -> int:
 def probe_begin(kernel_class, max_launches=60000):
     """Start CUDA-event timing of every launch of one kernel class."""
     _check(lib().wg_probe_begin(kernel_class, max_launches))
+
+
+def host_stats() -> dict:
+    """Host-side counters: slot encodings and their time, staged uploads, bytes, waits."""
+    out = (C.c_uint64 * 5)()
+    _check(lib().wg_host_stats(out, 5))
+    return {"encodes": out[0], "encode_ms": out[1] / 1e6, "stages": out[2], "stage_bytes": out[3],
+            "stage_wait_ms": out[4] / 1e6}
 
 
 def probe_end():

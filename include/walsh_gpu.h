@@ -323,6 +323,11 @@ uint64_t wg_launch_count(int kernel_class);
 int wg_probe_begin(int kernel_class, int max_launches);
 int wg_probe_end(uint64_t* launches, double* total_ms, double* total_bytes);
 
+/* Host-side counters: out[0] slot encodings, out[1] their wall time (ns), out[2] staged
+ * host-to-device uploads, out[3] their bytes, out[4] time spent waiting for staging space (ns).
+ * Writes the first n of them. */
+int wg_host_stats(uint64_t* out, size_t n);
+
 /* Plain device-memory helpers for C callers without another allocator. */
 int wg_malloc(void** ptr, size_t bytes);
 int wg_free(void* ptr);

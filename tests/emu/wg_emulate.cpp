@@ -13,6 +13,7 @@
 #include "wg_keyswitch.cuh"
 #include "wg_ntt.cuh"
 #include "wg_tables.hpp"
+#include "wg_walsh.cuh"
 
 using namespace wg;
 
@@ -186,6 +187,42 @@ void emu_keyswitch(void* h, size_t level, const uint64_t* key_term, const uint64
                 b[qi * N + i] = tb[qi * N + s];
                 a[qi * N + i] = ta[qi * N + s];
             }
+    }
+}
+
+static Modulus emu_modulus(uint64_t q) {
+    Modulus m{};
+    const unsigned __int128 mu = ~(unsigned __int128)0 / q;
+    m.q = q;
+    m.mu_lo = (uint64_t)mu;
+    m.mu_hi = (uint64_t)(mu >> 64);
+    return m;
+}
+
+// reduce128 on n values (hi[i], lo[i]) modulo q
+void emu_reduce128(uint64_t q, const uint64_t* hi, const uint64_t* lo, size_t n, uint64_t* out) {
+    const Modulus m = emu_modulus(q);
+    for (size_t i = 0; i < n; ++i) out[i] = reduce128(hi[i], lo[i], m);
+}
+
+// The fused Walsh products at n residue positions of one limb (limb index 0, modulus q).
+// low_b, low_a, high_b, high_a: [n][16] (mask 0 ignored); coefs: [2][16][16] int8; c0: [2][16];
+// out: [n][5] = acc b, acc a, raw b, raw a, raw c2.
+void emu_walsh_products(uint64_t q, size_t n, const uint64_t* low_b, const uint64_t* low_a, const uint64_t* high_b,
+                        const uint64_t* high_a, const uint64_t* pt_i, const int8_t* coefs, const uint64_t* c0,
+                        uint64_t* out) {
+    const Modulus m = emu_modulus(q);
+    WalshCoefs cf{};
+    std::memcpy(cf.cw, coefs, sizeof(cf.cw));  // [2][16][16] int8, little-endian words
+    for (int r = 0; r < 2; ++r)
+        for (int hm = 0; hm < kWalshMasks; ++hm) cf.c0[r][hm][0] = c0[r * kWalshMasks + hm];
+    for (size_t i = 0; i < n; ++i) {
+        WalshLow w;
+        walsh_load_low(low_b + i * 16, low_a + i * 16, w);
+        uint64_t* o = out + i * 5;
+        walsh_constant_pair(w, cf, 0, pt_i[i], m, o, o + 1);
+        for (int hm = 1; hm < kWalshMasks; ++hm)
+            walsh_product(w, cf, hm, 0, pt_i[i], m, high_b[i * 16 + hm], high_a[i * 16 + hm], o + 2, o + 3, o + 4);
     }
 }
 

@@ -1,6 +1,6 @@
 """CPU emulation of the device kernels against the oracle.
 
-tests/emu/wg_emulate.cpp compiles the product's kernel bodies (wg_ntt.cuh, wg_keyswitch.cuh)
+tests/emu/wg_emulate.cpp compiles the product's kernel bodies (wg_ntt.cuh, wg_keyswitch.cuh, wg_walsh.cuh)
 and table builder with the host compiler and runs them thread by thread.  This checks index
 logic, butterflies, HPS base changes and tables without a GPU; the GPU tests then check the
 compiled kernels themselves.
@@ -91,3 +91,87 @@ def test_emulated_ntt_large_rings(oracle_mod, emu, logN):
         assert (y == x).all()
     finally:
         emu.emu_destroy(h)
+
+
+# NTT-friendly moduli of the walsh15 chain (36, 50 and 61 bits), the Mersenne prime 2^61 - 1 and
+# the primes either side of 2^55 (where the Walsh sums switch from one word to 32-bit halves)
+WIDE_MODULI = [68718428161, 1125899904679937, 2305843009208713217, 2305843009211596801, (1 << 61) - 1,
+               36028797018963913, 36028797018963971]
+
+
+def _bind_walsh(E):
+    E.emu_reduce128.argtypes = [C.c_uint64, u64p, u64p, C.c_size_t, u64p]
+    i8p = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+    E.emu_walsh_products.argtypes = [C.c_uint64, C.c_size_t, u64p, u64p, u64p, u64p, u64p, i8p, u64p, u64p]
+
+
+@pytest.mark.parametrize("q", WIDE_MODULI)
+def test_reduce128_canonical(emu, q):
+    """reduce128 returns the canonical residue for any 128-bit value, including values a hair
+    above or below a multiple of q, where a single-correction Barrett product can stay in [q, 2q)."""
+    _bind_walsh(emu)
+    rng = np.random.default_rng(q % 1000003)
+    vals = [int(rng.integers(0, 1 << 63)) << 65 | int(rng.integers(0, 1 << 63)) for _ in range(4000)]
+    top = ((1 << 128) - 1) // q
+    for _ in range(4000):
+        k = int(rng.integers(0, 1 << 62)) * (top >> 62) + int(rng.integers(0, 1 << 20))
+        k = min(k, top)
+        for d in (0, 1, 2, 7, q - 1, q - 3):
+            v = k * q + d
+            if v < (1 << 128):
+                vals.append(v)
+    vals += [(1 << 128) - 1, q * q - 1, q - 1, 0, q]
+    hi = np.array([v >> 64 for v in vals], dtype=np.uint64)
+    lo = np.array([v & ((1 << 64) - 1) for v in vals], dtype=np.uint64)
+    out = np.zeros(len(vals), dtype=np.uint64)
+    emu.emu_reduce128(q, hi, lo, len(vals), out)
+    assert [int(x) for x in out] == [v % q for v in vals]
+
+
+def _walsh_model(q, lb, la, hb, ha, pt, coefs, c0):
+    """The reference's sequence on exact integers: canonical low combinations (sums of added
+    multiples), imaginary half times the encoded i, tensor products, products summed by mask."""
+    def pair(s, hm, const):
+        r = sum(int(coefs[0, hm, lm]) * s[lm] for lm in range(1, 16))
+        im = sum(int(coefs[1, hm, lm]) * s[lm] for lm in range(1, 16))
+        if const:
+            r += int(c0[0, hm])
+            im += int(c0[1, hm])
+        return (r % q + (im % q) * pt) % q
+    out = [pair(lb, 0, True), pair(la, 0, False)]
+    rb = ra = rc = 0
+    for hm in range(1, 16):
+        x_b, x_a = pair(lb, hm, True), pair(la, hm, False)
+        rb = (rb + x_b * hb[hm]) % q
+        ra = (ra + x_a * hb[hm] + x_b * ha[hm]) % q
+        rc = (rc + x_a * ha[hm]) % q
+    return out + [rb, ra, rc]
+
+
+@pytest.mark.parametrize("q", WIDE_MODULI)
+def test_walsh_products_exact(emu, q):
+    """The fused Walsh product body equals the reference's step-by-step modular sequence,
+    with signs spread over [0, q) and bunched next to 0 and q, coefficients up to +-8."""
+    _bind_walsh(emu)
+    rng = np.random.default_rng(q % 999983)
+    n = 48
+    def draw(shape):
+        v = rng.integers(0, q, size=shape, dtype=np.uint64)
+        edge = rng.integers(0, 3, size=shape)
+        small = rng.integers(0, 1 << 12, size=shape, dtype=np.uint64)
+        v = np.where(edge == 1, small, v)
+        v = np.where(edge == 2, np.uint64(q - 1) - small, v)
+        return np.ascontiguousarray(v.astype(np.uint64))
+    lb, la, hb, ha = (draw((n, 16)) for _ in range(4))
+    pt = draw(n)
+    coefs = rng.integers(-8, 9, size=(2, 16, 16)).astype(np.int8)
+    coefs[:, :, 0] = 0
+    coefs[0, 3, :] = 8
+    coefs[1, 5, :] = -8
+    c0 = rng.integers(0, q, size=(2, 16), dtype=np.uint64)
+    out = np.zeros((n, 5), dtype=np.uint64)
+    emu.emu_walsh_products(q, n, lb, la, hb, ha, pt, np.ascontiguousarray(coefs), np.ascontiguousarray(c0), out)
+    for i in range(n):
+        want = _walsh_model(q, [int(x) for x in lb[i]], [int(x) for x in la[i]], [int(x) for x in hb[i]],
+                            [int(x) for x in ha[i]], int(pt[i]), coefs, c0)
+        assert [int(x) for x in out[i]] == want, i
