@@ -1,15 +1,31 @@
 #!/usr/bin/env python
-"""Benchmark: the walsh15 batched-ops workload on the device library.
+"""Benchmark: walsh15 homomorphic AES-128-CTR on the device library.
 
-One step = 64 ciphertexts of the AESWalsh15 parameter set (N = 2^15, Q chain 36|61|42,42|
-38 x7|50,50, P = 4 x 61, dnum = 3) at seeded levels uniform in 1..12, each multiplied by a
-partner ciphertext, relinearized, rescaled and rotated by a seeded index from the walsh15
-AES rotation-key set (+-512 k, k = 1..31), through wg_batch_mul_relin_rescale_rotate.
+One step = one AES-CTR evaluation at the walsh15 parameter set (N = 2^15, Q chain
+36|61|42,42|38 x7|50,50, P = 4 x 61, dnum = 3, EvalMod bootstrapping) over a slot-filling batch
+of 1024 counter blocks (complex packing: block s in the real part and block 512 + s in the
+imaginary part of slot s), through wg_aes_ctr_walsh: ten rounds of SubBytes (the 16 byte
+positions as one batch of mask-packed Walsh S-boxes with bootstrapping), ShiftRows, MixColumns
+and AddRoundKey on lazy bits, the final refresh and the XOR with the ciphertext blocks.  The
+encrypted round-key bits and the switching keys stay device-resident; the step's counter and
+ciphertext blocks come from host memory.  value = AES blocks per second over the K timed steps.
+
+Key, diagonal and key-bit residues are uniform draws with the shapes of the reference's walsh15
+context (tests/golden/walsh15_plan.json: stage shapes, rotation set, EvalMod series, key-bit
+levels and scales): the launch sequence depends only on those shapes, levels and scales.
+Bit-exactness and 0 decrypted mismatches on the reference's own keys are the parity tests'.
+
+Further sections of the same JSON line:
+  batched_ops   64 walsh15 ciphertexts at seeded levels, each ct x ct multiply + relinearize +
+                rescale + rotate: one CUDA-graph replay vs the plain per-operation GPU path
+  bsgs          CoeffToSlot / SlotToCoeff stages on 8 ciphertexts
+  cpu_baseline  the reference's SubBytes layer (16 S-box instances, OpenMP over instances as its
+                AES does) on this host's cores, extrapolated to AES-CTR blocks/s
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl walsh|reference]
 
-Prints one JSON line (rank 0).  Under torchrun every rank runs its own 64 ciphertexts
-(replicas, weak scaling); the elapsed time is the max over ranks.
+Prints one JSON line (rank 0).  Under torchrun every rank runs its own AES-CTR (replicas, weak
+scaling); the elapsed time is the max over ranks.
 """
 import argparse
 import json
@@ -24,41 +40,43 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "aes-walsh-ckks_b200")
 sys.path.insert(0, PKG)
+PLAN_PATH = os.path.join(ROOT, "tests", "golden", "walsh15_plan.json")
 
 METRIC = "walsh15 AES-CTR latency, blocks/s: batched vs plain GPU; NTT/KS % of HBM peak"
-UNIT = "ciphertexts/s"
+UNIT = "blocks/s"
 LOGN = 15
 Q_BITS = [36, 61, 42, 42] + [38] * 7 + [50, 50]
 P_BITS = [61] * 4
 DNUM = 3
-COUNT = 64
+ROUNDS = 10
+SBOX_INSTANCES = 16  # byte positions per SubBytes layer
+WORKLOAD = ("walsh15 AES-128-CTR: 1024 counter blocks per evaluation (2 x 512 complex-packed slots), "
+            "10 rounds with batched Walsh S-boxes and EvalMod bootstrapping, final refresh and XOR")
+OPS_COUNT = 64
 ROT_POOL = [512 * k for k in range(1, 32)] + [-512 * k for k in range(1, 32)]
-WORKLOAD = ("walsh15 batched ops: 64 ciphertexts at seeded levels 1..12, each ct x ct multiply + "
-            "relinearize + rescale + rotate by a seeded walsh15 AES rotation index")
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="walsh", choices=["walsh", "reference"])
-    ap.add_argument("--count", type=int, default=COUNT)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-plain", action="store_true", help="skip the op-by-op comparison pass")
-    ap.add_argument("--no-probe", action="store_true", help="skip the per-kernel event-timing passes")
-    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass")
+    ap.add_argument("--no-probe", action="store_true", help="skip the per-kernel-class event-timing passes")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass")
+    ap.add_argument("--no-ops", action="store_true", help="skip the batched-ops section")
     ap.add_argument("--no-bsgs", action="store_true", help="skip the CoeffToSlot / SlotToCoeff section")
-    ap.add_argument("--e2e-chunk", type=int, default=16, help="ciphertexts per overlapped chunk (e2e)")
+    ap.add_argument("--ops-steps", type=int, default=50)
+    ap.add_argument("--ops-count", type=int, default=OPS_COUNT)
+    ap.add_argument("--e2e-chunk", type=int, default=16, help="ciphertexts per overlapped chunk (ops e2e)")
     return ap.parse_args()
 
 
-def workload(seed, count):
-    rng = np.random.default_rng(seed)
-    levels = rng.integers(1, len(Q_BITS), count)
-    rots = [int(r) for r in rng.choice(ROT_POOL, count)]
-    return levels, rots
+def load_plan():
+    with open(PLAN_PATH) as f:
+        return json.load(f)
 
 
 # ------------------------------------------------------------------------------------------
@@ -116,76 +134,64 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------
-# CPU arms (reference compiled from its own sources, else the oracle port)
+# CPU: the reference's SubBytes layer (compiled from its own sources)
 # ------------------------------------------------------------------------------------------
-def cpu_run(levels, rots, seconds_budget, threads=None):
-    """Time the reference CPU path on a bounded sample of the workload.  Returns a dict."""
+def _ref_sbox_setup():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    threads = threads or os.cpu_count()
-    N = 1 << LOGN
-    sample = 8 if seconds_budget < 60 else 16
-    lv, rt = np.asarray(levels[:sample]), list(rots[:sample])
-    L = len(Q_BITS)
-    stride = L * N
-    if O.ref_available():
-        kind = "reference"
-        R = O.RefCtx(N, Q_BITS, P_BITS, DNUM, h=256, rotations=sorted(set(rt)))
-        q = R.q
-    else:
-        kind = "port"
-        p, q = O.find_primes(P_BITS, Q_BITS, N)
-        o = O.OracleCtx(N, q, p, DNUM)
-        rng = np.random.default_rng(5)
-        ks = o.key_size()
-        keys = {r: np.concatenate([rng.integers(0, int(q[0]), ks, dtype=np.uint64)]) for r in set(rt)}
-        relin = rng.integers(0, int(q[0]), ks, dtype=np.uint64)
-    rng = np.random.default_rng(7)
-    mk = lambda: np.concatenate([rng.integers(0, int(q[i % L]), N, dtype=np.uint64) for i in range(sample * L)])
-    yb, ya = mk(), mk()
-    xb0, xa0 = mk(), mk()
-    done, elapsed = 0, 0.0
-    while elapsed < seconds_budget or done == 0:
-        xb, xa = xb0.copy(), xa0.copy()
-        t0 = time.perf_counter()
-        if kind == "reference":
-            import ctypes as C
+    if not O.ref_available():
+        raise RuntimeError("the reference library (oracle/_ref) is not built")
+    R = O.RefPlans(bootstrap_keys=True)
+    info = R.bts_info()
+    level = info["s2c_depth"]
+    N = R.N
+    rng = np.random.default_rng(17)
+    qc = np.repeat(R.q[: level + 1], N)
+    draw = lambda: (rng.integers(0, 1 << 62, (level + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
+    bits = [(draw(), draw()) for _ in range(8)]
+    return R, info, bits
 
-            sec = C.c_double()
-            rc = O.ref().ref_batched_ops(R.h, sample, np.ascontiguousarray(lv, dtype=np.uintp), xb, xa, yb, ya,
-                                         np.ascontiguousarray(rt, dtype=np.int64), stride, threads, C.byref(sec))
-            if rc != 0:
-                raise RuntimeError(O.ref().ref_last_error().decode())
-        else:
-            o.batched_ops(lv, xb, xa, yb, ya, relin, [keys[r] for r in rt], rt, stride, threads)
-        elapsed += time.perf_counter() - t0
-        done += sample
-        if elapsed > 4 * seconds_budget:
-            break
-    return {"value": done / elapsed, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{done} ciphertexts ({sample} per pass, the first {sample} of the seeded 64) in "
-                      f"{elapsed:.1f} s with {threads} threads"}
+
+def _layer_line(seconds, threads, layers):
+    blocks = 2 * 512
+    return {"value": blocks / (ROUNDS * seconds), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{layers} SubBytes layer(s) of {SBOX_INSTANCES} mask-packed Walsh S-box instances (the "
+                      f"reference's ckks_walsh_sbox_complex_blocks_mask_packed, OpenMP over instances as its AES "
+                      f"SubBytes runs them) on {threads} threads, {seconds:.2f} s per layer; AES-CTR time taken "
+                      f"as {ROUNDS} layers for {blocks} blocks (its linear layers and final refresh not counted, "
+                      f"which favours the reference)"}
+
+
+def cpu_baseline():
+    R, info, bits = _ref_sbox_setup()
+    threads = os.cpu_count()
+    sec = R.walsh_sbox_layer_seconds(512, info["s2c_depth"], info["scale"], bits, SBOX_INSTANCES, threads)
+    return _layer_line(sec, threads, 1)
 
 
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    levels, rots = workload(args.seed, args.count)
-    for _ in range(args.warmup):
-        cpu_run(levels, rots, 0.0)
-    t0 = time.perf_counter()
-    vals = [cpu_run(levels, rots, 0.0) for _ in range(args.steps)]
-    total = time.perf_counter() - t0
-    v = float(np.mean([x["value"] for x in vals]))
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / max(1, args.steps),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sampled": vals[0]["sample"]},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"], "kind": vals[0]["kind"],
-                             "sample": vals[0]["sample"]},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    R, info, bits = _ref_sbox_setup()
+    threads = os.cpu_count()
+    level, scale = info["s2c_depth"], info["scale"]
+    for _ in range(args.warmup):  # one instance each: pages in keys, plans and code
+        R.walsh_sbox_layer_seconds(512, level, scale, bits, 1, threads)
+    samples, t0 = [], time.perf_counter()
+    for i in range(args.steps):
+        samples.append(R.walsh_sbox_layer_seconds(512, level, scale, bits, SBOX_INSTANCES, threads))
+        if time.perf_counter() - t0 > 200.0:  # keep the arm within a few minutes
+            break
+    sec = float(np.mean(samples))
+    base = _layer_line(sec, threads, len(samples))
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sampled": base["sample"], "timed_layers": len(samples)},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -280,35 +286,18 @@ def bsgs_bench(wg, ctx, q, p, stream, timed, steps, warmup):
 
 
 # ------------------------------------------------------------------------------------------
-# device arm
+# batched ops: mul + relin + rescale + rotate on 64 ciphertexts, batched vs plain
 # ------------------------------------------------------------------------------------------
-def main():
-    args = parse()
-    if args.impl == "reference":
-        reference_arm(args)
-        return
-    import torch
-    import walshgpu as wg
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
+def ops_bench(args, wg, torch, stream, timed, rank, local):
     N = 1 << LOGN
     L = len(Q_BITS)
     p, q = wg.find_primes(P_BITS, Q_BITS, N)
     ctx = wg.Context(N, q, p, DNUM, device=local)
-    levels, rots = workload(args.seed + rank, args.count)
-    # Switching keys: uniform residues of the key shape.  The work is independent of key
-    # values; bit-exactness with real keys is covered by the parity tests.
+    rng = np.random.default_rng(args.seed + rank)
+    count = args.ops_count
+    levels = rng.integers(1, L, count)
+    rots = [int(r) for r in rng.choice(ROT_POOL, count)]
+    # switching keys: uniform residues of the key shape (the work does not depend on them)
     krng = np.random.default_rng(99)
     parts = ctx.parts(L - 1)
     mods = np.concatenate([q, p]).astype(np.uint64)
@@ -320,128 +309,50 @@ def main():
     ctx.set_key(wg.WG_KEY_RELIN, random_key())
     for r in sorted(set(rots)):
         ctx.set_key(wg.WG_KEY_ROTATION, random_key(), rotation=r)
-    stream = torch.cuda.current_stream()
     ctx.reserve(stream)
-
-    count = args.count
-    stride = L * N  # words per polynomial slot
+    stride = L * N
     qcol = np.repeat(q, N)
     drng = np.random.default_rng(1000 + rank)
-
-    def uniform_ct():
-        return (drng.integers(0, 1 << 62, L * N, dtype=np.uint64) % qcol).astype(np.uint64)
-
+    uniform_ct = lambda: (drng.integers(0, 1 << 62, L * N, dtype=np.uint64) % qcol).astype(np.uint64)
     host_x = np.stack([np.stack([uniform_ct(), uniform_ct()]) for _ in range(count)])  # [ct][b,a][L*N]
     host_y = np.stack([np.stack([uniform_ct(), uniform_ct()]) for _ in range(count)])
-    pristine = torch.from_numpy(host_x.view(np.int64)).cuda()
-    work = torch.empty_like(pristine)
+    work = torch.from_numpy(host_x.view(np.int64)).cuda()
     dy = torch.from_numpy(host_y.view(np.int64)).cuda()
     xb = [work[i, 0] for i in range(count)]
     xa = [work[i, 1] for i in range(count)]
     yb = [dy[i, 0] for i in range(count)]
     ya = [dy[i, 1] for i in range(count)]
-
-    work.copy_(pristine)
     plan = wg.BatchPlan(ctx, levels, xb, xa, yb, ya, rots)
-
-    def step():
-        # one graph replay of the whole batched pipeline; every step runs on the previous
-        # step's outputs (same levels and shapes: the work does not depend on residue values)
-        plan.launch(stream)
-
-    def step_nograph():
-        ctx.batch_mul_relin_rescale_rotate(levels, xb, xa, yb, ya, rots, stream=stream)
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-
-    def timed(fn, k):
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(k):
-            fn()
-        e1.record(stream)
-        barrier()
-        ms = e0.elapsed_time(e1) / k
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
-
+    steps = max(1, args.ops_steps)
+    # one graph replay of the whole batched pipeline per step, on the previous step's outputs
+    graph_step = lambda: plan.launch(stream)
+    nograph_step = lambda: ctx.batch_mul_relin_rescale_rotate(levels, xb, xa, yb, ya, rots, stream=stream)
+    plain_step = lambda: ctx.batch_mul_relin_rescale_rotate(levels, xb, xa, yb, ya, rots, stream=stream, plain=True)
     for _ in range(args.warmup):
-        step()
-    launches0 = wg.launch_count()
-    with ClockSampler(local) as clk:
-        ms = timed(step, args.steps)
-    launches = wg.launch_count() - launches0
-
+        graph_step()
+    l0 = wg.launch_count()
+    graph_ms = timed(graph_step, steps)
+    graph_launches = (wg.launch_count() - l0) / steps
     for _ in range(args.warmup):
-        step_nograph()
-    nograph_ms = timed(step_nograph, args.steps)
-
-    # per-kernel-class device time over the same K steps (CUDA events on the launch stream,
-    # so the un-captured batched call is used)
-    kernels = {}
-    for name, cls in ([] if args.no_probe else wg.KCLASS.items()):
-        wg.probe_begin(cls, 60000)
-        timed(step_nograph, args.steps)
-        n, kms, kbytes = wg.probe_end()
-        kernels[name] = {"launches": n, "ms": kms, "bytes": kbytes}
-    probed_total = sum(v["ms"] for v in kernels.values())
-    for v in kernels.values():
-        v["share"] = v["ms"] / probed_total if probed_total else None
-        v["gbs"] = v["bytes"] / (v["ms"] * 1e6) if v["ms"] else None
-    dom_name = max(kernels, key=lambda k: kernels[k]["ms"]) if kernels else "ntt"
-    dom = kernels.get(dom_name, {"ms": 0.0, "launches": 0, "bytes": 0.0, "gbs": None})
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
-    # DRAM traffic of the dominant kernel from the committed ncu capture summary (ratio of
-    # dram__bytes to algorithmic bytes, scaled to this launch size)
-    traffic = None
-    try:
-        tr = json.load(open(os.path.join(ROOT, "profiles", "ntt_phase_traffic.json")))
-        if dom_name == "ntt" and dom["launches"]:
-            traffic = tr["dram_traffic_over_algorithmic"] * dom["bytes"] / dom["launches"]
-    except (OSError, ValueError, KeyError):
-        pass
-    roofline = {"kernel": dom_name, "bound": "hbm", "achieved": dom["gbs"], "peak": hbm, "unit": "GB/s",
-                "frac": dom["gbs"] / hbm if dom["gbs"] else None, "traffic": traffic,
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "avg_launch_us": 1000 * dom["ms"] / max(1, dom["launches"]),
-                "bytes_per_launch": dom["bytes"] / max(1, dom["launches"])}
-
-    # the same workload op by op (the plain per-operation GPU path)
-    def plain_step():
-        ctx.batch_mul_relin_rescale_rotate(levels, xb, xa, yb, ya, rots, stream=stream, plain=True)
-
-    plain_ms, plain_launches = None, None
-    if not args.no_plain:
-        plain_step()
-        plain_launches0 = wg.launch_count()
-        plain_ms = timed(plain_step, max(1, args.steps // 2))
-        plain_launches = (wg.launch_count() - plain_launches0) / max(1, args.steps // 2)
-
-    # End to end through the C ABI with host buffers: H2D of each ciphertext's active limbs
-    # (x and y), the batched pipeline, D2H of the rescaled and rotated results.  The batch is
-    # cut into chunks, each with its own graph plan; chunk k's compute overlaps chunk k+1's
-    # upload and chunk k-1's download (copy-in, compute and copy-out streams).
-    pin_x = torch.from_numpy(host_x.view(np.int64)).pin_memory()
-    pin_y = torch.from_numpy(host_y.view(np.int64)).pin_memory()
-    pin_out = torch.empty((count, 2, stride), dtype=torch.int64).pin_memory()
-    h2d = int(sum(4 * (int(lv) + 1) * N * 8 for lv in levels))
-    d2h = int(sum(2 * int(lv) * N * 8 for lv in levels))
-    chunk = max(1, min(args.e2e_chunk, count))
-    bounds = [(i, min(count, i + chunk)) for i in range(0, count, chunk)]
-    e2e_ms = None
+        nograph_step()
+    nograph_ms = timed(nograph_step, steps)
+    plain_step()
+    l0 = wg.launch_count()
+    plain_ms = timed(plain_step, max(1, steps // 2))
+    plain_launches = (wg.launch_count() - l0) / max(1, steps // 2)
+    # NTT class over the batched call (CUDA events on the launch stream)
+    wg.probe_begin(wg.KCLASS["ntt"], 60000)
+    timed(nograph_step, 1)
+    n, kms, kbytes = wg.probe_end()
+    # end to end with host buffers: H2D of each ciphertext's active limbs, the pipeline in
+    # chunks (compute of chunk k overlaps the upload of k+1 and the download of k-1), D2H
+    e2e = None
     if not args.no_e2e:
+        pin_x = torch.from_numpy(host_x.view(np.int64)).pin_memory()
+        pin_y = torch.from_numpy(host_y.view(np.int64)).pin_memory()
+        pin_out = torch.empty((count, 2, stride), dtype=torch.int64).pin_memory()
+        chunk = max(1, min(args.e2e_chunk, count))
+        bounds = [(i, min(count, i + chunk)) for i in range(0, count, chunk)]
         cplans = [wg.BatchPlan(ctx, levels[a:b], xb[a:b], xa[a:b], yb[a:b], ya[a:b], rots[a:b]) for a, b in bounds]
         s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
         ev = lambda: torch.cuda.Event()
@@ -476,22 +387,255 @@ def main():
 
         for _ in range(args.warmup):
             e2e_step()
-        e2e_ms = timed(e2e_step, args.steps)
-        # the last chunk's results are back in pinned host memory and match the device copy
+        e2e_ms = timed(e2e_step, steps)
         torch.cuda.synchronize()
         i = count - 1
         nb = int(levels[i]) * N
         assert torch.equal(pin_out[i, 0, :nb], work[i, 0, :nb].cpu())
         for cp in cplans:
             cp.close()
+        e2e = {"value": count / (e2e_ms / 1000.0), "unit": "ciphertexts/s", "ms_per_step": e2e_ms,
+               "h2d_bytes_per_step": int(sum(4 * (int(lv) + 1) * N * 8 for lv in levels)),
+               "d2h_bytes_per_step": int(sum(2 * int(lv) * N * 8 for lv in levels)), "chunk": chunk}
+    plan.close()
+    res = {
+        "workload": f"{count} walsh15 ciphertexts at seeded levels 1..12, each ct x ct multiply + relinearize + "
+                    f"rescale + rotate by a seeded walsh15 AES rotation index",
+        "unit": "ciphertexts/s",
+        "batched_graph": {"value": count / (graph_ms / 1000.0), "ms_per_step": graph_ms,
+                          "launches_per_step": graph_launches},
+        "batched_nograph": {"value": count / (nograph_ms / 1000.0), "ms_per_step": nograph_ms},
+        "plain_per_op": {"value": count / (plain_ms / 1000.0), "ms_per_step": plain_ms,
+                         "launches_per_step": plain_launches},
+        "batched_over_plain": plain_ms / graph_ms,
+        "ntt": {"launches": n, "ms": kms, "gbs": kbytes / (kms * 1e6) if kms else None},
+        "e2e": e2e, "steps": steps,
+    }
+    return res, ctx, q, p
 
-    bsgs = None if args.no_bsgs else bsgs_bench(wg, ctx, q, p, stream, timed, max(1, args.steps // 2),
-                                                args.warmup)
+
+# ------------------------------------------------------------------------------------------
+# AES-CTR on the device
+# ------------------------------------------------------------------------------------------
+class AesRun:
+    """Context, keys, bootstrap stages and encrypted key bits of the walsh15 shapes."""
+
+    def __init__(self, wg, torch, plan, device, seed):
+        N = plan["ring_degree"]
+        q = np.array(plan["q"], dtype=np.uint64)
+        p = np.array(plan["p"], dtype=np.uint64)
+        K = len(p)
+        self.N, self.wg, self.torch = N, wg, torch
+        self.ctx = ctx = wg.Context(N, q, p, plan["dnum"], device=device)
+        rng = np.random.default_rng(seed)
+
+        def residues(limb_mods, copies):
+            col = np.tile(np.repeat(np.asarray(limb_mods, np.uint64), N), copies)
+            return (rng.integers(0, 1 << 62, col.size, dtype=np.uint64) % col).astype(np.uint64)
+
+        def key(spec):
+            kl = spec["key_level"]
+            flat = residues(np.concatenate([q[: kl + 1], p]), 2 * spec["parts"])
+            assert flat.size == spec["words"], (flat.size, spec)
+            return flat
+
+        keys = plan["keys"]
+        for name, kind in (("relin", wg.WG_KEY_RELIN), ("conj", wg.WG_KEY_CONJ),
+                           ("sparse_to_dense", wg.WG_KEY_SPARSE_TO_DENSE)):
+            ctx.set_key(kind, key(keys[name]), parts=keys[name]["parts"], key_level=keys[name]["key_level"])
+        ctx.set_key(wg.WG_KEY_DENSE_TO_SPARSE, residues([q[0], p[0], q[0], p[0]], 1))
+        rk = keys["rotation"]
+        for r in plan["rotations"]:
+            ctx.set_key(wg.WG_KEY_ROTATION, key(rk), rotation=int(r), parts=rk["parts"], key_level=rk["key_level"])
+
+        def stages(spec):
+            out = []
+            for st in spec:
+                level = st["qp_limbs"] - 1 - K
+                d = residues(np.concatenate([q[: level + 1], p]), len(st["indices"]))
+                out.append(wg.LtStage(ctx, level, st["indices"], d, st["baby"], st["slot_count"], st["rescale"]))
+            return out
+
+        self.s2c, self.s2c_x2, self.c2s = stages(plan["s2c"]), stages(plan["s2c_x2"]), stages(plan["c2s"])
+        b = plan["bootstrap"]
+        self.params = wg.BootstrapParams(b["s2c_depth"], b["depth"], b["evalmod_log_scale"], b["double_angle"],
+                                         b["active_slots"], b["slots"], b["scale"])
+        self.coeffs = np.asarray(plan["evalmod_coeffs"], dtype=np.float64)
+        a = plan["aes"]
+        self.kl, self.kscales = a["key_level"], np.asarray(a["key_scales"], dtype=np.float64)
+        self.pbc, self.psc, self.acb = a["packing_block_count"], a["packed_segment_count"], a["active_blocks"]
+        n = (self.kl + 1) * N
+        qcol = torch.from_numpy(np.repeat(q[: self.kl + 1], N).view(np.int64)).cuda()
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed)
+        self.key_dev = torch.randint(0, 1 << 62, (len(self.kscales), 2, n), dtype=torch.int64, device="cuda",
+                                     generator=gen) % qcol
+        self.key_bits = [(self.key_dev[k, 0], self.key_dev[k, 1]) for k in range(len(self.kscales))]
+        full = (b["depth"] + 1) * N
+        self.out_dev = torch.zeros((128, 2, full), dtype=torch.int64, device="cuda")
+        self.outs = [(self.out_dev[k, 0], self.out_dev[k, 1]) for k in range(128)]
+        self.blocks = 2 * self.acb
+        self.block_bytes = [bytes(rng.integers(0, 256, 16 * self.blocks, dtype=np.uint8)) for _ in range(4)]
+        self.calls = 0
+
+    def step(self, stream):
+        c = self.block_bytes[self.calls % 4]
+        x = self.block_bytes[(self.calls + 1) % 4]
+        self.calls += 1
+        return self.ctx.aes_ctr_walsh(self.params, self.s2c, self.s2c_x2, self.c2s, self.coeffs, self.pbc, self.psc,
+                                      self.key_bits, self.kscales, self.kl, c, x, self.acb, self.outs, stream=stream)
+
+
+# ------------------------------------------------------------------------------------------
+# device arm
+# ------------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    import walshgpu as wg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(ms):
+        if dist is None:
+            return ms
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, k):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / k)
+
+    plan = load_plan()
+    aes = AesRun(wg, torch, plan, local, args.seed + rank)
+    N = aes.N
+    aes_step = lambda: aes.step(stream)
+    for _ in range(args.warmup):
+        aes_step()
+    # timed region: K evaluations, an event after each for the latency distribution
+    barrier()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    launches0 = wg.launch_count()
+    host0 = wg.host_stats()
+    with ClockSampler(local) as clk:
+        evs[0].record(stream)
+        out_levels = None
+        for i in range(args.steps):
+            out_levels, _ = aes_step()
+            evs[i + 1].record(stream)
+        barrier()
+    launches = wg.launch_count() - launches0
+    host1 = wg.host_stats()
+    per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    ms = max_over_ranks(evs[0].elapsed_time(evs[-1]) / args.steps)
+    value = aes.blocks * world / (ms / 1000.0)
+    staged = (host1["stage_bytes"] - host0["stage_bytes"]) / args.steps
+
+    # end to end: the same call from host block bytes, plus the read-back of the 128 output
+    # bit ciphertexts into pinned host memory, every step
+    e2e = None
+    if not args.no_e2e:
+        full = aes.out_dev.shape[2]
+        pinned = torch.empty((128, 2, full), dtype=torch.int64).pin_memory()
+        d2h = [0]
+
+        def e2e_step():
+            lv, _ = aes_step()
+            d2h[0] = 0
+            for k in range(128):
+                nb = (lv[k] + 1) * N * 8
+                for j in range(2):
+                    wg.memcpy_dtoh(pinned[k, j].data_ptr(), aes.out_dev[k, j], nb, stream=stream)
+                d2h[0] += 2 * nb
+
+        e2e_step()
+        e2e_ms = timed(e2e_step, max(1, args.steps // 2))
+        torch.cuda.synchronize()
+        assert torch.equal(pinned[0, 0, :N], aes.out_dev[0, 0, :N].cpu())
+        e2e = {"value": aes.blocks * world / (e2e_ms / 1000.0), "unit": UNIT, "ms_per_step": e2e_ms,
+               "h2d_bytes_per_step": int(2 * 16 * aes.blocks + staged), "d2h_bytes_per_step": int(d2h[0]),
+               "h2d_detail": "counter and ciphertext blocks from host memory plus the slot encodings of their "
+                             "bits staged by the library",
+               "steps": max(1, args.steps // 2)}
+
+    # per-kernel-class device time of one evaluation (CUDA events on the launch stream)
+    kernels = {}
+    for name, cls in ([] if args.no_probe else wg.KCLASS.items()):
+        wg.probe_begin(cls, 65536)
+        aes_step()
+        torch.cuda.synchronize()
+        n, kms, kbytes = wg.probe_end()
+        kernels[name] = {"launches": n, "ms": kms, "bytes": kbytes}
+    probed = sum(v["ms"] for v in kernels.values())
+    for v in kernels.values():
+        v["share"] = v["ms"] / probed if probed else None
+        v["gbs"] = v["bytes"] / (v["ms"] * 1e6) if v["ms"] else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    dom_name = max(kernels, key=lambda k: kernels[k]["ms"]) if kernels else "ntt"
+    dom = kernels.get(dom_name, {"ms": 0.0, "launches": 0, "bytes": 0.0, "gbs": None})
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "ntt_phase_traffic.json")))
+        if dom_name == "ntt" and dom["launches"]:
+            traffic = tr["dram_traffic_over_algorithmic"] * dom["bytes"] / dom["launches"]
+    except (OSError, ValueError, KeyError):
+        pass
+    ks = [kernels[k] for k in ("modup", "keymac", "moddown") if k in kernels]
+    ks_ms, ks_bytes = sum(v["ms"] for v in ks), sum(v["bytes"] for v in ks)
+    roofline = {"kernel": dom_name, "bound": "hbm", "achieved": dom["gbs"], "peak": hbm, "unit": "GB/s",
+                "frac": dom["gbs"] / hbm if dom["gbs"] else None, "traffic": traffic,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "avg_launch_us": 1000 * dom["ms"] / max(1, dom["launches"]),
+                "bytes_per_launch": dom["bytes"] / max(1, dom["launches"]),
+                "keyswitch": {"achieved": ks_bytes / (ks_ms * 1e6) if ks_ms else None,
+                              "frac": ks_bytes / (ks_ms * 1e6) / hbm if ks_ms else None,
+                              "classes": "modup + key inner product + moddown"}}
+
+    ops, ops_ctx = None, None
+    if not args.no_ops:
+        ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local)
+    bsgs = None
+    if not args.no_bsgs:
+        if ops_ctx is None:
+            p, q = wg.find_primes(P_BITS, Q_BITS, N)
+            ops_ctx = wg.Context(N, q, p, DNUM, device=local)
+        bsgs = bsgs_bench(wg, ops_ctx, q, p, stream, timed, 10, args.warmup)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_run(levels, rots, 15.0)
+            cpu = cpu_baseline()
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable", "sample": str(e)}
 
@@ -500,27 +644,28 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
-    value = count * world / (ms / 1000.0)
+    per_sorted = sorted(per_step)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "ring_degree": N, "q_limbs": L, "p_limbs": len(P_BITS), "dnum": DNUM,
-                   "ciphertexts_per_gpu": count, "levels": [int(x) for x in levels],
-                   "rotation_keys": len(set(rots)), "keys": "uniform residues of the walsh15 key shape",
+        "config": {"workload": WORKLOAD, "ring_degree": N, "q_limbs": len(plan["q"]), "p_limbs": len(plan["p"]),
+                   "dnum": plan["dnum"], "blocks_per_step": aes.blocks, "rounds": ROUNDS,
+                   "keys": "uniform residues of the walsh15 key shapes (65 rotation keys, relin, conj, sparse/dense)",
+                   "shapes": "tests/golden/walsh15_plan.json (the reference's walsh15 bootstrapping plan)",
                    "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2: ~0.9 GB of ciphertexts plus ~1.1 GB of keys per step",
-                   "step": "one CUDA-graph replay of the batched pipeline on the previous step's outputs",
-                   "e2e_chunk": chunk},
+                   "l2": "inputs larger than L2: 2.2 GB of encrypted key bits and 1.7 GB of rotation keys per step",
+                   "step": "one wg_aes_ctr_walsh call on device-resident keys with host counter blocks"},
+        "latency_ms": {"mean": float(np.mean(per_step)), "p50": per_sorted[len(per_sorted) // 2],
+                       "p99": per_sorted[min(len(per_sorted) - 1, int(0.99 * len(per_sorted)))],
+                       "min": per_sorted[0], "max": per_sorted[-1]},
         "clocks": clk.summary(),
-        "e2e": {"value": count * world / (e2e_ms / 1000.0) if e2e_ms else None, "unit": UNIT,
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "e2e": e2e,
         "gpu_launches": int(launches),
-        "batched_nograph": {"value": count * world / (nograph_ms / 1000.0), "unit": UNIT, "ms_per_step": nograph_ms},
-        "plain_per_op": {"value": count * world / (plain_ms / 1000.0) if plain_ms else None, "unit": UNIT,
-                         "ms_per_step": plain_ms, "launches_per_step": plain_launches},
+        "output_levels": sorted(set(int(x) for x in out_levels)) if out_levels else None,
         "roofline": roofline,
         "kernels": kernels,
+        "batched_ops": ops,
         "bsgs": bsgs,
         "cpu_baseline": cpu,
     }

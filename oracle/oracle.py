@@ -436,6 +436,8 @@ class RefPlans:
         R.ref_decrypt.argtypes = [C.c_void_p, C.c_size_t, C.c_double, u64p, u64p, f64p, f64p]
         R.ref_encode.argtypes = [C.c_void_p, f64p, f64p, C.c_double, C.c_size_t, u64p]
         R.ref_walsh_sbox.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_double, u64p, u64p, szp, f64p]
+        R.ref_walsh_sbox_layer.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_double, u64p, C.c_size_t, C.c_int,
+                                           C.POINTER(C.c_double)]
         R.ref_bts_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_size_t)] * 6 + [C.POINTER(C.c_double),
                                                                                C.POINTER(C.c_size_t)]
         R.ref_bts_evalmod_coeffs.argtypes = [C.c_void_p, f64p]
@@ -607,6 +609,17 @@ class RefPlans:
         _check(ref().ref_encode(self.h, np.ascontiguousarray(re, np.float64), np.ascontiguousarray(im, np.float64),
                                 float(scale), level, out), "ref_encode")
         return out
+
+    def walsh_sbox_layer_seconds(self, block_count, level, scale, bits, instances, threads=0):
+        """Wall time of `instances` reference S-box calls on the 8 bit ciphertexts `bits`, run as
+        the reference's SubBytes runs its byte positions (OpenMP over instances)."""
+        n = (level + 1) * self.N
+        flat = np.concatenate([np.concatenate([np.asarray(b[:n], np.uint64), np.asarray(a[:n], np.uint64)])
+                               for b, a in bits])
+        sec = C.c_double()
+        _check(ref().ref_walsh_sbox_layer(self.h, block_count, level, float(scale), flat, instances, threads,
+                                          C.byref(sec)), "ref_walsh_sbox_layer")
+        return sec.value
 
     def walsh_sbox(self, block_count, level, scale, bits):
         """The reference's mask-packed Walsh S-box on 8 bit ciphertexts [(b, a)] x 8:

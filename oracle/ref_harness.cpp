@@ -618,6 +618,42 @@ int ref_walsh_sbox(void* h, size_t block_count, size_t level, double scale, cons
     });
 }
 
+// Timing sample of the reference's SubBytes layer: `instances` independent mask-packed Walsh
+// S-box calls on the same 8 input bits, run as sub_bytes_walsh_complex_blocks_mask_packed runs
+// its 16 byte positions (src/ckks/operations/circuits/aes/ckks_aes_ctr_walsh_sbox.cpp:659-706:
+// one OpenMP dynamic-schedule loop over bytes, one scratch per byte) on `threads` threads.
+// Returns the wall time of the loop in *seconds; outputs are discarded.
+int ref_walsh_sbox_layer(void* h, size_t block_count, size_t level, double scale, const uint64_t* in,
+                         size_t instances, int threads, double* seconds) {
+    return guarded([&] {
+        auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        std::vector<MyVector<CKKSCiphertext>> inputs(instances);
+        for (auto& bits : inputs)
+            for (size_t k = 0; k < 8; ++k)
+                bits.emplace_back(N, copy_in(in + (2 * k + 1) * n, n), copy_in(in + 2 * k * n, n),
+                                  (long double)scale, level);
+        std::vector<CKKSWalshSboxScratch> scratch(instances);
+        std::exception_ptr first;
+        if (threads > 0) omp_set_num_threads(threads);
+        const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic)
+        for (std::ptrdiff_t i = 0; i < (std::ptrdiff_t)instances; ++i) {
+            try {
+                auto res = ckks_walsh_sbox_complex_blocks_mask_packed(c, std::move(inputs[(size_t)i]), block_count,
+                                                                      scratch[(size_t)i]);
+                if (res.size() != 8) throw std::runtime_error("ref_walsh_sbox_layer: expected 8 output bits");
+            } catch (...) {
+#pragma omp critical
+                if (!first) first = std::current_exception();
+            }
+        }
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (first) std::rethrow_exception(first);
+    });
+}
+
 // ckks_encode (coefficient form, eval = false) of N/2 slot values re[i] + i im[i].
 int ref_encode(void* h, const double* re, const double* im, double scale, size_t level, uint64_t* out) {
     return guarded([&] {

@@ -64,3 +64,25 @@ def test_context_without_gpu_fails_cleanly(libwg):
     p, q = libwg.find_primes([55, 55], [50] * 3, 1024)
     with pytest.raises(libwg.WalshGpuError):
         libwg.Context(1024, q, p, 3)
+
+
+def test_walsh15_plan_fixture_consistent(oracle_mod):
+    """The bootstrap-structure fixture the benchmark builds its AES run from agrees with the
+    library's prime generator and with the walsh15 shapes (limbs, slots, key sizes)."""
+    import json
+
+    plan = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "walsh15_plan.json")))
+    N = plan["ring_degree"]
+    p, q = oracle_mod.find_primes([61] * 4, [36, 61, 42, 42] + [38] * 7 + [50, 50], N)
+    assert [int(x) for x in q] == plan["q"] and [int(x) for x in p] == plan["p"]
+    K = len(plan["p"])
+    for name in ("s2c", "s2c_x2", "c2s"):
+        for st in plan[name]:
+            assert 0 <= st["qp_limbs"] - 1 - K < len(plan["q"])
+            assert all(0 <= i < N // 2 for i in st["indices"])
+    for name, spec in plan["keys"].items():
+        if name == "dense_to_sparse":
+            assert spec["words"] == 4 * N
+        else:
+            assert spec["words"] == spec["parts"] * 2 * (spec["key_level"] + 1 + K) * N
+    assert len(plan["aes"]["key_scales"]) == 11 * 128
