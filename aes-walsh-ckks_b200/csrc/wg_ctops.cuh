@@ -45,6 +45,29 @@ __global__ void __launch_bounds__(kT) kb_scalar(const ScalarJob* jobs, int n, co
         j->x[k] = add_mod(j->x[k], j->s, q);
 }
 
+constexpr int kMaxLincombTerms = 16;
+
+struct LincombJob {
+    uint64_t* out;
+    const uint64_t* src[kMaxLincombTerms];
+    uint64_t c[kMaxLincombTerms], cs[kMaxLincombTerms];
+    uint64_t add;
+    int n, mod, accumulate, pad;
+};
+
+// out = (accumulate ? out : 0) + add + sum_t c_t src_t (mod q).  Shoup products and modular
+// additions of canonical residues: the value is the canonical residue of the sum, whatever the
+// order of the terms, equal to adding the scaled terms one multiply-add at a time.
+__global__ void __launch_bounds__(kT) kb_lincomb(const LincombJob* jobs, int n, const Modulus* mods) {
+    const LincombJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const uint64_t q = mods[j->mod].q;
+    uint64_t acc = add_mod(j->accumulate ? j->out[k] : 0, j->add, q);
+    for (int t = 0; t < j->n; ++t) acc = add_mod(acc, mul_shoup(j->src[t][k], j->c[t], j->cs[t], q), q);
+    j->out[k] = acc;
+}
+
 struct PmulJob {
     uint64_t* x;
     const uint64_t* p;
@@ -290,6 +313,54 @@ public:
         Probe probe(kClsElementwise, 8.0 * N * jobs.size() * (op == kScalarMulAdd ? 3.0 : 2.0), s_);
         kb_scalar<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
         check_cuda(cudaGetLastError(), "evalpoly scalar");
+    }
+
+    // One term of a linear combination: a batch and one constant per limb (canonical).
+    struct LinTerm {
+        CtBatch x;
+        std::vector<uint64_t> c;
+    };
+
+    // A fresh batch (level, np) = cadd (on the b polynomial) + sum of c_t x_t per limb; a term
+    // with fewer polynomials than np contributes zeros to the others.  Up to kMaxLincombTerms
+    // terms per launch.
+    CtBatch lincomb(size_t level, int np, long double scale, const std::vector<uint64_t>& cadd,
+                    const std::vector<LinTerm>& terms) {
+        const size_t N = c_.N;
+        CtBatch out = alloc(level, np);
+        out.scale = scale;
+        const size_t chunks = std::max<size_t>(1, (terms.size() + kMaxLincombTerms - 1) / kMaxLincombTerms);
+        for (size_t ch = 0; ch < chunks; ++ch) {
+            std::vector<LincombJob> jobs;
+            for (size_t i = 0; i < count_; ++i)
+                for (int poly = 0; poly < np; ++poly)
+                    for (size_t l = 0; l <= level; ++l) {
+                        LincombJob jb{};
+                        jb.out = out.p[i][poly] + l * N;
+                        jb.mod = (int)l;
+                        jb.accumulate = ch > 0;
+                        jb.add = (ch == 0 && poly == 0) ? cadd[l] : 0;
+                        const uint64_t q = c_.q[l];
+                        for (size_t t = ch * kMaxLincombTerms; t < std::min(terms.size(), (ch + 1) * kMaxLincombTerms); ++t) {
+                            const LinTerm& tm = terms[t];
+                            if (poly >= tm.x.np || tm.c[l] == 0) continue;
+                            jb.src[jb.n] = tm.x.p[i][poly] + l * N;
+                            jb.c[jb.n] = tm.c[l];
+                            jb.cs[jb.n] = host::shoup(tm.c[l], q);
+                            ++jb.n;
+                        }
+                        jobs.push_back(jb);
+                    }
+            JobTable t;
+            const LincombJob* j = t.add(jobs);
+            t.upload(c_, s_);
+            double words = 0;
+            for (const auto& jb : jobs) words += jb.n + 1 + jb.accumulate;
+            Probe probe(kClsElementwise, 8.0 * N * words, s_);
+            kb_lincomb<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+            check_cuda(cudaGetLastError(), "linear combination");
+        }
+        return out;
     }
 
     // ckks_conjugate: automorphism X -> X^(2N-1) of (b, a), then key switch of the permuted a.

@@ -330,32 +330,26 @@ private:
         ops_.scalar(x, nullptr, constants(value, scale, x.level), kScalarAdd);
     }
 
-    // multiply_by_integer_scalar_inplace
-    void mul_integer(CtBatch& x, long double scalar, long double out_scale) {
+    // the integer of multiply_by_integer_scalar_inplace, with its checks
+    static uint64_t checked_integer(long double scalar) {
         if (!std::isfinite(scalar) || scalar < 0.0L) throw std::invalid_argument("ckks_evalchebyshev: invalid scalar scale-up");
         const long double r = std::round(scalar);
         if (r < 1.0L || std::abs(scalar - r) > std::max<long double>(1.0L, std::abs(scalar)) * 0x1p-20L)
             throw std::invalid_argument("ckks_evalchebyshev: non-integral scalar scale-up");
         if (r > static_cast<long double>(std::numeric_limits<uint64_t>::max()))
             throw std::invalid_argument("ckks_evalchebyshev: scalar scale-up is too large");
-        const uint64_t s = static_cast<uint64_t>(r);
+        return static_cast<uint64_t>(r);
+    }
+
+    // multiply_by_integer_scalar_inplace
+    void mul_integer(CtBatch& x, long double scalar, long double out_scale) {
+        const uint64_t s = checked_integer(scalar);
         if (s != 1) {
             std::vector<uint64_t> v(x.level + 1);
             for (size_t l = 0; l <= x.level; ++l) v[l] = s % c_.q[l];
             ops_.scalar(x, nullptr, v, kScalarMul);
         }
         x.scale = static_cast<double>(out_scale);
-    }
-
-    void scale_up_to(CtBatch& x, long double target) {
-        const double cur = static_cast<double>(x.scale), tgt = static_cast<double>(target);
-        const double m = std::max({1.0, std::abs(cur), std::abs(tgt)});
-        if (std::isfinite(cur) && std::isfinite(tgt) && std::abs(cur - tgt) <= 0x1p-45 * m) {
-            x.scale = static_cast<double>(target);
-            return;
-        }
-        if (x.scale > target) throw std::invalid_argument("ckks_evalchebyshev: cannot scale down ciphertext during scale alignment");
-        mul_integer(x, target / x.scale, target);
     }
 
     long double rescale_product(size_t level) const {
@@ -373,22 +367,77 @@ private:
         ops_.pad(x, np);
     }
 
+    // A leaf of the Paterson-Stockmeyer evaluation, accumulated lazily: its metadata (level,
+    // polynomial count, scale) follows the reference's steps one by one, while the data steps
+    // (constant adds, multiply-adds of the powers, integer scale-ups of the running sum) are
+    // folded into one constant per power and limb and formed by one linear-combination launch.
+    // Every step is an exact modular operation on canonical residues, so the sum equals the
+    // step-by-step result.
+    struct Leaf {
+        size_t level;
+        int np;
+        long double scale;
+        std::vector<uint64_t> cadd;
+        std::vector<DeviceOps::LinTerm> terms;
+    };
+
+    static uint64_t mulmod(uint64_t a, uint64_t b, uint64_t q) { return (uint64_t)((unsigned __int128)a * b % q); }
+
+    void leaf_align(Leaf& r, size_t level, double scale, int np) {
+        if (level > r.level) throw std::invalid_argument("ckks_drop_to_level_inplace: cannot raise ciphertext level");
+        if (np < r.np) throw std::invalid_argument("ckks_evalchebyshev: cannot shrink ciphertext degree by padding");
+        r.level = level;
+        r.scale = scale;
+        r.np = np;
+    }
+
+    void leaf_add_constant(Leaf& r, double value, long double scale) {
+        if (value == 0.0) return;
+        const std::vector<uint64_t> v = constants(value, scale, r.level);
+        for (size_t l = 0; l <= r.level; ++l) r.cadd[l] = add_mod(r.cadd[l], v[l], c_.q[l]);
+    }
+
+    // multiply_by_integer_scalar_inplace on the running sum
+    void leaf_mul_integer(Leaf& r, long double scalar, long double out_scale) {
+        const uint64_t s = checked_integer(scalar);
+        if (s != 1)
+            for (size_t l = 0; l <= r.level; ++l) {
+                const uint64_t q = c_.q[l], sl = s % q;
+                r.cadd[l] = mulmod(r.cadd[l], sl, q);
+                for (auto& t : r.terms) t.c[l] = mulmod(t.c[l], sl, q);
+            }
+        r.scale = static_cast<double>(out_scale);
+    }
+
+    void leaf_scale_up_to(Leaf& r, long double target) {
+        const double cur = static_cast<double>(r.scale), tgt = static_cast<double>(target);
+        const double m = std::max({1.0, std::abs(cur), std::abs(tgt)});
+        if (std::isfinite(cur) && std::isfinite(tgt) && std::abs(cur - tgt) <= 0x1p-45 * m) {
+            r.scale = static_cast<double>(target);
+            return;
+        }
+        if (r.scale > target) throw std::invalid_argument("ckks_evalchebyshev: cannot scale down ciphertext during scale alignment");
+        leaf_mul_integer(r, target / r.scale, target);
+    }
+
     // multhenadd_real_scalar_scale_aware_inplace: out += scalar * x, scales reconciled.
-    void mul_then_add(const CtBatch& x, double scalar, CtBatch& out) {
+    void leaf_mul_then_add(const CtBatch& x, double scalar, Leaf& out) {
         if (scalar == 0.0) return;
         const size_t level = std::min(x.level, out.level);
         const double out_scale = static_cast<double>(out.scale);
         const int np = std::max(x.np, out.np);
-        align(out, level, out_scale, np);
-        CtBatch xa = ops_.clone(x);
-        align(xa, level, static_cast<double>(x.scale), np);
+        leaf_align(out, level, out_scale, np);
+        // x aligned to (level, its own scale): metadata only, x's buffers are read as they are
+        CtBatch xa = x;
+        xa.level = level;
+        xa.scale = static_cast<double>(x.scale);
         long double scale_rlwe = 0.0L;
         if (scales_close(static_cast<double>(xa.scale), static_cast<double>(out.scale))) {
             if (is_integer(scalar)) {
                 scale_rlwe = 1.0L;
             } else {
                 scale_rlwe = rescale_product(level);
-                scale_up_to(out, out.scale * scale_rlwe);
+                leaf_scale_up_to(out, out.scale * scale_rlwe);
             }
         } else if (xa.scale < out.scale) {
             scale_rlwe = out.scale / xa.scale;
@@ -398,29 +447,29 @@ private:
         const long double term_scale = xa.scale * scale_rlwe;
         if (!scales_close(static_cast<double>(term_scale), static_cast<double>(out.scale)))
             throw std::runtime_error("ckks_evalchebyshev: MulThenAdd scale mismatch");
-        ops_.scalar(out, &xa, constants(scalar, scale_rlwe, out.level), kScalarMulAdd);
+        out.terms.push_back({xa, constants(scalar, scale_rlwe, out.level)});
     }
 
     CtBatch eval_leaf(size_t target_level, const Poly& p) {
         const size_t degree = p.degree();
-        CtBatch r = ops_.zeros(target_level, static_cast<double>(p.scale));
-        if (p.even && p.coeffs[0] != 0.0) add_constant(r, p.coeffs[0], p.scale);
-        if (degree == 0) return r;
-        for (size_t e = degree; e > 0; --e) {
-            const double cf = p.coeffs[e];
-            if (cf == 0.0) continue;
-            if (!((!p.even && !p.odd) || ((e & 1U) == 0U && p.even) || ((e & 1U) == 1U && p.odd))) continue;
-            align(r, target_level, static_cast<double>(p.scale), r.np);
-            mul_then_add(values_.at(e), cf, r);
-        }
-        return r;
+        Leaf r{target_level, 2, static_cast<double>(p.scale), std::vector<uint64_t>(target_level + 1, 0), {}};
+        if (p.even && p.coeffs[0] != 0.0) leaf_add_constant(r, p.coeffs[0], p.scale);
+        if (degree > 0)
+            for (size_t e = degree; e > 0; --e) {
+                const double cf = p.coeffs[e];
+                if (cf == 0.0) continue;
+                if (!((!p.even && !p.odd) || ((e & 1U) == 0U && p.even) || ((e & 1U) == 1U && p.odd))) continue;
+                leaf_align(r, target_level, static_cast<double>(p.scale), r.np);
+                leaf_mul_then_add(values_.at(e), cf, r);
+            }
+        return ops_.lincomb(r.level, r.np, r.scale, r.cadd, r.terms);
     }
 
     // evaluate_monomial: odd <- even + rescale(relin(odd)) * xpow
     void monomial(CtBatch& even, CtBatch& odd, const CtBatch& xpow) {
         if (odd.np == 3) ops_.relin(odd);
         ops_.rescale(odd);
-        CtBatch xp = ops_.clone(xpow);
+        CtBatch xp = xpow;  // read only by the tensor product
         if (odd.level > xp.level) throw std::invalid_argument("ckks_drop_to_level_inplace: cannot raise ciphertext level");
         xp.level = odd.level;
         const long double prod = odd.scale * xp.scale;
@@ -461,7 +510,7 @@ private:
         const size_t level = a == b ? out.level : std::min(out.level, values_.at(b).level);
         out.level = level;
         const ExactScale prod = times(exact_.at(a), exact_.at(b));
-        CtBatch rhs = ops_.clone(values_.at(b));  // the square uses a second copy (no aliasing)
+        CtBatch rhs = values_.at(b);  // read only by the tensor product (out is a fresh copy)
         rhs.level = level;
         ops_.tensor(out, rhs);
         ops_.relin(out);
@@ -472,12 +521,19 @@ private:
             add_constant(out, -1.0, prod.value(c_.q));
         } else {
             gen_power(cdeg);
-            CtBatch corr = ops_.clone(values_.at(cdeg));
+            // out -= ratio * T_cdeg as one multiply-add by -ratio (T_cdeg itself is only read)
+            CtBatch corr = values_.at(cdeg);
             const uint64_t ratio = ratio_u64(prod, exact_.at(cdeg), c_.q);
             corr.scale = exact_.at(cdeg).value_d(c_.q);
             align(corr, out.level, static_cast<double>(corr.scale), out.np);
-            mul_integer(corr, static_cast<long double>(ratio), prod.value(c_.q));
-            ops_.add(out, corr, true);
+            const uint64_t s = checked_integer(static_cast<long double>(ratio));
+            if (s == 1) {
+                ops_.add(out, corr, true);
+            } else {
+                std::vector<uint64_t> v(out.level + 1);
+                for (size_t l = 0; l <= out.level; ++l) v[l] = (c_.q[l] - s % c_.q[l]) % c_.q[l];
+                ops_.scalar(out, &corr, v, kScalarMulAdd);
+            }
         }
         values_.insert_or_assign(n, std::move(out));
         exact_.insert_or_assign(n, prod);
