@@ -69,16 +69,45 @@ void check_ptr(const void* p, const char* who) {
     if (!p) wg::fail(wg::kInvalid, std::string(who) + ": null buffer");
 }
 
+bool stream_capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (s) cudaStreamIsCapturing(s, &cs);
+    return cs != cudaStreamCaptureStatusNone;
+}
+
+// One key switch of one ciphertext.  Outside stream capture it runs as a batch of one (each
+// stage of the switch, all digits included, in a single launch); under capture, stage by stage
+// on the stream's reserved workspace (the batched path stages a job table per call).
+void switch_one(wg::Context& c, size_t level, const uint64_t* key_term, const wg::KeyEntry& k, const uint64_t* b_in,
+                const uint64_t* a_in, uint64_t* b, uint64_t* a, bool a_add, uint64_t galois, cudaStream_t s) {
+    if (stream_capturing(s)) {
+        wg::keyswitch(c, level, key_term, k, b_in, a_in, b, a, true, a_add, galois, c.workspace(s), s);
+        return;
+    }
+    wg::KsItem it;
+    it.level = level;
+    it.key_term = key_term;
+    it.key = &k;
+    it.b_in = b_in;
+    it.a_in = a_in;
+    it.b = b;
+    it.a = a;
+    it.b_add = 1;
+    it.a_add = a_add ? 1 : 0;
+    it.galois = galois;
+    wg::batch_keyswitch(c, &it, 1, s);
+}
+
 void do_rotate(wg::Context& c, size_t level, uint64_t* b, uint64_t* a, int64_t rotation, cudaStream_t s) {
     const int64_t r = normalize_rotation(c, rotation);
     if (r == 0) return;
     const wg::KeyEntry& k = c.key(WG_KEY_ROTATION, r);
-    wg::keyswitch(c, level, a, k, b, a, b, a, true, false, rotation_galois(c, r), c.workspace(s), s);
+    switch_one(c, level, a, k, b, a, b, a, false, rotation_galois(c, r), s);
 }
 
 void do_relin(wg::Context& c, size_t level, uint64_t* c0, uint64_t* c1, const uint64_t* c2, cudaStream_t s) {
     const wg::KeyEntry& k = c.key(WG_KEY_RELIN, 0);
-    wg::keyswitch(c, level, c2, k, c0, c1, c0, c1, true, true, 0, c.workspace(s), s);
+    switch_one(c, level, c2, k, c0, c1, c0, c1, true, 0, s);
 }
 
 uint64_t* scratch_after_switch(wg::Context& c, cudaStream_t s) {

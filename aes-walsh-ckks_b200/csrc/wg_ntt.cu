@@ -137,13 +137,14 @@ void launch_phase(const Context& c, uint64_t* data, int limbs, int polys, size_t
     if (jobs) {
         enable_smem<LOGN, FWD, COLS, true>();
         const dim3 grid(P::N / P::TILE, njobs < 65535 ? njobs : 65535, (njobs + 65534) / 65535);
-        Probe probe(kClsNtt, 16.0 * P::N * njobs, s);
+        // algorithmic bytes: every residue read once and written once per transform, i.e. 8 B
+        // per residue for each of the two phases (16 N B per limb-transform)
+        Probe probe(kClsNtt, 8.0 * P::N * njobs, s);
         k_ntt_phase<LOGN, FWD, COLS, true><<<grid, P::THREADS, sm, s>>>(nullptr, 0, map, jobs, njobs, c.d_mod, c.d_tw);
     } else {
         enable_smem<LOGN, FWD, COLS, false>();
         const dim3 grid(P::N / P::TILE, limbs, polys);
-        // algorithmic bytes: every residue read once and written once
-        Probe probe(kClsNtt, 16.0 * P::N * limbs * polys, s);
+        Probe probe(kClsNtt, 8.0 * P::N * limbs * polys, s);
         k_ntt_phase<LOGN, FWD, COLS, false><<<grid, P::THREADS, sm, s>>>(data, stride, map, nullptr, 0, c.d_mod,
                                                                          c.d_tw);
     }

@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--no-probe", action="store_true", help="skip the per-kernel-class event-timing passes")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass")
     ap.add_argument("--no-ops", action="store_true", help="skip the batched-ops section")
+    ap.add_argument("--no-ntt", action="store_true", help="skip the NTT / rotation primitives section")
+    ap.add_argument("--no-aes", action="store_true",
+                    help="skip the AES-CTR headline (a small profiling case of the other sections; no headline value)")
     ap.add_argument("--no-bsgs", action="store_true", help="skip the CoeffToSlot / SlotToCoeff section")
     ap.add_argument("--ops-steps", type=int, default=50)
     ap.add_argument("--ops-count", type=int, default=OPS_COUNT)
@@ -398,6 +401,12 @@ def ops_bench(args, wg, torch, stream, timed, rank, local):
                "h2d_bytes_per_step": int(sum(4 * (int(lv) + 1) * N * 8 for lv in levels)),
                "d2h_bytes_per_step": int(sum(2 * int(lv) * N * 8 for lv in levels)), "chunk": chunk}
     plan.close()
+    K = len(P_BITS)
+    alg = 0.0
+    for lv in levels:
+        lq = int(lv) + 1
+        beta = ctx.parts(int(lv))
+        alg += 8.0 * N * (4 * lq + 2 * beta * 2 * (lq + K) + 2 * lq)
     res = {
         "workload": f"{count} walsh15 ciphertexts at seeded levels 1..12, each ct x ct multiply + relinearize + "
                     f"rescale + rotate by a seeded walsh15 AES rotation index",
@@ -408,10 +417,63 @@ def ops_bench(args, wg, torch, stream, timed, rank, local):
         "plain_per_op": {"value": count / (plain_ms / 1000.0), "ms_per_step": plain_ms,
                          "launches_per_step": plain_launches},
         "batched_over_plain": plain_ms / graph_ms,
+        "algorithmic_bytes_per_step": alg,
+        "algorithmic_gbs": alg / (graph_ms * 1e6),
+        "algorithmic_bytes_note": "per ciphertext 8 N [4 Lq (two inputs) + 2 beta 2 (Lq + K) (relin and "
+                                  "rotation keys) + 2 Lq (output)]: the pipeline's compulsory traffic",
         "ntt": {"launches": n, "ms": kms, "gbs": kbytes / (kms * 1e6) if kms else None},
         "e2e": e2e, "steps": steps,
     }
     return res, ctx, q, p
+
+
+# ------------------------------------------------------------------------------------------
+# primitives: batched NTT at walsh15, and the plain single-ciphertext config-1 primitives
+# ------------------------------------------------------------------------------------------
+def ntt_bench(wg, torch, stream, timed, local, steps, hbm):
+    """Forward and inverse negacyclic NTT over batches of limbs, and one hybrid key switch
+    (rotation by +1) of a single ciphertext.  Algorithmic bytes: 16 N B per limb-transform
+    (each residue read and written once); a rotation moves 8 N [2 Lq + beta 2 (Lq + K) + 2 Lq] B
+    (ciphertext in, evaluation key, ciphertext out)."""
+    res = {}
+    shapes = (("walsh15_batch", 15, Q_BITS, P_BITS, DNUM, 16),   # 16 ciphertext polynomials x 13 limbs
+              ("config1", 14, [50] * 16, [50] * 4, 4, 2))         # one ciphertext (a, b) x 16 limbs
+    for name, logn, qb, pb, dnum, polys in shapes:
+        N = 1 << logn
+        p, q = wg.find_primes(pb, qb, N)
+        ctx = wg.Context(N, q, p, dnum, device=local)
+        L, K = len(q), len(p)
+        rng = np.random.default_rng(logn)
+        qcol = np.repeat(q, N)
+        host = np.stack([(rng.integers(0, 1 << 62, L * N, dtype=np.uint64) % qcol).astype(np.uint64)
+                         for _ in range(polys)])
+        data = torch.from_numpy(host.view(np.int64)).cuda()
+        fwd = lambda: ctx.ntt_forward(data, L, polys=polys, stride=L * N, stream=stream)
+        inv = lambda: ctx.ntt_inverse(data, L, polys=polys, stride=L * N, stream=stream)
+        for _ in range(3):
+            fwd()
+            inv()
+        tf, ti = timed(fwd, steps), timed(inv, steps)
+        nbytes = 16.0 * N * L * polys
+        entry = {"ring_degree": N, "limbs": L, "polynomials": polys,
+                 "forward_us": 1000 * tf, "inverse_us": 1000 * ti,
+                 "forward_gbs": nbytes / (tf * 1e6), "inverse_gbs": nbytes / (ti * 1e6),
+                 "forward_frac": nbytes / (tf * 1e6) / hbm, "inverse_frac": nbytes / (ti * 1e6) / hbm}
+        if name == "config1":
+            parts = ctx.parts(L - 1)
+            mods = np.concatenate([q, p]).astype(np.uint64)
+            col = np.tile(np.repeat(mods, N), 2 * parts)
+            ctx.set_key(wg.WG_KEY_ROTATION, (rng.integers(0, 1 << 62, col.size, dtype=np.uint64) % col)
+                        .astype(np.uint64), rotation=1)
+            rot = lambda: ctx.rotate(L - 1, data[0], data[1], 1, stream=stream)
+            for _ in range(3):
+                rot()
+            tr = timed(rot, steps)
+            rbytes = 8.0 * N * (2 * L + parts * 2 * (L + K) + 2 * L)
+            entry.update({"rotation_us": 1000 * tr, "rotation_gbs": rbytes / (tr * 1e6),
+                          "rotation_frac": rbytes / (tr * 1e6) / hbm, "dnum": dnum})
+        res[name] = entry
+    return res
 
 
 # ------------------------------------------------------------------------------------------
@@ -533,6 +595,20 @@ def main():
         return max_over_ranks(e0.elapsed_time(e1) / k)
 
     plan = load_plan()
+    if args.no_aes:
+        hbm = 6650.0
+        try:
+            hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", hbm))
+        except (OSError, ValueError):
+            pass
+        prim = None if args.no_ntt else ntt_bench(wg, torch, stream, timed, local, 20, hbm)
+        ops = None if args.no_ops else ops_bench(args, wg, torch, stream, timed, rank, local)[0]
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "note": "--no-aes profiling run",
+                              "primitives": prim, "batched_ops": ops}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     aes = AesRun(wg, torch, plan, local, args.seed + rank)
     N = aes.N
     aes_step = lambda: aes.step(stream)
@@ -618,10 +694,11 @@ def main():
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "avg_launch_us": 1000 * dom["ms"] / max(1, dom["launches"]),
                 "bytes_per_launch": dom["bytes"] / max(1, dom["launches"]),
-                "keyswitch": {"achieved": ks_bytes / (ks_ms * 1e6) if ks_ms else None,
-                              "frac": ks_bytes / (ks_ms * 1e6) / hbm if ks_ms else None,
-                              "classes": "modup + key inner product + moddown"}}
+                "keyswitch_kernels": {"gbs": ks_bytes / (ks_ms * 1e6) if ks_ms else None,
+                                      "classes": "modup + key inner product + moddown, bytes each kernel "
+                                                 "reads and writes (intermediates included)"}}
 
+    prim = None if args.no_ntt else ntt_bench(wg, torch, stream, timed, local, 20, hbm)
     ops, ops_ctx = None, None
     if not args.no_ops:
         ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local)
@@ -631,6 +708,12 @@ def main():
             p, q = wg.find_primes(P_BITS, Q_BITS, N)
             ops_ctx = wg.Context(N, q, p, DNUM, device=local)
         bsgs = bsgs_bench(wg, ops_ctx, q, p, stream, timed, 10, args.warmup)
+    if ops:
+        # key switching against HBM: the batched mul + relin + rescale + rotate pipeline (two key
+        # switches per ciphertext) at its compulsory bytes over the graph-replay time
+        roofline["keyswitch"] = {"achieved": ops["algorithmic_gbs"], "peak": hbm, "unit": "GB/s",
+                                 "frac": ops["algorithmic_gbs"] / hbm,
+                                 "workload": "batched_ops (relin + rotation key switches dominate)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -665,6 +748,7 @@ def main():
         "output_levels": sorted(set(int(x) for x in out_levels)) if out_levels else None,
         "roofline": roofline,
         "kernels": kernels,
+        "primitives": prim,
         "batched_ops": ops,
         "bsgs": bsgs,
         "cpu_baseline": cpu,
