@@ -2,8 +2,7 @@
 //
 // Some callers cannot call cudaMalloc at the moment they need a rotation: an application whose
 // device memory was reserved up front by another allocator (a serving engine that claims most
-// of HBM at start-up), code running while a stream is being captured into a CUDA graph (where
-// allocation calls are not allowed), or latency-sensitive loops that must avoid the device-wide
+// of HBM at start-up), or latency-sensitive loops that must avoid the device-wide
 // synchronisation cudaMalloc/cudaFree can cause.  wg_rotate_noalloc serves them: apart from the
 // context's own tables and keys (allocated once at creation) it uses only the array below.
 //

@@ -281,14 +281,10 @@ int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const w
                      uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
                      void* stream);
 
-
-
-
 /* Rotation that allocates no device memory (no counterpart in the reference, whose
  * operations all allocate host vectors).  For callers that cannot call cudaMalloc when they
- * rotate: memory reserved up front by another allocator, work issued while a stream is being
- * captured into a CUDA graph, or loops that must not trigger the synchronisation allocation
- * can cause.  Same result as wg_rotate.  The key-switch scratch is a file-scope static device
+ * rotate: memory reserved up front by another allocator, or loops that must not trigger the
+ * synchronisation an allocation can cause.  Same result as wg_rotate.  The key-switch scratch is a file-scope static device
  * array of 32 MiB that every GPU loading the library holds until exit; a level needing more
  * returns WG_ERR_INVALID.  All calls share that array (nothing in it needs clearing between
  * calls), so calls that overlap on the GPU race: serialise them.  The first call on a device

@@ -1,6 +1,6 @@
 """wg_rotate_noalloc: the rotation for callers that cannot allocate device memory when they
-rotate (memory already claimed by another allocator, work issued during CUDA-graph capture,
-loops that must avoid allocation-induced synchronisation).  Its key-switch scratch is the
+rotate (memory already claimed by another allocator, loops that must avoid allocation-induced
+synchronisation).  Its key-switch scratch is the
 library's fixed 32 MiB static device array instead of per-stream workspace.
 
 Checked through the C ABI against wg_rotate, bit for bit, on two calls in a row (the array
