@@ -127,6 +127,14 @@ WG_HD uint64_t reduce128(uint64_t z_hi, uint64_t z_lo, const Modulus& m) {
     return r >= m.q ? r - m.q : r;
 }
 
+// Canonical residue of any a < 2^64: the estimate umulhi(a, mu_hi), mu_hi = floor(mu / 2^64)
+// >= 2^64 / q - 1, is at most one below floor(a / q) and never above it.
+WG_HD uint64_t reduce64(uint64_t a, const Modulus& m) {
+    uint64_t r = a - umulhi(a, m.mu_hi) * m.q;
+    if (r >= m.q) r -= m.q;
+    return r >= m.q ? r - m.q : r;
+}
+
 // barrett_reduce_u64 (modarith.hpp:53-58).
 WG_HD uint64_t barrett_u64(uint64_t a, uint64_t q, uint64_t mu_hi) {
     const uint64_t q_hat = umulhi(a, mu_hi);

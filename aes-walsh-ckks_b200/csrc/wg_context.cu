@@ -118,7 +118,51 @@ BatchBuffers& Context::batch_buffers(cudaStream_t s) {
     return batches[s];
 }
 
+void* Context::take_chunk(size_t bytes, cudaStream_t s, size_t* got) {
+    if (capturing(s)) return nullptr;  // no dependency on work outside a capture
+    std::lock_guard<std::mutex> g(chunk_mutex);
+    auto it = chunk_cache.lower_bound(bytes);
+    if (it == chunk_cache.end() || it->first > 2 * bytes) return nullptr;
+    const CachedChunk ch = it->second;
+    chunk_cache.erase(it);
+    chunk_cache_bytes -= ch.bytes;
+    check_cuda(cudaStreamWaitEvent(s, ch.done, 0), "chunk reuse");
+    chunk_events.push_back(ch.done);
+    *got = ch.bytes;
+    return ch.p;
+}
+
+void Context::give_chunk(void* p, size_t bytes, cudaStream_t s) {
+    std::lock_guard<std::mutex> g(chunk_mutex);
+    if (capturing(s) || chunk_cache_bytes + bytes > kChunkCacheBytes) {
+        cudaFreeAsync(p, s);
+        return;
+    }
+    cudaEvent_t ev = nullptr;
+    if (!chunk_events.empty()) {
+        ev = chunk_events.back();
+        chunk_events.pop_back();
+    } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeAsync(p, s);
+        return;
+    }
+    if (cudaEventRecord(ev, s) != cudaSuccess) {
+        cudaGetLastError();
+        chunk_events.push_back(ev);
+        cudaFreeAsync(p, s);
+        return;
+    }
+    chunk_cache.emplace(bytes, CachedChunk{p, bytes, ev});
+    chunk_cache_bytes += bytes;
+}
+
 Context::~Context() {
+    for (auto& kv : chunk_cache) {
+        cudaFree(kv.second.p);
+        cudaEventDestroy(kv.second.done);
+    }
+    for (cudaEvent_t ev : chunk_events) cudaEventDestroy(ev);
     for (auto& kv : consts) {
         cudaFree(kv.second.d);
         cudaEventDestroy(kv.second.ready);

@@ -124,7 +124,8 @@ public:
     DeviceOps(Context& c, size_t count, cudaStream_t s) : c_(c), count_(count), s_(s) {}
     ~DeviceOps() {
         WG_SPAN("free");
-        for (uint64_t* p : owned_) cudaFreeAsync(p, s_);
+        // chunks go back to the context for later operation sets (see Context::give_chunk)
+        for (const auto& ch : owned_) c_.give_chunk(ch.first, ch.second * 8, s_);
     }
     DeviceOps(const DeviceOps&) = delete;
     DeviceOps& operator=(const DeviceOps&) = delete;
@@ -618,14 +619,19 @@ private:
         words = (words + 31) & ~size_t{31};  // 256-byte alignment
         if (words > left_) {
             WG_SPAN("alloc");
-            const size_t chunk = std::max(words, next_chunk_);
+            // power-of-two chunk sizes, so chunks handed back by earlier operation sets fit
+            size_t chunk = kFirstChunkWords;
+            while (chunk < std::max(words, next_chunk_)) chunk <<= 1;
             next_chunk_ = std::min(next_chunk_ * 2, kMaxChunkWords);
-            uint64_t* p = nullptr;
-            if (cudaMallocAsync((void**)&p, chunk * 8, s_) != cudaSuccess) {
+            size_t got = 0;
+            uint64_t* p = static_cast<uint64_t*>(c_.take_chunk(chunk * 8, s_, &got));
+            if (p) {
+                chunk = got / 8;
+            } else if (cudaMallocAsync((void**)&p, chunk * 8, s_) != cudaSuccess) {
                 cudaGetLastError();
                 fail(kNoMemory, "ckks_evalchebyshev: device allocation failed");
             }
-            owned_.push_back(p);
+            owned_.push_back({p, chunk});
             cur_ = p;
             left_ = chunk;
         }
@@ -656,7 +662,7 @@ private:
     Context& c_;
     size_t count_;
     cudaStream_t s_;
-    std::vector<uint64_t*> owned_;
+    std::vector<std::pair<uint64_t*, size_t>> owned_;  // chunks and their sizes in words
     uint64_t* cur_ = nullptr;
     size_t left_ = 0, next_chunk_ = kFirstChunkWords;
     std::map<std::tuple<double, double, double, size_t>, uint64_t*> const_cache_;

@@ -157,6 +157,23 @@ struct Context {
     std::mutex const_mutex;
     std::map<std::tuple<double, double, double, size_t>, ConstPlain> consts;
     size_t const_bytes = 0;
+    // Chunks of stream-ordered device memory that finished operation sets hand back for later
+    // ones: each carries an event recorded on the stream that last used it, and a taker's stream
+    // waits on that event before its first use, so reuse needs no host synchronisation and
+    // works across streams.  At most kChunkCacheBytes are kept; the rest is freed.
+    struct CachedChunk {
+        void* p;
+        size_t bytes;
+        cudaEvent_t done;
+    };
+    static constexpr size_t kChunkCacheBytes = size_t{24} << 30;
+    std::mutex chunk_mutex;
+    std::multimap<size_t, CachedChunk> chunk_cache;
+    std::vector<cudaEvent_t> chunk_events;
+    size_t chunk_cache_bytes = 0;
+    // a cached chunk of at least `bytes` (at most twice that) made safe for use on s, or nullptr
+    void* take_chunk(size_t bytes, cudaStream_t s, size_t* got);
+    void give_chunk(void* p, size_t bytes, cudaStream_t s);
 
     ~Context();
     uint64_t* workspace(cudaStream_t s);   // scratch for one in-flight operation on stream s

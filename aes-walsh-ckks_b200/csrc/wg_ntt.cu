@@ -14,8 +14,9 @@
 //     round (one shared-memory round trip per three stages);
 //   * grid.y indexes limbs and grid.z polynomials, so one launch covers a whole ciphertext
 //     batch; each limb picks its modulus through a LimbMap (Q limbs, P limbs or a mix).
-// Butterflies are Harvey/Shoup with lazy ranges: forward values stay in [0, 4q), inverse in
-// [0, 2q); the last phase canonicalises (forward) or scales by N^-1 with Shoup (inverse).
+// Butterflies are Harvey/Shoup with lazy ranges: forward values stay in [0, 4q) (or, for moduli
+// below 2^58, grow by at most 2q per stage without reduction, see kLazyForwardLimit), inverse
+// in [0, 2q); the last phase canonicalises (forward) or scales by N^-1 with Shoup (inverse).
 #include <utility>
 
 #include "wg_internal.hpp"
@@ -25,10 +26,10 @@ namespace wg {
 namespace {
 using namespace ntt;
 
-template <int LOGN, bool FWD, bool COLS, int... RD>
+template <int LOGN, bool FWD, bool COLS, bool LAZY, int... RD>
 __device__ __forceinline__ void ntt_rounds(std::integer_sequence<int, RD...>, uint64_t* sm, int sub,
                                            int o, uint64_t q, const uint64_t* tw, const uint64_t* tws) {
-    ((ntt_round<LOGN, FWD, COLS, RD>(sm, sub, o, q, tw, tws), __syncthreads()), ...);
+    ((ntt_round<LOGN, FWD, COLS, RD, LAZY>(sm, sub, o, q, tw, tws), __syncthreads()), ...);
 }
 
 template <int LOGN, bool FWD, bool COLS>
@@ -102,7 +103,12 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS, 4)
 
     const int sub = COLS ? t % P::SUBS : t >> P::OB;
     const int o = COLS ? t / P::SUBS : t & ((1 << P::OB) - 1);
-    ntt_rounds<LOGN, FWD, COLS>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, q, tw_s, tws_s);
+    // forward transforms under kLazyForwardLimit skip the per-butterfly reduction (uniform per CTA)
+    const bool lazy = FWD && q < kLazyForwardLimit;
+    if (lazy)
+        ntt_rounds<LOGN, FWD, COLS, true>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, q, tw_s, tws_s);
+    else
+        ntt_rounds<LOGN, FWD, COLS, false>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, q, tw_s, tws_s);
 
     uint64_t n_inv = 0, n_inv_s = 0;
     if (P::LAST && !FWD) {
@@ -113,7 +119,7 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS, 4)
     for (int k = 0; k < 8; ++k) {
         const int e = t + k * P::THREADS;
         uint64_t val = sm[pad16(e)];
-        if (P::LAST) val = FWD ? red4q(val, q) : mul_shoup(val, n_inv, n_inv_s, q);
+        if (P::LAST) val = FWD ? (lazy ? reduce64(val, mods[mi]) : red4q(val, q)) : mul_shoup(val, n_inv, n_inv_s, q);
         x[tile_offset<LOGN, FWD, COLS>(tile, e)] = val;
     }
 }

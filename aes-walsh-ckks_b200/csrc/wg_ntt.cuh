@@ -90,15 +90,24 @@ WG_HDC int round_bits(const RoundPlan& p, int j) {
     return ((j & 1) << p.g[0]) | (((j >> 1) & 1) << p.g[1]) | (((j >> 2) & 1) << p.g[2]);
 }
 
+// Moduli for which the forward transform may skip the per-butterfly reduction of its upper
+// input: each stage then adds at most 2q to a value's bound, so the at most 16 stages of
+// N <= 2^16 take inputs below 4q to values below (4 + 2 x 16) q = 36 q < 2^64, and the Shoup
+// lazy product accepts any 64-bit input.  The last phase then reduces the full word (reduce64)
+// instead of a value below 4q.
+constexpr uint64_t kLazyForwardLimit = uint64_t{1} << 58;
+static_assert((4 + 2 * 16) < (1 << (64 - 58)), "lazy forward bound: 36 q < 2^64 for q < 2^58");
+
 // One round (up to three radix-2 stages) for thread (sub, o); tw / tws are the staged
-// twiddles of this CTA (twiddle_src order).
+// twiddles of this CTA (twiddle_src order).  LAZY (forward only, q < kLazyForwardLimit) keeps
+// the upper value unreduced through the round.
 //
 // The thread's 8 elements are base | round_bits(j), with base's bits disjoint from the group
 // positions, so every index splits into a runtime part (one per round, or one per stage for
 // twiddles) plus a compile-time offset: pad16 and shifts distribute over disjoint bit sets.
 // Loads then use immediate offsets, and butterflies of a stage that share a twiddle load it
 // once (same address).
-template <int LOGN, bool FWD, bool COLS, int RD>
+template <int LOGN, bool FWD, bool COLS, int RD, bool LAZY = false>
 WG_HD void ntt_round(uint64_t* sm, int sub, int o, uint64_t q, const uint64_t* __restrict__ tw,
                      const uint64_t* __restrict__ tws) {
     using P = Phase<LOGN, FWD, COLS>;
@@ -134,7 +143,7 @@ WG_HD void ntt_round(uint64_t* sm, int sub, int o, uint64_t q, const uint64_t* _
             const uint64_t w = tw_st[k], ws = tws_st[k];
             if (FWD) {
                 uint64_t t = v[j];
-                if (t >= two_q) t -= two_q;
+                if (!LAZY && t >= two_q) t -= two_q;
                 const uint64_t u = mul_shoup_lazy(v[j1], w, ws, q);
                 v[j] = t + u;
                 v[j1] = t + two_q - u;

@@ -50,13 +50,6 @@ WG_HD int clz64(uint64_t x) {
 #endif
 }
 
-// Canonical residue of a < 2^64: the estimate umulhi(a, mu_hi) is at most one below floor(a / q).
-WG_HD uint64_t reduce64(uint64_t a, const Modulus& m) {
-    uint64_t r = a - umulhi(a, m.mu_hi) * m.q;
-    if (r >= m.q) r -= m.q;
-    return r >= m.q ? r - m.q : r;
-}
-
 // canonical residue of sum_{lm=1..15} c[lm] s_lm for |c| <= 8 and canonical s
 WG_HD uint64_t walsh_small_sum(const uint64_t* s, const uint32_t* w, const Modulus& m) {
     if (m.q < (1ull << 55)) {

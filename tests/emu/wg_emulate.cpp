@@ -33,7 +33,7 @@ struct Emu {
     std::vector<std::vector<HostModUp>> modup;
 };
 
-template <int LOGN, bool FWD, bool COLS, int... RD>
+template <int LOGN, bool FWD, bool COLS, bool LAZY, int... RD>
 void rounds(std::integer_sequence<int, RD...>, uint64_t* sm, uint64_t q, const uint64_t* tw, const uint64_t* tws) {
     using P = ntt::Phase<LOGN, FWD, COLS>;
     auto one = [&](auto rd_const) {
@@ -41,7 +41,7 @@ void rounds(std::integer_sequence<int, RD...>, uint64_t* sm, uint64_t q, const u
         for (int t = 0; t < P::THREADS; ++t) {
             const int sub = COLS ? t % P::SUBS : t >> P::OB;
             const int o = COLS ? t / P::SUBS : t & ((1 << P::OB) - 1);
-            ntt::ntt_round<LOGN, FWD, COLS, R>(sm, sub, o, q, tw, tws);
+            ntt::ntt_round<LOGN, FWD, COLS, R, LAZY>(sm, sub, o, q, tw, tws);
         }
     };
     (one(std::integral_constant<int, RD>{}), ...);
@@ -62,10 +62,16 @@ void phase(const Emu& E, uint64_t* x, int mi) {
             tw_s[e] = tw[src];
             tws_s[e] = tws[src];
         }
-        rounds<LOGN, FWD, COLS>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), md.q, tw_s.data(), tws_s.data());
+        const bool lazy = FWD && md.q < ntt::kLazyForwardLimit;
+        if (lazy)
+            rounds<LOGN, FWD, COLS, true>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), md.q, tw_s.data(),
+                                          tws_s.data());
+        else
+            rounds<LOGN, FWD, COLS, false>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), md.q, tw_s.data(),
+                                           tws_s.data());
         for (int e = 0; e < P::TILE; ++e) {
             uint64_t v = sm[ntt::pad16(e)];
-            if (P::LAST) v = FWD ? red4q(v, md.q) : mul_shoup(v, md.n_inv, md.n_inv_shoup, md.q);
+            if (P::LAST) v = FWD ? (lazy ? reduce64(v, md) : red4q(v, md.q)) : mul_shoup(v, md.n_inv, md.n_inv_shoup, md.q);
             x[ntt::tile_offset<LOGN, FWD, COLS>(tile, e)] = v;
         }
     }
