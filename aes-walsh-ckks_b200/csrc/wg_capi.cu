@@ -8,6 +8,7 @@
 #include "wg_batch.hpp"
 #include "wg_encode.hpp"
 #include "wg_internal.hpp"
+#include "wg_serve.hpp"
 
 namespace wg {
 Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t* p, size_t np, size_t dnum,
@@ -561,6 +562,99 @@ int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const w
         wg::aes_ctr_walsh(c, bp, plans, ns2c_x2 ? 2 : 1, vc.data(), nc2s, coeffs, ncoeffs, a, out_b, out_a, out_level,
                           out_scale, S(stream));
     });
+}
+
+struct wg_server {
+    wg::Server* s;
+};
+
+int wg_serve_create(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
+                    const wg_lt_stage* const* s2c_x2, size_t ns2c_x2, const wg_lt_stage* const* c2s, size_t nc2s,
+                    const double* coeffs, size_t ncoeffs, size_t packing_block_count, size_t packed_segment_count,
+                    const uint64_t* const* key_b, const uint64_t* const* key_a, const double* key_scales,
+                    size_t key_level, const wg_serve_config* config, wg_server** out) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(out, "wg_serve");
+        check_ptr(config, "wg_serve");
+        check_ptr(key_scales, "wg_serve");
+        if (!key_b || !key_a) wg::fail(wg::kInvalid, "wg_serve: null key bits");
+        wg::ServeSetup su;
+        su.bp = boot_args(params, s2c, ns2c, c2s, nc2s, coeffs, su.s2c, su.c2s);
+        if (ns2c_x2 && !s2c_x2) wg::fail(wg::kInvalid, "wg_serve: null stage list");
+        for (size_t k = 0; k < ns2c_x2; ++k) {
+            check_ptr(s2c_x2[k], "wg_serve");
+            su.s2c_x2.push_back(s2c_x2[k]->s);
+        }
+        su.coeffs.assign(coeffs, coeffs + ncoeffs);
+        for (size_t k = 0; k < 1408; ++k) {
+            check_ptr(key_b[k], "wg_serve");
+            check_ptr(key_a[k], "wg_serve");
+            su.key_b.push_back(key_b[k]);
+            su.key_a.push_back(key_a[k]);
+            su.key_scales.push_back(key_scales[k]);
+        }
+        su.key_level = key_level;
+        su.packing_block_count = packing_block_count;
+        su.packed_segment_count = packed_segment_count;
+        wg::ServeConfig cfg;
+        cfg.workers = config->workers;
+        cfg.hbm_budget = config->hbm_budget_bytes;
+        cfg.eval_bytes = config->eval_bytes;
+        cfg.max_blocks = config->max_blocks;
+        cfg.batch_window_ms = config->batch_window_ms;
+        auto* h = new wg_server{nullptr};
+        try {
+            h->s = new wg::Server(c, std::move(su), cfg);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int wg_serve_submit(wg_server* server, const uint8_t* counters, const uint8_t* ciphertexts, size_t blocks,
+                    uint64_t* const* out_b, uint64_t* const* out_a, uint64_t* id) {
+    return guard([&] {
+        if (!server || !server->s) wg::fail(wg::kInvalid, "wg_serve: null server");
+        check_ptr(id, "wg_serve");
+        *id = server->s->submit(counters, ciphertexts, blocks, out_b, out_a);
+    });
+}
+
+int wg_serve_wait(wg_server* server, uint64_t id, double timeout_s, wg_serve_result* result) {
+    bool ready = false;
+    std::string err;
+    const int rc = guard([&] {
+        if (!server || !server->s) wg::fail(wg::kInvalid, "wg_serve: null server");
+        check_ptr(result, "wg_serve");
+        wg::ServeResult r;
+        ready = server->s->wait(id, timeout_s, &r);
+        if (!ready) return;
+        result->status = r.status;
+        result->block_offset = r.block_offset;
+        result->active_blocks = r.active_blocks;
+        result->batch_requests = r.batch_requests;
+        result->batch_blocks = r.batch_blocks;
+        result->queue_ms = r.queue_ms;
+        result->latency_ms = r.latency_ms;
+        for (size_t k = 0; k < 128; ++k) {
+            result->out_level[k] = r.out_level[k];
+            result->out_scale[k] = r.out_scale[k];
+        }
+        err = r.error;
+    });
+    if (rc != WG_OK) return rc;
+    if (!ready) return WG_NOT_READY;
+    if (!err.empty()) wg::set_last_error(err);
+    return WG_OK;
+}
+
+void wg_serve_destroy(wg_server* server) {
+    if (!server) return;
+    delete server->s;
+    delete server;
 }
 
 struct wg_batch_plan {

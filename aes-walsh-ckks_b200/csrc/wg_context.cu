@@ -82,7 +82,9 @@ uint64_t* BatchBuffers::arena(const Context& c, size_t words, cudaStream_t s) {
     if (words <= arena_words) return d_arena;
     if (capturing(s)) fail(kRuntime, "batched scratch must be sized (one uncaptured call) before graph capture");
     check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
-    cudaDeviceSynchronize();  // a smaller arena may still be in use by queued work
+    // the smaller arena may still be in use by work queued on this stream (the only user of
+    // this stream's arena); other streams keep running
+    check_cuda(cudaStreamSynchronize(s), "batched scratch resize");
     cudaFree(d_arena);
     d_arena = nullptr;
     arena_words = 0;

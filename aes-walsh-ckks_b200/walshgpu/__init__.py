@@ -92,6 +92,12 @@ def lib() -> C.CDLL:
         L.wg_aes_ctr_walsh.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, C.c_char_p,
                                        C.c_char_p, sz, vp, vp, vp, vp, vp]
         L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
+        L.wg_serve_create.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, vp,
+                                      C.POINTER(vp)]
+        L.wg_serve_submit.argtypes = [vp, C.c_char_p, C.c_char_p, sz, vp, vp, C.POINTER(C.c_uint64)]
+        L.wg_serve_wait.argtypes = [vp, C.c_uint64, C.c_double, vp]
+        L.wg_serve_destroy.argtypes = [vp]
+        L.wg_serve_destroy.restype = None
         L.wg_batch_plan_launch.argtypes = [vp, vp]
         L.wg_batch_plan_destroy.argtypes = [vp]
         L.wg_batch_plan_destroy.restype = None
@@ -248,6 +254,85 @@ class BootstrapParams(C.Structure):
     _fields_ = [("s2c_depth", C.c_size_t), ("depth", C.c_size_t), ("evalmod_log_scale", C.c_size_t),
                 ("double_angle", C.c_size_t), ("active_slots", C.c_size_t), ("slots", C.c_size_t),
                 ("scale", C.c_double)]
+
+
+class ServeConfig(C.Structure):
+    """wg_serve_config."""
+    _fields_ = [("workers", C.c_size_t), ("hbm_budget_bytes", C.c_size_t), ("eval_bytes", C.c_size_t),
+                ("max_blocks", C.c_size_t), ("batch_window_ms", C.c_double)]
+
+
+class ServeResult(C.Structure):
+    """wg_serve_result."""
+    _fields_ = [("status", C.c_int), ("block_offset", C.c_size_t), ("active_blocks", C.c_size_t),
+                ("batch_requests", C.c_size_t), ("batch_blocks", C.c_size_t), ("queue_ms", C.c_double),
+                ("latency_ms", C.c_double), ("out_level", C.c_size_t * 128), ("out_scale", C.c_double * 128)]
+
+
+WG_NOT_READY = 1
+
+
+class Server:
+    """Continuous-batching AES-CTR service (wg_serve_*): requests of an even number of counter
+    blocks are packed in arrival order into shared evaluations that `workers` streams run
+    concurrently.  The stages, key bits and coefficients must outlive the server."""
+
+    def __init__(self, ctx, params, s2c, s2c_x2, c2s, coeffs, packing_block_count, packed_segment_count, key_bits,
+                 key_scales, key_level, workers=2, hbm_budget_bytes=0, eval_bytes=0, max_blocks=0,
+                 batch_window_ms=0.0):
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        hs = lambda sts: np.ascontiguousarray([st.h.value for st in sts], dtype=np.uint64)
+        # kept alive with the server: the library holds their addresses
+        self._keep = (params, s2c, s2c_x2, c2s, key_bits)
+        self._kb, self._ka = arr([x[0] for x in key_bits]), arr([x[1] for x in key_bits])
+        self._ps, self._ps2, self._pc = hs(s2c), hs(s2c_x2), hs(c2s)
+        self._cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        self._ks = np.ascontiguousarray(key_scales, dtype=np.float64)
+        cfg = ServeConfig(workers, hbm_budget_bytes, eval_bytes, max_blocks, batch_window_ms)
+        h = C.c_void_p()
+        _check(lib().wg_serve_create(ctx.h, C.byref(params), self._ps.ctypes.data, len(self._ps), self._ps2.ctypes.data,
+                                     len(self._ps2), self._pc.ctypes.data, len(self._pc), self._cf.ctypes.data,
+                                     len(self._cf), packing_block_count, packed_segment_count, self._kb.ctypes.data,
+                                     self._ka.ctypes.data, self._ks.ctypes.data, key_level, C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._outs = {}
+
+    def submit(self, counters, ciphertexts, out_bits):
+        """Queue a request (bytes of `blocks` counter and ciphertext blocks, 128 (b, a) device
+        tensors for its output bits); returns its id."""
+        blocks = len(counters) // 16
+        ob = np.ascontiguousarray([_ptr(x[0]) for x in out_bits], dtype=np.uint64)
+        oa = np.ascontiguousarray([_ptr(x[1]) for x in out_bits], dtype=np.uint64)
+        rid = C.c_uint64()
+        _check(lib().wg_serve_submit(self.h, bytes(counters), bytes(ciphertexts), blocks, ob.ctypes.data,
+                                     oa.ctypes.data, C.byref(rid)))
+        self._outs[rid.value] = out_bits
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        """The finished request's result (dict), or None on timeout."""
+        r = ServeResult()
+        rc = lib().wg_serve_wait(self.h, rid, float(timeout), C.byref(r))
+        if rc == WG_NOT_READY:
+            return None
+        _check(rc)
+        self._outs.pop(rid, None)
+        if r.status != 0:
+            raise WalshGpuError(r.status, lib().wg_last_error().decode())
+        return {"block_offset": r.block_offset, "active_blocks": r.active_blocks,
+                "batch_requests": r.batch_requests, "batch_blocks": r.batch_blocks, "queue_ms": r.queue_ms,
+                "latency_ms": r.latency_ms, "levels": list(r.out_level), "scales": list(r.out_scale)}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wg_serve_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class BatchPlan:

@@ -36,6 +36,7 @@ extern "C" {
 #define WG_ERR_RUNTIME (-2)
 #define WG_ERR_CUDA (-3)
 #define WG_ERR_NOMEM (-4)
+#define WG_NOT_READY 1 /* wg_serve_wait: the request has not finished within the timeout */
 
 /* Switching-key kinds for wg_ctx_set_key / wg_keyswitch. */
 #define WG_KEY_RELIN 0       /* s^2 -> s           (relinearization_key_generation.cpp:130-199) */
@@ -280,6 +281,51 @@ int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const w
                      const uint8_t* counters, const uint8_t* ciphertexts, size_t active_blocks,
                      uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
                      void* stream);
+
+/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
+ * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
+ * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a
+ * stream, takes the queued requests in arrival order that fit into one evaluation's block slots
+ * (2 x packing_block_count by default; a request never splits), runs wg_aes_ctr_walsh on the
+ * concatenated blocks padded with zero blocks to the full 2 x packing_block_count slots (the
+ * walsh15 rotation keys serve that block count only) and copies the 128 output bit ciphertexts
+ * into every request's buffers.
+ * Evaluations of different workers run concurrently on the device; at most
+ * max(1, hbm_budget_bytes / eval_bytes) of them at once when both are set.  The stages, keys,
+ * coefficients and parameters passed to wg_serve_create must outlive the server.  Block b of an
+ * evaluation sits in slot b mod active_blocks, real part for b < active_blocks, imaginary part
+ * otherwise; a request's blocks are the evaluation blocks [block_offset, block_offset + blocks). */
+typedef struct wg_server wg_server;
+typedef struct wg_serve_config {
+    size_t workers;          /* concurrent evaluations (>= 1) */
+    size_t hbm_budget_bytes; /* device bytes the evaluations may take together (0: no limit) */
+    size_t eval_bytes;       /* device bytes one evaluation takes (admission estimate; 0: none) */
+    size_t max_blocks;       /* block slots per evaluation (0: 2 x packing_block_count) */
+    double batch_window_ms;  /* a free worker waits up to this long after the oldest queued request
+                                for more requests to fill its evaluation (0: start at once) */
+} wg_serve_config;
+typedef struct wg_serve_result {
+    int status;              /* WG_OK, or the error code of the request's evaluation */
+    size_t block_offset, active_blocks, batch_requests, batch_blocks;
+    double queue_ms, latency_ms; /* submission to evaluation start / to completion */
+    size_t out_level[128];
+    double out_scale[128];
+} wg_serve_result;
+int wg_serve_create(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
+                    const wg_lt_stage* const* s2c_x2, size_t ns2c_x2, const wg_lt_stage* const* c2s, size_t nc2s,
+                    const double* coeffs, size_t ncoeffs, size_t packing_block_count, size_t packed_segment_count,
+                    const uint64_t* const* key_b, const uint64_t* const* key_a, const double* key_scales,
+                    size_t key_level, const wg_serve_config* config, wg_server** out);
+/* Queue one request: `blocks` counter blocks and as many ciphertext blocks (16 bytes each,
+ * copied at submission); out_b / out_a: 128 device buffers of (depth + 1) N words each. */
+int wg_serve_submit(wg_server* server, const uint8_t* counters, const uint8_t* ciphertexts, size_t blocks,
+                    uint64_t* const* out_b, uint64_t* const* out_a, uint64_t* id);
+/* Wait up to timeout_s seconds (negative: no limit).  WG_OK with *result filled once the request
+ * has finished (its status in result->status; the message of a failed evaluation in
+ * wg_last_error()), WG_NOT_READY on timeout.  A finished request is collected once. */
+int wg_serve_wait(wg_server* server, uint64_t id, double timeout_s, wg_serve_result* result);
+/* Finishes every queued request, then stops the workers and frees the server. */
+void wg_serve_destroy(wg_server* server);
 
 /* Rotation that allocates no device memory (no counterpart in the reference, whose
  * operations all allocate host vectors).  For callers that cannot call cudaMalloc when they
