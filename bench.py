@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass")
     ap.add_argument("--no-ops", action="store_true", help="skip the batched-ops section")
     ap.add_argument("--no-ntt", action="store_true", help="skip the NTT / rotation primitives section")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-requests section")
+    ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not sample nvidia-smi clocks (for runs under a profiler, which wants the GPU to itself)")
     ap.add_argument("--no-aes", action="store_true",
@@ -553,6 +555,60 @@ class AesRun:
 
 
 # ------------------------------------------------------------------------------------------
+# served requests (config 5, walsh15 part): Poisson arrivals through the batching service
+# ------------------------------------------------------------------------------------------
+def serve_bench(wg, torch, aes, requests, seed, workers=2, window_ms=20.0, load=0.5):
+    """Requests of log-uniform size in [2, 1024] blocks (even) arrive as a seeded Poisson stream
+    at `load` x the measured full-slot capacity in requests/s, are served by the continuous-
+    batching service (wg_serve_*: `workers` concurrent evaluations, batching window) and
+    timed from submission to completion."""
+    rng = np.random.default_rng(seed)
+    full = aes.out_dev.shape[2]
+    srv = wg.Server(aes.ctx, aes.params, aes.s2c, aes.s2c_x2, aes.c2s, aes.coeffs, aes.pbc, aes.psc, aes.key_bits,
+                    aes.kscales, aes.kl, workers=workers, batch_window_ms=window_ms)
+    try:
+        mk = lambda: [(torch.empty(full, dtype=torch.int64, device="cuda"),
+                       torch.empty(full, dtype=torch.int64, device="cuda")) for _ in range(128)]
+        # warm-up: one full evaluation per worker, which also measures the full-slot capacity
+        t0 = time.perf_counter()
+        ids = [srv.submit(aes.block_bytes[0], aes.block_bytes[1], mk()) for _ in range(workers)]
+        for i in ids:
+            srv.wait(i)
+        warm_s = time.perf_counter() - t0
+        capacity_blocks = workers * aes.blocks / warm_s
+        sizes = [2 * int(round(np.exp(rng.uniform(np.log(1), np.log(512))))) for _ in range(requests)]
+        rate = load * capacity_blocks / float(np.mean(sizes))
+        gaps = rng.exponential(1.0 / rate, requests)
+        bufs = [mk() for _ in range(requests)]
+        ids = []
+        start = time.perf_counter()
+        t = start
+        for k, (n, gap) in enumerate(zip(sizes, gaps)):
+            t += gap
+            delay = t - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(srv.submit(aes.block_bytes[2][:16 * n], aes.block_bytes[3][:16 * n], bufs[k]))
+        res = [srv.wait(i) for i in ids]
+        wall = time.perf_counter() - start
+    finally:
+        srv.close()
+    lat = np.array([r["latency_ms"] for r in res])
+    queue = np.array([r["queue_ms"] for r in res])
+    evaluations = sum(1.0 / r["batch_requests"] for r in res)
+    return {"workload": f"{requests} requests, log-uniform 2..1024 blocks (even), Poisson arrivals at "
+                        f"{load} x full-slot capacity; walsh15 only (the xboot parameter sets are not built)",
+            "workers": workers, "batch_window_ms": window_ms, "requests": requests, "blocks": int(sum(sizes)),
+            "arrival_rate_per_s": rate, "offered_blocks_per_s": rate * float(np.mean(sizes)),
+            "wall_s": wall, "blocks_per_s": sum(sizes) / wall,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "mean": float(lat.mean()), "max": float(lat.max())},
+            "queue_ms": {"p50": float(np.percentile(queue, 50)), "p99": float(np.percentile(queue, 99))},
+            "evaluations": round(evaluations, 2), "requests_per_evaluation": requests / evaluations,
+            "full_slot_capacity_blocks_per_s": capacity_blocks}
+
+
+# ------------------------------------------------------------------------------------------
 # device arm
 # ------------------------------------------------------------------------------------------
 def main():
@@ -703,6 +759,7 @@ def main():
                                                  "reads and writes (intermediates included)"}}
 
     prim = None if args.no_ntt else ntt_bench(wg, torch, stream, timed, local, 20, hbm)
+    serving = None if args.no_serve else serve_bench(wg, torch, aes, args.serve_requests, args.seed + 17 + rank)
     ops, ops_ctx = None, None
     if not args.no_ops:
         ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local)
@@ -753,6 +810,7 @@ def main():
         "roofline": roofline,
         "kernels": kernels,
         "primitives": prim,
+        "serving": serving,
         "batched_ops": ops,
         "bsgs": bsgs,
         "cpu_baseline": cpu,
