@@ -81,6 +81,18 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(value, dist, device="cuda"):
+    """The maximum of a per-rank time over all ranks (every rank gets it); the value itself on
+    a single process."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_plan():
     with open(PLAN_PATH) as f:
         return json.load(f)
@@ -637,13 +649,6 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(ms):
-        if dist is None:
-            return ms
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     def timed(fn, k):
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -652,7 +657,7 @@ def main():
             fn()
         e1.record(stream)
         barrier()
-        return max_over_ranks(e0.elapsed_time(e1) / k)
+        return max_over_ranks(e0.elapsed_time(e1) / k, dist)
 
     plan = load_plan()
     if args.no_aes:
@@ -689,7 +694,7 @@ def main():
     launches = wg.launch_count() - launches0
     host1 = wg.host_stats()
     per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
-    ms = max_over_ranks(evs[0].elapsed_time(evs[-1]) / args.steps)
+    ms = max_over_ranks(evs[0].elapsed_time(evs[-1]) / args.steps, dist)
     value = aes.blocks * world / (ms / 1000.0)
     staged = (host1["stage_bytes"] - host0["stage_bytes"]) / args.steps
 
