@@ -540,8 +540,8 @@ private:
                 if (lm > 0 && (rcm < -(int)kMaxAbsCoeff || rcm > (int)kMaxAbsCoeff || icm < -(int)kMaxAbsCoeff ||
                                icm > (int)kMaxAbsCoeff))
                     throw std::runtime_error("ckks_walsh_sbox: missing low-sign multiple");
-                reinterpret_cast<int8_t*>(cf[0].cw[0][hm])[lm] = (int8_t)(lm ? rcm : 0);
-                reinterpret_cast<int8_t*>(cf[0].cw[1][hm])[lm] = (int8_t)(lm ? icm : 0);
+                reinterpret_cast<uint8_t*>(cf[0].cw[0][hm])[lm] = (uint8_t)((lm ? rcm : 0) + kWalshBias);
+                reinterpret_cast<uint8_t*>(cf[0].cw[1][hm])[lm] = (uint8_t)((lm ? icm : 0) + kWalshBias);
             }
             for (size_t l = 0; l < L; ++l) {
                 cf[0].c0[0][hm][l] = int_const(table_[rb][0][hm], scale, c_.q[l]);

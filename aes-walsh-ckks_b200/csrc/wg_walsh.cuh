@@ -21,14 +21,18 @@ namespace wg {
 constexpr int kWalshMasks = 16;     // nibble masks 0..15
 constexpr int kWalshLimbs = 16;     // limbs a combination can span
 
+constexpr int kWalshBias = 8;   // coefficients are stored as c + 8 in [0, 16] (|c| <= 8)
+
 struct WalshCoefs {
-    // [real|imag][hm]: the 16 int8 coefficients c[lm] packed little-endian (c[0] unused: the
-    // constant term is c0), one 16-byte vector per combination
+    // [real|imag][hm]: the 16 coefficients c[lm] stored as bytes c + kWalshBias, packed
+    // little-endian (c[0] unused: the constant term is c0), one 16-byte vector per combination
     uint32_t cw[2][kWalshMasks][4];
     uint64_t c0[2][kWalshMasks][kWalshLimbs];   // rounded c[.][hm][0] * scale mod q_limb
 };
 
-WG_HD int walsh_coef(const uint32_t* w, int t) { return (int)(int8_t)(uint8_t)(w[t >> 2] >> (8 * (t & 3))); }
+// the stored (biased) coefficient byte t, and the signed coefficient
+WG_HD uint32_t walsh_coef_biased(const uint32_t* w, int t) { return (w[t >> 2] >> (8 * (t & 3))) & 0xffu; }
+WG_HD int walsh_coef(const uint32_t* w, int t) { return (int)walsh_coef_biased(w, t) - kWalshBias; }
 
 WG_HD void walsh_coef_words(const WalshCoefs& cf, int r, int hm, uint32_t* w) {
 #if defined(__CUDA_ARCH__)
@@ -50,17 +54,19 @@ WG_HD int clz64(uint64_t x) {
 #endif
 }
 
-// canonical residue of sum_{lm=1..15} c[lm] s_lm for |c| <= 8 and canonical s
-WG_HD uint64_t walsh_small_sum(const uint64_t* s, const uint32_t* w, const Modulus& m) {
+// canonical residue of sum_{lm=1..15} c[lm] s_lm for |c| <= 8 and canonical s; s_sum is
+// sum_lm s_lm (used by the narrow path)
+WG_HD uint64_t walsh_small_sum(const uint64_t* s, uint64_t s_sum, const uint32_t* w, const Modulus& m) {
     if (m.q < (1ull << 55)) {
-        // |sum| < 120 * 2^55 < 2^62: exact in two's complement; adding q 2^sh in [2^62, 2^63)
-        // makes it a nonnegative value below 2^64
+        // sum (c + 8) s < 15 * 16 * 2^55 < 2^63 as an unsigned product of a small factor (two
+        // 32-bit multiply-adds per term); minus 8 sum s gives the exact signed sum, |sum| <
+        // 120 * 2^55 < 2^62, and adding q 2^sh in [2^62, 2^63) makes it a value in [0, 2^64)
         uint64_t acc = 0;
 #if defined(__CUDA_ARCH__)
 #pragma unroll
 #endif
-        for (int t = 1; t < kWalshMasks; ++t) acc += (uint64_t)((int64_t)walsh_coef(w, t) * (int64_t)s[t]);
-        return reduce64(acc + (m.q << (clz64(m.q) - 1)), m);
+        for (int t = 1; t < kWalshMasks; ++t) acc += (uint64_t)walsh_coef_biased(w, t) * s[t];
+        return reduce64(acc - (uint64_t)kWalshBias * s_sum + (m.q << (clz64(m.q) - 1)), m);
     }
     // wide moduli: 32-bit halves, R = ah 2^32 + al with |R| < 2^70; q 2^15 >= 2^70 lifts it
     int64_t al = 0, ah = 0;
@@ -77,13 +83,13 @@ WG_HD uint64_t walsh_small_sum(const uint64_t* s, const uint32_t* w, const Modul
 }
 
 // (c0r + sum cr s) + pt_i (c0i + sum ci s) for mask hm; the constants only on the b polynomial
-WG_HD uint64_t walsh_pair(const uint64_t* s, const WalshCoefs& cf, int hm, int limb, bool with_const, uint64_t pt_i,
-                          const Modulus& m) {
+WG_HD uint64_t walsh_pair(const uint64_t* s, uint64_t s_sum, const WalshCoefs& cf, int hm, int limb, bool with_const,
+                          uint64_t pt_i, const Modulus& m) {
     uint32_t wr[4], wi[4];
     walsh_coef_words(cf, 0, hm, wr);
     walsh_coef_words(cf, 1, hm, wi);
-    uint64_t r = walsh_small_sum(s, wr, m);
-    uint64_t im = walsh_small_sum(s, wi, m);
+    uint64_t r = walsh_small_sum(s, s_sum, wr, m);
+    uint64_t im = walsh_small_sum(s, s_sum, wi, m);
     if (with_const) {
         r = add_mod(cf.c0[0][hm][limb], r, m.q);
         im = add_mod(cf.c0[1][hm][limb], im, m.q);
@@ -94,31 +100,35 @@ WG_HD uint64_t walsh_pair(const uint64_t* s, const WalshCoefs& cf, int hm, int l
 // The low signs of one residue position (masks 1..15 at their index; index 0 is zero).
 struct WalshLow {
     uint64_t b[kWalshMasks], a[kWalshMasks];
+    uint64_t sb, sa;  // sums of the 15 signs (below 15 q < 2^64 for q < 2^60)
 };
 
 WG_HD void walsh_load_low(const uint64_t* low_b, const uint64_t* low_a, WalshLow& w) {
     w.b[0] = w.a[0] = 0;
+    w.sb = w.sa = 0;
 #if defined(__CUDA_ARCH__)
 #pragma unroll
 #endif
     for (int t = 1; t < kWalshMasks; ++t) {
         w.b[t] = low_b[t];
         w.a[t] = low_a[t];
+        w.sb += low_b[t];
+        w.sa += low_a[t];
     }
 }
 
 // the constant-term pair (hm = 0): (b, a)
 WG_HD void walsh_constant_pair(const WalshLow& w, const WalshCoefs& cf, int limb, uint64_t pt_i, const Modulus& m,
                                uint64_t* acc_b, uint64_t* acc_a) {
-    *acc_b = walsh_pair(w.b, cf, 0, limb, true, pt_i, m);
-    *acc_a = walsh_pair(w.a, cf, 0, limb, false, pt_i, m);
+    *acc_b = walsh_pair(w.b, w.sb, cf, 0, limb, true, pt_i, m);
+    *acc_a = walsh_pair(w.a, w.sa, cf, 0, limb, false, pt_i, m);
 }
 
 // product hm of the raw sum, added to (rb, ra, rc) (the first product initialises them)
 WG_HD void walsh_product(const WalshLow& w, const WalshCoefs& cf, int hm, int limb, uint64_t pt_i, const Modulus& m,
                          uint64_t yb, uint64_t ya, uint64_t* rb, uint64_t* ra, uint64_t* rc) {
-    const uint64_t lb = walsh_pair(w.b, cf, hm, limb, true, pt_i, m);
-    const uint64_t la = walsh_pair(w.a, cf, hm, limb, false, pt_i, m);
+    const uint64_t lb = walsh_pair(w.b, w.sb, cf, hm, limb, true, pt_i, m);
+    const uint64_t la = walsh_pair(w.a, w.sa, cf, hm, limb, false, pt_i, m);
     const uint64_t c2 = barrett_mul(la, ya, m);
     const uint64_t tmp = barrett_mul(lb, ya, m);
     const uint64_t b = barrett_mul(lb, yb, m);

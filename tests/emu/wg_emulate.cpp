@@ -219,7 +219,10 @@ void emu_walsh_products(uint64_t q, size_t n, const uint64_t* low_b, const uint6
                         uint64_t* out) {
     const Modulus m = emu_modulus(q);
     WalshCoefs cf{};
-    std::memcpy(cf.cw, coefs, sizeof(cf.cw));  // [2][16][16] int8, little-endian words
+    // [2][16][16] signed coefficients, stored biased as in the device table
+    uint8_t biased[2 * 16 * 16];
+    for (int i = 0; i < 2 * 16 * 16; ++i) biased[i] = (uint8_t)(coefs[i] + kWalshBias);
+    std::memcpy(cf.cw, biased, sizeof(cf.cw));
     for (int r = 0; r < 2; ++r)
         for (int hm = 0; hm < kWalshMasks; ++hm) cf.c0[r][hm][0] = c0[r * kWalshMasks + hm];
     for (size_t i = 0; i < n; ++i) {
