@@ -424,11 +424,10 @@ public:
             add_public(st, blocks, acb);
             return;
         }
-        std::vector<std::vector<uint64_t>> coeff(kBlockBits, std::vector<uint64_t>(L * N));
         std::vector<double> scale(kBlockBits);
         for (size_t bit = 0; bit < kBlockBits; ++bit) scale[bit] = static_cast<double>(st[bit].scale);
-        encode_bits_parallel(blocks, acb, scale, L, coeff);
-        std::vector<uint64_t*> pts = ops_.upload_plains(coeff, L);
+        std::vector<uint64_t*> pts = ops_.upload_plains_filled(
+            kBlockBits, L, [&](uint64_t* host) { encode_bits_parallel(blocks, acb, scale, L, host); });
         DeviceOps all(c_, kBlockBits, s_);
         std::vector<AddJob> jobs;
         for (size_t bit = 0; bit < kBlockBits; ++bit)
@@ -436,8 +435,9 @@ public:
         all.add_jobs(jobs);
     }
 
+    // the 128 bit patterns of `blocks`, encoded on host threads into out[bit][L][N]
     void encode_bits_parallel(const uint8_t* blocks, size_t acb, const std::vector<double>& scale, size_t L,
-                              std::vector<std::vector<uint64_t>>& coeff) {
+                              uint64_t* out) {
         const size_t nthreads = std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
         std::vector<std::thread> pool;
         std::vector<std::exception_ptr> errs(nthreads);
@@ -452,7 +452,8 @@ public:
                             re[s] = (double)((blocks[16 * s + bit / 8] >> (bit % 8)) & 1);
                             im[s] = (double)((blocks[16 * (acb + s) + bit / 8] >> (bit % 8)) & 1);
                         }
-                        host::encode_slots(c_.N, re.data(), im.data(), scale[bit], c_.q.data(), L, coeff[bit].data());
+                        host::encode_slots(c_.N, re.data(), im.data(), scale[bit], c_.q.data(), L,
+                                           out + bit * L * c_.N);
                     }
                 } catch (...) {
                     errs[w] = std::current_exception();
@@ -467,11 +468,10 @@ public:
     Bits initial_state_fast(const AesArgs& a) {
         WG_SPAN("aes.initial");
         const size_t level = a.key_level, L = level + 1, N = c_.N;
-        std::vector<std::vector<uint64_t>> coeff(kBlockBits, std::vector<uint64_t>(L * N));
         std::vector<double> scale(kBlockBits);
         for (size_t bit = 0; bit < kBlockBits; ++bit) scale[bit] = a.key_scales[bit];
-        encode_bits_parallel(a.counters, a.active_blocks, scale, L, coeff);
-        std::vector<uint64_t*> pts = ops_.upload_plains(coeff, L);
+        std::vector<uint64_t*> pts = ops_.upload_plains_filled(
+            kBlockBits, L, [&](uint64_t* host) { encode_bits_parallel(a.counters, a.active_blocks, scale, L, host); });
         Bits st(kBlockBits);
         std::vector<LinearJob> jobs;
         for (size_t bit = 0; bit < kBlockBits; ++bit) {

@@ -25,6 +25,12 @@ void stage_stats(uint64_t* calls, uint64_t* bytes, uint64_t* wait_ns) {
 }
 
 void* BatchBuffers::stage(const Context& c, const void* data, size_t bytes, cudaStream_t s) {
+    const size_t off = reserve(c, bytes, s);
+    std::memcpy(h_ring + off, data, bytes);
+    return commit(off, bytes, s);
+}
+
+size_t BatchBuffers::reserve(const Context& c, size_t bytes, cudaStream_t s) {
     g_stage_calls.fetch_add(1, std::memory_order_relaxed);
     g_stage_bytes.fetch_add(bytes, std::memory_order_relaxed);
     if (capturing(s))
@@ -63,7 +69,12 @@ void* BatchBuffers::stage(const Context& c, const void* data, size_t bytes, cuda
         spare_events.push_back(f.done);
         flights.pop_front();
     }
-    std::memcpy(h_ring + begin, data, bytes);
+    return begin;
+}
+
+void* BatchBuffers::commit(size_t begin, size_t bytes, cudaStream_t s) {
+    const size_t need = (std::max<size_t>(bytes, 1) + 255) & ~size_t{255};
+    const size_t end = begin + need;
     check_cuda(cudaMemcpyAsync(d_ring + begin, h_ring + begin, bytes, cudaMemcpyHostToDevice, s), "staging upload");
     cudaEvent_t ev = nullptr;
     if (!spare_events.empty()) {

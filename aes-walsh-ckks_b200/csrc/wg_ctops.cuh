@@ -477,13 +477,24 @@ public:
     // Many plaintexts at once: coeff[k] holds L limbs of plaintext k (coefficient form); one
     // staged upload and one NTT launch for all of them.
     std::vector<uint64_t*> upload_plains(const std::vector<std::vector<uint64_t>>& coeff, size_t L) {
+        const size_t words = L * c_.N;
+        return upload_plains_filled(coeff.size(), L, [&](uint64_t* host) {
+            for (size_t k = 0; k < coeff.size(); ++k) std::memcpy(host + k * words, coeff[k].data(), words * 8);
+        });
+    }
+
+    // `count` coefficient-form plaintexts of L limbs written by fill(host) straight into the
+    // pinned staging ring ([item][limb][N]), uploaded once and transformed in one NTT launch
+    template <class Fill>
+    std::vector<uint64_t*> upload_plains_filled(size_t count, size_t L, Fill&& fill) {
         const size_t N = c_.N, words = L * N;
-        std::vector<uint64_t> flat(coeff.size() * words);
-        for (size_t k = 0; k < coeff.size(); ++k) std::memcpy(flat.data() + k * words, coeff[k].data(), words * 8);
-        auto* staged = static_cast<uint64_t*>(c_.batch_buffers(s_).stage(c_, flat.data(), flat.size() * 8, s_));
-        std::vector<uint64_t*> out(coeff.size());
+        BatchBuffers& bb = c_.batch_buffers(s_);
+        const size_t off = bb.reserve(c_, count * words * 8, s_);
+        fill(reinterpret_cast<uint64_t*>(bb.h_ring + off));
+        auto* staged = static_cast<uint64_t*>(bb.commit(off, count * words * 8, s_));
+        std::vector<uint64_t*> out(count);
         std::vector<NttJob> jobs;
-        for (size_t k = 0; k < coeff.size(); ++k) {
+        for (size_t k = 0; k < count; ++k) {
             out[k] = buffer(L, false);
             for (size_t l = 0; l < L; ++l) jobs.push_back({staged + k * words + l * N, out[k] + l * N, (int)l, 0});
         }

@@ -112,6 +112,11 @@ struct BatchBuffers {
     // Copy `bytes` of host data into the ring and onto the device (stream order); returns the
     // device address, valid for kernels queued on `s` before the ring wraps back over it.
     void* stage(const Context& c, const void* data, size_t bytes, cudaStream_t s);
+    // The same in two steps, for callers that write the bytes in place: reserve() makes a
+    // region of `bytes` free (waiting for old uploads as stage() does) and returns its offset;
+    // the caller fills h_ring + offset; commit() uploads it and returns d_ring + offset.
+    size_t reserve(const Context& c, size_t bytes, cudaStream_t s);
+    void* commit(size_t offset, size_t bytes, cudaStream_t s);
     uint64_t* arena(const Context& c, size_t words, cudaStream_t s);
     void release();
 };
