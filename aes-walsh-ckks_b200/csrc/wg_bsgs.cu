@@ -47,7 +47,6 @@ struct LtStage {
 
 namespace {
 
-constexpr int kGiantBatch = 8;  // ciphertexts summed per thread in the giant-step kernel
 
 // Baby rotation `slot` of QP limb i for ciphertexts [c0, c0 + nc) of the batch: the key words
 // of a coefficient are loaded once and used for every ciphertext of the group.
@@ -67,16 +66,23 @@ struct CopyPair {
     const uint64_t* src;
 };
 
+constexpr int kGiantBatch = 8;  // ciphertexts per thread in the baby-step kernel (key words reused)
+
 struct TermRef {
     const uint64_t* diag;  // QP plaintext of the term (limb 0)
     int slot;              // baby slot
-    int pad;
+    int g;                 // giant step within its group
 };
 
+constexpr int kGiantGroup = 8;  // giant steps accumulated per thread
+
+// One ciphertext, one QP limb, a group of up to kGiantGroup giant steps: terms
+// [term0, term0 + nterms) of the term table, sorted by baby slot, so every baby-step value is
+// loaded once for all giant steps of the group.
 struct GiantJob {
     const uint64_t* babies;  // batch base: [C][slots][2][T][N]
     uint64_t* inner;         // batch base: [C][giants][2][T][N]
-    int term0, nterms, i, g, c0, nc;  // terms [term0, term0 + nterms) of the term table
+    int term0, nterms, i, g0, ng, c;
 };
 
 struct SubJob {
@@ -148,6 +154,9 @@ __global__ void __launch_bounds__(kT) kb_baby(const BabyJob* jobs, int n, const 
     }
 }
 
+// Giant-step inner sums: inner[c][g] = sum over the terms (g, slot) of diag x baby[c][slot], in
+// QP.  Montgomery products and modular additions of canonical residues, so the order of the
+// terms does not change the canonical sums.
 __global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, const TermRef* __restrict__ term_table,
                                                const Modulus* mods, int nq, int L, int T, int nslots, int ngiants,
                                                size_t N) {
@@ -159,26 +168,35 @@ __global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, cons
     const uint64_t q = m.q, qninv = m.qninv;
     const size_t limb = (size_t)i * N + x;
     const size_t slot_words = 2 * (size_t)T * N;
-    uint64_t acc_a[kGiantBatch], acc_b[kGiantBatch];
+    uint64_t acc_a[kGiantGroup], acc_b[kGiantGroup];
 #pragma unroll
-    for (int c = 0; c < kGiantBatch; ++c) acc_a[c] = acc_b[c] = 0;
+    for (int g = 0; g < kGiantGroup; ++g) acc_a[g] = acc_b[g] = 0;
+    const uint64_t* babies = j->babies + (size_t)j->c * nslots * slot_words;
+    int slot = -1;
+    uint64_t ba = 0, bb = 0;
     for (int t = 0; t < j->nterms; ++t) {
         const TermRef tr = term_table[j->term0 + t];
-        const uint64_t d = tr.diag[limb];
-#pragma unroll
-        for (int c = 0; c < kGiantBatch; ++c) {
-            if (c >= j->nc) break;
-            const uint64_t* bs = j->babies + ((size_t)(j->c0 + c) * nslots + tr.slot) * slot_words;
-            acc_a[c] = add_mod(acc_a[c], mont_mul(bs[limb], d, q, qninv), q);
-            acc_b[c] = add_mod(acc_b[c], mont_mul(bs[(size_t)T * N + limb], d, q, qninv), q);
+        if (tr.slot != slot) {
+            slot = tr.slot;
+            const uint64_t* bs = babies + (size_t)slot * slot_words;
+            ba = bs[limb];
+            bb = bs[(size_t)T * N + limb];
         }
+        const uint64_t d = tr.diag[limb];
+        const uint64_t pa = mont_mul(ba, d, q, qninv), pb = mont_mul(bb, d, q, qninv);
+#pragma unroll
+        for (int g = 0; g < kGiantGroup; ++g)
+            if (g == tr.g) {
+                acc_a[g] = add_mod(acc_a[g], pa, q);
+                acc_b[g] = add_mod(acc_b[g], pb, q);
+            }
     }
 #pragma unroll
-    for (int c = 0; c < kGiantBatch; ++c) {
-        if (c >= j->nc) break;
-        uint64_t* o = j->inner + ((size_t)(j->c0 + c) * ngiants + j->g) * slot_words;
-        o[limb] = acc_a[c];
-        o[(size_t)T * N + limb] = acc_b[c];
+    for (int g = 0; g < kGiantGroup; ++g) {
+        if (g >= j->ng) break;
+        uint64_t* o = j->inner + ((size_t)j->c * ngiants + j->g0 + g) * slot_words;
+        o[limb] = acc_a[g];
+        o[(size_t)T * N + limb] = acc_b[g];
     }
 }
 
@@ -364,15 +382,18 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     std::vector<TermRef> terms;
     std::vector<GiantJob> giant_jobs;
     const size_t qp_words = T * N;
-    for (size_t gk = 0; gk < ng; ++gk) {
-        const auto& tl = terms_by_giant[giants[gk]];
+    for (size_t g0 = 0; g0 < ng; g0 += kGiantGroup) {
+        const size_t gn = std::min<size_t>(kGiantGroup, ng - g0);
+        std::vector<TermRef> group;
+        for (size_t gk = g0; gk < g0 + gn; ++gk)
+            for (size_t term : terms_by_giant[giants[gk]])
+                group.push_back({st.d_diag + term * qp_words, slot_of[st.indices[term] % st.baby], (int)(gk - g0)});
+        std::stable_sort(group.begin(), group.end(), [](const TermRef& x, const TermRef& y) { return x.slot < y.slot; });
         const size_t off = terms.size();
-        for (size_t term : tl)
-            terms.push_back({st.d_diag + term * qp_words, slot_of[st.indices[term] % st.baby], 0});
-        for (size_t c0 = 0; c0 < count; c0 += kGiantBatch)
+        terms.insert(terms.end(), group.begin(), group.end());
+        for (size_t ci = 0; ci < count; ++ci)
             for (size_t i = 0; i < T; ++i)
-                giant_jobs.push_back({babybuf, inner, (int)off, (int)tl.size(), (int)i, (int)gk, (int)c0,
-                                      (int)std::min<size_t>(kGiantBatch, count - c0)});
+                giant_jobs.push_back({babybuf, inner, (int)off, (int)group.size(), (int)i, (int)g0, (int)gn, (int)ci});
     }
     // 4. giants >= 1: single ModDown of inner a, then QP key switch from that key term
     std::vector<NttJob> intt_pg, ntt_cs, intt_kt, ntt_dig2;

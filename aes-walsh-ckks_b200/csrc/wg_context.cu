@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "wg_internal.hpp"
+#include "wg_ring.hpp"
 #include "wg_tables.hpp"
 
 namespace wg {
@@ -54,20 +55,21 @@ size_t BatchBuffers::reserve(const Context& c, size_t bytes, cudaStream_t s) {
         ring_bytes = cap;
         head = 0;
     }
-    if (head + need > ring_bytes) head = 0;
-    const size_t begin = head, end = head + need;
-    // wait for the uploads whose host bytes this region still holds
-    while (!flights.empty()) {
-        const Flight& f = flights.front();
-        const bool overlap = f.begin < end && begin < f.end;
-        if (!overlap) break;
+    // wait for the uploads whose host bytes this region still holds (ring_place: the newest
+    // overlapping one, which completes every older one too; all of them are then released)
+    size_t wait = 0;
+    const size_t begin = ring_place(head, ring_bytes, need, flights, &wait);
+    head = begin;
+    if (wait > 0) {
         const auto t0 = std::chrono::steady_clock::now();
-        check_cuda(cudaEventSynchronize(f.done), "staging ring wait");
+        check_cuda(cudaEventSynchronize(flights[wait - 1].done), "staging ring wait");
         g_stage_wait_ns.fetch_add(
             (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count(),
             std::memory_order_relaxed);
-        spare_events.push_back(f.done);
-        flights.pop_front();
+        for (size_t k = 0; k < wait; ++k) {
+            spare_events.push_back(flights.front().done);
+            flights.pop_front();
+        }
     }
     return begin;
 }

@@ -14,6 +14,9 @@
 #include "wg_ntt.cuh"
 #include "wg_tables.hpp"
 #include "wg_walsh.cuh"
+#include "wg_ring.hpp"
+#include <deque>
+#include <random>
 
 using namespace wg;
 
@@ -233,6 +236,35 @@ void emu_walsh_products(uint64_t q, size_t n, const uint64_t* low_b, const uint6
         for (int hm = 1; hm < kWalshMasks; ++hm)
             walsh_product(w, cf, hm, 0, pt_i[i], m, high_b[i * 16 + hm], high_a[i * 16 + hm], o + 2, o + 3, o + 4);
     }
+}
+
+// The staging ring's placement (wg_ring.hpp) over `steps` seeded uploads of mixed sizes (1 in 100
+// a large one), with no upload ever completing on its own (the host arbitrarily far ahead of the
+// device): returns how many regions overlapped an upload the placement did not wait for.
+size_t emu_ring_violations(uint64_t seed, size_t steps) {
+    struct F {
+        size_t begin, end;
+    };
+    std::mt19937_64 g(seed);
+    std::deque<F> flights;
+    size_t ring = 0, head = 0, bad = 0;
+    for (size_t i = 0; i < steps; ++i) {
+        const size_t bytes = (g() % 100 == 0) ? (size_t{100} << 20) : (size_t)(1024 + g() % (128 * 1024));
+        const size_t need = (bytes + 255) & ~size_t{255};
+        if (need > ring) {  // growth: everything in flight completes first
+            flights.clear();
+            ring = std::max<size_t>(2 * need, size_t{64} << 20);
+            head = 0;
+        }
+        size_t wait = 0;
+        const size_t begin = wg::ring_place(head, ring, need, flights, &wait);
+        for (size_t k = 0; k < wait; ++k) flights.pop_front();
+        for (const F& f : flights)
+            if (f.begin < begin + need && begin < f.end) ++bad;
+        flights.push_back({begin, begin + need});
+        head = begin + need;
+    }
+    return bad;
 }
 
 }  // extern "C"

@@ -175,3 +175,13 @@ def test_walsh_products_exact(emu, q):
         want = _walsh_model(q, [int(x) for x in lb[i]], [int(x) for x in la[i]], [int(x) for x in hb[i]],
                             [int(x) for x in ha[i]], int(pt[i]), coefs, c0)
         assert [int(x) for x in out[i]] == want, i
+
+
+def test_staging_ring_never_overwrites_pending_uploads(emu):
+    """The staging ring's placement, with every upload still pending (the host far ahead of the
+    device, as in a long AES-CTR call): no region handed out may overlap an upload it did not wait
+    for, also after early wraps put old uploads in front of newer ones."""
+    emu.emu_ring_violations.restype = C.c_size_t
+    emu.emu_ring_violations.argtypes = [C.c_uint64, C.c_size_t]
+    for seed in (1, 2, 3):
+        assert emu.emu_ring_violations(seed, 20000) == 0
