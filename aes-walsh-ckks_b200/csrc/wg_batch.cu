@@ -35,7 +35,7 @@ struct KsPlan {
     int n_modup;
     const NttJob* ntt_digits;
     int n_ntt_digits;
-    const MacJob* mac;
+    const MacGroupJob* mac;
     int n_mac;
     const NttJob* intt_p;
     int n_intt_p;
@@ -60,11 +60,42 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
     const size_t N = c.N, K = c.np, nq = c.nq;
     std::vector<NttJob> intt_in, ntt_digits, intt_p, ntt_contrib;
     std::vector<ModUpJob> modup;
-    std::vector<MacJob> mac;
+    std::vector<MacGroupJob> mac;
     std::vector<ModDownJob> moddown;
     std::vector<CombineJob> combine;
     std::vector<GatherJob> gather;
     KsPlan p{};
+    // MAC groups: consecutive switches with the same key, level and digit layout (up to
+    // kMacGroup), one job per QP limb; [group_begin, it) is the open group
+    size_t group_begin = 0;
+    std::vector<uint64_t*> group_digits, group_acc;
+    auto close_group = [&](size_t end) {
+        if (end == group_begin) return;
+        const KsItem& g = items[group_begin];
+        const size_t L = g.level + 1, T = L + K, B = c.parts_at(g.level);
+        for (size_t i = 0; i < T; ++i) {
+            MacGroupJob jb{};
+            jb.key = g.key->d_data;
+            jb.part_stride = T * N;
+            jb.L = (int)L;
+            jb.K = (int)K;
+            jb.parts = (int)B;
+            jb.alpha = (int)c.alpha;
+            jb.key_level = (int)g.key->key_level;
+            jb.i = (int)i;
+            jb.n = (int)(end - group_begin);
+            for (size_t k = group_begin; k < end; ++k) {
+                jb.key_term[k - group_begin] = items[k].key_term;
+                jb.digits[k - group_begin] = group_digits[k - group_begin];
+                jb.acc[k - group_begin] = group_acc[k - group_begin];
+            }
+            mac.push_back(jb);
+        }
+        p.mac_bytes += 8.0 * N * T * (2.0 * B + (double)(end - group_begin) * (B + 2.0));
+        group_begin = end;
+        group_digits.clear();
+        group_acc.clear();
+    };
     for (size_t it = 0; it < n; ++it) {
         const KsItem& x = items[it];
         const size_t level = x.level, L = level + 1, T = L + K, B = c.parts_at(level);
@@ -88,10 +119,12 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
                 ntt_digits.push_back({ptr, ptr, (int)(l < L ? l : nq + (l - L)), 0});
             }
         }
-        for (size_t i = 0; i < T; ++i)
-            mac.push_back({x.key->d_data, x.key_term, digits, acc, T * N, (int)L, (int)K, (int)B, (int)c.alpha,
-                           (int)x.key->key_level, (int)i});
-        p.mac_bytes += 8.0 * N * T * (3.0 * B + 2.0);
+        if (it > group_begin) {
+            const KsItem& g = items[group_begin];
+            if (it - group_begin == (size_t)kMacGroup || g.key != x.key || g.level != x.level) close_group(it);
+        }
+        group_digits.push_back(digits);
+        group_acc.push_back(acc);
         for (int poly = 0; poly < 2; ++poly)
             for (size_t pi = 0; pi < K; ++pi) {
                 uint64_t* ptr = acc + (poly * T + L + pi) * N;
@@ -116,6 +149,7 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
         }
         p.combine_bytes += 8.0 * N * L * (x.b_add + x.a_add + 6.0) + (gal ? 8.0 * N * L * 4.0 : 0.0);
     }
+    close_group(n);
     p.intt_in = t.add(intt_in);
     p.n_intt_in = (int)intt_in.size();
     p.modup = t.add(modup);
@@ -147,7 +181,7 @@ static void run_keyswitch(const Context& c, const KsPlan& p, const JobTable& t, 
     ntt_jobs(c, t.at(p.ntt_digits), p.n_ntt_digits, true, s);
     {
         Probe probe(kClsKeyMac, p.mac_bytes, s);
-        kb_mac<<<grid_for(c, p.n_mac), kT, 0, s>>>(t.at(p.mac), p.n_mac, c.d_mod, (int)c.nq, N);
+        kb_mac_group<<<grid_for(c, p.n_mac), kT, 0, s>>>(t.at(p.mac), p.n_mac, c.d_mod, (int)c.nq, N);
     }
     ntt_jobs(c, t.at(p.intt_p), p.n_intt_p, false, s);
     {

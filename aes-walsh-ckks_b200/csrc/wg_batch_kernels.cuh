@@ -26,6 +26,17 @@ struct MacJob {
     size_t part_stride;
     int L, K, parts, alpha, key_level, i;
 };
+// Key inner product of up to kMacGroup switches that share the key, the level and the digit
+// layout, for one QP limb: the key words of a coefficient are loaded once for all of them.
+constexpr int kMacGroup = 8;
+struct MacGroupJob {
+    const uint64_t* key;
+    const uint64_t* key_term[kMacGroup];
+    const uint64_t* digits[kMacGroup];
+    uint64_t* acc[kMacGroup];
+    size_t part_stride;
+    int L, K, parts, alpha, key_level, i, n, pad;
+};
 struct ModDownJob {
     const uint64_t* src_p;  // P limbs of one accumulator (coefficient form)
     uint64_t* out;          // L contribution limbs
@@ -91,6 +102,44 @@ __global__ void __launch_bounds__(kT) kb_mac(const MacJob* jobs, int n, const Mo
     const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
     mac_coeff(mods, nq, j->L, j->K, j->parts, j->alpha, j->key, j->key_level, j->key_term, j->digits, j->part_stride,
               j->acc, N, j->i, coeff);
+}
+
+// acc_{a,b}[i] = sum_parts REDC(digit_part[i] * key_part_{a,b}[i]) for every switch of the group,
+// parts accumulated in order as in mac_accumulate (wg_keyswitch.cuh).
+__global__ void __launch_bounds__(kT) kb_mac_group(const MacGroupJob* jobs, int n, const Modulus* mods, int nq,
+                                                   size_t N) {
+    const MacGroupJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
+    const int i = j->i, L = j->L, K = j->K, T = L + K;
+    const bool is_p = i >= L;
+    const Modulus& m = mods[is_p ? nq + (i - L) : i];
+    const uint64_t q = m.q, qninv = m.qninv;
+    const size_t key_limbs = (size_t)j->key_level + 1 + K;
+    const size_t klimb = is_p ? (size_t)j->key_level + 1 + (i - L) : (size_t)i;
+    const size_t at = (size_t)i * N + coeff;
+    uint64_t acc_a[kMacGroup], acc_b[kMacGroup];
+#pragma unroll
+    for (int c = 0; c < kMacGroup; ++c) acc_a[c] = acc_b[c] = 0;
+    for (int p = 0; p < j->parts; ++p) {
+        const int s0 = p * j->alpha, s1 = s0 + j->alpha < L ? s0 + j->alpha : L;
+        const bool own = !is_p && i >= s0 && i < s1;
+        const uint64_t ka = j->key[(((size_t)p * 2 + 0) * key_limbs + klimb) * N + coeff];
+        const uint64_t kb = j->key[(((size_t)p * 2 + 1) * key_limbs + klimb) * N + coeff];
+#pragma unroll
+        for (int c = 0; c < kMacGroup; ++c) {
+            if (c >= j->n) break;
+            const uint64_t d = own ? j->key_term[c][at] : j->digits[c][p * j->part_stride + at];
+            acc_a[c] = add_mod(acc_a[c], mont_mul(d, ka, q, qninv), q);
+            acc_b[c] = add_mod(acc_b[c], mont_mul(d, kb, q, qninv), q);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kMacGroup; ++c) {
+        if (c >= j->n) break;
+        j->acc[c][at] = acc_a[c];
+        j->acc[c][(size_t)T * N + at] = acc_b[c];
+    }
 }
 
 __global__ void __launch_bounds__(kT) kb_moddown(const ModDownJob* jobs, int n, const Modulus* mods, int nq, int K,

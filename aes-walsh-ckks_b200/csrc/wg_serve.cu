@@ -2,7 +2,7 @@
 //
 // Each worker thread owns a non-blocking stream and one evaluation's output buffers.  A free
 // worker waits until requests are queued and fewer evaluations run than the memory budget
-// admits, takes the queued requests in arrival order while their blocks fit into one
+// admits, takes every queued request, in arrival order, whose blocks still fit into one
 // evaluation (a request never splits), concatenates their counter and ciphertext blocks and pads
 // them with zero blocks to the evaluation's full 2 x packing-block-count slots (block b: real slot
 // b for b < packing blocks, imaginary slot b - packing blocks otherwise; the circuit's final
@@ -67,15 +67,18 @@ Server::~Server() {
     release_workers();
 }
 
-// the queued requests that the next evaluation would take already fill it (the next one in
-// arrival order does not fit, or the slots are used up)
+// the queued requests already fill the next evaluation (one of them no longer fits beside the
+// others, or the slots are used up)
 bool Server::head_batch_full() const {
     size_t blocks = 0;
+    bool skipped = false;
     for (const auto& r : queue_) {
-        if (blocks + r.blocks > max_blocks_) return true;
-        blocks += r.blocks;
+        if (blocks + r.blocks <= max_blocks_)
+            blocks += r.blocks;
+        else
+            skipped = true;
     }
-    return blocks == max_blocks_;
+    return skipped || blocks == max_blocks_;
 }
 
 size_t Server::admitted() const {
@@ -150,10 +153,16 @@ void Server::worker(size_t w) {
                 cv_.wait_until(lk, deadline, [&] { return stop_ || queue_.empty() || head_batch_full(); });
                 if (queue_.empty() || running_ >= admitted()) continue;  // another worker took them
             }
-            while (!queue_.empty() && blocks + queue_.front().blocks <= max_blocks_) {
-                blocks += queue_.front().blocks;
-                batch.push_back(std::move(queue_.front()));
-                queue_.pop_front();
+            // every queued request that still fits, in arrival order (the oldest always fits an
+            // empty evaluation, so no request waits behind later ones for ever)
+            for (auto it = queue_.begin(); it != queue_.end() && blocks < max_blocks_;) {
+                if (blocks + it->blocks <= max_blocks_) {
+                    blocks += it->blocks;
+                    batch.push_back(std::move(*it));
+                    it = queue_.erase(it);
+                } else {
+                    ++it;
+                }
             }
             ++running_;
         }

@@ -2,7 +2,7 @@
 //
 // No counterpart in the reference, whose benchmark runs one AES-CTR evaluation at a time
 // (bench/aes_bench.cpp).  Requests of 2..1024 counter blocks queue up; each free worker takes
-// the waiting requests in arrival order that fit into one evaluation's 1024 block slots, runs
+// every waiting request, in arrival order, that still fits into one evaluation's 1024 block slots, runs
 // the homomorphic AES-CTR on its own stream and hands every request its output bit
 // ciphertexts.  Workers run evaluations concurrently (their kernels interleave on the device)
 // as far as the device-memory budget allows.

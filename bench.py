@@ -569,11 +569,11 @@ class AesRun:
 # ------------------------------------------------------------------------------------------
 # served requests (config 5, walsh15 part): Poisson arrivals through the batching service
 # ------------------------------------------------------------------------------------------
-def serve_bench(wg, torch, aes, requests, seed, workers=2, window_ms=20.0, load=0.5):
+def serve_bench(wg, torch, aes, requests, seed, capacity_blocks, workers=2, window_ms=20.0, load=0.5):
     """Requests of log-uniform size in [2, 1024] blocks (even) arrive as a seeded Poisson stream
-    at `load` x the measured full-slot capacity in requests/s, are served by the continuous-
-    batching service (wg_serve_*: `workers` concurrent evaluations, batching window) and
-    timed from submission to completion."""
+    at `load` x the full-slot capacity (the headline's measured blocks/s) in requests/s, are
+    served by the continuous-batching service (wg_serve_*: `workers` concurrent evaluations,
+    batching window) and timed from submission to completion."""
     rng = np.random.default_rng(seed)
     full = aes.out_dev.shape[2]
     srv = wg.Server(aes.ctx, aes.params, aes.s2c, aes.s2c_x2, aes.c2s, aes.coeffs, aes.pbc, aes.psc, aes.key_bits,
@@ -581,13 +581,10 @@ def serve_bench(wg, torch, aes, requests, seed, workers=2, window_ms=20.0, load=
     try:
         mk = lambda: [(torch.empty(full, dtype=torch.int64, device="cuda"),
                        torch.empty(full, dtype=torch.int64, device="cuda")) for _ in range(128)]
-        # warm-up: one full evaluation per worker, which also measures the full-slot capacity
-        t0 = time.perf_counter()
+        # warm-up: one full evaluation per worker (worker streams, their scratch and caches)
         ids = [srv.submit(aes.block_bytes[0], aes.block_bytes[1], mk()) for _ in range(workers)]
         for i in ids:
             srv.wait(i)
-        warm_s = time.perf_counter() - t0
-        capacity_blocks = workers * aes.blocks / warm_s
         sizes = [2 * int(round(np.exp(rng.uniform(np.log(1), np.log(512))))) for _ in range(requests)]
         rate = load * capacity_blocks / float(np.mean(sizes))
         gaps = rng.exponential(1.0 / rate, requests)
@@ -764,7 +761,8 @@ def main():
                                                  "reads and writes (intermediates included)"}}
 
     prim = None if args.no_ntt else ntt_bench(wg, torch, stream, timed, local, 20, hbm)
-    serving = None if args.no_serve else serve_bench(wg, torch, aes, args.serve_requests, args.seed + 17 + rank)
+    serving = None if args.no_serve else serve_bench(wg, torch, aes, args.serve_requests, args.seed + 17 + rank,
+                                                     aes.blocks / (ms / 1000.0))
     ops, ops_ctx = None, None
     if not args.no_ops:
         ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local)

@@ -285,8 +285,8 @@ int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const w
 /* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a
- * stream, takes the queued requests in arrival order that fit into one evaluation's block slots
- * (2 x packing_block_count by default; a request never splits), runs wg_aes_ctr_walsh on the
+ * stream, takes every queued request, in arrival order, that still fits into one evaluation's
+ * block slots (2 x packing_block_count by default; a request never splits), runs wg_aes_ctr_walsh on the
  * concatenated blocks padded with zero blocks to the full 2 x packing_block_count slots (the
  * walsh15 rotation keys serve that block count only) and copies the 128 output bit ciphertexts
  * into every request's buffers.
