@@ -3,6 +3,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
+#include <array>
 #include <vector>
 
 #include "wg_internal.hpp"
@@ -110,6 +111,16 @@ void bootstrap_evalmod(Context& c, const BootstrapParams& p, const S2cPlan* s2c,
 
 // Mask-packed Walsh S-box over `count` instances (wg_sbox.cu); in/out are bit-major arrays of
 // 8 * count ciphertext pointers.
+// The AES S-box from the FIPS-197 definition (GF(2^8) inverse, then the affine map).
+std::array<uint8_t, 256> aes_sbox_table();
+
+// The XBOOT S-box (wg_xboot.cu) on `count` instances of 8 bit ciphertexts ([bit][instance]) at
+// `level` and `scale`; outputs at out_level[bit] and out_scale[bit].
+void xboot_sbox(Context& c, size_t count, size_t level, double scale, uint64_t* const* in_b, uint64_t* const* in_a,
+                uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale, cudaStream_t s);
+// Integer coefficients of each S-box output bit over the 256 monomials of the input bits.
+std::array<std::array<int64_t, 256>, 8> xboot_sbox_coefficients();
+
 void walsh_sbox(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
                 size_t nc2s, const double* coeffs, size_t ncoeffs, size_t block_count, size_t count, size_t level,
                 double scale, uint64_t* const* in_b, uint64_t* const* in_a, uint64_t* const* out_b,

@@ -564,6 +564,29 @@ int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const w
     });
 }
 
+int wg_xboot_sbox(wg_context* ctx, size_t count, size_t level, double scale, uint64_t* const* in_b,
+                  uint64_t* const* in_a, uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level,
+                  double* out_scale, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(out_level, "ckks_aes");
+        check_ptr(out_scale, "ckks_aes");
+        if (level >= c.nq) wg::fail(wg::kInvalid, "ckks_aes: invalid XBOOT S-box input level");
+        check_cts(c, 8 * count, in_b, in_a, "ckks_aes");
+        check_cts(c, 8 * count, out_b, out_a, "ckks_aes");
+        wg::xboot_sbox(c, count, level, scale, in_b, in_a, out_b, out_a, out_level, out_scale, S(stream));
+    });
+}
+
+int wg_xboot_sbox_coefficients(int64_t* out) {
+    return guard([&] {
+        check_ptr(out, "ckks_aes");
+        const auto cf = wg::xboot_sbox_coefficients();
+        for (size_t b = 0; b < 8; ++b)
+            for (size_t m = 0; m < 256; ++m) out[b * 256 + m] = cf[b][m];
+    });
+}
+
 struct wg_server {
     wg::Server* s;
 };

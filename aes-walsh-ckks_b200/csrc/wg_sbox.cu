@@ -655,6 +655,8 @@ private:
 
 }  // namespace
 
+std::array<uint8_t, 256> aes_sbox_table() { return aes_sbox(); }
+
 void walsh_sbox(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
                 size_t nc2s, const double* coeffs, size_t ncoeffs, size_t block_count, size_t count, size_t level,
                 double scale, uint64_t* const* in_b, uint64_t* const* in_a, uint64_t* const* out_b,

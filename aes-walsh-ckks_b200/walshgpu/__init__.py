@@ -92,6 +92,8 @@ def lib() -> C.CDLL:
         L.wg_aes_ctr_walsh.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, C.c_char_p,
                                        C.c_char_p, sz, vp, vp, vp, vp, vp]
         L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
+        L.wg_xboot_sbox.argtypes = [vp, sz, sz, C.c_double, vp, vp, vp, vp, vp, vp, vp]
+        L.wg_xboot_sbox_coefficients.argtypes = [vp]
         L.wg_serve_create.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, vp,
                                       C.POINTER(vp)]
         L.wg_serve_submit.argtypes = [vp, C.c_char_p, C.c_char_p, sz, vp, vp, C.POINTER(C.c_uint64)]
@@ -159,6 +161,13 @@ def launch_count(kernel_class=-1) -> int:
 def probe_begin(kernel_class, max_launches=60000):
     """Start CUDA-event timing of every launch of one kernel class."""
     _check(lib().wg_probe_begin(kernel_class, max_launches))
+
+
+def xboot_sbox_coefficients():
+    """[8][256] integer coefficients of the S-box output bits over the input-bit monomials."""
+    out = np.zeros(8 * 256, np.int64)
+    _check(lib().wg_xboot_sbox_coefficients(out.ctypes.data))
+    return out.reshape(8, 256)
 
 
 def host_stats() -> dict:
@@ -519,6 +528,19 @@ class Context:
                                    cf.ctypes.data, len(cf), block_count, count, level, float(scale), ib.ctypes.data,
                                    ia.ctypes.data, ob.ctypes.data, oa.ctypes.data, lv.ctypes.data, sc.ctypes.data,
                                    _stream(stream)))
+        return [int(x) for x in lv], [float(x) for x in sc]
+
+    def xboot_sbox(self, level, scale, bits, outs):
+        """The XBOOT S-box on instances of 8 bit ciphertexts: bits[i][k] = (b, a) device tensors
+        at `level`; outs[i][k] receive the outputs.  Returns (levels, scales) of the 8 bits."""
+        count = len(bits)
+        flat = lambda sel, xs: np.ascontiguousarray([_ptr(xs[i][k][sel]) for k in range(8) for i in range(count)],
+                                                    dtype=np.uint64)
+        ib, ia, ob, oa = flat(0, bits), flat(1, bits), flat(0, outs), flat(1, outs)
+        lv = np.zeros(8, np.uintp)
+        sc = np.zeros(8, np.float64)
+        _check(lib().wg_xboot_sbox(self.h, count, level, float(scale), ib.ctypes.data, ia.ctypes.data, ob.ctypes.data,
+                                   oa.ctypes.data, lv.ctypes.data, sc.ctypes.data, _stream(None)))
         return [int(x) for x in lv], [float(x) for x in sc]
 
     def aes_ctr_walsh(self, params, s2c, s2c_x2, c2s, coeffs, packing_block_count, packed_segment_count, key_bits,

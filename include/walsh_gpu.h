@@ -282,6 +282,19 @@ int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const w
                      uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
                      void* stream);
 
+/* The XBOOT AES S-box on lazy bits (ckks_aes_xboot_sbox_impl,
+ * src/ckks/operations/circuits/aes/ckks_aes_ctr.cpp:280-336, with its monomial tree :185-256
+ * and coefficients :258-278) for `count` instances: in_b / in_a hold 8 x count ciphertexts
+ * ([bit][instance], (level + 1) N words each) at `level` and `scale`; out_b / out_a receive the
+ * 8 output bits (room for level + 1 limbs each) at out_level[bit], out_scale[bit] (three levels
+ * lower, same scale).  Needs the relinearisation key; level >= 3. */
+int wg_xboot_sbox(wg_context* ctx, size_t count, size_t level, double scale, uint64_t* const* in_b,
+                  uint64_t* const* in_a, uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level,
+                  double* out_scale, void* stream);
+/* The integer coefficients of each S-box output bit over the monomials of the 8 input bits:
+ * out[bit * 256 + mask] (mask 0 = constant term). */
+int wg_xboot_sbox_coefficients(int64_t* out);
+
 /* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a

@@ -417,6 +417,52 @@ class RefCtx:
         return out.reshape(len(rots), 2, n)
 
 
+class RefXboot(RefCtx):
+    """The reference's XBOOT chain at N = 2^15 (AESXBoot15Config without bootstrapping: 17 Q limbs,
+    5 P limbs, dnum 5) and the XBOOT S-box restated on its public operations
+    (ref_xboot_sbox, following src/ckks/operations/circuits/aes/ckks_aes_ctr.cpp:160-336)."""
+
+    def __init__(self):
+        R = ref()
+        R.ref_xboot15_create.restype = C.c_void_p
+        R.ref_xboot_sbox.argtypes = [C.c_void_p, C.c_size_t, C.c_double, u64p, u64p, szp, f64p]
+        R.ref_xboot_sbox_coefficients.argtypes = [np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+        self.h = R.ref_xboot15_create()
+        if not self.h:
+            raise RuntimeError("ref_xboot15_create: " + R.ref_last_error().decode())
+        self.N = 1 << 15
+        nq, np_ = C.c_size_t(), C.c_size_t()
+        _check(R.ref_ctx_moduli(self.h, np.zeros(64, np.uint64), C.byref(nq), np.zeros(64, np.uint64),
+                                C.byref(np_)), "ref_ctx_moduli")
+        self.q = np.zeros(nq.value, np.uint64)
+        self.p = np.zeros(np_.value, np.uint64)
+        _check(R.ref_ctx_moduli(self.h, self.q, C.byref(nq), self.p, C.byref(np_)), "ref_ctx_moduli")
+        self.dnum = 5
+
+    def sbox(self, level, scale, bits):
+        """The XBOOT S-box on 8 bit ciphertexts [(b, a)] at `level`: [(b, a, level, scale)] x 8."""
+        n = (level + 1) * self.N
+        flat = np.concatenate([np.concatenate([np.asarray(b[:n], np.uint64), np.asarray(a[:n], np.uint64)])
+                               for b, a in bits])
+        out = np.zeros(16 * len(self.q) * self.N, np.uint64)
+        lv = np.zeros(8, np.uintp)
+        sc = np.zeros(8, np.float64)
+        _check(ref().ref_xboot_sbox(self.h, level, float(scale), flat, out, lv, sc), "ref_xboot_sbox")
+        res, off = [], 0
+        for k in range(8):
+            m = (int(lv[k]) + 1) * self.N
+            res.append((out[off:off + m].copy(), out[off + m:off + 2 * m].copy(), int(lv[k]), float(sc[k])))
+            off += 2 * m
+        return res
+
+    @staticmethod
+    def coefficients():
+        out = np.zeros(8 * 256, np.int64)
+        ref().ref_xboot_sbox_coefficients.argtypes = [np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+        _check(ref().ref_xboot_sbox_coefficients(out), "ref_xboot_sbox_coefficients")
+        return out.reshape(8, 256)
+
+
 class RefPlans:
     """The reference's walsh15 S2C / C2S plans and rotation keys (ref_walsh15_plans_create)."""
 

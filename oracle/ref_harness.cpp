@@ -46,6 +46,8 @@
 #include "ckks_conjugate.hpp"
 #include "ckks_keyswitch.hpp"
 #include "ckks_mul.hpp"
+#include "ckks_addition.hpp"
+#include "aes/aes_tables.hpp"
 #include "ckks_params.hpp"
 #include "ckks_relin.hpp"
 #include "ckks_rescale.hpp"
@@ -615,6 +617,190 @@ int ref_walsh_sbox(void* h, size_t block_count, size_t level, double scale, cons
             copy_out(res[k].getA(), out + off);
             off += res[k].getA().size();
         }
+    });
+}
+
+// ---- XBOOT S-box (src/ckks/operations/circuits/aes/ckks_aes_ctr.cpp:48-336).  The reference
+// keeps it in an anonymous namespace of that file, so the harness restates its steps on the
+// reference's public operations: exact-add alignment (:48-158), multiply + relinearize + rescale
+// at a fixed scale (:160-183), the layered monomial tree (:185-256), the Moebius coefficients of
+// the S-box bits (:258-278) and the per-bit integer combination (:280-336).
+namespace xboot_ref {
+
+using Byte = MyVector<CKKSCiphertext>;
+
+bool close(long double l, long double r) {
+    if (!std::isfinite(l) || !std::isfinite(r)) return false;
+    return std::abs(l - r) <= 0x1p-45L * std::max<long double>({1.0L, std::abs(l), std::abs(r)});
+}
+
+bool is_zero(const CKKSCiphertext& ct) {
+    for (size_t k = 0; k < ct.getNumPolys(); ++k)
+        for (uint64_t v : ct.getPoly(k))
+            if (v) return false;
+    return true;
+}
+
+CKKSCiphertext align(const CKKSContext& c, CKKSCiphertext ct, size_t level, long double scale, size_t polys) {
+    ckks_drop_to_level_inplace(ct, level);
+    while (ct.getNumPolys() < polys) ct.addPoly(MyVector<uint64_t>(ct.getN() * (ct.getLevel() + 1), 0));
+    if (close(ct.getScale(), scale) || is_zero(ct)) {
+        ct.setScale(scale);
+        return ct;
+    }
+    if (ct.getScale() > scale) throw std::invalid_argument("xboot: cannot scale down");
+    const long double k = std::round(scale / ct.getScale());
+    if (k != 1.0L) ckks_mul_inplace(c, ct, (int64_t)k);
+    ct.setScale(scale);
+    return ct;
+}
+
+void add_term(const CKKSContext& c, CKKSCiphertext& acc, CKKSCiphertext term) {
+    const size_t level = std::min(acc.getLevel(), term.getLevel());
+    const long double scale = std::max(acc.getScale(), term.getScale());
+    const size_t polys = std::max(acc.getNumPolys(), term.getNumPolys());
+    acc = align(c, std::move(acc), level, scale, polys);
+    term = align(c, std::move(term), level, scale, polys);
+    ckks_add_inplace(c, acc, term);
+}
+
+CKKSCiphertext mul_relin_rescale(const CKKSContext& c, const CKKSCiphertext& l, const CKKSCiphertext& r,
+                                 long double scale) {
+    const size_t level = std::min(l.getLevel(), r.getLevel());
+    auto out = l.clone();
+    ckks_drop_to_level_inplace(out, level);
+    out.setScale(scale);
+    auto rr = r.clone();
+    ckks_drop_to_level_inplace(rr, level);
+    rr.setScale(scale);
+    ckks_mul_inplace(c, out, rr);
+    ckks_relin_hybrid_inplace(c, out);
+    ckks_rescale(c, out);
+    out.setScale(scale);
+    return out;
+}
+
+struct Mono {
+    size_t mask;
+    CKKSCiphertext value;
+};
+
+std::vector<Mono> layered(const CKKSContext& c, const Byte& in, size_t begin, size_t end, long double scale) {
+    const size_t n = end - begin;
+    std::vector<Mono> out;
+    if (n == 1) {
+        auto v = in[begin].clone();
+        v.setScale(scale);
+        out.push_back({size_t{1} << begin, std::move(v)});
+        return out;
+    }
+    if (n == 2) {
+        auto l = in[begin].clone();
+        l.setScale(scale);
+        auto r = in[begin + 1].clone();
+        r.setScale(scale);
+        auto p = mul_relin_rescale(c, l, r, scale);
+        out.push_back({size_t{1} << begin, std::move(l)});
+        out.push_back({size_t{1} << (begin + 1), std::move(r)});
+        out.push_back({(size_t{1} << begin) | (size_t{1} << (begin + 1)), std::move(p)});
+        return out;
+    }
+    const size_t mid = begin + n / 2;
+    auto left = layered(c, in, begin, mid, scale);
+    auto right = layered(c, in, mid, end, scale);
+    for (const auto& a : left)
+        for (const auto& b : right) out.push_back({a.mask | b.mask, mul_relin_rescale(c, a.value, b.value, scale)});
+    for (auto& a : left) out.push_back(std::move(a));
+    for (auto& b : right) out.push_back(std::move(b));
+    return out;
+}
+
+std::array<std::array<int64_t, 256>, 8> coefficients() {
+    std::array<std::array<int64_t, 256>, 8> out{};
+    for (size_t bit = 0; bit < 8; ++bit) {
+        for (size_t x = 0; x < 256; ++x) out[bit][x] = (int64_t)((kAesSboxTable[x] >> bit) & 1U);
+        for (size_t v = 0; v < 8; ++v)
+            for (size_t m = 0; m < 256; ++m)
+                if (m & (size_t{1} << v)) out[bit][m] -= out[bit][m ^ (size_t{1} << v)];
+    }
+    return out;
+}
+
+Byte sbox(const CKKSContext& c, const Byte& in) {
+    const long double scale = in.front().getScale();
+    std::vector<std::optional<CKKSCiphertext>> mono(256);
+    for (auto& m : layered(c, in, 0, 8, scale)) mono[m.mask] = std::move(m.value);
+    const auto cf = coefficients();
+    Byte out;
+    for (size_t bit = 0; bit < 8; ++bit) {
+        std::optional<CKKSCiphertext> acc;
+        if (cf[bit][0] != 0) {
+            acc = in.front().clone();
+            ckks_mul_inplace(c, *acc, int64_t{0});
+            ckks_add_integer_constant_inplace(c, *acc, cf[bit][0]);
+        }
+        for (size_t m = 1; m < 256; ++m) {
+            if (cf[bit][m] == 0) continue;
+            auto t = mono[m]->clone();
+            ckks_mul_inplace(c, t, cf[bit][m]);
+            if (acc)
+                add_term(c, *acc, std::move(t));
+            else
+                acc = std::move(t);
+        }
+        out.emplace_back(std::move(*acc));
+    }
+    return out;
+}
+
+}  // namespace xboot_ref
+
+// The XBOOT chain at N = 2^15 (AESXBoot15Config: 17 Q limbs of 36..38 bits, 5 P limbs, dnum 5,
+// h 256) without bootstrapping, so only the relinearisation key is generated.
+void* ref_xboot15_create(void) {
+    RefCtx* out = nullptr;
+    const int rc = guarded([&] {
+        CKKSParamsConfig cfg = ckks_aes_params_detail::AESXBoot15Config();
+        cfg.secure = false;
+        cfg.bts_keys = false;
+        cfg.bootstrap_params.reset();
+        cfg.q_mult_bits.clear();
+        cfg.mult_depth = cfg.q_bits.size() - 1;
+        out = new RefCtx(CKKSParams(std::move(cfg)));
+    });
+    return rc == 0 ? out : nullptr;
+}
+
+// The XBOOT S-box on 8 bit ciphertexts at `level` and `scale` (in: [bit][b, a][level+1][N]);
+// out: 8 x (b, a) at their levels, packed one after another.
+int ref_xboot_sbox(void* h, size_t level, double scale, const uint64_t* in, uint64_t* out, size_t* out_levels,
+                   double* out_scales) {
+    return guarded([&] {
+        auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        xboot_ref::Byte bits;
+        for (size_t k = 0; k < 8; ++k)
+            bits.emplace_back(N, copy_in(in + (2 * k + 1) * n, n), copy_in(in + 2 * k * n, n), (long double)scale,
+                              level);
+        auto res = xboot_ref::sbox(c, bits);
+        size_t off = 0;
+        for (size_t k = 0; k < 8; ++k) {
+            out_levels[k] = res[k].getLevel();
+            out_scales[k] = (double)res[k].getScale();
+            copy_out(res[k].getB(), out + off);
+            off += res[k].getB().size();
+            copy_out(res[k].getA(), out + off);
+            off += res[k].getA().size();
+        }
+    });
+}
+
+int ref_xboot_sbox_coefficients(int64_t* out) {
+    return guarded([&] {
+        const auto cf = xboot_ref::coefficients();
+        for (size_t b = 0; b < 8; ++b)
+            for (size_t m = 0; m < 256; ++m) out[b * 256 + m] = cf[b][m];
     });
 }
 
