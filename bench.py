@@ -19,6 +19,9 @@ Further sections of the same JSON line:
   batched_ops   64 walsh15 ciphertexts at seeded levels, each ct x ct multiply + relinearize +
                 rescale + rotate: one CUDA-graph replay vs the plain per-operation GPU path
   bsgs          CoeffToSlot / SlotToCoeff stages on 8 ciphertexts
+  primitives    batched NTT at walsh15; the config-1 NTT and single rotation (N = 2^14, dnum 4)
+  serving       Poisson stream of 2..1024-block requests through the continuous-batching service
+  xboot_sbox    the XBOOT S-box (the other AES path's SubBytes) on 16 instances at xboot15
   cpu_baseline  the reference's SubBytes layer (16 S-box instances, OpenMP over instances as its
                 AES does) on this host's cores, extrapolated to AES-CTR blocks/s
 
@@ -69,6 +72,7 @@ def parse():
     ap.add_argument("--no-ops", action="store_true", help="skip the batched-ops section")
     ap.add_argument("--no-ntt", action="store_true", help="skip the NTT / rotation primitives section")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-requests section")
+    ap.add_argument("--no-xboot", action="store_true", help="skip the XBOOT S-box section")
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not sample nvidia-smi clocks (for runs under a profiler, which wants the GPU to itself)")
@@ -567,6 +571,62 @@ class AesRun:
 
 
 # ------------------------------------------------------------------------------------------
+# XBOOT S-box layer (the xboot15 chain's SubBytes: 16 instances)
+# ------------------------------------------------------------------------------------------
+XB_Q_BITS = [38, 36, 36, 37, 37, 37] + [38] * 11
+XB_P_BITS = [38] * 5
+XB_DNUM = 5
+
+
+def xboot_bench(wg, torch, stream, timed, local, steps, with_cpu):
+    """The XBOOT S-box (wg_xboot_sbox) on one SubBytes layer, 16 instances of 8 bit ciphertexts at
+    level 5 of the xboot15 chain (N = 2^15, 17 Q + 5 P limbs, dnum 5; uniform residues, uniform
+    relinearisation key of its shape); optionally the reference's S-box on one instance on the
+    host cores (restated in the harness on its own operations)."""
+    N = 1 << 15
+    p, q = wg.find_primes(XB_P_BITS, XB_Q_BITS, N)
+    ctx = wg.Context(N, q, p, XB_DNUM, device=local)
+    L, K = len(q), len(p)
+    rng = np.random.default_rng(23)
+    parts = ctx.parts(L - 1)
+    col = np.tile(np.repeat(np.concatenate([q, p]).astype(np.uint64), N), 2 * parts)
+    ctx.set_key(wg.WG_KEY_RELIN, (rng.integers(0, 1 << 62, col.size, dtype=np.uint64) % col).astype(np.uint64))
+    level, scale, count = 5, 2.0 ** 37, 16
+    qcol = torch.from_numpy(np.repeat(q[: level + 1], N).view(np.int64)).cuda()
+    data = torch.randint(0, 1 << 62, (count, 8, 2, (level + 1) * N), dtype=torch.int64, device="cuda") % qcol
+    bits = [[(data[i, k, 0], data[i, k, 1]) for k in range(8)] for i in range(count)]
+    outs = [[(torch.empty((level + 1) * N, dtype=torch.int64, device="cuda"),
+              torch.empty((level + 1) * N, dtype=torch.int64, device="cuda")) for _ in range(8)] for _ in range(count)]
+    step = lambda: ctx.xboot_sbox(level, scale, bits, outs)
+    step()
+    l0 = wg.launch_count()
+    ms = timed(step, steps)
+    res = {"workload": "XBOOT S-box, one SubBytes layer: 16 instances of 8 bits at level 5 of the xboot15 chain "
+                       "(255 monomials from 247 multiply+relin+rescale per instance, 8 integer combinations)",
+           "ms_per_layer": ms, "sboxes_per_s": count / (ms / 1000.0),
+           "launches_per_layer": (wg.launch_count() - l0) / steps, "output_level": level - 3}
+    if with_cpu:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+
+            if O.ref_available():
+                R = O.RefXboot()
+                qc = np.repeat(R.q[: level + 1], N)
+                draw = lambda: (rng.integers(0, 1 << 62, (level + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
+                one = [(draw(), draw()) for _ in range(8)]
+                t0 = time.perf_counter()
+                R.sbox(level, scale, one)
+                t = time.perf_counter() - t0
+                res["reference_cpu"] = {"s_per_sbox": t, "cores": os.cpu_count(), "kind": "reference",
+                                        "sample": "one S-box instance, the reference's operations on all host "
+                                                  "threads (its AES runs 16 instances side by side)"}
+        except Exception as e:  # reported, never required
+            res["reference_cpu"] = {"unavailable": str(e)}
+    return res
+
+
+# ------------------------------------------------------------------------------------------
 # served requests (config 5, walsh15 part): Poisson arrivals through the batching service
 # ------------------------------------------------------------------------------------------
 def serve_bench(wg, torch, aes, requests, seed, capacity_blocks, workers=2, window_ms=20.0, load=0.5):
@@ -763,6 +823,8 @@ def main():
     prim = None if args.no_ntt else ntt_bench(wg, torch, stream, timed, local, 20, hbm)
     serving = None if args.no_serve else serve_bench(wg, torch, aes, args.serve_requests, args.seed + 17 + rank,
                                                      aes.blocks / (ms / 1000.0))
+    xboot = None if args.no_xboot else xboot_bench(wg, torch, stream, timed, local, 5,
+                                                     rank == 0 and world == 1 and not args.no_cpu_baseline)
     ops, ops_ctx = None, None
     if not args.no_ops:
         ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local)
@@ -814,6 +876,7 @@ def main():
         "kernels": kernels,
         "primitives": prim,
         "serving": serving,
+        "xboot_sbox": xboot,
         "batched_ops": ops,
         "bsgs": bsgs,
         "cpu_baseline": cpu,
