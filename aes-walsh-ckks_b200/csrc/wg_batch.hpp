@@ -121,6 +121,29 @@ void xboot_sbox(Context& c, size_t count, size_t level, double scale, uint64_t* 
 // Integer coefficients of each S-box output bit over the 256 monomials of the input bits.
 std::array<std::array<int64_t, 256>, 8> xboot_sbox_coefficients();
 
+// ckks_batch_bootstrap_evalmod_inplace for `count` pairs at once (wg_xboot.cu): ct0 + i ct1
+// labelled with `scale` (ct0's), bootstrapped; the two results overwrite (b0, a0) and (b1, a1),
+// which hold s2c_depth + 1 limbs on entry and need room for depth + 1.
+void bootstrap_pair(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
+                    size_t nc2s, const double* coeffs, size_t ncoeffs, size_t count, double scale, uint64_t* const* b0,
+                    uint64_t* const* a0, uint64_t* const* b1, uint64_t* const* a1, size_t* out_level, double* out_scale,
+                    cudaStream_t s);
+
+// AES-128-CTR on lazy bits with the XBOOT S-box and pair bootstraps (wg_xboot.cu).
+struct XbootAesArgs {
+    const uint64_t* const* key_b = nullptr;  // 1408 round-key bit ciphertexts
+    const uint64_t* const* key_a = nullptr;
+    const double* key_scales = nullptr;
+    const size_t* key_levels = nullptr;
+    const uint8_t* counters = nullptr;       // `blocks` public 16-byte blocks each
+    const uint8_t* ciphertexts = nullptr;
+    size_t blocks = 0;
+    size_t pair_batch = 32;                  // pair bootstraps per batched call
+};
+void aes_ctr_xboot(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
+                   size_t nc2s, const double* coeffs, size_t ncoeffs, const XbootAesArgs& a, uint64_t* const* out_b,
+                   uint64_t* const* out_a, size_t* out_level, double* out_scale, cudaStream_t s);
+
 void walsh_sbox(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
                 size_t nc2s, const double* coeffs, size_t ncoeffs, size_t block_count, size_t count, size_t level,
                 double scale, uint64_t* const* in_b, uint64_t* const* in_a, uint64_t* const* out_b,

@@ -578,6 +578,60 @@ int wg_xboot_sbox(wg_context* ctx, size_t count, size_t level, double scale, uin
     });
 }
 
+int wg_bootstrap_pair(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
+                      const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs, size_t count,
+                      double scale, uint64_t* const* b0, uint64_t* const* a0, uint64_t* const* b1,
+                      uint64_t* const* a1, size_t* out_level, double* out_scale, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(out_level, "ckks_batch_bootstrap_evalmod");
+        check_ptr(out_scale, "ckks_batch_bootstrap_evalmod");
+        check_cts(c, count, b0, a0, "ckks_batch_bootstrap_evalmod");
+        check_cts(c, count, b1, a1, "ckks_batch_bootstrap_evalmod");
+        std::vector<const wg::LtStage*> vs, vc;
+        const wg::BootstrapParams bp = boot_args(params, s2c, ns2c, c2s, nc2s, coeffs, vs, vc);
+        const wg::S2cPlan plan{1, vs.data(), ns2c};
+        wg::bootstrap_pair(c, bp, &plan, 1, vc.data(), nc2s, coeffs, ncoeffs, count, scale, b0, a0, b1, a1, out_level,
+                           out_scale, S(stream));
+    });
+}
+
+int wg_aes_ctr_xboot(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
+                     const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                     const uint64_t* const* key_b, const uint64_t* const* key_a, const double* key_scales,
+                     const size_t* key_levels, const uint8_t* counters, const uint8_t* ciphertexts, size_t blocks,
+                     uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                     void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(out_level, "ckks_aes");
+        check_ptr(out_scale, "ckks_aes");
+        check_ptr(key_scales, "ckks_aes");
+        check_ptr(key_levels, "ckks_aes");
+        check_ptr(counters, "ckks_aes");
+        check_ptr(ciphertexts, "ckks_aes");
+        check_cts(c, 128, out_b, out_a, "ckks_aes");
+        if (!key_b || !key_a) wg::fail(wg::kInvalid, "ckks_aes: null key bits");
+        for (size_t k = 0; k < 1408; ++k) {
+            check_ptr(key_b[k], "ckks_aes");
+            check_ptr(key_a[k], "ckks_aes");
+        }
+        std::vector<const wg::LtStage*> vs, vc;
+        const wg::BootstrapParams bp = boot_args(params, s2c, ns2c, c2s, nc2s, coeffs, vs, vc);
+        const wg::S2cPlan plan{1, vs.data(), ns2c};
+        wg::XbootAesArgs a;
+        a.key_b = key_b;
+        a.key_a = key_a;
+        a.key_scales = key_scales;
+        a.key_levels = key_levels;
+        a.counters = counters;
+        a.ciphertexts = ciphertexts;
+        a.blocks = blocks;
+        wg::aes_ctr_xboot(c, bp, &plan, 1, vc.data(), nc2s, coeffs, ncoeffs, a, out_b, out_a, out_level, out_scale,
+                          S(stream));
+    });
+}
+
 int wg_xboot_sbox_coefficients(int64_t* out) {
     return guard([&] {
         check_ptr(out, "ckks_aes");

@@ -94,6 +94,10 @@ def lib() -> C.CDLL:
         L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_xboot_sbox.argtypes = [vp, sz, sz, C.c_double, vp, vp, vp, vp, vp, vp, vp]
         L.wg_xboot_sbox_coefficients.argtypes = [vp]
+        L.wg_bootstrap_pair.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, sz, C.c_double, vp, vp, vp, vp,
+                                        C.POINTER(C.c_size_t), C.POINTER(C.c_double), vp]
+        L.wg_aes_ctr_xboot.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, vp, vp, vp, C.c_char_p, C.c_char_p, sz,
+                                       vp, vp, vp, vp, vp]
         L.wg_serve_create.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, vp,
                                       C.POINTER(vp)]
         L.wg_serve_submit.argtypes = [vp, C.c_char_p, C.c_char_p, sz, vp, vp, C.POINTER(C.c_uint64)]
@@ -561,6 +565,44 @@ class Context:
                                       pc.ctypes.data, len(pc), cf.ctypes.data, len(cf), packing_block_count,
                                       packed_segment_count, kb.ctypes.data, ka.ctypes.data, ks.ctypes.data, key_level,
                                       bytes(counters), bytes(ciphertexts), active_blocks, ob.ctypes.data,
+                                      oa.ctypes.data, lv.ctypes.data, sc.ctypes.data, _stream(stream)))
+        return [int(x) for x in lv], [float(x) for x in sc]
+
+    def bootstrap_pair(self, params, s2c, c2s, coeffs, scale, pairs, stream=None):
+        """XBOOT pair bootstraps: pairs = [((b0, a0), (b1, a1))] device tensors at level
+        s2c_depth with room for depth+1 limbs, every first ciphertext at `scale`; the results
+        overwrite them.  Returns (out_level, out_scale)."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        hs = lambda sts: np.ascontiguousarray([st.h.value for st in sts], dtype=np.uint64)
+        ps, pc = hs(s2c), hs(c2s)
+        b0, a0 = arr([x[0][0] for x in pairs]), arr([x[0][1] for x in pairs])
+        b1, a1 = arr([x[1][0] for x in pairs]), arr([x[1][1] for x in pairs])
+        cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        lvl, sc = C.c_size_t(), C.c_double()
+        _check(lib().wg_bootstrap_pair(self.h, C.byref(params), ps.ctypes.data, len(ps), pc.ctypes.data, len(pc),
+                                       cf.ctypes.data, len(cf), len(pairs), float(scale), b0.ctypes.data,
+                                       a0.ctypes.data, b1.ctypes.data, a1.ctypes.data, C.byref(lvl), C.byref(sc),
+                                       _stream(stream)))
+        return lvl.value, sc.value
+
+    def aes_ctr_xboot(self, params, s2c, c2s, coeffs, key_bits, key_scales, key_levels, counters, ciphertexts,
+                      blocks, out_bits, stream=None):
+        """Homomorphic AES-128-CTR with the XBOOT S-box: key_bits = 1408 (b, a) device tensors at
+        key_levels, counters / ciphertexts = bytes of `blocks` blocks, out_bits = 128 (b, a)
+        device tensors with room for depth+1 limbs.  Returns (levels, scales) of the outputs."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        hs = lambda sts: np.ascontiguousarray([st.h.value for st in sts], dtype=np.uint64)
+        kb, ka = arr([x[0] for x in key_bits]), arr([x[1] for x in key_bits])
+        ob, oa = arr([x[0] for x in out_bits]), arr([x[1] for x in out_bits])
+        ps, pc = hs(s2c), hs(c2s)
+        cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        ks = np.ascontiguousarray(key_scales, dtype=np.float64)
+        kl = np.ascontiguousarray(key_levels, dtype=np.uintp)
+        lv = np.zeros(128, np.uintp)
+        sc = np.zeros(128, np.float64)
+        _check(lib().wg_aes_ctr_xboot(self.h, C.byref(params), ps.ctypes.data, len(ps), pc.ctypes.data, len(pc),
+                                      cf.ctypes.data, len(cf), kb.ctypes.data, ka.ctypes.data, ks.ctypes.data,
+                                      kl.ctypes.data, bytes(counters), bytes(ciphertexts), blocks, ob.ctypes.data,
                                       oa.ctypes.data, lv.ctypes.data, sc.ctypes.data, _stream(stream)))
         return [int(x) for x in lv], [float(x) for x in sc]
 

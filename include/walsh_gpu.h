@@ -295,6 +295,36 @@ int wg_xboot_sbox(wg_context* ctx, size_t count, size_t level, double scale, uin
  * out[bit * 256 + mask] (mask 0 = constant term). */
 int wg_xboot_sbox_coefficients(int64_t* out);
 
+/* The XBOOT pair bootstrap for `count` pairs at once (the reference boots one pair per call):
+ * replaces ckks_batch_bootstrap_evalmod_inplace (src/ckks/operations/bootstrap/
+ * ckks_bootstrap_evalmod_inplace.cpp:393-414).  Pair i is (b0[i], a0[i]) and (b1[i], a1[i]) at
+ * level s2c_depth; every first ciphertext has scale `scale`.  ct0 + i * ct1 (the slot constant
+ * i encoded at scale 1) is bootstrapped as in wg_bootstrap_evalmod, and the two results
+ * overwrite the pair's buffers (room for depth+1 limbs each) at *out_level with *out_scale. */
+int wg_bootstrap_pair(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
+                      const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs, size_t count,
+                      double scale, uint64_t* const* b0, uint64_t* const* a0, uint64_t* const* b1,
+                      uint64_t* const* a1, size_t* out_level, double* out_scale, void* stream);
+
+/* AES-128 in CTR mode on lazy bits with the XBOOT S-box, evaluated on the device: replaces
+ * ckks_aes_ctr (src/ckks/operations/circuits/aes/ckks_aes_ctr.cpp:757-779).  Each of the 128
+ * state-bit ciphertexts carries block (s mod active_slots) in slot s.  key_b / key_a: the 1408
+ * encrypted expanded-key bits (device pointers, as ckks_aes128_encrypt_expanded_round_key_bits
+ * makes them: round 0 at key_levels[0..127], the others at the S2C depth) with their scales and
+ * levels; counters / ciphertexts: `blocks` public 16-byte blocks each (host memory, 1 <= blocks
+ * <= params->active_slots).  Initial public XOR of the counter bits, rounds 1..10 (SubBytes by
+ * the XBOOT S-box on all 16 bytes at once, ShiftRows, MixColumns except in round 10,
+ * AddRoundKey, then, in rounds 1..9, the 64 pair bootstraps of the state), the public
+ * ciphertext XOR and a last pair-bootstrap refresh; the 128 results go to out_b / out_a (room
+ * for depth+1 limbs) with their levels and scales.  Keys: relinearisation, conjugation, both
+ * secret switches and the plans' rotations. */
+int wg_aes_ctr_xboot(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
+                     const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                     const uint64_t* const* key_b, const uint64_t* const* key_a, const double* key_scales,
+                     const size_t* key_levels, const uint8_t* counters, const uint8_t* ciphertexts, size_t blocks,
+                     uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                     void* stream);
+
 /* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a

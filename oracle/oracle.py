@@ -464,12 +464,20 @@ class RefXboot(RefCtx):
 
 
 class RefPlans:
-    """The reference's walsh15 S2C / C2S plans and rotation keys (ref_walsh15_plans_create)."""
+    """The reference's S2C / C2S plans and rotation keys of a bootstrapping parameter set:
+    walsh15 (ref_walsh15_plans_create, or ref_walsh15_bts_create with bootstrap_keys), or the
+    XBOOT N = 2^15 sets with their bootstrapping keys (preset "xboot15" / "xboot15-sparse",
+    ref_xboot15_bts_create)."""
 
-    def __init__(self, bootstrap_keys=False):
+    def __init__(self, bootstrap_keys=False, preset="walsh15"):
         R = ref()
         R.ref_walsh15_plans_create.restype = C.c_void_p
         R.ref_walsh15_bts_create.restype = C.c_void_p
+        R.ref_xboot15_bts_create.restype = C.c_void_p
+        R.ref_xboot15_bts_create.argtypes = [C.c_int]
+        R.ref_bootstrap_pair.argtypes = [C.c_void_p, C.c_size_t, C.c_double, C.c_double] + [u64p] * 8 + \
+            [C.POINTER(C.c_size_t), C.POINTER(C.c_double)]
+        R.ref_xboot_key_bits.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, u64p, f64p, szp]
         R.ref_ctx_key_words.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.POINTER(C.c_size_t)]
         R.ref_modraise.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p]
         R.ref_dense_to_sparse.argtypes = [C.c_void_p, u64p, u64p]
@@ -498,9 +506,17 @@ class RefPlans:
         R.ref_lt_stage.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, u64p, u64p, u64p, u64p,
                                    C.POINTER(C.c_size_t)]
         R.ref_ctx_rotations.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_size_t)]
-        self.h = R.ref_walsh15_bts_create() if bootstrap_keys else R.ref_walsh15_plans_create()
+        if preset == "walsh15":
+            self.h = R.ref_walsh15_bts_create() if bootstrap_keys else R.ref_walsh15_plans_create()
+            self.dnum = 3
+        elif preset in ("xboot15", "xboot15-sparse"):
+            self.h = R.ref_xboot15_bts_create(1 if preset == "xboot15-sparse" else 0)
+            self.dnum = 5
+        else:
+            raise ValueError(f"unknown parameter preset {preset!r}")
         if not self.h:
-            raise RuntimeError("ref_walsh15 context: " + R.ref_last_error().decode())
+            raise RuntimeError(f"ref {preset} context: " + R.ref_last_error().decode())
+        self.preset = preset
         nq, np_ = C.c_size_t(), C.c_size_t()
         _check(R.ref_ctx_moduli(self.h, np.zeros(64, np.uint64), C.byref(nq), np.zeros(64, np.uint64), C.byref(np_)),
                "ref_ctx_moduli")
@@ -508,7 +524,6 @@ class RefPlans:
         self.p = np.zeros(np_.value, np.uint64)
         _check(R.ref_ctx_moduli(self.h, self.q, C.byref(nq), self.p, C.byref(np_)), "ref_ctx_moduli")
         self.N = 1 << 15
-        self.dnum = 3
         sc = C.c_double()
         _check(R.ref_ctx_scale(self.h, C.byref(sc)), "ref_ctx_scale")
         self.scale = sc.value
@@ -608,6 +623,37 @@ class RefPlans:
                                            C.byref(sc)), "ref_bootstrap_evalmod")
         k = (lvl.value + 1) * self.N
         return (bufs[0][:k].copy(), bufs[1][:k].copy()), (bufs[2][:k].copy(), bufs[3][:k].copy()), lvl.value, sc.value
+
+    def bootstrap_pair(self, level, scale0, scale1, ct0, ct1):
+        """The reference's pair bootstrap (ckks_batch_bootstrap_evalmod_inplace) of ct0 = (b, a)
+        and ct1: (out0, out1, level, scale)."""
+        n = self.N * len(self.q)
+        bufs = [np.zeros(n, np.uint64) for _ in range(4)]
+        lvl, sc = C.c_size_t(), C.c_double()
+        m = (level + 1) * self.N
+        ins = [np.ascontiguousarray(x[:m], dtype=np.uint64) for x in (ct0[0], ct0[1], ct1[0], ct1[1])]
+        _check(ref().ref_bootstrap_pair(self.h, level, float(scale0), float(scale1), *ins, *bufs, C.byref(lvl),
+                                        C.byref(sc)), "ref_bootstrap_pair")
+        k = (lvl.value + 1) * self.N
+        return (bufs[0][:k].copy(), bufs[1][:k].copy()), (bufs[2][:k].copy(), bufs[3][:k].copy()), lvl.value, sc.value
+
+    def xboot_key_bits(self, expanded_key, first_round_key_level=4):
+        """The reference's encrypted expanded-key bits for the XBOOT AES
+        (ckks_aes128_encrypt_expanded_round_key_bits): ([(b, a)] x 1408, scales, levels)."""
+        s2c = self.bts_info()["s2c_depth"]
+        top = s2c + first_round_key_level
+        words = 2 * self.N * (128 * (top + 1) + 1280 * (s2c + 1))
+        out = np.zeros(words, np.uint64)
+        scales = np.zeros(1408, np.float64)
+        levels = np.zeros(1408, np.uintp)
+        _check(ref().ref_xboot_key_bits(self.h, bytes(expanded_key), first_round_key_level, out, scales, levels),
+               "ref_xboot_key_bits")
+        bits, off = [], 0
+        for k in range(1408):
+            m = (int(levels[k]) + 1) * self.N
+            bits.append((out[off:off + m], out[off + m:off + 2 * m]))
+            off += 2 * m
+        return bits, scales, levels.astype(np.int64)
 
     def build_scaled_s2c(self, ratio):
         """Build the SlotToCoeff plan for inputs at `ratio` x the parameter scale; its stages are

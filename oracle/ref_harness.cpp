@@ -38,6 +38,7 @@
 #include "ckks_evalpoly.hpp"
 #include "ckks_bootstrap_dft.hpp"
 #include "ckks_aes_ctr_walsh_sbox.hpp"
+#include "ckks_aes_ctr.hpp"
 #include "ckks_walsh_sbox.hpp"
 #include "ckks_encoding.hpp"
 #include "ckks_bootstrap_evalmod_inplace.hpp"
@@ -801,6 +802,64 @@ int ref_xboot_sbox_coefficients(int64_t* out) {
         const auto cf = xboot_ref::coefficients();
         for (size_t b = 0; b < 8; ++b)
             for (size_t m = 0; m < 256; ++m) out[b * 256 + m] = cf[b][m];
+    });
+}
+
+// The XBOOT N = 2^15 parameter set as the reference defines it (AESXBoot15Config, or
+// AESXBoot15Sparse1024Config when `sparse`, src/ckks/parameters/ckks_aes_params.hpp:179-209),
+// bootstrapping keys included.  The EvalMod fit comes from the stand-in in
+// ref_evalmod_stub.cpp (see ref_walsh15_bts_create).
+void* ref_xboot15_bts_create(int sparse) {
+    RefCtx* out = nullptr;
+    const int rc = guarded([&] {
+        CKKSParamsConfig cfg = sparse ? ckks_aes_params_detail::AESXBoot15Sparse1024Config()
+                                      : ckks_aes_params_detail::AESXBoot15Config();
+        out = new RefCtx(CKKSParams(std::move(cfg)));
+    });
+    return rc == 0 ? out : nullptr;
+}
+
+// ckks_batch_bootstrap_evalmod_inplace (ckks_bootstrap_evalmod_inplace.cpp:393-414) on the
+// pair (ct0, ct1) at `level` with scales scale0 / scale1: both results (b, a) with
+// (*out_level + 1) * N residues each and their common scale.
+int ref_bootstrap_pair(void* h, size_t level, double scale0, double scale1, const uint64_t* b0, const uint64_t* a0,
+                       const uint64_t* b1, const uint64_t* a1, uint64_t* out0_b, uint64_t* out0_a, uint64_t* out1_b,
+                       uint64_t* out1_a, size_t* out_level, double* out_scale) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        CKKSCiphertext ct0(N, copy_in(a0, n), copy_in(b0, n), (long double)scale0, level);
+        CKKSCiphertext ct1(N, copy_in(a1, n), copy_in(b1, n), (long double)scale1, level);
+        ckks_batch_bootstrap_evalmod_inplace(c, ct0, ct1);
+        if (ct0.getLevel() != ct1.getLevel()) throw std::runtime_error("ref_bootstrap_pair: level mismatch");
+        *out_level = ct0.getLevel();
+        *out_scale = (double)ct0.getScale();
+        copy_out(ct0.getB(), out0_b);
+        copy_out(ct0.getA(), out0_a);
+        copy_out(ct1.getB(), out1_b);
+        copy_out(ct1.getA(), out1_a);
+    });
+}
+
+// ckks_aes128_encrypt_expanded_round_key_bits (ckks_aes_ctr.cpp:687-725): the 1408 key-bit
+// ciphertexts, bit k as b then a with (levels[k] + 1) * N residues each, back to back.
+int ref_xboot_key_bits(void* h, const uint8_t* expanded_key, size_t first_round_key_level, uint64_t* out,
+                       double* scales, size_t* levels) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        std::array<uint8_t, 176> ek{};
+        std::memcpy(ek.data(), expanded_key, 176);
+        auto bits = ckks_aes128_encrypt_expanded_round_key_bits(c, ek, first_round_key_level);
+        size_t off = 0;
+        for (size_t k = 0; k < bits.size(); ++k) {
+            copy_out(bits[k].getB(), out + off);
+            off += bits[k].getB().size();
+            copy_out(bits[k].getA(), out + off);
+            off += bits[k].getA().size();
+            scales[k] = (double)bits[k].getScale();
+            levels[k] = bits[k].getLevel();
+        }
     });
 }
 
