@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--no-ntt", action="store_true", help="skip the NTT / rotation primitives section")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-requests section")
     ap.add_argument("--no-xboot", action="store_true", help="skip the XBOOT S-box section")
+    ap.add_argument("--no-xboot-aes", action="store_true", help="skip the XBOOT AES-CTR section")
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not sample nvidia-smi clocks (for runs under a profiler, which wants the GPU to itself)")
@@ -627,6 +628,132 @@ def xboot_bench(wg, torch, stream, timed, local, steps, with_cpu):
 
 
 # ------------------------------------------------------------------------------------------
+# XBOOT AES-CTR (xboot15-full: 16384 blocks per evaluation)
+# ------------------------------------------------------------------------------------------
+XBOOT_PLAN_PATH = os.path.join(ROOT, "tests", "golden", "xboot15_plan.json")
+
+
+class XbootAesRun:
+    """Context, keys, bootstrap stages and encrypted round-key bits of one XBOOT N = 2^15 parameter
+    set's shapes (uniform residues), and block bytes for every active slot."""
+
+    def __init__(self, wg, torch, plan, device, seed):
+        N = plan["ring_degree"]
+        q = np.array(plan["q"], dtype=np.uint64)
+        p = np.array(plan["p"], dtype=np.uint64)
+        K = len(p)
+        self.N, self.wg = N, wg
+        self.ctx = ctx = wg.Context(N, q, p, plan["dnum"], device=device)
+        rng = np.random.default_rng(seed)
+
+        def residues(limb_mods, copies):
+            col = np.tile(np.repeat(np.asarray(limb_mods, np.uint64), N), copies)
+            return (rng.integers(0, 1 << 62, col.size, dtype=np.uint64) % col).astype(np.uint64)
+
+        keys = plan["keys"]
+        for name, kind in (("relin", wg.WG_KEY_RELIN), ("conj", wg.WG_KEY_CONJ),
+                           ("sparse_to_dense", wg.WG_KEY_SPARSE_TO_DENSE)):
+            k = keys[name]
+            ctx.set_key(kind, residues(np.concatenate([q[: k["key_level"] + 1], p]), 2 * k["parts"]),
+                        parts=k["parts"], key_level=k["key_level"])
+        ctx.set_key(wg.WG_KEY_DENSE_TO_SPARSE, residues([q[0], p[0], q[0], p[0]], 1))
+        rk = keys["rotation"]
+        rkey = residues(np.concatenate([q[: rk["key_level"] + 1], p]), 2 * rk["parts"])
+        for r in plan["rotations"]:
+            ctx.set_key(wg.WG_KEY_ROTATION, rkey, rotation=int(r), parts=rk["parts"], key_level=rk["key_level"])
+
+        def stages(spec):
+            out = []
+            for st in spec:
+                level = st["qp_limbs"] - 1 - K
+                d = residues(np.concatenate([q[: level + 1], p]), len(st["indices"]))
+                out.append(wg.LtStage(ctx, level, st["indices"], d, st["baby"], st["slot_count"], st["rescale"]))
+            return out
+
+        self.s2c, self.c2s = stages(plan["s2c"]), stages(plan["c2s"])
+        b = plan["bootstrap"]
+        self.params = wg.BootstrapParams(b["s2c_depth"], b["depth"], b["evalmod_log_scale"], b["double_angle"],
+                                         b["active_slots"], b["slots"], b["scale"])
+        self.coeffs = np.asarray(plan["evalmod_coeffs"], dtype=np.float64)
+        a = plan["aes"]
+        self.klevels = np.asarray(a["key_levels"], dtype=np.int64)
+        self.kscales = np.asarray(a["key_scales"], dtype=np.float64)
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed)
+        self.key_dev, self.key_bits = [], [None] * len(self.klevels)
+        for lv in sorted(set(int(x) for x in self.klevels)):
+            idx = [k for k in range(len(self.klevels)) if self.klevels[k] == lv]
+            qcol = torch.from_numpy(np.repeat(q[: lv + 1], N).view(np.int64)).cuda()
+            t = torch.randint(0, 1 << 62, (len(idx), 2, (lv + 1) * N), dtype=torch.int64, device="cuda",
+                              generator=gen) % qcol
+            self.key_dev.append(t)
+            for j, k in enumerate(idx):
+                self.key_bits[k] = (t[j, 0], t[j, 1])
+        full = (b["depth"] + 1) * N
+        self.out_dev = torch.zeros((128, 2, full), dtype=torch.int64, device="cuda")
+        self.outs = [(self.out_dev[k, 0], self.out_dev[k, 1]) for k in range(128)]
+        self.blocks = b["active_slots"]
+        self.block_bytes = [bytes(rng.integers(0, 256, 16 * self.blocks, dtype=np.uint8)) for _ in range(3)]
+        self.calls = 0
+
+    def step(self, stream):
+        c = self.block_bytes[self.calls % 3]
+        x = self.block_bytes[(self.calls + 1) % 3]
+        self.calls += 1
+        return self.ctx.aes_ctr_xboot(self.params, self.s2c, self.c2s, self.coeffs, self.key_bits, self.kscales,
+                                      self.klevels, c, x, self.blocks, self.outs, stream=stream)
+
+
+def xboot_aes_bench(wg, torch, stream, timed, local, seed, steps, with_cpu, sbox_seconds=None):
+    """AES-128-CTR with the XBOOT S-box (wg_aes_ctr_xboot) on xboot15-full: 16384 counter blocks
+    per evaluation (every slot one block), ten rounds with 64 pair bootstraps after rounds 1..9
+    and a final refresh.  Optionally the reference's pair bootstrap once on the host cores and an
+    estimate of its full evaluation from that sample and the S-box sample."""
+    with open(XBOOT_PLAN_PATH) as f:
+        plan = json.load(f)["xboot15"]
+    run = XbootAesRun(wg, torch, plan, local, seed)
+    step = lambda: run.step(stream)
+    step()
+    l0 = wg.launch_count()
+    ms = timed(step, steps)
+    res = {"workload": "xboot15-full AES-128-CTR: 16384 counter blocks per evaluation (one block per slot), "
+                       "XBOOT S-box on all 16 bytes per round, 64 pair bootstraps after rounds 1..9 and at the end",
+           "shapes": "tests/golden/xboot15_plan.json (the reference's xboot15 bootstrapping plan), uniform residues",
+           "blocks": run.blocks, "ms_per_evaluation": ms, "blocks_per_s": run.blocks / (ms / 1000.0),
+           "steps": steps, "launches_per_evaluation": (wg.launch_count() - l0) / steps,
+           "pair_bootstraps_per_evaluation": 640, "sboxes_per_evaluation": 160}
+    blocks = run.blocks
+    del run
+    torch.cuda.synchronize()
+    if with_cpu:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+
+            if O.ref_available():
+                R = O.RefPlans(bootstrap_keys=True, preset="xboot15")
+                lv, N = 2, R.N
+                rng = np.random.default_rng(seed)
+                qc = np.repeat(R.q[: lv + 1], N)
+                draw = lambda: (rng.integers(0, 1 << 62, (lv + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
+                c0, c1 = (draw(), draw()), (draw(), draw())
+                t0 = time.perf_counter()
+                R.bootstrap_pair(lv, R.scale, R.scale, c0, c1)
+                tp = time.perf_counter() - t0
+                ref = {"s_per_pair_bootstrap": tp, "cores": os.cpu_count(), "kind": "reference",
+                       "sample": "one pair bootstrap (ckks_batch_bootstrap_evalmod_inplace) on all host threads"}
+                if sbox_seconds:
+                    est = 640 * tp + 160 * sbox_seconds
+                    ref.update({"estimated_s_per_evaluation": est, "estimated_blocks_per_s": blocks / est,
+                                "estimate": "640 pair bootstraps + 160 S-box instances at the sampled per-call "
+                                            "times (the reference runs them one call per thread group)"})
+                res["reference_cpu"] = ref
+        except Exception as e:  # reported, never required
+            res["reference_cpu"] = {"unavailable": str(e)}
+    return res
+
+
+# ------------------------------------------------------------------------------------------
 # served requests (config 5, walsh15 part): Poisson arrivals through the batching service
 # ------------------------------------------------------------------------------------------
 def serve_bench(wg, torch, aes, requests, seed, capacity_blocks, workers=2, window_ms=20.0, load=0.5):
@@ -825,6 +952,11 @@ def main():
                                                      aes.blocks / (ms / 1000.0))
     xboot = None if args.no_xboot else xboot_bench(wg, torch, stream, timed, local, 5,
                                                      rank == 0 and world == 1 and not args.no_cpu_baseline)
+    xboot_aes = None
+    if not args.no_xboot_aes:
+        sbox_s = ((xboot or {}).get("reference_cpu") or {}).get("s_per_sbox")
+        xboot_aes = xboot_aes_bench(wg, torch, stream, timed, local, args.seed + 29 + rank, 2,
+                                    rank == 0 and world == 1 and not args.no_cpu_baseline, sbox_s)
     ops, ops_ctx = None, None
     if not args.no_ops:
         ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local)
@@ -877,6 +1009,7 @@ def main():
         "primitives": prim,
         "serving": serving,
         "xboot_sbox": xboot,
+        "xboot_aes": xboot_aes,
         "batched_ops": ops,
         "bsgs": bsgs,
         "cpu_baseline": cpu,
