@@ -630,7 +630,7 @@ def xboot_bench(wg, torch, stream, timed, local, steps, with_cpu):
 # ------------------------------------------------------------------------------------------
 # XBOOT AES-CTR (xboot15-full: 16384 blocks per evaluation)
 # ------------------------------------------------------------------------------------------
-XBOOT_PLAN_PATH = os.path.join(ROOT, "tests", "golden", "xboot15_plan.json")
+XBOOT_PLAN_PATH = os.path.join(ROOT, "tests", "golden", "xboot_plans.json")
 
 
 class XbootAesRun:
@@ -718,7 +718,7 @@ def xboot_aes_bench(wg, torch, stream, timed, local, seed, steps, with_cpu, sbox
     ms = timed(step, steps)
     res = {"workload": "xboot15-full AES-128-CTR: 16384 counter blocks per evaluation (one block per slot), "
                        "XBOOT S-box on all 16 bytes per round, 64 pair bootstraps after rounds 1..9 and at the end",
-           "shapes": "tests/golden/xboot15_plan.json (the reference's xboot15 bootstrapping plan), uniform residues",
+           "shapes": "tests/golden/xboot_plans.json (the reference's xboot15 bootstrapping plan), uniform residues",
            "blocks": run.blocks, "ms_per_evaluation": ms, "blocks_per_s": run.blocks / (ms / 1000.0),
            "steps": steps, "launches_per_evaluation": (wg.launch_count() - l0) / steps,
            "pair_bootstraps_per_evaluation": 640, "sboxes_per_evaluation": 160}

@@ -466,8 +466,8 @@ class RefXboot(RefCtx):
 class RefPlans:
     """The reference's S2C / C2S plans and rotation keys of a bootstrapping parameter set:
     walsh15 (ref_walsh15_plans_create, or ref_walsh15_bts_create with bootstrap_keys), or the
-    XBOOT N = 2^15 sets with their bootstrapping keys (preset "xboot15" / "xboot15-sparse",
-    ref_xboot15_bts_create)."""
+    XBOOT sets with their bootstrapping keys (preset "xboot15" / "xboot15-sparse",
+    ref_xboot15_bts_create; "xboot14" / "xboot14-sparse", ref_xboot14_bts_create)."""
 
     def __init__(self, bootstrap_keys=False, preset="walsh15"):
         R = ref()
@@ -475,6 +475,8 @@ class RefPlans:
         R.ref_walsh15_bts_create.restype = C.c_void_p
         R.ref_xboot15_bts_create.restype = C.c_void_p
         R.ref_xboot15_bts_create.argtypes = [C.c_int]
+        R.ref_xboot14_bts_create.restype = C.c_void_p
+        R.ref_xboot14_bts_create.argtypes = [C.c_int]
         R.ref_bootstrap_pair.argtypes = [C.c_void_p, C.c_size_t, C.c_double, C.c_double] + [u64p] * 8 + \
             [C.POINTER(C.c_size_t), C.POINTER(C.c_double)]
         R.ref_xboot_key_bits.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, u64p, f64p, szp]
@@ -512,6 +514,9 @@ class RefPlans:
         elif preset in ("xboot15", "xboot15-sparse"):
             self.h = R.ref_xboot15_bts_create(1 if preset == "xboot15-sparse" else 0)
             self.dnum = 5
+        elif preset in ("xboot14", "xboot14-sparse"):
+            self.h = R.ref_xboot14_bts_create(1 if preset == "xboot14-sparse" else 0)
+            self.dnum = 13
         else:
             raise ValueError(f"unknown parameter preset {preset!r}")
         if not self.h:
@@ -523,7 +528,7 @@ class RefPlans:
         self.q = np.zeros(nq.value, np.uint64)
         self.p = np.zeros(np_.value, np.uint64)
         _check(R.ref_ctx_moduli(self.h, self.q, C.byref(nq), self.p, C.byref(np_)), "ref_ctx_moduli")
-        self.N = 1 << 15
+        self.N = 1 << (14 if preset.startswith("xboot14") else 15)
         sc = C.c_double()
         _check(R.ref_ctx_scale(self.h, C.byref(sc)), "ref_ctx_scale")
         self.scale = sc.value

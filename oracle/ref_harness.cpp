@@ -819,6 +819,19 @@ void* ref_xboot15_bts_create(int sparse) {
     return rc == 0 ? out : nullptr;
 }
 
+// The secure XBOOT N = 2^14 parameter set (AESXBoot14SecureConfig, or
+// AESXBoot14SecureSparse1024Config when `sparse`, ckks_aes_params.hpp:133-154) with its
+// bootstrapping keys; EvalMod fit from the stand-in.
+void* ref_xboot14_bts_create(int sparse) {
+    RefCtx* out = nullptr;
+    const int rc = guarded([&] {
+        CKKSParamsConfig cfg = sparse ? ckks_aes_params_detail::AESXBoot14SecureSparse1024Config()
+                                      : ckks_aes_params_detail::AESXBoot14SecureConfig();
+        out = new RefCtx(CKKSParams(std::move(cfg)));
+    });
+    return rc == 0 ? out : nullptr;
+}
+
 // ckks_batch_bootstrap_evalmod_inplace (ckks_bootstrap_evalmod_inplace.cpp:393-414) on the
 // pair (ct0, ct1) at `level` with scales scale0 / scale1: both results (b, a) with
 // (*out_level + 1) * N residues each and their common scale.

@@ -1,6 +1,7 @@
-"""Write xboot15_plan.json: the public structure of the reference's XBOOT N = 2^15 bootstrapping
-contexts (AESXBoot15Config and AESXBoot15Sparse1024Config) that a device XBOOT AES-CTR run needs
-besides key and plaintext values.
+"""Write xboot_plans.json: the public structure of the reference's XBOOT bootstrapping contexts
+(AESXBoot15Config, AESXBoot15Sparse1024Config, AESXBoot14SecureConfig and
+AESXBoot14SecureSparse1024Config) that a device XBOOT AES-CTR run needs besides key and plaintext
+values.
 
 Generated from the reference compiled from its own sources (oracle/_ref, through oracle.RefPlans)
 like walsh15_plan.json: prime chain, EvalMod bootstrap parameters and series coefficients (from
@@ -10,7 +11,7 @@ round-key bits (ckks_aes128_encrypt_expanded_round_key_bits with the first round
 as the reference benchmark encrypts them).  Residues are not stored: the benchmark draws them at
 random with these shapes.
 
-    python tests/golden/make_xboot15_plan.py
+    python tests/golden/make_xboot_plans.py
 """
 import json
 import os
@@ -58,8 +59,9 @@ def main():
     import oracle as O
     from aes_util import expand_key
 
-    plans = {preset: plan_of(O, preset, expand_key) for preset in ("xboot15", "xboot15-sparse")}
-    path = os.path.join(HERE, "xboot15_plan.json")
+    plans = {preset: plan_of(O, preset, expand_key)
+             for preset in ("xboot15", "xboot15-sparse", "xboot14", "xboot14-sparse")}
+    path = os.path.join(HERE, "xboot_plans.json")
     with open(path, "w") as f:
         json.dump(plans, f, separators=(",", ":"))
         f.write("\n")

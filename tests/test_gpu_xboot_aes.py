@@ -1,5 +1,6 @@
-"""The XBOOT AES path on the device, on the reference's XBOOT N = 2^15 parameter sets
-(AESXBoot15Config and its 1024-active-slot variant, bootstrapping keys from the reference):
+"""The XBOOT AES path on the device, on the reference's XBOOT parameter sets (AESXBoot15Config,
+AESXBoot14SecureConfig and their 1024-active-slot variants, bootstrapping keys from the
+reference):
 
 * the pair bootstrap (wg_bootstrap_pair) against the reference's
   ckks_batch_bootstrap_evalmod_inplace (ckks_bootstrap_evalmod_inplace.cpp:393-414): two
@@ -23,7 +24,7 @@ from aes_util import encrypt_block, expand_key
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module", params=["xboot15", "xboot15-sparse"])
+@pytest.fixture(scope="module", params=["xboot15", "xboot15-sparse", "xboot14", "xboot14-sparse"])
 def xb(request, wg, ref_mod):
     R = ref_mod.RefPlans(bootstrap_keys=True, preset=request.param)
     info = R.bts_info()
