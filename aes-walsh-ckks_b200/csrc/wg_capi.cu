@@ -691,6 +691,47 @@ int wg_serve_create(wg_context* ctx, const wg_bootstrap_params* params, const wg
     });
 }
 
+int wg_serve_create_xboot(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
+                          size_t ns2c, const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs,
+                          size_t ncoeffs, const uint64_t* const* key_b, const uint64_t* const* key_a,
+                          const double* key_scales, const size_t* key_levels, const wg_serve_config* config,
+                          wg_server** out) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(out, "wg_serve");
+        check_ptr(config, "wg_serve");
+        check_ptr(key_scales, "wg_serve");
+        if (!key_b || !key_a) wg::fail(wg::kInvalid, "wg_serve: null key bits");
+        wg::ServeSetup su;
+        su.bp = boot_args(params, s2c, ns2c, c2s, nc2s, coeffs, su.s2c, su.c2s);
+        check_ptr(key_levels, "wg_serve");
+        su.xboot = true;
+        su.coeffs.assign(coeffs, coeffs + ncoeffs);
+        for (size_t k = 0; k < 1408; ++k) {
+            check_ptr(key_b[k], "wg_serve");
+            check_ptr(key_a[k], "wg_serve");
+            su.key_b.push_back(key_b[k]);
+            su.key_a.push_back(key_a[k]);
+            su.key_scales.push_back(key_scales[k]);
+            su.key_levels.push_back(key_levels[k]);
+        }
+        wg::ServeConfig cfg;
+        cfg.workers = config->workers;
+        cfg.hbm_budget = config->hbm_budget_bytes;
+        cfg.eval_bytes = config->eval_bytes;
+        cfg.max_blocks = config->max_blocks;
+        cfg.batch_window_ms = config->batch_window_ms;
+        auto* h = new wg_server{nullptr};
+        try {
+            h->s = new wg::Server(c, std::move(su), cfg);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
 int wg_serve_submit(wg_server* server, const uint8_t* counters, const uint8_t* ciphertexts, size_t blocks,
                     uint64_t* const* out_b, uint64_t* const* out_a, uint64_t* id) {
     return guard([&] {

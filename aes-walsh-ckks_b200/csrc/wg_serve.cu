@@ -3,8 +3,9 @@
 // Each worker thread owns a non-blocking stream and one evaluation's output buffers.  A free
 // worker waits until requests are queued and fewer evaluations run than the memory budget
 // admits, takes every queued request, in arrival order, whose blocks still fit into one
-// evaluation (a request never splits), concatenates their counter and ciphertext blocks and pads
-// them with zero blocks to the evaluation's full 2 x packing-block-count slots (block b: real slot
+// evaluation (a request never splits) and concatenates their counter and ciphertext blocks.
+// An XBOOT evaluation (aes_ctr_xboot) takes them as they are, block b in slot b.  A Walsh one
+// pads them with zero blocks to the evaluation's full 2 x packing-block-count slots (block b: real slot
 // b for b < packing blocks, imaginary slot b - packing blocks otherwise; the circuit's final
 // refresh packs by rotations of multiples of the active block count, and the walsh15 context
 // holds rotation keys for the full count only, as the reference's does), runs aes_ctr_walsh on
@@ -29,10 +30,18 @@ constexpr size_t kBlockBytes = 16;
 Server::Server(Context& c, ServeSetup setup, const ServeConfig& cfg) : c_(c), setup_(std::move(setup)), cfg_(cfg) {
     if (setup_.key_b.size() != kKeyBits || setup_.key_a.size() != kKeyBits || setup_.key_scales.size() != kKeyBits)
         throw std::invalid_argument("wg_serve: expected 1408 encrypted round-key bits");
-    if (setup_.packing_block_count == 0) throw std::invalid_argument("wg_serve: packing block count must be nonzero");
-    max_blocks_ = cfg_.max_blocks ? cfg_.max_blocks : 2 * setup_.packing_block_count;
-    if (max_blocks_ < 2 || (max_blocks_ & 1) || max_blocks_ > 2 * setup_.packing_block_count)
-        throw std::invalid_argument("wg_serve: block slots per evaluation must be even and at most 2 x packing blocks");
+    if (setup_.xboot) {
+        if (setup_.key_levels.size() != kKeyBits) throw std::invalid_argument("wg_serve: expected 1408 key-bit levels");
+        const size_t slots = setup_.bp.active_slots;
+        max_blocks_ = cfg_.max_blocks ? cfg_.max_blocks : slots;
+        if (max_blocks_ == 0 || max_blocks_ > slots)
+            throw std::invalid_argument("wg_serve: block slots per evaluation must be 1..active slots");
+    } else {
+        if (setup_.packing_block_count == 0) throw std::invalid_argument("wg_serve: packing block count must be nonzero");
+        max_blocks_ = cfg_.max_blocks ? cfg_.max_blocks : 2 * setup_.packing_block_count;
+        if (max_blocks_ < 2 || (max_blocks_ & 1) || max_blocks_ > 2 * setup_.packing_block_count)
+            throw std::invalid_argument("wg_serve: block slots per evaluation must be even and at most 2 x packing blocks");
+    }
     if (cfg_.workers == 0) throw std::invalid_argument("wg_serve: at least one worker");
     check_cuda(cudaSetDevice(c_.device), "cudaSetDevice");
     workers_.resize(cfg_.workers);
@@ -90,8 +99,10 @@ size_t Server::admitted() const {
 uint64_t Server::submit(const uint8_t* counters, const uint8_t* ciphertexts, size_t blocks, uint64_t* const* out_b,
                         uint64_t* const* out_a) {
     if (!counters || !ciphertexts || !out_b || !out_a) throw std::invalid_argument("wg_serve: null argument");
-    if (blocks < 2 || (blocks & 1) || blocks > max_blocks_)
-        throw std::invalid_argument("wg_serve: block count must be even, at least 2 and at most the evaluation's slots");
+    if (setup_.xboot ? (blocks == 0 || blocks > max_blocks_) : (blocks < 2 || (blocks & 1) || blocks > max_blocks_))
+        throw std::invalid_argument(setup_.xboot
+                                        ? "wg_serve: block count must be at least 1 and at most the evaluation's slots"
+                                        : "wg_serve: block count must be even, at least 2 and at most the evaluation's slots");
     Request r;
     r.counters.assign(counters, counters + blocks * kBlockBytes);
     r.ciphertexts.assign(ciphertexts, ciphertexts + blocks * kBlockBytes);
@@ -167,7 +178,7 @@ void Server::worker(size_t w) {
             ++running_;
         }
         const auto started = Clock::now();
-        const size_t active = setup_.packing_block_count;
+        const size_t active = setup_.xboot ? setup_.bp.active_slots : setup_.packing_block_count;
         ServeResult base;
         base.batch_requests = batch.size();
         base.batch_blocks = blocks;
@@ -180,21 +191,36 @@ void Server::worker(size_t w) {
                 counters.insert(counters.end(), r.counters.begin(), r.counters.end());
                 cts.insert(cts.end(), r.ciphertexts.begin(), r.ciphertexts.end());
             }
-            counters.resize(2 * active * kBlockBytes, 0);
-            cts.resize(2 * active * kBlockBytes, 0);
-            AesArgs a;
-            a.key_b = setup_.key_b.data();
-            a.key_a = setup_.key_a.data();
-            a.key_scales = setup_.key_scales.data();
-            a.key_level = setup_.key_level;
-            a.counters = counters.data();
-            a.ciphertexts = cts.data();
-            a.active_blocks = active;
-            a.packing_block_count = setup_.packing_block_count;
-            a.packed_segment_count = setup_.packed_segment_count;
-            aes_ctr_walsh(c_, setup_.bp, plans, setup_.s2c_x2.empty() ? 1 : 2, setup_.c2s.data(), setup_.c2s.size(),
-                          setup_.coeffs.data(), setup_.coeffs.size(), a, ob.data(), oa.data(), base.out_level,
-                          base.out_scale, me.stream);
+            if (setup_.xboot) {
+                // the XBOOT circuit takes the batch's blocks as they are (slot b = block b)
+                XbootAesArgs x;
+                x.key_b = setup_.key_b.data();
+                x.key_a = setup_.key_a.data();
+                x.key_scales = setup_.key_scales.data();
+                x.key_levels = setup_.key_levels.data();
+                x.counters = counters.data();
+                x.ciphertexts = cts.data();
+                x.blocks = blocks;
+                aes_ctr_xboot(c_, setup_.bp, plans, 1, setup_.c2s.data(), setup_.c2s.size(), setup_.coeffs.data(),
+                              setup_.coeffs.size(), x, ob.data(), oa.data(), base.out_level, base.out_scale,
+                              me.stream);
+            } else {
+                counters.resize(2 * active * kBlockBytes, 0);
+                cts.resize(2 * active * kBlockBytes, 0);
+                AesArgs a;
+                a.key_b = setup_.key_b.data();
+                a.key_a = setup_.key_a.data();
+                a.key_scales = setup_.key_scales.data();
+                a.key_level = setup_.key_level;
+                a.counters = counters.data();
+                a.ciphertexts = cts.data();
+                a.active_blocks = active;
+                a.packing_block_count = setup_.packing_block_count;
+                a.packed_segment_count = setup_.packed_segment_count;
+                aes_ctr_walsh(c_, setup_.bp, plans, setup_.s2c_x2.empty() ? 1 : 2, setup_.c2s.data(), setup_.c2s.size(),
+                              setup_.coeffs.data(), setup_.coeffs.size(), a, ob.data(), oa.data(), base.out_level,
+                              base.out_scale, me.stream);
+            }
             for (const auto& r : batch)
                 for (size_t k = 0; k < kStateBits; ++k) {
                     const size_t bytes = (base.out_level[k] + 1) * N * 8;

@@ -1,11 +1,11 @@
 // Continuous-batching AES-CTR transciphering service on one device (wg_serve.cu).
 //
 // No counterpart in the reference, whose benchmark runs one AES-CTR evaluation at a time
-// (bench/aes_bench.cpp).  Requests of 2..1024 counter blocks queue up; each free worker takes
-// every waiting request, in arrival order, that still fits into one evaluation's 1024 block slots, runs
-// the homomorphic AES-CTR on its own stream and hands every request its output bit
-// ciphertexts.  Workers run evaluations concurrently (their kernels interleave on the device)
-// as far as the device-memory budget allows.
+// (bench/aes_bench.cpp).  Requests of counter blocks queue up; each free worker takes every
+// waiting request, in arrival order, that still fits into one evaluation's block slots (1024 for
+// walsh15, one per active slot for the XBOOT parameter sets), runs the homomorphic AES-CTR on its
+// own stream and hands every request its output bit ciphertexts.  Workers run evaluations
+// concurrently (their kernels interleave on the device) as far as the device-memory budget allows.
 #pragma once
 #include <chrono>
 #include <condition_variable>
@@ -30,13 +30,18 @@ struct ServeSetup {
     std::vector<const uint64_t*> key_b, key_a;  // 1408 encrypted round-key bits
     std::vector<double> key_scales;
     size_t key_level = 0, packing_block_count = 0, packed_segment_count = 0;
+    // XBOOT evaluations (aes_ctr_xboot) instead of Walsh ones: key bits at key_levels, one block
+    // per active slot, no packing; s2c_x2, key_level and the packing counts are unused
+    bool xboot = false;
+    std::vector<size_t> key_levels;
 };
 
 struct ServeConfig {
     size_t workers = 2;        // evaluations that may run at once
     size_t hbm_budget = 0;     // device bytes the evaluations may take together (0: no limit)
     size_t eval_bytes = 0;     // device bytes one evaluation takes (admission estimate)
-    size_t max_blocks = 0;     // block slots per evaluation (0: 2 x packing block count)
+    size_t max_blocks = 0;     // block slots per evaluation (0: 2 x packing block count, or the
+                               // active slot count for XBOOT)
     double batch_window_ms = 0.0;  // a free worker waits this long after the oldest queued
                                    // request for more to fill its batch (0: start at once)
 };
@@ -45,8 +50,9 @@ struct ServeResult {
     int status = 0;            // WG_OK, or the error code of the failed evaluation
     std::string error;
     size_t block_offset = 0;   // first evaluation block of the request
-    size_t active_blocks = 0;  // the evaluation's blocks per lane (= packing block count; block b
-                               // sits in slot b mod it, real part for b < it, imaginary otherwise)
+    size_t active_blocks = 0;  // the evaluation's blocks per lane (Walsh: the packing block count;
+                               // block b sits in slot b mod it, real part for b < it, imaginary
+                               // otherwise.  XBOOT: the active slot count; block b in slot b)
     size_t batch_requests = 0, batch_blocks = 0;
     double queue_ms = 0.0, latency_ms = 0.0;  // submission to start, submission to completion
     size_t out_level[128] = {};
@@ -67,8 +73,9 @@ public:
     Server& operator=(const Server&) = delete;
 
     // Queue a request: `blocks` counter blocks and as many ciphertext blocks (16 bytes each;
-    // blocks even, 2 <= blocks <= max_blocks); out_b / out_a are 128 device buffers of
-    // (depth + 1) N words each that receive the output bit ciphertexts.  Returns its id.
+    // Walsh: blocks even, 2 <= blocks <= max_blocks; XBOOT: 1 <= blocks <= max_blocks); out_b /
+    // out_a are 128 device buffers of (depth + 1) N words each that receive the output bit
+    // ciphertexts.  Returns its id.
     uint64_t submit(const uint8_t* counters, const uint8_t* ciphertexts, size_t blocks, uint64_t* const* out_b,
                     uint64_t* const* out_a);
     // Wait up to timeout_s (negative: no limit) for a request; true when it has finished.

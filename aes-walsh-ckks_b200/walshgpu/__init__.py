@@ -100,6 +100,7 @@ def lib() -> C.CDLL:
                                        vp, vp, vp, vp, vp]
         L.wg_serve_create.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, vp,
                                       C.POINTER(vp)]
+        L.wg_serve_create_xboot.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_serve_submit.argtypes = [vp, C.c_char_p, C.c_char_p, sz, vp, vp, C.POINTER(C.c_uint64)]
         L.wg_serve_wait.argtypes = [vp, C.c_uint64, C.c_double, vp]
         L.wg_serve_destroy.argtypes = [vp]
@@ -286,9 +287,10 @@ WG_NOT_READY = 1
 
 
 class Server:
-    """Continuous-batching AES-CTR service (wg_serve_*): requests of an even number of counter
-    blocks are packed in arrival order into shared evaluations that `workers` streams run
-    concurrently.  The stages, key bits and coefficients must outlive the server."""
+    """Continuous-batching AES-CTR service (wg_serve_*): requests of counter blocks (an even
+    number for Walsh evaluations) are packed in arrival order into shared evaluations that
+    `workers` streams run concurrently; Server.xboot(...) serves XBOOT evaluations.  The stages,
+    key bits and coefficients must outlive the server."""
 
     def __init__(self, ctx, params, s2c, s2c_x2, c2s, coeffs, packing_block_count, packed_segment_count, key_bits,
                  key_scales, key_level, workers=2, hbm_budget_bytes=0, eval_bytes=0, max_blocks=0,
@@ -309,6 +311,30 @@ class Server:
                                      self._ka.ctypes.data, self._ks.ctypes.data, key_level, C.byref(cfg), C.byref(h)))
         self.h = h
         self._outs = {}
+
+    @classmethod
+    def xboot(cls, ctx, params, s2c, c2s, coeffs, key_bits, key_scales, key_levels, workers=2, hbm_budget_bytes=0,
+              eval_bytes=0, max_blocks=0, batch_window_ms=0.0):
+        """The service over XBOOT evaluations (wg_serve_create_xboot): requests of 1..active-slot
+        blocks, block b of an evaluation in slot b."""
+        self = cls.__new__(cls)
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        hs = lambda sts: np.ascontiguousarray([st.h.value for st in sts], dtype=np.uint64)
+        self._keep = (params, s2c, c2s, key_bits)
+        self._kb, self._ka = arr([x[0] for x in key_bits]), arr([x[1] for x in key_bits])
+        self._ps, self._pc = hs(s2c), hs(c2s)
+        self._cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        self._ks = np.ascontiguousarray(key_scales, dtype=np.float64)
+        self._kl = np.ascontiguousarray(key_levels, dtype=np.uintp)
+        cfg = ServeConfig(workers, hbm_budget_bytes, eval_bytes, max_blocks, batch_window_ms)
+        h = C.c_void_p()
+        _check(lib().wg_serve_create_xboot(ctx.h, C.byref(params), self._ps.ctypes.data, len(self._ps),
+                                           self._pc.ctypes.data, len(self._pc), self._cf.ctypes.data, len(self._cf),
+                                           self._kb.ctypes.data, self._ka.ctypes.data, self._ks.ctypes.data,
+                                           self._kl.ctypes.data, C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._outs = {}
+        return self
 
     def submit(self, counters, ciphertexts, out_bits):
         """Queue a request (bytes of `blocks` counter and ciphertext blocks, 128 (b, a) device

@@ -75,6 +75,7 @@ def parse():
     ap.add_argument("--no-xboot", action="store_true", help="skip the XBOOT S-box section")
     ap.add_argument("--no-xboot-aes", action="store_true", help="skip the XBOOT AES-CTR section")
     ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-mix-requests", type=int, default=16)
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not sample nvidia-smi clocks (for runs under a profiler, which wants the GPU to itself)")
     ap.add_argument("--no-aes", action="store_true",
@@ -704,14 +705,11 @@ class XbootAesRun:
                                       self.klevels, c, x, self.blocks, self.outs, stream=stream)
 
 
-def xboot_aes_bench(wg, torch, stream, timed, local, seed, steps, with_cpu, sbox_seconds=None):
+def xboot_aes_bench(wg, torch, stream, timed, run, seed, steps, with_cpu, sbox_seconds=None):
     """AES-128-CTR with the XBOOT S-box (wg_aes_ctr_xboot) on xboot15-full: 16384 counter blocks
     per evaluation (every slot one block), ten rounds with 64 pair bootstraps after rounds 1..9
     and a final refresh.  Optionally the reference's pair bootstrap once on the host cores and an
     estimate of its full evaluation from that sample and the S-box sample."""
-    with open(XBOOT_PLAN_PATH) as f:
-        plan = json.load(f)["xboot15"]
-    run = XbootAesRun(wg, torch, plan, local, seed)
     step = lambda: run.step(stream)
     step()
     l0 = wg.launch_count()
@@ -723,7 +721,6 @@ def xboot_aes_bench(wg, torch, stream, timed, local, seed, steps, with_cpu, sbox
            "steps": steps, "launches_per_evaluation": (wg.launch_count() - l0) / steps,
            "pair_bootstraps_per_evaluation": 640, "sboxes_per_evaluation": 160}
     blocks = run.blocks
-    del run
     torch.cuda.synchronize()
     if with_cpu:
         try:
@@ -793,7 +790,7 @@ def serve_bench(wg, torch, aes, requests, seed, capacity_blocks, workers=2, wind
     queue = np.array([r["queue_ms"] for r in res])
     evaluations = sum(1.0 / r["batch_requests"] for r in res)
     return {"workload": f"{requests} requests, log-uniform 2..1024 blocks (even), Poisson arrivals at "
-                        f"{load} x full-slot capacity; walsh15 only (the xboot parameter sets are not built)",
+                        f"{load} x full-slot capacity; walsh15 alone (the mixed stream is serving_mix)",
             "workers": workers, "batch_window_ms": window_ms, "requests": requests, "blocks": int(sum(sizes)),
             "arrival_rate_per_s": rate, "offered_blocks_per_s": rate * float(np.mean(sizes)),
             "wall_s": wall, "blocks_per_s": sum(sizes) / wall,
@@ -802,6 +799,68 @@ def serve_bench(wg, torch, aes, requests, seed, capacity_blocks, workers=2, wind
             "queue_ms": {"p50": float(np.percentile(queue, 50)), "p99": float(np.percentile(queue, 99))},
             "evaluations": round(evaluations, 2), "requests_per_evaluation": requests / evaluations,
             "full_slot_capacity_blocks_per_s": capacity_blocks}
+
+
+def serve_mix_bench(wg, torch, aes, xrun, requests, seed, walsh_cap, xboot_cap, window_ms=20.0, load=0.5):
+    """Config 5's mixed stream: requests alternate between walsh15 (log-uniform 2..1024 blocks,
+    even) and xboot15-full (log-uniform 1..16384 blocks), arriving as one seeded Poisson stream;
+    each parameter set has its own continuous-batching server (walsh15: two workers, xboot15:
+    one) on the same device, keys resident.  The arrival rate makes the offered work `load` x the
+    device at each set's measured full-slot capacity."""
+    rng = np.random.default_rng(seed)
+    wfull, xfull = aes.out_dev.shape[2], xrun.out_dev.shape[2]
+    ws = wg.Server(aes.ctx, aes.params, aes.s2c, aes.s2c_x2, aes.c2s, aes.coeffs, aes.pbc, aes.psc, aes.key_bits,
+                   aes.kscales, aes.kl, workers=2, batch_window_ms=window_ms)
+    xs = wg.Server.xboot(xrun.ctx, xrun.params, xrun.s2c, xrun.c2s, xrun.coeffs, xrun.key_bits, xrun.kscales,
+                         xrun.klevels, workers=1, batch_window_ms=window_ms)
+    srv = {"walsh15": ws, "xboot15": xs}
+    cap = {"walsh15": walsh_cap, "xboot15": xboot_cap}
+    blocks_src = {"walsh15": aes.block_bytes, "xboot15": xrun.block_bytes}
+    mk = lambda full: [(torch.empty(full, dtype=torch.int64, device="cuda"),
+                        torch.empty(full, dtype=torch.int64, device="cuda")) for _ in range(128)]
+    try:
+        ids = [ws.submit(aes.block_bytes[0][:32], aes.block_bytes[1][:32], mk(wfull)),
+               xs.submit(xrun.block_bytes[0][:32], xrun.block_bytes[1][:32], mk(xfull))]
+        ws.wait(ids[0])
+        xs.wait(ids[1])
+        kinds = ["walsh15" if k % 2 == 0 else "xboot15" for k in range(requests)]
+        sizes = [2 * int(round(np.exp(rng.uniform(0.0, np.log(512))))) if kd == "walsh15"
+                 else int(round(np.exp(rng.uniform(0.0, np.log(16384))))) for kd in kinds]
+        work = [n / cap[kd] for kd, n in zip(kinds, sizes)]
+        rate = load / float(np.mean(work))
+        gaps = rng.exponential(1.0 / rate, requests)
+        bufs = [mk(wfull if kd == "walsh15" else xfull) for kd in kinds]
+        ids = []
+        start = time.perf_counter()
+        t = start
+        for k, (kd, n, gap) in enumerate(zip(kinds, sizes, gaps)):
+            t += gap
+            delay = t - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            src = blocks_src[kd]
+            ids.append(srv[kd].submit(src[1][:16 * n], src[2][:16 * n], bufs[k]))
+        res = [srv[kd].wait(i) for kd, i in zip(kinds, ids)]
+        wall = time.perf_counter() - start
+    finally:
+        ws.close()
+        xs.close()
+    out = {"workload": f"{requests} requests alternating walsh15 (log-uniform 2..1024 blocks, even) and xboot15-full "
+                       f"(log-uniform 1..16384 blocks), one Poisson stream at {load} x the device's full-slot "
+                       f"capacity; one server per parameter set on the same device",
+           "batch_window_ms": window_ms, "arrival_rate_per_s": rate, "wall_s": wall,
+           "blocks_per_s": sum(sizes) / wall}
+    for kd in ("walsh15", "xboot15"):
+        sel = [k for k in range(requests) if kinds[k] == kd]
+        lat = np.array([res[k]["latency_ms"] for k in sel])
+        evaluations = sum(1.0 / res[k]["batch_requests"] for k in sel)
+        out[kd] = {"requests": len(sel), "blocks": int(sum(sizes[k] for k in sel)),
+                   "blocks_per_s": sum(sizes[k] for k in sel) / wall,
+                   "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                                  "max": float(lat.max())},
+                   "requests_per_evaluation": len(sel) / evaluations,
+                   "full_slot_capacity_blocks_per_s": cap[kd]}
+    return out
 
 
 # ------------------------------------------------------------------------------------------
@@ -952,11 +1011,18 @@ def main():
                                                      aes.blocks / (ms / 1000.0))
     xboot = None if args.no_xboot else xboot_bench(wg, torch, stream, timed, local, 5,
                                                      rank == 0 and world == 1 and not args.no_cpu_baseline)
-    xboot_aes = None
+    xboot_aes, serving_mix = None, None
     if not args.no_xboot_aes:
         sbox_s = ((xboot or {}).get("reference_cpu") or {}).get("s_per_sbox")
-        xboot_aes = xboot_aes_bench(wg, torch, stream, timed, local, args.seed + 29 + rank, 2,
+        with open(XBOOT_PLAN_PATH) as f:
+            xrun = XbootAesRun(wg, torch, json.load(f)["xboot15"], local, args.seed + 29 + rank)
+        xboot_aes = xboot_aes_bench(wg, torch, stream, timed, xrun, args.seed + 29 + rank, 2,
                                     rank == 0 and world == 1 and not args.no_cpu_baseline, sbox_s)
+        if not args.no_serve:
+            serving_mix = serve_mix_bench(wg, torch, aes, xrun, args.serve_mix_requests, args.seed + 31 + rank,
+                                          aes.blocks / (ms / 1000.0), xboot_aes["blocks_per_s"])
+        del xrun
+        torch.cuda.synchronize()
     ops, ops_ctx = None, None
     if not args.no_ops:
         ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local)
@@ -1010,6 +1076,7 @@ def main():
         "serving": serving,
         "xboot_sbox": xboot,
         "xboot_aes": xboot_aes,
+        "serving_mix": serving_mix,
         "batched_ops": ops,
         "bsgs": bsgs,
         "cpu_baseline": cpu,

@@ -359,6 +359,16 @@ int wg_serve_create(wg_context* ctx, const wg_bootstrap_params* params, const wg
                     const double* coeffs, size_t ncoeffs, size_t packing_block_count, size_t packed_segment_count,
                     const uint64_t* const* key_b, const uint64_t* const* key_a, const double* key_scales,
                     size_t key_level, const wg_serve_config* config, wg_server** out);
+/* The same service over XBOOT evaluations (wg_aes_ctr_xboot) of an XBOOT parameter set: requests
+ * of 1..max_blocks blocks (max_blocks 0: params->active_slots), concatenated in arrival order with
+ * no padding; block b of an evaluation sits in slot b (real part), active_blocks reports the
+ * active slot count.  Key bits with their scales and levels as for wg_aes_ctr_xboot.  A server
+ * per parameter set on one device serves a mixed stream (e.g. walsh15 beside xboot15). */
+int wg_serve_create_xboot(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
+                          size_t ns2c, const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs,
+                          size_t ncoeffs, const uint64_t* const* key_b, const uint64_t* const* key_a,
+                          const double* key_scales, const size_t* key_levels, const wg_serve_config* config,
+                          wg_server** out);
 /* Queue one request: `blocks` counter blocks and as many ciphertext blocks (16 bytes each,
  * copied at submission); out_b / out_a: 128 device buffers of (depth + 1) N words each. */
 int wg_serve_submit(wg_server* server, const uint8_t* counters, const uint8_t* ciphertexts, size_t blocks,

@@ -10,7 +10,9 @@ reference):
   (ckks_aes128_encrypt_expanded_round_key_bits, first round key 4 levels up as its benchmark
   does): every output bit decrypts, in every active block slot, to the plaintext of plain
   AES-128-CTR with error below 0.5 (the reference benchmark's acceptance rule,
-  bench/aes_bench.cpp:305-307).
+  bench/aes_bench.cpp:305-307);
+* the serving path over XBOOT evaluations (wg_serve_create_xboot): three odd-sized requests
+  queued within the batching window share one evaluation, each decrypting to its own plaintext.
 
 The EvalMod polynomial is the one the reference context reports (its fit built by the
 harness's stand-in), so the parity holds for that polynomial."""
@@ -114,3 +116,41 @@ def test_xboot_aes_ctr_decrypts_to_plain_aes(wg, xb):
     print(f"{R.preset}: {blocks} blocks in {seconds:.2f} s on the device; max error {max_err:.3e}")
     assert mismatched == 0
     assert max_err < 0.5
+
+
+def test_xboot_served_requests_share_an_evaluation(wg, xb):
+    import torch
+
+    R, ctx, params, s2c, c2s, info = xb
+    N, full = R.N, info["depth"] + 1
+    rng = np.random.default_rng(97)
+    ek = expand_key(bytes(rng.integers(0, 256, 16, dtype=np.uint8)))
+    kbits, kscales, klevels = R.xboot_key_bits(ek, 4)
+    key_bits = [(wg.to_device(b), wg.to_device(a)) for b, a in kbits]
+    srv = wg.Server.xboot(ctx, params, s2c, c2s, info["coeffs"], key_bits, kscales, klevels, workers=1,
+                          batch_window_ms=300.0)
+    try:
+        reqs = []
+        for blocks in (3, 17, 5):
+            counters = bytes(rng.integers(0, 256, 16 * blocks, dtype=np.uint8))
+            plain = bytes(rng.integers(0, 256, 16 * blocks, dtype=np.uint8))
+            stream = b"".join(encrypt_block(ek, counters[16 * i:16 * i + 16]) for i in range(blocks))
+            cts = bytes(x ^ y for x, y in zip(plain, stream))
+            outs = [(torch.zeros(full * N, dtype=torch.int64, device="cuda"),
+                     torch.zeros(full * N, dtype=torch.int64, device="cuda")) for _ in range(128)]
+            reqs.append((blocks, plain, outs, srv.submit(counters, cts, outs)))
+        offsets = []
+        for blocks, plain, outs, rid in reqs:
+            res = srv.wait(rid, 600)
+            assert res["batch_requests"] == 3 and res["active_blocks"] == info["active_slots"]
+            offsets.append(res["block_offset"])
+            off = res["block_offset"]
+            for bit in range(128):
+                m = (res["levels"][bit] + 1) * N
+                z = R.decrypt(res["levels"][bit], res["scales"][bit], wg.to_host(outs[bit][0])[:m],
+                              wg.to_host(outs[bit][1])[:m])
+                want = [(plain[16 * b + bit // 8] >> (bit % 8)) & 1 for b in range(blocks)]
+                assert (np.round(z[off:off + blocks].real) == want).all(), (blocks, bit)
+        assert offsets == [0, 3, 20]
+    finally:
+        srv.close()
