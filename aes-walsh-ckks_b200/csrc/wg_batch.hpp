@@ -143,6 +143,14 @@ struct XbootAesArgs {
 void aes_ctr_xboot(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
                    size_t nc2s, const double* coeffs, size_t ncoeffs, const XbootAesArgs& a, uint64_t* const* out_b,
                    uint64_t* const* out_a, size_t* out_level, double* out_scale, cudaStream_t s);
+// Its steps on their own: the initial public XOR of the counter bits (key bits 0..127 of `a`,
+// outputs with room for their level + 1 limbs), and ShiftRows + MixColumns (when `mix`) +
+// AddRoundKey of 128 state bits at `level` with the key bits 0..127 of `a`.
+void xboot_initial_state(Context& c, const BootstrapParams& p, const XbootAesArgs& a, uint64_t* const* out_b,
+                         uint64_t* const* out_a, size_t* out_level, double* out_scale, cudaStream_t s);
+void xboot_linear_layer(Context& c, size_t level, const double* in_scale, uint64_t* const* in_b,
+                        uint64_t* const* in_a, const XbootAesArgs& a, bool mix, uint64_t* const* out_b,
+                        uint64_t* const* out_a, double* out_scale, cudaStream_t s);
 
 void walsh_sbox(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
                 size_t nc2s, const double* coeffs, size_t ncoeffs, size_t block_count, size_t count, size_t level,

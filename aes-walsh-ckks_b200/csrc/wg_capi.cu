@@ -393,6 +393,14 @@ static void check_cts(wg::Context& c, size_t count, uint64_t* const* b, uint64_t
     }
 }
 
+static void check_key_bits(const uint64_t* const* key_b, const uint64_t* const* key_a, size_t count) {
+    if (!key_b || !key_a) wg::fail(wg::kInvalid, "ckks_aes: null key bits");
+    for (size_t k = 0; k < count; ++k) {
+        check_ptr(key_b[k], "ckks_aes");
+        check_ptr(key_a[k], "ckks_aes");
+    }
+}
+
 int wg_modraise(wg_context* ctx, size_t count, size_t target_level, uint64_t* const* b, uint64_t* const* a,
                 void* stream) {
     return guard([&] {
@@ -629,6 +637,59 @@ int wg_aes_ctr_xboot(wg_context* ctx, const wg_bootstrap_params* params, const w
         a.blocks = blocks;
         wg::aes_ctr_xboot(c, bp, &plan, 1, vc.data(), nc2s, coeffs, ncoeffs, a, out_b, out_a, out_level, out_scale,
                           S(stream));
+    });
+}
+
+int wg_xboot_initial_state(wg_context* ctx, const wg_bootstrap_params* params, const uint64_t* const* key_b,
+                           const uint64_t* const* key_a, const double* key_scales, const size_t* key_levels,
+                           const uint8_t* counters, size_t blocks, uint64_t* const* out_b, uint64_t* const* out_a,
+                           size_t* out_level, double* out_scale, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(params, "ckks_aes");
+        check_ptr(key_scales, "ckks_aes");
+        check_ptr(key_levels, "ckks_aes");
+        check_ptr(counters, "ckks_aes");
+        check_ptr(out_level, "ckks_aes");
+        check_ptr(out_scale, "ckks_aes");
+        check_cts(c, 128, out_b, out_a, "ckks_aes");
+        check_key_bits(key_b, key_a, 128);
+        wg::BootstrapParams bp;
+        bp.active_slots = params->active_slots;
+        bp.slots = params->slots;
+        bp.scale = params->scale;
+        if (bp.active_slots == 0 || bp.active_slots > c.N / 2) wg::fail(wg::kInvalid, "ckks_aes: invalid slot counts");
+        wg::XbootAesArgs a;
+        a.key_b = key_b;
+        a.key_a = key_a;
+        a.key_scales = key_scales;
+        a.key_levels = key_levels;
+        a.counters = counters;
+        a.blocks = blocks;
+        wg::xboot_initial_state(c, bp, a, out_b, out_a, out_level, out_scale, S(stream));
+    });
+}
+
+int wg_xboot_linear_layer(wg_context* ctx, size_t level, const double* in_scale, uint64_t* const* in_b,
+                          uint64_t* const* in_a, const uint64_t* const* key_b, const uint64_t* const* key_a,
+                          const size_t* key_levels, int mix, uint64_t* const* out_b, uint64_t* const* out_a,
+                          double* out_scale, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(in_scale, "ckks_aes");
+        check_ptr(key_levels, "ckks_aes");
+        check_ptr(out_scale, "ckks_aes");
+        check_cts(c, 128, in_b, in_a, "ckks_aes");
+        check_key_bits(key_b, key_a, 128);
+        check_cts(c, 128, out_b, out_a, "ckks_aes");
+        for (size_t k = 0; k < 128; ++k)
+            if (in_b[k] == out_b[k] || in_a[k] == out_a[k] || in_b[k] == out_a[k] || in_a[k] == out_b[k])
+                wg::fail(wg::kInvalid, "ckks_aes: linear layer outputs must not alias its inputs");
+        wg::XbootAesArgs a;
+        a.key_b = key_b;
+        a.key_a = key_a;
+        a.key_levels = key_levels;
+        wg::xboot_linear_layer(c, level, in_scale, in_b, in_a, a, mix != 0, out_b, out_a, out_scale, S(stream));
     });
 }
 

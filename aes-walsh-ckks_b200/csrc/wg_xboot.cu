@@ -261,17 +261,24 @@ struct Bit {
 
 class XbootAes {
 public:
+    // own_state: the state buffers (room for depth + 1 limbs) come from the operation set;
+    // otherwise the caller binds its own before use
     XbootAes(Context& c, const BootstrapParams& p, const S2cPlan* plans, size_t nplans, const LtStage* const* c2s,
-             size_t nc2s, const double* coeffs, size_t ncoeffs, const XbootAesArgs& a, cudaStream_t s)
+             size_t nc2s, const double* coeffs, size_t ncoeffs, const XbootAesArgs& a, cudaStream_t s,
+             bool own_state = true)
         : c_(c), p_(p), plans_(plans), nplans_(nplans), c2s_(c2s), nc2s_(nc2s), coeffs_(coeffs), ncoeffs_(ncoeffs),
           a_(a), s_(s), ops_(c, 1, s) {
         const size_t full = p.depth + 1;
-        for (auto* set : {&st_, &tmp_})
-            for (Bit& x : *set) {
-                x.b = ops_.raw(full);
-                x.a = ops_.raw(full);
-            }
+        if (own_state)
+            for (auto* set : {&st_, &tmp_})
+                for (Bit& x : *set) {
+                    x.b = ops_.raw(full);
+                    x.a = ops_.raw(full);
+                }
     }
+
+    Bit& state(size_t bit) { return st_[bit]; }
+    Bit& staged(size_t bit) { return tmp_[bit]; }
 
     // make_batched_initial_counter_state (ckks_aes_ctr.cpp:576-683): per state bit, the
     // round-0 key bit XOR the counter bit plane, one level down.  An all-zero plane only drops
@@ -409,10 +416,11 @@ public:
     }
 
     // shift_rows_inplace (ckks_aes_ctr.cpp:511-526) on tmp_, then fmix_columns_inplace (:528-554,
-    // when `mix`) and add_round_key_lazy_inplace (:460-472) as one fused launch into st_.  Every
+    // when `mix`) and add_round_key_lazy_inplace (:460-472, key bits key_base + 0..127) as one
+    // fused launch into st_.  Every
     // output is an integer combination of state bits plus the key bit; its scale label is the
     // one the reference's chain of in-place additions keeps (that of its first operand).
-    void linear(size_t round, bool mix) {
+    void linear(size_t key_base, bool mix) {
         WG_SPAN("xboot.linear");
         std::array<Bit, kStateBits> sh;
         size_t w = 0;
@@ -435,7 +443,7 @@ public:
         static constexpr size_t kXtimeFirst[8] = {7, 0, 1, 2, 3, 4, 5, 6};
         std::vector<LinearJob> jobs;
         for (size_t o = 0; o < kStateBits; ++o) {
-            const size_t key = round * kStateBits + o;
+            const size_t key = key_base + o;
             if (a_.key_levels[key] < level) throw std::invalid_argument("ckks_aes: round key bit below the state level");
             Bit& x = st_[o];
             x.level = level;
@@ -592,12 +600,49 @@ void aes_ctr_xboot(Context& c, const BootstrapParams& p, const S2cPlan* s2c, siz
     aes.initial_state();
     for (size_t round = 1; round <= kAesRounds; ++round) {
         aes.sub_bytes();
-        aes.linear(round, round < kAesRounds);
+        aes.linear(round * kStateBits, round < kAesRounds);
         if (round < kAesRounds) aes.refresh();
     }
     aes.add_message();
     aes.refresh();
     aes.copy_out(out_b, out_a, out_level, out_scale);
+}
+
+void xboot_initial_state(Context& c, const BootstrapParams& p, const XbootAesArgs& a, uint64_t* const* out_b,
+                         uint64_t* const* out_a, size_t* out_level, double* out_scale, cudaStream_t s) {
+    if (a.blocks == 0 || a.blocks > p.active_slots)
+        throw std::invalid_argument("ckks_aes: public counter count exceeds logical slot count");
+    if (!a.key_b || !a.key_a || !a.key_scales || !a.key_levels || !a.counters)
+        throw std::invalid_argument("ckks_aes: null argument");
+    if (a.key_levels[0] >= c.nq) throw std::invalid_argument("ckks_aes: invalid round key bit level");
+    XbootAes aes(c, p, nullptr, 0, nullptr, 0, nullptr, 0, a, s, false);
+    for (size_t bit = 0; bit < kStateBits; ++bit) {
+        aes.state(bit).b = out_b[bit];
+        aes.state(bit).a = out_a[bit];
+    }
+    aes.initial_state();
+    *out_level = aes.state(0).level;
+    for (size_t bit = 0; bit < kStateBits; ++bit) out_scale[bit] = static_cast<double>(aes.state(bit).scale);
+}
+
+void xboot_linear_layer(Context& c, size_t level, const double* in_scale, uint64_t* const* in_b,
+                        uint64_t* const* in_a, const XbootAesArgs& a, bool mix, uint64_t* const* out_b,
+                        uint64_t* const* out_a, double* out_scale, cudaStream_t s) {
+    if (level >= c.nq) throw std::invalid_argument("ckks_aes: invalid state level");
+    if (!a.key_b || !a.key_a || !a.key_levels) throw std::invalid_argument("ckks_aes: null argument");
+    BootstrapParams none;
+    XbootAes aes(c, none, nullptr, 0, nullptr, 0, nullptr, 0, a, s, false);
+    for (size_t bit = 0; bit < kStateBits; ++bit) {
+        Bit& x = aes.staged(bit);
+        x.b = in_b[bit];
+        x.a = in_a[bit];
+        x.level = level;
+        x.scale = in_scale[bit];
+        aes.state(bit).b = out_b[bit];
+        aes.state(bit).a = out_a[bit];
+    }
+    aes.linear(0, mix);
+    for (size_t bit = 0; bit < kStateBits; ++bit) out_scale[bit] = static_cast<double>(aes.state(bit).scale);
 }
 
 }  // namespace wg

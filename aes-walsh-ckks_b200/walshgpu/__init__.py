@@ -100,6 +100,9 @@ def lib() -> C.CDLL:
                                        vp, vp, vp, vp, vp]
         L.wg_serve_create.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, vp,
                                       C.POINTER(vp)]
+        L.wg_xboot_initial_state.argtypes = [vp, vp, vp, vp, vp, vp, C.c_char_p, sz, vp, vp, C.POINTER(C.c_size_t),
+                                             vp, vp]
+        L.wg_xboot_linear_layer.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp]
         L.wg_serve_create_xboot.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_serve_submit.argtypes = [vp, C.c_char_p, C.c_char_p, sz, vp, vp, C.POINTER(C.c_uint64)]
         L.wg_serve_wait.argtypes = [vp, C.c_uint64, C.c_double, vp]
@@ -631,6 +634,36 @@ class Context:
                                       kl.ctypes.data, bytes(counters), bytes(ciphertexts), blocks, ob.ctypes.data,
                                       oa.ctypes.data, lv.ctypes.data, sc.ctypes.data, _stream(stream)))
         return [int(x) for x in lv], [float(x) for x in sc]
+
+    def xboot_initial_state(self, params, key_bits, key_scales, key_levels, counters, blocks, out_bits, stream=None):
+        """The XBOOT AES's initial public XOR (wg_xboot_initial_state) from 128 round-0 key bits:
+        returns (level, scales) of the 128 state bits written to out_bits."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        kb, ka = arr([x[0] for x in key_bits]), arr([x[1] for x in key_bits])
+        ob, oa = arr([x[0] for x in out_bits]), arr([x[1] for x in out_bits])
+        ks = np.ascontiguousarray(key_scales, dtype=np.float64)
+        kl = np.ascontiguousarray(key_levels, dtype=np.uintp)
+        lvl = C.c_size_t()
+        sc = np.zeros(128, np.float64)
+        _check(lib().wg_xboot_initial_state(self.h, C.byref(params), kb.ctypes.data, ka.ctypes.data, ks.ctypes.data,
+                                            kl.ctypes.data, bytes(counters), blocks, ob.ctypes.data, oa.ctypes.data,
+                                            C.byref(lvl), sc.ctypes.data, _stream(stream)))
+        return lvl.value, [float(x) for x in sc]
+
+    def xboot_linear_layer(self, level, in_scales, in_bits, key_bits, key_levels, mix, out_bits, stream=None):
+        """ShiftRows + MixColumns (when mix) + AddRoundKey of the XBOOT AES
+        (wg_xboot_linear_layer); returns the 128 output scales."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        ib, ia = arr([x[0] for x in in_bits]), arr([x[1] for x in in_bits])
+        kb, ka = arr([x[0] for x in key_bits]), arr([x[1] for x in key_bits])
+        ob, oa = arr([x[0] for x in out_bits]), arr([x[1] for x in out_bits])
+        isc = np.ascontiguousarray(in_scales, dtype=np.float64)
+        kl = np.ascontiguousarray(key_levels, dtype=np.uintp)
+        sc = np.zeros(128, np.float64)
+        _check(lib().wg_xboot_linear_layer(self.h, level, isc.ctypes.data, ib.ctypes.data, ia.ctypes.data,
+                                           kb.ctypes.data, ka.ctypes.data, kl.ctypes.data, 1 if mix else 0,
+                                           ob.ctypes.data, oa.ctypes.data, sc.ctypes.data, _stream(stream)))
+        return [float(x) for x in sc]
 
     def mul(self, level, b1, a1, b2, a2, c2, stream=None):
         _check(lib().wg_mul(self.h, level, _ptr(b1), _ptr(a1), _ptr(b2), _ptr(a2), _ptr(c2), _stream(stream)))

@@ -325,6 +325,26 @@ int wg_aes_ctr_xboot(wg_context* ctx, const wg_bootstrap_params* params, const w
                      uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
                      void* stream);
 
+/* Two steps of wg_aes_ctr_xboot on their own (file-internal in the reference, so no reference
+ * interface is replaced): the initial public XOR of the counter bit planes
+ * (make_batched_initial_counter_state, src/ckks/operations/circuits/aes/ckks_aes_ctr.cpp:576-683)
+ * from the 128 round-0 key bits (key_b / key_a with their scales and levels, one common level
+ * L >= 1) and `blocks` counter blocks; out_b / out_a need room for L + 1 limbs and receive the
+ * state at *out_level = L - 1 with per-bit scales out_scale[128]. */
+int wg_xboot_initial_state(wg_context* ctx, const wg_bootstrap_params* params, const uint64_t* const* key_b,
+                           const uint64_t* const* key_a, const double* key_scales, const size_t* key_levels,
+                           const uint8_t* counters, size_t blocks, uint64_t* const* out_b, uint64_t* const* out_a,
+                           size_t* out_level, double* out_scale, void* stream);
+/* ... and one round's linear layers (shift_rows_inplace, fmix_columns_inplace when `mix`,
+ * add_round_key_lazy_inplace; ckks_aes_ctr.cpp:460-554) on 128 state bits at `level` with
+ * scales in_scale[128], adding the 128 key bits key_b / key_a (levels >= level); results at
+ * `level` in out_b / out_a (not aliasing the inputs) with the scales the reference's in-place
+ * additions keep in out_scale[128]. */
+int wg_xboot_linear_layer(wg_context* ctx, size_t level, const double* in_scale, uint64_t* const* in_b,
+                          uint64_t* const* in_a, const uint64_t* const* key_b, const uint64_t* const* key_a,
+                          const size_t* key_levels, int mix, uint64_t* const* out_b, uint64_t* const* out_a,
+                          double* out_scale, void* stream);
+
 /* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a

@@ -660,6 +660,41 @@ class RefPlans:
             off += 2 * m
         return bits, scales, levels.astype(np.int64)
 
+    def xboot_initial_state(self, keys, key_scales, key_level, counters, blocks):
+        """The XBOOT initial state restated on the reference's operations
+        (ref_xboot_initial_state): ([(b, a)] x 128, level, scales)."""
+        n = (key_level + 1) * self.N
+        flat = np.concatenate([np.concatenate([np.asarray(b[:n], np.uint64), np.asarray(a[:n], np.uint64)])
+                               for b, a in keys])
+        out = np.zeros(128 * 2 * n, np.uint64)
+        lvl = C.c_size_t()
+        sc = np.zeros(128, np.float64)
+        R = ref()
+        R.ref_xboot_initial_state.argtypes = [C.c_void_p, u64p, f64p, C.c_size_t, C.c_char_p, C.c_size_t, u64p,
+                                              C.POINTER(C.c_size_t), f64p]
+        _check(R.ref_xboot_initial_state(self.h, flat, np.ascontiguousarray(key_scales, np.float64), key_level,
+                                         bytes(counters), blocks, out, C.byref(lvl), sc), "ref_xboot_initial_state")
+        m = (lvl.value + 1) * self.N
+        return [(out[2 * k * m:(2 * k + 1) * m].copy(), out[(2 * k + 1) * m:(2 * k + 2) * m].copy())
+                for k in range(128)], lvl.value, sc
+
+    def xboot_linear(self, state, in_scales, level, keys, key_level, mix):
+        """ShiftRows, MixColumns (when mix) and AddRoundKey restated on the reference's operations
+        (ref_xboot_linear): ([(b, a)] x 128, scales)."""
+        n, kn = (level + 1) * self.N, (key_level + 1) * self.N
+        flat = np.concatenate([np.concatenate([np.asarray(b[:n], np.uint64), np.asarray(a[:n], np.uint64)])
+                               for b, a in state])
+        kflat = np.concatenate([np.concatenate([np.asarray(b[:kn], np.uint64), np.asarray(a[:kn], np.uint64)])
+                                for b, a in keys])
+        out = np.zeros(128 * 2 * n, np.uint64)
+        sc = np.zeros(128, np.float64)
+        R = ref()
+        R.ref_xboot_linear.argtypes = [C.c_void_p, u64p, f64p, C.c_size_t, u64p, C.c_size_t, C.c_int, u64p, f64p]
+        _check(R.ref_xboot_linear(self.h, flat, np.ascontiguousarray(in_scales, np.float64), level, kflat, key_level,
+                                  1 if mix else 0, out, sc), "ref_xboot_linear")
+        return [(out[2 * k * n:(2 * k + 1) * n].copy(), out[(2 * k + 1) * n:(2 * k + 2) * n].copy())
+                for k in range(128)], sc
+
     def build_scaled_s2c(self, ratio):
         """Build the SlotToCoeff plan for inputs at `ratio` x the parameter scale; its stages are
         then plan 100 + ratio for stages() / stage()."""

@@ -754,6 +754,106 @@ Byte sbox(const CKKSContext& c, const Byte& in) {
     return out;
 }
 
+// make_batched_initial_counter_state (ckks_aes_ctr.cpp:576-683), restated on the reference's
+// public operations (the original is file-internal): the round-0 key bits XOR the counter bit
+// planes, one level down.
+MyVector<CKKSCiphertext> initial_state(const CKKSContext& c, const MyVector<CKKSCiphertext>& keys,
+                                       const std::vector<std::array<uint8_t, 16>>& blocks) {
+    const auto& params = c.getParams();
+    const size_t logical = params.hasBootstrapParams() ? params.getBootstrapActiveSlotCount() : params.getSlots();
+    if (blocks.empty() || blocks.size() > logical) throw std::invalid_argument("xboot: invalid counter count");
+    MyVector<CKKSCiphertext> state;
+    for (size_t bit = 0; bit < 128; ++bit) {
+        bool saw_zero = blocks.size() < logical, saw_one = false;
+        for (const auto& b : blocks) {
+            const bool v = ((b[bit / 8] >> (bit % 8)) & 1u) != 0;
+            saw_zero = saw_zero || !v;
+            saw_one = saw_one || v;
+        }
+        auto out = keys[bit].clone();
+        if (out.getLevel() == 0) throw std::invalid_argument("xboot: exact public XOR requires one level");
+        const size_t in_level = out.getLevel();
+        if (!saw_one || !saw_zero) {
+            ckks_drop_to_level_inplace(out, in_level - 1);
+            if (saw_one) {
+                ckks_mul_inplace(c, out, int64_t{-1});
+                ckks_add_integer_constant_inplace(c, out, int64_t{1});
+            }
+            state.emplace_back(std::move(out));
+            continue;
+        }
+        MyVector<Complex> signs(params.getSlots()), bits(params.getSlots());
+        for (size_t s = 0; s < params.getSlots(); ++s) {
+            const size_t ls = s % logical;
+            const uint8_t v = ls < blocks.size() ? (uint8_t)((blocks[ls][bit / 8] >> (bit % 8)) & 1u) : 0;
+            bits[s] = Complex((double)v, 0.0);
+            signs[s] = Complex(v == 0 ? 1.0 : -1.0, 0.0);
+        }
+        auto sel = ckks_encode(c, signs, (double)params.getModuli()[in_level], in_level, true);
+        ckks_mul_inplace(c, out, sel);
+        ckks_rescale(c, out);
+        auto pt = ckks_encode(c, bits, out.getLevel(), true);
+        ckks_add_inplace(c, out, pt);
+        state.emplace_back(std::move(out));
+    }
+    return state;
+}
+
+// shift_rows_inplace, fmix_columns_inplace (when `mix`) and add_round_key_lazy_inplace
+// (ckks_aes_ctr.cpp:365-472, 511-554), restated with the same clones and in-place additions.
+MyVector<CKKSCiphertext> linear_layer(const CKKSContext& c, MyVector<CKKSCiphertext> state,
+                                      const MyVector<CKKSCiphertext>& round_keys, bool mix) {
+    MyVector<CKKSCiphertext> sh;
+    for (size_t col = 0; col < 4; ++col)
+        for (size_t row = 0; row < 4; ++row) {
+            const size_t src = 4 * ((col + row) % 4) + row;
+            for (size_t bit = 0; bit < 8; ++bit) sh.emplace_back(std::move(state[src * 8 + bit]));
+        }
+    auto add = [&](const CKKSCiphertext& l, const CKKSCiphertext& r) {
+        auto o = l.clone();
+        ckks_add_inplace(c, o, r);
+        return o;
+    };
+    MyVector<CKKSCiphertext> out;
+    if (!mix) {
+        out = std::move(sh);
+    } else {
+        std::array<Byte, 16> bytes;
+        auto byte = [&](size_t b) {
+            Byte o;
+            for (size_t k = 0; k < 8; ++k) o.emplace_back(sh[b * 8 + k].clone());
+            return o;
+        };
+        auto mixb = [&](const Byte& b0, const Byte& b1, const Byte& b2, const Byte& b3) {
+            Byte s01;
+            for (size_t k = 0; k < 8; ++k) s01.emplace_back(add(b0[k], b1[k]));
+            Byte d;
+            d.emplace_back(s01[7].clone());
+            d.emplace_back(add(s01[0], s01[7]));
+            d.emplace_back(s01[1].clone());
+            d.emplace_back(add(s01[2], s01[7]));
+            d.emplace_back(add(s01[3], s01[7]));
+            d.emplace_back(s01[4].clone());
+            d.emplace_back(s01[5].clone());
+            d.emplace_back(s01[6].clone());
+            for (const Byte* t : {&b1, &b2, &b3})
+                for (size_t k = 0; k < 8; ++k) ckks_add_inplace(c, d[k], (*t)[k]);
+            return d;
+        };
+        for (size_t col = 0; col < 4; ++col) {
+            const Byte b0 = byte(4 * col), b1 = byte(4 * col + 1), b2 = byte(4 * col + 2), b3 = byte(4 * col + 3);
+            bytes[4 * col] = mixb(b0, b1, b2, b3);
+            bytes[4 * col + 1] = mixb(b1, b2, b3, b0);
+            bytes[4 * col + 2] = mixb(b2, b3, b0, b1);
+            bytes[4 * col + 3] = mixb(b3, b0, b1, b2);
+        }
+        for (auto& b : bytes)
+            for (auto& x : b) out.emplace_back(std::move(x));
+    }
+    for (size_t bit = 0; bit < 128; ++bit) ckks_add_inplace(c, out[bit], round_keys[bit]);
+    return out;
+}
+
 }  // namespace xboot_ref
 
 // The XBOOT chain at N = 2^15 (AESXBoot15Config: 17 Q limbs of 36..38 bits, 5 P limbs, dnum 5,
@@ -852,6 +952,62 @@ int ref_bootstrap_pair(void* h, size_t level, double scale0, double scale1, cons
         copy_out(ct0.getA(), out0_a);
         copy_out(ct1.getB(), out1_b);
         copy_out(ct1.getA(), out1_a);
+    });
+}
+
+// The XBOOT initial state (xboot_ref::initial_state) from 128 round-0 key bits at `key_level`
+// (in: [bit][b, a][key_level + 1][N]) and `blocks` counter blocks: out [bit][b, a][level + 1][N]
+// with the common output level and per-bit scales.
+int ref_xboot_initial_state(void* h, const uint64_t* keys, const double* key_scales, size_t key_level,
+                            const uint8_t* counters, size_t blocks, uint64_t* out, size_t* out_level,
+                            double* out_scales) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (key_level + 1) * N;
+        MyVector<CKKSCiphertext> kb;
+        for (size_t k = 0; k < 128; ++k)
+            kb.emplace_back(N, copy_in(keys + (2 * k + 1) * n, n), copy_in(keys + 2 * k * n, n),
+                            (long double)key_scales[k], key_level);
+        std::vector<std::array<uint8_t, 16>> bl(blocks);
+        for (size_t b = 0; b < blocks; ++b) std::memcpy(bl[b].data(), counters + 16 * b, 16);
+        auto st = xboot_ref::initial_state(c, kb, bl);
+        *out_level = st[0].getLevel();
+        const size_t m = (*out_level + 1) * N;
+        for (size_t k = 0; k < 128; ++k) {
+            if (st[k].getLevel() != *out_level) throw std::runtime_error("ref_xboot_initial_state: level mismatch");
+            copy_out(st[k].getB(), out + 2 * k * m);
+            copy_out(st[k].getA(), out + (2 * k + 1) * m);
+            out_scales[k] = (double)st[k].getScale();
+        }
+    });
+}
+
+// The XBOOT round's linear layers (xboot_ref::linear_layer) on 128 state bits at `level` with
+// scales in_scales (in: [bit][b, a][level + 1][N]) and 128 round-key bits at key_level (keys:
+// [bit][b, a][key_level + 1][N]): out [bit][b, a][level + 1][N] and the output scales.
+int ref_xboot_linear(void* h, const uint64_t* in, const double* in_scales, size_t level, const uint64_t* keys,
+                     size_t key_level, int mix, uint64_t* out, double* out_scales) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N, kn = (key_level + 1) * N;
+        MyVector<CKKSCiphertext> st, kb;
+        for (size_t k = 0; k < 128; ++k) {
+            st.emplace_back(N, copy_in(in + (2 * k + 1) * n, n), copy_in(in + 2 * k * n, n),
+                            (long double)in_scales[k], level);
+            // the reference adds a key bit above the state level limb by limb over the state's limbs
+            CKKSCiphertext key(N, copy_in(keys + (2 * k + 1) * kn, kn), copy_in(keys + 2 * k * kn, kn), 1.0L,
+                               key_level);
+            ckks_drop_to_level_inplace(key, level);
+            kb.emplace_back(std::move(key));
+        }
+        auto o = xboot_ref::linear_layer(c, std::move(st), kb, mix != 0);
+        for (size_t k = 0; k < 128; ++k) {
+            copy_out(o[k].getB(), out + 2 * k * n);
+            copy_out(o[k].getA(), out + (2 * k + 1) * n);
+            out_scales[k] = (double)o[k].getScale();
+        }
     });
 }
 

@@ -11,6 +11,11 @@ reference):
   does): every output bit decrypts, in every active block slot, to the plaintext of plain
   AES-128-CTR with error below 0.5 (the reference benchmark's acceptance rule,
   bench/aes_bench.cpp:305-307);
+* the circuit's own steps against the reference's, restated by the harness on the reference's
+  public operations because the originals are file-internal: the initial public XOR of the
+  counter bit planes (make_batched_initial_counter_state, ckks_aes_ctr.cpp:576-683; all-zero,
+  all-one and varying planes) and one round's ShiftRows + MixColumns + AddRoundKey
+  (ckks_aes_ctr.cpp:460-554), residue for residue with the same levels and scale labels;
 * the serving path over XBOOT evaluations (wg_serve_create_xboot): three odd-sized requests
   queued within the batching window share one evaluation, each decrypting to its own plaintext.
 
@@ -154,3 +159,64 @@ def test_xboot_served_requests_share_an_evaluation(wg, xb):
         assert offsets == [0, 3, 20]
     finally:
         srv.close()
+
+
+def test_xboot_initial_state_matches_reference(wg, xb):
+    import torch
+
+    R, ctx, params, s2c, c2s, info = xb
+    N = R.N
+    rng = np.random.default_rng(101)
+    ek = expand_key(bytes(rng.integers(0, 256, 16, dtype=np.uint8)))
+    kbits, kscales, klevels = R.xboot_key_bits(ek, 4)
+    # every slot filled on the sparse sets, so constant planes are all-zero or all-one there
+    blocks = info["active_slots"] if info["active_slots"] <= 1024 else 40
+    raw = rng.integers(0, 256, (blocks, 16), dtype=np.uint8)
+    raw[:, 0] = 0x00
+    raw[:, 1] = 0xFF
+    raw[:, 2] = 0x0F
+    counters = raw.tobytes()
+    L = int(klevels[0])
+    key_bits = [(wg.to_device(b), wg.to_device(a)) for b, a in kbits[:128]]
+    outs = [(torch.zeros((L + 1) * N, dtype=torch.int64, device="cuda"),
+             torch.zeros((L + 1) * N, dtype=torch.int64, device="cuda")) for _ in range(128)]
+    lvl, sc = ctx.xboot_initial_state(params, key_bits, kscales[:128], klevels[:128], counters, blocks, outs)
+    torch.cuda.synchronize()
+    want, rl, rs = R.xboot_initial_state(kbits[:128], kscales[:128], L, counters, blocks)
+    assert lvl == rl == L - 1
+    n = (rl + 1) * N
+    for k in range(128):
+        assert sc[k] == rs[k], k
+        assert (wg.to_host(outs[k][0])[:n] == want[k][0]).all(), (k, "b")
+        assert (wg.to_host(outs[k][1])[:n] == want[k][1]).all(), (k, "a")
+
+
+@pytest.mark.parametrize("mix", [True, False])
+def test_xboot_linear_layer_matches_reference(wg, xb, mix):
+    import torch
+
+    R, ctx, params, s2c, c2s, info = xb
+    N, level = R.N, info["s2c_depth"]
+    rng = np.random.default_rng(103 + int(mix))
+    qc = np.repeat(R.q[: level + 1], N)
+    draw = lambda: (rng.integers(0, 1 << 62, (level + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
+    state = [(draw(), draw()) for _ in range(128)]
+    # distinct scale labels per input byte, to follow which operand's label each sum keeps
+    scales = [info["scale"] * (1.0 + ((k // 8) % 3)) for k in range(128)]
+    ek = expand_key(bytes(rng.integers(0, 256, 16, dtype=np.uint8)))
+    kbits, kscales, klevels = R.xboot_key_bits(ek, 4)
+    keys = kbits[128:256]
+    kl = int(klevels[128])
+    dev = lambda x: wg.to_device(x)
+    ins = [(dev(b), dev(a)) for b, a in state]
+    key_dev = [(dev(b), dev(a)) for b, a in keys]
+    outs = [(torch.zeros((level + 1) * N, dtype=torch.int64, device="cuda"),
+             torch.zeros((level + 1) * N, dtype=torch.int64, device="cuda")) for _ in range(128)]
+    sc = ctx.xboot_linear_layer(level, scales, ins, key_dev, klevels[128:256], mix, outs)
+    torch.cuda.synchronize()
+    want, rs = R.xboot_linear(state, scales, level, keys, kl, mix)
+    n = (level + 1) * N
+    for k in range(128):
+        assert sc[k] == rs[k], k
+        assert (wg.to_host(outs[k][0])[:n] == want[k][0]).all(), (k, "b")
+        assert (wg.to_host(outs[k][1])[:n] == want[k][1]).all(), (k, "a")
