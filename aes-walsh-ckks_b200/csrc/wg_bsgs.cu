@@ -184,13 +184,29 @@ __global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, cons
         }
         const uint64_t d = tr.diag[limb];
         const uint64_t pa = mont_mul(ba, d, q, qninv), pb = mont_mul(bb, d, q, qninv);
-#pragma unroll
-        for (int g = 0; g < kGiantGroup; ++g)
-            if (g == tr.g) {
-                acc_a[g] = add_mod(acc_a[g], pa, q);
-                acc_b[g] = add_mod(acc_b[g], pb, q);
-            }
+        // tr.g is the same for every thread of the block (one job per block), so this is a
+        // uniform branch to the one accumulator pair the term adds to; the accumulators keep
+        // constant indices and stay in registers
+        switch (tr.g) {
+#define WG_GIANT_ADD(G)                          \
+    case G:                                      \
+        acc_a[G] = add_mod(acc_a[G], pa, q);     \
+        acc_b[G] = add_mod(acc_b[G], pb, q);     \
+        break;
+            WG_GIANT_ADD(0)
+            WG_GIANT_ADD(1)
+            WG_GIANT_ADD(2)
+            WG_GIANT_ADD(3)
+            WG_GIANT_ADD(4)
+            WG_GIANT_ADD(5)
+            WG_GIANT_ADD(6)
+            WG_GIANT_ADD(7)
+#undef WG_GIANT_ADD
+            default:
+                break;
+        }
     }
+    static_assert(kGiantGroup == 8, "one case per giant step of a group");
 #pragma unroll
     for (int g = 0; g < kGiantGroup; ++g) {
         if (g >= j->ng) break;

@@ -74,12 +74,14 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the served-requests section")
     ap.add_argument("--no-xboot", action="store_true", help="skip the XBOOT S-box section")
     ap.add_argument("--no-xboot-aes", action="store_true", help="skip the XBOOT AES-CTR section")
+    ap.add_argument("--xboot-aes-steps", type=int, default=2, help="timed XBOOT AES-CTR evaluations (after one warm-up)")
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-mix-requests", type=int, default=16)
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not sample nvidia-smi clocks (for runs under a profiler, which wants the GPU to itself)")
     ap.add_argument("--no-aes", action="store_true",
-                    help="skip the AES-CTR headline (a small profiling case of the other sections; no headline value)")
+                    help="skip the AES-CTR headline (profiling runs of the NTT, batched-ops and XBOOT AES sections; "
+                         "no headline value)")
     ap.add_argument("--no-bsgs", action="store_true", help="skip the CoeffToSlot / SlotToCoeff section")
     ap.add_argument("--ops-steps", type=int, default=50)
     ap.add_argument("--ops-count", type=int, default=OPS_COUNT)
@@ -911,9 +913,15 @@ def main():
             pass
         prim = None if args.no_ntt else ntt_bench(wg, torch, stream, timed, local, 20, hbm)
         ops = None if args.no_ops else ops_bench(args, wg, torch, stream, timed, rank, local)[0]
+        xaes = None
+        if not args.no_xboot_aes:
+            with open(XBOOT_PLAN_PATH) as f:
+                xrun = XbootAesRun(wg, torch, json.load(f)["xboot15"], local, args.seed + 29 + rank)
+            xaes = xboot_aes_bench(wg, torch, stream, timed, xrun, args.seed + 29 + rank, args.xboot_aes_steps, False)
+            del xrun
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "note": "--no-aes profiling run",
-                              "primitives": prim, "batched_ops": ops}), flush=True)
+                              "primitives": prim, "batched_ops": ops, "xboot_aes": xaes}), flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return
@@ -1016,7 +1024,7 @@ def main():
         sbox_s = ((xboot or {}).get("reference_cpu") or {}).get("s_per_sbox")
         with open(XBOOT_PLAN_PATH) as f:
             xrun = XbootAesRun(wg, torch, json.load(f)["xboot15"], local, args.seed + 29 + rank)
-        xboot_aes = xboot_aes_bench(wg, torch, stream, timed, xrun, args.seed + 29 + rank, 2,
+        xboot_aes = xboot_aes_bench(wg, torch, stream, timed, xrun, args.seed + 29 + rank, args.xboot_aes_steps,
                                     rank == 0 and world == 1 and not args.no_cpu_baseline, sbox_s)
         if not args.no_serve:
             serving_mix = serve_mix_bench(wg, torch, aes, xrun, args.serve_mix_requests, args.seed + 31 + rank,
