@@ -408,6 +408,31 @@ class RefCtx:
         _check(ref().ref_rescale(self.h, level, len(polys), flat), "ref_rescale")
         return [flat[k * n:k * n + level * self.N].copy() for k in range(len(polys))]
 
+    def secret_coeffs(self):
+        """The context's ternary secret as N int8 coefficients (inverse NTT of its limb 0)."""
+        sk = np.zeros(len(self.q) * self.N, np.uint64)
+        _check(ref().ref_ctx_secret(self.h, sk), "ref_ctx_secret")
+        c0 = self.ntt(sk[: self.N], inverse=True)
+        q0 = int(self.q[0])
+        return np.array([0 if v == 0 else (1 if v == 1 else -1) for v in c0.tolist()], dtype=np.int8) \
+            if all(v in (0, 1, q0 - 1) for v in c0.tolist()) else None
+
+    def automorphism_key_from_parts(self, kind, rotation, secret, a, e):
+        """The reference's rotation (kind 0) / conjugation (kind 1) key construction with the mask
+        a and noise e given (ref_automorphism_key_from_parts): flat [part][a|b][limbs][N]."""
+        R = ref()
+        R.ref_automorphism_key_from_parts.argtypes = [C.c_void_p, C.c_int, C.c_int64,
+                                                      np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS"),
+                                                      u64p, np.ctypeslib.ndpointer(dtype=np.int64,
+                                                                                   flags="C_CONTIGUOUS"), u64p]
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        out = np.zeros(2 * a.size, np.uint64)
+        _check(R.ref_automorphism_key_from_parts(self.h, int(kind), int(rotation),
+                                                 np.ascontiguousarray(secret, dtype=np.int8), a,
+                                                 np.ascontiguousarray(e, dtype=np.int64), out),
+               "ref_automorphism_key_from_parts")
+        return out
+
     def hoisted_rotations(self, level, b, a, rots):
         n = (level + 1) * self.N
         out = np.zeros(len(rots) * 2 * n, np.uint64)

@@ -39,6 +39,12 @@
 #include "ckks_bootstrap_dft.hpp"
 #include "ckks_aes_ctr_walsh_sbox.hpp"
 #include "ckks_aes_ctr.hpp"
+#include "hybrid_key_folding.hpp"
+#include "polynomial.hpp"
+#include "hybrid_key_montgomery.hpp"
+#include "secret_key_generation.hpp"
+#include "rotation_key_generation.hpp"
+#include "conjugation_key_generation.hpp"
 #include "ckks_walsh_sbox.hpp"
 #include "ckks_encoding.hpp"
 #include "ckks_bootstrap_evalmod_inplace.hpp"
@@ -245,6 +251,83 @@ int ref_ctx_map(void* h, int kind, int64_t rot, uint64_t* map_out) {
         const auto& c = static_cast<RefCtx*>(h)->ctx;
         const auto& m = kind == 0 ? c.getRotationNttMap(rot) : c.getConjugationNttMap();
         for (size_t i = 0; i < m.size(); ++i) map_out[i] = m[i];
+    });
+}
+
+// The rotation (kind 0) or conjugation (kind 1) switching key that generate_rotation_key_hybrid
+// (src/ckks/context/rotation_key_generation.cpp:92-199) / generate_conjugation_key_hybrid
+// (conjugation_key_generation.cpp) build from `secret` (N ternary coefficients), with the mask
+// `a` ([part][limbs][N], canonical, evaluation form) and the noise `e` ([part][N] integers)
+// given instead of drawn: the same steps on the reference's own NTT, pointwise, folding and
+// Montgomery helpers.  out: [part][a|b][limbs][N] as the context stores keys.
+int ref_automorphism_key_from_parts(void* h, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a,
+                                    const int64_t* e, uint64_t* out) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const auto& params = c.getParams();
+        const size_t N = params.getN(), L = params.getMaxLevel() + 1, dnum = params.getDnum();
+        const auto& qm = params.getModuli();
+        const auto& pm = params.getPModuli();
+        MyVector<uint64_t> qup(qm.begin(), qm.begin() + L);
+        qup.insert(qup.end(), pm.begin(), pm.end());
+        MyVector<Negacyclic_NTT_Twiddles> tw;
+        for (size_t i = 0; i < L; ++i) tw.emplace_back(c.getTwiddleNtt()[i]);
+        for (size_t i = 0; i < pm.size(); ++i) tw.emplace_back(c.getPTwiddleNtt()[i]);
+        // apply_automorphism_to_secret with build_automorphism_map: coefficient i goes to
+        // i * index mod 2N, negated past N
+        auto automorph = [&](const MyVector<int8_t>& x, uint64_t index) {
+            MyVector<int8_t> y(N, int8_t{0});
+            for (size_t i = 0; i < N; ++i) {
+                const size_t m = (size_t)(((unsigned __int128)i * index) % (2 * N));
+                y[m >= N ? m - N : m] = m >= N ? (int8_t)-x[i] : x[i];
+            }
+            return y;
+        };
+        const MyVector<int8_t> s(secret, secret + N);
+        MyVector<int8_t> x, y;  // b = P x (own limbs) + e - a y
+        if (kind == 0) {
+            x = s;
+            y = automorph(s, rotation_automorphism_index(N, -rotation));
+        } else {
+            x = automorph(s, conjugation_automorphism_index(N));
+            y = s;
+        }
+        const auto x_qup = ntt_secret_key(x, tw, N, qup);
+        const auto y_qup = ntt_secret_key(y, tw, N, qup);
+        MyVector<uint64_t> p_mod_m(qup.size(), 1);
+        for (size_t i = 0; i < qup.size(); ++i)
+            for (uint64_t p : pm) p_mod_m[i] = mul_mod_u64(p_mod_m[i], p % qup[i], qup[i], &tw[i].barrett_const);
+        const size_t alpha = (L + dnum - 1) / dnum;
+        const size_t T = qup.size();
+        size_t off = 0, part_index = 0;
+        for (size_t part = 0; part < dnum; ++part) {
+            const size_t s0 = part * alpha, s1 = std::min(s0 + alpha, L);
+            if (s0 >= s1) continue;
+            MyVector<uint64_t> b_poly(N * T, 0);
+            for (size_t i = s0; i < s1; ++i) {
+                std::copy(x_qup[i].begin(), x_qup[i].end(), b_poly.data() + i * N);
+                pointwise_multiply_scalar_inplace_dispatch(b_poly.data() + i * N, p_mod_m[i], N, qup[i], tw[i]);
+            }
+            MyVector<uint64_t> a_poly(a + part_index * T * N, a + (part_index + 1) * T * N);
+            MyVector<uint64_t> e_poly(N * T);
+            for (size_t i = 0; i < T; ++i)
+                for (size_t j = 0; j < N; ++j) e_poly[i * N + j] = reduce_i64_mod_q(e[part_index * N + j], qup[i]);
+            ntt_forward_rns_flat_inplace(e_poly.data(), N, T, qup, tw, false);
+            MyVector<uint64_t> as(N);
+            for (size_t i = 0; i < T; ++i) {
+                pointwise_multiply_dispatch(a_poly.data() + i * N, y_qup[i].data(), as.data(), N, qup[i], tw[i]);
+                poly_add_modq_inplace(b_poly.data() + i * N, e_poly.data() + i * N, N, qup[i]);
+                poly_sub_modq_inplace(b_poly.data() + i * N, as.data(), N, qup[i]);
+            }
+            CKKSCiphertext key(N, std::move(a_poly), std::move(b_poly), 1.0, L - 1);
+            if (params.fold_hybrid_keyswitch) ckks_fold_hybrid_switch_key_constants(key, qm, pm, tw);
+            if (params.montgomery) ckks_convert_switch_key_to_montgomery_inplace(key, qup, tw);
+            copy_out(key.getA(), out + off);
+            off += key.getA().size();
+            copy_out(key.getB(), out + off);
+            off += key.getB().size();
+            ++part_index;
+        }
     });
 }
 
