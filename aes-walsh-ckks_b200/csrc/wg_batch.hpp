@@ -129,11 +129,12 @@ void bootstrap_pair(Context& c, const BootstrapParams& p, const S2cPlan* s2c, si
                     uint64_t* const* a0, uint64_t* const* b1, uint64_t* const* a1, size_t* out_level, double* out_scale,
                     cudaStream_t s);
 
-// A rotation (kind WG_KEY_ROTATION) or conjugation (WG_KEY_CONJ) switching key of the secret
+// A rotation (kind WG_KEY_ROTATION), conjugation (WG_KEY_CONJ) or relinearisation
+// (WG_KEY_RELIN) switching key of the secret
 // `secret` (N ternary coefficients) generated on the device and installed in the context
 // (wg_keygen.cu); mask a ([part][QP limb][N]) and noise e ([part][N]) from the caller, or drawn
 // from `seed` when both are null; out_host (optional) receives the key as stored.
-void keygen_automorphism(Context& c, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a_host,
+void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a_host,
                          const int64_t* e_host, uint64_t seed, double sigma, uint64_t* out_host, cudaStream_t s);
 
 // AES-128-CTR on lazy bits with the XBOOT S-box and pair bootstraps (wg_xboot.cu).

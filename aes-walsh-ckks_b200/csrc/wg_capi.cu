@@ -206,9 +206,9 @@ int wg_ctx_set_key(wg_context* ctx, int kind, int64_t rotation, const uint64_t* 
     });
 }
 
-int wg_keygen_automorphism(wg_context* ctx, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a,
+int wg_keygen_switch_key(wg_context* ctx, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a,
                            const int64_t* e, uint64_t seed, double sigma, uint64_t* out, void* stream) {
-    return guard([&] { wg::keygen_automorphism(C(ctx), kind, rotation, secret, a, e, seed, sigma, out, S(stream)); });
+    return guard([&] { wg::keygen_switch_key(C(ctx), kind, rotation, secret, a, e, seed, sigma, out, S(stream)); });
 }
 
 int wg_ctx_has_key(const wg_context* ctx, int kind, int64_t rotation) {

@@ -1,7 +1,9 @@
-// Rotation and conjugation switching keys generated on the device.
+// Rotation, conjugation and relinearisation switching keys generated on the device.
 //
-// Reference: generate_rotation_key_hybrid (src/ckks/context/rotation_key_generation.cpp:92-199)
-// and generate_conjugation_key_hybrid (src/ckks/context/conjugation_key_generation.cpp:63-167).
+// Reference: generate_rotation_key_hybrid (src/ckks/context/rotation_key_generation.cpp:92-199),
+// generate_conjugation_key_hybrid (src/ckks/context/conjugation_key_generation.cpp:63-167) and
+// encrypt_rlk_hybrid (src/ckks/context/relinearization_key_generation.cpp:131-199, which
+// encrypts P s^2 with ckks_encrypt_custom_eval: the same form with x = s^2, y = s).
 // For each non-empty part of the hybrid decomposition (alpha = ceil(L / dnum) Q limbs each) and
 // every QP limb m:
 //     b = [limb in the part] (P mod m) x + e - a y,   then a and b times fold_m * 2^64 (mod m)
@@ -61,7 +63,7 @@ struct AssembleJob {
     uint64_t* b_out;
     uint64_t pm;  // P mod m on the part's own Q limbs, 0 elsewhere
     uint64_t c;   // fold constant times the Montgomery radix, mod m
-    int mod, pad;
+    int mod, square;  // square: x times x (relinearisation key)
 };
 
 __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
@@ -132,7 +134,8 @@ __global__ void __launch_bounds__(kT) kb_key_assemble(const AssembleJob* jobs, i
     const Modulus m = mods[j->mod];
     const uint64_t q = m.q;
     const uint64_t a = j->a_in[k];
-    uint64_t b = j->pm ? barrett_mul(j->x[k], j->pm, m) : 0;
+    const uint64_t xv = j->square ? barrett_mul(j->x[k], j->x[k], m) : j->x[k];
+    uint64_t b = j->pm ? barrett_mul(xv, j->pm, m) : 0;
     b = add_mod(b, j->e[k], q);
     b = sub_mod(b, barrett_mul(a, j->y[k], m), q);
     j->b_out[k] = barrett_mul(b, j->c, m);
@@ -164,10 +167,10 @@ void run_jobs(Context& c, const std::vector<Job>& jobs, Kernel kernel, double by
 
 }  // namespace
 
-void keygen_automorphism(Context& c, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a_host,
+void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a_host,
                          const int64_t* e_host, uint64_t seed, double sigma, uint64_t* out_host, cudaStream_t s) {
-    if (kind != WG_KEY_ROTATION && kind != WG_KEY_CONJ)
-        throw std::invalid_argument("wg_keygen: only rotation and conjugation keys are generated");
+    if (kind != WG_KEY_ROTATION && kind != WG_KEY_CONJ && kind != WG_KEY_RELIN)
+        throw std::invalid_argument("wg_keygen: only rotation, conjugation and relinearisation keys are generated");
     if (!secret) throw std::invalid_argument("wg_keygen: null secret");
     if (!a_host != !e_host) throw std::invalid_argument("wg_keygen: give both the mask and the noise, or neither");
     const size_t N = c.N, L = c.nq, K = c.np, T = L + K, slots = N / 2;
@@ -187,6 +190,9 @@ void keygen_automorphism(Context& c, int kind, int64_t rotation, const int8_t* s
         x.assign(secret, secret + N);
         // rotation_automorphism_index(N, -r) = 5^(slots - r) mod 2N
         y = automorph_secret(secret, N, host::powmod(5, (uint64_t)((int64_t)slots - r) % slots, 2 * N));
+    } else if (kind == WG_KEY_RELIN) {
+        x.assign(secret, secret + N);  // squared limb by limb in the evaluation domain
+        y.assign(secret, secret + N);
     } else {
         x = automorph_secret(secret, N, 2 * N - 1);
         y.assign(secret, secret + N);
@@ -292,7 +298,7 @@ void keygen_automorphism(Context& c, int kind, int64_t rotation, const int8_t* s
                 jb.pm = (i >= s0 && i < s1) ? pm[i] : 0;
                 jb.c = cst[i];
                 jb.mod = mod_of(i);
-                jb.pad = 0;
+                jb.square = kind == WG_KEY_RELIN ? 1 : 0;
                 asm_jobs.push_back(jb);
             }
         }

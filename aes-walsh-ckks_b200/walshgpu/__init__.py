@@ -103,7 +103,7 @@ def lib() -> C.CDLL:
         L.wg_xboot_initial_state.argtypes = [vp, vp, vp, vp, vp, vp, C.c_char_p, sz, vp, vp, C.POINTER(C.c_size_t),
                                              vp, vp]
         L.wg_xboot_linear_layer.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp]
-        L.wg_keygen_automorphism.argtypes = [vp, C.c_int, C.c_int64, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
+        L.wg_keygen_switch_key.argtypes = [vp, C.c_int, C.c_int64, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
         L.wg_serve_create_xboot.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_serve_submit.argtypes = [vp, C.c_char_p, C.c_char_p, sz, vp, vp, C.POINTER(C.c_uint64)]
         L.wg_serve_wait.argtypes = [vp, C.c_uint64, C.c_double, vp]
@@ -474,10 +474,10 @@ class Context:
         _check(lib().wg_keyswitch(self.h, level, _ptr(key_term), kind, int(rotation), _ptr(b), _ptr(a),
                                   int(b_add), int(a_add), _stream(stream)))
 
-    def keygen_automorphism(self, kind, rotation, secret, a=None, e=None, seed=0, sigma=3.2, want_key=False,
+    def keygen_switch_key(self, kind, rotation, secret, a=None, e=None, seed=0, sigma=3.2, want_key=False,
                             stream=None):
-        """Generate and install a rotation (WG_KEY_ROTATION) or conjugation (WG_KEY_CONJ) key on
-        the device from the ternary secret (N int8 coefficients); a ([part][nq + np][N]) and e
+        """Generate and install a rotation (WG_KEY_ROTATION), conjugation (WG_KEY_CONJ) or
+        relinearisation (WG_KEY_RELIN) key on the device from the ternary secret (N int8 coefficients); a ([part][nq + np][N]) and e
         ([part][N]) given, or drawn from `seed` when None.  Returns the key as stored (flat uint64,
         wg_ctx_set_key layout) when want_key."""
         sec = np.ascontiguousarray(secret, dtype=np.int8)
@@ -493,7 +493,7 @@ class Context:
         out = None
         if want_key:
             out = np.zeros(self.parts(self.nq - 1) * 2 * (self.nq + self.np_) * self.N, np.uint64)
-        _check(lib().wg_keygen_automorphism(self.h, int(kind), int(rotation), sec.ctypes.data,
+        _check(lib().wg_keygen_switch_key(self.h, int(kind), int(rotation), sec.ctypes.data,
                                             None if ap is None else ap.ctypes.data,
                                             None if ep is None else ep.ctypes.data, int(seed) & (2**64 - 1),
                                             float(sigma), None if out is None else out.ctypes.data,

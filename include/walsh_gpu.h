@@ -82,17 +82,19 @@ void wg_ctx_destroy(wg_context* ctx);
 int wg_ctx_set_key(wg_context* ctx, int kind, int64_t rotation, const uint64_t* host_key,
                    size_t parts, size_t key_level);
 /* 1 if the key is installed, else 0.  CKKSContext::hasRotationKey, ckks_context.cpp:769-775. */
-/* Generate a rotation (WG_KEY_ROTATION, `rotation`) or conjugation (WG_KEY_CONJ) switching key
- * on the device from the ternary secret `secret` (N coefficients, host memory) and install it
- * like wg_ctx_set_key (all Q limbs, the context's hybrid parts, folded, Montgomery form):
- * replaces generate_rotation_key_hybrid (src/ckks/context/rotation_key_generation.cpp:92-199) and
- * generate_conjugation_key_hybrid (src/ckks/context/conjugation_key_generation.cpp:63-167).
- * a ([part][nq + np][N] canonical residues, evaluation form) and e ([part][N] integers) are the
- * mask and noise, both given or both null; when null they are drawn on the device from `seed`
- * (uniform mask; rounded normal noise of deviation sigma; a statistical generator, so a
- * deployment that needs cryptographic randomness passes its own a and e).  out (optional, host)
- * receives the key in the wg_ctx_set_key layout. */
-int wg_keygen_automorphism(wg_context* ctx, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a,
+/* Generate a rotation (WG_KEY_ROTATION, `rotation`), conjugation (WG_KEY_CONJ) or
+ * relinearisation (WG_KEY_RELIN) switching key on the device from the ternary secret `secret`
+ * (N coefficients, host memory) and install it like wg_ctx_set_key (all Q limbs, the context's
+ * hybrid parts, folded, Montgomery form): replaces generate_rotation_key_hybrid
+ * (src/ckks/context/rotation_key_generation.cpp:92-199), generate_conjugation_key_hybrid
+ * (src/ckks/context/conjugation_key_generation.cpp:63-167) and encrypt_rlk_hybrid
+ * (src/ckks/context/relinearization_key_generation.cpp:131-199).  a ([part][nq + np][N]
+ * canonical residues, evaluation form) and e ([part][N] integers) are the mask and noise, both
+ * given or both null; when null they are drawn on the device from `seed` (uniform mask; rounded
+ * normal noise of deviation sigma; a statistical generator, so a deployment that needs
+ * cryptographic randomness passes its own a and e).  out (optional, host) receives the key in
+ * the wg_ctx_set_key layout. */
+int wg_keygen_switch_key(wg_context* ctx, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a,
                            const int64_t* e, uint64_t seed, double sigma, uint64_t* out, void* stream);
 int wg_ctx_has_key(const wg_context* ctx, int kind, int64_t rotation);
 /* Allocate the scratch of `stream` now (required before capturing the stream in a graph). */

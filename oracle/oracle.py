@@ -417,20 +417,21 @@ class RefCtx:
         return np.array([0 if v == 0 else (1 if v == 1 else -1) for v in c0.tolist()], dtype=np.int8) \
             if all(v in (0, 1, q0 - 1) for v in c0.tolist()) else None
 
-    def automorphism_key_from_parts(self, kind, rotation, secret, a, e):
-        """The reference's rotation (kind 0) / conjugation (kind 1) key construction with the mask
-        a and noise e given (ref_automorphism_key_from_parts): flat [part][a|b][limbs][N]."""
+    def switch_key_from_parts(self, kind, rotation, secret, a, e):
+        """The reference's rotation (kind 0) / conjugation (kind 1) / relinearisation (kind 2) key
+        construction with the mask
+        a and noise e given (ref_switch_key_from_parts): flat [part][a|b][limbs][N]."""
         R = ref()
-        R.ref_automorphism_key_from_parts.argtypes = [C.c_void_p, C.c_int, C.c_int64,
+        R.ref_switch_key_from_parts.argtypes = [C.c_void_p, C.c_int, C.c_int64,
                                                       np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS"),
                                                       u64p, np.ctypeslib.ndpointer(dtype=np.int64,
                                                                                    flags="C_CONTIGUOUS"), u64p]
         a = np.ascontiguousarray(a, dtype=np.uint64)
         out = np.zeros(2 * a.size, np.uint64)
-        _check(R.ref_automorphism_key_from_parts(self.h, int(kind), int(rotation),
+        _check(R.ref_switch_key_from_parts(self.h, int(kind), int(rotation),
                                                  np.ascontiguousarray(secret, dtype=np.int8), a,
                                                  np.ascontiguousarray(e, dtype=np.int64), out),
-               "ref_automorphism_key_from_parts")
+               "ref_switch_key_from_parts")
         return out
 
     def hoisted_rotations(self, level, b, a, rots):

@@ -254,13 +254,15 @@ int ref_ctx_map(void* h, int kind, int64_t rot, uint64_t* map_out) {
     });
 }
 
-// The rotation (kind 0) or conjugation (kind 1) switching key that generate_rotation_key_hybrid
-// (src/ckks/context/rotation_key_generation.cpp:92-199) / generate_conjugation_key_hybrid
-// (conjugation_key_generation.cpp) build from `secret` (N ternary coefficients), with the mask
+// The rotation (kind 0), conjugation (kind 1) or relinearisation (kind 2) switching key that
+// generate_rotation_key_hybrid (src/ckks/context/rotation_key_generation.cpp:92-199) /
+// generate_conjugation_key_hybrid (conjugation_key_generation.cpp) / encrypt_rlk_hybrid
+// (relinearization_key_generation.cpp:131-199, through ckks_encrypt_custom_eval) build from
+// `secret` (N ternary coefficients), with the mask
 // `a` ([part][limbs][N], canonical, evaluation form) and the noise `e` ([part][N] integers)
 // given instead of drawn: the same steps on the reference's own NTT, pointwise, folding and
 // Montgomery helpers.  out: [part][a|b][limbs][N] as the context stores keys.
-int ref_automorphism_key_from_parts(void* h, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a,
+int ref_switch_key_from_parts(void* h, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a,
                                     const int64_t* e, uint64_t* out) {
     return guarded([&] {
         const auto& c = static_cast<RefCtx*>(h)->ctx;
@@ -284,12 +286,15 @@ int ref_automorphism_key_from_parts(void* h, int kind, int64_t rotation, const i
             return y;
         };
         const MyVector<int8_t> s(secret, secret + N);
-        MyVector<int8_t> x, y;  // b = P x (own limbs) + e - a y
+        MyVector<int8_t> x, y;  // b = P x (own limbs) + e - a y; kind 2: P s^2 + e - a s
         if (kind == 0) {
             x = s;
             y = automorph(s, rotation_automorphism_index(N, -rotation));
-        } else {
+        } else if (kind == 1) {
             x = automorph(s, conjugation_automorphism_index(N));
+            y = s;
+        } else {
+            x = s;
             y = s;
         }
         const auto x_qup = ntt_secret_key(x, tw, N, qup);
@@ -306,6 +311,8 @@ int ref_automorphism_key_from_parts(void* h, int kind, int64_t rotation, const i
             MyVector<uint64_t> b_poly(N * T, 0);
             for (size_t i = s0; i < s1; ++i) {
                 std::copy(x_qup[i].begin(), x_qup[i].end(), b_poly.data() + i * N);
+                // encrypt_rlk_hybrid (relinearization_key_generation.cpp:131-199): s times s first
+                if (kind == 2) pointwise_multiply_inplace_dispatch(b_poly.data() + i * N, x_qup[i].data(), N, qup[i], tw[i]);
                 pointwise_multiply_scalar_inplace_dispatch(b_poly.data() + i * N, p_mod_m[i], N, qup[i], tw[i]);
             }
             MyVector<uint64_t> a_poly(a + part_index * T * N, a + (part_index + 1) * T * N);

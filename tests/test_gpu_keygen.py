@@ -1,14 +1,17 @@
-"""Rotation and conjugation switching keys generated on the device (wg_keygen_automorphism) on the
-walsh15 chain (N = 2^15, 13 Q limbs, 4 P limbs, dnum 3) with the reference context's own secret:
+"""Rotation, conjugation and relinearisation switching keys generated on the device
+(wg_keygen_switch_key) on the walsh15 chain (N = 2^15, 13 Q limbs, 4 P limbs, dnum 3) with the
+reference context's own secret:
 
 * with the mask and noise given, the device key equals, word for word, the key the reference's
   construction (generate_rotation_key_hybrid, rotation_key_generation.cpp:92-199, and
-  generate_conjugation_key_hybrid, conjugation_key_generation.cpp:63-167) makes from the same
+  generate_conjugation_key_hybrid, conjugation_key_generation.cpp:63-167, and encrypt_rlk_hybrid,
+  relinearization_key_generation.cpp:131-199) makes from the same
   mask and noise on its own NTT, pointwise, folding and Montgomery helpers (the harness passes
   them in place of its random draws);
-* with mask and noise drawn on the device, a rotation through the installed key and the same
-  rotation through the reference's key (its own random draws) decrypt to the same values: their
-  difference under the secret is key-switching noise, far below the modulus."""
+* with mask and noise drawn on the device, a rotation (and a relinearisation) through the
+  installed key and the same operation through the reference's key (its own random draws)
+  decrypt to the same values: their difference under the secret is key-switching noise, far
+  below the modulus."""
 import numpy as np
 import pytest
 
@@ -27,7 +30,8 @@ def setup(wg, ref_mod):
     return R, ctx, s
 
 
-@pytest.mark.parametrize("kind,rotation", [("rotation", 1), ("rotation", -512), ("conjugation", 0)])
+@pytest.mark.parametrize("kind,rotation", [("rotation", 1), ("rotation", -512), ("conjugation", 0),
+                                           ("relinearisation", 0)])
 def test_key_from_given_mask_and_noise_matches_reference(wg, setup, kind, rotation):
     R, ctx, s = setup
     N, L, K = R.N, len(R.q), len(R.p)
@@ -36,9 +40,10 @@ def test_key_from_given_mask_and_noise_matches_reference(wg, setup, kind, rotati
     mods = np.concatenate([R.q, R.p]).astype(np.uint64)
     a = (rng.integers(0, 1 << 62, (parts, L + K, N), dtype=np.uint64) % mods[None, :, None]).astype(np.uint64)
     e = np.round(rng.normal(0.0, 3.2, (parts, N))).astype(np.int64)
-    want = R.automorphism_key_from_parts(0 if kind == "rotation" else 1, rotation, s, a, e)
-    wkind = wg.WG_KEY_ROTATION if kind == "rotation" else wg.WG_KEY_CONJ
-    got = ctx.keygen_automorphism(wkind, rotation, s, a=a, e=e, want_key=True)
+    ref_kind = {"rotation": 0, "conjugation": 1, "relinearisation": 2}[kind]
+    want = R.switch_key_from_parts(ref_kind, rotation, s, a, e)
+    wkind = {"rotation": wg.WG_KEY_ROTATION, "conjugation": wg.WG_KEY_CONJ, "relinearisation": wg.WG_KEY_RELIN}[kind]
+    got = ctx.keygen_switch_key(wkind, rotation, s, a=a, e=e, want_key=True)
     assert got.size == want.size
     assert (got == want).all(), int((got != want).sum())
 
@@ -60,7 +65,7 @@ def test_sampled_key_rotates_like_the_reference_key(wg, setup, ref_mod):
 
     R, ctx, s = setup
     N, level = R.N, 6
-    ctx.keygen_automorphism(wg.WG_KEY_ROTATION, 3, s, seed=2026)
+    ctx.keygen_switch_key(wg.WG_KEY_ROTATION, 3, s, seed=2026)
     n = (level + 1) * N
     rng = np.random.default_rng(3)
     qc = np.repeat(R.q[: level + 1], N)
@@ -77,3 +82,25 @@ def test_sampled_key_rotates_like_the_reference_key(wg, setup, ref_mod):
     assert bits < 20, bits  # random residues would reach the size of q0 (36 bits)
     # and the keys themselves differ (independent draws)
     assert not (got[1] == want[1]).all()
+
+
+def test_sampled_relin_key_relinearises_like_the_reference_key(wg, setup, ref_mod):
+    import torch
+
+    R, ctx, s = setup
+    N, level = R.N, 5
+    ctx.keygen_switch_key(wg.WG_KEY_RELIN, 0, s, seed=77)
+    n = (level + 1) * N
+    rng = np.random.default_rng(5)
+    qc = np.repeat(R.q[: level + 1], N)
+    draw = lambda: (rng.integers(0, 1 << 62, n, dtype=np.uint64) % qc).astype(np.uint64)
+    c0, c1, c2 = draw(), draw(), draw()
+    d0, d1, d2 = wg.to_device(c0), wg.to_device(c1), wg.to_device(c2)
+    ctx.relin(level, d0, d1, d2)
+    torch.cuda.synchronize()
+    got = (wg.to_host(d0), wg.to_host(d1))
+    want = R.relin(level, c0, c1, c2)
+    sk = np.zeros(len(R.q) * N, np.uint64)
+    ref_mod.ref().ref_ctx_secret(R.h, sk)
+    bits = _centered_limb0_error(R, sk[:N].astype(object), got, want[:2])
+    assert bits < 20, bits
