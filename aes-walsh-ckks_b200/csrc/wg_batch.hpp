@@ -135,7 +135,11 @@ void bootstrap_pair(Context& c, const BootstrapParams& p, const S2cPlan* s2c, si
 // (wg_keygen.cu); mask a ([part][QP limb][N]) and noise e ([part][N]) from the caller, or drawn
 // from `seed` when both are null; out_host (optional) receives the key as stored.
 void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a_host,
-                         const int64_t* e_host, uint64_t seed, double sigma, uint64_t* out_host, cudaStream_t s);
+                       const int64_t* e_host, uint64_t seed, double sigma, uint64_t* out_host, cudaStream_t s);
+// The bootstrapping secret switches (wg_keygen.cu): WG_KEY_SPARSE_TO_DENSE as a hybrid key from
+// `source` to `target`, WG_KEY_DENSE_TO_SPARSE as the compact level-0 key over (q0, p0).
+void keygen_secret_switch(Context& c, int kind, const int8_t* source, const int8_t* target, const uint64_t* a_host,
+                          const int64_t* e_host, uint64_t seed, double sigma, uint64_t* out_host, cudaStream_t s);
 
 // AES-128-CTR on lazy bits with the XBOOT S-box and pair bootstraps (wg_xboot.cu).
 struct XbootAesArgs {

@@ -211,6 +211,11 @@ int wg_keygen_switch_key(wg_context* ctx, int kind, int64_t rotation, const int8
     return guard([&] { wg::keygen_switch_key(C(ctx), kind, rotation, secret, a, e, seed, sigma, out, S(stream)); });
 }
 
+int wg_keygen_secret_switch(wg_context* ctx, int kind, const int8_t* source, const int8_t* target, const uint64_t* a,
+                            const int64_t* e, uint64_t seed, double sigma, uint64_t* out, void* stream) {
+    return guard([&] { wg::keygen_secret_switch(C(ctx), kind, source, target, a, e, seed, sigma, out, S(stream)); });
+}
+
 int wg_ctx_has_key(const wg_context* ctx, int kind, int64_t rotation) {
     if (!ctx || !ctx->c) return 0;
     const int64_t r = kind == WG_KEY_ROTATION ? normalize_rotation(*ctx->c, rotation) : 0;

@@ -24,6 +24,8 @@
 // randomness through `a` and `e`.
 #include <cmath>
 #include <stdexcept>
+#include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/walsh_gpu.h"
@@ -165,55 +167,61 @@ void run_jobs(Context& c, const std::vector<Job>& jobs, Kernel kernel, double by
     check_cuda(cudaGetLastError(), "key generation");
 }
 
-}  // namespace
+// Shape of a key: the moduli of its limbs (table indices), per limb P mod m (used on the own Q
+// limbs of a part) and the fold-and-radix constant, the parts' own Q limb ranges.
+struct KeyShape {
+    std::vector<int> mods;
+    std::vector<uint64_t> pm, cst;
+    std::vector<std::pair<size_t, size_t>> ranges;
+    size_t key_level = 0;
+};
 
-void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a_host,
-                         const int64_t* e_host, uint64_t seed, double sigma, uint64_t* out_host, cudaStream_t s) {
-    if (kind != WG_KEY_ROTATION && kind != WG_KEY_CONJ && kind != WG_KEY_RELIN)
-        throw std::invalid_argument("wg_keygen: only rotation, conjugation and relinearisation keys are generated");
-    if (!secret) throw std::invalid_argument("wg_keygen: null secret");
-    if (!a_host != !e_host) throw std::invalid_argument("wg_keygen: give both the mask and the noise, or neither");
-    const size_t N = c.N, L = c.nq, K = c.np, T = L + K, slots = N / 2;
-    const size_t parts = c.parts_at(L - 1);
-    int64_t r = 0;
-    if (kind == WG_KEY_ROTATION) {
-        r = rotation % (int64_t)slots;
-        if (r < 0) r += (int64_t)slots;
-        if (r == 0) throw std::invalid_argument("wg_keygen: zero rotation needs no key");
-    }
-    if (!a_host && !(sigma > 0.0 && sigma < 1e6)) throw std::invalid_argument("wg_keygen: invalid noise deviation");
-    for (size_t i = 0; i < N; ++i)
-        if (secret[i] < -1 || secret[i] > 1) throw std::invalid_argument("wg_keygen: secret must be ternary");
-    // (x, y): b = P x + e - a y
-    std::vector<int8_t> x, y;
-    if (kind == WG_KEY_ROTATION) {
-        x.assign(secret, secret + N);
-        // rotation_automorphism_index(N, -r) = 5^(slots - r) mod 2N
-        y = automorph_secret(secret, N, host::powmod(5, (uint64_t)((int64_t)slots - r) % slots, 2 * N));
-    } else if (kind == WG_KEY_RELIN) {
-        x.assign(secret, secret + N);  // squared limb by limb in the evaluation domain
-        y.assign(secret, secret + N);
-    } else {
-        x = automorph_secret(secret, N, 2 * N - 1);
-        y.assign(secret, secret + N);
-    }
-    // per-limb constants
-    std::vector<uint64_t> pm(T), cst(T);
-    for (size_t i = 0; i < T; ++i) {
+uint64_t radix_mod(uint64_t m) { return (uint64_t)(((unsigned __int128)1 << 64) % m); }
+
+// every Q limb and P limb, the context's hybrid parts (ckks_fold_hybrid_switch_key_constants
+// over all P moduli)
+KeyShape full_shape(const Context& c) {
+    KeyShape k;
+    const size_t L = c.nq, K = c.np;
+    for (size_t i = 0; i < L + K; ++i) {
         const uint64_t m = i < L ? c.q[i] : c.p[i - L];
         uint64_t prod = 1, phat = 1;
         for (size_t j = 0; j < K; ++j) {
             prod = host::mulmod(prod, c.p[j] % m, m);
             if (i >= L && j != i - L) phat = host::mulmod(phat, c.p[j] % m, m);
         }
-        pm[i] = prod;
-        const uint64_t fold = i < L ? inv_mod(prod, m) : inv_mod(phat, m);
-        const uint64_t radix = (uint64_t)(((unsigned __int128)1 << 64) % m);
-        cst[i] = host::mulmod(fold, radix, m);
+        k.mods.push_back((int)i);  // P limbs follow the Q limbs in the modulus table
+        k.pm.push_back(prod);
+        k.cst.push_back(host::mulmod(i < L ? inv_mod(prod, m) : inv_mod(phat, m), radix_mod(m), m));
     }
+    for (size_t part = 0; part < c.parts_at(L - 1); ++part)
+        k.ranges.push_back({part * c.alpha, std::min((part + 1) * c.alpha, L)});
+    k.key_level = L - 1;
+    return k;
+}
+
+// the compact level-0 key over (q0, p0) (generate_secret_key_switch_key_q0p0_hybrid: the
+// plaintext is the source times p0 on q0, folded over {q0} and {p0} alone)
+KeyShape q0p0_shape(const Context& c) {
+    KeyShape k;
+    const uint64_t q0 = c.q[0], p0 = c.p[0];
+    k.mods = {0, (int)c.nq};
+    k.pm = {p0 % q0, 0};
+    k.cst = {host::mulmod(inv_mod(p0 % q0, q0), radix_mod(q0), q0), radix_mod(p0)};
+    k.ranges = {{0, 1}};
+    k.key_level = 0;
+    return k;
+}
+
+// b = P x + e - a y per part and limb (x squared limb by limb when `square`), then a and b
+// times the limb's constant; returns the device key [part][a|b][limbs][N]
+KeyEntry build_key(Context& c, const KeyShape& k, const std::vector<int8_t>& x, const std::vector<int8_t>& y,
+                   bool square, const uint64_t* a_host, const int64_t* e_host, uint64_t key_seed, double sigma,
+                   uint64_t* out_host, cudaStream_t s) {
+    const size_t N = c.N, T = k.mods.size(), parts = k.ranges.size();
     check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
     // device scratch: x, y limbs [2][T][N], mask [parts][T][N], noise limbs [parts][T][N], the
-    // secrets' bytes [2][N] and the noise integers [parts][N]
+    // noise integers [parts][N] and the secrets' bytes [2][N]
     const size_t limb_words = T * N;
     const size_t words = 2 * limb_words + 2 * parts * limb_words + parts * N + (2 * N + 7) / 8;
     uint64_t* ws = nullptr;
@@ -227,10 +235,10 @@ void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* sec
     uint64_t* de = da + parts * limb_words;
     int64_t* dei = reinterpret_cast<int64_t*>(de + parts * limb_words);
     int8_t* dsec = reinterpret_cast<int8_t*>(dei + parts * N);
-    size_t key_words = parts * 2 * limb_words;
+    const size_t key_words = parts * 2 * limb_words;
     KeyEntry entry;
     entry.parts = parts;
-    entry.key_level = L - 1;
+    entry.key_level = k.key_level;
     if (cudaMalloc((void**)&entry.d_data, key_words * 8) != cudaSuccess) {
         cudaGetLastError();
         cudaFreeAsync(ws, s);
@@ -243,27 +251,24 @@ void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* sec
             check_cuda(cudaMemcpyAsync(da, a_host, parts * limb_words * 8, cudaMemcpyHostToDevice, s), "wg_keygen upload");
             check_cuda(cudaMemcpyAsync(dei, e_host, parts * N * 8, cudaMemcpyHostToDevice, s), "wg_keygen upload");
         }
-        auto mod_of = [&](size_t i) { return (int)i; };  // P limbs follow the Q limbs in the modulus table
         std::vector<SecretJob> sec;
         std::vector<NttJob> ntt;
         for (size_t i = 0; i < T; ++i) {
-            sec.push_back({dsec, dx + i * N, mod_of(i), 0});
-            sec.push_back({dsec + N, dy + i * N, mod_of(i), 0});
-            ntt.push_back({dx + i * N, dx + i * N, mod_of(i), 0});
-            ntt.push_back({dy + i * N, dy + i * N, mod_of(i), 0});
+            sec.push_back({dsec, dx + i * N, k.mods[i], 0});
+            sec.push_back({dsec + N, dy + i * N, k.mods[i], 0});
+            ntt.push_back({dx + i * N, dx + i * N, k.mods[i], 0});
+            ntt.push_back({dy + i * N, dy + i * N, k.mods[i], 0});
         }
         std::vector<UniformJob> uni;
         std::vector<NoiseJob> noise;
         for (size_t part = 0; part < parts; ++part)
             for (size_t i = 0; i < T; ++i) {
-                uni.push_back({da + (part * T + i) * N, (uint64_t)(part * T + i), mod_of(i), 0});
-                noise.push_back({dei + part * N, de + (part * T + i) * N, mod_of(i), 0});
-                ntt.push_back({de + (part * T + i) * N, de + (part * T + i) * N, mod_of(i), 0});
+                uni.push_back({da + (part * T + i) * N, (uint64_t)(part * T + i), k.mods[i], 0});
+                noise.push_back({dei + part * N, de + (part * T + i) * N, k.mods[i], 0});
+                ntt.push_back({de + (part * T + i) * N, de + (part * T + i) * N, k.mods[i], 0});
             }
         run_jobs(c, sec, kb_secret_limbs, 9.0 * N, s);
         if (!a_host) {
-            // distinct streams per key (kind, rotation) so that keys of one seed differ
-            const uint64_t key_seed = seed ^ ((uint64_t)kind << 56) ^ ((uint64_t)r * 0xA24BAED4963EE407ull);
             JobTable t;
             const UniformJob* j = t.add(uni);
             t.upload(c, s);
@@ -284,7 +289,7 @@ void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* sec
         }
         std::vector<AssembleJob> asm_jobs;
         for (size_t part = 0; part < parts; ++part) {
-            const size_t s0 = part * c.alpha, s1 = std::min(s0 + c.alpha, L);
+            const size_t s0 = k.ranges[part].first, s1 = k.ranges[part].second;
             uint64_t* key_a = entry.d_data + (part * 2 + 0) * limb_words;
             uint64_t* key_b = entry.d_data + (part * 2 + 1) * limb_words;
             for (size_t i = 0; i < T; ++i) {
@@ -295,10 +300,10 @@ void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* sec
                 jb.e = de + (part * T + i) * N;
                 jb.a_out = key_a + i * N;
                 jb.b_out = key_b + i * N;
-                jb.pm = (i >= s0 && i < s1) ? pm[i] : 0;
-                jb.c = cst[i];
-                jb.mod = mod_of(i);
-                jb.square = kind == WG_KEY_RELIN ? 1 : 0;
+                jb.pm = (i >= s0 && i < s1) ? k.pm[i] : 0;
+                jb.c = k.cst[i];
+                jb.mod = k.mods[i];
+                jb.square = square ? 1 : 0;
                 asm_jobs.push_back(jb);
             }
         }
@@ -315,6 +320,10 @@ void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* sec
         cudaFree(entry.d_data);
         throw;
     }
+    return entry;
+}
+
+void install_key(Context& c, int kind, int64_t r, const KeyEntry& entry) {
     auto it = c.keys.find({kind, r});
     if (it != c.keys.end()) {
         cudaFree(it->second.d_data);
@@ -322,6 +331,63 @@ void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* sec
     } else {
         c.keys.emplace(std::make_pair(kind, r), entry);
     }
+}
+
+void check_ternary(const int8_t* s, size_t N, const char* what) {
+    if (!s) throw std::invalid_argument(std::string("wg_keygen: null ") + what);
+    for (size_t i = 0; i < N; ++i)
+        if (s[i] < -1 || s[i] > 1) throw std::invalid_argument(std::string("wg_keygen: ") + what + " must be ternary");
+}
+
+}  // namespace
+
+void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a_host,
+                       const int64_t* e_host, uint64_t seed, double sigma, uint64_t* out_host, cudaStream_t s) {
+    if (kind != WG_KEY_ROTATION && kind != WG_KEY_CONJ && kind != WG_KEY_RELIN)
+        throw std::invalid_argument("wg_keygen: only rotation, conjugation and relinearisation keys are generated");
+    check_ternary(secret, c.N, "secret");
+    if (!a_host != !e_host) throw std::invalid_argument("wg_keygen: give both the mask and the noise, or neither");
+    if (!a_host && !(sigma > 0.0 && sigma < 1e6)) throw std::invalid_argument("wg_keygen: invalid noise deviation");
+    const size_t N = c.N, slots = N / 2;
+    int64_t r = 0;
+    if (kind == WG_KEY_ROTATION) {
+        r = rotation % (int64_t)slots;
+        if (r < 0) r += (int64_t)slots;
+        if (r == 0) throw std::invalid_argument("wg_keygen: zero rotation needs no key");
+    }
+    // (x, y): b = P x + e - a y
+    std::vector<int8_t> x, y;
+    if (kind == WG_KEY_ROTATION) {
+        x.assign(secret, secret + N);
+        // rotation_automorphism_index(N, -r) = 5^(slots - r) mod 2N
+        y = automorph_secret(secret, N, host::powmod(5, (uint64_t)((int64_t)slots - r) % slots, 2 * N));
+    } else if (kind == WG_KEY_RELIN) {
+        x.assign(secret, secret + N);  // squared limb by limb in the evaluation domain
+        y.assign(secret, secret + N);
+    } else {
+        x = automorph_secret(secret, N, 2 * N - 1);
+        y.assign(secret, secret + N);
+    }
+    // distinct streams per key (kind, rotation) so that keys of one seed differ
+    const uint64_t key_seed = seed ^ ((uint64_t)kind << 56) ^ ((uint64_t)r * 0xA24BAED4963EE407ull);
+    const KeyEntry entry = build_key(c, full_shape(c), x, y, kind == WG_KEY_RELIN, a_host, e_host, key_seed, sigma,
+                                     out_host, s);
+    install_key(c, kind, r, entry);
+}
+
+void keygen_secret_switch(Context& c, int kind, const int8_t* source, const int8_t* target, const uint64_t* a_host,
+                          const int64_t* e_host, uint64_t seed, double sigma, uint64_t* out_host, cudaStream_t s) {
+    if (kind != WG_KEY_DENSE_TO_SPARSE && kind != WG_KEY_SPARSE_TO_DENSE)
+        throw std::invalid_argument("wg_keygen: secret switches are dense-to-sparse or sparse-to-dense");
+    check_ternary(source, c.N, "source secret");
+    check_ternary(target, c.N, "target secret");
+    if (!a_host != !e_host) throw std::invalid_argument("wg_keygen: give both the mask and the noise, or neither");
+    if (!a_host && !(sigma > 0.0 && sigma < 1e6)) throw std::invalid_argument("wg_keygen: invalid noise deviation");
+    const std::vector<int8_t> x(source, source + c.N), y(target, target + c.N);
+    const uint64_t key_seed = seed ^ ((uint64_t)kind << 56) ^ 0x3C6EF372FE94F82Bull;
+    const KeyShape k = kind == WG_KEY_DENSE_TO_SPARSE ? q0p0_shape(c) : full_shape(c);
+    const KeyEntry entry = build_key(c, k, x, y, false, a_host, e_host, key_seed, sigma, out_host, s);
+    install_key(c, kind, 0, entry);
 }
 
 }  // namespace wg

@@ -104,6 +104,7 @@ def lib() -> C.CDLL:
                                              vp, vp]
         L.wg_xboot_linear_layer.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp]
         L.wg_keygen_switch_key.argtypes = [vp, C.c_int, C.c_int64, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
+        L.wg_keygen_secret_switch.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
         L.wg_serve_create_xboot.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_serve_submit.argtypes = [vp, C.c_char_p, C.c_char_p, sz, vp, vp, C.POINTER(C.c_uint64)]
         L.wg_serve_wait.argtypes = [vp, C.c_uint64, C.c_double, vp]
@@ -498,6 +499,33 @@ class Context:
                                             None if ep is None else ep.ctypes.data, int(seed) & (2**64 - 1),
                                             float(sigma), None if out is None else out.ctypes.data,
                                             _stream(stream)))
+        return out
+
+    def keygen_secret_switch(self, kind, source, target, a=None, e=None, seed=0, sigma=3.2, want_key=False,
+                             stream=None):
+        """Generate and install a bootstrapping secret switch on the device: WG_KEY_SPARSE_TO_DENSE
+        (hybrid key, a [part][nq + np][N], e [part][N]) or WG_KEY_DENSE_TO_SPARSE (compact q0/p0
+        key, a [1][2][N], e [1][N]) from `source` to `target` (N int8 ternary coefficients each).
+        Returns the key as stored when want_key."""
+        src = np.ascontiguousarray(source, dtype=np.int8)
+        tgt = np.ascontiguousarray(target, dtype=np.int8)
+        if src.size != self.N or tgt.size != self.N:
+            raise ValueError("secrets must have N coefficients")
+        compact = kind == WG_KEY_DENSE_TO_SPARSE
+        parts = 1 if compact else self.parts(self.nq - 1)
+        limbs = 2 if compact else self.nq + self.np_
+        ap = ep = None
+        if a is not None:
+            ap = np.ascontiguousarray(a, dtype=np.uint64)
+            ep = np.ascontiguousarray(e, dtype=np.int64)
+            if ap.size != parts * limbs * self.N or ep.size != parts * self.N:
+                raise ValueError("mask / noise sizes do not match the key's parts and limbs")
+        out = np.zeros(parts * 2 * limbs * self.N, np.uint64) if want_key else None
+        _check(lib().wg_keygen_secret_switch(self.h, int(kind), src.ctypes.data, tgt.ctypes.data,
+                                             None if ap is None else ap.ctypes.data,
+                                             None if ep is None else ep.ctypes.data, int(seed) & (2**64 - 1),
+                                             float(sigma), None if out is None else out.ctypes.data,
+                                             _stream(stream)))
         return out
 
     def rotate(self, level, b, a, rotation, stream=None):

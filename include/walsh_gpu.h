@@ -96,6 +96,13 @@ int wg_ctx_set_key(wg_context* ctx, int kind, int64_t rotation, const uint64_t* 
  * the wg_ctx_set_key layout. */
 int wg_keygen_switch_key(wg_context* ctx, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a,
                            const int64_t* e, uint64_t seed, double sigma, uint64_t* out, void* stream);
+/* The bootstrapping secret switches generated the same way: WG_KEY_SPARSE_TO_DENSE from `source`
+ * to `target` as a hybrid key (generate_secret_key_switch_key_hybrid,
+ * src/ckks/context/secret_key_generation.cpp:227-300), WG_KEY_DENSE_TO_SPARSE as the compact
+ * level-0 key over q0 and p0 (generate_secret_key_switch_key_q0p0_hybrid, :302-364; a [1][2][N],
+ * e [1][N]).  Other arguments as for wg_keygen_switch_key. */
+int wg_keygen_secret_switch(wg_context* ctx, int kind, const int8_t* source, const int8_t* target, const uint64_t* a,
+                            const int64_t* e, uint64_t seed, double sigma, uint64_t* out, void* stream);
 int wg_ctx_has_key(const wg_context* ctx, int kind, int64_t rotation);
 /* Allocate the scratch of `stream` now (required before capturing the stream in a graph). */
 int wg_ctx_reserve(wg_context* ctx, void* stream);

@@ -417,19 +417,20 @@ class RefCtx:
         return np.array([0 if v == 0 else (1 if v == 1 else -1) for v in c0.tolist()], dtype=np.int8) \
             if all(v in (0, 1, q0 - 1) for v in c0.tolist()) else None
 
-    def switch_key_from_parts(self, kind, rotation, secret, a, e):
-        """The reference's rotation (kind 0) / conjugation (kind 1) / relinearisation (kind 2) key
-        construction with the mask
+    def switch_key_from_parts(self, kind, rotation, secret, a, e, target=None):
+        """The reference's rotation (kind 0) / conjugation (kind 1) / relinearisation (kind 2) /
+        dense-to-sparse (kind 3, compact q0 p0) / sparse-to-dense (kind 4) key construction (secret
+        switches from `secret` to `target`) with the mask
         a and noise e given (ref_switch_key_from_parts): flat [part][a|b][limbs][N]."""
         R = ref()
-        R.ref_switch_key_from_parts.argtypes = [C.c_void_p, C.c_int, C.c_int64,
-                                                      np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS"),
-                                                      u64p, np.ctypeslib.ndpointer(dtype=np.int64,
-                                                                                   flags="C_CONTIGUOUS"), u64p]
+        i8p = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+        R.ref_switch_key_from_parts.argtypes = [C.c_void_p, C.c_int, C.c_int64, i8p, i8p, u64p,
+                                                np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS"), u64p]
         a = np.ascontiguousarray(a, dtype=np.uint64)
         out = np.zeros(2 * a.size, np.uint64)
+        tgt = np.ascontiguousarray(secret if target is None else target, dtype=np.int8)
         _check(R.ref_switch_key_from_parts(self.h, int(kind), int(rotation),
-                                                 np.ascontiguousarray(secret, dtype=np.int8), a,
+                                                 np.ascontiguousarray(secret, dtype=np.int8), tgt, a,
                                                  np.ascontiguousarray(e, dtype=np.int64), out),
                "ref_switch_key_from_parts")
         return out

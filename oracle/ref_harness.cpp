@@ -254,16 +254,18 @@ int ref_ctx_map(void* h, int kind, int64_t rot, uint64_t* map_out) {
     });
 }
 
-// The rotation (kind 0), conjugation (kind 1) or relinearisation (kind 2) switching key that
-// generate_rotation_key_hybrid (src/ckks/context/rotation_key_generation.cpp:92-199) /
-// generate_conjugation_key_hybrid (conjugation_key_generation.cpp) / encrypt_rlk_hybrid
-// (relinearization_key_generation.cpp:131-199, through ckks_encrypt_custom_eval) build from
-// `secret` (N ternary coefficients), with the mask
+// The rotation (kind 0), conjugation (kind 1), relinearisation (kind 2), dense-to-sparse (kind 3)
+// or sparse-to-dense (kind 4) switching key that generate_rotation_key_hybrid
+// (src/ckks/context/rotation_key_generation.cpp:92-199) / generate_conjugation_key_hybrid
+// (conjugation_key_generation.cpp) / encrypt_rlk_hybrid (relinearization_key_generation.cpp:
+// 131-199, through ckks_encrypt_custom_eval) / generate_secret_key_switch_key_q0p0_hybrid and
+// generate_secret_key_switch_key_hybrid (secret_key_generation.cpp:227-364; source `secret`,
+// target `target`) build from `secret` (N ternary coefficients), with the mask
 // `a` ([part][limbs][N], canonical, evaluation form) and the noise `e` ([part][N] integers)
 // given instead of drawn: the same steps on the reference's own NTT, pointwise, folding and
 // Montgomery helpers.  out: [part][a|b][limbs][N] as the context stores keys.
-int ref_switch_key_from_parts(void* h, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a,
-                                    const int64_t* e, uint64_t* out) {
+int ref_switch_key_from_parts(void* h, int kind, int64_t rotation, const int8_t* secret, const int8_t* target,
+                              const uint64_t* a, const int64_t* e, uint64_t* out) {
     return guarded([&] {
         const auto& c = static_cast<RefCtx*>(h)->ctx;
         const auto& params = c.getParams();
@@ -293,9 +295,39 @@ int ref_switch_key_from_parts(void* h, int kind, int64_t rotation, const int8_t*
         } else if (kind == 1) {
             x = automorph(s, conjugation_automorphism_index(N));
             y = s;
-        } else {
+        } else if (kind == 2) {
             x = s;
             y = s;
+        } else {
+            x = s;  // secret switch from `secret` to `target`
+            y = MyVector<int8_t>(target, target + N);
+        }
+        if (kind == 3) {
+            // generate_secret_key_switch_key_q0p0_hybrid (secret_key_generation.cpp:302-364): the
+            // compact key over (q0, p0), plaintext source * p0 on q0, folded over {q0} and {p0}
+            const MyVector<uint64_t> b01{qm[0], pm[0]}, q0v{qm[0]}, p0v{pm[0]};
+            MyVector<Negacyclic_NTT_Twiddles> t01{c.getTwiddleNtt()[0], c.getPTwiddleNtt()[0]};
+            const auto xs = ntt_secret_key(x, t01, N, b01);
+            const auto ys = ntt_secret_key(y, t01, N, b01);
+            MyVector<uint64_t> ptxt(2 * N, 0);
+            std::copy(xs[0].begin(), xs[0].end(), ptxt.begin());
+            pointwise_multiply_scalar_inplace_dispatch(ptxt.data(), pm[0] % qm[0], N, qm[0], t01[0]);
+            MyVector<uint64_t> a_poly(a, a + 2 * N), e_poly(2 * N);
+            for (size_t i = 0; i < 2; ++i)
+                for (size_t j = 0; j < N; ++j) e_poly[i * N + j] = reduce_i64_mod_q(e[j], b01[i]);
+            ntt_forward_rns_flat_inplace(e_poly.data(), N, 2, b01, t01, false);
+            MyVector<uint64_t> as(N);
+            for (size_t i = 0; i < 2; ++i) {
+                pointwise_multiply_dispatch(a_poly.data() + i * N, ys[i].data(), as.data(), N, b01[i], t01[i]);
+                poly_add_modq_inplace(ptxt.data() + i * N, e_poly.data() + i * N, N, b01[i]);
+                poly_sub_modq_inplace(ptxt.data() + i * N, as.data(), N, b01[i]);
+            }
+            CKKSCiphertext key(N, std::move(a_poly), std::move(ptxt), 1.0, 0);
+            if (params.fold_hybrid_keyswitch) ckks_fold_hybrid_switch_key_constants(key, q0v, p0v, t01);
+            if (params.montgomery) ckks_convert_switch_key_to_montgomery_inplace(key, b01, t01);
+            copy_out(key.getA(), out);
+            copy_out(key.getB(), out + 2 * N);
+            return;
         }
         const auto x_qup = ntt_secret_key(x, tw, N, qup);
         const auto y_qup = ntt_secret_key(y, tw, N, qup);

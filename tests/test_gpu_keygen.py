@@ -4,8 +4,10 @@ reference context's own secret:
 
 * with the mask and noise given, the device key equals, word for word, the key the reference's
   construction (generate_rotation_key_hybrid, rotation_key_generation.cpp:92-199, and
-  generate_conjugation_key_hybrid, conjugation_key_generation.cpp:63-167, and encrypt_rlk_hybrid,
-  relinearization_key_generation.cpp:131-199) makes from the same
+  generate_conjugation_key_hybrid, conjugation_key_generation.cpp:63-167, encrypt_rlk_hybrid,
+  relinearization_key_generation.cpp:131-199, and the bootstrapping secret switches of
+  secret_key_generation.cpp:227-364, the dense-to-sparse one as the compact q0/p0 key) makes
+  from the same
   mask and noise on its own NTT, pointwise, folding and Montgomery helpers (the harness passes
   them in place of its random draws);
 * with mask and noise drawn on the device, a rotation (and a relinearisation) through the
@@ -104,3 +106,26 @@ def test_sampled_relin_key_relinearises_like_the_reference_key(wg, setup, ref_mo
     ref_mod.ref().ref_ctx_secret(R.h, sk)
     bits = _centered_limb0_error(R, sk[:N].astype(object), got, want[:2])
     assert bits < 20, bits
+
+
+@pytest.mark.parametrize("kind", ["sparse_to_dense", "dense_to_sparse"])
+def test_secret_switch_key_matches_reference(wg, setup, kind):
+    R, ctx, s = setup
+    N, L, K = R.N, len(R.q), len(R.p)
+    rng = np.random.default_rng(11 if kind == "sparse_to_dense" else 13)
+    sparse = np.zeros(N, np.int8)
+    sparse[rng.choice(N, 32, replace=False)] = rng.choice([-1, 1], 32).astype(np.int8)
+    if kind == "sparse_to_dense":
+        source, target, ref_kind, wkind = sparse, s, 4, wg.WG_KEY_SPARSE_TO_DENSE
+        mods = np.concatenate([R.q, R.p]).astype(np.uint64)
+        parts = ctx.parts(L - 1)
+    else:
+        source, target, ref_kind, wkind = s, sparse, 3, wg.WG_KEY_DENSE_TO_SPARSE
+        mods = np.array([R.q[0], R.p[0]], dtype=np.uint64)
+        parts = 1
+    a = (rng.integers(0, 1 << 62, (parts, mods.size, N), dtype=np.uint64) % mods[None, :, None]).astype(np.uint64)
+    e = np.round(rng.normal(0.0, 3.2, (parts, N))).astype(np.int64)
+    want = R.switch_key_from_parts(ref_kind, 0, source, a, e, target=target)
+    got = ctx.keygen_secret_switch(wkind, source, target, a=a, e=e, want_key=True)
+    assert got.size == want.size
+    assert (got == want).all(), int((got != want).sum())
