@@ -136,6 +136,22 @@ void bootstrap_pair(Context& c, const BootstrapParams& p, const S2cPlan* s2c, si
 // from `seed` when both are null; out_host (optional) receives the key as stored.
 void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* secret, const uint64_t* a_host,
                        const int64_t* e_host, uint64_t seed, double sigma, uint64_t* out_host, cudaStream_t s);
+// Secret-key encryption (ckks_encrypt_custom_eval) of `count` evaluation-form plaintexts at
+// `level` under the ternary `secret` (wg_keygen.cu): b = pt + e - a s into out_b / out_a (level +
+// 1 limbs each); mask a ([count][level+1][N]) and noise e ([count][N]) given, or drawn from
+// `seed` when both are null.
+void encrypt_symmetric(Context& c, size_t count, size_t level, const uint64_t* const* pts, const int8_t* secret,
+                       const uint64_t* a_host, const int64_t* e_host, uint64_t seed, double sigma,
+                       uint64_t* const* out_b, uint64_t* const* out_a, cudaStream_t s);
+// ckks_aes128_encrypt_expanded_round_key_bits on the device (wg_xboot.cu): the 1408 bits of the
+// expanded key as constant-slot plaintexts at the parameter scale, encrypted under `secret` at
+// the S2C depth (round 0: first_round_key_level above it); out_b / out_a need room for the
+// level + 1 limbs of each bit.
+void xboot_encrypt_round_key_bits(Context& c, const BootstrapParams& p, const uint8_t* expanded_key,
+                                  size_t first_round_key_level, const int8_t* secret, uint64_t seed, double sigma,
+                                  uint64_t* const* out_b, uint64_t* const* out_a, double* out_scale,
+                                  size_t* out_level, cudaStream_t s);
+
 // The bootstrapping secret switches (wg_keygen.cu): WG_KEY_SPARSE_TO_DENSE as a hybrid key from
 // `source` to `target`, WG_KEY_DENSE_TO_SPARSE as the compact level-0 key over (q0, p0).
 void keygen_secret_switch(Context& c, int kind, const int8_t* source, const int8_t* target, const uint64_t* a_host,

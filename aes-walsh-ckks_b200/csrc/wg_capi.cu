@@ -703,6 +703,37 @@ int wg_xboot_linear_layer(wg_context* ctx, size_t level, const double* in_scale,
     });
 }
 
+int wg_encrypt_symmetric(wg_context* ctx, size_t count, size_t level, const uint64_t* const* pts, const int8_t* secret,
+                         const uint64_t* a, const int64_t* e, uint64_t seed, double sigma, uint64_t* const* out_b,
+                         uint64_t* const* out_a, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_cts(c, count, out_b, out_a, "ckks_encrypt");
+        if (count && !pts) wg::fail(wg::kInvalid, "ckks_encrypt: null plaintext array");
+        for (size_t i = 0; i < count; ++i) check_ptr(pts[i], "ckks_encrypt");
+        wg::encrypt_symmetric(c, count, level, pts, secret, a, e, seed, sigma, out_b, out_a, S(stream));
+    });
+}
+
+int wg_aes_xboot_encrypt_round_key_bits(wg_context* ctx, const wg_bootstrap_params* params,
+                                        const uint8_t* expanded_key, size_t first_round_key_level,
+                                        const int8_t* secret, uint64_t seed, double sigma, uint64_t* const* out_b,
+                                        uint64_t* const* out_a, double* out_scale, size_t* out_level, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(params, "ckks_aes");
+        check_ptr(out_scale, "ckks_aes");
+        check_ptr(out_level, "ckks_aes");
+        check_cts(c, 1408, out_b, out_a, "ckks_aes");
+        wg::BootstrapParams bp;
+        bp.s2c_depth = params->s2c_depth;
+        bp.scale = params->scale;
+        if (!(bp.scale > 0.0)) wg::fail(wg::kInvalid, "ckks_aes: invalid scale");
+        wg::xboot_encrypt_round_key_bits(c, bp, expanded_key, first_round_key_level, secret, seed, sigma, out_b, out_a,
+                                         out_scale, out_level, S(stream));
+    });
+}
+
 int wg_xboot_sbox_coefficients(int64_t* out) {
     return guard([&] {
         check_ptr(out, "ckks_aes");

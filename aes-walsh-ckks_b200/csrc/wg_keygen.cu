@@ -144,6 +144,25 @@ __global__ void __launch_bounds__(kT) kb_key_assemble(const AssembleJob* jobs, i
     j->a_out[k] = barrett_mul(a, j->c, m);
 }
 
+struct EncryptJob {
+    uint64_t* b;          // out
+    const uint64_t* a;    // mask (evaluation form)
+    const uint64_t* pt;   // plaintext (evaluation form)
+    const uint64_t* e;    // noise limb (evaluation form)
+    const uint64_t* s;    // secret limb (evaluation form)
+    int mod, pad;
+};
+
+// ckks_encrypt_custom_eval: b = pt + e - a s
+__global__ void __launch_bounds__(kT) kb_encrypt(const EncryptJob* jobs, int n, const Modulus* mods) {
+    const EncryptJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    const Modulus m = mods[j->mod];
+    const uint64_t q = m.q;
+    j->b[k] = sub_mod(add_mod(j->pt[k], j->e[k], q), barrett_mul(j->a[k], j->s[k], m), q);
+}
+
 uint64_t inv_mod(uint64_t a, uint64_t m) { return host::powmod(a % m, m - 2, m); }  // m prime
 
 // apply_automorphism_to_secret: coefficient i moves to i * index mod 2N, negated past N
@@ -388,6 +407,98 @@ void keygen_secret_switch(Context& c, int kind, const int8_t* source, const int8
     const KeyShape k = kind == WG_KEY_DENSE_TO_SPARSE ? q0p0_shape(c) : full_shape(c);
     const KeyEntry entry = build_key(c, k, x, y, false, a_host, e_host, key_seed, sigma, out_host, s);
     install_key(c, kind, 0, entry);
+}
+
+void encrypt_symmetric(Context& c, size_t count, size_t level, const uint64_t* const* pts, const int8_t* secret,
+                       const uint64_t* a_host, const int64_t* e_host, uint64_t seed, double sigma,
+                       uint64_t* const* out_b, uint64_t* const* out_a, cudaStream_t s) {
+    if (count == 0) return;
+    if (level >= c.nq) throw std::invalid_argument("ckks_encrypt: invalid level");
+    check_ternary(secret, c.N, "secret");
+    if (!a_host != !e_host) throw std::invalid_argument("wg_encrypt: give both the mask and the noise, or neither");
+    if (!a_host && !(sigma > 0.0 && sigma < 1e6)) throw std::invalid_argument("wg_encrypt: invalid noise deviation");
+    const size_t N = c.N, L = level + 1;
+    check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+    constexpr size_t kChunk = 128;  // ciphertexts per pass (bounds the noise scratch)
+    const size_t chunk = std::min(count, kChunk);
+    // scratch: secret limbs [L][N], noise limbs [chunk][L][N], noise integers [chunk][N], secret bytes
+    const size_t words = L * N + chunk * L * N + chunk * N + (N + 7) / 8;
+    uint64_t* ws = nullptr;
+    if (cudaMallocAsync((void**)&ws, words * 8, s) != cudaSuccess) {
+        cudaGetLastError();
+        fail(kNoMemory, "wg_encrypt: scratch allocation failed");
+    }
+    uint64_t* ds = ws;
+    uint64_t* de = ds + L * N;
+    int64_t* dei = reinterpret_cast<int64_t*>(de + chunk * L * N);
+    int8_t* dsec = reinterpret_cast<int8_t*>(dei + chunk * N);
+    try {
+        check_cuda(cudaMemcpyAsync(dsec, secret, N, cudaMemcpyHostToDevice, s), "wg_encrypt upload");
+        std::vector<SecretJob> sec;
+        std::vector<NttJob> sntt;
+        for (size_t l = 0; l < L; ++l) {
+            sec.push_back({dsec, ds + l * N, (int)l, 0});
+            sntt.push_back({ds + l * N, ds + l * N, (int)l, 0});
+        }
+        run_jobs(c, sec, kb_secret_limbs, 9.0 * N, s);
+        {
+            JobTable t;
+            const NttJob* j = t.add(sntt);
+            t.upload(c, s);
+            ntt_jobs(c, t.at(j), (int)sntt.size(), true, s);
+        }
+        for (size_t c0 = 0; c0 < count; c0 += chunk) {
+            const size_t nc = std::min(chunk, count - c0);
+            std::vector<UniformJob> uni;
+            std::vector<NoiseJob> noise;
+            std::vector<NttJob> entt;
+            std::vector<EncryptJob> enc;
+            for (size_t i = 0; i < nc; ++i)
+                for (size_t l = 0; l < L; ++l) {
+                    uni.push_back({out_a[c0 + i] + l * N, (uint64_t)((c0 + i) * L + l), (int)l, 0});
+                    noise.push_back({dei + i * N, de + (i * L + l) * N, (int)l, 0});
+                    entt.push_back({de + (i * L + l) * N, de + (i * L + l) * N, (int)l, 0});
+                    enc.push_back({out_b[c0 + i] + l * N, out_a[c0 + i] + l * N, pts[c0 + i] + l * N,
+                                   de + (i * L + l) * N, ds + l * N, (int)l, 0});
+                }
+            if (a_host) {
+                for (size_t i = 0; i < nc; ++i)
+                    check_cuda(cudaMemcpyAsync(out_a[c0 + i], a_host + (c0 + i) * L * N, L * N * 8,
+                                               cudaMemcpyHostToDevice, s), "wg_encrypt upload");
+                check_cuda(cudaMemcpyAsync(dei, e_host + c0 * N, nc * N * 8, cudaMemcpyHostToDevice, s),
+                           "wg_encrypt upload");
+            } else {
+                const uint64_t key_seed = seed ^ 0x6A09E667F3BCC909ull ^ ((uint64_t)level << 48);
+                JobTable t;
+                const UniformJob* j = t.add(uni);
+                t.upload(c, s);
+                {
+                    Probe probe(kClsElementwise, 8.0 * N * uni.size(), s);
+                    kb_uniform<<<grid_for(c, uni.size()), kT, 0, s>>>(t.at(j), (int)uni.size(), c.d_mod, key_seed);
+                }
+                kb_gauss<<<(unsigned)((nc * N + kT - 1) / kT), kT, 0, s>>>(dei, nc * N, key_seed, (uint64_t)c0 + 1,
+                                                                          sigma);
+                check_cuda(cudaGetLastError(), "wg_encrypt sampling");
+            }
+            run_jobs(c, noise, kb_noise_limbs, 16.0 * N, s);
+            {
+                JobTable t;
+                const NttJob* j = t.add(entt);
+                t.upload(c, s);
+                ntt_jobs(c, t.at(j), (int)entt.size(), true, s);
+            }
+            run_jobs(c, enc, kb_encrypt, 40.0 * N, s);
+            // the next chunk's uploads and draws reuse the noise scratch only after this one
+            // has been consumed (stream order)
+        }
+        check_cuda(cudaFreeAsync(ws, s), "wg_encrypt scratch");
+        ws = nullptr;
+        check_cuda(cudaStreamSynchronize(s), "wg_encrypt");
+    } catch (...) {
+        if (ws) cudaFreeAsync(ws, s);
+        cudaStreamSynchronize(s);
+        throw;
+    }
 }
 
 }  // namespace wg

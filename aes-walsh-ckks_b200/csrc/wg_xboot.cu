@@ -645,4 +645,36 @@ void xboot_linear_layer(Context& c, size_t level, const double* in_scale, uint64
     for (size_t bit = 0; bit < kStateBits; ++bit) out_scale[bit] = static_cast<double>(aes.state(bit).scale);
 }
 
+void xboot_encrypt_round_key_bits(Context& c, const BootstrapParams& p, const uint8_t* expanded_key,
+                                  size_t first_round_key_level, const int8_t* secret, uint64_t seed, double sigma,
+                                  uint64_t* const* out_b, uint64_t* const* out_a, double* out_scale,
+                                  size_t* out_level, cudaStream_t s) {
+    if (!expanded_key) throw std::invalid_argument("ckks_aes: null expanded key");
+    const size_t base = p.s2c_depth;
+    if (base + first_round_key_level > c.nq - 1)
+        throw std::invalid_argument("ckks_aes: invalid encryption level for first round key bits");
+    constexpr size_t kKeyBits = 11 * kStateBits;
+    DeviceOps ops(c, 1, s);
+    // round 0 at base + first_round_key_level, the other rounds at base; plaintext of the bit's
+    // value in every slot at the parameter scale (closed-form constant encodings)
+    for (int round0 = 1; round0 >= 0; --round0) {
+        const size_t level = round0 ? base + first_round_key_level : base;
+        const size_t k0 = round0 ? 0 : kStateBits, k1 = round0 ? kStateBits : kKeyBits;
+        const uint64_t* pt[2] = {ops.constant_plaintext(level + 1, 0.0, 0.0, p.scale),
+                                 ops.constant_plaintext(level + 1, 1.0, 0.0, p.scale)};
+        std::vector<const uint64_t*> pts;
+        std::vector<uint64_t*> ob, oa;
+        for (size_t k = k0; k < k1; ++k) {
+            const int bit = (expanded_key[k / 8] >> (k % 8)) & 1;
+            pts.push_back(pt[bit]);
+            ob.push_back(out_b[k]);
+            oa.push_back(out_a[k]);
+            out_scale[k] = p.scale;
+            out_level[k] = level;
+        }
+        encrypt_symmetric(c, pts.size(), level, pts.data(), secret, nullptr, nullptr, seed + (uint64_t)round0, sigma,
+                          ob.data(), oa.data(), s);
+    }
+}
+
 }  // namespace wg

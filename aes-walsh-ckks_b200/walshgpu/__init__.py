@@ -105,6 +105,9 @@ def lib() -> C.CDLL:
         L.wg_xboot_linear_layer.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp]
         L.wg_keygen_switch_key.argtypes = [vp, C.c_int, C.c_int64, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
         L.wg_keygen_secret_switch.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
+        L.wg_encrypt_symmetric.argtypes = [vp, sz, sz, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp, vp]
+        L.wg_aes_xboot_encrypt_round_key_bits.argtypes = [vp, vp, vp, sz, vp, C.c_uint64, C.c_double, vp, vp, vp,
+                                                          vp, vp]
         L.wg_serve_create_xboot.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_serve_submit.argtypes = [vp, C.c_char_p, C.c_char_p, sz, vp, vp, C.POINTER(C.c_uint64)]
         L.wg_serve_wait.argtypes = [vp, C.c_uint64, C.c_double, vp]
@@ -500,6 +503,38 @@ class Context:
                                             float(sigma), None if out is None else out.ctypes.data,
                                             _stream(stream)))
         return out
+
+    def encrypt_symmetric(self, level, pts, secret, outs, a=None, e=None, seed=0, sigma=3.2, stream=None):
+        """Secret-key encryption of evaluation-form plaintexts (device tensors, level+1 limbs)
+        into outs = [(b, a)] device tensors (wg_encrypt_symmetric); a ([count][level+1][N]) and
+        e ([count][N]) given, or drawn from `seed`."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        pp, ob, oa = arr(pts), arr([x[0] for x in outs]), arr([x[1] for x in outs])
+        sec = np.ascontiguousarray(secret, dtype=np.int8)
+        ap = None if a is None else np.ascontiguousarray(a, dtype=np.uint64)
+        ep = None if e is None else np.ascontiguousarray(e, dtype=np.int64)
+        _check(lib().wg_encrypt_symmetric(self.h, len(pts), level, pp.ctypes.data, sec.ctypes.data,
+                                          None if ap is None else ap.ctypes.data,
+                                          None if ep is None else ep.ctypes.data, int(seed) & (2**64 - 1),
+                                          float(sigma), ob.ctypes.data, oa.ctypes.data, _stream(stream)))
+
+    def aes_xboot_encrypt_round_key_bits(self, params, expanded_key, first_round_key_level, secret, outs, seed=0,
+                                         sigma=3.2, stream=None):
+        """The XBOOT AES's 1408 encrypted round-key bits on the device
+        (wg_aes_xboot_encrypt_round_key_bits) into outs = [(b, a)] device tensors; returns
+        (scales, levels)."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        ob, oa = arr([x[0] for x in outs]), arr([x[1] for x in outs])
+        sec = np.ascontiguousarray(secret, dtype=np.int8)
+        ek = np.frombuffer(bytes(expanded_key), dtype=np.uint8).copy()
+        sc = np.zeros(1408, np.float64)
+        lv = np.zeros(1408, np.uintp)
+        _check(lib().wg_aes_xboot_encrypt_round_key_bits(self.h, C.byref(params), ek.ctypes.data,
+                                                         int(first_round_key_level), sec.ctypes.data,
+                                                         int(seed) & (2**64 - 1), float(sigma), ob.ctypes.data,
+                                                         oa.ctypes.data, sc.ctypes.data, lv.ctypes.data,
+                                                         _stream(stream)))
+        return sc, lv.astype(np.int64)
 
     def keygen_secret_switch(self, kind, source, target, a=None, e=None, seed=0, sigma=3.2, want_key=False,
                              stream=None):

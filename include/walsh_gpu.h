@@ -366,6 +366,26 @@ int wg_xboot_linear_layer(wg_context* ctx, size_t level, const double* in_scale,
                           const size_t* key_levels, int mix, uint64_t* const* out_b, uint64_t* const* out_a,
                           double* out_scale, void* stream);
 
+/* Secret-key encryption on the device of `count` evaluation-form plaintexts (device pointers,
+ * level + 1 limbs each) under the ternary `secret` (host, N coefficients): b = pt + e - a s into
+ * out_b / out_a; replaces ckks_encrypt (src/ckks/encoding/ckks_encoding.cpp:522-566, through
+ * ckks_encrypt_custom_eval :478-520).  a ([count][level + 1][N] canonical residues) and e
+ * ([count][N] integers) both given or both null (then drawn from `seed`, as for
+ * wg_keygen_switch_key; give each call its own seed). */
+int wg_encrypt_symmetric(wg_context* ctx, size_t count, size_t level, const uint64_t* const* pts, const int8_t* secret,
+                         const uint64_t* a, const int64_t* e, uint64_t seed, double sigma, uint64_t* const* out_b,
+                         uint64_t* const* out_a, void* stream);
+/* The XBOOT AES's encrypted round-key bits on the device: replaces
+ * ckks_aes128_encrypt_expanded_round_key_bits (src/ckks/operations/circuits/aes/
+ * ckks_aes_ctr.cpp:687-725).  Bit k of the 176-byte expanded key as the constant slot value at
+ * params->scale, encrypted at params->s2c_depth (bits 0..127: first_round_key_level above it);
+ * out_b / out_a: 1408 device buffers with room for their level + 1 limbs; their scales and
+ * levels in out_scale[1408] / out_level[1408]. */
+int wg_aes_xboot_encrypt_round_key_bits(wg_context* ctx, const wg_bootstrap_params* params,
+                                        const uint8_t* expanded_key, size_t first_round_key_level,
+                                        const int8_t* secret, uint64_t seed, double sigma, uint64_t* const* out_b,
+                                        uint64_t* const* out_a, double* out_scale, size_t* out_level, void* stream);
+
 /* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a

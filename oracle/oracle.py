@@ -325,6 +325,32 @@ class OracleCtx:
         _check(rc, "orc_batched_ops")
 
 
+def _secret_from_ntt(h, N, nq, low=False):
+    """A context's ternary secret (or its bootstrapping sparse secret) as N int8 coefficients:
+    the inverse NTT of limb 0 of its NTT form."""
+    R = ref()
+    R.ref_ctx_low_secret.argtypes = [C.c_void_p, u64p]
+    R.ref_ctx_ntt.argtypes = [C.c_void_p, u64p, C.c_size_t, C.c_int, C.c_int]
+    sk = np.zeros(nq * N, np.uint64)
+    _check((R.ref_ctx_low_secret if low else R.ref_ctx_secret)(h, sk), "ref_ctx_secret")
+    c0 = np.ascontiguousarray(sk[:N]).copy()
+    _check(R.ref_ctx_ntt(h, c0, 1, 1, 0), "ref_ctx_ntt")
+    q0 = None
+    vals = c0.tolist()
+    out = np.zeros(N, np.int8)
+    big = max(vals)
+    for i, v in enumerate(vals):
+        if v == 0:
+            continue
+        if v == 1:
+            out[i] = 1
+        elif v == big:  # q0 - 1
+            out[i] = -1
+        else:
+            return q0
+    return out
+
+
 class RefCtx:
     """The reference's own CKKSContext (custom moduli schedule, no bootstrapping keys)."""
 
@@ -410,12 +436,22 @@ class RefCtx:
 
     def secret_coeffs(self):
         """The context's ternary secret as N int8 coefficients (inverse NTT of its limb 0)."""
-        sk = np.zeros(len(self.q) * self.N, np.uint64)
-        _check(ref().ref_ctx_secret(self.h, sk), "ref_ctx_secret")
-        c0 = self.ntt(sk[: self.N], inverse=True)
-        q0 = int(self.q[0])
-        return np.array([0 if v == 0 else (1 if v == 1 else -1) for v in c0.tolist()], dtype=np.int8) \
-            if all(v in (0, 1, q0 - 1) for v in c0.tolist()) else None
+        return _secret_from_ntt(self.h, self.N, len(self.q))
+
+    def encrypt_from_parts(self, level, pt, secret, a, e):
+        """ckks_encrypt_custom_eval of the evaluation-form plaintext pt with the mask a and noise e
+        given (ref_encrypt_from_parts): (b, a)."""
+        R = ref()
+        R.ref_encrypt_from_parts.argtypes = [C.c_void_p, C.c_size_t, u64p,
+                                             np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS"), u64p,
+                                             np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS"), u64p,
+                                             u64p]
+        n = (level + 1) * self.N
+        ob, oa = np.zeros(n, np.uint64), np.zeros(n, np.uint64)
+        _check(R.ref_encrypt_from_parts(self.h, level, np.ascontiguousarray(pt[:n], np.uint64),
+                                        np.ascontiguousarray(secret, np.int8), np.ascontiguousarray(a[:n], np.uint64),
+                                        np.ascontiguousarray(e, np.int64), ob, oa), "ref_encrypt_from_parts")
+        return ob, oa
 
     def switch_key_from_parts(self, kind, rotation, secret, a, e, target=None):
         """The reference's rotation (kind 0) / conjugation (kind 1) / relinearisation (kind 2) /
@@ -655,6 +691,11 @@ class RefPlans:
                                            C.byref(sc)), "ref_bootstrap_evalmod")
         k = (lvl.value + 1) * self.N
         return (bufs[0][:k].copy(), bufs[1][:k].copy()), (bufs[2][:k].copy(), bufs[3][:k].copy()), lvl.value, sc.value
+
+    def secret_coeffs(self, sparse=False):
+        """The context's ternary secret (or, when sparse, its bootstrapping sparse secret) as N
+        int8 coefficients."""
+        return _secret_from_ntt(self.h, self.N, len(self.q), low=sparse)
 
     def bootstrap_pair(self, level, scale0, scale1, ct0, ct1):
         """The reference's pair bootstrap (ckks_batch_bootstrap_evalmod_inplace) of ct0 = (b, a)

@@ -382,6 +382,44 @@ int ref_ctx_secret(void* h, uint64_t* out) {
     });
 }
 
+// The bootstrapping sparse secret in NTT form for every Q limb: [limb][N].
+int ref_ctx_low_secret(void* h, uint64_t* out) {
+    return guarded([&] {
+        const auto& sk = static_cast<RefCtx*>(h)->ctx.getLowSecretKey();
+        size_t off = 0;
+        for (const auto& limb : sk) {
+            std::memcpy(out + off, limb.data(), limb.size() * sizeof(uint64_t));
+            off += limb.size();
+        }
+    });
+}
+
+// ckks_encrypt_custom_eval (src/ckks/encoding/ckks_encoding.cpp:478-520) of the evaluation-form
+// plaintext `pt` at `level` under `secret` (N ternary coefficients), with the mask `a`
+// ([level + 1][N]) and the noise `e` ([N] integers) given instead of drawn.
+int ref_encrypt_from_parts(void* h, size_t level, const uint64_t* pt, const int8_t* secret, const uint64_t* a,
+                           const int64_t* e, uint64_t* out_b, uint64_t* out_a) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN(), L = level + 1;
+        const auto& qm = c.getParams().getModuli();
+        MyVector<uint64_t> mods(qm.begin(), qm.begin() + L);
+        MyVector<Negacyclic_NTT_Twiddles> tw(c.getTwiddleNtt().begin(), c.getTwiddleNtt().begin() + L);
+        const auto sk = ntt_secret_key(MyVector<int8_t>(secret, secret + N), tw, N, mods);
+        MyVector<uint64_t> e_poly(L * N), m(pt, pt + L * N), as(N);
+        for (size_t i = 0; i < L; ++i)
+            for (size_t j = 0; j < N; ++j) e_poly[i * N + j] = reduce_i64_mod_q(e[j], mods[i]);
+        ntt_forward_rns_flat_inplace(e_poly.data(), N, L, mods, tw, false);
+        for (size_t i = 0; i < L; ++i) {
+            pointwise_multiply_dispatch(a + i * N, sk[i].data(), as.data(), N, mods[i], tw[i]);
+            poly_add_modq_inplace(m.data() + i * N, e_poly.data() + i * N, N, mods[i]);
+            poly_sub_modq_inplace(m.data() + i * N, as.data(), N, mods[i]);
+        }
+        copy_out(m, out_b);
+        std::memcpy(out_a, a, L * N * sizeof(uint64_t));
+    });
+}
+
 // Hybrid key switch with caller-supplied key material (flat layout as above).
 int ref_keyswitch(void* h, size_t level, uint64_t* key_term, const uint64_t* key_flat, size_t parts,
                   size_t key_level, uint64_t* b, uint64_t* a, int b_add, int a_add, int montgomery) {

@@ -129,3 +129,25 @@ def test_secret_switch_key_matches_reference(wg, setup, kind):
     got = ctx.keygen_secret_switch(wkind, source, target, a=a, e=e, want_key=True)
     assert got.size == want.size
     assert (got == want).all(), int((got != want).sum())
+
+
+def test_encrypt_from_given_mask_and_noise_matches_reference(wg, setup):
+    import torch
+
+    R, ctx, s = setup
+    N, level, count = R.N, 4, 3
+    n = (level + 1) * N
+    rng = np.random.default_rng(17)
+    qc = np.repeat(R.q[: level + 1], N)
+    draw = lambda: (rng.integers(0, 1 << 62, n, dtype=np.uint64) % qc).astype(np.uint64)
+    pts = [draw() for _ in range(count)]
+    a = np.stack([draw() for _ in range(count)])
+    e = np.round(rng.normal(0.0, 3.2, (count, N))).astype(np.int64)
+    outs = [(torch.zeros(n, dtype=torch.int64, device="cuda"), torch.zeros(n, dtype=torch.int64, device="cuda"))
+            for _ in range(count)]
+    ctx.encrypt_symmetric(level, [wg.to_device(p) for p in pts], s, outs, a=a, e=e)
+    torch.cuda.synchronize()
+    for i in range(count):
+        wb, wa = R.encrypt_from_parts(level, pts[i], s, a[i], e[i])
+        assert (wg.to_host(outs[i][0]) == wb).all(), i
+        assert (wg.to_host(outs[i][1]) == wa).all(), i
