@@ -75,6 +75,7 @@ def parse():
     ap.add_argument("--no-xboot", action="store_true", help="skip the XBOOT S-box section")
     ap.add_argument("--no-xboot-aes", action="store_true", help="skip the XBOOT AES-CTR section")
     ap.add_argument("--xboot-aes-steps", type=int, default=2, help="timed XBOOT AES-CTR evaluations (after one warm-up)")
+    ap.add_argument("--no-keygen", action="store_true", help="skip the device key generation section")
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-mix-requests", type=int, default=16)
     ap.add_argument("--no-clocks", action="store_true",
@@ -803,6 +804,77 @@ def serve_bench(wg, torch, aes, requests, seed, capacity_blocks, workers=2, wind
             "full_slot_capacity_blocks_per_s": capacity_blocks}
 
 
+def keygen_bench(wg, torch, local, seed, with_cpu):
+    """The client setup of xboot15 on the device: every switching key the bootstrapped AES uses
+    (relinearisation, conjugation, the plan's rotations, both secret switches) generated from a
+    seeded ternary secret, and the 1408 encrypted round-key bits; wall time of the host-synchronous
+    calls.  Optionally the reference's encryption of the round-key bits on the host cores."""
+    with open(XBOOT_PLAN_PATH) as f:
+        plan = json.load(f)["xboot15"]
+    N = plan["ring_degree"]
+    q = np.array(plan["q"], dtype=np.uint64)
+    p = np.array(plan["p"], dtype=np.uint64)
+    ctx = wg.Context(N, q, p, plan["dnum"], device=local)
+    rng = np.random.default_rng(seed)
+    secret = np.zeros(N, np.int8)
+    secret[rng.choice(N, 256, replace=False)] = rng.choice([-1, 1], 256).astype(np.int8)
+    sparse = np.zeros(N, np.int8)
+    sparse[rng.choice(N, 32, replace=False)] = rng.choice([-1, 1], 32).astype(np.int8)
+    b = plan["bootstrap"]
+    params = wg.BootstrapParams(b["s2c_depth"], b["depth"], b["evalmod_log_scale"], b["double_angle"],
+                                b["active_slots"], b["slots"], b["scale"])
+    full = (b["depth"] + 1) * N
+    key_dev = torch.zeros((1408, 2, full), dtype=torch.int64, device="cuda")
+    key_bits = [(key_dev[k, 0], key_dev[k, 1]) for k in range(1408)]
+    ek = bytes(rng.integers(0, 256, 176, dtype=np.uint8))
+
+    def keys(tag):
+        ctx.keygen_switch_key(wg.WG_KEY_RELIN, 0, secret, seed=tag + 1)
+        ctx.keygen_switch_key(wg.WG_KEY_CONJ, 0, secret, seed=tag + 2)
+        for r in plan["rotations"]:
+            ctx.keygen_switch_key(wg.WG_KEY_ROTATION, int(r), secret, seed=tag + 3)
+        ctx.keygen_secret_switch(wg.WG_KEY_DENSE_TO_SPARSE, secret, sparse, seed=tag + 4)
+        ctx.keygen_secret_switch(wg.WG_KEY_SPARSE_TO_DENSE, sparse, secret, seed=tag + 5)
+
+    keys(0)  # warm-up (allocations, tables)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    keys(100)
+    torch.cuda.synchronize()
+    t_keys = time.perf_counter() - t0
+    ctx.aes_xboot_encrypt_round_key_bits(params, ek, 4, secret, key_bits, seed=7)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.aes_xboot_encrypt_round_key_bits(params, ek, 4, secret, key_bits, seed=8)
+    torch.cuda.synchronize()
+    t_bits = time.perf_counter() - t0
+    nkeys = len(plan["rotations"]) + 4
+    res = {"workload": f"xboot15 client setup: {nkeys} switching keys (relinearisation, conjugation, "
+                       f"{len(plan['rotations'])} rotations, both secret switches) and 1408 encrypted round-key bits",
+           "keys_s": t_keys, "keys_per_s": nkeys / t_keys, "key_bits_s": t_bits}
+    del key_dev, key_bits, ctx
+    torch.cuda.synchronize()
+    if with_cpu:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+
+            if O.ref_available():
+                t0 = time.perf_counter()
+                R = O.RefPlans(bootstrap_keys=True, preset="xboot15")
+                t_ctx = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                R.xboot_key_bits(ek, 4)
+                t_ref_bits = time.perf_counter() - t0
+                res["reference_cpu"] = {"key_bits_s": t_ref_bits, "context_build_s": t_ctx, "cores": os.cpu_count(),
+                                        "kind": "reference",
+                                        "sample": "ckks_aes128_encrypt_expanded_round_key_bits (OpenMP) and the whole "
+                                                  "xboot15 context build (keys, plans and EvalMod fit together)"}
+        except Exception as e:  # reported, never required
+            res["reference_cpu"] = {"unavailable": str(e)}
+    return res
+
+
 def serve_mix_bench(wg, torch, aes, xrun, requests, seed, walsh_cap, xboot_cap, window_ms=20.0, load=0.5):
     """Config 5's mixed stream: requests alternate between walsh15 (log-uniform 2..1024 blocks,
     even) and xboot15-full (log-uniform 1..16384 blocks), arriving as one seeded Poisson stream;
@@ -919,9 +991,10 @@ def main():
                 xrun = XbootAesRun(wg, torch, json.load(f)["xboot15"], local, args.seed + 29 + rank)
             xaes = xboot_aes_bench(wg, torch, stream, timed, xrun, args.seed + 29 + rank, args.xboot_aes_steps, False)
             del xrun
+        kg = None if args.no_keygen else keygen_bench(wg, torch, local, args.seed + 37 + rank, False)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "note": "--no-aes profiling run",
-                              "primitives": prim, "batched_ops": ops, "xboot_aes": xaes}), flush=True)
+                              "primitives": prim, "batched_ops": ops, "xboot_aes": xaes, "keygen": kg}), flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return
@@ -1031,6 +1104,13 @@ def main():
                                           aes.blocks / (ms / 1000.0), xboot_aes["blocks_per_s"])
         del xrun
         torch.cuda.synchronize()
+    keygen = None
+    if not args.no_keygen:
+        try:
+            keygen = keygen_bench(wg, torch, local, args.seed + 37 + rank,
+                                  rank == 0 and world == 1 and not args.no_cpu_baseline)
+        except Exception as e:  # a side section: reported, never fatal for the headline
+            keygen = {"error": str(e)}
     ops, ops_ctx = None, None
     if not args.no_ops:
         ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local)
@@ -1085,6 +1165,7 @@ def main():
         "xboot_sbox": xboot,
         "xboot_aes": xboot_aes,
         "serving_mix": serving_mix,
+        "keygen": keygen,
         "batched_ops": ops,
         "bsgs": bsgs,
         "cpu_baseline": cpu,
