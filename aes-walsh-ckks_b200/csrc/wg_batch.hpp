@@ -152,6 +152,10 @@ void xboot_encrypt_round_key_bits(Context& c, const BootstrapParams& p, const ui
                                   uint64_t* const* out_b, uint64_t* const* out_a, double* out_scale,
                                   size_t* out_level, cudaStream_t s);
 
+// CKKS slot encoding of `count` slot vectors (re / im host arrays [count][N/2]) at `scale` into
+// out[c] (limbs limbs), evaluation form when `eval`, else coefficient form (wg_encode_dev.cu).
+void encode_slots_device(Context& c, size_t count, size_t limbs, double scale, const double* re, const double* im,
+                         uint64_t* const* out, bool eval, cudaStream_t s);
 // The bootstrapping secret switches (wg_keygen.cu): WG_KEY_SPARSE_TO_DENSE as a hybrid key from
 // `source` to `target`, WG_KEY_DENSE_TO_SPARSE as the compact level-0 key over (q0, p0).
 void keygen_secret_switch(Context& c, int kind, const int8_t* source, const int8_t* target, const uint64_t* a_host,

@@ -734,6 +734,16 @@ int wg_aes_xboot_encrypt_round_key_bits(wg_context* ctx, const wg_bootstrap_para
     });
 }
 
+int wg_encode_slots_device(wg_context* ctx, size_t count, size_t limbs, double scale, const double* re, const double* im,
+                    uint64_t* const* out, int eval, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        if (count && !out) wg::fail(wg::kInvalid, "ckks_encode: null output array");
+        for (size_t i = 0; i < count; ++i) check_ptr(out[i], "ckks_encode");
+        wg::encode_slots_device(c, count, limbs, scale, re, im, out, eval != 0, S(stream));
+    });
+}
+
 int wg_xboot_sbox_coefficients(int64_t* out) {
     return guard([&] {
         check_ptr(out, "ckks_aes");

@@ -123,6 +123,17 @@ std::atomic<uint64_t> g_encode_calls{0}, g_encode_ns{0};
 
 }  // namespace
 
+void encode_tables(size_t N, std::vector<double>& twiddles, std::vector<uint32_t>& perm) {
+    if (N < 2 || (N & (N - 1))) throw std::invalid_argument("ckks_encode: ring degree must be a power of two");
+    const FftTables& t = tables(N);
+    twiddles.resize(2 * N);
+    for (size_t i = 0; i < N; ++i) {
+        twiddles[2 * i] = t.fwd[i].real();
+        twiddles[2 * i + 1] = t.fwd[i].imag();
+    }
+    perm.assign(t.perm.begin(), t.perm.end());
+}
+
 void encode_stats(uint64_t* calls, uint64_t* ns) {
     *calls = g_encode_calls.load();
     *ns = g_encode_ns.load();

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace wg {
 namespace host {
@@ -10,6 +11,11 @@ namespace host {
 // modulus: out[l * N + k].
 void encode_slots(size_t N, const double* re, const double* im, double scale, const uint64_t* moduli, size_t limbs,
                   uint64_t* out);
+
+// The tables encode_slots uses: the DIF twiddles with the twist folded in (interleaved re, im;
+// N entries, stage m at [m, 2m)) and the slot permutation (slot i -> evaluation index), for the
+// device encoder, which repeats the same operations.
+void encode_tables(size_t N, std::vector<double>& twiddles, std::vector<uint32_t>& perm);
 
 // Calls of encode_slots so far and their summed wall time (ns).
 void encode_stats(uint64_t* calls, uint64_t* ns);

@@ -105,6 +105,7 @@ def lib() -> C.CDLL:
         L.wg_xboot_linear_layer.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp]
         L.wg_keygen_switch_key.argtypes = [vp, C.c_int, C.c_int64, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
         L.wg_keygen_secret_switch.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
+        L.wg_encode_slots_device.argtypes = [vp, sz, sz, C.c_double, vp, vp, vp, C.c_int, vp]
         L.wg_encrypt_symmetric.argtypes = [vp, sz, sz, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp, vp]
         L.wg_aes_xboot_encrypt_round_key_bits.argtypes = [vp, vp, vp, sz, vp, C.c_uint64, C.c_double, vp, vp, vp,
                                                           vp, vp]
@@ -503,6 +504,18 @@ class Context:
                                             float(sigma), None if out is None else out.ctypes.data,
                                             _stream(stream)))
         return out
+
+    def encode_slots_device(self, limbs, scale, re, im, outs, eval_form=False, stream=None):
+        """CKKS encoding on the device (wg_encode_slots_device) of slot vectors re / im ([count][N/2]
+        float64) into outs (device tensors of limbs * N words)."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        r = np.ascontiguousarray(re, dtype=np.float64)
+        i = np.ascontiguousarray(im, dtype=np.float64)
+        ob = arr(outs)
+        if r.size != len(outs) * (self.N // 2) or i.size != r.size:
+            raise ValueError("slot arrays must be [count][N/2]")
+        _check(lib().wg_encode_slots_device(self.h, len(outs), int(limbs), float(scale), r.ctypes.data, i.ctypes.data,
+                                     ob.ctypes.data, 1 if eval_form else 0, _stream(stream)))
 
     def encrypt_symmetric(self, level, pts, secret, outs, a=None, e=None, seed=0, sigma=3.2, stream=None):
         """Secret-key encryption of evaluation-form plaintexts (device tensors, level+1 limbs)

@@ -386,7 +386,15 @@ int wg_aes_xboot_encrypt_round_key_bits(wg_context* ctx, const wg_bootstrap_para
                                         const int8_t* secret, uint64_t seed, double sigma, uint64_t* const* out_b,
                                         uint64_t* const* out_a, double* out_scale, size_t* out_level, void* stream);
 
-/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
+/* CKKS slot encoding on the device of `count` slot vectors (re / im: host arrays [count][N/2])
+ * at `scale` into out[c] (device, `limbs` Q limbs of N words), in evaluation form when `eval`,
+ * else coefficient form: replaces ckks_encode (src/ckks/encoding/ckks_encoding.cpp:332-414).
+ * The same FP64 operations as the reference's encoder (and as the host wg_encode_slots), so the
+ * same residues. */
+int wg_encode_slots_device(wg_context* ctx, size_t count, size_t limbs, double scale, const double* re, const double* im,
+                    uint64_t* const* out, int eval, void* stream);
+
+/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a
  * stream, takes every queued request, in arrival order, that still fits into one evaluation's
