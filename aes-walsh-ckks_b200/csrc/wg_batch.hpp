@@ -6,6 +6,7 @@
 #include <array>
 #include <vector>
 
+#include "wg_bundle.hpp"
 #include "wg_internal.hpp"
 
 namespace wg {
@@ -102,6 +103,8 @@ struct S2cPlan {
     size_t n = 0;
 };
 size_t lt_stage_level(const LtStage& st);
+// A stage's shape and diagonals (downloaded) for a bundle file.
+void lt_stage_export(const Context& c, const LtStage& st, BundleStage& out);
 bool lt_stage_rescales(const LtStage& st);
 void bootstrap_evalmod(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans,
                        const LtStage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs, size_t count,

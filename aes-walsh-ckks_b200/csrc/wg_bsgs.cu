@@ -261,6 +261,18 @@ __global__ void __launch_bounds__(kT) kb_accumulate(const AccumJob* jobs, int n,
 
 }  // namespace
 
+void lt_stage_export(const Context& c, const LtStage& st, BundleStage& out) {
+    out.level = st.level;
+    out.baby = st.baby;
+    out.slots = st.slots;
+    out.rescale = st.rescale ? 1 : 0;
+    out.indices.assign(st.indices.begin(), st.indices.end());
+    out.diagonals.resize(st.nterms * (st.level + 1 + c.np) * c.N);
+    check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+    check_cuda(cudaMemcpy(out.diagonals.data(), st.d_diag, out.diagonals.size() * 8, cudaMemcpyDeviceToHost),
+               "linear transform: diagonal download");
+}
+
 size_t lt_stage_level(const LtStage& st) { return st.level; }
 bool lt_stage_rescales(const LtStage& st) { return st.rescale; }
 

@@ -1,5 +1,7 @@
 // C ABI (include/walsh_gpu.h): argument checks, key registry, workspace routing and the
 // operation sequences of rotation, conjugation, relinearization and the batched workload.
+#include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -742,6 +744,88 @@ int wg_encode_slots_device(wg_context* ctx, size_t count, size_t limbs, double s
         for (size_t i = 0; i < count; ++i) check_ptr(out[i], "ckks_encode");
         wg::encode_slots_device(c, count, limbs, scale, re, im, out, eval != 0, S(stream));
     });
+}
+
+int wg_bundle_save(wg_context* ctx, const char* path, const wg_lt_stage* const* stages, size_t nstages) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(path, "wg_bundle");
+        if (nstages && !stages) wg::fail(wg::kInvalid, "wg_bundle: null stage list");
+        wg::Bundle b;
+        b.N = c.N;
+        b.dnum = c.dnum;
+        b.q.assign(c.q.begin(), c.q.end());
+        b.p.assign(c.p.begin(), c.p.end());
+        wg::check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+        wg::check_cuda(cudaDeviceSynchronize(), "wg_bundle");
+        for (const auto& [id, e] : c.keys) {
+            wg::BundleKey k;
+            k.kind = id.first;
+            k.rotation = id.second;
+            k.parts = e.parts;
+            k.key_level = e.key_level;
+            const size_t words = id.first == WG_KEY_DENSE_TO_SPARSE ? 4 * c.N
+                                                                    : e.parts * 2 * (e.key_level + 1 + c.np) * c.N;
+            k.data.resize(words);
+            wg::check_cuda(cudaMemcpy(k.data.data(), e.d_data, words * 8, cudaMemcpyDeviceToHost), "wg_bundle: key download");
+            b.keys.push_back(std::move(k));
+        }
+        for (size_t i = 0; i < nstages; ++i) {
+            check_ptr(stages[i], "wg_bundle");
+            b.stages.emplace_back();
+            wg::lt_stage_export(c, *stages[i]->s, b.stages.back());
+        }
+        const std::vector<uint8_t> bytes = wg::bundle_encode(b);
+        FILE* f = std::fopen(path, "wb");
+        if (!f) wg::fail(wg::kRuntime, std::string("wg_bundle: cannot open ") + path);
+        const size_t written = std::fwrite(bytes.data(), 1, bytes.size(), f);
+        const bool ok = written == bytes.size() && std::fclose(f) == 0;
+        if (!ok) wg::fail(wg::kRuntime, std::string("wg_bundle: write failed: ") + path);
+    });
+}
+
+int wg_bundle_load(wg_context* ctx, const char* path, wg_lt_stage** stages, size_t max_stages, size_t* nstages) {
+    std::vector<wg_lt_stage*> made;
+    const int rc = guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(path, "wg_bundle");
+        check_ptr(nstages, "wg_bundle");
+        FILE* f = std::fopen(path, "rb");
+        if (!f) wg::fail(wg::kInvalid, std::string("wg_bundle: cannot open ") + path);
+        std::vector<uint8_t> bytes;
+        uint8_t buf[1 << 16];
+        size_t got;
+        while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) bytes.insert(bytes.end(), buf, buf + got);
+        std::fclose(f);
+        const wg::Bundle b = wg::bundle_decode(bytes.data(), bytes.size());
+        if (b.N != c.N || b.dnum != c.dnum || b.q.size() != c.nq || b.p.size() != c.np ||
+            !std::equal(b.q.begin(), b.q.end(), c.q.begin()) || !std::equal(b.p.begin(), b.p.end(), c.p.begin()))
+            wg::fail(wg::kInvalid, "wg_bundle: the bundle's parameters differ from the context's");
+        if (b.stages.size() > max_stages || (!b.stages.empty() && !stages))
+            wg::fail(wg::kInvalid, "wg_bundle: more stages in the bundle than room for their handles");
+        for (const auto& k : b.keys) {
+            const size_t words = k.kind == WG_KEY_DENSE_TO_SPARSE ? 4 * c.N
+                                                                  : k.parts * 2 * (k.key_level + 1 + c.np) * c.N;
+            if (k.data.size() != words) wg::fail(wg::kInvalid, "wg_bundle: key size does not match its shape");
+            const int r = wg_ctx_set_key(ctx, (int)k.kind, k.rotation, k.data.data(), k.parts, k.key_level);
+            if (r != WG_OK) wg::fail(r, g_err);
+        }
+        for (const auto& st : b.stages) {
+            const size_t per = (st.level + 1 + c.np) * c.N;
+            if (st.indices.empty() || st.diagonals.size() != st.indices.size() * per)
+                wg::fail(wg::kInvalid, "wg_bundle: stage size does not match its shape");
+            wg_lt_stage* h = nullptr;
+            const int r = wg_lt_stage_create(ctx, st.level, st.indices.size(), st.indices.data(), st.diagonals.data(),
+                                             st.baby, st.slots, (int)st.rescale, &h);
+            if (r != WG_OK) wg::fail(r, g_err);
+            made.push_back(h);
+        }
+        for (size_t i = 0; i < made.size(); ++i) stages[i] = made[i];
+        *nstages = made.size();
+    });
+    if (rc != WG_OK)
+        for (auto* h : made) wg_lt_stage_destroy(h);
+    return rc;
 }
 
 int wg_xboot_sbox_coefficients(int64_t* out) {

@@ -105,6 +105,8 @@ def lib() -> C.CDLL:
         L.wg_xboot_linear_layer.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp]
         L.wg_keygen_switch_key.argtypes = [vp, C.c_int, C.c_int64, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
         L.wg_keygen_secret_switch.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
+        L.wg_bundle_save.argtypes = [vp, C.c_char_p, vp, sz]
+        L.wg_bundle_load.argtypes = [vp, C.c_char_p, vp, sz, C.POINTER(C.c_size_t)]
         L.wg_encode_slots_device.argtypes = [vp, sz, sz, C.c_double, vp, vp, vp, C.c_int, vp]
         L.wg_encrypt_symmetric.argtypes = [vp, sz, sz, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp, vp]
         L.wg_aes_xboot_encrypt_round_key_bits.argtypes = [vp, vp, vp, sz, vp, C.c_uint64, C.c_double, vp, vp, vp,
@@ -253,6 +255,13 @@ class LtStage:
         self.h = h
         self.level = level
         self.rescale = rescale
+
+    @classmethod
+    def from_handle(cls, ctx, h, level=None, rescale=None):
+        """Wrap a stage handle the library created (wg_bundle_load)."""
+        self = cls.__new__(cls)
+        self.ctx, self.h, self.level, self.rescale = ctx, h, level, rescale
+        return self
 
     def apply(self, bs, as_, stream=None):
         """Apply to a batch of ciphertexts (lists of device tensors), in place."""
@@ -504,6 +513,19 @@ class Context:
                                             float(sigma), None if out is None else out.ctypes.data,
                                             _stream(stream)))
         return out
+
+    def bundle_save(self, path, stages=()):
+        """Write the context's keys and the given LtStage objects to `path` (wg_bundle_save)."""
+        hs = np.ascontiguousarray([st.h.value for st in stages], dtype=np.uint64)
+        _check(lib().wg_bundle_save(self.h, str(path).encode(), hs.ctypes.data if len(stages) else None, len(stages)))
+
+    def bundle_load(self, path, max_stages=64):
+        """Install the keys of a bundle file and return its stages as LtStage objects
+        (wg_bundle_load)."""
+        hs = (C.c_void_p * max_stages)()
+        n = C.c_size_t()
+        _check(lib().wg_bundle_load(self.h, str(path).encode(), hs, max_stages, C.byref(n)))
+        return [LtStage.from_handle(self, C.c_void_p(hs[i])) for i in range(n.value)]
 
     def encode_slots_device(self, limbs, scale, re, im, outs, eval_form=False, stream=None):
         """CKKS encoding on the device (wg_encode_slots_device) of slot vectors re / im ([count][N/2]

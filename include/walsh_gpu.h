@@ -394,7 +394,18 @@ int wg_aes_xboot_encrypt_round_key_bits(wg_context* ctx, const wg_bootstrap_para
 int wg_encode_slots_device(wg_context* ctx, size_t count, size_t limbs, double scale, const double* re, const double* im,
                     uint64_t* const* out, int eval, void* stream);
 
-/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
+/* Keys and plans on disk (no counterpart in the reference, which rebuilds both in every
+ * context constructor): wg_bundle_save writes the context's parameters, every installed
+ * switching key and the given linear-transform stages to `path`; wg_bundle_load checks that the
+ * file's ring degree, moduli and dnum are the context's, installs its keys (as wg_ctx_set_key)
+ * and creates its stages (up to max_stages handles into stages, their number in *nstages).
+ * Format: "WGB1", version, parameters, key records, stage records and a 64-bit FNV-1a checksum
+ * (aes-walsh-ckks_b200/csrc/wg_bundle.hpp); a damaged or foreign file is rejected with
+ * WG_ERR_INVALID. */
+int wg_bundle_save(wg_context* ctx, const char* path, const wg_lt_stage* const* stages, size_t nstages);
+int wg_bundle_load(wg_context* ctx, const char* path, wg_lt_stage** stages, size_t max_stages, size_t* nstages);
+
+/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a
  * stream, takes every queued request, in arrival order, that still fits into one evaluation's

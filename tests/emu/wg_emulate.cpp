@@ -15,6 +15,7 @@
 #include "wg_tables.hpp"
 #include "wg_walsh.cuh"
 #include "wg_ring.hpp"
+#include "wg_bundle.hpp"
 #include <deque>
 #include <random>
 
@@ -265,6 +266,95 @@ size_t emu_ring_violations(uint64_t seed, size_t steps) {
         head = begin + need;
     }
     return bad;
+}
+
+// The bundle file format (wg_bundle.hpp): a seeded random bundle survives encode + decode
+// unchanged (returns 0), and the reader rejects every damaged variant tried: each single flipped
+// byte at `trials` seeded positions, every truncation length tried, a wrong magic and a wrong
+// version (returns how many damaged variants it accepted).
+int emu_bundle_roundtrip(uint64_t seed) {
+    std::mt19937_64 g(seed);
+    Bundle b;
+    b.N = 1u << 10;
+    b.dnum = 3;
+    for (int i = 0; i < 5; ++i) b.q.push_back(g());
+    for (int i = 0; i < 2; ++i) b.p.push_back(g());
+    for (int k = 0; k < 3; ++k) {
+        BundleKey key;
+        key.kind = (int64_t)(g() % 5);
+        key.rotation = (int64_t)(g() % 1000) - 500;
+        key.parts = 1 + g() % 3;
+        key.key_level = g() % 5;
+        key.data.resize(1 + g() % 5000);
+        for (auto& w : key.data) w = g();
+        b.keys.push_back(key);
+    }
+    for (int k = 0; k < 2; ++k) {
+        BundleStage st;
+        st.level = g() % 5;
+        st.baby = 1 + g() % 16;
+        st.slots = 512;
+        st.rescale = g() & 1;
+        st.indices.resize(1 + g() % 40);
+        for (auto& w : st.indices) w = g() % 512;
+        st.diagonals.resize(st.indices.size() * 7);
+        for (auto& w : st.diagonals) w = g();
+        b.stages.push_back(st);
+    }
+    const auto bytes = bundle_encode(b);
+    const Bundle r = bundle_decode(bytes.data(), bytes.size());
+    bool same = r.N == b.N && r.dnum == b.dnum && r.q == b.q && r.p == b.p && r.keys.size() == b.keys.size() &&
+                r.stages.size() == b.stages.size();
+    for (size_t k = 0; same && k < b.keys.size(); ++k)
+        same = r.keys[k].kind == b.keys[k].kind && r.keys[k].rotation == b.keys[k].rotation &&
+               r.keys[k].parts == b.keys[k].parts && r.keys[k].key_level == b.keys[k].key_level &&
+               r.keys[k].data == b.keys[k].data;
+    for (size_t k = 0; same && k < b.stages.size(); ++k)
+        same = r.stages[k].level == b.stages[k].level && r.stages[k].baby == b.stages[k].baby &&
+               r.stages[k].slots == b.stages[k].slots && r.stages[k].rescale == b.stages[k].rescale &&
+               r.stages[k].indices == b.stages[k].indices && r.stages[k].diagonals == b.stages[k].diagonals;
+    return same ? 0 : 1;
+}
+
+size_t emu_bundle_damage_accepted(uint64_t seed, size_t trials) {
+    std::mt19937_64 g(seed);
+    Bundle b;
+    b.N = 64;
+    b.dnum = 2;
+    b.q = {g(), g()};
+    b.p = {g()};
+    BundleKey key;
+    key.data.resize(100);
+    for (auto& w : key.data) w = g();
+    b.keys.push_back(key);
+    BundleStage st;
+    st.indices = {1, 2};
+    st.diagonals.resize(10);
+    b.stages.push_back(st);
+    const auto good = bundle_encode(b);
+    size_t accepted = 0;
+    auto accepts = [&](const std::vector<uint8_t>& v) {
+        try {
+            bundle_decode(v.data(), v.size());
+            return true;
+        } catch (const std::invalid_argument&) {
+            return false;
+        }
+    };
+    for (size_t t = 0; t < trials; ++t) {
+        auto v = good;
+        v[g() % v.size()] ^= (uint8_t)(1u << (g() % 8));
+        accepted += accepts(v);
+    }
+    for (size_t len = 0; len < good.size(); len += 1 + good.size() / 97)
+        accepted += accepts(std::vector<uint8_t>(good.begin(), good.begin() + len));
+    auto magic = good;
+    magic[0] = 'X';
+    accepted += accepts(magic);
+    auto version = good;
+    version[4] = 2;
+    accepted += accepts(version);
+    return accepted;
 }
 
 }  // extern "C"

@@ -185,3 +185,16 @@ def test_staging_ring_never_overwrites_pending_uploads(emu):
     emu.emu_ring_violations.argtypes = [C.c_uint64, C.c_size_t]
     for seed in (1, 2, 3):
         assert emu.emu_ring_violations(seed, 20000) == 0
+
+
+def test_bundle_file_round_trip_and_damage(emu):
+    """The key / plan bundle format (wg_bundle.hpp): random bundles survive encode and decode
+    word for word; flipped bytes, truncations, a foreign magic and a newer version are all
+    rejected."""
+    emu.emu_bundle_roundtrip.restype = C.c_int
+    emu.emu_bundle_roundtrip.argtypes = [C.c_uint64]
+    emu.emu_bundle_damage_accepted.restype = C.c_size_t
+    emu.emu_bundle_damage_accepted.argtypes = [C.c_uint64, C.c_size_t]
+    for seed in range(5):
+        assert emu.emu_bundle_roundtrip(seed) == 0
+    assert emu.emu_bundle_damage_accepted(7, 500) == 0
