@@ -572,4 +572,38 @@ void aes_ctr_walsh(Context& c, const BootstrapParams& p, const S2cPlan* s2c, siz
     }
 }
 
+void walsh_encrypt_round_key_bits(Context& c, const BootstrapParams& p, const uint8_t* expanded_key,
+                                  size_t active_blocks, const int8_t* secret, uint64_t seed, double sigma,
+                                  uint64_t* const* out_b, uint64_t* const* out_a, double* out_scale,
+                                  size_t* out_level, cudaStream_t s) {
+    if (!expanded_key) throw std::invalid_argument("ckks_aes_walsh: null expanded key");
+    const size_t slots = c.N / 2;
+    if (active_blocks == 0 || active_blocks > slots)
+        throw std::invalid_argument("ckks_aes_walsh: invalid active complex block count");
+    // aes_walsh_state_entry_level: one selection limb above the S2C input level
+    const size_t level = p.s2c_depth + 1;
+    if (level >= c.nq) throw std::invalid_argument("ckks_aes_walsh: selection key level exceeds parameter chain");
+    DeviceOps ops(c, 1, s);
+    // the bit's value in the real and imaginary part of the first active_blocks slots, zero
+    // elsewhere; rounds 1..9 at a quarter of the parameter scale, rounds 0 and 10 at it
+    const double full = p.scale, quarter = p.scale / 4.0;
+    auto encode = [&](double v, double scale) {
+        std::vector<double> re(slots, 0.0), im(slots, 0.0);
+        for (size_t i = 0; i < active_blocks; ++i) re[i] = im[i] = v;
+        std::vector<uint64_t> coeff((level + 1) * c.N);
+        host::encode_slots(c.N, re.data(), im.data(), scale, c.q.data(), level + 1, coeff.data());
+        return ops.upload_plain(coeff.data(), level + 1);
+    };
+    const uint64_t* pt[2][2] = {{encode(0.0, full), encode(1.0, full)}, {encode(0.0, quarter), encode(1.0, quarter)}};
+    std::vector<const uint64_t*> pts(kKeyBits);
+    for (size_t k = 0; k < kKeyBits; ++k) {
+        const bool edge = k < kBlockBits || k >= kRounds * kBlockBits;
+        const int bit = (expanded_key[k / 8] >> (k % 8)) & 1;
+        pts[k] = pt[edge ? 0 : 1][bit];
+        out_scale[k] = edge ? full : quarter;
+        out_level[k] = level;
+    }
+    encrypt_symmetric(c, kKeyBits, level, pts.data(), secret, nullptr, nullptr, seed, sigma, out_b, out_a, s);
+}
+
 }  // namespace wg

@@ -146,6 +146,13 @@ void keygen_switch_key(Context& c, int kind, int64_t rotation, const int8_t* sec
 void encrypt_symmetric(Context& c, size_t count, size_t level, const uint64_t* const* pts, const int8_t* secret,
                        const uint64_t* a_host, const int64_t* e_host, uint64_t seed, double sigma,
                        uint64_t* const* out_b, uint64_t* const* out_a, cudaStream_t s);
+// ckks_aes128_encrypt_expanded_round_key_bits_walsh_complex_blocks on the device (wg_aes.cu):
+// the 1408 bits as (v, v) in the first active_blocks slots, rounds 1..9 at a quarter of the
+// parameter scale, all at the S2C depth + 1; out_b / out_a need room for that level + 1 limbs.
+void walsh_encrypt_round_key_bits(Context& c, const BootstrapParams& p, const uint8_t* expanded_key,
+                                  size_t active_blocks, const int8_t* secret, uint64_t seed, double sigma,
+                                  uint64_t* const* out_b, uint64_t* const* out_a, double* out_scale,
+                                  size_t* out_level, cudaStream_t s);
 // ckks_aes128_encrypt_expanded_round_key_bits on the device (wg_xboot.cu): the 1408 bits of the
 // expanded key as constant-slot plaintexts at the parameter scale, encrypted under `secret` at
 // the S2C depth (round 0: first_round_key_level above it); out_b / out_a need room for the

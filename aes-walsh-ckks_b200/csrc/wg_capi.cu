@@ -828,6 +828,25 @@ int wg_bundle_load(wg_context* ctx, const char* path, wg_lt_stage** stages, size
     return rc;
 }
 
+int wg_aes_walsh_encrypt_round_key_bits(wg_context* ctx, const wg_bootstrap_params* params,
+                                        const uint8_t* expanded_key, size_t active_blocks, const int8_t* secret,
+                                        uint64_t seed, double sigma, uint64_t* const* out_b, uint64_t* const* out_a,
+                                        double* out_scale, size_t* out_level, void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        check_ptr(params, "ckks_aes_walsh");
+        check_ptr(out_scale, "ckks_aes_walsh");
+        check_ptr(out_level, "ckks_aes_walsh");
+        check_cts(c, 1408, out_b, out_a, "ckks_aes_walsh");
+        wg::BootstrapParams bp;
+        bp.s2c_depth = params->s2c_depth;
+        bp.scale = params->scale;
+        if (!(bp.scale > 0.0)) wg::fail(wg::kInvalid, "ckks_aes_walsh: invalid scale");
+        wg::walsh_encrypt_round_key_bits(c, bp, expanded_key, active_blocks, secret, seed, sigma, out_b, out_a,
+                                         out_scale, out_level, S(stream));
+    });
+}
+
 int wg_xboot_sbox_coefficients(int64_t* out) {
     return guard([&] {
         check_ptr(out, "ckks_aes");

@@ -109,6 +109,8 @@ def lib() -> C.CDLL:
         L.wg_bundle_load.argtypes = [vp, C.c_char_p, vp, sz, C.POINTER(C.c_size_t)]
         L.wg_encode_slots_device.argtypes = [vp, sz, sz, C.c_double, vp, vp, vp, C.c_int, vp]
         L.wg_encrypt_symmetric.argtypes = [vp, sz, sz, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp, vp]
+        L.wg_aes_walsh_encrypt_round_key_bits.argtypes = [vp, vp, vp, sz, vp, C.c_uint64, C.c_double, vp, vp, vp,
+                                                          vp, vp]
         L.wg_aes_xboot_encrypt_round_key_bits.argtypes = [vp, vp, vp, sz, vp, C.c_uint64, C.c_double, vp, vp, vp,
                                                           vp, vp]
         L.wg_serve_create_xboot.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, vp, vp, vp, vp, C.POINTER(vp)]
@@ -552,6 +554,23 @@ class Context:
                                           None if ap is None else ap.ctypes.data,
                                           None if ep is None else ep.ctypes.data, int(seed) & (2**64 - 1),
                                           float(sigma), ob.ctypes.data, oa.ctypes.data, _stream(stream)))
+
+    def aes_walsh_encrypt_round_key_bits(self, params, expanded_key, active_blocks, secret, outs, seed=0, sigma=3.2,
+                                         stream=None):
+        """The Walsh AES's 1408 encrypted round-key bits on the device
+        (wg_aes_walsh_encrypt_round_key_bits) into outs = [(b, a)] device tensors; returns
+        (scales, levels)."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        ob, oa = arr([x[0] for x in outs]), arr([x[1] for x in outs])
+        sec = np.ascontiguousarray(secret, dtype=np.int8)
+        ek = np.frombuffer(bytes(expanded_key), dtype=np.uint8).copy()
+        sc = np.zeros(1408, np.float64)
+        lv = np.zeros(1408, np.uintp)
+        _check(lib().wg_aes_walsh_encrypt_round_key_bits(self.h, C.byref(params), ek.ctypes.data, int(active_blocks),
+                                                         sec.ctypes.data, int(seed) & (2**64 - 1), float(sigma),
+                                                         ob.ctypes.data, oa.ctypes.data, sc.ctypes.data,
+                                                         lv.ctypes.data, _stream(stream)))
+        return sc, lv.astype(np.int64)
 
     def aes_xboot_encrypt_round_key_bits(self, params, expanded_key, first_round_key_level, secret, outs, seed=0,
                                          sigma=3.2, stream=None):

@@ -405,7 +405,19 @@ int wg_encode_slots_device(wg_context* ctx, size_t count, size_t limbs, double s
 int wg_bundle_save(wg_context* ctx, const char* path, const wg_lt_stage* const* stages, size_t nstages);
 int wg_bundle_load(wg_context* ctx, const char* path, wg_lt_stage** stages, size_t max_stages, size_t* nstages);
 
-/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
+/* The Walsh AES's encrypted round-key bits on the device: replaces
+ * ckks_aes128_encrypt_expanded_round_key_bits_walsh_complex_blocks (src/ckks/operations/circuits/
+ * aes/ckks_aes_ctr_walsh_sbox.cpp:981-1035).  Bit k of the 176-byte expanded key as (v, v) in the
+ * first active_blocks slots (zero elsewhere) at params->scale for rounds 0 and 10 and a quarter
+ * of it for rounds 1..9, encrypted under `secret` at params->s2c_depth + 1; out_b / out_a: 1408
+ * device buffers with room for that level + 1 limbs; scales and levels in out_scale[1408] /
+ * out_level[1408].  Mask and noise drawn on the device from `seed`. */
+int wg_aes_walsh_encrypt_round_key_bits(wg_context* ctx, const wg_bootstrap_params* params,
+                                        const uint8_t* expanded_key, size_t active_blocks, const int8_t* secret,
+                                        uint64_t seed, double sigma, uint64_t* const* out_b, uint64_t* const* out_a,
+                                        double* out_scale, size_t* out_level, void* stream);
+
+/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a
  * stream, takes every queued request, in arrival order, that still fits into one evaluation's

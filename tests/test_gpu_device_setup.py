@@ -74,3 +74,43 @@ def test_device_generated_keys_and_key_bits_run_the_xboot_aes(wg, ref_mod):
         mismatched += int((np.round(z[:blocks].real) != want).sum())
     print(f"device-generated setup: max error {max_err:.3e}")
     assert mismatched == 0 and max_err < 0.5
+
+
+def test_device_encrypted_walsh_key_bits_decrypt_to_the_key(wg, ref_mod):
+    """The Walsh AES's round-key bits encrypted on the device (wg_aes_walsh_encrypt_round_key_bits,
+    the reference's ckks_aes128_encrypt_expanded_round_key_bits_walsh_complex_blocks,
+    ckks_aes_ctr_walsh_sbox.cpp:981-1035) under the reference walsh15 context's secret: level S2C
+    depth + 1, scale the parameter scale for rounds 0 and 10 and a quarter of it otherwise
+    (:1010-1014), and each sampled bit decrypts, under the reference's decryption, to (v, v) in the
+    first 512 slots and 0 elsewhere."""
+    import json
+    import os
+
+    import torch
+
+    plan = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "walsh15_plan.json")))
+    R = ref_mod.RefPlans()
+    assert [int(x) for x in R.q] == plan["q"]
+    N = R.N
+    s = R.secret_coeffs()
+    b = plan["bootstrap"]
+    params = wg.BootstrapParams(b["s2c_depth"], b["depth"], b["evalmod_log_scale"], b["double_angle"],
+                                b["active_slots"], b["slots"], b["scale"])
+    ctx = wg.Context(N, R.q, R.p, R.dnum)
+    rng = np.random.default_rng(223)
+    ek = expand_key(bytes(rng.integers(0, 256, 16, dtype=np.uint8)))
+    level = b["s2c_depth"] + 1
+    outs = [(torch.zeros((level + 1) * N, dtype=torch.int64, device="cuda"),
+             torch.zeros((level + 1) * N, dtype=torch.int64, device="cuda")) for _ in range(1408)]
+    sc, lv = ctx.aes_walsh_encrypt_round_key_bits(params, ek, 512, s, outs, seed=9)
+    torch.cuda.synchronize()
+    assert set(lv.tolist()) == {level}
+    for k in range(1408):
+        want = b["scale"] if (k < 128 or k >= 1280) else b["scale"] / 4.0
+        assert sc[k] == want, k
+    m = (level + 1) * N
+    for k in (0, 5, 200, 700, 1279, 1300, 1407):
+        v = (ek[k // 8] >> (k % 8)) & 1
+        z = R.decrypt(level, float(sc[k]), wg.to_host(outs[k][0])[:m], wg.to_host(outs[k][1])[:m])
+        assert np.abs(z[:512].real - v).max() < 1e-3 and np.abs(z[:512].imag - v).max() < 1e-3, k
+        assert np.abs(z[512:]).max() < 1e-3, k
