@@ -401,7 +401,8 @@ int wg_encode_slots_device(wg_context* ctx, size_t count, size_t limbs, double s
  * and creates its stages (up to max_stages handles into stages, their number in *nstages).
  * Format: "WGB1", version, parameters, key records, stage records and a 64-bit FNV-1a checksum
  * (aes-walsh-ckks_b200/csrc/wg_bundle.hpp); a damaged or foreign file is rejected with
- * WG_ERR_INVALID. */
+ * WG_ERR_INVALID.  Both hold the whole bundle in host memory while they run (about twice the
+ * keys' and diagonals' size); keys installed before a failing record stay installed. */
 int wg_bundle_save(wg_context* ctx, const char* path, const wg_lt_stage* const* stages, size_t nstages);
 int wg_bundle_load(wg_context* ctx, const char* path, wg_lt_stage** stages, size_t max_stages, size_t* nstages);
 
