@@ -166,6 +166,12 @@ void xboot_encrypt_round_key_bits(Context& c, const BootstrapParams& p, const ui
 // out[c] (limbs limbs), evaluation form when `eval`, else coefficient form (wg_encode_dev.cu).
 void encode_slots_device(Context& c, size_t count, size_t limbs, double scale, const double* re, const double* im,
                          uint64_t* const* out, bool eval, cudaStream_t s);
+// ckks_decrypt on the device (wg_encode_dev.cu): slots of `count` ciphertexts at `level` (b, a
+// and optional c2 per ciphertext; scales[k] each) under the ternary `secret`, into host arrays
+// re / im [count][N/2].
+void decrypt_decode_device(Context& c, size_t count, size_t level, const double* scales, const uint64_t* const* b,
+                           const uint64_t* const* a, const uint64_t* const* c2, const int8_t* secret, double* re,
+                           double* im, cudaStream_t s);
 // The bootstrapping secret switches (wg_keygen.cu): WG_KEY_SPARSE_TO_DENSE as a hybrid key from
 // `source` to `target`, WG_KEY_DENSE_TO_SPARSE as the compact level-0 key over (q0, p0).
 void keygen_secret_switch(Context& c, int kind, const int8_t* source, const int8_t* target, const uint64_t* a_host,

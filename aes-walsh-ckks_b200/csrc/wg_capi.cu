@@ -847,6 +847,20 @@ int wg_aes_walsh_encrypt_round_key_bits(wg_context* ctx, const wg_bootstrap_para
     });
 }
 
+int wg_decrypt_decode(wg_context* ctx, size_t count, size_t level, const double* scales, const uint64_t* const* b,
+                      const uint64_t* const* a, const uint64_t* const* c2, const int8_t* secret, double* re, double* im,
+                      void* stream) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        if (count && (!b || !a)) wg::fail(wg::kInvalid, "ckks_decrypt: null ciphertext array");
+        for (size_t k = 0; k < count; ++k) {
+            check_ptr(b[k], "ckks_decrypt");
+            check_ptr(a[k], "ckks_decrypt");
+        }
+        wg::decrypt_decode_device(c, count, level, scales, b, a, c2, secret, re, im, S(stream));
+    });
+}
+
 int wg_xboot_sbox_coefficients(int64_t* out) {
     return guard([&] {
         check_ptr(out, "ckks_aes");

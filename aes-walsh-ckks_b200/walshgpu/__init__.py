@@ -107,6 +107,7 @@ def lib() -> C.CDLL:
         L.wg_keygen_secret_switch.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp]
         L.wg_bundle_save.argtypes = [vp, C.c_char_p, vp, sz]
         L.wg_bundle_load.argtypes = [vp, C.c_char_p, vp, sz, C.POINTER(C.c_size_t)]
+        L.wg_decrypt_decode.argtypes = [vp, sz, sz, vp, vp, vp, vp, vp, vp, vp, vp]
         L.wg_encode_slots_device.argtypes = [vp, sz, sz, C.c_double, vp, vp, vp, C.c_int, vp]
         L.wg_encrypt_symmetric.argtypes = [vp, sz, sz, vp, vp, vp, vp, C.c_uint64, C.c_double, vp, vp, vp]
         L.wg_aes_walsh_encrypt_round_key_bits.argtypes = [vp, vp, vp, sz, vp, C.c_uint64, C.c_double, vp, vp, vp,
@@ -528,6 +529,19 @@ class Context:
         n = C.c_size_t()
         _check(lib().wg_bundle_load(self.h, str(path).encode(), hs, max_stages, C.byref(n)))
         return [LtStage.from_handle(self, C.c_void_p(hs[i])) for i in range(n.value)]
+
+    def decrypt_decode(self, level, scales, cts, secret, stream=None):
+        """Decrypt and decode on the device (wg_decrypt_decode): cts = [(b, a)] device tensors at
+        `level` with scales[k]; returns the complex slots as a [count][N/2] array."""
+        arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
+        pb, pa = arr([x[0] for x in cts]), arr([x[1] for x in cts])
+        sc = np.ascontiguousarray(scales, dtype=np.float64)
+        sec = np.ascontiguousarray(secret, dtype=np.int8)
+        re = np.zeros((len(cts), self.N // 2))
+        im = np.zeros((len(cts), self.N // 2))
+        _check(lib().wg_decrypt_decode(self.h, len(cts), int(level), sc.ctypes.data, pb.ctypes.data, pa.ctypes.data,
+                                       None, sec.ctypes.data, re.ctypes.data, im.ctypes.data, _stream(stream)))
+        return re + 1j * im
 
     def encode_slots_device(self, limbs, scale, re, im, outs, eval_form=False, stream=None):
         """CKKS encoding on the device (wg_encode_slots_device) of slot vectors re / im ([count][N/2]

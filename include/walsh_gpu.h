@@ -418,7 +418,17 @@ int wg_aes_walsh_encrypt_round_key_bits(wg_context* ctx, const wg_bootstrap_para
                                         uint64_t seed, double sigma, uint64_t* const* out_b, uint64_t* const* out_a,
                                         double* out_scale, size_t* out_level, void* stream);
 
-/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
+/* Decryption and decoding on the device (client side): replaces ckks_decrypt
+ * (src/ckks/encoding/ckks_encoding.cpp:89-171, 567-575) for `count` ciphertexts at `level`
+ * (device pointers b[k], a[k], and c2[k] for three-polynomial ones or c2 null) with scales[k],
+ * under the ternary `secret` (host, N coefficients); the N/2 slot values of each go to the host
+ * arrays re / im ([count][N/2]).  Floating-point results agree with the reference's to FP64
+ * rounding (a two-modulus CRT and another FFT evaluation order), not bit for bit. */
+int wg_decrypt_decode(wg_context* ctx, size_t count, size_t level, const double* scales, const uint64_t* const* b,
+                      const uint64_t* const* a, const uint64_t* const* c2, const int8_t* secret, double* re, double* im,
+                      void* stream);
+
+/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a
  * stream, takes every queued request, in arrival order, that still fits into one evaluation's

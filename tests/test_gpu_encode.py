@@ -2,7 +2,8 @@
 (src/ckks/encoding/ckks_encoding.cpp:332-414) on the walsh15 chain: residue for residue, for
 several plaintexts per call, on random complex slot vectors, on AES-style 0/1 bit planes at the
 parameter scale, on a constant and on large values at a small scale; and the evaluation-form
-output is the NTT of the coefficient-form one."""
+output is the NTT of the coefficient-form one.  Decryption and decoding on the device
+(wg_decrypt_decode) against the reference's ckks_decrypt, to FP64 rounding."""
 import numpy as np
 import pytest
 
@@ -44,3 +45,28 @@ def test_device_encoder_matches_reference(wg, ref_mod):
             ctx.ntt_forward(coeff, limbs)
             torch.cuda.synchronize()
             assert (wg.to_host(evals[k]) == wg.to_host(coeff)).all(), (scale, k)
+
+
+def test_device_decrypt_decode_matches_reference(wg, ref_mod):
+    import torch
+
+    R = ref_mod.RefPlans()
+    N, half = R.N, R.N // 2
+    s = R.secret_coeffs()
+    ctx = wg.Context(N, R.q, R.p, R.dnum)
+    rng = np.random.default_rng(31)
+    for level, scale in ((3, 2.0 ** 35), (0, 2.0 ** 30)):
+        n = (level + 1) * N
+        vecs = [(rng.uniform(-1, 1, half), rng.uniform(-1, 1, half)) for _ in range(3)]
+        pts = [torch.zeros(n, dtype=torch.int64, device="cuda") for _ in vecs]
+        ctx.encode_slots_device(level + 1, scale, np.stack([v[0] for v in vecs]), np.stack([v[1] for v in vecs]),
+                                pts, eval_form=True)
+        cts = [(torch.zeros(n, dtype=torch.int64, device="cuda"), torch.zeros(n, dtype=torch.int64, device="cuda"))
+               for _ in vecs]
+        ctx.encrypt_symmetric(level, pts, s, cts, seed=5 + level)
+        torch.cuda.synchronize()
+        got = ctx.decrypt_decode(level, [scale] * len(vecs), cts, s)
+        for k, (vr, vi) in enumerate(vecs):
+            want = R.decrypt(level, scale, wg.to_host(cts[k][0]), wg.to_host(cts[k][1]))
+            assert np.abs(got[k] - want).max() < 1e-9, (level, k, float(np.abs(got[k] - want).max()))
+            assert np.abs(got[k] - (vr + 1j * vi)).max() < 1e-5, (level, k)
