@@ -86,3 +86,29 @@ def test_walsh15_plan_fixture_consistent(oracle_mod):
         else:
             assert spec["words"] == spec["parts"] * 2 * (spec["key_level"] + 1 + K) * N
     assert len(plan["aes"]["key_scales"]) == 11 * 128
+
+
+def test_entry_points_reject_a_null_context(libwg):
+    """Every context-taking entry point of the client setup, the XBOOT path and the bundle files
+    returns an error status with a message for a null context (no exception crosses the ABI and
+    no GPU is touched)."""
+    L = libwg.lib()
+    calls = {
+        "wg_keygen_switch_key": lambda: L.wg_keygen_switch_key(None, 2, 1, None, None, None, 0, 3.2, None, None),
+        "wg_keygen_secret_switch": lambda: L.wg_keygen_secret_switch(None, 3, None, None, None, None, 0, 3.2, None,
+                                                                     None),
+        "wg_encrypt_symmetric": lambda: L.wg_encrypt_symmetric(None, 0, 0, None, None, None, None, 0, 3.2, None, None,
+                                                               None),
+        "wg_encode_slots_device": lambda: L.wg_encode_slots_device(None, 0, 1, 1.0, None, None, None, 0, None),
+        "wg_decrypt_decode": lambda: L.wg_decrypt_decode(None, 0, 0, None, None, None, None, None, None, None, None),
+        "wg_bundle_save": lambda: L.wg_bundle_save(None, b"/nonexistent/x.wgb", None, 0),
+        "wg_bundle_load": lambda: L.wg_bundle_load(None, b"/nonexistent/x.wgb", None, 0, None),
+        "wg_bootstrap_pair": lambda: L.wg_bootstrap_pair(None, None, None, 0, None, 0, None, 0, 0, 1.0, None, None,
+                                                         None, None, None, None, None),
+        "wg_xboot_linear_layer": lambda: L.wg_xboot_linear_layer(None, 0, None, None, None, None, None, None, 1, None,
+                                                                 None, None, None),
+    }
+    for name, call in calls.items():
+        rc = call()
+        assert rc != 0, name
+        assert b"null context" in L.wg_last_error(), (name, L.wg_last_error())
