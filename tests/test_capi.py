@@ -112,3 +112,36 @@ def test_entry_points_reject_a_null_context(libwg):
         rc = call()
         assert rc != 0, name
         assert b"null context" in L.wg_last_error(), (name, L.wg_last_error())
+
+
+def test_xboot_plan_fixture_consistent(oracle_mod):
+    """The XBOOT bootstrap-structure fixture the benchmark's XBOOT sections build from agrees with
+    the prime generator on the reference's XBOOT bit schedules (ckks_aes_params.hpp:133-209) and
+    with its own shapes: stage limbs and diagonal indices, key sizes, and the round-key bits'
+    levels (round 0 four levels above the S2C depth, the others at it) and scales."""
+    import json
+
+    plans = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "xboot_plans.json")))
+    bits = {"xboot15": ([38] * 5, [38, 36, 36, 37, 37, 37] + [38] * 11),
+            "xboot14": ([32], [31, 27, 30, 30, 30] + [31] * 6 + [27, 27])}
+    assert set(plans) == {"xboot15", "xboot15-sparse", "xboot14", "xboot14-sparse"}
+    for name, plan in plans.items():
+        N = plan["ring_degree"]
+        pb, qb = bits[name.split("-")[0]]
+        p, q = oracle_mod.find_primes(pb, qb, N)
+        assert [int(x) for x in q] == plan["q"] and [int(x) for x in p] == plan["p"], name
+        K = len(plan["p"])
+        b = plan["bootstrap"]
+        assert b["slots"] == N // 2 and b["active_slots"] in (N // 2, 1024)
+        for which in ("s2c", "c2s"):
+            for st in plan[which]:
+                assert 0 <= st["qp_limbs"] - 1 - K < len(plan["q"])
+                assert all(0 <= i < st["slot_count"] for i in st["indices"])
+        for kname, spec in plan["keys"].items():
+            if kname == "dense_to_sparse":
+                assert spec["words"] == 4 * N
+            else:
+                assert spec["words"] == spec["parts"] * 2 * (spec["key_level"] + 1 + K) * N
+        lv = plan["aes"]["key_levels"]
+        assert lv[:128] == [b["s2c_depth"] + 4] * 128 and lv[128:] == [b["s2c_depth"]] * 1280
+        assert plan["aes"]["key_scales"] == [b["scale"]] * 1408
