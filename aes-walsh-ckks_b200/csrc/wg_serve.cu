@@ -16,6 +16,7 @@
 #include <stdexcept>
 
 #include "../../include/walsh_gpu.h"
+#include "wg_batching.hpp"
 #include "wg_internal.hpp"
 #include "wg_serve.hpp"
 
@@ -76,18 +77,9 @@ Server::~Server() {
     release_workers();
 }
 
-// the queued requests already fill the next evaluation (one of them no longer fits beside the
-// others, or the slots are used up)
+// the queued requests already fill the next evaluation (wg_batching.hpp)
 bool Server::head_batch_full() const {
-    size_t blocks = 0;
-    bool skipped = false;
-    for (const auto& r : queue_) {
-        if (blocks + r.blocks <= max_blocks_)
-            blocks += r.blocks;
-        else
-            skipped = true;
-    }
-    return skipped || blocks == max_blocks_;
+    return batch_full(queue_, max_blocks_, [](const Request& r) { return r.blocks; });
 }
 
 size_t Server::admitted() const {
@@ -164,17 +156,19 @@ void Server::worker(size_t w) {
                 cv_.wait_until(lk, deadline, [&] { return stop_ || queue_.empty() || head_batch_full(); });
                 if (queue_.empty() || running_ >= admitted()) continue;  // another worker took them
             }
-            // every queued request that still fits, in arrival order (the oldest always fits an
-            // empty evaluation, so no request waits behind later ones for ever)
-            for (auto it = queue_.begin(); it != queue_.end() && blocks < max_blocks_;) {
-                if (blocks + it->blocks <= max_blocks_) {
-                    blocks += it->blocks;
-                    batch.push_back(std::move(*it));
-                    it = queue_.erase(it);
+            // every queued request that still fits, in arrival order (first fit, wg_batching.hpp)
+            const std::vector<size_t> take = first_fit(queue_, max_blocks_, [](const Request& r) { return r.blocks; });
+            std::deque<Request> rest;
+            for (size_t k = 0, t = 0; k < queue_.size(); ++k) {
+                if (t < take.size() && take[t] == k) {
+                    blocks += queue_[k].blocks;
+                    batch.push_back(std::move(queue_[k]));
+                    ++t;
                 } else {
-                    ++it;
+                    rest.push_back(std::move(queue_[k]));
                 }
             }
+            queue_.swap(rest);
             ++running_;
         }
         const auto started = Clock::now();

@@ -16,6 +16,7 @@
 #include "wg_walsh.cuh"
 #include "wg_ring.hpp"
 #include "wg_bundle.hpp"
+#include "wg_batching.hpp"
 #include <deque>
 #include <random>
 
@@ -355,6 +356,40 @@ size_t emu_bundle_damage_accepted(uint64_t seed, size_t trials) {
     version[4] = 2;
     accepted += accepts(version);
     return accepted;
+}
+
+// The service's request packing (wg_batching.hpp) on `trials` seeded queues of 0..12 requests of
+// 1..max_blocks blocks: returns how many queues broke a property of first fit — positions
+// ascending, the oldest request taken, the taken blocks within the slots, every skipped request
+// too large for the slots left at its turn — or of batch_full (some request skipped, or the
+// slots used up exactly).
+size_t emu_first_fit_violations(uint64_t seed, size_t trials) {
+    std::mt19937_64 g(seed);
+    size_t bad = 0;
+    for (size_t t = 0; t < trials; ++t) {
+        const size_t max_blocks = 1 + g() % 64;
+        std::deque<size_t> q(g() % 13);
+        for (auto& n : q) n = 1 + g() % max_blocks;
+        const auto id = [](size_t n) { return n; };
+        const std::vector<size_t> take = wg::first_fit(q, max_blocks, id);
+        bool ok = q.empty() ? take.empty() : (!take.empty() && take[0] == 0);
+        size_t used = 0, ti = 0;
+        bool skipped = false;
+        for (size_t k = 0; k < q.size(); ++k) {
+            if (ti < take.size() && take[ti] == k) {
+                used += q[k];
+                ++ti;
+            } else {
+                skipped = true;
+                ok = ok && used + q[k] > max_blocks;
+            }
+        }
+        ok = ok && ti == take.size() && used <= max_blocks;
+        for (size_t k = 1; k < take.size(); ++k) ok = ok && take[k] > take[k - 1];
+        ok = ok && wg::batch_full(q, max_blocks, id) == (skipped || used == max_blocks);
+        bad += ok ? 0 : 1;
+    }
+    return bad;
 }
 
 }  // extern "C"

@@ -198,3 +198,12 @@ def test_bundle_file_round_trip_and_damage(emu):
     for seed in range(5):
         assert emu.emu_bundle_roundtrip(seed) == 0
     assert emu.emu_bundle_damage_accepted(7, 500) == 0
+
+
+def test_request_packing_is_first_fit(emu):
+    """The batching service's packing (wg_batching.hpp): on seeded queues the taken requests are
+    the first-fit choice in arrival order (oldest always taken, nothing skipped that fits) and
+    the batch counts as full exactly when a request no longer fits or the slots are used up."""
+    emu.emu_first_fit_violations.restype = C.c_size_t
+    emu.emu_first_fit_violations.argtypes = [C.c_uint64, C.c_size_t]
+    assert emu.emu_first_fit_violations(3, 20000) == 0
