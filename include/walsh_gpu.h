@@ -428,7 +428,7 @@ int wg_decrypt_decode(wg_context* ctx, size_t count, size_t level, const double*
                       const uint64_t* const* a, const uint64_t* const* c2, const int8_t* secret, double* re, double* im,
                       void* stream);
 
-/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
+/* Continuous-batching AES-CTR transciphering service (no counterpart in the reference, whose
  * benchmark evaluates one AES-CTR batch at a time, bench/aes_bench.cpp:197-291).  Requests of
  * 2..max_blocks counter blocks (even counts) queue up; each of `workers` worker threads owns a
  * stream, takes every queued request, in arrival order, that still fits into one evaluation's

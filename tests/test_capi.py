@@ -145,3 +145,15 @@ def test_xboot_plan_fixture_consistent(oracle_mod):
         lv = plan["aes"]["key_levels"]
         assert lv[:128] == [b["s2c_depth"] + 4] * 128 and lv[128:] == [b["s2c_depth"]] * 1280
         assert plan["aes"]["key_scales"] == [b["scale"]] * 1408
+
+
+def test_header_is_clean_c11(tmp_path):
+    """include/walsh_gpu.h is plain C (what a cgo / ctypes / JNI binding consumes): it compiles as
+    C11 with every warning an error, and as C++."""
+    src = tmp_path / "use_header.c"
+    src.write_text('#include "walsh_gpu.h"\nint main(void) { return sizeof(wg_bootstrap_params) == 0; }\n')
+    inc = os.path.join(ROOT, "include")
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", inc, "-c", str(src), "-o",
+                    str(tmp_path / "a.o")], check=True)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", inc, "-x", "c++", "-c", str(src), "-o",
+                    str(tmp_path / "b.o")], check=True)
