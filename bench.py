@@ -620,12 +620,16 @@ def xboot_bench(wg, torch, stream, timed, local, steps, with_cpu):
                 qc = np.repeat(R.q[: level + 1], N)
                 draw = lambda: (rng.integers(0, 1 << 62, (level + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
                 one = [(draw(), draw()) for _ in range(8)]
-                t0 = time.perf_counter()
-                R.sbox(level, scale, one)
-                t = time.perf_counter() - t0
-                res["reference_cpu"] = {"s_per_sbox": t, "cores": os.cpu_count(), "kind": "reference",
-                                        "sample": "one S-box instance, the reference's operations on all host "
-                                                  "threads (its AES runs 16 instances side by side)"}
+                threads = os.cpu_count()
+                width = min(count, threads)  # one wave: every thread runs one instance
+                t = R.sbox_layer_seconds(level, scale, one, width, threads)
+                waves = -(-count // width)
+                res["reference_cpu"] = {"s_per_subbytes_layer": waves * t, "sboxes_per_s": count / (waves * t),
+                                        "cores": threads, "kind": "reference",
+                                        "sample": f"{width} S-box instances side by side on {threads} threads "
+                                                  f"(OpenMP over instances, as the reference's SubBytes runs its "
+                                                  f"16 byte positions), {t:.2f} s; a layer of {count} taken as "
+                                                  f"{waves} such wave(s)"}
         except Exception as e:  # reported, never required
             res["reference_cpu"] = {"unavailable": str(e)}
     return res
@@ -737,16 +741,20 @@ def xboot_aes_bench(wg, torch, stream, timed, run, seed, steps, with_cpu, sbox_s
                 qc = np.repeat(R.q[: lv + 1], N)
                 draw = lambda: (rng.integers(0, 1 << 62, (lv + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
                 c0, c1 = (draw(), draw()), (draw(), draw())
-                t0 = time.perf_counter()
-                R.bootstrap_pair(lv, R.scale, R.scale, c0, c1)
-                tp = time.perf_counter() - t0
-                ref = {"s_per_pair_bootstrap": tp, "cores": os.cpu_count(), "kind": "reference",
-                       "sample": "one pair bootstrap (ckks_batch_bootstrap_evalmod_inplace) on all host threads"}
+                threads = os.cpu_count()
+                width = min(64, threads)  # one wave of the 64 pairs of a refresh
+                tp = R.bootstrap_pair_layer_seconds(lv, R.scale, c0, c1, width, threads)
+                waves = -(-64 // width)
+                ref = {"s_per_refresh": waves * tp, "cores": threads, "kind": "reference",
+                       "sample": f"{width} pair bootstraps (ckks_batch_bootstrap_evalmod_inplace) side by side on "
+                                 f"{threads} threads (OpenMP over pairs, as the reference's state refresh runs its "
+                                 f"64 pairs), {tp:.2f} s; a refresh of 64 pairs taken as {waves} such wave(s)"}
                 if sbox_seconds:
-                    est = 640 * tp + 160 * sbox_seconds
+                    est = 10 * waves * tp + 10 * sbox_seconds
                     ref.update({"estimated_s_per_evaluation": est, "estimated_blocks_per_s": blocks / est,
-                                "estimate": "640 pair bootstraps + 160 S-box instances at the sampled per-call "
-                                            "times (the reference runs them one call per thread group)"})
+                                "estimate": "10 refreshes of 64 pairs + 10 SubBytes layers of 16 S-boxes at the "
+                                            "sampled layer times (its linear layers and XORs not counted, which "
+                                            "favours the reference)"})
                 res["reference_cpu"] = ref
         except Exception as e:  # reported, never required
             res["reference_cpu"] = {"unavailable": str(e)}
@@ -1094,7 +1102,7 @@ def main():
                                                      rank == 0 and world == 1 and not args.no_cpu_baseline)
     xboot_aes, serving_mix = None, None
     if not args.no_xboot_aes:
-        sbox_s = ((xboot or {}).get("reference_cpu") or {}).get("s_per_sbox")
+        sbox_s = ((xboot or {}).get("reference_cpu") or {}).get("s_per_subbytes_layer")
         with open(XBOOT_PLAN_PATH) as f:
             xrun = XbootAesRun(wg, torch, json.load(f)["xboot15"], local, args.seed + 29 + rank)
         xboot_aes = xboot_aes_bench(wg, torch, stream, timed, xrun, args.seed + 29 + rank, args.xboot_aes_steps,

@@ -518,6 +518,22 @@ class RefXboot(RefCtx):
             off += 2 * m
         return res
 
+    def sbox_layer_seconds(self, level, scale, bits, instances, threads=0):
+        """Wall time of `instances` XBOOT S-boxes on copies of the 8 bit ciphertexts `bits`, run as
+        the reference's sub_bytes_inplace runs its byte positions (OpenMP dynamic over instances,
+        src/ckks/operations/circuits/aes/ckks_aes_ctr.cpp:474-509) on `threads` threads (0: the
+        OpenMP default).  The outputs are discarded."""
+        R = ref()
+        R.ref_xboot_sbox_layer.argtypes = [C.c_void_p, C.c_size_t, C.c_double, u64p, C.c_size_t, C.c_int,
+                                           C.POINTER(C.c_double)]
+        n = (level + 1) * self.N
+        flat = np.concatenate([np.concatenate([np.asarray(b[:n], np.uint64), np.asarray(a[:n], np.uint64)])
+                               for b, a in bits])
+        sec = C.c_double()
+        _check(R.ref_xboot_sbox_layer(self.h, level, float(scale), flat, instances, threads, C.byref(sec)),
+               "ref_xboot_sbox_layer")
+        return sec.value
+
     @staticmethod
     def coefficients():
         out = np.zeros(8 * 256, np.int64)
@@ -709,6 +725,21 @@ class RefPlans:
                                         C.byref(sc)), "ref_bootstrap_pair")
         k = (lvl.value + 1) * self.N
         return (bufs[0][:k].copy(), bufs[1][:k].copy()), (bufs[2][:k].copy(), bufs[3][:k].copy()), lvl.value, sc.value
+
+    def bootstrap_pair_layer_seconds(self, level, scale, ct0, ct1, pairs, threads=0):
+        """Wall time of `pairs` reference pair bootstraps on copies of ct0 = (b, a) and ct1, run as
+        the reference's xboot_state_inplace runs the pairs of a state (OpenMP dynamic over pairs,
+        src/ckks/operations/circuits/aes/ckks_aes_ctr.cpp:556-574) on `threads` threads (0: the
+        OpenMP default).  The outputs are discarded."""
+        R = ref()
+        R.ref_bootstrap_pair_layer.argtypes = [C.c_void_p, C.c_size_t, C.c_double] + [u64p] * 4 + \
+            [C.c_size_t, C.c_int, C.POINTER(C.c_double)]
+        m = (level + 1) * self.N
+        ins = [np.ascontiguousarray(x[:m], dtype=np.uint64) for x in (ct0[0], ct0[1], ct1[0], ct1[1])]
+        sec = C.c_double()
+        _check(R.ref_bootstrap_pair_layer(self.h, level, float(scale), *ins, pairs, threads, C.byref(sec)),
+               "ref_bootstrap_pair_layer")
+        return sec.value
 
     def xboot_key_bits(self, expanded_key, first_round_key_level=4):
         """The reference's encrypted expanded-key bits for the XBOOT AES

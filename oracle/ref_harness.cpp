@@ -1228,6 +1228,68 @@ int ref_walsh_sbox_layer(void* h, size_t block_count, size_t level, double scale
     });
 }
 
+// Timing samples of the XBOOT AES's two layers as the reference runs them: `instances` XBOOT
+// S-boxes (sub_bytes_inplace, ckks_aes_ctr.cpp:474-509: OpenMP dynamic over byte positions; the
+// S-box as restated in xboot_ref) on copies of the same 8 bits, or `pairs` pair bootstraps
+// (xboot_state_inplace, :556-574: OpenMP dynamic over pairs) on copies of one pair, on `threads`
+// threads.  *seconds = wall time of the loop; outputs are discarded.
+int ref_xboot_sbox_layer(void* h, size_t level, double scale, const uint64_t* in, size_t instances, int threads,
+                         double* seconds) {
+    return guarded([&] {
+        auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        std::vector<xboot_ref::Byte> inputs(instances);
+        for (auto& bits : inputs)
+            for (size_t k = 0; k < 8; ++k)
+                bits.emplace_back(N, copy_in(in + (2 * k + 1) * n, n), copy_in(in + 2 * k * n, n),
+                                  (long double)scale, level);
+        std::exception_ptr first;
+        if (threads > 0) omp_set_num_threads(threads);
+        const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic)
+        for (std::ptrdiff_t i = 0; i < (std::ptrdiff_t)instances; ++i) {
+            try {
+                auto res = xboot_ref::sbox(c, inputs[(size_t)i]);
+                if (res.size() != 8) throw std::runtime_error("ref_xboot_sbox_layer: expected 8 output bits");
+            } catch (...) {
+#pragma omp critical
+                if (!first) first = std::current_exception();
+            }
+        }
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (first) std::rethrow_exception(first);
+    });
+}
+
+int ref_bootstrap_pair_layer(void* h, size_t level, double scale, const uint64_t* b0, const uint64_t* a0,
+                             const uint64_t* b1, const uint64_t* a1, size_t pairs, int threads, double* seconds) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        std::vector<CKKSCiphertext> x0, x1;
+        for (size_t i = 0; i < pairs; ++i) {
+            x0.emplace_back(N, copy_in(a0, n), copy_in(b0, n), (long double)scale, level);
+            x1.emplace_back(N, copy_in(a1, n), copy_in(b1, n), (long double)scale, level);
+        }
+        std::exception_ptr first;
+        if (threads > 0) omp_set_num_threads(threads);
+        const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic)
+        for (std::ptrdiff_t i = 0; i < (std::ptrdiff_t)pairs; ++i) {
+            try {
+                ckks_batch_bootstrap_evalmod_inplace(c, x0[(size_t)i], x1[(size_t)i]);
+            } catch (...) {
+#pragma omp critical
+                if (!first) first = std::current_exception();
+            }
+        }
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (first) std::rethrow_exception(first);
+    });
+}
+
 // ckks_encode (coefficient form, eval = false) of N/2 slot values re[i] + i im[i].
 int ref_encode(void* h, const double* re, const double* im, double scale, size_t level, uint64_t* out) {
     return guarded([&] {
