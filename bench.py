@@ -586,8 +586,9 @@ XB_DNUM = 5
 def xboot_bench(wg, torch, stream, timed, local, steps, with_cpu):
     """The XBOOT S-box (wg_xboot_sbox) on one SubBytes layer, 16 instances of 8 bit ciphertexts at
     level 5 of the xboot15 chain (N = 2^15, 17 Q + 5 P limbs, dnum 5; uniform residues, uniform
-    relinearisation key of its shape); optionally the reference's S-box on one instance on the
-    host cores (restated in the harness on its own operations)."""
+    relinearisation key of its shape); optionally one reference SubBytes layer (16 S-boxes
+    side by side under OpenMP, the S-box restated in the harness on the reference's own
+    operations) on the host cores."""
     N = 1 << 15
     p, q = wg.find_primes(XB_P_BITS, XB_Q_BITS, N)
     ctx = wg.Context(N, q, p, XB_DNUM, device=local)
@@ -621,15 +622,12 @@ def xboot_bench(wg, torch, stream, timed, local, steps, with_cpu):
                 draw = lambda: (rng.integers(0, 1 << 62, (level + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
                 one = [(draw(), draw()) for _ in range(8)]
                 threads = os.cpu_count()
-                width = min(count, threads)  # one wave: every thread runs one instance
-                t = R.sbox_layer_seconds(level, scale, one, width, threads)
-                waves = -(-count // width)
-                res["reference_cpu"] = {"s_per_subbytes_layer": waves * t, "sboxes_per_s": count / (waves * t),
+                t = R.sbox_layer_seconds(level, scale, one, count, threads)
+                res["reference_cpu"] = {"s_per_subbytes_layer": t, "sboxes_per_s": count / t,
                                         "cores": threads, "kind": "reference",
-                                        "sample": f"{width} S-box instances side by side on {threads} threads "
+                                        "sample": f"one SubBytes layer: {count} S-box instances on {threads} threads "
                                                   f"(OpenMP over instances, as the reference's SubBytes runs its "
-                                                  f"16 byte positions), {t:.2f} s; a layer of {count} taken as "
-                                                  f"{waves} such wave(s)"}
+                                                  f"16 byte positions), {t:.2f} s"}
         except Exception as e:  # reported, never required
             res["reference_cpu"] = {"unavailable": str(e)}
     return res
@@ -715,8 +713,9 @@ class XbootAesRun:
 def xboot_aes_bench(wg, torch, stream, timed, run, seed, steps, with_cpu, sbox_seconds=None):
     """AES-128-CTR with the XBOOT S-box (wg_aes_ctr_xboot) on xboot15-full: 16384 counter blocks
     per evaluation (every slot one block), ten rounds with 64 pair bootstraps after rounds 1..9
-    and a final refresh.  Optionally the reference's pair bootstrap once on the host cores and an
-    estimate of its full evaluation from that sample and the S-box sample."""
+    and a final refresh.  Optionally one reference state refresh (64 pair bootstraps side by side
+    under OpenMP) on the host cores, and an estimate of the reference's full evaluation from it
+    and the SubBytes layer of the S-box section."""
     step = lambda: run.step(stream)
     step()
     l0 = wg.launch_count()
@@ -742,18 +741,16 @@ def xboot_aes_bench(wg, torch, stream, timed, run, seed, steps, with_cpu, sbox_s
                 draw = lambda: (rng.integers(0, 1 << 62, (lv + 1) * N, dtype=np.uint64) % qc).astype(np.uint64)
                 c0, c1 = (draw(), draw()), (draw(), draw())
                 threads = os.cpu_count()
-                width = min(64, threads)  # one wave of the 64 pairs of a refresh
-                tp = R.bootstrap_pair_layer_seconds(lv, R.scale, c0, c1, width, threads)
-                waves = -(-64 // width)
-                ref = {"s_per_refresh": waves * tp, "cores": threads, "kind": "reference",
-                       "sample": f"{width} pair bootstraps (ckks_batch_bootstrap_evalmod_inplace) side by side on "
-                                 f"{threads} threads (OpenMP over pairs, as the reference's state refresh runs its "
-                                 f"64 pairs), {tp:.2f} s; a refresh of 64 pairs taken as {waves} such wave(s)"}
+                tp = R.bootstrap_pair_layer_seconds(lv, R.scale, c0, c1, 64, threads)
+                ref = {"s_per_refresh": tp, "cores": threads, "kind": "reference",
+                       "sample": f"one state refresh: 64 pair bootstraps (ckks_batch_bootstrap_evalmod_inplace) on "
+                                 f"{threads} threads (OpenMP over pairs, as the reference's refresh runs them), "
+                                 f"{tp:.2f} s"}
                 if sbox_seconds:
-                    est = 10 * waves * tp + 10 * sbox_seconds
+                    est = 10 * tp + 10 * sbox_seconds
                     ref.update({"estimated_s_per_evaluation": est, "estimated_blocks_per_s": blocks / est,
                                 "estimate": "10 refreshes of 64 pairs + 10 SubBytes layers of 16 S-boxes at the "
-                                            "sampled layer times (its linear layers and XORs not counted, which "
+                                            "timed layer times (its linear layers and XORs not counted, which "
                                             "favours the reference)"})
                 res["reference_cpu"] = ref
         except Exception as e:  # reported, never required
