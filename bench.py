@@ -318,7 +318,7 @@ def bsgs_bench(wg, ctx, q, p, stream, timed, steps, warmup):
 # ------------------------------------------------------------------------------------------
 # batched ops: mul + relin + rescale + rotate on 64 ciphertexts, batched vs plain
 # ------------------------------------------------------------------------------------------
-def ops_bench(args, wg, torch, stream, timed, rank, local):
+def ops_bench(args, wg, torch, stream, timed, rank, local, with_cpu=False):
     N = 1 << LOGN
     L = len(Q_BITS)
     p, q = wg.find_primes(P_BITS, Q_BITS, N)
@@ -451,7 +451,37 @@ def ops_bench(args, wg, torch, stream, timed, rank, local):
         "ntt": {"launches": n, "ms": kms, "gbs": kbytes / (kms * 1e6) if kms else None},
         "e2e": e2e, "steps": steps,
     }
+    if with_cpu:
+        res["reference_cpu"] = ref_ops_sample(levels, rots, args.seed + 41)
     return res, ctx, q, p
+
+
+def ref_ops_sample(levels, rots, seed):
+    """The batched-ops workload (same levels and rotation indices) on the reference's CPU path:
+    its own multiply, relinearize, rescale and rotate per ciphertext with OpenMP over
+    ciphertexts (ref_batched_ops), on a reference context of the same chain holding the
+    relinearisation key and the rotation keys the workload uses; uniform residues."""
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        if not O.ref_available():
+            return {"unavailable": "the reference library (oracle/_ref) is not built"}
+        N, L, count = 1 << LOGN, len(Q_BITS), len(levels)
+        R = O.RefCtx(N, Q_BITS, P_BITS, DNUM, rotations=sorted(set(int(r) for r in rots)))
+        stride = L * N
+        rng = np.random.default_rng(seed)
+        qcol = np.tile(np.repeat(R.q, N), count)
+        draw = lambda: (rng.integers(0, 1 << 62, count * stride, dtype=np.uint64) % qcol).astype(np.uint64)
+        xb, xa, yb, ya = draw(), draw(), draw(), draw()
+        threads = os.cpu_count()
+        sec = R.batched_ops_seconds(levels, xb, xa, yb, ya, rots, stride, threads)
+        return {"value": count / sec, "unit": "ciphertexts/s", "seconds": sec, "cores": threads, "kind": "reference",
+                "sample": f"the whole workload ({count} ciphertexts, the same levels and rotation indices) through "
+                          f"the reference's ckks_mul_inplace, ckks_relin_hybrid_inplace, ckks_rescale and "
+                          f"ckks_rotate_inplace, OpenMP over ciphertexts on {threads} threads"}
+    except Exception as e:  # reported, never required
+        return {"unavailable": str(e)}
 
 
 # ------------------------------------------------------------------------------------------
@@ -1118,7 +1148,8 @@ def main():
             keygen = {"error": str(e)}
     ops, ops_ctx = None, None
     if not args.no_ops:
-        ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local)
+        ops, ops_ctx, q, p = ops_bench(args, wg, torch, stream, timed, rank, local,
+                                       rank == 0 and world == 1 and not args.no_cpu_baseline)
     bsgs = None
     if not args.no_bsgs:
         if ops_ctx is None:

@@ -402,6 +402,16 @@ class RefCtx:
                                    int(b_add), int(a_add), 1), "ref_keyswitch")
         return b, a
 
+    def batched_ops_seconds(self, levels, x_b, x_a, y_b, y_a, rots, stride, threads):
+        """Wall time of the reference's mul + relin + rescale + rotate on every ciphertext i at
+        levels[i] (buffers of `stride` words per ciphertext, x updated in place), OpenMP over
+        ciphertexts on `threads` threads (ref_batched_ops)."""
+        sec = C.c_double()
+        _check(ref().ref_batched_ops(self.h, len(levels), np.ascontiguousarray(levels, np.uintp), x_b, x_a, y_b, y_a,
+                                     np.ascontiguousarray(rots, np.int64), stride, int(threads), C.byref(sec)),
+               "ref_batched_ops")
+        return sec.value
+
     def rotate(self, level, b, a, rot):
         b = np.ascontiguousarray(b, dtype=np.uint64).copy()
         a = np.ascontiguousarray(a, dtype=np.uint64).copy()
