@@ -247,7 +247,7 @@ C2S_STAGES = [(12, [1024 * k for k in range(16)], 8192, False),
 BSGS_BATCH = 8
 
 
-def bsgs_bench(wg, ctx, q, p, stream, timed, steps, warmup):
+def bsgs_bench(wg, ctx, q, p, stream, timed, steps, warmup, with_cpu=False):
     """Config 3: CoeffToSlot (4 stages from level 12) and SlotToCoeff (3 stages at level 1) over
     a batch of 8 ciphertexts, diagonals with the plans' index sets (uniform residues), keys of
     the walsh15 key shape (uniform residues)."""
@@ -312,7 +312,34 @@ def bsgs_bench(wg, ctx, q, p, stream, timed, steps, warmup):
             st.close()
     res["batch"] = BSGS_BATCH
     res["data"] = "diagonals with the walsh15 plans' index sets, uniform residues; uniform keys"
+    if with_cpu:
+        res["reference_cpu"] = ref_bsgs_sample()
     return res
+
+
+def ref_bsgs_sample():
+    """Both plans on the reference's CPU path: its own walsh15 CoeffToSlot (from level 12) and
+    SlotToCoeff (level 1) plans and rotation keys, every stage through its QP evaluator, on a
+    batch of copies of one uniform ciphertext with OpenMP over ciphertexts."""
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        if not O.ref_available():
+            return {"unavailable": "the reference library (oracle/_ref) is not built"}
+        R = O.RefPlans()
+        N, threads = R.N, os.cpu_count()
+        rng = np.random.default_rng(43)
+        out = {"cores": threads, "kind": "reference",
+               "sample": f"{BSGS_BATCH} ciphertexts per plan, OpenMP over ciphertexts on {threads} threads"}
+        for name, which, level in (("coeff_to_slot", 1, 12), ("slot_to_coeff", 0, 1)):
+            qc = np.repeat(R.q[: level + 1], N)
+            b, a = [(rng.integers(0, 1 << 62, qc.size, dtype=np.uint64) % qc).astype(np.uint64) for _ in range(2)]
+            sec = R.plan_seconds(which, level, b, a, BSGS_BATCH, threads)
+            out[name] = {"ciphertexts_per_s": BSGS_BATCH / sec, "seconds": sec}
+        return out
+    except Exception as e:  # reported, never required
+        return {"unavailable": str(e)}
 
 
 # ------------------------------------------------------------------------------------------
@@ -1155,7 +1182,8 @@ def main():
         if ops_ctx is None:
             p, q = wg.find_primes(P_BITS, Q_BITS, N)
             ops_ctx = wg.Context(N, q, p, DNUM, device=local)
-        bsgs = bsgs_bench(wg, ops_ctx, q, p, stream, timed, 10, args.warmup)
+        bsgs = bsgs_bench(wg, ops_ctx, q, p, stream, timed, 10, args.warmup,
+                          rank == 0 and world == 1 and not args.no_cpu_baseline)
     if ops:
         # key switching against HBM: the batched mul + relin + rescale + rotate pipeline (two key
         # switches per ciphertext) at its compulsory bytes over the graph-replay time

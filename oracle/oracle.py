@@ -644,6 +644,20 @@ class RefPlans:
         return dict(nterms=nt.value, baby=baby.value, rescale=bool(resc.value), qp_limbs=qpl.value,
                     montgomery=bool(mont.value), slot_count=slots.value, indices=idx, diagonals=diags)
 
+    def plan_seconds(self, which, level, b, a, count, threads=0):
+        """Wall time of the whole plan `which` (0: SlotToCoeff, 1: CoeffToSlot; every stage in
+        order through ckks_apply_linear_transform_owned_stage_qp) on `count` copies of (b, a) at
+        `level`, OpenMP over ciphertexts on `threads` threads (ref_lt_plan_seconds)."""
+        R = ref()
+        R.ref_lt_plan_seconds.argtypes = [C.c_void_p, C.c_int, C.c_size_t, u64p, u64p, C.c_size_t, C.c_int,
+                                          C.POINTER(C.c_double)]
+        n = (level + 1) * self.N
+        sec = C.c_double()
+        _check(R.ref_lt_plan_seconds(self.h, which, level, np.ascontiguousarray(b[:n], np.uint64),
+                                     np.ascontiguousarray(a[:n], np.uint64), count, threads, C.byref(sec)),
+               "ref_lt_plan_seconds")
+        return sec.value
+
     def apply_stage(self, which, stage, level, b, a):
         n = (level + 1) * self.N
         ob = np.zeros(n, np.uint64)

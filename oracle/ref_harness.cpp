@@ -1476,6 +1476,38 @@ int ref_lt_stage(void* h, int which, size_t stage, size_t level, const uint64_t*
     });
 }
 
+// Timing sample of a whole plan (every stage in order, each through
+// ckks_apply_linear_transform_owned_stage_qp) on `count` copies of (b, a) at `level`, OpenMP
+// dynamic over ciphertexts on `threads` threads, the way the reference runs independent
+// ciphertexts side by side.  *seconds = wall time of the loop; outputs are discarded.
+int ref_lt_plan_seconds(void* h, int which, size_t level, const uint64_t* b, const uint64_t* a, size_t count,
+                        int threads, double* seconds) {
+    return guarded([&] {
+        const auto& c = static_cast<RefCtx*>(h)->ctx;
+        const size_t N = c.getParams().getN();
+        const size_t n = (level + 1) * N;
+        const auto& plan = plan_of(h, which);
+        std::vector<CKKSCiphertext> cts;
+        for (size_t i = 0; i < count; ++i)
+            cts.emplace_back(N, copy_in(a, n), copy_in(b, n), c.getParams().getScale(), level);
+        std::exception_ptr first;
+        if (threads > 0) omp_set_num_threads(threads);
+        const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic)
+        for (std::ptrdiff_t i = 0; i < (std::ptrdiff_t)count; ++i) {
+            try {
+                CKKSCiphertext x = std::move(cts[(size_t)i]);
+                for (const auto& st : plan.stages) x = ckks_apply_linear_transform_owned_stage_qp(c, x, st);
+            } catch (...) {
+#pragma omp critical
+                if (!first) first = std::current_exception();
+            }
+        }
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (first) std::rethrow_exception(first);
+    });
+}
+
 // Every rotation value with a key in the context.
 int ref_ctx_rotations(void* h, int64_t* out, size_t* n) {
     return guarded([&] {
