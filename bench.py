@@ -560,6 +560,45 @@ def ntt_bench(wg, torch, stream, timed, local, steps, hbm):
     return res
 
 
+def ref_config1_sample(repeats=5):
+    """Config 1 on the reference's own CPU functions as it calls them for one ciphertext:
+    forward and inverse NTT of both polynomials' 16 limbs (ntt_forward_rns_flat_inplace /
+    ntt_inverse_rns_flat_inplace with the context's tables) and one rotation by +1
+    (ckks_rotate_inplace) at level 15, N = 2^14, dnum 4; medians of `repeats` calls."""
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        if not O.ref_available():
+            return {"unavailable": "the reference library (oracle/_ref) is not built"}
+        R, lib = O.RefCtx(1 << 14, [50] * 16, [50] * 4, 4, rotations=(1,)), O.ref()
+        N, L = R.N, len(R.q)
+        rng = np.random.default_rng(14)
+        qcol = np.repeat(R.q, N)
+        b, a = [(rng.integers(0, 1 << 62, L * N, dtype=np.uint64) % qcol).astype(np.uint64) for _ in range(2)]
+
+        def median(call):
+            ts = []
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                call()
+                ts.append(time.perf_counter() - t0)
+            return float(np.median(ts))
+
+        def ntt(inverse):
+            for x in (b, a):
+                O._check(lib.ref_ctx_ntt(R.h, x, L, int(inverse), 0), "ref_ctx_ntt")
+
+        tf = median(lambda: ntt(False))
+        ti = median(lambda: ntt(True))
+        tr = median(lambda: O._check(lib.ref_rotate(R.h, L - 1, b, a, 1), "ref_rotate"))
+        return {"forward_us": 1e6 * tf, "inverse_us": 1e6 * ti, "rotation_us": 1e6 * tr, "cores": os.cpu_count(),
+                "kind": "reference", "sample": f"one ciphertext (2 x {L} limbs), the reference's functions with "
+                                              f"their own threading, median of {repeats} calls"}
+    except Exception as e:  # reported, never required
+        return {"unavailable": str(e)}
+
+
 # ------------------------------------------------------------------------------------------
 # AES-CTR on the device
 # ------------------------------------------------------------------------------------------
@@ -1150,6 +1189,8 @@ def main():
                                                  "reads and writes (intermediates included)"}}
 
     prim = None if args.no_ntt else ntt_bench(wg, torch, stream, timed, local, 20, hbm)
+    if prim and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        prim["config1"]["reference_cpu"] = ref_config1_sample()
     serving = None if args.no_serve else serve_bench(wg, torch, aes, args.serve_requests, args.seed + 17 + rank,
                                                      aes.blocks / (ms / 1000.0))
     xboot = None if args.no_xboot else xboot_bench(wg, torch, stream, timed, local, 5,
