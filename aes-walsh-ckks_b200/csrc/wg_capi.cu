@@ -17,9 +17,6 @@ Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t
                         int device);
 }
 
-struct wg_context {
-    wg::Context* c;
-};
 struct wg_lt_stage {
     wg::LtStage* s;
 };

@@ -271,3 +271,9 @@ void add_sub(const Context& c, size_t level, uint64_t* x, const uint64_t* y, int
              size_t poly_stride, bool subtract, cudaStream_t s);
 
 }  // namespace wg
+
+// The public context handle of include/walsh_gpu.h: a wrapper around the engine context, defined
+// once here for every file that implements entry points on it.
+struct wg_context {
+    wg::Context* c;
+};

@@ -13,6 +13,7 @@
 //     every scratch word it later reads, so nothing has to be cleared between calls;
 //   * calls that overlap on the GPU (different streams, or concurrent host threads) race on the
 //     array; serialise them.
+//   * every call makes the context's device current and leaves it current;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
 //     that device current; make that first call before any stream capture.
 #include <mutex>
@@ -31,12 +32,12 @@ static __device__ __align__(256) uint64_t g_rotation_scratch[kScratchWords];
 std::mutex g_setup_mutex;
 uint64_t* g_scratch_ptr[kMaxDevices] = {};
 
-// Device address of the scratch array on `device` (looked up once per device).
+// Device address of the scratch array on `device`, looked up once per device.  The caller has
+// made `device` current; the lookup itself allocates nothing.
 uint64_t* scratch_on(int device) {
     if (device < 0 || device >= kMaxDevices) fail(kInvalid, "rotate_noalloc: device index out of range");
     std::lock_guard<std::mutex> g(g_setup_mutex);
     if (!g_scratch_ptr[device]) {
-        check_cuda(cudaSetDevice(device), "rotate_noalloc: cudaSetDevice");
         void* ptr = nullptr;
         check_cuda(cudaGetSymbolAddress(&ptr, g_rotation_scratch), "rotate_noalloc: cudaGetSymbolAddress");
         g_scratch_ptr[device] = static_cast<uint64_t*>(ptr);
@@ -49,11 +50,6 @@ uint64_t* scratch_on(int device) {
 
 extern "C" int wg_rotate_noalloc(wg_context* ctx, size_t level, uint64_t* b, uint64_t* a, int64_t rotation,
                                  void* stream);
-
-// The public context handle wraps a wg::Context pointer (wg_capi.cu).
-struct wg_context {
-    wg::Context* c;
-};
 
 extern "C" int wg_rotate_noalloc(wg_context* ctx, size_t level, uint64_t* b, uint64_t* a, int64_t rotation,
                                  void* stream) {
@@ -71,6 +67,9 @@ extern "C" int wg_rotate_noalloc(wg_context* ctx, size_t level, uint64_t* b, uin
             wg::fail(wg::kInvalid, "rotate_noalloc: this level needs " + std::to_string(words * 8 >> 20) +
                                        " MiB of scratch, above the 32 MiB static array");
         const wg::KeyEntry& k = c.key(WG_KEY_ROTATION, r);
+        // Every call makes the context's device current (and leaves it current, as the other
+        // entry points do): the scratch address and the context's tables belong to that device.
+        wg::check_cuda(cudaSetDevice(c.device), "rotate_noalloc: cudaSetDevice");
         uint64_t* scratch = wg::scratch_on(c.device);
         const uint64_t galois = wg::host::powmod(5, (uint64_t)r, 2 * c.N);
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

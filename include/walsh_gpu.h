@@ -489,8 +489,9 @@ void wg_serve_destroy(wg_server* server);
  * synchronisation an allocation can cause.  Same result as wg_rotate.  The key-switch scratch is a file-scope static device
  * array of 32 MiB that every GPU loading the library holds until exit; a level needing more
  * returns WG_ERR_INVALID.  All calls share that array (nothing in it needs clearing between
- * calls), so calls that overlap on the GPU race: serialise them.  The first call on a device
- * looks up the array's address; make it before any stream capture. */
+ * calls), so calls that overlap on the GPU race: serialise them.  Every call makes the
+ * context's device current and leaves it current.  The first call on a device looks up the
+ * array's address; make it before any stream capture. */
 int wg_rotate_noalloc(wg_context* ctx, size_t level, uint64_t* b, uint64_t* a, int64_t rotation,
                       void* stream);
 

@@ -29,10 +29,15 @@ i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 szp = np.ctypeslib.ndpointer(dtype=np.uintp, flags="C_CONTIGUOUS")
 
 
+# Where the reference project's sources are looked for: $REF_ROOT, else a checkout named
+# `reference` beside this repository.  Only the build of the compiled reference reads them.
+REF_ROOT = os.environ.get("REF_ROOT") or os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference"))
+
+
 def build(ref: bool = False) -> None:
     """Compile the oracle (and, when asked and the sources exist, the reference harness)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and os.path.isdir(os.environ.get("REF_ROOT", "/root/reference")):
+    if ref and os.path.isdir(REF_ROOT):
         subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
 
 

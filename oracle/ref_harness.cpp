@@ -600,10 +600,8 @@ void* ref_walsh15_plans_create(void) {
     return rc == 0 ? out : nullptr;
 }
 
-// The same chain with bootstrapping keys (dense-to-sparse, sparse-to-dense, EvalMod
-// polynomial).  The EvalMod fit comes from the stand-in in ref_evalmod_stub.cpp, so the
-// polynomial is not the reference's MPFR fit; nothing built from this context is compared
-// on EvalMod coefficients other than those it reports itself.
+// The same chain with bootstrapping keys (dense-to-sparse, sparse-to-dense) and the EvalMod
+// polynomial of the reference's own MPFR fit (src/math/poly_approx.cpp:565).
 void* ref_walsh15_bts_create(void) {
     RefCtx* out = nullptr;
     const int rc = guarded([&] {
@@ -1067,8 +1065,7 @@ int ref_xboot_sbox_coefficients(int64_t* out) {
 
 // The XBOOT N = 2^15 parameter set as the reference defines it (AESXBoot15Config, or
 // AESXBoot15Sparse1024Config when `sparse`, src/ckks/parameters/ckks_aes_params.hpp:179-209),
-// bootstrapping keys included.  The EvalMod fit comes from the stand-in in
-// ref_evalmod_stub.cpp (see ref_walsh15_bts_create).
+// bootstrapping keys and the reference's MPFR EvalMod fit included.
 void* ref_xboot15_bts_create(int sparse) {
     RefCtx* out = nullptr;
     const int rc = guarded([&] {
@@ -1081,7 +1078,7 @@ void* ref_xboot15_bts_create(int sparse) {
 
 // The secure XBOOT N = 2^14 parameter set (AESXBoot14SecureConfig, or
 // AESXBoot14SecureSparse1024Config when `sparse`, ckks_aes_params.hpp:133-154) with its
-// bootstrapping keys; EvalMod fit from the stand-in.
+// bootstrapping keys and the reference's MPFR EvalMod fit.
 void* ref_xboot14_bts_create(int sparse) {
     RefCtx* out = nullptr;
     const int rc = guarded([&] {

@@ -33,8 +33,9 @@ def oracle_mod():
 @pytest.fixture(scope="session")
 def ref_mod(oracle_mod):
     if not oracle_mod.ref_available():
-        if os.path.isdir(os.environ.get("REF_ROOT", "/root/reference")):
-            subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        if os.path.isdir(oracle_mod.REF_ROOT):
+            subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref",
+                            "REF_ROOT=" + oracle_mod.REF_ROOT], check=True)
     if not oracle_mod.ref_available():
         pytest.skip("reference sources not available on this machine")
     return oracle_mod

@@ -2,8 +2,8 @@
 device AES-CTR run needs besides key and plaintext values.
 
 Generated from the reference compiled from its own sources (oracle/_ref, through oracle.RefPlans):
-the prime chain, the EvalMod bootstrap parameters and its series coefficients (from the
-stand-in EvalMod fit of oracle/ref_evalmod_stub.cpp), the rotation-key set, every
+the prime chain, the EvalMod bootstrap parameters and its series coefficients (the reference's
+own MPFR fit, src/math/poly_approx.cpp:565), the rotation-key set, every
 SlotToCoeff (input scale ratio 1 and 2) and CoeffToSlot stage's shape (diagonal indices,
 baby-step count, limbs, slot count, rescale flag), the switching-key shapes and the level and
 scales of the encrypted AES key bits.  Values that do not steer the operation sequence (key

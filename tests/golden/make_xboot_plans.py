@@ -5,7 +5,7 @@ values.
 
 Generated from the reference compiled from its own sources (oracle/_ref, through oracle.RefPlans)
 like walsh15_plan.json: prime chain, EvalMod bootstrap parameters and series coefficients (from
-the stand-in EvalMod fit of oracle/ref_evalmod_stub.cpp), rotation-key set, every SlotToCoeff and
+the reference's own MPFR EvalMod fit, src/math/poly_approx.cpp:565), rotation-key set, every SlotToCoeff and
 CoeffToSlot stage's shape, switching-key shapes, and the levels and scales of the encrypted
 round-key bits (ckks_aes128_encrypt_expanded_round_key_bits with the first round key 4 levels up,
 as the reference benchmark encrypts them).  Residues are not stored: the benchmark draws them at

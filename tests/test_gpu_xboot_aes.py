@@ -19,8 +19,8 @@ reference):
 * the serving path over XBOOT evaluations (wg_serve_create_xboot): three odd-sized requests
   queued within the batching window share one evaluation, each decrypting to its own plaintext.
 
-The EvalMod polynomial is the one the reference context reports (its fit built by the
-harness's stand-in), so the parity holds for that polynomial."""
+The EvalMod polynomial is the one the reference context reports: the reference's own MPFR fit
+(src/math/poly_approx.cpp:565)."""
 import time
 
 import numpy as np
