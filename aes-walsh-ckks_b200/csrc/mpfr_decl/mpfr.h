@@ -1,12 +1,12 @@
-/* Declarations of the MPFR 4.x entry points that the reference's EvalMod fit
- * (src/math/poly_approx.cpp) calls.  TEST INFRASTRUCTURE ONLY.
+/* Declarations of the MPFR 4.x entry points used to fit the EvalMod Chebyshev series in
+ * 256-bit arithmetic (wg_evalmod_fit.cpp, and the reference's src/math/poly_approx.cpp when the
+ * oracle recipe compiles it).
  *
- * This image carries the MPFR runtime (libmpfr.so.6) but not its development header, so the
- * recipe in oracle/Makefile compiles the reference's poly_approx.cpp against this header and
- * links the installed runtime by its versioned name.  Only the public interface is declared:
- * the documented mpfr_t record (precision, sign, exponent, limb pointer) of LP64 builds, the
- * rounding-mode enumeration, and one prototype per function used; every function named here
- * is an exported symbol of libmpfr.so.6. */
+ * The image carries the MPFR runtime (libmpfr.so.6) but not its development header, so this
+ * header declares the public interface only: the documented mpfr_t record (precision, sign,
+ * exponent, limb pointer) of LP64 builds, the rounding-mode enumeration, and one prototype per
+ * function used; every function named here is an exported symbol of libmpfr.so.6, which the
+ * builds link by its versioned name. */
 #ifndef WG_ORACLE_MPFR_DECL_H
 #define WG_ORACLE_MPFR_DECL_H
 

@@ -72,9 +72,21 @@ void batch_graph_launch(BatchGraph& g, cudaStream_t s);
 
 // One baby-step / giant-step linear-transform stage (wg_bsgs.cu).
 struct LtStage;
+// diags == nullptr: allocate the diagonal store only (filled by the caller through lt_stage_data).
 LtStage* lt_stage_create(Context& c, size_t level, size_t nterms, const uint64_t* indices, const uint64_t* diags,
                          size_t baby, size_t slots, bool rescale);
 void lt_stage_destroy(LtStage* st);
+uint64_t* lt_stage_data(LtStage& st);  // [term][QP limbs][N], Montgomery form
+void lt_stage_set_plaintext_scale(LtStage& st, double scale);
+// level, term count, baby steps, logical slots, rescale flag, plaintext scale (0 if not known)
+void lt_stage_info(const LtStage& st, size_t& level, size_t& nterms, size_t& baby, size_t& slots, bool& rescale,
+                   double& pt_scale);
+const std::vector<size_t>& lt_stage_indices(const LtStage& st);
+namespace dft {
+struct Literal;
+}
+// The factorized DFT's stages generated and encoded on the context's device (wg_dftplan_dev.cu).
+std::vector<LtStage*> dft_plan_create(Context& c, const dft::Literal& lit, cudaStream_t s);
 void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const* b, uint64_t* const* a,
                     cudaStream_t s);
 
@@ -166,6 +178,10 @@ void xboot_encrypt_round_key_bits(Context& c, const BootstrapParams& p, const ui
 // out[c] (limbs limbs), evaluation form when `eval`, else coefficient form (wg_encode_dev.cu).
 void encode_slots_device(Context& c, size_t count, size_t limbs, double scale, const double* re, const double* im,
                          uint64_t* const* out, bool eval, cudaStream_t s);
+// The same encoding into an arbitrary basis (modulus index per limb: Q moduli 0..nq-1, P moduli
+// nq..), optionally converted to Montgomery form after the NTT.
+void encode_slots_device_basis(Context& c, size_t count, const std::vector<int>& mods, double scale, const double* re,
+                               const double* im, uint64_t* const* out, bool eval, bool montgomery, cudaStream_t s);
 // ckks_decrypt on the device (wg_encode_dev.cu): slots of `count` ciphertexts at `level` (b, a
 // and optional c2 per ciphertext; scales[k] each) under the ternary `secret`, into host arrays
 // re / im [count][N/2].

@@ -40,10 +40,24 @@ struct LtStage {
     size_t baby = 0;
     size_t slots = 0;
     bool rescale = false;
+    double pt_scale = 0.0;       // plaintext scale of the diagonals (0: not known)
     std::vector<size_t> indices;
     uint64_t* d_diag = nullptr;  // [term][QP limbs][N], Montgomery form
     ~LtStage() { cudaFree(d_diag); }
 };
+
+uint64_t* lt_stage_data(LtStage& st) { return st.d_diag; }
+void lt_stage_set_plaintext_scale(LtStage& st, double scale) { st.pt_scale = scale; }
+void lt_stage_info(const LtStage& st, size_t& level, size_t& nterms, size_t& baby, size_t& slots, bool& rescale,
+                   double& pt_scale) {
+    level = st.level;
+    nterms = st.nterms;
+    baby = st.baby;
+    slots = st.slots;
+    rescale = st.rescale;
+    pt_scale = st.pt_scale;
+}
+const std::vector<size_t>& lt_stage_indices(const LtStage& st) { return st.indices; }
 
 namespace {
 
@@ -300,7 +314,7 @@ LtStage* lt_stage_create(Context& c, size_t level, size_t nterms, const uint64_t
         cudaGetLastError();
         fail(kNoMemory, "linear transform: diagonal allocation failed");
     }
-    check_cuda(cudaMemcpy(st->d_diag, diags, words * 8, cudaMemcpyHostToDevice), "upload diagonals");
+    if (diags) check_cuda(cudaMemcpy(st->d_diag, diags, words * 8, cudaMemcpyHostToDevice), "upload diagonals");
     return st.release();
 }
 
@@ -419,8 +433,11 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
         std::stable_sort(group.begin(), group.end(), [](const TermRef& x, const TermRef& y) { return x.slot < y.slot; });
         const size_t off = terms.size();
         terms.insert(terms.end(), group.begin(), group.end());
-        for (size_t ci = 0; ci < count; ++ci)
-            for (size_t i = 0; i < T; ++i)
+        // limb-outer, ciphertext-inner: the blocks of consecutive jobs read the same diagonal
+        // words (this group's terms on limb i), so each diagonal limb comes from HBM once per
+        // batch and from L2 for the other ciphertexts
+        for (size_t i = 0; i < T; ++i)
+            for (size_t ci = 0; ci < count; ++ci)
                 giant_jobs.push_back({babybuf, inner, (int)off, (int)group.size(), (int)i, (int)g0, (int)gn, (int)ci});
     }
     // 4. giants >= 1: single ModDown of inner a, then QP key switch from that key term

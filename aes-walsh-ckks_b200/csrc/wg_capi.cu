@@ -1,6 +1,7 @@
 // C ABI (include/walsh_gpu.h): argument checks, key registry, workspace routing and the
 // operation sequences of rotation, conjugation, relinearization and the batched workload.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -9,6 +10,8 @@
 #include "../../include/walsh_gpu.h"
 #include "wg_batch.hpp"
 #include "wg_encode.hpp"
+#include "wg_evalmod_fit.hpp"
+#include "wg_dftplan.hpp"
 #include "wg_internal.hpp"
 #include "wg_serve.hpp"
 
@@ -252,6 +255,52 @@ int wg_ntt_forward(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, 
 int wg_ntt_inverse(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, int basis, size_t polys,
                    size_t poly_stride, void* stream) {
     return ntt_call(ctx, poly, limbs, first, basis, polys, poly_stride, stream, false);
+}
+
+int wg_evalmod_fit(double K, size_t degree, size_t double_angle, double interval_radius, size_t validation_points,
+                   double prune_threshold, double* coeffs, size_t* ncoeffs, double* max_error, double* interval) {
+    return guard([&] {
+        if (!coeffs || !ncoeffs) wg::fail(wg::kInvalid, "evalmod fit: null output");
+        const wg::fit::EvalModFit f =
+            wg::fit::fit_evalmod(K, degree, double_angle, interval_radius, validation_points, prune_threshold);
+        if (f.coeffs.size() > degree + 1) wg::fail(wg::kRuntime, "evalmod fit: more coefficients than degree + 1");
+        std::copy(f.coeffs.begin(), f.coeffs.end(), coeffs);
+        *ncoeffs = f.coeffs.size();
+        if (max_error) *max_error = f.max_error;
+        if (interval) {
+            interval[0] = f.interval_min;
+            interval[1] = f.interval_max;
+        }
+    });
+}
+
+int wg_evalmod_k_bound(size_t coefficients, size_t hamming_weight, double log2_failure, size_t* k) {
+    return guard([&] {
+        if (!k) wg::fail(wg::kInvalid, "evalmod K bound: null output");
+        *k = wg::fit::evalmod_k_bound(coefficients, hamming_weight, std::exp2((long double)log2_failure));
+    });
+}
+
+int wg_ntt_tuning(const wg_context* ctx, int* chosen, float* ms, int* limbs) {
+    return guard([&] {
+        if (!ctx || !ctx->c) wg::fail(wg::kInvalid, "null context");
+        const wg::Context& c = *ctx->c;
+        for (int d = 0; d < 2; ++d)
+            for (int p = 0; p < 2; ++p) {
+                if (chosen) chosen[d * 2 + p] = c.ntt_variant[d][p];
+                for (int v = 0; v < wg::kNttGeometries && ms; ++v) ms[(d * 2 + p) * wg::kNttGeometries + v] = c.tuning.ms[d][p][v];
+            }
+        if (limbs) *limbs = c.tuning.limbs;
+    });
+}
+
+int wg_ntt_set_geometry(wg_context* ctx, int direction, int phase, int geometry) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        if (direction < 0 || direction > 1 || phase < 0 || phase > 1) wg::fail(wg::kInvalid, "ntt: invalid direction or phase");
+        if (geometry >= wg::kNttGeometries) wg::fail(wg::kInvalid, "ntt: unknown geometry");
+        c.ntt_variant[direction][phase] = geometry < 0 ? c.tuning.chosen[direction][phase] : geometry;
+    });
 }
 
 int wg_keyswitch(wg_context* ctx, size_t level, const uint64_t* key_term, int kind, int64_t rotation, uint64_t* b,
@@ -1072,6 +1121,102 @@ int wg_lt_stage_create(wg_context* ctx, size_t level, size_t nterms, const uint6
                                               rescale_after != 0);
         *out = new wg_lt_stage{st};
     });
+}
+
+int wg_lt_stage_info(const wg_lt_stage* st, size_t* level, size_t* nterms, size_t* baby, size_t* slots,
+                     int* rescale_after, double* plaintext_scale) {
+    return guard([&] {
+        if (!st || !st->s) wg::fail(wg::kInvalid, "ckks_linear_transform: null stage");
+        size_t l, n, b, sl;
+        bool r;
+        double ps;
+        wg::lt_stage_info(*st->s, l, n, b, sl, r, ps);
+        if (level) *level = l;
+        if (nterms) *nterms = n;
+        if (baby) *baby = b;
+        if (slots) *slots = sl;
+        if (rescale_after) *rescale_after = r ? 1 : 0;
+        if (plaintext_scale) *plaintext_scale = ps;
+    });
+}
+
+int wg_lt_stage_download(wg_context* ctx, const wg_lt_stage* st, uint64_t* indices, uint64_t* diagonals) {
+    return guard([&] {
+        wg::Context& c = C(ctx);
+        if (!st || !st->s) wg::fail(wg::kInvalid, "ckks_linear_transform: null stage");
+        wg::BundleStage b;
+        wg::lt_stage_export(c, *st->s, b);
+        if (indices) std::copy(b.indices.begin(), b.indices.end(), indices);
+        if (diagonals) std::copy(b.diagonals.begin(), b.diagonals.end(), diagonals);
+    });
+}
+
+static wg::dft::Literal dft_literal(const wg_dft_literal* lit) {
+    if (!lit) wg::fail(wg::kInvalid, "ckks_bootstrap_dft: null literal");
+    wg::dft::Literal L;
+    L.coeffs_to_slots = lit->coeffs_to_slots != 0;
+    L.level = lit->level;
+    L.baby_step_count = lit->baby_step_count;
+    L.log_bsgs_ratio = lit->log_bsgs_ratio;
+    L.stage_count = lit->stage_count;
+    size_t k = 0;
+    for (size_t g = 0; g < lit->ngroups; ++g) {
+        if (!lit->group_sizes || !lit->group_bits) wg::fail(wg::kInvalid, "ckks_bootstrap_dft: null scale schedule");
+        L.scale_groups.emplace_back(lit->group_bits + k, lit->group_bits + k + lit->group_sizes[g]);
+        k += lit->group_sizes[g];
+    }
+    if (lit->nmerge) {
+        if (!lit->merge_depths) wg::fail(wg::kInvalid, "ckks_bootstrap_dft: null merge depths");
+        L.merge_depths.assign(lit->merge_depths, lit->merge_depths + lit->nmerge);
+    }
+    L.active_slots = lit->active_slots;
+    L.transform_scale = lit->transform_scale;
+    L.input_selector_start = lit->input_selector_start;
+    L.input_selector_size = lit->input_selector_size;
+    return L;
+}
+
+int wg_dft_plan_describe(uint64_t N, const uint64_t* q, size_t nq, const wg_dft_literal* lit, size_t stage,
+                         size_t* nstages, size_t* level, size_t* nterms, size_t* baby, int* rescale_after,
+                         double* plaintext_scale, uint64_t* indices, double* diagonals) {
+    return guard([&] {
+        if (!q || nq == 0) wg::fail(wg::kInvalid, "ckks_bootstrap_dft: empty modulus chain");
+        if (N < 1024 || N > 65536 || (N & (N - 1))) wg::fail(wg::kInvalid, "ckks_bootstrap_dft: invalid ring degree");
+        const auto stages = wg::dft::generate_plan(dft_literal(lit), N, std::vector<uint64_t>(q, q + nq));
+        if (nstages) *nstages = stages.size();
+        if (stage >= stages.size()) wg::fail(wg::kInvalid, "ckks_bootstrap_dft: stage index out of range");
+        const auto& st = stages[stage];
+        if (level) *level = st.level;
+        if (nterms) *nterms = st.indices.size();
+        if (baby) *baby = st.baby;
+        if (rescale_after) *rescale_after = st.rescale_after ? 1 : 0;
+        if (plaintext_scale) *plaintext_scale = st.plaintext_scale;
+        if (indices) std::copy(st.indices.begin(), st.indices.end(), indices);
+        if (diagonals)
+            for (size_t t = 0; t < st.diagonals.size(); ++t)
+                for (size_t i = 0; i < st.diagonals[t].size(); ++i) {
+                    diagonals[2 * (t * st.slots + i)] = st.diagonals[t][i].real();
+                    diagonals[2 * (t * st.slots + i) + 1] = st.diagonals[t][i].imag();
+                }
+    });
+}
+
+int wg_dft_plan_create(wg_context* ctx, const wg_dft_literal* lit, wg_lt_stage** stages, size_t max_stages,
+                       size_t* nstages, void* stream) {
+    std::vector<wg::LtStage*> made;
+    const int rc = guard([&] {
+        wg::Context& c = C(ctx);
+        if (!lit || !stages || !nstages) wg::fail(wg::kInvalid, "ckks_bootstrap_dft: null argument");
+        const wg::dft::Literal L = dft_literal(lit);
+        wg::check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+        made = wg::dft_plan_create(c, L, S(stream));
+        *nstages = made.size();
+        if (made.size() > max_stages) wg::fail(wg::kInvalid, "ckks_bootstrap_dft: more stages than max_stages");
+        for (size_t i = 0; i < made.size(); ++i) stages[i] = new wg_lt_stage{made[i]};
+        made.clear();
+    });
+    for (auto* m : made) wg::lt_stage_destroy(m);
+    return rc;
 }
 
 void wg_lt_stage_destroy(wg_lt_stage* st) {

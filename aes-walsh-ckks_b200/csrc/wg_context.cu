@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "wg_internal.hpp"
+#include "wg_ntt.cuh"
 #include "wg_ring.hpp"
 #include "wg_tables.hpp"
 
@@ -273,7 +274,13 @@ Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t
     c->tables_words = H.words.size() + 1;
     dev_alloc((void**)&c->d_tables, c->tables_words * 8);
     check_cuda(cudaMemcpy(c->d_mod, c->mods.data(), nm * sizeof(Modulus), cudaMemcpyHostToDevice), "upload moduli");
-    check_cuda(cudaMemcpy(c->d_tw, H.tw.data(), H.tw.size() * 8, cudaMemcpyHostToDevice), "upload twiddles");
+    {
+        // interleaved (w, Shoup w) pairs per modulus and direction, as the NTT kernels read them
+        std::vector<ntt::TwPair> pairs(nm * 2 * N);
+        for (size_t i = 0; i < nm; ++i) ntt::interleave_twiddles(N, H.tw.data() + i * 4 * N, pairs.data() + i * 2 * N);
+        check_cuda(cudaMemcpy(c->d_tw, pairs.data(), pairs.size() * sizeof(ntt::TwPair), cudaMemcpyHostToDevice),
+                   "upload twiddles");
+    }
     check_cuda(cudaMemcpy(c->d_tables, H.words.data(), H.words.size() * 8, cudaMemcpyHostToDevice),
                "upload tables");
     const uint64_t* T = c->d_tables;
@@ -326,6 +333,7 @@ Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t
         c->rs_inv_p_s[d] = T + H.rescale[d] + 2 * d;
         c->rs_half[d] = T + H.rescale[d] + 3 * d;
     }
+    ntt_autotune(*c);
     return c.release();
 }
 

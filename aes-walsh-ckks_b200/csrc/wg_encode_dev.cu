@@ -174,13 +174,40 @@ __global__ void __launch_bounds__(kT) kb_extract_slots(const double2* __restrict
     im[t] = v.y / scale[c];
 }
 
+// x = x * (2^64 mod q) with the Barrett product, limb by limb (the Montgomery form of the
+// reference's precomputed plaintexts, ckks_convert_plaintext_to_montgomery_inplace,
+// src/ckks/encoding/ckks_encoding.cpp:177-194).
+struct MontJob {
+    uint64_t* x;
+    uint64_t r;  // 2^64 mod q
+    int mod, pad;
+};
+
+__global__ void __launch_bounds__(kT) kb_to_montgomery(const MontJob* jobs, int n, const Modulus* mods) {
+    const MontJob* j = job_of(jobs, n);
+    if (!j) return;
+    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
+    j->x[k] = barrett_mul(j->x[k], j->r, mods[j->mod]);
+}
+
 }  // namespace
 
 void encode_slots_device(Context& c, size_t count, size_t limbs, double scale, const double* re, const double* im,
                          uint64_t* const* out, bool eval, cudaStream_t s) {
+    if (limbs == 0 || limbs > c.nq) throw std::invalid_argument("ckks_encode: invalid level");
+    std::vector<int> mods(limbs);
+    for (size_t l = 0; l < limbs; ++l) mods[l] = (int)l;
+    encode_slots_device_basis(c, count, mods, scale, re, im, out, eval, false, s);
+}
+
+void encode_slots_device_basis(Context& c, size_t count, const std::vector<int>& mods, double scale, const double* re,
+                               const double* im, uint64_t* const* out, bool eval, bool montgomery, cudaStream_t s) {
     if (count == 0) return;
     if (!(scale > 0.0)) throw std::invalid_argument("ckks_encode: scale must be positive");
-    if (limbs == 0 || limbs > c.nq) throw std::invalid_argument("ckks_encode: invalid level");
+    const size_t limbs = mods.size();
+    if (limbs == 0) throw std::invalid_argument("ckks_encode: invalid level");
+    for (int m : mods)
+        if (m < 0 || m >= (int)(c.nq + c.np)) throw std::invalid_argument("ckks_encode: invalid modulus index");
     if (!re || !im) throw std::invalid_argument("ckks_encode: null slot values");
     const size_t N = c.N, half = N >> 1;
     std::vector<double> tw;
@@ -211,14 +238,18 @@ void encode_slots_device(Context& c, size_t count, size_t limbs, double scale, c
         check_cuda(cudaGetLastError(), "encode transform");
         std::vector<EncodeOutJob> jobs;
         std::vector<NttJob> ntt;
+        std::vector<MontJob> mont;
         for (size_t ci = 0; ci < count; ++ci)
             for (size_t l = 0; l < limbs; ++l) {
-                jobs.push_back({out[ci] + l * N, (int)ci, (int)l});
-                ntt.push_back({out[ci] + l * N, out[ci] + l * N, (int)l, 0});
+                jobs.push_back({out[ci] + l * N, (int)ci, mods[l]});
+                ntt.push_back({out[ci] + l * N, out[ci] + l * N, mods[l], 0});
+                const uint64_t q = c.mods[mods[l]].q;
+                mont.push_back({out[ci] + l * N, (uint64_t)(((unsigned __int128)1 << 64) % q), mods[l], 0});
             }
         JobTable t;
         const EncodeOutJob* jo = t.add(jobs);
         const NttJob* jn = t.add(ntt);
+        const MontJob* jm = t.add(mont);
         t.upload(c, s);
         {
             Probe probe(kClsElementwise, (16.0 + 8.0) * N * jobs.size(), s);
@@ -226,6 +257,10 @@ void encode_slots_device(Context& c, size_t count, size_t limbs, double scale, c
                                                                   scale / static_cast<double>(N), N, c.d_mod);
         }
         if (eval) ntt_jobs(c, t.at(jn), (int)ntt.size(), true, s);
+        if (montgomery) {
+            Probe probe(kClsElementwise, 16.0 * N * mont.size(), s);
+            kb_to_montgomery<<<grid_for(c, mont.size()), kT, 0, s>>>(t.at(jm), (int)mont.size(), c.d_mod);
+        }
         check_cuda(cudaGetLastError(), "encode output");
         check_cuda(cudaFreeAsync(ws, s), "encode scratch");
         ws = nullptr;

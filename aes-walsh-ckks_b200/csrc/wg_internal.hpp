@@ -121,6 +121,16 @@ struct BatchBuffers {
     void release();
 };
 
+// NTT geometries (wg_ntt.cu): 0 = 8 residues per thread, staged twiddles; 1 = 8, twiddles
+// from the table; 2 = 16, staged; 3 = 16, from the table.  Device timings of each (ms, best of
+// three over a scratch batch) per [direction: forward, inverse][phase: rows, columns].
+constexpr int kNttGeometries = 4;
+struct NttTuning {
+    float ms[2][2][kNttGeometries];
+    int chosen[2][2];
+    int limbs;  // limbs of the timed batch
+};
+
 struct Context {
     int device = 0;
     uint64_t N = 0;
@@ -129,7 +139,9 @@ struct Context {
     std::vector<uint64_t> q, p;
     std::vector<Modulus> mods;       // nq + np entries (P after Q)
     Modulus* d_mod = nullptr;
-    uint64_t* d_tw = nullptr;        // [mod][4][N]: fwd, fwd_shoup, inv, inv_shoup
+    uint64_t* d_tw = nullptr;        // [mod][2][N] (w, Shoup w) pairs: forward, inverse (ntt::TwPair)
+    int ntt_variant[2][2] = {{0, 0}, {0, 0}};  // NTT geometry per [direction][phase: rows, columns]
+    NttTuning tuning{};
     // ModUp descriptors, host copies holding device pointers: [level][part]
     std::vector<std::vector<ModUpDesc>> modup;
     uint64_t* d_tables = nullptr;    // backing store for all small tables
@@ -191,7 +203,6 @@ struct Context {
         const size_t p_ = (L + alpha - 1) / alpha;
         return p_ < dnum ? p_ : dnum;
     }
-    const uint64_t* tw(int mod) const { return d_tw + (size_t)mod * 4 * N; }
 };
 
 // Modulus-index rule for a batch of limbs: limb l of a polynomial uses modulus
@@ -244,6 +255,12 @@ struct NttJob {
     int pad;
 };
 void ntt_jobs(const Context& c, const NttJob* d_jobs, int njobs, bool forward, cudaStream_t s);
+// Time every NTT geometry on the context's device and keep the fastest per direction and phase
+// (cached per device and ring degree for the process).
+void ntt_autotune(Context& c);
+// One phase (cols: the high-bit phase) of a strided batch with a given geometry.
+void ntt_phase_geometry(const Context& c, bool forward, bool cols, int variant, uint64_t* data, int limbs,
+                        int polys, size_t poly_stride, LimbMap map, cudaStream_t s);
 
 // NTT over `polys` polynomials of `limbs` limbs each, `poly_stride` words apart.
 void ntt_forward(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride,

@@ -10,13 +10,21 @@
 //     "row" phase the n2 low bits.  Forward = columns then rows, inverse = rows then columns.
 //   * a CTA stages a 2048-element tile (or the whole limb for N < 2048) in shared memory with
 //     one pad word every 16 words, so strided 64-bit accesses stay at two wavefronts per warp;
-//   * each thread carries 8 elements through up to three radix-2 stages in registers per
-//     round (one shared-memory round trip per three stages);
+//   * each thread carries 8 or 16 elements (the geometry's EB) through up to three or four
+//     radix-2 stages in registers per round (one shared-memory round trip per round);
+//   * twiddles come as (w, Shoup w) pairs, one 16-byte load each, either staged in shared
+//     memory per CTA or read from the L2-resident table directly (the geometry's STAGED);
 //   * grid.y indexes limbs and grid.z polynomials, so one launch covers a whole ciphertext
 //     batch; each limb picks its modulus through a LimbMap (Q limbs, P limbs or a mix).
 // Butterflies are Harvey/Shoup with lazy ranges: forward values stay in [0, 4q) (or, for moduli
 // below 2^58, grow by at most 2q per stage without reduction, see kLazyForwardLimit), inverse
 // in [0, 2q); the last phase canonicalises (forward) or scales by N^-1 with Shoup (inverse).
+// Every geometry performs the same butterflies on the same values, so all of them give the
+// same words; which one runs is chosen per (direction, phase) by timing them on the device
+// when a context is created (ntt_autotune).
+#include <algorithm>
+#include <map>
+#include <mutex>
 #include <utility>
 
 #include "wg_internal.hpp"
@@ -26,33 +34,40 @@ namespace wg {
 namespace {
 using namespace ntt;
 
-template <int LOGN, bool FWD, bool COLS, bool LAZY, int... RD>
-__device__ __forceinline__ void ntt_rounds(std::integer_sequence<int, RD...>, uint64_t* sm, int sub,
-                                           int o, uint64_t q, const uint64_t* tw, const uint64_t* tws) {
-    ((ntt_round<LOGN, FWD, COLS, RD, LAZY>(sm, sub, o, q, tw, tws), __syncthreads()), ...);
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, bool LAZY, int... RD>
+__device__ __forceinline__ void ntt_rounds(std::integer_sequence<int, RD...>, uint64_t* sm, int sub, int o, int tile,
+                                           uint64_t q, const TwPair* tw) {
+    ((ntt_round<LOGN, FWD, COLS, EB, STAGED, RD, LAZY>(sm, sub, o, tile, q, tw), __syncthreads()), ...);
 }
 
-template <int LOGN, bool FWD, bool COLS>
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED>
 constexpr size_t smem_bytes() {
-    using P = Phase<LOGN, FWD, COLS>;
-    return 8 * (size_t)(P::TILE + P::TILE / 16 + 2 * P::TW);
+    using P = Phase<LOGN, FWD, COLS, EB, STAGED>;
+    return 8 * (size_t)(P::TILE + P::TILE / 16) + (STAGED ? 16 * (size_t)P::TW : 0);
+}
+
+// Registers: 8-residue rounds fit 64 registers (4 CTAs of 256 threads per SM); 16-residue
+// rounds get up to 128 (4 CTAs of 128 threads).
+template <int EB>
+constexpr int min_blocks() {
+    return 4;
 }
 
 // Addressing of one limb: either a strided batch (blockIdx.y = limb, blockIdx.z = polynomial,
 // modulus from a LimbMap) or an entry of a job table (blockIdx.y + 65535 * blockIdx.z).  The
 // first phase may read from a different buffer than it writes (src -> dst); the second phase
 // works in place on dst.
-template <int LOGN, bool FWD, bool COLS, bool TABLE>
-__global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS, 4)
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, bool TABLE>
+__global__ void __launch_bounds__(Phase<LOGN, FWD, COLS, EB, STAGED>::THREADS, min_blocks<EB>())
     k_ntt_phase(uint64_t* __restrict__ data, size_t poly_stride, LimbMap map, const NttJob* __restrict__ jobs,
-                int njobs, const Modulus* __restrict__ mods, const uint64_t* __restrict__ tw_base) {
-    using P = Phase<LOGN, FWD, COLS>;
+                int njobs, const Modulus* __restrict__ mods, const TwPair* __restrict__ tw_base) {
+    using P = Phase<LOGN, FWD, COLS, EB, STAGED>;
     constexpr int N = P::N;
+    constexpr int E = P::E;
     constexpr bool FIRST = FWD ? COLS : !COLS;
-    extern __shared__ uint64_t smem[];
-    uint64_t* sm = smem;                                  // data tile, padded
-    uint64_t* tw_s = smem + P::TILE + P::TILE / 16;       // staged twiddles
-    uint64_t* tws_s = tw_s + P::TW;
+    extern __shared__ __align__(16) uint64_t smem[];
+    uint64_t* sm = smem;                                                             // data tile, padded
+    TwPair* tw_s = reinterpret_cast<TwPair*>(smem + P::TILE + P::TILE / 16);        // staged twiddles
 
     const uint64_t* __restrict__ xin;
     uint64_t* __restrict__ x;
@@ -71,31 +86,28 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS, 4)
         mi = map(limb);
     }
     const uint64_t q = mods[mi].q;
-    const uint64_t* tw = tw_base + (size_t)mi * 4 * N + (FWD ? 0 : 2 * N);
-    const uint64_t* tws = tw + N;
+    const TwPair* tw = tw_base + (size_t)mi * 2 * N + (FWD ? 0 : N);
     const int tile = blockIdx.x;
     const int t = threadIdx.x;
 
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < E; ++k) {
         const int e = t + k * P::THREADS;
-        sm[pad16(e)] = xin[tile_offset<LOGN, FWD, COLS>(tile, e)];
+        sm[pad16(e)] = xin[tile_offset<LOGN, FWD, COLS, EB, STAGED>(tile, e)];
     }
-    if (COLS) {
-        for (int e = t; e < P::TW; e += P::THREADS) {
-            tw_s[e] = __ldg(tw + e);
-            tws_s[e] = __ldg(tws + e);
-        }
-    } else {
-        // row-stage k: SUBS * 2^k contiguous table entries (twiddle_src order)
+    if (STAGED) {
+        const ulonglong2* src2 = reinterpret_cast<const ulonglong2*>(tw);
+        ulonglong2* dst2 = reinterpret_cast<ulonglong2*>(tw_s);
+        if (COLS) {
+            for (int e = t; e < P::TW; e += P::THREADS) dst2[e] = __ldg(src2 + e);
+        } else {
+            // row-stage k: SUBS * 2^k contiguous table entries (twiddle_src order)
 #pragma unroll
-        for (int k = 0; k < P::MB; ++k) {
-            const int cnt = P::SUBS << k;
-            const int dst = P::SUBS * ((1 << k) - 1);
-            const size_t src = ((size_t)1 << (P::NB1 + k)) + (size_t)tile * cnt;
-            for (int e = t; e < cnt; e += P::THREADS) {
-                tw_s[dst + e] = __ldg(tw + src + e);
-                tws_s[dst + e] = __ldg(tws + src + e);
+            for (int k = 0; k < P::MB; ++k) {
+                const int cnt = P::SUBS << k;
+                const int dst = P::SUBS * ((1 << k) - 1);
+                const size_t src = ((size_t)1 << (P::NB1 + k)) + (size_t)tile * cnt;
+                for (int e = t; e < cnt; e += P::THREADS) dst2[dst + e] = __ldg(src2 + src + e);
             }
         }
     }
@@ -103,12 +115,15 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS, 4)
 
     const int sub = COLS ? t % P::SUBS : t >> P::OB;
     const int o = COLS ? t / P::SUBS : t & ((1 << P::OB) - 1);
+    const TwPair* twr = STAGED ? tw_s : tw;
     // forward transforms under kLazyForwardLimit skip the per-butterfly reduction (uniform per CTA)
     const bool lazy = FWD && q < kLazyForwardLimit;
     if (lazy)
-        ntt_rounds<LOGN, FWD, COLS, true>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, q, tw_s, tws_s);
+        ntt_rounds<LOGN, FWD, COLS, EB, STAGED, true>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, tile,
+                                                      q, twr);
     else
-        ntt_rounds<LOGN, FWD, COLS, false>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, q, tw_s, tws_s);
+        ntt_rounds<LOGN, FWD, COLS, EB, STAGED, false>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, tile,
+                                                       q, twr);
 
     uint64_t n_inv = 0, n_inv_s = 0;
     if (P::LAST && !FWD) {
@@ -116,55 +131,83 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS>::THREADS, 4)
         n_inv_s = mods[mi].n_inv_shoup;
     }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < E; ++k) {
         const int e = t + k * P::THREADS;
         uint64_t val = sm[pad16(e)];
         if (P::LAST) val = FWD ? (lazy ? reduce64(val, mods[mi]) : red4q(val, q)) : mul_shoup(val, n_inv, n_inv_s, q);
-        x[tile_offset<LOGN, FWD, COLS>(tile, e)] = val;
+        x[tile_offset<LOGN, FWD, COLS, EB, STAGED>(tile, e)] = val;
     }
 }
 
-template <int LOGN, bool FWD, bool COLS, bool TABLE>
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, bool TABLE>
 void enable_smem() {
     // opt in to more than 48 KiB of dynamic shared memory once per kernel instance
     static const bool done = [] {
-        cudaFuncSetAttribute(k_ntt_phase<LOGN, FWD, COLS, TABLE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_bytes<LOGN, FWD, COLS>());
+        cudaFuncSetAttribute(k_ntt_phase<LOGN, FWD, COLS, EB, STAGED, TABLE>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<LOGN, FWD, COLS, EB, STAGED>());
         return true;
     }();
     (void)done;
 }
 
-template <int LOGN, bool FWD, bool COLS>
-void launch_phase(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map,
-                  const NttJob* jobs, int njobs, cudaStream_t s) {
-    using P = Phase<LOGN, FWD, COLS>;
-    constexpr size_t sm = smem_bytes<LOGN, FWD, COLS>();
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED>
+void launch_geom(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map,
+                 const NttJob* jobs, int njobs, cudaStream_t s) {
+    using P = Phase<LOGN, FWD, COLS, EB, STAGED>;
+    constexpr size_t sm = smem_bytes<LOGN, FWD, COLS, EB, STAGED>();
+    const TwPair* tw = reinterpret_cast<const TwPair*>(c.d_tw);
     if (jobs) {
-        enable_smem<LOGN, FWD, COLS, true>();
+        enable_smem<LOGN, FWD, COLS, EB, STAGED, true>();
         const dim3 grid(P::N / P::TILE, njobs < 65535 ? njobs : 65535, (njobs + 65534) / 65535);
         // algorithmic bytes: every residue read once and written once per transform, i.e. 8 B
         // per residue for each of the two phases (16 N B per limb-transform)
         Probe probe(kClsNtt, 8.0 * P::N * njobs, s);
-        k_ntt_phase<LOGN, FWD, COLS, true><<<grid, P::THREADS, sm, s>>>(nullptr, 0, map, jobs, njobs, c.d_mod, c.d_tw);
+        k_ntt_phase<LOGN, FWD, COLS, EB, STAGED, true><<<grid, P::THREADS, sm, s>>>(nullptr, 0, map, jobs, njobs,
+                                                                                   c.d_mod, tw);
     } else {
-        enable_smem<LOGN, FWD, COLS, false>();
+        enable_smem<LOGN, FWD, COLS, EB, STAGED, false>();
         const dim3 grid(P::N / P::TILE, limbs, polys);
         Probe probe(kClsNtt, 8.0 * P::N * limbs * polys, s);
-        k_ntt_phase<LOGN, FWD, COLS, false><<<grid, P::THREADS, sm, s>>>(data, stride, map, nullptr, 0, c.d_mod,
-                                                                         c.d_tw);
+        k_ntt_phase<LOGN, FWD, COLS, EB, STAGED, false><<<grid, P::THREADS, sm, s>>>(data, stride, map, nullptr, 0,
+                                                                                    c.d_mod, tw);
+    }
+}
+
+// One phase with the geometry `variant` (kNttGeometries order).
+template <int LOGN, bool FWD, bool COLS>
+void launch_phase(const Context& c, int variant, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map,
+                  const NttJob* jobs, int njobs, cudaStream_t s) {
+    switch (variant) {
+        case 0: launch_geom<LOGN, FWD, COLS, 3, true>(c, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        case 1: launch_geom<LOGN, FWD, COLS, 3, false>(c, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        case 2: launch_geom<LOGN, FWD, COLS, 4, true>(c, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        default: launch_geom<LOGN, FWD, COLS, 4, false>(c, data, limbs, polys, stride, map, jobs, njobs, s); break;
     }
 }
 
 template <int LOGN>
-void run(const Context& c, uint64_t* data, int limbs, int polys, size_t stride, LimbMap map, const NttJob* jobs,
-         int njobs, bool fwd, cudaStream_t s) {
+void run_phase(const Context& c, bool fwd, bool cols, int variant, uint64_t* data, int limbs, int polys, size_t stride,
+               LimbMap map, const NttJob* jobs, int njobs, cudaStream_t s) {
     if (fwd) {
-        launch_phase<LOGN, true, true>(c, data, limbs, polys, stride, map, jobs, njobs, s);
-        launch_phase<LOGN, true, false>(c, data, limbs, polys, stride, map, jobs, njobs, s);
+        if (cols) launch_phase<LOGN, true, true>(c, variant, data, limbs, polys, stride, map, jobs, njobs, s);
+        else launch_phase<LOGN, true, false>(c, variant, data, limbs, polys, stride, map, jobs, njobs, s);
     } else {
-        launch_phase<LOGN, false, false>(c, data, limbs, polys, stride, map, jobs, njobs, s);
-        launch_phase<LOGN, false, true>(c, data, limbs, polys, stride, map, jobs, njobs, s);
+        if (cols) launch_phase<LOGN, false, true>(c, variant, data, limbs, polys, stride, map, jobs, njobs, s);
+        else launch_phase<LOGN, false, false>(c, variant, data, limbs, polys, stride, map, jobs, njobs, s);
+    }
+}
+
+void phase_dispatch(const Context& c, bool fwd, bool cols, int variant, uint64_t* data, int limbs, int polys,
+                    size_t stride, LimbMap map, const NttJob* jobs, int njobs, cudaStream_t s) {
+    switch (c.logN) {
+        case 10: run_phase<10>(c, fwd, cols, variant, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        case 11: run_phase<11>(c, fwd, cols, variant, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        case 12: run_phase<12>(c, fwd, cols, variant, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        case 13: run_phase<13>(c, fwd, cols, variant, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        case 14: run_phase<14>(c, fwd, cols, variant, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        case 15: run_phase<15>(c, fwd, cols, variant, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        case 16: run_phase<16>(c, fwd, cols, variant, data, limbs, polys, stride, map, jobs, njobs, s); break;
+        default: fail(kInvalid, "ntt: ring degree must be 2^10 .. 2^16");
     }
 }
 
@@ -172,18 +215,23 @@ void dispatch(const Context& c, uint64_t* data, int limbs, int polys, size_t str
               const NttJob* jobs, int njobs, bool fwd, cudaStream_t s) {
     if (jobs ? njobs <= 0 : (limbs <= 0 || polys <= 0)) return;
     if (!jobs && (polys > 65535 || limbs > 65535)) fail(kInvalid, "ntt: too many limbs or polynomials in one batch");
-    switch (c.logN) {
-        case 10: run<10>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
-        case 11: run<11>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
-        case 12: run<12>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
-        case 13: run<13>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
-        case 14: run<14>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
-        case 15: run<15>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
-        case 16: run<16>(c, data, limbs, polys, stride, map, jobs, njobs, fwd, s); break;
-        default: fail(kInvalid, "ntt: ring degree must be 2^10 .. 2^16");
-    }
+    const int d = fwd ? 0 : 1;
+    // forward: columns then rows; inverse: rows then columns
+    const bool first_cols = fwd;
+    phase_dispatch(c, fwd, first_cols, c.ntt_variant[d][first_cols ? 1 : 0], data, limbs, polys, stride, map, jobs,
+                   njobs, s);
+    phase_dispatch(c, fwd, !first_cols, c.ntt_variant[d][first_cols ? 0 : 1], data, limbs, polys, stride, map, jobs,
+                   njobs, s);
     check_cuda(cudaGetLastError(), "ntt launch");
 }
+
+// Tuned choices per (device, ring degree), shared by every context of the process.
+struct TuneKey {
+    int device, logN;
+    bool operator<(const TuneKey& o) const { return device != o.device ? device < o.device : logN < o.logN; }
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, NttTuning> g_tuned;
 
 }  // namespace
 
@@ -199,6 +247,96 @@ void ntt_inverse(const Context& c, uint64_t* data, int limbs, int polys, size_t 
 
 void ntt_jobs(const Context& c, const NttJob* d_jobs, int njobs, bool forward, cudaStream_t s) {
     dispatch(c, nullptr, 0, 0, 0, LimbMap{0, 0, 0}, d_jobs, njobs, forward, s);
+}
+
+void ntt_phase_geometry(const Context& c, bool forward, bool cols, int variant, uint64_t* data, int limbs, int polys,
+                        size_t poly_stride, LimbMap map, cudaStream_t s) {
+    if (variant < 0 || variant >= kNttGeometries) fail(kInvalid, "ntt: unknown geometry");
+    if (limbs <= 0 || polys <= 0) return;
+    phase_dispatch(c, forward, cols, variant, data, limbs, polys, poly_stride, map, nullptr, 0, s);
+    check_cuda(cudaGetLastError(), "ntt launch");
+}
+
+// Time every geometry of every (direction, phase) on a scratch batch larger than the L2 cache
+// (160 MB of limbs, as the batched circuits stream them) cycling over the context's moduli (so
+// lazy and full-reduction moduli are both represented), best of three launches after one
+// warm-up, and keep the fastest.  Phases are timed on their own: each is one full pass over the
+// batch whatever the other phase does, and every geometry computes the same words, so the
+// choices combine freely.
+void ntt_autotune(Context& c) {
+    {
+        std::lock_guard<std::mutex> g(g_tune_mutex);
+        auto it = g_tuned.find({c.device, c.logN});
+        if (it != g_tuned.end()) {
+            c.tuning = it->second;
+            for (int d = 0; d < 2; ++d)
+                for (int p = 0; p < 2; ++p) c.ntt_variant[d][p] = it->second.chosen[d][p];
+            return;
+        }
+    }
+    const size_t N = c.N;
+    const int kTuneLimbs = (int)((size_t{160} << 20) / (8 * N));
+    const int nm = (int)(c.nq + c.np);
+    check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+    uint64_t* buf = nullptr;
+    if (cudaMalloc(&buf, (size_t)kTuneLimbs * N * 8) != cudaSuccess) {
+        // no room for the timing batch: keep the default geometry (tuning.limbs = 0 says so)
+        cudaGetLastError();
+        return;
+    }
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    NttTuning tn{};
+    try {
+        check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "ntt autotune: stream");
+        check_cuda(cudaEventCreate(&e0), "ntt autotune: event");
+        check_cuda(cudaEventCreate(&e1), "ntt autotune: event");
+        check_cuda(cudaMemsetAsync(buf, 0, (size_t)kTuneLimbs * N * 8, s), "ntt autotune: clear");
+        // limb l uses modulus l mod nm: LimbMap{nA = kTuneLimbs, firstA = 0} would run past the
+        // moduli, so launch the batch as polynomials of nm limbs (the last one partial)
+        const int polys = kTuneLimbs / nm > 0 ? kTuneLimbs / nm : 1;
+        const int limbs = kTuneLimbs / nm > 0 ? nm : kTuneLimbs;
+        const LimbMap map{limbs, 0, 0};
+        for (int d = 0; d < 2; ++d)
+            for (int p = 0; p < 2; ++p) {
+                float best = 1e30f;
+                int best_v = 0;
+                for (int v = 0; v < kNttGeometries; ++v) {
+                    float t_best = 1e30f;
+                    for (int rep = 0; rep < 4; ++rep) {
+                        check_cuda(cudaEventRecord(e0, s), "ntt autotune: record");
+                        phase_dispatch(c, d == 0, p == 1, v, buf, limbs, polys, (size_t)limbs * N, map, nullptr, 0, s);
+                        check_cuda(cudaEventRecord(e1, s), "ntt autotune: record");
+                        check_cuda(cudaEventSynchronize(e1), "ntt autotune: wait");
+                        float ms = 0;
+                        check_cuda(cudaEventElapsedTime(&ms, e0, e1), "ntt autotune: time");
+                        if (rep > 0) t_best = std::min(t_best, ms);
+                    }
+                    tn.ms[d][p][v] = t_best;
+                    if (t_best < best) {
+                        best = t_best;
+                        best_v = v;
+                    }
+                }
+                tn.chosen[d][p] = best_v;
+            }
+        tn.limbs = limbs * polys;
+    } catch (...) {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (s) cudaStreamDestroy(s);
+        cudaFree(buf);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    cudaFree(buf);
+    c.tuning = tn;
+    for (int d = 0; d < 2; ++d)
+        for (int p = 0; p < 2; ++p) c.ntt_variant[d][p] = tn.chosen[d][p];
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    g_tuned[{c.device, c.logN}] = tn;
 }
 
 }  // namespace wg

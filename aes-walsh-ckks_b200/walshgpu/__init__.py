@@ -69,6 +69,14 @@ def lib() -> C.CDLL:
         L.wg_ctx_workspace_words.restype = sz
         for f in (L.wg_ntt_forward, L.wg_ntt_inverse):
             f.argtypes = [vp, vp, sz, sz, C.c_int, sz, sz, vp]
+        L.wg_ntt_tuning.argtypes = [vp, vp, vp, vp]
+        L.wg_evalmod_fit.argtypes = [C.c_double, sz, sz, C.c_double, sz, C.c_double, vp, vp, vp, vp]
+        L.wg_evalmod_k_bound.argtypes = [sz, sz, C.c_double, vp]
+        L.wg_dft_plan_describe.argtypes = [u64, vp, sz, vp, sz] + [vp] * 8
+        L.wg_dft_plan_create.argtypes = [vp, vp, vp, sz, vp, vp]
+        L.wg_lt_stage_info.argtypes = [vp] * 7
+        L.wg_lt_stage_download.argtypes = [vp, vp, vp, vp]
+        L.wg_ntt_set_geometry.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.wg_keyswitch.argtypes = [vp, sz, vp, C.c_int, C.c_int64, vp, vp, C.c_int, C.c_int, vp]
         L.wg_rotate.argtypes = [vp, sz, vp, vp, C.c_int64, vp]
         L.wg_rotate_noalloc.argtypes = [vp, sz, vp, vp, C.c_int64, vp]
@@ -222,6 +230,24 @@ def find_primes(p_bits, q_bits, N):
     return p, q
 
 
+def evalmod_fit(K, degree, double_angle, interval_radius, validation_points, prune_threshold):
+    """The EvalMod Chebyshev series (host, 256-bit): {"coeffs", "max_error", "interval"}."""
+    out = np.zeros(int(degree) + 1, np.float64)
+    n = C.c_size_t()
+    err = C.c_double()
+    iv = np.zeros(2, np.float64)
+    _check(lib().wg_evalmod_fit(float(K), int(degree), int(double_angle), float(interval_radius),
+                                int(validation_points), float(prune_threshold), out.ctypes.data, C.byref(n),
+                                C.byref(err), iv.ctypes.data))
+    return {"coeffs": out[: n.value].copy(), "max_error": err.value, "interval": (iv[0], iv[1])}
+
+
+def evalmod_k_bound(coefficients, hamming_weight, log2_failure):
+    k = C.c_size_t()
+    _check(lib().wg_evalmod_k_bound(int(coefficients), int(hamming_weight), float(log2_failure), C.byref(k)))
+    return k.value
+
+
 def to_device(arr, device="cuda"):
     """uint64 numpy array -> int64 torch tensor on the GPU (bit-identical)."""
     import torch
@@ -259,6 +285,23 @@ class LtStage:
         self.level = level
         self.rescale = rescale
 
+    def info(self):
+        """{"level", "nterms", "baby", "slots", "rescale", "plaintext_scale"} of the stage."""
+        lv, nt, bb, sl = C.c_size_t(), C.c_size_t(), C.c_size_t(), C.c_size_t()
+        rs, ps = C.c_int(), C.c_double()
+        _check(lib().wg_lt_stage_info(self.h, C.byref(lv), C.byref(nt), C.byref(bb), C.byref(sl), C.byref(rs),
+                                      C.byref(ps)))
+        return dict(level=lv.value, nterms=nt.value, baby=bb.value, slots=sl.value, rescale=bool(rs.value),
+                    plaintext_scale=ps.value)
+
+    def download(self):
+        """(indices, diagonals [term][QP limbs][N]) in host memory."""
+        inf = self.info()
+        idx = np.zeros(inf["nterms"], np.uint64)
+        d = np.zeros(inf["nterms"] * (inf["level"] + 1 + len(self.ctx.p)) * self.ctx.N, np.uint64)
+        _check(lib().wg_lt_stage_download(self.ctx.h, self.h, idx.ctypes.data, d.ctypes.data))
+        return idx, d
+
     @classmethod
     def from_handle(cls, ctx, h, level=None, rescale=None):
         """Wrap a stage handle the library created (wg_bundle_load)."""
@@ -282,6 +325,57 @@ class LtStage:
             self.close()
         except Exception:
             pass
+
+
+class DftLiteral(C.Structure):
+    """wg_dft_literal: one homomorphic DFT to factorize into BSGS stages."""
+    _fields_ = [("coeffs_to_slots", C.c_int), ("level", C.c_size_t), ("baby_step_count", C.c_size_t),
+                ("log_bsgs_ratio", C.c_int), ("stage_count", C.c_size_t), ("group_sizes", C.c_void_p),
+                ("group_bits", C.c_void_p), ("ngroups", C.c_size_t), ("merge_depths", C.c_void_p),
+                ("nmerge", C.c_size_t), ("active_slots", C.c_size_t), ("transform_scale", C.c_double),
+                ("input_selector_start", C.c_size_t), ("input_selector_size", C.c_size_t)]
+
+    @classmethod
+    def make(cls, coeffs_to_slots, level, transform_scale, scale_groups=(), stage_count=0, merge_depths=(),
+             active_slots=0, baby_step_count=0, log_bsgs_ratio=1, input_selector=(0, 0)):
+        lit = cls()
+        lit._keep = [np.ascontiguousarray([len(g) for g in scale_groups], dtype=np.uintp),
+                     np.ascontiguousarray([b for g in scale_groups for b in g], dtype=np.uintp),
+                     np.ascontiguousarray(list(merge_depths), dtype=np.uintp)]
+        lit.coeffs_to_slots = int(bool(coeffs_to_slots))
+        lit.level = int(level)
+        lit.baby_step_count = int(baby_step_count)
+        lit.log_bsgs_ratio = int(log_bsgs_ratio)
+        lit.stage_count = int(stage_count)
+        lit.group_sizes = lit._keep[0].ctypes.data if len(scale_groups) else None
+        lit.group_bits = lit._keep[1].ctypes.data if len(scale_groups) else None
+        lit.ngroups = len(scale_groups)
+        lit.merge_depths = lit._keep[2].ctypes.data if len(merge_depths) else None
+        lit.nmerge = len(merge_depths)
+        lit.active_slots = int(active_slots)
+        lit.transform_scale = float(transform_scale)
+        lit.input_selector_start, lit.input_selector_size = (int(input_selector[0]), int(input_selector[1]))
+        return lit
+
+
+def dft_plan_describe(N, q, literal, stage, diagonals=False):
+    """One stage of the factorized DFT generated on the host (no device): its shape, indices
+    and optionally its diagonals before encoding (complex [nterms][active slots])."""
+    qa = _u64(q)
+    ns, lv, nt, bb = C.c_size_t(), C.c_size_t(), C.c_size_t(), C.c_size_t()
+    rs, ps = C.c_int(), C.c_double()
+    _check(lib().wg_dft_plan_describe(int(N), qa.ctypes.data, len(qa), C.byref(literal), int(stage), C.byref(ns),
+                                      C.byref(lv), C.byref(nt), C.byref(bb), C.byref(rs), C.byref(ps), None, None))
+    idx = np.zeros(nt.value, np.uint64)
+    slots = literal.active_slots or int(N) // 2
+    d = np.zeros(2 * nt.value * slots, np.float64) if diagonals else None
+    _check(lib().wg_dft_plan_describe(int(N), qa.ctypes.data, len(qa), C.byref(literal), int(stage), None, None,
+                                      None, None, None, None, idx.ctypes.data, None if d is None else d.ctypes.data))
+    out = dict(stages=ns.value, level=lv.value, nterms=nt.value, baby=bb.value, rescale=bool(rs.value),
+               plaintext_scale=ps.value, indices=idx)
+    if d is not None:
+        out["diagonals"] = (d[0::2] + 1j * d[1::2]).reshape(nt.value, slots)
+    return out
 
 
 class BootstrapParams(C.Structure):
@@ -486,6 +580,36 @@ class Context:
 
     def ntt_inverse(self, poly, limbs, first=0, basis=0, polys=1, stride=0, stream=None):
         _check(lib().wg_ntt_inverse(self.h, _ptr(poly), limbs, first, basis, polys, stride, _stream(stream)))
+
+    def dft_plan(self, literal, stream=None):
+        """Generate the factorized DFT's stages on this context's device: a list of LtStage."""
+        hs = (C.c_void_p * 64)()
+        n = C.c_size_t()
+        _check(lib().wg_dft_plan_create(self.h, C.byref(literal), hs, 64, C.byref(n), _stream(stream)))
+        out = []
+        for i in range(n.value):
+            st = LtStage.from_handle(self, C.c_void_p(hs[i]))
+            inf = st.info()
+            st.level, st.rescale = inf["level"], inf["rescale"]
+            out.append(st)
+        return out
+
+    NTT_GEOMETRIES = ("8 residues/thread, staged twiddles", "8 residues/thread, table twiddles",
+                      "16 residues/thread, staged twiddles", "16 residues/thread, table twiddles")
+
+    def ntt_tuning(self):
+        """The NTT autotuner's result: {"chosen": [[fwd rows, fwd cols], [inv rows, inv cols]],
+        "ms": array [direction][phase][geometry], "limbs": limbs of the timed batch}."""
+        chosen = np.zeros(4, np.int32)
+        ms = np.zeros(16, np.float32)
+        limbs = C.c_int()
+        _check(lib().wg_ntt_tuning(self.h, chosen.ctypes.data, ms.ctypes.data, C.byref(limbs)))
+        return {"chosen": chosen.reshape(2, 2).tolist(), "ms": ms.reshape(2, 2, 4), "limbs": limbs.value}
+
+    def set_ntt_geometry(self, direction, phase, geometry):
+        """Pin the NTT geometry of (direction 0 fwd / 1 inv, phase 0 rows / 1 cols); -1 restores
+        the tuned choice."""
+        _check(lib().wg_ntt_set_geometry(self.h, int(direction), int(phase), int(geometry)))
 
     def keyswitch(self, level, key_term, kind, b, a, b_add=True, a_add=False, rotation=0, stream=None):
         _check(lib().wg_keyswitch(self.h, level, _ptr(key_term), kind, int(rotation), _ptr(b), _ptr(a),

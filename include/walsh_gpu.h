@@ -118,6 +118,35 @@ int wg_ntt_forward(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, 
 int wg_ntt_inverse(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, int basis,
                    size_t polys, size_t poly_stride, void* stream);
 
+/* EvalMod polynomial fit on the host (no device needed): the Chebyshev series of
+ * 1/2 - 1/2 cos(2 pi K u / 2^double_angle) over the 2K - 1 intervals of radius
+ * interval_radius / K around the multiples of 1/(2K), in 256-bit arithmetic, odd coefficients
+ * zeroed and those below prune_threshold dropped.  Replaces
+ * binboot_han_ki_discrete_multi_interval_approximate (src/math/poly_approx.cpp:565-681), with
+ * the same coefficients bit for bit.  coeffs: room for degree + 1 doubles (*ncoeffs receives
+ * the count); max_error and interval (2 doubles: min, max) may be null. */
+int wg_evalmod_fit(double K, size_t degree, size_t double_angle, double interval_radius,
+                   size_t validation_points, double prune_threshold, double* coeffs, size_t* ncoeffs,
+                   double* max_error, double* interval);
+/* EvalMod K of a sparse secret of `hamming_weight` over `coefficients` coefficients at failure
+ * probability 2^log2_failure (an integer exponent is exact): replaces required_binboot_k_bound
+ * (src/math/binboot_k_bound.cpp:53-89), returning its evalmod_k. */
+int wg_evalmod_k_bound(size_t coefficients, size_t hamming_weight, double log2_failure, size_t* k);
+
+/* NTT geometry autotuner (no counterpart in the reference, whose transform has one loop
+ * order, ntt.cpp:235-386).  Four geometries compute the same words: 0 = 8 residues per thread
+ * with twiddles staged in shared memory, 1 = 8 residues, twiddles read from the table,
+ * 2 = 16 residues, staged, 3 = 16 residues, from the table.  wg_ctx_create times each one per
+ * direction and phase on the device (once per device and ring degree in the process) and
+ * keeps the fastest.  wg_ntt_tuning reports chosen[direction][phase] (direction 0 forward,
+ * 1 inverse; phase 0 rows = low index bits, 1 columns = high bits; 4 ints), the timings
+ * ms[direction][phase][geometry] (16 floats, best of three launches over a batch of `limbs`
+ * limb-transforms) and that batch size.  Either output pointer may be null. */
+int wg_ntt_tuning(const wg_context* ctx, int* chosen, float* ms, int* limbs);
+/* Pin the geometry of one (direction, phase) for this context (geometry < 0: restore the
+ * tuned choice). */
+int wg_ntt_set_geometry(wg_context* ctx, int direction, int phase, int geometry);
+
 /* Hybrid key switch of key_term at `level` with the installed key (kind, rotation):
  * b = (b_add ? b + ks_b : ks_b), a = (a_add ? a + ks_a : ks_a).  key_term may alias a.
  * Replaces ckks_hybrid_key_switch_inplace (Montgomery, folded keys),
@@ -240,6 +269,46 @@ int wg_lt_stage_create(wg_context* ctx, size_t level, size_t nterms, const uint6
                        const uint64_t* diagonals, size_t baby_step_count, size_t slot_count,
                        int rescale_after, wg_lt_stage** out);
 void wg_lt_stage_destroy(wg_lt_stage* stage);
+/* Shape of a stage: level, term count, baby-step count, logical slots, rescale flag and the
+ * plaintext scale of its diagonals (0 when the stage was made from caller-supplied words). */
+int wg_lt_stage_info(const wg_lt_stage* stage, size_t* level, size_t* nterms, size_t* baby, size_t* slots,
+                     int* rescale_after, double* plaintext_scale);
+/* Copy a stage's diagonal indices (nterms) and QP diagonals ([term][level + 1 + P limbs][N],
+ * Montgomery form) to host memory. */
+int wg_lt_stage_download(wg_context* ctx, const wg_lt_stage* stage, uint64_t* indices, uint64_t* diagonals);
+
+/* One homomorphic DFT to factorize into BSGS stages (the reference's
+ * CKKSBootstrapDftMatrixLiteral, src/ckks/operations/bootstrap/ckks_bootstrap_dft.hpp). */
+typedef struct wg_dft_literal {
+    int coeffs_to_slots;        /* 1: CoeffsToSlots, 0: SlotsToCoeffs */
+    size_t level;               /* level of the first stage */
+    size_t baby_step_count;     /* 0: the cheapest split per stage */
+    int log_bsgs_ratio;         /* giant steps weigh 2^log_bsgs_ratio baby steps */
+    size_t stage_count;         /* factors when ngroups == 0 (then each stage rescales) */
+    const size_t* group_sizes;  /* ngroups entries: factors per rescale group */
+    const size_t* group_bits;   /* one log2 plaintext scale per factor, group after group */
+    size_t ngroups;
+    const size_t* merge_depths; /* FFT levels per factor (nmerge == 0: balanced) */
+    size_t nmerge;
+    size_t active_slots;        /* 0: N/2 */
+    double transform_scale;
+    size_t input_selector_start, input_selector_size; /* SlotsToCoeffs only; size 0: none */
+} wg_dft_literal;
+/* Generate the factorized DFT's stages on the context's device: diagonals on the host, encoded
+ * on the device as QP plaintexts in Montgomery form.  Replaces ckks_generate_bootstrap_dft_plan
+ * (src/ckks/operations/bootstrap/ckks_bootstrap_dft.cpp:961-1079), with the reference's
+ * diagonal residues; the stages are ordinary wg_lt_stage handles (wg_lt_stage_destroy each).
+ * *nstages receives the stage count (at most max_stages are written). */
+int wg_dft_plan_create(wg_context* ctx, const wg_dft_literal* literal, wg_lt_stage** stages, size_t max_stages,
+                       size_t* nstages, void* stream);
+/* The same plan on the host only (no device): for stage `stage` of the plan of a ring of degree
+ * N with Q moduli q[nq], its level, term count, baby steps, rescale flag, plaintext scale,
+ * diagonal indices (nterms) and, when diagonals is not null, the diagonals before encoding
+ * ([term][active slots] complex values as re, im pairs).  *nstages receives the stage count.
+ * Pass null indices to query the sizes first. */
+int wg_dft_plan_describe(uint64_t N, const uint64_t* q, size_t nq, const wg_dft_literal* literal, size_t stage,
+                         size_t* nstages, size_t* level, size_t* nterms, size_t* baby, int* rescale_after,
+                         double* plaintext_scale, uint64_t* indices, double* diagonals);
 int wg_lt_stage_apply(wg_context* ctx, const wg_lt_stage* stage, size_t count, uint64_t* const* b,
                       uint64_t* const* a, void* stream);
 

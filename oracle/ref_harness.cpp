@@ -49,6 +49,8 @@
 #include "ckks_encoding.hpp"
 #include "ckks_bootstrap_evalmod_inplace.hpp"
 #include "ckks_evalmod_scale_plan.hpp"
+#include "binboot_k_bound.hpp"
+#include "poly_approx.hpp"
 #include "ckks_context.hpp"
 #include "ckks_conjugate.hpp"
 #include "ckks_keyswitch.hpp"
@@ -577,6 +579,27 @@ int ref_batched_ops(void* h, size_t count, const size_t* levels, uint64_t* x_b, 
 }
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
+
+// binboot_han_ki_discrete_multi_interval_approximate (src/math/poly_approx.cpp:565) called
+// directly: coefficients, their count, max_error and the interval it reports.
+int ref_evalmod_fit(double K, size_t degree, size_t double_angle, double radius, size_t points, double prune,
+                    double* coeffs, size_t* n, double* max_error, double* interval) {
+    return guarded([&] {
+        const PolynomialApproximation a =
+            binboot_han_ki_discrete_multi_interval_approximate(K, degree, double_angle, radius, points, prune);
+        std::copy(a.chebyshev_coeffs.begin(), a.chebyshev_coeffs.end(), coeffs);
+        *n = a.chebyshev_coeffs.size();
+        *max_error = a.max_error;
+        interval[0] = a.interval_min;
+        interval[1] = a.interval_max;
+    });
+}
+
+// required_binboot_k_bound (src/math/binboot_k_bound.cpp:53) at failure probability
+// 2^log2_failure: its evalmod_k.
+int ref_evalmod_k_bound(size_t coefficients, size_t h, double log2_failure, size_t* k) {
+    return guarded([&] { *k = required_binboot_k_bound(coefficients, h, std::exp2((long double)log2_failure)).evalmod_k; });
+}
 
 // The AESWalsh15 modulus chain and bootstrapping DFT parameters with CoeffToSlot / SlotToCoeff
 // plaintext plans but no bootstrapping keys (the EvalMod fit needs MPFR): the context builds

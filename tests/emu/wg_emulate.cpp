@@ -38,58 +38,72 @@ struct Emu {
     std::vector<std::vector<HostModUp>> modup;
 };
 
-template <int LOGN, bool FWD, bool COLS, bool LAZY, int... RD>
-void rounds(std::integer_sequence<int, RD...>, uint64_t* sm, uint64_t q, const uint64_t* tw, const uint64_t* tws) {
-    using P = ntt::Phase<LOGN, FWD, COLS>;
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, bool LAZY, int... RD>
+void rounds(std::integer_sequence<int, RD...>, uint64_t* sm, int tile, uint64_t q, const ntt::TwPair* tw) {
+    using P = ntt::Phase<LOGN, FWD, COLS, EB, STAGED>;
     auto one = [&](auto rd_const) {
         constexpr int R = decltype(rd_const)::value;
         for (int t = 0; t < P::THREADS; ++t) {
             const int sub = COLS ? t % P::SUBS : t >> P::OB;
             const int o = COLS ? t / P::SUBS : t & ((1 << P::OB) - 1);
-            ntt::ntt_round<LOGN, FWD, COLS, R, LAZY>(sm, sub, o, q, tw, tws);
+            ntt::ntt_round<LOGN, FWD, COLS, EB, STAGED, R, LAZY>(sm, sub, o, tile, q, tw);
         }
     };
     (one(std::integral_constant<int, RD>{}), ...);
 }
 
-template <int LOGN, bool FWD, bool COLS>
+// NTT geometry the emulated phases use (the device's kNttGeometries order: 0 = 8 residues per
+// thread, staged twiddles; 1 = 8, table; 2 = 16, staged; 3 = 16, table).
+int g_geometry = 0;
+
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED>
 void phase(const Emu& E, uint64_t* x, int mi) {
-    using P = ntt::Phase<LOGN, FWD, COLS>;
+    using P = ntt::Phase<LOGN, FWD, COLS, EB, STAGED>;
     const size_t N = P::N;
-    const uint64_t* tw = E.H.tw.data() + (size_t)mi * 4 * N + (FWD ? 0 : 2 * N);
-    const uint64_t* tws = tw + N;
+    std::vector<ntt::TwPair> table(2 * N);
+    ntt::interleave_twiddles(N, E.H.tw.data() + (size_t)mi * 4 * N, table.data());
+    const ntt::TwPair* tw = table.data() + (FWD ? 0 : N);
     const Modulus& md = E.H.mods[mi];
-    std::vector<uint64_t> sm(P::TILE + P::TILE / 16), tw_s(P::TW), tws_s(P::TW);
+    std::vector<uint64_t> sm(P::TILE + P::TILE / 16);
+    std::vector<ntt::TwPair> tw_s(P::TW);
     for (int tile = 0; tile < (int)(N / P::TILE); ++tile) {
-        for (int e = 0; e < P::TILE; ++e) sm[ntt::pad16(e)] = x[ntt::tile_offset<LOGN, FWD, COLS>(tile, e)];
-        for (int e = 0; e < P::TW; ++e) {
-            const size_t src = ntt::twiddle_src<LOGN, FWD, COLS>(tile, e);
-            tw_s[e] = tw[src];
-            tws_s[e] = tws[src];
-        }
+        for (int e = 0; e < P::TILE; ++e) sm[ntt::pad16(e)] = x[ntt::tile_offset<LOGN, FWD, COLS, EB, STAGED>(tile, e)];
+        if (STAGED)
+            for (int e = 0; e < P::TW; ++e) tw_s[e] = tw[ntt::twiddle_src<LOGN, FWD, COLS, EB, STAGED>(tile, e)];
+        const ntt::TwPair* twr = STAGED ? tw_s.data() : tw;
         const bool lazy = FWD && md.q < ntt::kLazyForwardLimit;
         if (lazy)
-            rounds<LOGN, FWD, COLS, true>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), md.q, tw_s.data(),
-                                          tws_s.data());
+            rounds<LOGN, FWD, COLS, EB, STAGED, true>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), tile, md.q,
+                                                      twr);
         else
-            rounds<LOGN, FWD, COLS, false>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), md.q, tw_s.data(),
-                                           tws_s.data());
+            rounds<LOGN, FWD, COLS, EB, STAGED, false>(std::make_integer_sequence<int, P::ROUNDS>{}, sm.data(), tile,
+                                                       md.q, twr);
         for (int e = 0; e < P::TILE; ++e) {
             uint64_t v = sm[ntt::pad16(e)];
             if (P::LAST) v = FWD ? (lazy ? reduce64(v, md) : red4q(v, md.q)) : mul_shoup(v, md.n_inv, md.n_inv_shoup, md.q);
-            x[ntt::tile_offset<LOGN, FWD, COLS>(tile, e)] = v;
+            x[ntt::tile_offset<LOGN, FWD, COLS, EB, STAGED>(tile, e)] = v;
         }
+    }
+}
+
+template <int LOGN, bool FWD, bool COLS>
+void phase_geom(const Emu& E, uint64_t* x, int mi) {
+    switch (g_geometry) {
+        case 0: phase<LOGN, FWD, COLS, 3, true>(E, x, mi); break;
+        case 1: phase<LOGN, FWD, COLS, 3, false>(E, x, mi); break;
+        case 2: phase<LOGN, FWD, COLS, 4, true>(E, x, mi); break;
+        default: phase<LOGN, FWD, COLS, 4, false>(E, x, mi); break;
     }
 }
 
 template <int LOGN>
 void ntt_limb(const Emu& E, uint64_t* x, int mi, bool fwd) {
     if (fwd) {
-        phase<LOGN, true, true>(E, x, mi);
-        phase<LOGN, true, false>(E, x, mi);
+        phase_geom<LOGN, true, true>(E, x, mi);
+        phase_geom<LOGN, true, false>(E, x, mi);
     } else {
-        phase<LOGN, false, false>(E, x, mi);
-        phase<LOGN, false, true>(E, x, mi);
+        phase_geom<LOGN, false, false>(E, x, mi);
+        phase_geom<LOGN, false, true>(E, x, mi);
     }
 }
 
@@ -137,6 +151,8 @@ void* emu_create(uint64_t N, const uint64_t* q, size_t nq, const uint64_t* p, si
 }
 
 void emu_destroy(void* h) { delete static_cast<Emu*>(h); }
+
+void emu_set_ntt_geometry(int geometry) { g_geometry = geometry; }
 
 // limbs consecutive limbs using modulus index first.. (basis 0 = Q, 1 = P)
 void emu_ntt(void* h, uint64_t* poly, size_t limbs, size_t first, int basis, int inverse) {

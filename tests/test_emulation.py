@@ -30,6 +30,7 @@ def emu(tmp_path_factory):
     E.emu_create.argtypes = [C.c_uint64, u64p, C.c_size_t, u64p, C.c_size_t, C.c_size_t]
     E.emu_destroy.argtypes = [C.c_void_p]
     E.emu_ntt.argtypes = [C.c_void_p, u64p, C.c_size_t, C.c_size_t, C.c_int, C.c_int]
+    E.emu_set_ntt_geometry.argtypes = [C.c_int]
     E.emu_keyswitch.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, C.c_size_t, u64p, u64p, C.c_int, C.c_int,
                                 C.c_uint64]
     return E
@@ -74,14 +75,18 @@ def test_emulated_kernels_match_oracle(oracle_mod, emu, prm):
         emu.emu_destroy(h)
 
 
-@pytest.mark.parametrize("logN", [13, 14, 15, 16])
-def test_emulated_ntt_large_rings(oracle_mod, emu, logN):
-    """Round plans of the larger rings (column / row phases of 6..8 bits)."""
+@pytest.mark.parametrize("logN", [10, 11, 12, 13, 14, 15, 16])
+@pytest.mark.parametrize("geometry", [0, 1, 2, 3])
+def test_emulated_ntt_geometries(oracle_mod, emu, logN, geometry):
+    """Every NTT geometry the autotuner chooses from (8 or 16 residues per thread, twiddles
+    staged or read from the table) on every supported ring degree (column / row phases of 5..8
+    bits), against the oracle: lazy (36-bit) and fully reduced (61-bit) moduli."""
     O = oracle_mod
     N = 1 << logN
     p, q = O.find_primes([61], [36, 61], N)
     o = O.OracleCtx(N, q, p, 1)
     h = emu.emu_create(N, q, len(q), p, len(p), 1)
+    emu.emu_set_ntt_geometry(geometry)
     try:
         x = o.uniform(len(q), 17)
         y = x.copy()
@@ -90,6 +95,7 @@ def test_emulated_ntt_large_rings(oracle_mod, emu, logN):
         emu.emu_ntt(h, y, len(q), 0, 0, 1)
         assert (y == x).all()
     finally:
+        emu.emu_set_ntt_geometry(0)
         emu.emu_destroy(h)
 
 
