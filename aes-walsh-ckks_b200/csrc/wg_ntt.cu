@@ -257,10 +257,12 @@ void ntt_phase_geometry(const Context& c, bool forward, bool cols, int variant, 
     check_cuda(cudaGetLastError(), "ntt launch");
 }
 
-// Time every geometry of every (direction, phase) on a scratch batch larger than the L2 cache
-// (160 MB of limbs, as the batched circuits stream them) cycling over the context's moduli (so
-// lazy and full-reduction moduli are both represented), best of three launches after one
-// warm-up, and keep the fastest.  Phases are timed on their own: each is one full pass over the
+// Time every geometry of every (direction, phase) the way the batched circuits launch the
+// transform: one job-table launch over a scratch batch larger than the L2 cache (160 MB of
+// limbs) cycling over the context's moduli, so lazy and full-reduction moduli are both
+// represented; best of three launches after one warm-up.  A geometry replaces the default
+// (8 residues per thread, staged twiddles) only when it is at least 2 % faster, so timing noise
+// does not flip the choice.  Phases are timed on their own: each is one full pass over the
 // batch whatever the other phase does, and every geometry computes the same words, so the
 // choices combine freely.
 void ntt_autotune(Context& c) {
@@ -279,33 +281,41 @@ void ntt_autotune(Context& c) {
     const int nm = (int)(c.nq + c.np);
     check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
     uint64_t* buf = nullptr;
-    if (cudaMalloc(&buf, (size_t)kTuneLimbs * N * 8) != cudaSuccess) {
+    NttJob* d_jobs = nullptr;
+    if (cudaMalloc(&buf, (size_t)kTuneLimbs * N * 8) != cudaSuccess ||
+        cudaMalloc(&d_jobs, (size_t)kTuneLimbs * sizeof(NttJob)) != cudaSuccess) {
         // no room for the timing batch: keep the default geometry (tuning.limbs = 0 says so)
         cudaGetLastError();
+        cudaFree(buf);
         return;
     }
     cudaStream_t s = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     NttTuning tn{};
+    auto release = [&] {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (s) cudaStreamDestroy(s);
+        cudaFree(buf);
+        cudaFree(d_jobs);
+    };
     try {
         check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "ntt autotune: stream");
         check_cuda(cudaEventCreate(&e0), "ntt autotune: event");
         check_cuda(cudaEventCreate(&e1), "ntt autotune: event");
         check_cuda(cudaMemsetAsync(buf, 0, (size_t)kTuneLimbs * N * 8, s), "ntt autotune: clear");
-        // limb l uses modulus l mod nm: LimbMap{nA = kTuneLimbs, firstA = 0} would run past the
-        // moduli, so launch the batch as polynomials of nm limbs (the last one partial)
-        const int polys = kTuneLimbs / nm > 0 ? kTuneLimbs / nm : 1;
-        const int limbs = kTuneLimbs / nm > 0 ? nm : kTuneLimbs;
-        const LimbMap map{limbs, 0, 0};
+        std::vector<NttJob> jobs(kTuneLimbs);
+        for (int l = 0; l < kTuneLimbs; ++l) jobs[l] = {buf + (size_t)l * N, buf + (size_t)l * N, l % nm, 0};
+        check_cuda(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(NttJob), cudaMemcpyHostToDevice, s),
+                   "ntt autotune: jobs");
         for (int d = 0; d < 2; ++d)
             for (int p = 0; p < 2; ++p) {
-                float best = 1e30f;
-                int best_v = 0;
                 for (int v = 0; v < kNttGeometries; ++v) {
                     float t_best = 1e30f;
                     for (int rep = 0; rep < 4; ++rep) {
                         check_cuda(cudaEventRecord(e0, s), "ntt autotune: record");
-                        phase_dispatch(c, d == 0, p == 1, v, buf, limbs, polys, (size_t)limbs * N, map, nullptr, 0, s);
+                        phase_dispatch(c, d == 0, p == 1, v, nullptr, 0, 0, 0, LimbMap{0, 0, 0}, d_jobs, kTuneLimbs,
+                                       s);
                         check_cuda(cudaEventRecord(e1, s), "ntt autotune: record");
                         check_cuda(cudaEventSynchronize(e1), "ntt autotune: wait");
                         float ms = 0;
@@ -313,25 +323,18 @@ void ntt_autotune(Context& c) {
                         if (rep > 0) t_best = std::min(t_best, ms);
                     }
                     tn.ms[d][p][v] = t_best;
-                    if (t_best < best) {
-                        best = t_best;
-                        best_v = v;
-                    }
                 }
+                int best_v = 0;
+                for (int v = 1; v < kNttGeometries; ++v)
+                    if (tn.ms[d][p][v] < 0.98f * tn.ms[d][p][0] && tn.ms[d][p][v] < tn.ms[d][p][best_v]) best_v = v;
                 tn.chosen[d][p] = best_v;
             }
-        tn.limbs = limbs * polys;
+        tn.limbs = kTuneLimbs;
     } catch (...) {
-        if (e0) cudaEventDestroy(e0);
-        if (e1) cudaEventDestroy(e1);
-        if (s) cudaStreamDestroy(s);
-        cudaFree(buf);
+        release();
         throw;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaStreamDestroy(s);
-    cudaFree(buf);
+    release();
     c.tuning = tn;
     for (int d = 0; d < 2; ++d)
         for (int p = 0; p < 2; ++p) c.ntt_variant[d][p] = tn.chosen[d][p];

@@ -580,6 +580,31 @@ int ref_batched_ops(void* h, size_t count, const size_t* levels, uint64_t* x_b, 
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
+// The reference's own CKKSParams presets (src/ckks/parameters/ckks_aes_params.hpp:211-235):
+// 0 AESWalsh15, 1 XBootParamAes13Reference, 2 AESXBoot14Secure, 3 AESXBoot14SecureSparse1024,
+// 4 AESXBoot15, 5 AESXBoot15Sparse1024.  Moduli (q: room for 64, p: room for 16), scale,
+// depth, active slots, EvalMod K, S2C and C2S depths.
+int ref_preset(int which, uint64_t* q, size_t* nq, uint64_t* p, size_t* np, double* scale, size_t* info) {
+    return guarded([&] {
+        const CKKSParams prm = which == 0   ? CKKSParams::AESWalsh15()
+                               : which == 1 ? CKKSParams::XBootParamAes13Reference()
+                               : which == 2 ? CKKSParams::AESXBoot14Secure()
+                               : which == 3 ? CKKSParams::AESXBoot14SecureSparse1024()
+                               : which == 4 ? CKKSParams::AESXBoot15()
+                                            : CKKSParams::AESXBoot15Sparse1024();
+        *nq = prm.getModuli().size();
+        *np = prm.getPModuli().size();
+        std::copy(prm.getModuli().begin(), prm.getModuli().end(), q);
+        std::copy(prm.getPModuli().begin(), prm.getPModuli().end(), p);
+        *scale = prm.getScale();
+        info[0] = prm.getDepth();
+        info[1] = prm.getBootstrapActiveSlotCount();
+        info[2] = prm.getBootstrapEvalModK();
+        info[3] = prm.getBootstrapS2CDepth();
+        info[4] = prm.getBootstrapC2SDepth();
+    });
+}
+
 // binboot_han_ki_discrete_multi_interval_approximate (src/math/poly_approx.cpp:565) called
 // directly: coefficients, their count, max_error and the interval it reports.
 int ref_evalmod_fit(double K, size_t degree, size_t double_angle, double radius, size_t points, double prune,
