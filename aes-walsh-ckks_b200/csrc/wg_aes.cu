@@ -176,8 +176,26 @@ public:
             }
         size_t lv[8];
         double sc[8];
-        walsh_sbox(c_, p_, plans_, nplans_, c2s_, nc2s_, coeffs_, ncoeffs_, pack_count, 16, level,
-                   static_cast<double>(st[0].scale), ib.data(), ia.data(), ob.data(), oa.data(), lv, sc, s_);
+        if (!per_instance_) {
+            walsh_sbox(c_, p_, plans_, nplans_, c2s_, nc2s_, coeffs_, ncoeffs_, pack_count, 16, level,
+                       static_cast<double>(st[0].scale), ib.data(), ia.data(), ob.data(), oa.data(), lv, sc, s_);
+        } else {
+            // one S-box instance per call: its 8 bit pointers, bit-major with count 1
+            for (size_t byte = 0; byte < 16; ++byte) {
+                uint64_t* i1b[8];
+                uint64_t* i1a[8];
+                uint64_t* o1b[8];
+                uint64_t* o1a[8];
+                for (size_t k = 0; k < 8; ++k) {
+                    i1b[k] = ib[k * 16 + byte];
+                    i1a[k] = ia[k * 16 + byte];
+                    o1b[k] = ob[k * 16 + byte];
+                    o1a[k] = oa[k * 16 + byte];
+                }
+                walsh_sbox(c_, p_, plans_, nplans_, c2s_, nc2s_, coeffs_, ncoeffs_, pack_count, 1, level,
+                           static_cast<double>(st[0].scale), i1b, i1a, o1b, o1a, lv, sc, s_);
+            }
+        }
         Bits out(kBlockBits);
         for (size_t byte = 0; byte < 16; ++byte)
             for (size_t k = 0; k < 8; ++k) {
@@ -497,9 +515,16 @@ public:
         }
         size_t blv = 0;
         double bsc = 0.0;
-        bootstrap_evalmod(c_, p_, plans_, nplans_, c2s_, nc2s_, coeffs_, ncoeffs_, batches,
-                          static_cast<double>(packed.scale), pb.data(), pa.data(), o0b.data(), o0a.data(), o1b.data(),
-                          o1a.data(), &blv, &bsc, s_);
+        if (!per_instance_) {
+            bootstrap_evalmod(c_, p_, plans_, nplans_, c2s_, nc2s_, coeffs_, ncoeffs_, batches,
+                              static_cast<double>(packed.scale), pb.data(), pa.data(), o0b.data(), o0a.data(),
+                              o1b.data(), o1a.data(), &blv, &bsc, s_);
+        } else {
+            for (size_t b = 0; b < batches; ++b)
+                bootstrap_evalmod(c_, p_, plans_, nplans_, c2s_, nc2s_, coeffs_, ncoeffs_, 1,
+                                  static_cast<double>(packed.scale), &pb[b], &pa[b], &o0b[b], &o0a[b], &o1b[b],
+                                  &o1a[b], &blv, &bsc, s_);
+        }
         CtBatch real = bops.wrap(o0b.data(), o0a.data(), blv, bsc);
         CtBatch imag = bops.wrap(o1b.data(), o1a.data(), blv, bsc);
         real.cap = imag.cap = full;
@@ -525,7 +550,10 @@ public:
         refresh_mask(st, stride, 0);
     }
 
+    void set_per_instance(bool v) { per_instance_ = v; }
+
 private:
+    bool per_instance_ = false;
     Context& c_;
     DeviceOps& ops_;
     const BootstrapParams& p_;
@@ -555,6 +583,7 @@ void aes_ctr_walsh(Context& c, const BootstrapParams& p, const S2cPlan* s2c, siz
         throw std::invalid_argument("ckks_aes_walsh: null argument");
     DeviceOps ops(c, 1, s);
     Aes aes(c, ops, p, s2c, nplans, c2s, nc2s, coeffs, ncoeffs, s);
+    aes.set_per_instance(a.per_instance);
     Bits st = aes.initial_state_fast(a);
     for (size_t round = 1; round <= kRounds; ++round) {
         aes.mask_inactive(st, pack);

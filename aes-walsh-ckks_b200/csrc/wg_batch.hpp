@@ -231,6 +231,9 @@ struct AesArgs {
     const uint8_t* ciphertexts = nullptr;
     size_t active_blocks = 0;
     size_t packing_block_count = 0, packed_segment_count = 0;
+    // the reference's call granularity: each S-box instance and each refresh bootstrap as its
+    // own call (the plain per-operation path; same words as the batched one)
+    bool per_instance = false;
 };
 void aes_ctr_walsh(Context& c, const BootstrapParams& p, const S2cPlan* s2c, size_t nplans, const LtStage* const* c2s,
                    size_t nc2s, const double* coeffs, size_t ncoeffs, const AesArgs& args, uint64_t* const* out_b,

@@ -12,6 +12,7 @@
 #include "wg_encode.hpp"
 #include "wg_evalmod_fit.hpp"
 #include "wg_dftplan.hpp"
+#include "wg_ctwire.hpp"
 #include "wg_internal.hpp"
 #include "wg_serve.hpp"
 
@@ -255,6 +256,46 @@ int wg_ntt_forward(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, 
 int wg_ntt_inverse(wg_context* ctx, uint64_t* poly, size_t limbs, size_t first, int basis, size_t polys,
                    size_t poly_stride, void* stream) {
     return ntt_call(ctx, poly, limbs, first, basis, polys, poly_stride, stream, false);
+}
+
+size_t wg_ct_wire_bytes(uint64_t N, size_t level, size_t npolys) { return wg::ct_wire_bytes(N, level, npolys); }
+
+int wg_ct_wire_encode(uint64_t N, const uint64_t* q, size_t level, size_t npolys, const uint64_t* polys, double scale,
+                      int secret_owner, int encoding_state, uint8_t* out, size_t cap) {
+    return guard([&] {
+        if (!q || !polys || !out) wg::fail(wg::kInvalid, "ciphertext wire: null argument");
+        if (npolys == 0 || npolys > 3 || (secret_owner & ~1) || (encoding_state & ~1))
+            wg::fail(wg::kInvalid, "ciphertext wire: invalid polynomial count or labels");
+        wg::CtRecord r;
+        r.N = N;
+        r.level = level;
+        r.npolys = npolys;
+        r.scale = scale;
+        r.owner = (uint8_t)secret_owner;
+        r.state = (uint8_t)encoding_state;
+        r.q.assign(q, q + level + 1);
+        r.polys.assign(polys, polys + npolys * (level + 1) * N);
+        wg::ct_wire_encode(r, out, cap);
+    });
+}
+
+int wg_ct_wire_decode(const uint8_t* in, size_t len, uint64_t N, const uint64_t* q, size_t nq, uint64_t* polys,
+                      size_t cap_words, size_t* level, size_t* npolys, double* scale, int* secret_owner,
+                      int* encoding_state) {
+    return guard([&] {
+        if (!in || !q || !polys) wg::fail(wg::kInvalid, "ciphertext wire: null argument");
+        const wg::CtRecord r = wg::ct_wire_decode(in, len);
+        if (r.N != N) wg::fail(wg::kInvalid, "ciphertext wire: ring degree differs from the context's");
+        if (r.level >= nq || !std::equal(r.q.begin(), r.q.end(), q))
+            wg::fail(wg::kInvalid, "ciphertext wire: moduli differ from the context's");
+        if (r.polys.size() > cap_words) wg::fail(wg::kInvalid, "ciphertext wire: output buffer too small");
+        std::copy(r.polys.begin(), r.polys.end(), polys);
+        if (level) *level = r.level;
+        if (npolys) *npolys = r.npolys;
+        if (scale) *scale = r.scale;
+        if (secret_owner) *secret_owner = r.owner;
+        if (encoding_state) *encoding_state = r.state;
+    });
 }
 
 int wg_evalmod_fit(double K, size_t degree, size_t double_angle, double interval_radius, size_t validation_points,
@@ -589,14 +630,14 @@ int wg_walsh_sbox(wg_context* ctx, const wg_bootstrap_params* params, const wg_l
     });
 }
 
-int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
-                     size_t ns2c, const wg_lt_stage* const* s2c_x2, size_t ns2c_x2,
-                     const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
-                     size_t packing_block_count, size_t packed_segment_count, const uint64_t* const* key_b,
-                     const uint64_t* const* key_a, const double* key_scales, size_t key_level,
-                     const uint8_t* counters, const uint8_t* ciphertexts, size_t active_blocks,
-                     uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
-                     void* stream) {
+static int aes_ctr_walsh_call(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
+                              size_t ns2c, const wg_lt_stage* const* s2c_x2, size_t ns2c_x2,
+                              const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                              size_t packing_block_count, size_t packed_segment_count, const uint64_t* const* key_b,
+                              const uint64_t* const* key_a, const double* key_scales, size_t key_level,
+                              const uint8_t* counters, const uint8_t* ciphertexts, size_t active_blocks,
+                              uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                              void* stream, bool per_instance) {
     return guard([&] {
         wg::Context& c = C(ctx);
         check_ptr(out_level, "ckks_aes_walsh");
@@ -625,9 +666,36 @@ int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const w
         a.active_blocks = active_blocks;
         a.packing_block_count = packing_block_count;
         a.packed_segment_count = packed_segment_count;
+        a.per_instance = per_instance;
         wg::aes_ctr_walsh(c, bp, plans, ns2c_x2 ? 2 : 1, vc.data(), nc2s, coeffs, ncoeffs, a, out_b, out_a, out_level,
                           out_scale, S(stream));
     });
+}
+
+int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
+                     size_t ns2c, const wg_lt_stage* const* s2c_x2, size_t ns2c_x2,
+                     const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                     size_t packing_block_count, size_t packed_segment_count, const uint64_t* const* key_b,
+                     const uint64_t* const* key_a, const double* key_scales, size_t key_level,
+                     const uint8_t* counters, const uint8_t* ciphertexts, size_t active_blocks,
+                     uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                     void* stream) {
+    return aes_ctr_walsh_call(ctx, params, s2c, ns2c, s2c_x2, ns2c_x2, c2s, nc2s, coeffs, ncoeffs, packing_block_count,
+                              packed_segment_count, key_b, key_a, key_scales, key_level, counters, ciphertexts,
+                              active_blocks, out_b, out_a, out_level, out_scale, stream, false);
+}
+
+int wg_aes_ctr_walsh_plain(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
+                           size_t ns2c, const wg_lt_stage* const* s2c_x2, size_t ns2c_x2,
+                           const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                           size_t packing_block_count, size_t packed_segment_count, const uint64_t* const* key_b,
+                           const uint64_t* const* key_a, const double* key_scales, size_t key_level,
+                           const uint8_t* counters, const uint8_t* ciphertexts, size_t active_blocks,
+                           uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                           void* stream) {
+    return aes_ctr_walsh_call(ctx, params, s2c, ns2c, s2c_x2, ns2c_x2, c2s, nc2s, coeffs, ncoeffs, packing_block_count,
+                              packed_segment_count, key_b, key_a, key_scales, key_level, counters, ciphertexts,
+                              active_blocks, out_b, out_a, out_level, out_scale, stream, true);
 }
 
 int wg_xboot_sbox(wg_context* ctx, size_t count, size_t level, double scale, uint64_t* const* in_b,
@@ -920,6 +988,21 @@ struct wg_server {
     wg::Server* s;
 };
 
+struct wg_serve_budget {
+    wg::ServeBudget b;
+};
+
+int wg_serve_budget_create(size_t bytes, wg_serve_budget** out) {
+    return guard([&] {
+        if (!out) wg::fail(wg::kInvalid, "wg_serve: null output");
+        if (bytes == 0) wg::fail(wg::kInvalid, "wg_serve: budget must be positive");
+        *out = new wg_serve_budget;
+        (*out)->b.capacity = bytes;
+    });
+}
+
+void wg_serve_budget_destroy(wg_serve_budget* budget) { delete budget; }
+
 int wg_serve_create(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c, size_t ns2c,
                     const wg_lt_stage* const* s2c_x2, size_t ns2c_x2, const wg_lt_stage* const* c2s, size_t nc2s,
                     const double* coeffs, size_t ncoeffs, size_t packing_block_count, size_t packed_segment_count,
@@ -955,6 +1038,8 @@ int wg_serve_create(wg_context* ctx, const wg_bootstrap_params* params, const wg
         cfg.eval_bytes = config->eval_bytes;
         cfg.max_blocks = config->max_blocks;
         cfg.batch_window_ms = config->batch_window_ms;
+        cfg.priority = config->priority;
+        cfg.budget = config->budget ? &config->budget->b : nullptr;
         auto* h = new wg_server{nullptr};
         try {
             h->s = new wg::Server(c, std::move(su), cfg);
@@ -996,6 +1081,8 @@ int wg_serve_create_xboot(wg_context* ctx, const wg_bootstrap_params* params, co
         cfg.eval_bytes = config->eval_bytes;
         cfg.max_blocks = config->max_blocks;
         cfg.batch_window_ms = config->batch_window_ms;
+        cfg.priority = config->priority;
+        cfg.budget = config->budget ? &config->budget->b : nullptr;
         auto* h = new wg_server{nullptr};
         try {
             h->s = new wg::Server(c, std::move(su), cfg);

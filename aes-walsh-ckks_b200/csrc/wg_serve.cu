@@ -28,6 +28,23 @@ constexpr size_t kKeyBits = 11 * kStateBits;
 constexpr size_t kBlockBytes = 16;
 }  // namespace
 
+size_t ServeBudget::acquire(size_t bytes) {
+    std::unique_lock<std::mutex> lk(mu);
+    const size_t take = capacity ? std::min(bytes, capacity) : 0;
+    if (!take) return 0;
+    cv.wait(lk, [&] { return in_use + take <= capacity; });
+    in_use += take;
+    return take;
+}
+
+void ServeBudget::release(size_t bytes) {
+    {
+        std::lock_guard<std::mutex> g(mu);
+        in_use -= std::min(bytes, in_use);
+    }
+    cv.notify_all();
+}
+
 Server::Server(Context& c, ServeSetup setup, const ServeConfig& cfg) : c_(c), setup_(std::move(setup)), cfg_(cfg) {
     if (setup_.key_b.size() != kKeyBits || setup_.key_a.size() != kKeyBits || setup_.key_scales.size() != kKeyBits)
         throw std::invalid_argument("wg_serve: expected 1408 encrypted round-key bits");
@@ -47,8 +64,14 @@ Server::Server(Context& c, ServeSetup setup, const ServeConfig& cfg) : c_(c), se
     check_cuda(cudaSetDevice(c_.device), "cudaSetDevice");
     workers_.resize(cfg_.workers);
     const size_t words = kStateBits * 2 * (setup_.bp.depth + 1) * c_.N;
+    int prio = 0;
+    if (cfg_.priority) {
+        int least = 0, greatest = 0;
+        check_cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest), "wg_serve: stream priorities");
+        prio = greatest;
+    }
     for (auto& w : workers_) {
-        if (cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        if (cudaStreamCreateWithPriority(&w.stream, cudaStreamNonBlocking, prio) != cudaSuccess ||
             cudaMalloc((void**)&w.out, words * 8) != cudaSuccess) {
             cudaGetLastError();
             release_workers();
@@ -171,6 +194,8 @@ void Server::worker(size_t w) {
             queue_.swap(rest);
             ++running_;
         }
+        // a budget shared with other servers: hold this evaluation's bytes while it runs
+        const size_t held = cfg_.budget && cfg_.eval_bytes ? cfg_.budget->acquire(cfg_.eval_bytes) : 0;
         const auto started = Clock::now();
         const size_t active = setup_.xboot ? setup_.bp.active_slots : setup_.packing_block_count;
         ServeResult base;
@@ -233,6 +258,7 @@ void Server::worker(size_t w) {
             base.error = e.what();
         }
         const auto finished = Clock::now();
+        if (held) cfg_.budget->release(held);
         {
             std::lock_guard<std::mutex> g(mu_);
             size_t off = 0;

@@ -36,6 +36,18 @@ struct ServeSetup {
     std::vector<size_t> key_levels;
 };
 
+// Device bytes that the evaluations of several servers on one device share: a worker takes its
+// evaluation's bytes before it starts (waiting while the others hold them) and returns them when
+// it finishes.  An evaluation larger than the whole budget runs alone.
+struct ServeBudget {
+    std::mutex mu;
+    std::condition_variable cv;
+    size_t capacity = 0;
+    size_t in_use = 0;
+    size_t acquire(size_t bytes);  // returns the bytes taken (clamped to the capacity)
+    void release(size_t bytes);
+};
+
 struct ServeConfig {
     size_t workers = 2;        // evaluations that may run at once
     size_t hbm_budget = 0;     // device bytes the evaluations may take together (0: no limit)
@@ -44,6 +56,11 @@ struct ServeConfig {
                                // active slot count for XBOOT)
     double batch_window_ms = 0.0;  // a free worker waits this long after the oldest queued
                                    // request for more to fill its batch (0: start at once)
+    int priority = 0;              // 1: the workers' streams take the device's highest scheduling
+                                   // priority, so this server's kernels go first when servers
+                                   // share the device (short evaluations do not wait behind long
+                                   // ones); 0: default priority
+    ServeBudget* budget = nullptr; // shared with other servers (null: this server's own limit)
 };
 
 struct ServeResult {

@@ -70,6 +70,13 @@ def lib() -> C.CDLL:
         for f in (L.wg_ntt_forward, L.wg_ntt_inverse):
             f.argtypes = [vp, vp, sz, sz, C.c_int, sz, sz, vp]
         L.wg_ntt_tuning.argtypes = [vp, vp, vp, vp]
+        L.wg_ct_wire_bytes.argtypes = [u64, sz, sz]
+        L.wg_ct_wire_bytes.restype = sz
+        L.wg_ct_wire_encode.argtypes = [u64, vp, sz, sz, vp, C.c_double, C.c_int, C.c_int, vp, sz]
+        L.wg_ct_wire_decode.argtypes = [vp, sz, u64, vp, sz, vp, sz, vp, vp, vp, vp, vp]
+        L.wg_serve_budget_create.argtypes = [sz, vp]
+        L.wg_serve_budget_destroy.argtypes = [vp]
+        L.wg_serve_budget_destroy.restype = None
         L.wg_evalmod_fit.argtypes = [C.c_double, sz, sz, C.c_double, sz, C.c_double, vp, vp, vp, vp]
         L.wg_evalmod_k_bound.argtypes = [sz, sz, C.c_double, vp]
         L.wg_dft_plan_describe.argtypes = [u64, vp, sz, vp, sz] + [vp] * 8
@@ -97,8 +104,9 @@ def lib() -> C.CDLL:
         L.wg_bootstrap_evalmod.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, sz, vp, vp, vp, vp, vp, vp,
                                            C.POINTER(C.c_size_t), C.POINTER(C.c_double), vp]
         L.wg_walsh_sbox.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, sz, sz, sz, C.c_double, vp, vp, vp, vp, vp, vp, vp]
-        L.wg_aes_ctr_walsh.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, C.c_char_p,
-                                       C.c_char_p, sz, vp, vp, vp, vp, vp]
+        for f in (L.wg_aes_ctr_walsh, L.wg_aes_ctr_walsh_plain):
+            f.argtypes = [vp, vp, vp, sz, vp, sz, vp, sz, vp, sz, sz, sz, vp, vp, vp, sz, C.c_char_p, C.c_char_p, sz,
+                          vp, vp, vp, vp, vp]
         L.wg_batch_plan_create.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
         L.wg_xboot_sbox.argtypes = [vp, sz, sz, C.c_double, vp, vp, vp, vp, vp, vp, vp]
         L.wg_xboot_sbox_coefficients.argtypes = [vp]
@@ -248,6 +256,30 @@ def evalmod_k_bound(coefficients, hamming_weight, log2_failure):
     return k.value
 
 
+def ct_wire_encode(N, q, level, polys, scale, secret_owner=0, encoding_state=0) -> bytes:
+    """The wire record of a ciphertext: polys = host residues [npolys][level + 1][N]."""
+    qa = _u64(q)
+    pa = _u64(polys)
+    npolys = pa.size // ((level + 1) * int(N))
+    n = lib().wg_ct_wire_bytes(int(N), int(level), npolys)
+    out = np.zeros(n, np.uint8)
+    _check(lib().wg_ct_wire_encode(int(N), qa.ctypes.data, int(level), npolys, pa.ctypes.data, float(scale),
+                                   int(secret_owner), int(encoding_state), out.ctypes.data, n))
+    return out.tobytes()
+
+
+def ct_wire_decode(record, N, q):
+    """(residues [npolys][level + 1][N] as a flat array, level, scale, secret_owner, encoding_state)
+    of a wire record checked against the context's ring degree and Q moduli."""
+    buf = np.frombuffer(bytes(record), dtype=np.uint8).copy()
+    qa = _u64(q)
+    out = np.zeros(3 * len(qa) * int(N), np.uint64)
+    lv, npl, sc, ow, st = C.c_size_t(), C.c_size_t(), C.c_double(), C.c_int(), C.c_int()
+    _check(lib().wg_ct_wire_decode(buf.ctypes.data, buf.size, int(N), qa.ctypes.data, len(qa), out.ctypes.data,
+                                   out.size, C.byref(lv), C.byref(npl), C.byref(sc), C.byref(ow), C.byref(st)))
+    return out[: npl.value * (lv.value + 1) * int(N)], lv.value, sc.value, ow.value, st.value
+
+
 def to_device(arr, device="cuda"):
     """uint64 numpy array -> int64 torch tensor on the GPU (bit-identical)."""
     import torch
@@ -388,7 +420,23 @@ class BootstrapParams(C.Structure):
 class ServeConfig(C.Structure):
     """wg_serve_config."""
     _fields_ = [("workers", C.c_size_t), ("hbm_budget_bytes", C.c_size_t), ("eval_bytes", C.c_size_t),
-                ("max_blocks", C.c_size_t), ("batch_window_ms", C.c_double)]
+                ("max_blocks", C.c_size_t), ("batch_window_ms", C.c_double), ("priority", C.c_int),
+                ("budget", C.c_void_p)]
+
+
+class ServeBudget:
+    """A device-memory budget shared by several servers (wg_serve_budget_create); keep it alive
+    until the servers using it are closed."""
+
+    def __init__(self, nbytes):
+        h = C.c_void_p()
+        _check(lib().wg_serve_budget_create(int(nbytes), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wg_serve_budget_destroy(self.h)
+            self.h = None
 
 
 class ServeResult(C.Structure):
@@ -409,7 +457,7 @@ class Server:
 
     def __init__(self, ctx, params, s2c, s2c_x2, c2s, coeffs, packing_block_count, packed_segment_count, key_bits,
                  key_scales, key_level, workers=2, hbm_budget_bytes=0, eval_bytes=0, max_blocks=0,
-                 batch_window_ms=0.0):
+                 batch_window_ms=0.0, priority=0, budget=None):
         arr = lambda ts: np.ascontiguousarray([_ptr(t) for t in ts], dtype=np.uint64)
         hs = lambda sts: np.ascontiguousarray([st.h.value for st in sts], dtype=np.uint64)
         # kept alive with the server: the library holds their addresses
@@ -418,7 +466,8 @@ class Server:
         self._ps, self._ps2, self._pc = hs(s2c), hs(s2c_x2), hs(c2s)
         self._cf = np.ascontiguousarray(coeffs, dtype=np.float64)
         self._ks = np.ascontiguousarray(key_scales, dtype=np.float64)
-        cfg = ServeConfig(workers, hbm_budget_bytes, eval_bytes, max_blocks, batch_window_ms)
+        cfg = ServeConfig(workers, hbm_budget_bytes, eval_bytes, max_blocks, batch_window_ms, int(priority),
+                          None if budget is None else budget.h.value)
         h = C.c_void_p()
         _check(lib().wg_serve_create(ctx.h, C.byref(params), self._ps.ctypes.data, len(self._ps), self._ps2.ctypes.data,
                                      len(self._ps2), self._pc.ctypes.data, len(self._pc), self._cf.ctypes.data,
@@ -429,7 +478,7 @@ class Server:
 
     @classmethod
     def xboot(cls, ctx, params, s2c, c2s, coeffs, key_bits, key_scales, key_levels, workers=2, hbm_budget_bytes=0,
-              eval_bytes=0, max_blocks=0, batch_window_ms=0.0):
+              eval_bytes=0, max_blocks=0, batch_window_ms=0.0, priority=0, budget=None):
         """The service over XBOOT evaluations (wg_serve_create_xboot): requests of 1..active-slot
         blocks, block b of an evaluation in slot b."""
         self = cls.__new__(cls)
@@ -441,7 +490,8 @@ class Server:
         self._cf = np.ascontiguousarray(coeffs, dtype=np.float64)
         self._ks = np.ascontiguousarray(key_scales, dtype=np.float64)
         self._kl = np.ascontiguousarray(key_levels, dtype=np.uintp)
-        cfg = ServeConfig(workers, hbm_budget_bytes, eval_bytes, max_blocks, batch_window_ms)
+        cfg = ServeConfig(workers, hbm_budget_bytes, eval_bytes, max_blocks, batch_window_ms, int(priority),
+                          None if budget is None else budget.h.value)
         h = C.c_void_p()
         _check(lib().wg_serve_create_xboot(ctx.h, C.byref(params), self._ps.ctypes.data, len(self._ps),
                                            self._pc.ctypes.data, len(self._pc), self._cf.ctypes.data, len(self._cf),
@@ -859,7 +909,7 @@ class Context:
         return [int(x) for x in lv], [float(x) for x in sc]
 
     def aes_ctr_walsh(self, params, s2c, s2c_x2, c2s, coeffs, packing_block_count, packed_segment_count, key_bits,
-                      key_scales, key_level, counters, ciphertexts, active_blocks, out_bits, stream=None):
+                      key_scales, key_level, counters, ciphertexts, active_blocks, out_bits, stream=None, plain=False):
         """Homomorphic AES-128-CTR on lazy bits: key_bits = 1408 (b, a) device tensors, counters /
         ciphertexts = bytes of 2 * active_blocks blocks, out_bits = 128 (b, a) device tensors.
         Returns (levels, scales) of the 128 output bits."""
@@ -872,11 +922,11 @@ class Context:
         ks = np.ascontiguousarray(key_scales, dtype=np.float64)
         lv = np.zeros(128, np.uintp)
         sc = np.zeros(128, np.float64)
-        _check(lib().wg_aes_ctr_walsh(self.h, C.byref(params), ps.ctypes.data, len(ps), ps2.ctypes.data, len(ps2),
-                                      pc.ctypes.data, len(pc), cf.ctypes.data, len(cf), packing_block_count,
-                                      packed_segment_count, kb.ctypes.data, ka.ctypes.data, ks.ctypes.data, key_level,
-                                      bytes(counters), bytes(ciphertexts), active_blocks, ob.ctypes.data,
-                                      oa.ctypes.data, lv.ctypes.data, sc.ctypes.data, _stream(stream)))
+        fn = lib().wg_aes_ctr_walsh_plain if plain else lib().wg_aes_ctr_walsh
+        _check(fn(self.h, C.byref(params), ps.ctypes.data, len(ps), ps2.ctypes.data, len(ps2), pc.ctypes.data,
+                  len(pc), cf.ctypes.data, len(cf), packing_block_count, packed_segment_count, kb.ctypes.data,
+                  ka.ctypes.data, ks.ctypes.data, key_level, bytes(counters), bytes(ciphertexts), active_blocks,
+                  ob.ctypes.data, oa.ctypes.data, lv.ctypes.data, sc.ctypes.data, _stream(stream)))
         return [int(x) for x in lv], [float(x) for x in sc]
 
     def bootstrap_pair(self, params, s2c, c2s, coeffs, scale, pairs, stream=None):

@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the per-kernel-class event-timing passes")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-operation AES pass")
     ap.add_argument("--no-ops", action="store_true", help="skip the batched-ops section")
     ap.add_argument("--no-ntt", action="store_true", help="skip the NTT / rotation primitives section")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-requests section")
@@ -77,7 +78,7 @@ def parse():
     ap.add_argument("--xboot-aes-steps", type=int, default=2, help="timed XBOOT AES-CTR evaluations (after one warm-up)")
     ap.add_argument("--no-keygen", action="store_true", help="skip the device key generation section")
     ap.add_argument("--serve-requests", type=int, default=32)
-    ap.add_argument("--serve-mix-requests", type=int, default=16)
+    ap.add_argument("--serve-mix-requests", type=int, default=20)
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not sample nvidia-smi clocks (for runs under a profiler, which wants the GPU to itself)")
     ap.add_argument("--no-aes", action="store_true",
@@ -603,72 +604,150 @@ def ref_config1_sample(repeats=5):
 # AES-CTR on the device
 # ------------------------------------------------------------------------------------------
 class AesRun:
-    """Context, keys, bootstrap stages and encrypted key bits of the walsh15 shapes."""
+    """The walsh15 AES-CTR evaluation with real key material, all of it made by the library on
+    the device: a seeded ternary secret of Hamming weight 256 and the sparse bootstrapping secret
+    of weight 32, every switching key from them (wg_keygen_switch_key / wg_keygen_secret_switch,
+    one seed per key), the SlotToCoeff (x1, x2 input scale) and CoeffToSlot plans
+    (wg_dft_plan_create), the EvalMod series (wg_evalmod_fit) and the 1408 encrypted round-key
+    bits of a seeded AES key (wg_aes_walsh_encrypt_round_key_bits).  The chain and bootstrap
+    parameters are the walsh15 preset's (tests/golden/walsh15_plan.json).  Counter blocks and
+    CTR ciphertexts of seeded plaintexts, so every output can be decrypted and checked against
+    plain AES-128 (check())."""
 
     def __init__(self, wg, torch, plan, device, seed):
         N = plan["ring_degree"]
         q = np.array(plan["q"], dtype=np.uint64)
         p = np.array(plan["p"], dtype=np.uint64)
-        K = len(p)
         self.N, self.wg, self.torch = N, wg, torch
         self.ctx = ctx = wg.Context(N, q, p, plan["dnum"], device=device)
         rng = np.random.default_rng(seed)
 
-        def residues(limb_mods, copies):
-            col = np.tile(np.repeat(np.asarray(limb_mods, np.uint64), N), copies)
-            return (rng.integers(0, 1 << 62, col.size, dtype=np.uint64) % col).astype(np.uint64)
+        def ternary(h):
+            s = np.zeros(N, np.int8)
+            pos = rng.choice(N, h, replace=False)
+            s[pos] = rng.choice(np.array([-1, 1], np.int8), h)
+            return s
 
-        def key(spec):
-            kl = spec["key_level"]
-            flat = residues(np.concatenate([q[: kl + 1], p]), 2 * spec["parts"])
-            assert flat.size == spec["words"], (flat.size, spec)
-            return flat
-
-        keys = plan["keys"]
-        for name, kind in (("relin", wg.WG_KEY_RELIN), ("conj", wg.WG_KEY_CONJ),
-                           ("sparse_to_dense", wg.WG_KEY_SPARSE_TO_DENSE)):
-            ctx.set_key(kind, key(keys[name]), parts=keys[name]["parts"], key_level=keys[name]["key_level"])
-        ctx.set_key(wg.WG_KEY_DENSE_TO_SPARSE, residues([q[0], p[0], q[0], p[0]], 1))
-        rk = keys["rotation"]
-        for r in plan["rotations"]:
-            ctx.set_key(wg.WG_KEY_ROTATION, key(rk), rotation=int(r), parts=rk["parts"], key_level=rk["key_level"])
-
-        def stages(spec):
-            out = []
-            for st in spec:
-                level = st["qp_limbs"] - 1 - K
-                d = residues(np.concatenate([q[: level + 1], p]), len(st["indices"]))
-                out.append(wg.LtStage(ctx, level, st["indices"], d, st["baby"], st["slot_count"], st["rescale"]))
-            return out
-
-        self.s2c, self.s2c_x2, self.c2s = stages(plan["s2c"]), stages(plan["s2c_x2"]), stages(plan["c2s"])
+        self.secret, self.low_secret = ternary(256), ternary(32)
         b = plan["bootstrap"]
         self.params = wg.BootstrapParams(b["s2c_depth"], b["depth"], b["evalmod_log_scale"], b["double_angle"],
                                          b["active_slots"], b["slots"], b["scale"])
-        self.coeffs = np.asarray(plan["evalmod_coeffs"], dtype=np.float64)
+        # the walsh15 preset's DFT literals (its scale schedules, bootstrap depths and EvalMod K)
+        q0, scale = float(q[0]), b["scale"]
+        K = wg.evalmod_k_bound(N, 32, -16.0)
+        s2c = lambda ratio: wg.DftLiteral.make(False, b["s2c_depth"], (q0 * 0.5) / (scale * ratio),
+                                               scale_groups=[[18, 20, 23]], active_slots=b["active_slots"])
+        c2s = wg.DftLiteral.make(True, b["depth"], np.ldexp(scale, b["evalmod_log_scale"] - 36) / q0 / K,
+                                 scale_groups=[[25, 25], [25, 25]], active_slots=b["active_slots"])
+        self.s2c, self.s2c_x2, self.c2s = ctx.dft_plan(s2c(1)), ctx.dft_plan(s2c(2)), ctx.dft_plan(c2s)
+        self.coeffs = wg.evalmod_fit(K, 100, 0, np.nextafter(0.25, 0.0), 128, 1e-10)["coeffs"]
+        rots = set()
+        for st in self.s2c + self.c2s:
+            idx, _ = st.download()
+            baby = st.info()["baby"]
+            for d in idx.tolist():
+                rots.update(r for r in (d % baby, d - d % baby) if r)
         a = plan["aes"]
-        self.kl, self.kscales = a["key_level"], np.asarray(a["key_scales"], dtype=np.float64)
         self.pbc, self.psc, self.acb = a["packing_block_count"], a["packed_segment_count"], a["active_blocks"]
+        half = N // 2
+        rots.update(r % half for k in range(1, self.psc) for r in (k * self.pbc, -k * self.pbc))
+        self.rotations = sorted(r for r in rots if r)
+        seeds = iter(rng.integers(1, 2**63, len(self.rotations) + 8).tolist())
+        for r in self.rotations:
+            ctx.keygen_switch_key(wg.WG_KEY_ROTATION, r, self.secret, seed=next(seeds))
+        ctx.keygen_switch_key(wg.WG_KEY_CONJ, 0, self.secret, seed=next(seeds))
+        ctx.keygen_switch_key(wg.WG_KEY_RELIN, 0, self.secret, seed=next(seeds))
+        ctx.keygen_secret_switch(wg.WG_KEY_DENSE_TO_SPARSE, self.secret, self.low_secret, seed=next(seeds))
+        ctx.keygen_secret_switch(wg.WG_KEY_SPARSE_TO_DENSE, self.low_secret, self.secret, seed=next(seeds))
+        # a seeded AES key, its 1408 encrypted expanded-key bits on the device
+        from cryptography.hazmat.primitives.ciphers import Cipher, algorithms, modes
+
+        self.aes_key = bytes(rng.integers(0, 256, 16, dtype=np.uint8))
+        self._ecb = Cipher(algorithms.AES(self.aes_key), modes.ECB())
+        self.kl = b["s2c_depth"] + 1
         n = (self.kl + 1) * N
-        qcol = torch.from_numpy(np.repeat(q[: self.kl + 1], N).view(np.int64)).cuda()
-        gen = torch.Generator(device="cuda")
-        gen.manual_seed(seed)
-        self.key_dev = torch.randint(0, 1 << 62, (len(self.kscales), 2, n), dtype=torch.int64, device="cuda",
-                                     generator=gen) % qcol
-        self.key_bits = [(self.key_dev[k, 0], self.key_dev[k, 1]) for k in range(len(self.kscales))]
+        self.key_dev = torch.empty((1408, 2, n), dtype=torch.int64, device="cuda")
+        self.key_bits = [(self.key_dev[k, 0], self.key_dev[k, 1]) for k in range(1408)]
+        self.kscales, lv = ctx.aes_walsh_encrypt_round_key_bits(self.params, expand_key(self.aes_key), self.acb,
+                                                                self.secret, self.key_bits, seed=next(seeds))
+        assert (np.asarray(lv) == self.kl).all()
         full = (b["depth"] + 1) * N
         self.out_dev = torch.zeros((128, 2, full), dtype=torch.int64, device="cuda")
         self.outs = [(self.out_dev[k, 0], self.out_dev[k, 1]) for k in range(128)]
         self.blocks = 2 * self.acb
-        self.block_bytes = [bytes(rng.integers(0, 256, 16 * self.blocks, dtype=np.uint8)) for _ in range(4)]
+        # block_bytes[2i] counters, block_bytes[2i+1] CTR ciphertexts of plaintexts[i]
+        self.plaintexts, self.block_bytes = [], []
+        for _ in range(2):
+            ctr = bytes(rng.integers(0, 256, 16 * self.blocks, dtype=np.uint8))
+            pt = bytes(rng.integers(0, 256, 16 * self.blocks, dtype=np.uint8))
+            e = self._ecb.encryptor()
+            stream = e.update(ctr) + e.finalize()
+            self.plaintexts.append(pt)
+            self.block_bytes += [ctr, bytes(x ^ y for x, y in zip(pt, stream))]
         self.calls = 0
+        self.last = None
 
-    def step(self, stream):
-        c = self.block_bytes[self.calls % 4]
-        x = self.block_bytes[(self.calls + 1) % 4]
+    def step(self, stream, plain=False):
+        k = self.calls % 2
         self.calls += 1
+        self.last = k
         return self.ctx.aes_ctr_walsh(self.params, self.s2c, self.s2c_x2, self.c2s, self.coeffs, self.pbc, self.psc,
-                                      self.key_bits, self.kscales, self.kl, c, x, self.acb, self.outs, stream=stream)
+                                      self.key_bits, self.kscales, self.kl, self.block_bytes[2 * k],
+                                      self.block_bytes[2 * k + 1], self.acb, self.outs, stream=stream, plain=plain)
+
+    def check(self, levels, scales):
+        """Decrypt the last evaluation's 128 output bits on the device and compare them with the
+        plaintext the way the reference benchmark does (validate_walsh_outputs,
+        bench/aes_bench.cpp:156-195): mismatched blocks, max and average |lane - bit|."""
+        self.torch.cuda.synchronize()
+        pt = np.frombuffer(self.plaintexts[self.last], dtype=np.uint8).reshape(self.blocks, 16)
+        acb = self.acb
+        err_max, err_sum, count = 0.0, 0.0, 0
+        decoded = np.zeros((self.blocks, 16), np.uint8)
+        for lvl in sorted(set(int(x) for x in levels)):
+            bits = [i for i in range(128) if int(levels[i]) == lvl]
+            z = self.ctx.decrypt_decode(lvl, [scales[i] for i in bits], [self.outs[i] for i in bits], self.secret)
+            for j, bit in enumerate(bits):
+                vals = np.concatenate([z[j, :acb].real, z[j, :acb].imag])  # block s, then block acb + s
+                want = ((pt[:, bit // 8] >> (bit % 8)) & 1).astype(np.float64)
+                e = np.abs(vals - want)
+                err_max = max(err_max, float(e.max()))
+                err_sum += float(e.sum())
+                count += e.size
+                decoded[:, bit // 8] |= ((vals >= 0.5).astype(np.uint8) << (bit % 8))
+        mism = int((decoded != pt).any(axis=1).sum())
+        return {"max_error": err_max, "average_error": err_sum / count, "mismatches": mism, "blocks": self.blocks}
+
+
+def expand_key(key):
+    """AES-128 key expansion (FIPS-197): the 176-byte schedule."""
+    sbox = []
+    for x in range(256):
+        inv = 0
+        for y in range(1, 256):
+            a, b_, r = x, y, 0
+            while b_:
+                if b_ & 1:
+                    r ^= a
+                a = ((a << 1) ^ (0x1B if a & 0x80 else 0)) & 0xFF
+                b_ >>= 1
+            if r == 1:
+                inv = y
+                break
+        v, out = inv, 0x63
+        for _ in range(5):
+            out ^= v
+            v = ((v << 1) | (v >> 7)) & 0xFF
+        sbox.append(out)
+    w = list(key)
+    rcon = 1
+    for i in range(4, 44):
+        t = w[4 * (i - 1): 4 * i]
+        if i % 4 == 0:
+            t = [sbox[t[1]] ^ rcon, sbox[t[2]], sbox[t[3]], sbox[t[0]]]
+            rcon = ((rcon << 1) ^ (0x1B if rcon & 0x80 else 0)) & 0xFF
+        w += [w[4 * (i - 4) + k] ^ t[k] for k in range(4)]
+    return bytes(w)
 
 
 # ------------------------------------------------------------------------------------------
@@ -976,35 +1055,46 @@ def keygen_bench(wg, torch, local, seed, with_cpu):
     return res
 
 
-def serve_mix_bench(wg, torch, aes, xrun, requests, seed, walsh_cap, xboot_cap, window_ms=20.0, load=0.5):
-    """Config 5's mixed stream: requests alternate between walsh15 (log-uniform 2..1024 blocks,
-    even) and xboot15-full (log-uniform 1..16384 blocks), arriving as one seeded Poisson stream;
-    each parameter set has its own continuous-batching server (walsh15: two workers, xboot15:
-    one) on the same device, keys resident.  The arrival rate makes the offered work `load` x the
-    device at each set's measured full-slot capacity."""
+MIX_SETS = ("walsh15", "xboot15", "xboot15-sparse", "xboot14", "xboot14-sparse")
+MIX_MAX_BLOCKS = {"walsh15": 1024, "xboot15": 16384, "xboot15-sparse": 1024, "xboot14": 8192, "xboot14-sparse": 1024}
+
+
+def serve_mix_bench(wg, torch, aes, xruns, requests, seed, caps, window_ms=20.0, load=0.5, budget_gb=48):
+    """Config 5's mixed stream over all five AES parameter sets: requests cycle through walsh15
+    (log-uniform 2..1024 blocks, even), xboot15-full (1..16384), xboot15-sparse-1024 (1..1024),
+    xboot14-full (1..8192) and xboot14-sparse-1024 (1..1024), arriving as one seeded Poisson
+    stream whose offered work is `load` x the device at each set's measured full-slot capacity.
+    One continuous-batching server per set on the same device, keys resident, all admitted
+    through one shared device-memory budget (each evaluation holds an estimate of its working
+    set: four times its 128 output ciphertexts); the walsh15 server's streams have the highest
+    scheduling priority, so its one-second evaluations are not queued behind the XBOOT ones."""
     rng = np.random.default_rng(seed)
-    wfull, xfull = aes.out_dev.shape[2], xrun.out_dev.shape[2]
-    ws = wg.Server(aes.ctx, aes.params, aes.s2c, aes.s2c_x2, aes.c2s, aes.coeffs, aes.pbc, aes.psc, aes.key_bits,
-                   aes.kscales, aes.kl, workers=2, batch_window_ms=window_ms)
-    xs = wg.Server.xboot(xrun.ctx, xrun.params, xrun.s2c, xrun.c2s, xrun.coeffs, xrun.key_bits, xrun.kscales,
-                         xrun.klevels, workers=1, batch_window_ms=window_ms)
-    srv = {"walsh15": ws, "xboot15": xs}
-    cap = {"walsh15": walsh_cap, "xboot15": xboot_cap}
-    blocks_src = {"walsh15": aes.block_bytes, "xboot15": xrun.block_bytes}
-    mk = lambda full: [(torch.empty(full, dtype=torch.int64, device="cuda"),
-                        torch.empty(full, dtype=torch.int64, device="cuda")) for _ in range(128)]
+    runs = dict(xruns, walsh15=aes)
+    full = {k: r.out_dev.shape[2] for k, r in runs.items()}
+    budget = wg.ServeBudget(budget_gb << 30)
+    eval_bytes = {k: 4 * 128 * 2 * full[k] * 8 for k in runs}
+    srv = {"walsh15": wg.Server(aes.ctx, aes.params, aes.s2c, aes.s2c_x2, aes.c2s, aes.coeffs, aes.pbc, aes.psc,
+                                aes.key_bits, aes.kscales, aes.kl, workers=2, batch_window_ms=window_ms, priority=1,
+                                budget=budget, eval_bytes=eval_bytes["walsh15"])}
+    for k, r in xruns.items():
+        srv[k] = wg.Server.xboot(r.ctx, r.params, r.s2c, r.c2s, r.coeffs, r.key_bits, r.kscales, r.klevels, workers=1,
+                                 batch_window_ms=window_ms, budget=budget, eval_bytes=eval_bytes[k])
+    mk = lambda n: [(torch.empty(n, dtype=torch.int64, device="cuda"), torch.empty(n, dtype=torch.int64, device="cuda"))
+                    for _ in range(128)]
     try:
-        ids = [ws.submit(aes.block_bytes[0][:32], aes.block_bytes[1][:32], mk(wfull)),
-               xs.submit(xrun.block_bytes[0][:32], xrun.block_bytes[1][:32], mk(xfull))]
-        ws.wait(ids[0])
-        xs.wait(ids[1])
-        kinds = ["walsh15" if k % 2 == 0 else "xboot15" for k in range(requests)]
-        sizes = [2 * int(round(np.exp(rng.uniform(0.0, np.log(512))))) if kd == "walsh15"
-                 else int(round(np.exp(rng.uniform(0.0, np.log(16384))))) for kd in kinds]
-        work = [n / cap[kd] for kd, n in zip(kinds, sizes)]
+        warm = {k: srv[k].submit(runs[k].block_bytes[0][:32], runs[k].block_bytes[1][:32], mk(full[k])) for k in srv}
+        for k, i in warm.items():
+            srv[k].wait(i)
+        kinds = [MIX_SETS[k % len(MIX_SETS)] for k in range(requests)]
+        sizes = []
+        for kd in kinds:
+            top = MIX_MAX_BLOCKS[kd] // (2 if kd == "walsh15" else 1)
+            n = int(round(np.exp(rng.uniform(0.0, np.log(top)))))
+            sizes.append(2 * n if kd == "walsh15" else n)
+        work = [n / caps[kd] for kd, n in zip(kinds, sizes)]
         rate = load / float(np.mean(work))
         gaps = rng.exponential(1.0 / rate, requests)
-        bufs = [mk(wfull if kd == "walsh15" else xfull) for kd in kinds]
+        bufs = [mk(full[kd]) for kd in kinds]
         ids = []
         start = time.perf_counter()
         t = start
@@ -1013,20 +1103,25 @@ def serve_mix_bench(wg, torch, aes, xrun, requests, seed, walsh_cap, xboot_cap, 
             delay = t - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            src = blocks_src[kd]
+            src = runs[kd].block_bytes
             ids.append(srv[kd].submit(src[1][:16 * n], src[2][:16 * n], bufs[k]))
         res = [srv[kd].wait(i) for kd, i in zip(kinds, ids)]
         wall = time.perf_counter() - start
     finally:
-        ws.close()
-        xs.close()
-    out = {"workload": f"{requests} requests alternating walsh15 (log-uniform 2..1024 blocks, even) and xboot15-full "
-                       f"(log-uniform 1..16384 blocks), one Poisson stream at {load} x the device's full-slot "
-                       f"capacity; one server per parameter set on the same device",
+        for v in srv.values():
+            v.close()
+        budget.close()
+    offered = sum(sizes) / (sum(gaps) or 1.0)
+    out = {"workload": f"{requests} requests cycling walsh15, xboot15-full, xboot15-sparse-1024, xboot14-full and "
+                       f"xboot14-sparse-1024 (log-uniform sizes up to each set's slots), one Poisson stream at {load} "
+                       f"x the device's full-slot capacity; one server per set on the device, one shared "
+                       f"{budget_gb} GB device-memory budget, walsh15 streams at the highest priority",
            "batch_window_ms": window_ms, "arrival_rate_per_s": rate, "wall_s": wall,
-           "blocks_per_s": sum(sizes) / wall}
-    for kd in ("walsh15", "xboot15"):
+           "blocks_per_s": sum(sizes) / wall, "offered_blocks_per_s": offered}
+    for kd in MIX_SETS:
         sel = [k for k in range(requests) if kinds[k] == kd]
+        if not sel:
+            continue
         lat = np.array([res[k]["latency_ms"] for k in sel])
         evaluations = sum(1.0 / res[k]["batch_requests"] for k in sel)
         out[kd] = {"requests": len(sel), "blocks": int(sum(sizes[k] for k in sel)),
@@ -1034,8 +1129,20 @@ def serve_mix_bench(wg, torch, aes, xrun, requests, seed, walsh_cap, xboot_cap, 
                    "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                                   "max": float(lat.max())},
                    "requests_per_evaluation": len(sel) / evaluations,
-                   "full_slot_capacity_blocks_per_s": cap[kd]}
+                   "full_slot_capacity_blocks_per_s": caps[kd]}
     return out
+
+
+def evaluation_capacity(run, stream, torch):
+    """Full-slot blocks/s of one XBOOT evaluation (one warm-up, one timed)."""
+    run.step(stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run.step(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return run.blocks / (e0.elapsed_time(e1) / 1000.0)
 
 
 # ------------------------------------------------------------------------------------------
@@ -1111,12 +1218,30 @@ def main():
     host0 = wg.host_stats()
     with ClockSampler(None if args.no_clocks else local) as clk:
         evs[0].record(stream)
-        out_levels = None
+        out_levels = out_scales = None
         for i in range(args.steps):
-            out_levels, _ = aes_step()
+            out_levels, out_scales = aes_step()
             evs[i + 1].record(stream)
         barrier()
     launches = wg.launch_count() - launches0
+    # decrypt the last timed evaluation and check it against plain AES (outside the timing)
+    correctness = aes.check(out_levels, out_scales)
+
+    # the plain per-operation GPU path: the same circuit with every S-box instance and every
+    # refresh bootstrap as its own call (the reference's call granularity), same output words
+    aes_plain = None
+    if not args.no_plain:
+        ref_words = aes.out_dev.clone()
+        aes.calls -= 1  # the same counter blocks as the last timed evaluation
+        aes.step(stream, plain=True)
+        torch.cuda.synchronize()
+        same = bool(torch.equal(ref_words, aes.out_dev))
+        plain_ms = timed(lambda: aes.step(stream, plain=True), max(1, args.steps // 4))
+        aes_plain = {"value": aes.blocks * world / (plain_ms / 1000.0), "unit": UNIT, "ms_per_step": plain_ms,
+                     "steps": max(1, args.steps // 4), "batched_over_plain": plain_ms / ms,
+                     "same_output_words": same,
+                     "path": "wg_aes_ctr_walsh_plain: 16 S-box calls per round and one bootstrap call per refresh "
+                             "batch instead of one batched call each"}
     host1 = wg.host_stats()
     per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     ms = max_over_ranks(evs[0].elapsed_time(evs[-1]) / args.steps, dist)
@@ -1203,8 +1328,17 @@ def main():
         xboot_aes = xboot_aes_bench(wg, torch, stream, timed, xrun, args.seed + 29 + rank, args.xboot_aes_steps,
                                     rank == 0 and world == 1 and not args.no_cpu_baseline, sbox_s)
         if not args.no_serve:
-            serving_mix = serve_mix_bench(wg, torch, aes, xrun, args.serve_mix_requests, args.seed + 31 + rank,
-                                          aes.blocks / (ms / 1000.0), xboot_aes["blocks_per_s"])
+            xruns = {"xboot15": xrun}
+            caps = {"walsh15": aes.blocks / (ms / 1000.0), "xboot15": xboot_aes["blocks_per_s"]}
+            with open(XBOOT_PLAN_PATH) as f:
+                xplans = json.load(f)
+            for name, key in (("xboot15-sparse", "xboot15-sparse"), ("xboot14", "xboot14"),
+                              ("xboot14-sparse", "xboot14-sparse")):
+                xruns[name] = XbootAesRun(wg, torch, xplans[key], local, args.seed + 41 + rank)
+                caps[name] = evaluation_capacity(xruns[name], stream, torch)
+            serving_mix = serve_mix_bench(wg, torch, aes, xruns, args.serve_mix_requests, args.seed + 31 + rank,
+                                          caps)
+            del xruns
         del xrun
         torch.cuda.synchronize()
     keygen = None
@@ -1251,8 +1385,10 @@ def main():
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "ring_degree": N, "q_limbs": len(plan["q"]), "p_limbs": len(plan["p"]),
                    "dnum": plan["dnum"], "blocks_per_step": aes.blocks, "rounds": ROUNDS,
-                   "keys": "uniform residues of the walsh15 key shapes (65 rotation keys, relin, conj, sparse/dense)",
-                   "shapes": "tests/golden/walsh15_plan.json (the reference's walsh15 bootstrapping plan)",
+                   "keys": "made on the device from a seeded ternary secret (h = 256) and sparse secret (h = 32): "
+                           f"{len(aes.rotations)} rotation keys, relin, conj, dense-to-sparse, sparse-to-dense",
+                   "plans": "SlotToCoeff (x1, x2) and CoeffToSlot generated by the library (wg_dft_plan_create), "
+                            "EvalMod series by wg_evalmod_fit, key bits of a seeded AES key encrypted on the device",
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2: 2.2 GB of encrypted key bits and 1.7 GB of rotation keys per step",
                    "step": "one wg_aes_ctr_walsh call on device-resident keys with host counter blocks"},
@@ -1273,9 +1409,60 @@ def main():
         "keygen": keygen,
         "batched_ops": ops,
         "bsgs": bsgs,
+        "aes_plain": aes_plain,
         "cpu_baseline": cpu,
     }
+    line["correctness"] = dict(correctness, reference_result=REFERENCE_RESULT)
+    line["summary"] = summary_keys(line)
     print(json.dumps(line), flush=True)
+
+
+# The reference's own RESULT line for this workload (aes_bench walsh15 on 8 host cores).
+REFERENCE_RESULT = {"seconds": 210.037, "max_error": 1.083466e-05, "average_error": 2.766340e-07, "mismatches": 0,
+                    "cores": 8}
+
+
+def summary_keys(line):
+    """The headline figures and the device-over-reference ratio of every section in one short
+    record at the end of the line (the part of the output that survives a truncated log)."""
+    def ratio(dev, ref):
+        try:
+            return float(dev) / float(ref) if dev and ref else None
+        except (TypeError, ValueError):
+            return None
+
+    def get(d, *path):
+        for k in path:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    out = {"blocks_per_s": line["value"], "e2e_blocks_per_s": get(line, "e2e", "value"),
+           "ntt_frac_of_hbm": get(line, "roofline", "frac"),
+           "max_error": get(line, "correctness", "max_error"),
+           "average_error": get(line, "correctness", "average_error"),
+           "mismatches": get(line, "correctness", "mismatches")}
+    cpu = line.get("cpu_baseline") or {}
+    out["aes_vs_reference_cpu"] = ratio(line["value"], cpu.get("value"))
+    c1 = get(line, "primitives", "config1") or {}
+    r1 = c1.get("reference_cpu") or {}
+    out["config1_ntt_fwd_vs_reference"] = ratio(r1.get("forward_us"), c1.get("forward_us"))
+    out["config1_rotation_vs_reference"] = ratio(r1.get("rotation_us"), c1.get("rotation_us"))
+    ops = line.get("batched_ops") or {}
+    out["config2_graph_vs_reference"] = ratio(get(ops, "batched_graph", "value"), get(ops, "reference_cpu", "value"))
+    out["config2_graph_vs_plain_gpu"] = ops.get("batched_over_plain")
+    bs = line.get("bsgs") or {}
+    out["config3_c2s_vs_reference"] = ratio(get(bs, "coeff_to_slot", "ciphertexts_per_s"),
+                                           get(bs, "reference_cpu", "coeff_to_slot", "ciphertexts_per_s"))
+    out["config3_s2c_vs_reference"] = ratio(get(bs, "slot_to_coeff", "ciphertexts_per_s"),
+                                           get(bs, "reference_cpu", "slot_to_coeff", "ciphertexts_per_s"))
+    xa = line.get("xboot_aes") or {}
+    out["xboot_aes_vs_reference"] = ratio(xa.get("blocks_per_s"),
+                                          get(xa, "reference_cpu", "estimated_blocks_per_s"))
+    pl = line.get("aes_plain") or {}
+    out["aes_batched_vs_plain_gpu"] = pl.get("batched_over_plain")
+    return out
 
 
 if __name__ == "__main__":

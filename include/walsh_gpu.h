@@ -371,6 +371,18 @@ int wg_aes_ctr_walsh(wg_context* ctx, const wg_bootstrap_params* params, const w
                      const uint8_t* counters, const uint8_t* ciphertexts, size_t active_blocks,
                      uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
                      void* stream);
+/* The same AES-CTR issued at the reference's call granularity (no counterpart in the reference
+ * as an entry point): every S-box instance and every refresh bootstrap as its own call instead
+ * of one batch per round, the plain per-operation GPU path the batched evaluation is measured
+ * against.  Same arguments and the same output words as wg_aes_ctr_walsh. */
+int wg_aes_ctr_walsh_plain(wg_context* ctx, const wg_bootstrap_params* params, const wg_lt_stage* const* s2c,
+                           size_t ns2c, const wg_lt_stage* const* s2c_x2, size_t ns2c_x2,
+                           const wg_lt_stage* const* c2s, size_t nc2s, const double* coeffs, size_t ncoeffs,
+                           size_t packing_block_count, size_t packed_segment_count, const uint64_t* const* key_b,
+                           const uint64_t* const* key_a, const double* key_scales, size_t key_level,
+                           const uint8_t* counters, const uint8_t* ciphertexts, size_t active_blocks,
+                           uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale,
+                           void* stream);
 
 /* The XBOOT AES S-box on lazy bits (ckks_aes_xboot_sbox_impl,
  * src/ckks/operations/circuits/aes/ckks_aes_ctr.cpp:280-336, with its monomial tree :185-256
@@ -475,6 +487,22 @@ int wg_encode_slots_device(wg_context* ctx, size_t count, size_t limbs, double s
 int wg_bundle_save(wg_context* ctx, const char* path, const wg_lt_stage* const* stages, size_t nstages);
 int wg_bundle_load(wg_context* ctx, const char* path, wg_lt_stage** stages, size_t max_stages, size_t* nstages);
 
+/* Ciphertext wire format (host memory only; no counterpart in the reference, which keeps
+ * ciphertexts in memory): a self-checking record of one ciphertext ("WGC1", version, N, level,
+ * polynomial count, scale, secret owner and encoding labels, the level + 1 moduli, the
+ * residues [poly][level + 1][N] in evaluation form, FNV-1a checksum).  wg_ct_wire_bytes gives
+ * the record's size; wg_ct_wire_encode writes it from host residues `polys`; wg_ct_wire_decode
+ * checks a record against the ring degree N and the Q moduli q[nq] of the receiving context
+ * (same degree, the record's moduli a prefix of q, every residue below its modulus, checksum)
+ * and copies out its residues (polys: room for cap_words words) and labels.  Move residues to
+ * and from the device with wg_memcpy_dtoh / wg_memcpy_htod. */
+size_t wg_ct_wire_bytes(uint64_t N, size_t level, size_t npolys);
+int wg_ct_wire_encode(uint64_t N, const uint64_t* q, size_t level, size_t npolys, const uint64_t* polys, double scale,
+                      int secret_owner, int encoding_state, uint8_t* out, size_t cap);
+int wg_ct_wire_decode(const uint8_t* in, size_t len, uint64_t N, const uint64_t* q, size_t nq, uint64_t* polys,
+                      size_t cap_words, size_t* level, size_t* npolys, double* scale, int* secret_owner,
+                      int* encoding_state);
+
 /* The Walsh AES's encrypted round-key bits on the device: replaces
  * ckks_aes128_encrypt_expanded_round_key_bits_walsh_complex_blocks (src/ckks/operations/circuits/
  * aes/ckks_aes_ctr_walsh_sbox.cpp:981-1035).  Bit k of the 176-byte expanded key as (v, v) in the
@@ -518,7 +546,18 @@ typedef struct wg_serve_config {
     size_t max_blocks;       /* block slots per evaluation (0: 2 x packing_block_count) */
     double batch_window_ms;  /* a free worker waits up to this long after the oldest queued request
                                 for more requests to fill its evaluation (0: start at once) */
+    int priority;            /* 1: the workers' streams take the device's highest scheduling
+                                priority, so this server's (short) evaluations are not queued behind
+                                another server's long ones; 0: default */
+    struct wg_serve_budget* budget; /* device bytes shared with other servers (null: none); each
+                                evaluation holds eval_bytes of it while it runs */
 } wg_serve_config;
+/* A device-memory budget shared by several servers on one device (no counterpart in the
+ * reference): an evaluation starts only when its eval_bytes fit beside the evaluations of every
+ * server holding the budget.  Destroy it after the servers that use it. */
+typedef struct wg_serve_budget wg_serve_budget;
+int wg_serve_budget_create(size_t bytes, wg_serve_budget** out);
+void wg_serve_budget_destroy(wg_serve_budget* budget);
 typedef struct wg_serve_result {
     int status;              /* WG_OK, or the error code of the request's evaluation */
     size_t block_offset, active_blocks, batch_requests, batch_blocks;

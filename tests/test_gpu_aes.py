@@ -90,6 +90,18 @@ def test_aes_ctr_matches_reference_and_plain_aes(wg, ref_mod):
     assert dev_err.max <= ref_err.max and dev_err.avg <= ref_err.avg
     assert dev_err.max < 0.5  # the reference benchmark's acceptance rule (bench/aes_bench.cpp:305-307)
 
+    # the plain per-operation path (every S-box instance and refresh bootstrap as its own call)
+    # gives the same words
+    plain = [(torch.zeros(full, dtype=torch.int64, device="cuda"), torch.zeros(full, dtype=torch.int64, device="cuda"))
+             for _ in range(128)]
+    plv, psc = ctx.aes_ctr_walsh(params, s2c, s2c2, c2s, info["coeffs"], 512, 32, key_bits, kscales, kl, counters,
+                                 cts, acb, plain, plain=True)
+    torch.cuda.synchronize()
+    assert (plv, psc) == (lvls, scs)
+    for bit in range(128):
+        m = (lvls[bit] + 1) * N
+        assert torch.equal(plain[bit][0][:m], outs[bit][0][:m]) and torch.equal(plain[bit][1][:m], outs[bit][1][:m]), bit
+
 
 class _ErrorStats:
     """max and average of |lane value - expected bit| over lanes, as validate_walsh_outputs

@@ -181,16 +181,17 @@ def test_config1_ntt_and_rotation(wg, oracle_mod):
     assert (_host(wg, db) == ob).all() and (_host(wg, da) == oa).all()
 
 
-def test_walsh15_batched_ops(wg, oracle_mod):
-    """Config 2 shape: walsh15 chain, ciphertexts at seeded levels 1..12, each mul + relin +
-    rescale + rotate by a seeded index, through the batched entry point, bit-exact."""
+@pytest.mark.parametrize("count,nrot", [(16, 4), (64, 16)])
+def test_walsh15_batched_ops(wg, oracle_mod, count, nrot):
+    """Config 2: walsh15 chain, ciphertexts at seeded levels 1..12, each mul + relin + rescale +
+    rotate by a seeded index, through the batched entry point, bit-exact; at the benchmark's 64
+    ciphertexts and a smaller batch."""
     import torch
 
-    rng = np.random.default_rng(2)
+    rng = np.random.default_rng(2 + count)
     pool = [512 * k for k in range(1, 32)] + [-512 * k for k in range(1, 32)]
-    rots = [int(r) for r in rng.choice(pool, 4, replace=False)]
+    rots = [int(r) for r in rng.choice(pool, nrot, replace=False)]
     N, o, ctx, keys, _, relin = _oracle_setup(oracle_mod, wg, WALSH15, rots)
-    count = 16
     levels = rng.integers(1, 13, count)
     ct_rots = [rots[i % len(rots)] for i in range(count)]
     L = o.nq
