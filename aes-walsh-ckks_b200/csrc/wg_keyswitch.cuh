@@ -97,7 +97,9 @@ WG_HD uint64_t moddown_coeff(const Modulus& mq, const Modulus* __restrict__ pmod
     for (int pi = 0; pi < K; ++pi) {
         const uint64_t s = red4q(src_p[(size_t)pi * N + coeff], pmods[pi].q);
         alpha = dfma(u2d(s), pmods[pi].inv_q, alpha);
-        const uint64_t term = mul_shoup(barrett_u64(s, q, mq.mu_hi), WG_LDG(inv + pi), WG_LDG(inv_s + pi), q);
+        // the reference reduces s mod q first (barrett_reduce_u64); the Shoup product is the
+        // canonical residue of s * inv for any 64-bit s, so the reduction cannot change it
+        const uint64_t term = mul_shoup(s, WG_LDG(inv + pi), WG_LDG(inv_s + pi), q);
         acc = add_mod(acc, term, q);
     }
     uint64_t hps = round_half_up(alpha);
@@ -130,10 +132,10 @@ WG_HD void moddown_all_limbs_k(const Modulus* __restrict__ mods, int nq, int L, 
         const uint64_t* iv = inv + (size_t)qi * K;
         const uint64_t* ivs = inv_s + (size_t)qi * K;
         uint64_t acc = 0;
+        // s[pi] mod q need not be formed: the Shoup product is canonical for any 64-bit input
 #pragma unroll
         for (int pi = 0; pi < KW; ++pi)
-            if (pi < K)
-                acc = add_mod(acc, mul_shoup(barrett_u64(s[pi], q, mq.mu_hi), WG_LDG(iv + pi), WG_LDG(ivs + pi), q), q);
+            if (pi < K) acc = add_mod(acc, mul_shoup(s[pi], WG_LDG(iv + pi), WG_LDG(ivs + pi), q), q);
         out[(size_t)qi * N + coeff] = sub_mod(acc, hps, q);
     }
 }

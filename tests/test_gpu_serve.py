@@ -42,7 +42,9 @@ def _plain_bits(plain, blocks):
     return np.array([[(plain[16 * b + bit // 8] >> (bit % 8)) & 1 for bit in range(128)] for b in range(blocks)])
 
 
-def test_served_requests_alone_and_in_a_mix(wg, ref_mod):
+@pytest.fixture(scope="module")
+def walsh15_service(wg, ref_mod):
+    """The reference walsh15 context's keys, plans and encrypted key bits on the device."""
     import torch
 
     R = ref_mod.RefPlans(bootstrap_keys=True)
@@ -79,9 +81,16 @@ def test_served_requests_alone_and_in_a_mix(wg, ref_mod):
     full = (info["depth"] + 1) * N
     mk = lambda: [(torch.zeros(full, dtype=torch.int64, device="cuda"),
                    torch.zeros(full, dtype=torch.int64, device="cuda")) for _ in range(128)]
+    return dict(R=R, rng=rng, ek=ek, ctx=ctx, params=params, s2c=s2c, s2c2=s2c2, c2s=c2s, coeffs=info["coeffs"],
+                key_bits=key_bits, kscales=kscales, kl=kl, mk=mk)
+
+
+def test_served_requests_alone_and_in_a_mix(wg, walsh15_service):
+    S = walsh15_service
+    R, rng, ek, mk = S["R"], S["rng"], S["ek"], S["mk"]
     # a 300 ms batching window: requests queued within it share an evaluation when they fit
-    srv = wg.Server(ctx, params, s2c, s2c2, c2s, info["coeffs"], 512, 32, key_bits, kscales, kl, workers=2,
-                    batch_window_ms=300.0)
+    srv = wg.Server(S["ctx"], S["params"], S["s2c"], S["s2c2"], S["c2s"], S["coeffs"], 512, 32, S["key_bits"],
+                    S["kscales"], S["kl"], workers=2, batch_window_ms=300.0)
     try:
         a_ctr, a_ct, a_plain = _request(rng, ek, 6)
         b_ctr, b_ct, b_plain = _request(rng, ek, 20)
@@ -112,3 +121,32 @@ def test_served_requests_alone_and_in_a_mix(wg, ref_mod):
               f"C {rc['latency_ms']:.0f} ms (queued {rc['queue_ms']:.0f} ms)")
     finally:
         srv.close()
+
+
+def test_servers_sharing_a_budget(wg, walsh15_service):
+    """Two servers on one device (one at the highest stream priority) share a device-memory
+    budget that admits one evaluation at a time: their evaluations run one after the other, and
+    each request still decrypts to its plaintext."""
+    S = walsh15_service
+    R, rng, ek, mk = S["R"], S["rng"], S["ek"], S["mk"]
+    budget = wg.ServeBudget(1 << 30)
+    args = (S["ctx"], S["params"], S["s2c"], S["s2c2"], S["c2s"], S["coeffs"], 512, 32, S["key_bits"], S["kscales"],
+            S["kl"])
+    hi = wg.Server(*args, workers=1, priority=1, budget=budget, eval_bytes=1 << 30)
+    lo = wg.Server(*args, workers=1, priority=0, budget=budget, eval_bytes=1 << 30)
+    try:
+        x_ctr, x_ct, x_plain = _request(rng, ek, 8)
+        y_ctr, y_ct, y_plain = _request(rng, ek, 10)
+        ox, oy = mk(), mk()
+        ix = lo.submit(x_ctr, x_ct, ox)
+        iy = hi.submit(y_ctr, y_ct, oy)
+        rx, ry = lo.wait(ix, 600), hi.wait(iy, 600)
+        first, second = (rx, ry) if rx["queue_ms"] <= ry["queue_ms"] else (ry, rx)
+        # the second evaluation started only after the first had released the budget
+        assert second["queue_ms"] >= first["latency_ms"] - 50.0
+        assert (_decrypt_bits(wg, R, ox, rx, 8) == _plain_bits(x_plain, 8)).all()
+        assert (_decrypt_bits(wg, R, oy, ry, 10) == _plain_bits(y_plain, 10)).all()
+    finally:
+        hi.close()
+        lo.close()
+        budget.close()
