@@ -48,6 +48,8 @@ struct KsPlan {
     const GatherJob* gather;
     int n_gather;
     double mac_bytes, modup_bytes, moddown_bytes, combine_bytes;
+    bool fused;   // ModUp / ModDown fused with the NTT column phases (Context::ks_fused)
+    int max_src;  // widest digit (fused ModUp shared memory)
 };
 
 size_t batch_keyswitch_words(const Context& c, const KsItem* items, size_t n) {
@@ -65,6 +67,7 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
     std::vector<CombineJob> combine;
     std::vector<GatherJob> gather;
     KsPlan p{};
+    p.fused = c.ks_fused;
     // MAC groups: consecutive switches with the same key, level and digit layout (up to
     // kMacGroup), one job per QP limb; [group_begin, it) is the open group
     size_t group_begin = 0;
@@ -111,6 +114,7 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
         for (size_t j = 0; j < B; ++j) {
             modup.push_back({c.d_modup + level * c.dnum + j, coeff, digits + j * T * N});
             const ModUpDesc& d = c.modup[level][j];
+            p.max_src = std::max(p.max_src, d.src_count);
             p.modup_bytes += 8.0 * N * (d.src_count + d.dst_count);
             const size_t s0 = j * c.alpha, s1 = std::min(s0 + c.alpha, L);
             for (size_t l = 0; l < T; ++l) {
@@ -173,6 +177,27 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
 
 static void run_keyswitch(const Context& c, const KsPlan& p, const JobTable& t, cudaStream_t s) {
     const size_t N = c.N;
+    if (p.fused) {
+        // inverse row phase -> [inverse column phase, ModUp, forward column phase] -> forward
+        // row phase; the same around ModDown (wg_ksfuse.cu)
+        ntt_jobs_phase(c, t.at(p.intt_in), p.n_intt_in, false, false, s);
+        modup_ntt_jobs(c, t.at(p.modup), p.n_modup, p.max_src, p.modup_bytes, s);
+        ntt_jobs_phase(c, t.at(p.ntt_digits), p.n_ntt_digits, true, false, s);
+        {
+            Probe probe(kClsKeyMac, p.mac_bytes, s);
+            kb_mac_group<<<grid_for(c, p.n_mac), kT, 0, s>>>(t.at(p.mac), p.n_mac, c.d_mod, (int)c.nq, N);
+        }
+        ntt_jobs_phase(c, t.at(p.intt_p), p.n_intt_p, false, false, s);
+        moddown_ntt_jobs(c, t.at(p.moddown), p.n_moddown, p.moddown_bytes, s);
+        ntt_jobs_phase(c, t.at(p.ntt_contrib), p.n_ntt_contrib, true, false, s);
+        {
+            Probe probe(kClsCombine, p.combine_bytes, s);
+            kb_combine<<<grid_for(c, p.n_combine), kT, 0, s>>>(t.at(p.combine), p.n_combine, c.d_mod, N);
+            if (p.n_gather) kb_gather<<<grid_for(c, p.n_gather), kT, 0, s>>>(t.at(p.gather), p.n_gather, c.logN);
+        }
+        check_cuda(cudaGetLastError(), "batched keyswitch launch");
+        return;
+    }
     ntt_jobs(c, t.at(p.intt_in), p.n_intt_in, false, s);
     {
         Probe probe(kClsModUp, p.modup_bytes, s);

@@ -13,11 +13,10 @@ namespace {  // each translation unit gets its own copy of the kernels
 
 constexpr int kT = 256;
 
-struct ModUpJob {
-    const ModUpDesc* desc;
-    const uint64_t* src;
-    uint64_t* digit;
-};
+// One digit (ModUp) or one accumulator polynomial (ModDown): the same jobs feed the fused
+// kernels of wg_ksfuse.cu.
+using ModUpJob = ModUpNttJob;
+using ModDownJob = ModDownNttJob;
 struct MacJob {
     const uint64_t* key;
     const uint64_t* key_term;
@@ -36,14 +35,6 @@ struct MacGroupJob {
     uint64_t* acc[kMacGroup];
     size_t part_stride;
     int L, K, parts, alpha, key_level, i, n, pad;
-};
-struct ModDownJob {
-    const uint64_t* src_p;  // P limbs of one accumulator (coefficient form)
-    uint64_t* out;          // L contribution limbs
-    const uint64_t* inv;    // folded P^-1 table of the level, [qi][pi]
-    const uint64_t* inv_s;
-    int L;
-    int pad;
 };
 struct CombineJob {
     const uint64_t* acc;

@@ -344,6 +344,10 @@ int wg_ntt_set_geometry(wg_context* ctx, int direction, int phase, int geometry)
     });
 }
 
+int wg_set_keyswitch_fusion(wg_context* ctx, int fused) {
+    return guard([&] { C(ctx).ks_fused = fused != 0; });
+}
+
 int wg_keyswitch(wg_context* ctx, size_t level, const uint64_t* key_term, int kind, int64_t rotation, uint64_t* b,
                  uint64_t* a, int b_add, int a_add, void* stream) {
     return guard([&] {

@@ -141,6 +141,9 @@ struct Context {
     Modulus* d_mod = nullptr;
     uint64_t* d_tw = nullptr;        // [mod][2][N] (w, Shoup w) pairs: forward, inverse (ntt::TwPair)
     int ntt_variant[2][2] = {{0, 0}, {0, 0}};  // NTT geometry per [direction][phase: rows, columns]
+    // key switches run ModUp and ModDown fused with the adjacent NTT column phases
+    // (wg_ksfuse.cu); false: the separate launches (same words)
+    bool ks_fused = true;
     NttTuning tuning{};
     // ModUp descriptors, host copies holding device pointers: [level][part]
     std::vector<std::vector<ModUpDesc>> modup;
@@ -261,6 +264,36 @@ void ntt_autotune(Context& c);
 // One phase (cols: the high-bit phase) of a strided batch with a given geometry.
 void ntt_phase_geometry(const Context& c, bool forward, bool cols, int variant, uint64_t* data, int limbs,
                         int polys, size_t poly_stride, LimbMap map, cudaStream_t s);
+
+// One phase of a job-table NTT (cols: the high-bit phase) with the context's geometry; the
+// inverse transform is rows then columns, the forward one columns then rows, and the first
+// phase reads src and writes dst.
+void ntt_jobs_phase(const Context& c, const NttJob* d_jobs, int njobs, bool forward, bool cols, cudaStream_t s);
+
+// ModUp and ModDown jobs of the batched kernels (kb_modup, kb_moddown: coefficient-form limbs in
+// and out) and of the fused key-switch steps (wg_ksfuse.cu).  A ModUp job is one digit of one
+// switch: for the fused kernel src holds the switch's L Q limbs after the inverse row phase, and
+// every destination limb of the digit is written after the forward column phase (the forward
+// row phase follows as a job-table launch).  A ModDown job is one accumulator polynomial: for
+// the fused kernel src_p holds its K P limbs after the inverse row phase, and out receives the L
+// contribution limbs after the forward column phase.
+struct ModUpNttJob {
+    const ModUpDesc* desc;
+    const uint64_t* src;
+    uint64_t* digit;
+};
+struct ModDownNttJob {
+    const uint64_t* src_p;
+    uint64_t* out;
+    const uint64_t* inv;  // folded P^-1 table of the level, [qi][pi]
+    const uint64_t* inv_s;
+    int L;
+    int pad;
+};
+// max_src: the largest source-limb count of the jobs (shared-memory size).
+void modup_ntt_jobs(const Context& c, const ModUpNttJob* d_jobs, int njobs, int max_src, double bytes,
+                    cudaStream_t s);
+void moddown_ntt_jobs(const Context& c, const ModDownNttJob* d_jobs, int njobs, double bytes, cudaStream_t s);
 
 // NTT over `polys` polynomials of `limbs` limbs each, `poly_stride` words apart.
 void ntt_forward(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride,

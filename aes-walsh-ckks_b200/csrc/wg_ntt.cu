@@ -249,6 +249,13 @@ void ntt_jobs(const Context& c, const NttJob* d_jobs, int njobs, bool forward, c
     dispatch(c, nullptr, 0, 0, 0, LimbMap{0, 0, 0}, d_jobs, njobs, forward, s);
 }
 
+void ntt_jobs_phase(const Context& c, const NttJob* d_jobs, int njobs, bool forward, bool cols, cudaStream_t s) {
+    if (njobs <= 0) return;
+    phase_dispatch(c, forward, cols, c.ntt_variant[forward ? 0 : 1][cols ? 1 : 0], nullptr, 0, 0, 0, LimbMap{0, 0, 0},
+                   d_jobs, njobs, s);
+    check_cuda(cudaGetLastError(), "ntt launch");
+}
+
 void ntt_phase_geometry(const Context& c, bool forward, bool cols, int variant, uint64_t* data, int limbs, int polys,
                         size_t poly_stride, LimbMap map, cudaStream_t s) {
     if (variant < 0 || variant >= kNttGeometries) fail(kInvalid, "ntt: unknown geometry");

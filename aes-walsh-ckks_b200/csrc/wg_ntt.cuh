@@ -70,14 +70,15 @@ WG_HDC constexpr RoundPlan make_plan(int rd) {
 //   STAGED: the CTA first copies the twiddle pairs it will read into shared memory; otherwise
 //           the rounds read them from the (L2-resident) global table directly, which leaves
 //           shared memory to the data tile and admits more CTAs per SM.
-template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED>
+//   TL:     largest tile (elements per CTA); a column-phase tile holds TL >> NB1 whole columns.
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, int TL = kMaxTile>
 struct Phase {
     static constexpr int N = 1 << LOGN;
     static constexpr int NB1 = LOGN / 2;
     static constexpr int NB2 = LOGN - NB1;
     static constexpr int MB = COLS ? NB1 : NB2;
     static constexpr int E = 1 << EB;
-    static constexpr int TILE = N < kMaxTile ? N : kMaxTile;
+    static constexpr int TILE = N < TL ? N : TL;
     static constexpr int THREADS = TILE / E;
     static constexpr int SUBS = TILE >> MB;  // sub-transforms per tile
     static constexpr int OB = MB - EB;
@@ -94,9 +95,9 @@ struct Phase {
 // Table index of staged twiddle t (see Phase::TW).  Row-stage k occupies staged entries
 // [SUBS (2^k - 1), SUBS (2^(k+1) - 1)) and maps to table entries starting at
 // 2^(NB1 + k) + tile * SUBS * 2^k.
-template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED>
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, int TL = kMaxTile>
 WG_HD size_t twiddle_src(int tile, int t) {
-    using P = Phase<LOGN, FWD, COLS, EB, STAGED>;
+    using P = Phase<LOGN, FWD, COLS, EB, STAGED, TL>;
     if (COLS) return (size_t)t;
     const int k = floor_log2((unsigned)(t / P::SUBS + 1));
     const int off = P::SUBS * ((1 << k) - 1);
@@ -128,9 +129,9 @@ static_assert((4 + 2 * 16) < (1 << (64 - 58)), "lazy forward bound: 36 q < 2^64 
 // twiddles) plus a compile-time offset: pad16 and shifts distribute over disjoint bit sets.
 // Loads then use immediate offsets, and butterflies of a stage that share a twiddle load it
 // once (same address).
-template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, int RD, bool LAZY = false>
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, int RD, bool LAZY = false, int TL = kMaxTile>
 WG_HD void ntt_round(uint64_t* sm, int sub, int o, int tile, uint64_t q, const TwPair* __restrict__ tw) {
-    using P = Phase<LOGN, FWD, COLS, EB, STAGED>;
+    using P = Phase<LOGN, FWD, COLS, EB, STAGED, TL>;
     constexpr int E = P::E;
     constexpr RoundPlan plan = make_plan<P::MB, FWD, EB>(RD);
     const uint64_t two_q = q << 1;
@@ -201,9 +202,9 @@ WG_HD void ntt_round(uint64_t* sm, int sub, int o, int tile, uint64_t q, const T
 }
 
 // Global offset (within one limb) of tile element e.
-template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED>
+template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, int TL = kMaxTile>
 WG_HD size_t tile_offset(int tile, int e) {
-    using P = Phase<LOGN, FWD, COLS, EB, STAGED>;
+    using P = Phase<LOGN, FWD, COLS, EB, STAGED, TL>;
     if (COLS) {
         const int hh = e / P::SUBS, c = e % P::SUBS;
         return ((size_t)hh << P::NB2) + (size_t)tile * P::SUBS + c;

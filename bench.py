@@ -394,6 +394,11 @@ def ops_bench(args, wg, torch, stream, timed, rank, local, with_cpu=False):
     for _ in range(args.warmup):
         nograph_step()
     nograph_ms = timed(nograph_step, steps)
+    # the same batched call with ModUp / ModDown as separate launches (no NTT column fusion)
+    ctx.set_keyswitch_fusion(False)
+    nograph_step()
+    unfused_ms = timed(nograph_step, steps)
+    ctx.set_keyswitch_fusion(True)
     plain_step()
     l0 = wg.launch_count()
     plain_ms = timed(plain_step, max(1, steps // 2))
@@ -469,6 +474,8 @@ def ops_bench(args, wg, torch, stream, timed, rank, local, with_cpu=False):
         "batched_graph": {"value": count / (graph_ms / 1000.0), "ms_per_step": graph_ms,
                           "launches_per_step": graph_launches},
         "batched_nograph": {"value": count / (nograph_ms / 1000.0), "ms_per_step": nograph_ms},
+        "batched_nograph_unfused_keyswitch": {"value": count / (unfused_ms / 1000.0), "ms_per_step": unfused_ms,
+                                              "fused_speedup": unfused_ms / nograph_ms},
         "plain_per_op": {"value": count / (plain_ms / 1000.0), "ms_per_step": plain_ms,
                          "launches_per_step": plain_launches},
         "batched_over_plain": plain_ms / graph_ms,
@@ -1224,6 +1231,11 @@ def main():
             evs[i + 1].record(stream)
         barrier()
     launches = wg.launch_count() - launches0
+    host1 = wg.host_stats()
+    per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    ms = max_over_ranks(evs[0].elapsed_time(evs[-1]) / args.steps, dist)
+    value = aes.blocks * world / (ms / 1000.0)
+    staged = (host1["stage_bytes"] - host0["stage_bytes"]) / args.steps
     # decrypt the last timed evaluation and check it against plain AES (outside the timing)
     correctness = aes.check(out_levels, out_scales)
 
@@ -1242,11 +1254,17 @@ def main():
                      "same_output_words": same,
                      "path": "wg_aes_ctr_walsh_plain: 16 S-box calls per round and one bootstrap call per refresh "
                              "batch instead of one batched call each"}
-    host1 = wg.host_stats()
-    per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
-    ms = max_over_ranks(evs[0].elapsed_time(evs[-1]) / args.steps, dist)
-    value = aes.blocks * world / (ms / 1000.0)
-    staged = (host1["stage_bytes"] - host0["stage_bytes"]) / args.steps
+    # the same evaluation with the key switches' ModUp / ModDown as separate launches
+    aes_unfused = None
+    if not args.no_plain:
+        aes.ctx.set_keyswitch_fusion(False)
+        aes_step()
+        unfused_ms = timed(aes_step, max(1, args.steps // 4))
+        aes.ctx.set_keyswitch_fusion(True)
+        aes_unfused = {"value": aes.blocks * world / (unfused_ms / 1000.0), "unit": UNIT,
+                       "ms_per_step": unfused_ms, "fused_speedup": unfused_ms / ms,
+                       "path": "wg_aes_ctr_walsh with ModUp and ModDown as separate launches from the NTT "
+                               "column phases (wg_set_keyswitch_fusion 0)"}
 
     # end to end: the same call from host block bytes, plus the read-back of the 128 output
     # bit ciphertexts into pinned host memory, every step
@@ -1410,6 +1428,7 @@ def main():
         "batched_ops": ops,
         "bsgs": bsgs,
         "aes_plain": aes_plain,
+        "aes_unfused_keyswitch": aes_unfused,
         "cpu_baseline": cpu,
     }
     line["correctness"] = dict(correctness, reference_result=REFERENCE_RESULT)
@@ -1462,6 +1481,8 @@ def summary_keys(line):
                                           get(xa, "reference_cpu", "estimated_blocks_per_s"))
     pl = line.get("aes_plain") or {}
     out["aes_batched_vs_plain_gpu"] = pl.get("batched_over_plain")
+    out["aes_fused_vs_unfused_keyswitch"] = get(line, "aes_unfused_keyswitch", "fused_speedup")
+    out["config2_fused_vs_unfused_keyswitch"] = get(ops, "batched_nograph_unfused_keyswitch", "fused_speedup")
     return out
 
 

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "wg_keyswitch.cuh"
+#include "wg_ksfuse.cuh"
 #include "wg_ntt.cuh"
 #include "wg_tables.hpp"
 #include "wg_walsh.cuh"
@@ -36,6 +37,7 @@ struct Emu {
     HostTables H;
     int logN;
     std::vector<std::vector<HostModUp>> modup;
+    std::vector<ntt::TwPair> tw;  // interleaved table of every modulus: [mod][fwd N, inv N]
 };
 
 template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, bool LAZY, int... RD>
@@ -120,6 +122,121 @@ void ntt_one(const Emu& E, uint64_t* x, int mi, bool fwd) {
     }
 }
 
+// Key switches run the fused ModUp / ModDown sequence of wg_ksfuse.cu (Context::ks_fused).
+int g_fused = 0;
+
+template <int LOGN, bool FWD, bool LAZY, int... RD>
+void col_rounds(std::integer_sequence<int, RD...>, uint64_t* sm, int tile, uint64_t q, const ntt::TwPair* tw) {
+    using G = ksf::Geom<LOGN>;
+    auto one = [&](auto rd_const) {
+        constexpr int R = decltype(rd_const)::value;
+        for (int t = 0; t < G::THREADS; ++t) ksf::col_round<LOGN, FWD, R, LAZY>(sm, tile, t, q, tw);
+    };
+    (one(std::integral_constant<int, RD>{}), ...);
+}
+
+template <int LOGN>
+void inverse_cols(const Emu& E, uint64_t* sm, int tile, int mi) {
+    using G = ksf::Geom<LOGN>;
+    const Modulus& m = E.H.mods[mi];
+    col_rounds<LOGN, false, false>(std::make_integer_sequence<int, G::ROUNDS>{}, sm, tile, m.q,
+                                   E.tw.data() + (size_t)mi * 2 * G::N + G::N);
+    for (int t = 0; t < G::THREADS; ++t) ksf::scale_n_inv<LOGN>(sm, t, m);
+}
+
+template <int LOGN>
+void forward_cols(const Emu& E, uint64_t* sm, int tile, int mi) {
+    using G = ksf::Geom<LOGN>;
+    const uint64_t q = E.H.mods[mi].q;
+    const ntt::TwPair* tw = E.tw.data() + (size_t)mi * 2 * G::N;
+    if (q < ntt::kLazyForwardLimit)
+        col_rounds<LOGN, true, true>(std::make_integer_sequence<int, G::ROUNDS>{}, sm, tile, q, tw);
+    else
+        col_rounds<LOGN, true, false>(std::make_integer_sequence<int, G::ROUNDS>{}, sm, tile, q, tw);
+}
+
+// k_modup_ntt over every column tile of one digit.
+template <int LOGN>
+void modup_fused(const Emu& E, const HostModUp& d, const uint64_t* src, uint64_t* digit) {
+    using G = ksf::Geom<LOGN>;
+    const int n = d.src_count;
+    std::vector<uint64_t> smem((size_t)(n + 1) * G::PAD);
+    uint64_t* work = smem.data() + (size_t)n * G::PAD;
+    for (int tile = 0; tile < G::TILES; ++tile) {
+        std::vector<double> alpha((size_t)G::THREADS * G::E, 0.0);
+        for (int i = 0; i < n; ++i) {
+            const int mi = d.src_first + i;
+            uint64_t* sm = smem.data() + (size_t)i * G::PAD;
+            for (int t = 0; t < G::THREADS; ++t) ksf::load_tile<LOGN>(sm, src + (size_t)mi * G::N, tile, t);
+            inverse_cols<LOGN>(E, sm, tile, mi);
+            for (int t = 0; t < G::THREADS; ++t)
+                ksf::modup_scale<LOGN>(sm, t, d, i, E.H.mods[mi].q, alpha.data() + (size_t)t * G::E);
+        }
+        std::vector<uint32_t> hps((size_t)G::THREADS * G::E);
+        for (size_t k = 0; k < hps.size(); ++k) hps[k] = ksf::hps_count(alpha[k], n);
+        for (int dst = 0; dst < d.dst_count; ++dst) {
+            const int mi = d.dst_mod[dst];
+            for (int t = 0; t < G::THREADS; ++t)
+                ksf::modup_value<LOGN>(work, smem.data(), t, d, dst, E.H.mods[mi].q, hps.data() + (size_t)t * G::E);
+            forward_cols<LOGN>(E, work, tile, mi);
+            for (int t = 0; t < G::THREADS; ++t)
+                ksf::store_tile<LOGN>(work, digit + (size_t)d.dst_limb[dst] * G::N, tile, t);
+        }
+    }
+}
+
+// k_moddown_ntt over every column tile of one accumulator polynomial.
+template <int LOGN>
+void moddown_fused(const Emu& E, const uint64_t* src_p, uint64_t* out, int L, const uint64_t* inv,
+                   const uint64_t* inv_s) {
+    using G = ksf::Geom<LOGN>;
+    const int K = (int)E.H.np, nq = (int)E.H.nq;
+    const Modulus* pmods = E.H.mods.data() + nq;
+    std::vector<uint64_t> smem((size_t)(K + 1) * G::PAD);
+    uint64_t* work = smem.data() + (size_t)K * G::PAD;
+    for (int tile = 0; tile < G::TILES; ++tile) {
+        for (int pi = 0; pi < K; ++pi) {
+            uint64_t* sm = smem.data() + (size_t)pi * G::PAD;
+            for (int t = 0; t < G::THREADS; ++t) ksf::load_tile<LOGN>(sm, src_p + (size_t)pi * G::N, tile, t);
+            inverse_cols<LOGN>(E, sm, tile, nq + pi);
+        }
+        std::vector<uint32_t> hps((size_t)G::THREADS * G::E);
+        for (int t = 0; t < G::THREADS; ++t)
+            ksf::moddown_hps<LOGN>(smem.data(), t, pmods, K, hps.data() + (size_t)t * G::E);
+        for (int qi = 0; qi < L; ++qi) {
+            for (int t = 0; t < G::THREADS; ++t)
+                ksf::moddown_value<LOGN>(work, smem.data(), t, pmods, K, E.H.mods[qi].q, inv + (size_t)qi * K,
+                                         inv_s + (size_t)qi * K, hps.data() + (size_t)t * G::E);
+            forward_cols<LOGN>(E, work, tile, qi);
+            for (int t = 0; t < G::THREADS; ++t) ksf::store_tile<LOGN>(work, out + (size_t)qi * G::N, tile, t);
+        }
+    }
+}
+
+// One phase of one limb with the emulated geometry (cols: the high-bit phase).
+template <int LOGN>
+void phase_one(const Emu& E, uint64_t* x, int mi, bool fwd, bool cols) {
+    if (fwd) {
+        if (cols) phase_geom<LOGN, true, true>(E, x, mi);
+        else phase_geom<LOGN, true, false>(E, x, mi);
+    } else {
+        if (cols) phase_geom<LOGN, false, true>(E, x, mi);
+        else phase_geom<LOGN, false, false>(E, x, mi);
+    }
+}
+
+#define EMU_LOGN_SWITCH(logN, CALL)                                        \
+    do switch (logN) {                                                     \
+        case 10: { constexpr int LG = 10; CALL; } break;                   \
+        case 11: { constexpr int LG = 11; CALL; } break;                   \
+        case 12: { constexpr int LG = 12; CALL; } break;                   \
+        case 13: { constexpr int LG = 13; CALL; } break;                   \
+        case 14: { constexpr int LG = 14; CALL; } break;                   \
+        case 15: { constexpr int LG = 15; CALL; } break;                   \
+        case 16: { constexpr int LG = 16; CALL; } break;                   \
+        default: throw std::invalid_argument("emu: unsupported ring degree"); \
+    } while (0)
+
 }  // namespace
 
 extern "C" {
@@ -147,12 +264,16 @@ void* emu_create(uint64_t N, const uint64_t* q, size_t nq, const uint64_t* p, si
             d.dst_mod = reinterpret_cast<const int*>(T + o.dst_mod);
             E->modup[l].push_back(d);
         }
+    E->tw.resize((nq + np) * 2 * N);
+    for (size_t m = 0; m < nq + np; ++m)
+        ntt::interleave_twiddles(N, E->H.tw.data() + m * 4 * N, E->tw.data() + m * 2 * N);
     return E;
 }
 
 void emu_destroy(void* h) { delete static_cast<Emu*>(h); }
 
 void emu_set_ntt_geometry(int geometry) { g_geometry = geometry; }
+void emu_set_keyswitch_fusion(int fused) { g_fused = fused; }
 
 // limbs consecutive limbs using modulus index first.. (basis 0 = Q, 1 = P)
 void emu_ntt(void* h, uint64_t* poly, size_t limbs, size_t first, int basis, int inverse) {
@@ -175,29 +296,52 @@ void emu_keyswitch(void* h, size_t level, const uint64_t* key_term, const uint64
     uint64_t* contrib = acc + 2 * T * N;
     const Modulus* mods = E.H.mods.data();
     std::memcpy(coeff, key_term, L * N * 8);
-    for (size_t l = 0; l < L; ++l) ntt_one(E, coeff + l * N, (int)l, false);
-    for (size_t j = 0; j < B; ++j)
-        for (size_t c = 0; c < N; ++c) modup_coeff(E.modup[level][j], mods, coeff, digits + j * T * N, N, c);
+    if (g_fused) {
+        // inverse row phase, fused [inverse columns, ModUp, forward columns], forward row phase
+        for (size_t l = 0; l < L; ++l) EMU_LOGN_SWITCH(E.logN, phase_one<LG>(E, coeff + l * N, (int)l, false, false));
+        for (size_t j = 0; j < B; ++j)
+            EMU_LOGN_SWITCH(E.logN, modup_fused<LG>(E, E.modup[level][j], coeff, digits + j * T * N));
+    } else {
+        for (size_t l = 0; l < L; ++l) ntt_one(E, coeff + l * N, (int)l, false);
+        for (size_t j = 0; j < B; ++j)
+            for (size_t c = 0; c < N; ++c) modup_coeff(E.modup[level][j], mods, coeff, digits + j * T * N, N, c);
+    }
     for (size_t j = 0; j < B; ++j) {
         const size_t s0 = j * alpha, s1 = std::min(s0 + alpha, L);
         for (size_t l = 0; l < T; ++l) {
             if (l >= s0 && l < s1) continue;
-            ntt_one(E, digits + j * T * N + l * N, (int)(l < L ? l : nq + (l - L)), true);
+            const int mi = (int)(l < L ? l : nq + (l - L));
+            if (g_fused)
+                EMU_LOGN_SWITCH(E.logN, phase_one<LG>(E, digits + j * T * N + l * N, mi, true, false));
+            else
+                ntt_one(E, digits + j * T * N + l * N, mi, true);
         }
     }
     for (size_t i = 0; i < T; ++i)
         for (size_t c = 0; c < N; ++c)
             mac_coeff(mods, (int)nq, (int)L, (int)K, (int)B, (int)alpha, key, (int)key_level, key_term, digits, T * N,
                       acc, N, (int)i, c);
-    for (int poly = 0; poly < 2; ++poly)
-        for (size_t pi = 0; pi < K; ++pi) ntt_one(E, acc + (poly * T + L + pi) * N, (int)(nq + pi), false);
     const uint64_t* W = E.H.words.data();
-    for (int poly = 0; poly < 2; ++poly)
-        for (size_t c = 0; c < N; ++c)
-            moddown_all_limbs(mods, (int)nq, (int)L, (int)K, acc + (poly * T + L) * N, N, c, W + E.H.fold_inv[level],
-                              W + E.H.fold_inv_s[level], contrib + poly * L * N);
-    for (int poly = 0; poly < 2; ++poly)
-        for (size_t qi = 0; qi < L; ++qi) ntt_one(E, contrib + (poly * L + qi) * N, (int)qi, true);
+    if (g_fused) {
+        for (int poly = 0; poly < 2; ++poly)
+            for (size_t pi = 0; pi < K; ++pi)
+                EMU_LOGN_SWITCH(E.logN, phase_one<LG>(E, acc + (poly * T + L + pi) * N, (int)(nq + pi), false, false));
+        for (int poly = 0; poly < 2; ++poly)
+            EMU_LOGN_SWITCH(E.logN, moddown_fused<LG>(E, acc + (poly * T + L) * N, contrib + poly * L * N, (int)L,
+                                                      W + E.H.fold_inv[level], W + E.H.fold_inv_s[level]));
+        for (int poly = 0; poly < 2; ++poly)
+            for (size_t qi = 0; qi < L; ++qi)
+                EMU_LOGN_SWITCH(E.logN, phase_one<LG>(E, contrib + (poly * L + qi) * N, (int)qi, true, false));
+    } else {
+        for (int poly = 0; poly < 2; ++poly)
+            for (size_t pi = 0; pi < K; ++pi) ntt_one(E, acc + (poly * T + L + pi) * N, (int)(nq + pi), false);
+        for (int poly = 0; poly < 2; ++poly)
+            for (size_t c = 0; c < N; ++c)
+                moddown_all_limbs(mods, (int)nq, (int)L, (int)K, acc + (poly * T + L) * N, N, c,
+                                  W + E.H.fold_inv[level], W + E.H.fold_inv_s[level], contrib + poly * L * N);
+        for (int poly = 0; poly < 2; ++poly)
+            for (size_t qi = 0; qi < L; ++qi) ntt_one(E, contrib + (poly * L + qi) * N, (int)qi, true);
+    }
     if (galois == 0) {
         for (size_t qi = 0; qi < L; ++qi)
             for (size_t c = 0; c < N; ++c)

@@ -31,18 +31,24 @@ def emu(tmp_path_factory):
     E.emu_destroy.argtypes = [C.c_void_p]
     E.emu_ntt.argtypes = [C.c_void_p, u64p, C.c_size_t, C.c_size_t, C.c_int, C.c_int]
     E.emu_set_ntt_geometry.argtypes = [C.c_int]
+    E.emu_set_keyswitch_fusion.argtypes = [C.c_int]
     E.emu_keyswitch.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, C.c_size_t, u64p, u64p, C.c_int, C.c_int,
                                 C.c_uint64]
     return E
 
 
+@pytest.mark.parametrize("fused", [0, 1])
 @pytest.mark.parametrize("prm", SMALL)
-def test_emulated_kernels_match_oracle(oracle_mod, emu, prm):
+def test_emulated_kernels_match_oracle(oracle_mod, emu, prm, fused):
+    """NTT and key switch (rotation, relinearisation) at three levels; fused = 1 runs the key
+    switch as the device does by default: ModUp and ModDown inside the NTT column phases
+    (wg_ksfuse.cuh), the row phases as separate passes."""
     O = oracle_mod
     N = 1 << prm["logN"]
     p, q = O.find_primes(prm["p_bits"], prm["q_bits"], N)
     o = O.OracleCtx(N, q, p, prm["dnum"])
     h = emu.emu_create(N, q, len(q), p, len(p), prm["dnum"])
+    emu.emu_set_keyswitch_fusion(fused)
     try:
         L = len(q)
         x = o.uniform(L, 5)
@@ -72,6 +78,7 @@ def test_emulated_kernels_match_oracle(oracle_mod, emu, prm):
             emu.emu_keyswitch(h, level, c2, rl, L - 1, e0, e1, 1, 1, 0)
             assert (e0 == r0).all() and (e1 == r1).all()
     finally:
+        emu.emu_set_keyswitch_fusion(0)
         emu.emu_destroy(h)
 
 

@@ -189,7 +189,9 @@ def test_walsh15_batched_ops(wg, oracle_mod, count, nrot):
     import torch
 
     rng = np.random.default_rng(2 + count)
-    pool = [512 * k for k in range(1, 32)] + [-512 * k for k in range(1, 32)]
+    # distinct rotations modulo the N/2 slots (-512 k and 512 (32 - k) would share one Galois
+    # element, hence one key slot on the device, while the oracle is handed two different keys)
+    pool = [512 * k for k in range(1, 16)] + [-512 * k for k in range(1, 16)]
     rots = [int(r) for r in rng.choice(pool, nrot, replace=False)]
     N, o, ctx, keys, _, relin = _oracle_setup(oracle_mod, wg, WALSH15, rots)
     levels = rng.integers(1, 13, count)
@@ -211,6 +213,13 @@ def test_walsh15_batched_ops(wg, oracle_mod, count, nrot):
                                        [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots,
                                        plain=True)
     assert (_host(wg, pxb) == gb).all() and (_host(wg, pxa) == ga).all()
+    # ModUp / ModDown as separate launches instead of inside the NTT column phases: same residues
+    ctx.set_keyswitch_fusion(False)
+    uxb, uxa = _dev(wg, xb), _dev(wg, xa)
+    ctx.batch_mul_relin_rescale_rotate(levels, [sl(uxb, i) for i in range(count)], [sl(uxa, i) for i in range(count)],
+                                       [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots)
+    ctx.set_keyswitch_fusion(True)
+    assert (_host(wg, uxb) == gb).all() and (_host(wg, uxa) == ga).all()
     # the graph-captured plan over its own buffers: same residues, replayable
     gxb, gxa = _dev(wg, xb), _dev(wg, xa)
     plan = wg.BatchPlan(ctx, levels, [sl(gxb, i) for i in range(count)], [sl(gxa, i) for i in range(count)],
