@@ -344,6 +344,10 @@ int wg_ntt_set_geometry(wg_context* ctx, int direction, int phase, int geometry)
     });
 }
 
+int wg_ctx_trim(wg_context* ctx, void* stream) {
+    return guard([&] { C(ctx).trim(S(stream)); });
+}
+
 int wg_set_keyswitch_fusion(wg_context* ctx, int fused) {
     return guard([&] { C(ctx).ks_fused = fused != 0; });
 }

@@ -134,6 +134,9 @@ BatchBuffers& Context::batch_buffers(cudaStream_t s) {
     return batches[s];
 }
 
+// bytes cached by the chunk caches of every context of the process
+static std::atomic<size_t> chunk_cache_total{0};
+
 void* Context::take_chunk(size_t bytes, cudaStream_t s, size_t* got) {
     if (capturing(s)) return nullptr;  // no dependency on work outside a capture
     std::lock_guard<std::mutex> g(chunk_mutex);
@@ -142,6 +145,7 @@ void* Context::take_chunk(size_t bytes, cudaStream_t s, size_t* got) {
     const CachedChunk ch = it->second;
     chunk_cache.erase(it);
     chunk_cache_bytes -= ch.bytes;
+    chunk_cache_total -= ch.bytes;
     check_cuda(cudaStreamWaitEvent(s, ch.done, 0), "chunk reuse");
     chunk_events.push_back(ch.done);
     *got = ch.bytes;
@@ -150,7 +154,7 @@ void* Context::take_chunk(size_t bytes, cudaStream_t s, size_t* got) {
 
 void Context::give_chunk(void* p, size_t bytes, cudaStream_t s) {
     std::lock_guard<std::mutex> g(chunk_mutex);
-    if (capturing(s) || chunk_cache_bytes + bytes > kChunkCacheBytes) {
+    if (capturing(s) || chunk_cache_total.load() + bytes > kChunkCacheBytes) {
         cudaFreeAsync(p, s);
         return;
     }
@@ -171,9 +175,40 @@ void Context::give_chunk(void* p, size_t bytes, cudaStream_t s) {
     }
     chunk_cache.emplace(bytes, CachedChunk{p, bytes, ev});
     chunk_cache_bytes += bytes;
+    chunk_cache_total += bytes;
+}
+
+void Context::trim(cudaStream_t s) {
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    {
+        std::lock_guard<std::mutex> g(ws_mutex);
+        if (capturing(s)) fail(kRuntime, "trim: the stream is capturing a graph");
+        auto bi = batches.find(s);
+        if (bi != batches.end()) {
+            check_cuda(cudaStreamSynchronize(s), "trim");
+            bi->second.release();
+            batches.erase(bi);
+        }
+        auto wi = workspaces.find(s);
+        if (wi != workspaces.end()) {
+            check_cuda(cudaStreamSynchronize(s), "trim");
+            cudaFree(wi->second.base);
+            workspaces.erase(wi);
+        }
+    }
+    std::lock_guard<std::mutex> g(chunk_mutex);
+    for (auto& kv : chunk_cache) {
+        cudaEventSynchronize(kv.second.done);
+        cudaFree(kv.second.p);
+        chunk_events.push_back(kv.second.done);
+    }
+    chunk_cache.clear();
+    chunk_cache_total -= chunk_cache_bytes;
+    chunk_cache_bytes = 0;
 }
 
 Context::~Context() {
+    chunk_cache_total -= chunk_cache_bytes;
     for (auto& kv : chunk_cache) {
         cudaFree(kv.second.p);
         cudaEventDestroy(kv.second.done);

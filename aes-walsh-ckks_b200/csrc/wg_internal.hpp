@@ -180,7 +180,9 @@ struct Context {
     // Chunks of stream-ordered device memory that finished operation sets hand back for later
     // ones: each carries an event recorded on the stream that last used it, and a taker's stream
     // waits on that event before its first use, so reuse needs no host synchronisation and
-    // works across streams.  At most kChunkCacheBytes are kept; the rest is freed.
+    // works across streams.  At most kChunkCacheBytes are kept over all contexts of the
+    // process together (chunk_cache_total), so many contexts on one device do not each hold
+    // their own reserve; the rest is freed.
     struct CachedChunk {
         void* p;
         size_t bytes;
@@ -194,6 +196,10 @@ struct Context {
     // a cached chunk of at least `bytes` (at most twice that) made safe for use on s, or nullptr
     void* take_chunk(size_t bytes, cudaStream_t s, size_t* got);
     void give_chunk(void* p, size_t bytes, cudaStream_t s);
+    // Give back what the context holds for stream s beyond its tables and keys: the stream's
+    // batched scratch arena and staging ring, its single-operation workspace, and every cached
+    // chunk (waiting for their last users first).  The next call on s allocates again.
+    void trim(cudaStream_t s);
 
     ~Context();
     uint64_t* workspace(cudaStream_t s);   // scratch for one in-flight operation on stream s

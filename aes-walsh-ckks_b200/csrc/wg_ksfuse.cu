@@ -11,9 +11,9 @@
 //   phase of every output limb
 //
 // in shared memory (wg_ksfuse.cuh), so the coefficient-form source limbs and the un-transformed
-// outputs never reach device memory.  Per switch at walsh15 (L = 13, K = 4, dnum 3) the
-// NTT/ModUp/ModDown traffic falls from 417 to 251 limb passes of 8N bytes, with the same words
-// written.
+// outputs never reach device memory.  Per switch at walsh15's top level (L = 13, K = 4, three
+// digits of 5, 5 and 3 source limbs, 38 destination limbs) the NTT/ModUp/ModDown traffic falls
+// from 425 to 255 limb passes of 8N bytes, with the same words written.
 #include <utility>
 
 #include "wg_internal.hpp"

@@ -247,6 +247,9 @@ void Server::worker(size_t w) {
                     check_cuda(cudaMemcpyAsync(r.out_a[k], oa[k], bytes, cudaMemcpyDeviceToDevice, me.stream), "serve out");
                 }
             check_cuda(cudaStreamSynchronize(me.stream), "serve evaluation");
+            // under a budget shared with other servers the bytes held between evaluations count
+            // too: give back this stream's scratch and the context's cached chunks
+            if (cfg_.budget) c_.trim(me.stream);
         } catch (const Error& e) {
             base.status = e.code;
             base.error = e.what();

@@ -60,7 +60,9 @@ struct ServeConfig {
                                    // priority, so this server's kernels go first when servers
                                    // share the device (short evaluations do not wait behind long
                                    // ones); 0: default priority
-    ServeBudget* budget = nullptr; // shared with other servers (null: this server's own limit)
+    ServeBudget* budget = nullptr; // shared with other servers (null: this server's own limit);
+                                   // workers then release their stream's scratch after each
+                                   // evaluation (Context::trim), so idle servers hold none
 };
 
 struct ServeResult {

@@ -65,6 +65,7 @@ def lib() -> C.CDLL:
         L.wg_ctx_set_key.argtypes = [vp, C.c_int, C.c_int64, vp, sz, sz]
         L.wg_ctx_has_key.argtypes = [vp, C.c_int, C.c_int64]
         L.wg_ctx_reserve.argtypes = [vp, vp]
+        L.wg_ctx_trim.argtypes = [vp, vp]
         L.wg_ctx_workspace_words.argtypes = [vp]
         L.wg_ctx_workspace_words.restype = sz
         for f in (L.wg_ntt_forward, L.wg_ntt_inverse):
@@ -624,6 +625,14 @@ class Context:
 
     def reserve(self, stream=None):
         _check(lib().wg_ctx_reserve(self.h, _stream(stream)))
+
+    def workspace_words(self):
+        """Scratch words one in-flight single operation uses on a stream."""
+        return int(lib().wg_ctx_workspace_words(self.h))
+
+    def trim(self, stream=None):
+        """Free the stream's scratch and the cached scratch chunks (after the stream's work)."""
+        _check(lib().wg_ctx_trim(self.h, _stream(stream)))
 
     # --- operations on device buffers -------------------------------------------------
     def ntt_forward(self, poly, limbs, first=0, basis=0, polys=1, stride=0, stream=None):

@@ -1066,42 +1066,48 @@ MIX_SETS = ("walsh15", "xboot15", "xboot15-sparse", "xboot14", "xboot14-sparse")
 MIX_MAX_BLOCKS = {"walsh15": 1024, "xboot15": 16384, "xboot15-sparse": 1024, "xboot14": 8192, "xboot14-sparse": 1024}
 
 
-def serve_mix_bench(wg, torch, aes, xruns, requests, seed, caps, window_ms=20.0, load=0.5, budget_gb=48):
+def serve_mix_bench(wg, torch, aes, xruns, requests, seed, caps, eval_bytes, budget_frac=0.85, window_ms=20.0,
+                    load=0.5):
     """Config 5's mixed stream over all five AES parameter sets: requests cycle through walsh15
     (log-uniform 2..1024 blocks, even), xboot15-full (1..16384), xboot15-sparse-1024 (1..1024),
     xboot14-full (1..8192) and xboot14-sparse-1024 (1..1024), arriving as one seeded Poisson
     stream whose offered work is `load` x the device at each set's measured full-slot capacity.
     One continuous-batching server per set on the same device, keys resident, all admitted
-    through one shared device-memory budget (each evaluation holds an estimate of its working
-    set: four times its 128 output ciphertexts); the walsh15 server's streams have the highest
-    scheduling priority, so its one-second evaluations are not queued behind the XBOOT ones."""
+    through one shared device-memory budget (budget_frac of the device memory left free once
+    every set's keys, plans and request buffers are resident; each evaluation holds its measured
+    working set, evaluation_bytes, and workers give their scratch back after each evaluation);
+    the walsh15 server's streams have the highest scheduling priority, so its one-second
+    evaluations are not queued behind the XBOOT ones."""
     rng = np.random.default_rng(seed)
     runs = dict(xruns, walsh15=aes)
     full = {k: r.out_dev.shape[2] for k, r in runs.items()}
-    budget = wg.ServeBudget(budget_gb << 30)
-    eval_bytes = {k: 4 * 128 * 2 * full[k] * 8 for k in runs}
+    kinds = [MIX_SETS[k % len(MIX_SETS)] for k in range(requests)]
+    sizes = []
+    for kd in kinds:
+        top = MIX_MAX_BLOCKS[kd] // (2 if kd == "walsh15" else 1)
+        n = int(round(np.exp(rng.uniform(0.0, np.log(top)))))
+        sizes.append(2 * n if kd == "walsh15" else n)
+    work = [n / caps[kd] for kd, n in zip(kinds, sizes)]
+    mk = lambda n: [(torch.empty(n, dtype=torch.int64, device="cuda"), torch.empty(n, dtype=torch.int64, device="cuda"))
+                    for _ in range(128)]
+    # every request's output buffers first, then the budget: the device memory left over
+    bufs = [mk(full[kd]) for kd in kinds]
+    warm_bufs = {k: mk(full[k]) for k in runs}
+    torch.cuda.synchronize()
+    budget_bytes = budget_frac * torch.cuda.mem_get_info()[0]
+    budget = wg.ServeBudget(int(budget_bytes))
     srv = {"walsh15": wg.Server(aes.ctx, aes.params, aes.s2c, aes.s2c_x2, aes.c2s, aes.coeffs, aes.pbc, aes.psc,
                                 aes.key_bits, aes.kscales, aes.kl, workers=2, batch_window_ms=window_ms, priority=1,
                                 budget=budget, eval_bytes=eval_bytes["walsh15"])}
     for k, r in xruns.items():
         srv[k] = wg.Server.xboot(r.ctx, r.params, r.s2c, r.c2s, r.coeffs, r.key_bits, r.kscales, r.klevels, workers=1,
                                  batch_window_ms=window_ms, budget=budget, eval_bytes=eval_bytes[k])
-    mk = lambda n: [(torch.empty(n, dtype=torch.int64, device="cuda"), torch.empty(n, dtype=torch.int64, device="cuda"))
-                    for _ in range(128)]
     try:
-        warm = {k: srv[k].submit(runs[k].block_bytes[0][:32], runs[k].block_bytes[1][:32], mk(full[k])) for k in srv}
+        warm = {k: srv[k].submit(runs[k].block_bytes[0][:32], runs[k].block_bytes[1][:32], warm_bufs[k]) for k in srv}
         for k, i in warm.items():
             srv[k].wait(i)
-        kinds = [MIX_SETS[k % len(MIX_SETS)] for k in range(requests)]
-        sizes = []
-        for kd in kinds:
-            top = MIX_MAX_BLOCKS[kd] // (2 if kd == "walsh15" else 1)
-            n = int(round(np.exp(rng.uniform(0.0, np.log(top)))))
-            sizes.append(2 * n if kd == "walsh15" else n)
-        work = [n / caps[kd] for kd, n in zip(kinds, sizes)]
         rate = load / float(np.mean(work))
         gaps = rng.exponential(1.0 / rate, requests)
-        bufs = [mk(full[kd]) for kd in kinds]
         ids = []
         start = time.perf_counter()
         t = start
@@ -1122,7 +1128,9 @@ def serve_mix_bench(wg, torch, aes, xruns, requests, seed, caps, window_ms=20.0,
     out = {"workload": f"{requests} requests cycling walsh15, xboot15-full, xboot15-sparse-1024, xboot14-full and "
                        f"xboot14-sparse-1024 (log-uniform sizes up to each set's slots), one Poisson stream at {load} "
                        f"x the device's full-slot capacity; one server per set on the device, one shared "
-                       f"{budget_gb} GB device-memory budget, walsh15 streams at the highest priority",
+                       f"device-memory budget of {budget_bytes / 2**30:.1f} GiB, walsh15 streams at the highest "
+                       f"priority",
+           "budget_gib": budget_bytes / 2**30, "evaluation_gib": {k: v / 2**30 for k, v in eval_bytes.items()},
            "batch_window_ms": window_ms, "arrival_rate_per_s": rate, "wall_s": wall,
            "blocks_per_s": sum(sizes) / wall, "offered_blocks_per_s": offered}
     for kd in MIX_SETS:
@@ -1150,6 +1158,21 @@ def evaluation_capacity(run, stream, torch):
     e1.record(stream)
     torch.cuda.synchronize()
     return run.blocks / (e0.elapsed_time(e1) / 1000.0)
+
+
+def evaluation_bytes(run, stream, torch):
+    """Device bytes one evaluation of the run's context keeps after it ends (its stream's
+    scratch plus the reusable chunks it handed back), measured from a trimmed context: the
+    admission estimate of the served mix.  The context is trimmed again afterwards."""
+    run.ctx.trim(stream)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    run.step(stream)
+    torch.cuda.synchronize()
+    held = max(0, free0 - torch.cuda.mem_get_info()[0])
+    run.ctx.trim(stream)
+    torch.cuda.synchronize()
+    return held
 
 
 # ------------------------------------------------------------------------------------------
@@ -1199,7 +1222,12 @@ def main():
         except (OSError, ValueError):
             pass
         prim = None if args.no_ntt else ntt_bench(wg, torch, stream, timed, local, 20, hbm)
-        ops = None if args.no_ops else ops_bench(args, wg, torch, stream, timed, rank, local)[0]
+        ops = bs = None
+        if not args.no_ops:
+            ops, octx, oq, op_ = ops_bench(args, wg, torch, stream, timed, rank, local)
+            if not args.no_bsgs:
+                bs = bsgs_bench(wg, octx, oq, op_, stream, timed, 2, args.warmup)
+            del octx
         xaes = None
         if not args.no_xboot_aes:
             with open(XBOOT_PLAN_PATH) as f:
@@ -1209,7 +1237,8 @@ def main():
         kg = None if args.no_keygen else keygen_bench(wg, torch, local, args.seed + 37 + rank, False)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "note": "--no-aes profiling run",
-                              "primitives": prim, "batched_ops": ops, "xboot_aes": xaes, "keygen": kg}), flush=True)
+                              "primitives": prim, "batched_ops": ops, "bsgs": bs, "xboot_aes": xaes, "keygen": kg}),
+                  flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return
@@ -1348,14 +1377,18 @@ def main():
         if not args.no_serve:
             xruns = {"xboot15": xrun}
             caps = {"walsh15": aes.blocks / (ms / 1000.0), "xboot15": xboot_aes["blocks_per_s"]}
+            # every set's keys and plans resident, no evaluation scratch held between sections
+            eval_bytes = {"walsh15": evaluation_bytes(aes, stream, torch),
+                          "xboot15": evaluation_bytes(xrun, stream, torch)}
             with open(XBOOT_PLAN_PATH) as f:
                 xplans = json.load(f)
             for name, key in (("xboot15-sparse", "xboot15-sparse"), ("xboot14", "xboot14"),
                               ("xboot14-sparse", "xboot14-sparse")):
                 xruns[name] = XbootAesRun(wg, torch, xplans[key], local, args.seed + 41 + rank)
                 caps[name] = evaluation_capacity(xruns[name], stream, torch)
+                eval_bytes[name] = evaluation_bytes(xruns[name], stream, torch)
             serving_mix = serve_mix_bench(wg, torch, aes, xruns, args.serve_mix_requests, args.seed + 31 + rank,
-                                          caps)
+                                          caps, eval_bytes)
             del xruns
         del xrun
         torch.cuda.synchronize()

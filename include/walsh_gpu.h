@@ -106,6 +106,12 @@ int wg_keygen_secret_switch(wg_context* ctx, int kind, const int8_t* source, con
 int wg_ctx_has_key(const wg_context* ctx, int kind, int64_t rotation);
 /* Allocate the scratch of `stream` now (required before capturing the stream in a graph). */
 int wg_ctx_reserve(wg_context* ctx, void* stream);
+/* Give back the device memory the context holds for `stream` beyond its tables and keys (the
+ * stream's scratch and staging buffers) and its cache of reusable scratch chunks, after the
+ * stream's queued work finishes; the next call on the stream allocates again.  For processes
+ * that keep several contexts on one device and use them in turn.  (No counterpart in the
+ * reference, which allocates per operation.) */
+int wg_ctx_trim(wg_context* ctx, void* stream);
 /* Scratch words one in-flight operation uses (informational). */
 size_t wg_ctx_workspace_words(const wg_context* ctx);
 

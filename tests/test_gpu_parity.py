@@ -181,6 +181,27 @@ def test_config1_ntt_and_rotation(wg, oracle_mod):
     assert (_host(wg, db) == ob).all() and (_host(wg, da) == oa).all()
 
 
+def test_trim_gives_back_scratch(wg, oracle_mod):
+    """wg_ctx_trim frees the stream's scratch (device free memory rises by at least four
+    ciphertext polynomials' worth: the key switch's digits alone are larger) and the context
+    keeps working: a rotation before and after, bit-exact."""
+    import torch
+
+    N, o, ctx, keys, _, _ = _oracle_setup(oracle_mod, wg, CONFIG1, (1,))
+    L = o.nq
+    b, a = o.uniform(L, 5), o.uniform(L, 6)
+    ob, oa = o.rotate(L - 1, b, a, keys[1], 1)
+    for _ in range(2):
+        db, da = _dev(wg, b), _dev(wg, a)
+        ctx.rotate(L - 1, db, da, 1)
+        assert (_host(wg, db) == ob).all() and (_host(wg, da) == oa).all()
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        ctx.trim()
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] - free0 >= 4 * 8 * L * N
+
+
 @pytest.mark.parametrize("count,nrot", [(16, 4), (64, 16)])
 def test_walsh15_batched_ops(wg, oracle_mod, count, nrot):
     """Config 2: walsh15 chain, ciphertexts at seeded levels 1..12, each mul + relin + rescale +
