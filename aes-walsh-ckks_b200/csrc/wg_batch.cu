@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <optional>
 
 #include "wg_batch.hpp"
 #include "wg_batch_kernels.cuh"
@@ -47,8 +48,10 @@ struct KsPlan {
     int n_combine;
     const GatherJob* gather;
     int n_gather;
+    const NttEpiJob* contrib_epi;  // fused: forward row phase of the contributions + combine
+    int n_contrib_epi;
     double mac_bytes, modup_bytes, moddown_bytes, combine_bytes;
-    bool fused;   // ModUp / ModDown fused with the NTT column phases (Context::ks_fused)
+    bool fused;   // ModUp / ModDown fused with the NTT column phases (Context::ntt_fusion)
     int max_src;  // widest digit (fused ModUp shared memory)
 };
 
@@ -66,8 +69,9 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
     std::vector<ModDownJob> moddown;
     std::vector<CombineJob> combine;
     std::vector<GatherJob> gather;
+    std::vector<NttEpiJob> contrib_epi;
     KsPlan p{};
-    p.fused = c.ks_fused;
+    p.fused = c.ntt_fusion;
     // MAC groups: consecutive switches with the same key, level and digit layout (up to
     // kMacGroup), one job per QP limb; [group_begin, it) is the open group
     size_t group_begin = 0;
@@ -137,17 +141,28 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
         for (int poly = 0; poly < 2; ++poly) {
             moddown.push_back({acc + (poly * T + L) * N, contrib + poly * L * N, c.fold_inv[level],
                                c.fold_inv_s[level], (int)L, 0});
-            for (size_t qi = 0; qi < L; ++qi) {
-                uint64_t* ptr = contrib + (poly * L + qi) * N;
-                ntt_contrib.push_back({ptr, ptr, (int)qi, 0});
-            }
+            if (!p.fused)
+                for (size_t qi = 0; qi < L; ++qi) {
+                    uint64_t* ptr = contrib + (poly * L + qi) * N;
+                    ntt_contrib.push_back({ptr, ptr, (int)qi, 0});
+                }
         }
         p.moddown_bytes += 8.0 * N * 2.0 * (K + L);
         const bool gal = x.galois != 0;
         for (size_t qi = 0; qi < L; ++qi) {
             uint64_t* bo = gal ? acc + T * N : x.b;
             uint64_t* ao = gal ? acc : x.a;
-            combine.push_back({acc, contrib, x.b_in, x.a_in, bo, ao, (int)L, (int)K, (int)qi, x.b_add, x.a_add, 0});
+            if (p.fused) {
+                // a: accumulator poly 0, contribution limbs [0, L); b: poly 1, [L, 2L)
+                contrib_epi.push_back({contrib + qi * N, acc + qi * N, x.a_in ? x.a_in + qi * N : nullptr,
+                                       ao + qi * N, (uint64_t)x.a_add, 0, (int)qi, kEpiCombine});
+                contrib_epi.push_back({contrib + (L + qi) * N, acc + (T + qi) * N,
+                                       x.b_in ? x.b_in + qi * N : nullptr, bo + qi * N, (uint64_t)x.b_add, 0,
+                                       (int)qi, kEpiCombine});
+            } else {
+                combine.push_back(
+                    {acc, contrib, x.b_in, x.a_in, bo, ao, (int)L, (int)K, (int)qi, x.b_add, x.a_add, 0});
+            }
             if (gal)
                 gather.push_back({acc + T * N + qi * N, acc + qi * N, x.b + qi * N, x.a + qi * N, x.galois});
         }
@@ -172,6 +187,8 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
     p.n_combine = (int)combine.size();
     p.gather = t.add(gather);
     p.n_gather = (int)gather.size();
+    p.contrib_epi = t.add(contrib_epi);
+    p.n_contrib_epi = (int)contrib_epi.size();
     return p;
 }
 
@@ -189,11 +206,10 @@ static void run_keyswitch(const Context& c, const KsPlan& p, const JobTable& t, 
         }
         ntt_jobs_phase(c, t.at(p.intt_p), p.n_intt_p, false, false, s);
         moddown_ntt_jobs(c, t.at(p.moddown), p.n_moddown, p.moddown_bytes, s);
-        ntt_jobs_phase(c, t.at(p.ntt_contrib), p.n_ntt_contrib, true, false, s);
-        {
-            Probe probe(kClsCombine, p.combine_bytes, s);
-            kb_combine<<<grid_for(c, p.n_combine), kT, 0, s>>>(t.at(p.combine), p.n_combine, c.d_mod, N);
-            if (p.n_gather) kb_gather<<<grid_for(c, p.n_gather), kT, 0, s>>>(t.at(p.gather), p.n_gather, c.logN);
+        ntt_rows_epilogue_jobs(c, t.at(p.contrib_epi), p.n_contrib_epi, 8.0 * N * p.n_contrib_epi, s);
+        if (p.n_gather) {
+            Probe probe(kClsCombine, 8.0 * N * 4.0 * p.n_gather, s);
+            kb_gather<<<grid_for(c, p.n_gather), kT, 0, s>>>(t.at(p.gather), p.n_gather, c.logN);
         }
         check_cuda(cudaGetLastError(), "batched keyswitch launch");
         return;
@@ -240,14 +256,11 @@ void batch_keyswitch(Context& c, const KsItem* items, size_t n, cudaStream_t s) 
 struct PipelinePlan {
     JobTable t;
     const TensorJob* jt = nullptr;
-    const NttJob* jd = nullptr;
-    const RescalePrepJob* jp = nullptr;
-    const NttJob* jr = nullptr;
-    const RescaleFinishJob* jf = nullptr;
-    int nt = 0, nd = 0, np = 0, nr = 0, nf = 0;
+    int nt = 0;
+    std::optional<RescaleJobs> rescale;
     KsPlan p1{}, p2{};
     bool rotate = false;
-    double tb = 0, pb = 0, fb = 0;
+    double tb = 0;
 };
 
 // Arena: c2 per ciphertext, rescale remainders, then the larger of the two key-switch batches.
@@ -285,9 +298,7 @@ static void plan_pipeline(const Context& c, PipelinePlan& P, size_t count, const
     uint64_t* ksbase = rembase + rem_words;
     std::vector<KsItem> relin_items(count), rot_items;
     std::vector<TensorJob> tensor;
-    std::vector<NttJob> drop_intt, rem_ntt;
-    std::vector<RescalePrepJob> prep;
-    std::vector<RescaleFinishJob> fin;
+    RescaleJobs& rs = P.rescale.emplace(c);
     uint64_t* c2p = c2base;
     uint64_t* remp = rembase;
     for (size_t i = 0; i < count; ++i) {
@@ -306,16 +317,8 @@ static void plan_pipeline(const Context& c, PipelinePlan& P, size_t count, const
         ri.a_add = 1;
         ri.galois = 0;
         c2p += L * N;
-        const uint64_t* rc = c.rs_host.data() + c.rs_host_off[lv];
         for (int poly = 0; poly < 2; ++poly) {
-            uint64_t* x = poly ? xa[i] : xb[i];
-            uint64_t* drop = x + lv * N;
-            drop_intt.push_back({drop, drop, (int)lv, 0});
-            for (size_t q = 0; q < lv; ++q) {
-                prep.push_back({drop, remp + q * N, rc[q], rc[3 * lv + q], (int)lv, (int)q});
-                rem_ntt.push_back({remp + q * N, remp + q * N, (int)q, 0});
-                fin.push_back({x + q * N, remp + q * N, rc[lv + q], rc[2 * lv + q], (int)q, 0});
-            }
+            rs.add(c, poly ? xa[i] : xb[i], lv, remp);
             remp += lv * N;
         }
         if (galois[i]) {
@@ -333,19 +336,10 @@ static void plan_pipeline(const Context& c, PipelinePlan& P, size_t count, const
             rot_items.push_back(it);
         }
         P.tb += 8.0 * N * (lv + 1) * 7.0;
-        P.pb += 8.0 * N * 2.0 * (1.0 + lv);
-        P.fb += 8.0 * N * 2.0 * 3.0 * lv;
     }
     P.jt = P.t.add(tensor);
     P.nt = (int)tensor.size();
-    P.jd = P.t.add(drop_intt);
-    P.nd = (int)drop_intt.size();
-    P.jp = P.t.add(prep);
-    P.np = (int)prep.size();
-    P.jr = P.t.add(rem_ntt);
-    P.nr = (int)rem_ntt.size();
-    P.jf = P.t.add(fin);
-    P.nf = (int)fin.size();
+    rs.plan(P.t);
     P.p1 = plan_keyswitch(c, relin_items.data(), count, ksbase, P.t);
     P.p2 = plan_keyswitch(c, rot_items.data(), rot_items.size(), ksbase, P.t);
     P.rotate = !rot_items.empty();
@@ -358,16 +352,7 @@ static void launch_pipeline(const Context& c, const PipelinePlan& P, cudaStream_
         kb_tensor<<<grid_for(c, P.nt), kT, 0, s>>>(t.at(P.jt), P.nt, c.d_mod);
     }
     run_keyswitch(c, P.p1, t, s);
-    ntt_jobs(c, t.at(P.jd), P.nd, false, s);
-    {
-        Probe probe(kClsElementwise, P.pb, s);
-        kb_rescale_prep<<<grid_for(c, P.np), kT, 0, s>>>(t.at(P.jp), P.np, c.d_mod);
-    }
-    ntt_jobs(c, t.at(P.jr), P.nr, true, s);
-    {
-        Probe probe(kClsElementwise, P.fb, s);
-        kb_rescale_finish<<<grid_for(c, P.nf), kT, 0, s>>>(t.at(P.jf), P.nf, c.d_mod);
-    }
+    P.rescale->run(c, t, s);
     if (P.rotate) run_keyswitch(c, P.p2, t, s);
     check_cuda(cudaGetLastError(), "batched pipeline launch");
 }

@@ -4,6 +4,7 @@
 #pragma once
 #include <algorithm>
 
+#include "wg_batch.hpp"
 #include "wg_internal.hpp"
 #include "wg_keyswitch.cuh"
 
@@ -194,6 +195,80 @@ __global__ void __launch_bounds__(kT) kb_rescale_finish(const RescaleFinishJob* 
 dim3 grid_for(const Context& c, size_t njobs) {
     return dim3((unsigned)(c.N / kT), (unsigned)std::min<size_t>(njobs, 65535), (unsigned)((njobs + 65534) / 65535));
 }
+
+// The launches of one batched rescale (ckks_rescale, src/ckks/operations/arith/ckks_rescale.cpp:
+// 68-148) over polynomials of any levels: add() records a polynomial x at level lv with lv
+// remainder limbs of scratch, plan() puts the job tables into a JobTable, run() launches.
+// With Context::ntt_fusion: the inverse row phase of the dropped limbs, one fused launch
+// (inverse column phase, rounded remainders, forward column phase; k_rescale_ntt) and the
+// forward row phase with the finish step as its epilogue (k_ntt_rows_epi): 3 launches.
+// Without: inverse NTT, kb_rescale_prep, forward NTT, kb_rescale_finish: 6 launches.  Same words.
+struct RescaleJobs {
+    bool fused;
+    size_t N;
+    std::vector<NttJob> drop, rem_ntt;
+    std::vector<RescalePrepJob> prep;
+    std::vector<RescaleFinishJob> fin;
+    std::vector<RescaleNttJob> cols;
+    std::vector<NttEpiJob> rows;
+    double prep_bytes = 0.0, fin_bytes = 0.0;
+    const NttJob *jd = nullptr, *jr = nullptr;
+    const RescalePrepJob* jp = nullptr;
+    const RescaleFinishJob* jf = nullptr;
+    const RescaleNttJob* jc = nullptr;
+    const NttEpiJob* je = nullptr;
+
+    explicit RescaleJobs(const Context& c) : fused(c.ntt_fusion), N(c.N) {}
+    bool empty() const { return drop.empty(); }
+    void add(const Context& c, uint64_t* x, size_t lv, uint64_t* rem) {
+        const uint64_t* rc = c.rs_host.data() + c.rs_host_off[lv];
+        uint64_t* dl = x + lv * N;
+        drop.push_back({dl, dl, (int)lv, 0});
+        if (fused) {
+            cols.push_back({dl, rem, c.rs_one_s[lv], (int)lv, 0});
+            for (size_t q = 0; q < lv; ++q)
+                rows.push_back({rem + q * N, nullptr, x + q * N, x + q * N, rc[lv + q], rc[2 * lv + q], (int)q,
+                                kEpiRescale});
+        } else {
+            for (size_t q = 0; q < lv; ++q) {
+                prep.push_back({dl, rem + q * N, rc[q], rc[3 * lv + q], (int)lv, (int)q});
+                rem_ntt.push_back({rem + q * N, rem + q * N, (int)q, 0});
+                fin.push_back({x + q * N, rem + q * N, rc[lv + q], rc[2 * lv + q], (int)q, 0});
+            }
+        }
+        prep_bytes += 8.0 * N * (1.0 + lv);
+        fin_bytes += 8.0 * N * 3.0 * lv;
+    }
+    void plan(JobTable& t) {
+        jd = t.add(drop);
+        if (fused) {
+            jc = t.add(cols);
+            je = t.add(rows);
+        } else {
+            jp = t.add(prep);
+            jr = t.add(rem_ntt);
+            jf = t.add(fin);
+        }
+    }
+    void run(const Context& c, const JobTable& t, cudaStream_t s) const {
+        if (drop.empty()) return;
+        if (fused) {
+            ntt_jobs_phase(c, t.at(jd), (int)drop.size(), false, false, s);
+            rescale_ntt_jobs(c, t.at(jc), (int)cols.size(), prep_bytes, s);
+            ntt_rows_epilogue_jobs(c, t.at(je), (int)rows.size(), 8.0 * N * rows.size(), s);
+        } else {
+            ntt_jobs(c, t.at(jd), (int)drop.size(), false, s);
+            {
+                Probe probe(kClsElementwise, prep_bytes, s);
+                kb_rescale_prep<<<grid_for(c, prep.size()), kT, 0, s>>>(t.at(jp), (int)prep.size(), c.d_mod);
+            }
+            ntt_jobs(c, t.at(jr), (int)rem_ntt.size(), true, s);
+            Probe probe(kClsElementwise, fin_bytes, s);
+            kb_rescale_finish<<<grid_for(c, fin.size()), kT, 0, s>>>(t.at(jf), (int)fin.size(), c.d_mod);
+        }
+        check_cuda(cudaGetLastError(), "batched rescale launch");
+    }
+};
 
 }  // namespace
 }  // namespace bk

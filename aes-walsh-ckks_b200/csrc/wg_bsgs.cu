@@ -501,24 +501,12 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
             }
         }
     }
-    std::vector<NttJob> drop_intt, rem_ntt;
-    std::vector<RescalePrepJob> prep;
-    std::vector<RescaleFinishJob> fin;
+    RescaleJobs rescale_jobs(c);
     if (st.rescale) {
         if (level == 0) fail(kInvalid, "ckks_rescale: invalid level");
-        const uint64_t* rc = c.rs_host.data() + c.rs_host_off[level];
         for (size_t ci = 0; ci < count; ++ci)
-            for (int poly = 0; poly < 2; ++poly) {
-                uint64_t* x = poly ? a[ci] : b[ci];
-                uint64_t* drop = x + level * N;
-                uint64_t* r = rem + (ci * 2 + poly) * level * N;
-                drop_intt.push_back({drop, drop, (int)level, 0});
-                for (size_t q = 0; q < level; ++q) {
-                    prep.push_back({drop, r + q * N, rc[q], rc[3 * level + q], (int)level, (int)q});
-                    rem_ntt.push_back({r + q * N, r + q * N, (int)q, 0});
-                    fin.push_back({x + q * N, r + q * N, rc[level + q], rc[2 * level + q], (int)q, 0});
-                }
-            }
+            for (int poly = 0; poly < 2; ++poly)
+                rescale_jobs.add(c, poly ? a[ci] : b[ci], level, rem + (ci * 2 + poly) * level * N);
     }
 
     // Baby slot 0 holds (a, b) with zero P limbs: copy Q limbs, clear P limbs.
@@ -551,10 +539,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     const ModDownJob* j_mdp = t.add(md_pair);
     const NttJob* j_ntt_cf = t.add(ntt_cf);
     const SubJob* j_final = t.add(final_sub);
-    const NttJob* j_drop = t.add(drop_intt);
-    const RescalePrepJob* j_prep = t.add(prep);
-    const NttJob* j_rem = t.add(rem_ntt);
-    const RescaleFinishJob* j_fin = t.add(fin);
+    rescale_jobs.plan(t);
     t.upload(c, s);
     // 1.
     ntt_jobs(c, t.at(j_intt_a), (int)intt_a.size(), false, s);
@@ -618,16 +603,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
         Probe probe(kClsElementwise, 8.0 * N * 3.0 * final_sub.size(), s);
         kb_sub<<<grid_for(c, final_sub.size()), kT, 0, s>>>(t.at(j_final), (int)final_sub.size(), c.d_mod);
     }
-    if (st.rescale) {
-        ntt_jobs(c, t.at(j_drop), (int)drop_intt.size(), false, s);
-        {
-            Probe probe(kClsElementwise, 8.0 * N * 2.0 * prep.size(), s);
-            kb_rescale_prep<<<grid_for(c, prep.size()), kT, 0, s>>>(t.at(j_prep), (int)prep.size(), c.d_mod);
-        }
-        ntt_jobs(c, t.at(j_rem), (int)rem_ntt.size(), true, s);
-        Probe probe(kClsElementwise, 8.0 * N * 3.0 * fin.size(), s);
-        kb_rescale_finish<<<grid_for(c, fin.size()), kT, 0, s>>>(t.at(j_fin), (int)fin.size(), c.d_mod);
-    }
+    rescale_jobs.run(c, t, s);
     check_cuda(cudaGetLastError(), "linear transform launch");
 }
 

@@ -231,41 +231,17 @@ public:
     void rescale(CtBatch& x) {
         const size_t N = c_.N, lv = x.level;
         if (lv == 0) throw std::invalid_argument("ckks_rescale: invalid level");
-        uint64_t* rem = scratch(count_ * x.np * lv);
-        const uint64_t* rc = c_.rs_host.data() + c_.rs_host_off[lv];
-        std::vector<NttJob> drop_intt, rem_ntt;
-        std::vector<RescalePrepJob> prep;
-        std::vector<RescaleFinishJob> fin;
-        uint64_t* r = rem;
+        uint64_t* r = scratch(count_ * x.np * lv);
+        RescaleJobs rj(c_);
         for (size_t i = 0; i < count_; ++i)
             for (int k = 0; k < x.np; ++k) {
-                uint64_t* poly = x.p[i][k];
-                uint64_t* drop = poly + lv * N;
-                drop_intt.push_back({drop, drop, (int)lv, 0});
-                for (size_t q = 0; q < lv; ++q) {
-                    prep.push_back({drop, r + q * N, rc[q], rc[3 * lv + q], (int)lv, (int)q});
-                    rem_ntt.push_back({r + q * N, r + q * N, (int)q, 0});
-                    fin.push_back({poly + q * N, r + q * N, rc[lv + q], rc[2 * lv + q], (int)q, 0});
-                }
+                rj.add(c_, x.p[i][k], lv, r);
                 r += lv * N;
             }
         JobTable t;
-        const NttJob* jd = t.add(drop_intt);
-        const RescalePrepJob* jp = t.add(prep);
-        const NttJob* jr = t.add(rem_ntt);
-        const RescaleFinishJob* jf = t.add(fin);
+        rj.plan(t);
         t.upload(c_, s_);
-        ntt_jobs(c_, t.at(jd), (int)drop_intt.size(), false, s_);
-        {
-            Probe probe(kClsElementwise, 8.0 * N * prep.size() * 2.0, s_);
-            kb_rescale_prep<<<grid_for(c_, prep.size()), kT, 0, s_>>>(t.at(jp), (int)prep.size(), c_.d_mod);
-        }
-        ntt_jobs(c_, t.at(jr), (int)rem_ntt.size(), true, s_);
-        {
-            Probe probe(kClsElementwise, 8.0 * N * fin.size() * 3.0, s_);
-            kb_rescale_finish<<<grid_for(c_, fin.size()), kT, 0, s_>>>(t.at(jf), (int)fin.size(), c_.d_mod);
-        }
-        check_cuda(cudaGetLastError(), "evalpoly rescale");
+        rj.run(c_, t, s_);
         x.scale = x.scale / static_cast<long double>(c_.q[lv]);
         x.level = lv - 1;
     }

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "wg_arith.cuh"
+#include "wg_ntt.cuh"
 
 namespace wg {
 
@@ -141,9 +142,10 @@ struct Context {
     Modulus* d_mod = nullptr;
     uint64_t* d_tw = nullptr;        // [mod][2][N] (w, Shoup w) pairs: forward, inverse (ntt::TwPair)
     int ntt_variant[2][2] = {{0, 0}, {0, 0}};  // NTT geometry per [direction][phase: rows, columns]
-    // key switches run ModUp and ModDown fused with the adjacent NTT column phases
-    // (wg_ksfuse.cu); false: the separate launches (same words)
-    bool ks_fused = true;
+    // key switches and rescales run their base changes fused with the adjacent NTT column
+    // phases and their final element-wise steps in the last row phase's epilogue
+    // (wg_ksfuse.cu, k_ntt_rows_epi); false: the separate launches (same words)
+    bool ntt_fusion = true;
     NttTuning tuning{};
     // ModUp descriptors, host copies holding device pointers: [level][part]
     std::vector<std::vector<ModUpDesc>> modup;
@@ -296,6 +298,24 @@ struct ModDownNttJob {
     int L;
     int pad;
 };
+// Rescale of one polynomial at level lv (ckks_rescale): drop holds its last limb after the
+// inverse row phase; the kernel finishes that inverse transform, forms the rounded remainder
+// for every lower limb and writes it to rem (lv limbs) after the forward column phase.  rc: the
+// device rescale constants of level lv (one_s, inv_p, inv_p_s, half; lv words each).
+struct RescaleNttJob {
+    const uint64_t* drop;
+    uint64_t* rem;
+    const uint64_t* rc;
+    int lv;
+    int pad;
+};
+// The forward row phase of job-table limbs with an element-wise epilogue (NttEpiJob, wg_ntt.cuh).
+using ntt::NttEpiJob;
+using ntt::kEpiRescale;
+using ntt::kEpiCombine;
+void ntt_rows_epilogue_jobs(const Context& c, const NttEpiJob* d_jobs, int njobs, double bytes, cudaStream_t s);
+void rescale_ntt_jobs(const Context& c, const RescaleNttJob* d_jobs, int njobs, double bytes, cudaStream_t s);
+
 // max_src: the largest source-limb count of the jobs (shared-memory size).
 void modup_ntt_jobs(const Context& c, const ModUpNttJob* d_jobs, int njobs, int max_src, double bytes,
                     cudaStream_t s);

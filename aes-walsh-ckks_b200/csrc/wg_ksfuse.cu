@@ -1,4 +1,5 @@
-// Key-switch ModUp and ModDown fused with the NTT column phases around them.
+// Key-switch ModUp and ModDown, and the rescale's remainder step, fused with the NTT column
+// phases around them.
 //
 // Unfused, a hybrid key switch (ckks_hybrid_key_switch_inplace,
 // src/ckks/operations/keyswitch/ckks_keyswitch.cpp:1330-1641) moves every intermediate limb
@@ -123,6 +124,40 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
     }
 }
 
+// Block (tile, job): one polynomial's column tile of a rescale.
+template <int LOGN>
+__global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
+    k_rescale_ntt(const RescaleNttJob* __restrict__ jobs, int njobs, const Modulus* __restrict__ mods,
+                  const TwPair* __restrict__ tw_base) {
+    using G = Geom<LOGN>;
+    const int j = blockIdx.y + 65535 * blockIdx.z;
+    if (j >= njobs) return;
+    extern __shared__ __align__(16) uint64_t smem[];
+    const RescaleNttJob job = jobs[j];
+    const int tile = blockIdx.x, t = threadIdx.x, lv = job.lv;
+    uint64_t* drop = smem;
+    uint64_t* work = smem + G::PAD;
+    const Modulus mp = mods[lv];
+    load_tile<LOGN>(drop, job.drop, tile, t);
+    __syncthreads();
+    inverse_cols<LOGN>(drop, tile, t, mp, tw_base + (size_t)lv * 2 * G::N + G::N);
+    for (int qi = 0; qi < lv; ++qi) {
+        const uint64_t q = mods[qi].q;
+        rescale_value<LOGN>(work, drop, t, mp.q, q, __ldg(job.rc + qi), __ldg(job.rc + 3 * lv + qi));
+        __syncthreads();
+        forward_cols<LOGN>(work, tile, t, q, tw_base + (size_t)qi * 2 * G::N);
+        store_tile<LOGN>(work, job.rem + (size_t)qi * G::N, tile, t);
+    }
+}
+
+template <int LOGN>
+void launch_rescale(const Context& c, const RescaleNttJob* jobs, int njobs, cudaStream_t s) {
+    using G = Geom<LOGN>;
+    const dim3 grid(G::TILES, njobs < 65535 ? njobs : 65535, (njobs + 65534) / 65535);
+    k_rescale_ntt<LOGN><<<grid, G::THREADS, fused_smem<LOGN>(1), s>>>(jobs, njobs, c.d_mod,
+                                                                      reinterpret_cast<const TwPair*>(c.d_tw));
+}
+
 template <int LOGN>
 void launch_modup(const Context& c, const ModUpNttJob* jobs, int njobs, int max_src, cudaStream_t s) {
     using G = Geom<LOGN>;
@@ -169,6 +204,22 @@ void modup_ntt_jobs(const Context& c, const ModUpNttJob* d_jobs, int njobs, int 
         default: fail(kInvalid, "fused modup: ring degree must be 2^10 .. 2^16");
     }
     check_cuda(cudaGetLastError(), "fused modup launch");
+}
+
+void rescale_ntt_jobs(const Context& c, const RescaleNttJob* d_jobs, int njobs, double bytes, cudaStream_t s) {
+    if (njobs <= 0) return;
+    Probe probe(kClsElementwise, bytes, s);
+    switch (c.logN) {
+        case 10: launch_rescale<10>(c, d_jobs, njobs, s); break;
+        case 11: launch_rescale<11>(c, d_jobs, njobs, s); break;
+        case 12: launch_rescale<12>(c, d_jobs, njobs, s); break;
+        case 13: launch_rescale<13>(c, d_jobs, njobs, s); break;
+        case 14: launch_rescale<14>(c, d_jobs, njobs, s); break;
+        case 15: launch_rescale<15>(c, d_jobs, njobs, s); break;
+        case 16: launch_rescale<16>(c, d_jobs, njobs, s); break;
+        default: fail(kInvalid, "fused rescale: ring degree must be 2^10 .. 2^16");
+    }
+    check_cuda(cudaGetLastError(), "fused rescale launch");
 }
 
 void moddown_ntt_jobs(const Context& c, const ModDownNttJob* d_jobs, int njobs, double bytes, cudaStream_t s) {

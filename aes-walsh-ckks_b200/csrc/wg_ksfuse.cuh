@@ -1,7 +1,7 @@
-// Per-thread steps of the fused key-switch kernels (wg_ksfuse.cu), shared with the CPU
+// Per-thread steps of the fused key-switch and rescale kernels (wg_ksfuse.cu), shared with the CPU
 // emulation test, which runs them thread by thread between the same barriers.
 //
-// Both fused kernels work on one column tile of the two-phase NTT (wg_ntt.cu): the TILE
+// The fused kernels work on one column tile of the two-phase NTT (wg_ntt.cu): the TILE
 // coefficients {(h << NB2) + tile * SUBS + c : h < 2^NB1, c < SUBS}, i.e. SUBS whole columns.
 // The inverse transform ends with the column phase and the forward transform starts with it,
 // and both phases cover exactly these coefficients, so a CTA can finish the inverse transform
@@ -14,7 +14,10 @@
 //            forward column phase of every destination limb;
 //   ModDown: inverse column phase of the K P limbs of one accumulator, N^-1 scaling, the folded
 //            ModDown of moddown_all_limbs (ckks_apply_folded_approx_crt_moddown_pair_eval_q,
-//            ckks_keyswitch.cpp:521-607), then the forward column phase of every Q limb.
+//            ckks_keyswitch.cpp:521-607), then the forward column phase of every Q limb;
+//   Rescale: inverse column phase of the dropped limb, N^-1 scaling, the rounded remainder
+//            for every lower limb, then the forward column phase of each remainder (the row
+//            phase that follows finishes the rescale in its epilogue, k_ntt_rows_epi).
 //
 // The butterflies, reductions and FP64 sums are those of the unfused kernels in the same
 // order, so the words written equal the ones the separate launches write.  Thread t owns tile
@@ -169,6 +172,22 @@ WG_HD void moddown_value(uint64_t* work, const uint64_t* p_tiles, int t, const M
             acc = add_mod(acc, mul_shoup(s, WG_LDG(iv + pi), WG_LDG(ivs + pi), q), q);
         }
         work[pe] = sub_mod(acc, (uint64_t)hps[k], q);
+    }
+}
+
+// Rescale: thread t's rounded remainders of the dropped limb (coefficients in drop, canonical,
+// modulus p) for target limb q into the work tile, as kb_rescale_prep forms them
+// (ckks_rescale, src/ckks/operations/arith/ckks_rescale.cpp:68-148).
+template <int LOGN>
+WG_HD void rescale_value(uint64_t* work, const uint64_t* drop, int t, uint64_t p, uint64_t q, uint64_t one_s,
+                         uint64_t half) {
+    using G = Geom<LOGN>;
+#pragma unroll
+    for (int k = 0; k < G::E; ++k) {
+        const int pe = ntt::pad16(t + k * G::THREADS);
+        uint64_t shift = drop[pe] + (p >> 1);
+        if (shift >= p) shift -= p;
+        work[pe] = sub_mod(reduce_shoup(shift, q, one_s), half, q);
     }
 }
 

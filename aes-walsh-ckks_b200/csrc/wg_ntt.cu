@@ -139,6 +139,87 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS, EB, STAGED>::THREADS, m
     }
 }
 
+// The forward row phase of one job-table limb with an element-wise epilogue (NttEpiJob): the
+// same rounds and final reduction as k_ntt_phase<LOGN, true, false, ...>, then
+// ntt_epilogue(v) in place of the store.
+template <int LOGN, int EB, bool STAGED>
+__global__ void __launch_bounds__(Phase<LOGN, true, false, EB, STAGED>::THREADS, min_blocks<EB>())
+    k_ntt_rows_epi(const NttEpiJob* __restrict__ jobs, int njobs, const Modulus* __restrict__ mods,
+                   const TwPair* __restrict__ tw_base) {
+    using P = Phase<LOGN, true, false, EB, STAGED>;
+    constexpr int N = P::N;
+    constexpr int E = P::E;
+    extern __shared__ __align__(16) uint64_t smem[];
+    uint64_t* sm = smem;
+    TwPair* tw_s = reinterpret_cast<TwPair*>(smem + P::TILE + P::TILE / 16);
+    const int j = blockIdx.y + 65535 * blockIdx.z;
+    if (j >= njobs) return;
+    const NttEpiJob job = jobs[j];
+    const int mi = job.mod;
+    const Modulus m = mods[mi];
+    const TwPair* tw = tw_base + (size_t)mi * 2 * N;
+    const int tile = blockIdx.x;
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        const int e = t + k * P::THREADS;
+        sm[pad16(e)] = job.data[tile_offset<LOGN, true, false, EB, STAGED>(tile, e)];
+    }
+    if (STAGED) {
+        const ulonglong2* src2 = reinterpret_cast<const ulonglong2*>(tw);
+        ulonglong2* dst2 = reinterpret_cast<ulonglong2*>(tw_s);
+#pragma unroll
+        for (int k = 0; k < P::MB; ++k) {
+            const int cnt = P::SUBS << k;
+            const int dst = P::SUBS * ((1 << k) - 1);
+            const size_t src = ((size_t)1 << (P::NB1 + k)) + (size_t)tile * cnt;
+            for (int e = t; e < cnt; e += P::THREADS) dst2[dst + e] = __ldg(src2 + src + e);
+        }
+    }
+    __syncthreads();
+    const int sub = t >> P::OB;
+    const int o = t & ((1 << P::OB) - 1);
+    const TwPair* twr = STAGED ? tw_s : tw;
+    const bool lazy = m.q < kLazyForwardLimit;
+    if (lazy)
+        ntt_rounds<LOGN, true, false, EB, STAGED, true>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o, tile,
+                                                       m.q, twr);
+    else
+        ntt_rounds<LOGN, true, false, EB, STAGED, false>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o,
+                                                        tile, m.q, twr);
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        const int e = t + k * P::THREADS;
+        const uint64_t raw = sm[pad16(e)];
+        const uint64_t v = lazy ? reduce64(raw, m) : red4q(raw, m.q);
+        ntt_epilogue(job, tile_offset<LOGN, true, false, EB, STAGED>(tile, e), v, m.q);
+    }
+}
+
+template <int LOGN, int EB, bool STAGED>
+void launch_rows_epi(const Context& c, const NttEpiJob* jobs, int njobs, cudaStream_t s) {
+    using P = Phase<LOGN, true, false, EB, STAGED>;
+    constexpr size_t sm = smem_bytes<LOGN, true, false, EB, STAGED>();
+    static const bool opted = [] {
+        cudaFuncSetAttribute(k_ntt_rows_epi<LOGN, EB, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        return true;
+    }();
+    (void)opted;
+    const dim3 grid(P::N / P::TILE, njobs < 65535 ? njobs : 65535, (njobs + 65534) / 65535);
+    k_ntt_rows_epi<LOGN, EB, STAGED><<<grid, P::THREADS, sm, s>>>(jobs, njobs, c.d_mod,
+                                                                  reinterpret_cast<const TwPair*>(c.d_tw));
+}
+
+template <int LOGN>
+void rows_epi_variant(const Context& c, int variant, const NttEpiJob* jobs, int njobs, cudaStream_t s) {
+    switch (variant) {
+        case 0: launch_rows_epi<LOGN, 3, true>(c, jobs, njobs, s); break;
+        case 1: launch_rows_epi<LOGN, 3, false>(c, jobs, njobs, s); break;
+        case 2: launch_rows_epi<LOGN, 4, true>(c, jobs, njobs, s); break;
+        default: launch_rows_epi<LOGN, 4, false>(c, jobs, njobs, s); break;
+    }
+}
+
 template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, bool TABLE>
 void enable_smem() {
     // opt in to more than 48 KiB of dynamic shared memory once per kernel instance
@@ -254,6 +335,25 @@ void ntt_jobs_phase(const Context& c, const NttJob* d_jobs, int njobs, bool forw
     phase_dispatch(c, forward, cols, c.ntt_variant[forward ? 0 : 1][cols ? 1 : 0], nullptr, 0, 0, 0, LimbMap{0, 0, 0},
                    d_jobs, njobs, s);
     check_cuda(cudaGetLastError(), "ntt launch");
+}
+
+void ntt_rows_epilogue_jobs(const Context& c, const NttEpiJob* d_jobs, int njobs, double bytes, cudaStream_t s) {
+    if (njobs <= 0) return;
+    // booked as NTT work at the caller's bytes (the phase's own 8 N B per limb); the epilogue's
+    // reads replace the separate element-wise launch
+    Probe probe(kClsNtt, bytes, s);
+    const int v = c.ntt_variant[0][0];
+    switch (c.logN) {
+        case 10: rows_epi_variant<10>(c, v, d_jobs, njobs, s); break;
+        case 11: rows_epi_variant<11>(c, v, d_jobs, njobs, s); break;
+        case 12: rows_epi_variant<12>(c, v, d_jobs, njobs, s); break;
+        case 13: rows_epi_variant<13>(c, v, d_jobs, njobs, s); break;
+        case 14: rows_epi_variant<14>(c, v, d_jobs, njobs, s); break;
+        case 15: rows_epi_variant<15>(c, v, d_jobs, njobs, s); break;
+        case 16: rows_epi_variant<16>(c, v, d_jobs, njobs, s); break;
+        default: fail(kInvalid, "ntt: ring degree must be 2^10 .. 2^16");
+    }
+    check_cuda(cudaGetLastError(), "ntt epilogue launch");
 }
 
 void ntt_phase_geometry(const Context& c, bool forward, bool cols, int variant, uint64_t* data, int limbs, int polys,

@@ -201,6 +201,35 @@ WG_HD void ntt_round(uint64_t* sm, int sub, int o, int tile, uint64_t q, const T
     }
 }
 
+// The forward row phase of one limb (data: after the forward column phase, read only) with an
+// element-wise epilogue on the finished canonical words v instead of storing them:
+//   kEpiRescale: out = (in - v) * p^-1 mod q  (in reduced below q first; c0, c1 = p^-1 and its
+//                Shoup constant: the rescale finish step, as kb_rescale_finish);
+//   kEpiCombine: out = c0 ? in + (acc - v) : acc - v  (the key switch's final combine, as
+//                combine_coeff).
+// out may alias in or acc (each word is read and written by the same thread).
+enum NttEpilogue : int { kEpiRescale = 1, kEpiCombine = 2 };
+struct NttEpiJob {
+    const uint64_t* data;
+    const uint64_t* acc;
+    const uint64_t* in;
+    uint64_t* out;
+    uint64_t c0, c1;
+    int mod;
+    int kind;
+};
+
+WG_HD void ntt_epilogue(const NttEpiJob& j, size_t off, uint64_t v, uint64_t q) {
+    if (j.kind == kEpiRescale) {
+        uint64_t x = j.in[off];
+        if (x >= q) x -= q;
+        j.out[off] = mul_shoup(sub_mod(x, v, q), j.c0, j.c1, q);
+    } else {
+        const uint64_t d = sub_mod(j.acc[off], v, q);
+        j.out[off] = j.c0 ? add_mod(j.in[off], d, q) : d;
+    }
+}
+
 // Global offset (within one limb) of tile element e.
 template <int LOGN, bool FWD, bool COLS, int EB, bool STAGED, int TL = kMaxTile>
 WG_HD size_t tile_offset(int tile, int e) {

@@ -85,7 +85,7 @@ def lib() -> C.CDLL:
         L.wg_lt_stage_info.argtypes = [vp] * 7
         L.wg_lt_stage_download.argtypes = [vp, vp, vp, vp]
         L.wg_ntt_set_geometry.argtypes = [vp, C.c_int, C.c_int, C.c_int]
-        L.wg_set_keyswitch_fusion.argtypes = [vp, C.c_int]
+        L.wg_set_ntt_fusion.argtypes = [vp, C.c_int]
         L.wg_keyswitch.argtypes = [vp, sz, vp, C.c_int, C.c_int64, vp, vp, C.c_int, C.c_int, vp]
         L.wg_rotate.argtypes = [vp, sz, vp, vp, C.c_int64, vp]
         L.wg_rotate_noalloc.argtypes = [vp, sz, vp, vp, C.c_int64, vp]
@@ -671,10 +671,11 @@ class Context:
         the tuned choice."""
         _check(lib().wg_ntt_set_geometry(self.h, int(direction), int(phase), int(geometry)))
 
-    def set_keyswitch_fusion(self, fused):
-        """Batched key switches with ModUp / ModDown fused into the NTT column phases (default)
-        or as separate launches; the words are the same."""
-        _check(lib().wg_set_keyswitch_fusion(self.h, int(bool(fused))))
+    def set_ntt_fusion(self, fused):
+        """Batched key switches and rescales with their base changes fused into the NTT column
+        phases and their last element-wise steps into the row-phase epilogue (default), or as
+        separate launches; the words are the same."""
+        _check(lib().wg_set_ntt_fusion(self.h, int(bool(fused))))
 
     def keyswitch(self, level, key_term, kind, b, a, b_add=True, a_add=False, rotation=0, stream=None):
         _check(lib().wg_keyswitch(self.h, level, _ptr(key_term), kind, int(rotation), _ptr(b), _ptr(a),

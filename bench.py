@@ -395,10 +395,10 @@ def ops_bench(args, wg, torch, stream, timed, rank, local, with_cpu=False):
         nograph_step()
     nograph_ms = timed(nograph_step, steps)
     # the same batched call with ModUp / ModDown as separate launches (no NTT column fusion)
-    ctx.set_keyswitch_fusion(False)
+    ctx.set_ntt_fusion(False)
     nograph_step()
     unfused_ms = timed(nograph_step, steps)
-    ctx.set_keyswitch_fusion(True)
+    ctx.set_ntt_fusion(True)
     plain_step()
     l0 = wg.launch_count()
     plain_ms = timed(plain_step, max(1, steps // 2))
@@ -1286,14 +1286,15 @@ def main():
     # the same evaluation with the key switches' ModUp / ModDown as separate launches
     aes_unfused = None
     if not args.no_plain:
-        aes.ctx.set_keyswitch_fusion(False)
+        aes.ctx.set_ntt_fusion(False)
         aes_step()
         unfused_ms = timed(aes_step, max(1, args.steps // 4))
-        aes.ctx.set_keyswitch_fusion(True)
+        aes.ctx.set_ntt_fusion(True)
         aes_unfused = {"value": aes.blocks * world / (unfused_ms / 1000.0), "unit": UNIT,
                        "ms_per_step": unfused_ms, "fused_speedup": unfused_ms / ms,
-                       "path": "wg_aes_ctr_walsh with ModUp and ModDown as separate launches from the NTT "
-                               "column phases (wg_set_keyswitch_fusion 0)"}
+                       "path": "wg_aes_ctr_walsh with ModUp, ModDown, the rescale remainders, the combine "
+                               "and the rescale finish as separate launches from the NTT phases "
+                               "(wg_set_ntt_fusion 0)"}
 
     # end to end: the same call from host block bytes, plus the read-back of the 128 output
     # bit ciphertexts into pinned host memory, every step

@@ -152,13 +152,16 @@ int wg_ntt_tuning(const wg_context* ctx, int* chosen, float* ms, int* limbs);
 /* Pin the geometry of one (direction, phase) for this context (geometry < 0: restore the
  * tuned choice). */
 int wg_ntt_set_geometry(wg_context* ctx, int direction, int phase, int geometry);
-/* Batched key switches (every circuit entry point) run ModUp and ModDown inside the NTT column
- * phases around them by default: one kernel finishes the inverse transform of the source limbs,
- * changes the basis and starts the forward transform of every output limb, so those limbs do
- * not pass through device memory in between (ckks_hybrid_key_switch_inplace,
- * src/ckks/operations/keyswitch/ckks_keyswitch.cpp:1330-1641, computes the same words step by
- * step).  fused = 0 selects the separate launches, for comparison; the words are identical. */
-int wg_set_keyswitch_fusion(wg_context* ctx, int fused);
+/* Batched key switches and rescales (every circuit entry point) run their base changes inside
+ * the NTT column phases around them by default: one kernel finishes the inverse transform of the
+ * source limbs, changes the basis (ModUp, ModDown, the rescale's rounded remainders) and starts
+ * the forward transform of every output limb, so those limbs do not pass through device memory
+ * in between; the final combine of a key switch and the rescale's finish step run as the
+ * epilogue of the last forward row phase.  ckks_hybrid_key_switch_inplace
+ * (src/ckks/operations/keyswitch/ckks_keyswitch.cpp:1330-1641) and ckks_rescale
+ * (src/ckks/operations/arith/ckks_rescale.cpp:68-148) compute the same words step by step.
+ * fused = 0 selects the separate launches, for comparison; the words are identical. */
+int wg_set_ntt_fusion(wg_context* ctx, int fused);
 
 /* Hybrid key switch of key_term at `level` with the installed key (kind, rotation):
  * b = (b_add ? b + ks_b : ks_b), a = (a_add ? a + ks_a : ks_a).  key_term may alias a.

@@ -122,7 +122,7 @@ void ntt_one(const Emu& E, uint64_t* x, int mi, bool fwd) {
     }
 }
 
-// Key switches run the fused ModUp / ModDown sequence of wg_ksfuse.cu (Context::ks_fused).
+// Key switches and rescales run the fused sequences of wg_ksfuse.cu (Context::ntt_fusion).
 int g_fused = 0;
 
 template <int LOGN, bool FWD, bool LAZY, int... RD>
@@ -209,6 +209,37 @@ void moddown_fused(const Emu& E, const uint64_t* src_p, uint64_t* out, int L, co
                                          inv_s + (size_t)qi * K, hps.data() + (size_t)t * G::E);
             forward_cols<LOGN>(E, work, tile, qi);
             for (int t = 0; t < G::THREADS; ++t) ksf::store_tile<LOGN>(work, out + (size_t)qi * G::N, tile, t);
+        }
+    }
+}
+
+// k_ntt_rows_epi for one job: the forward row phase of a copy of the job's limb (the kernel
+// reads it and stores nothing back) with the emulated geometry, then the epilogue per word.
+template <int LOGN>
+void rows_epi(const Emu& E, const ntt::NttEpiJob& j) {
+    const size_t N = (size_t)1 << LOGN;
+    std::vector<uint64_t> v(j.data, j.data + N);
+    phase_geom<LOGN, true, false>(E, v.data(), j.mod);
+    for (size_t off = 0; off < N; ++off) ntt::ntt_epilogue(j, off, v[off], E.H.mods[j.mod].q);
+}
+
+// k_rescale_ntt over every column tile of one polynomial (dropped limb after the inverse row
+// phase); rc: the rescale constants of level lv (one_s, inv_p, inv_p_s, half).
+template <int LOGN>
+void rescale_fused(const Emu& E, const uint64_t* drop, uint64_t* rem, int lv, const uint64_t* rc) {
+    using G = ksf::Geom<LOGN>;
+    std::vector<uint64_t> smem((size_t)2 * G::PAD);
+    uint64_t* dl = smem.data();
+    uint64_t* work = smem.data() + G::PAD;
+    const uint64_t p = E.H.mods[lv].q;
+    for (int tile = 0; tile < G::TILES; ++tile) {
+        for (int t = 0; t < G::THREADS; ++t) ksf::load_tile<LOGN>(dl, drop, tile, t);
+        inverse_cols<LOGN>(E, dl, tile, lv);
+        for (int qi = 0; qi < lv; ++qi) {
+            for (int t = 0; t < G::THREADS; ++t)
+                ksf::rescale_value<LOGN>(work, dl, t, p, E.H.mods[qi].q, rc[qi], rc[3 * lv + qi]);
+            forward_cols<LOGN>(E, work, tile, qi);
+            for (int t = 0; t < G::THREADS; ++t) ksf::store_tile<LOGN>(work, rem + (size_t)qi * G::N, tile, t);
         }
     }
 }
@@ -329,9 +360,25 @@ void emu_keyswitch(void* h, size_t level, const uint64_t* key_term, const uint64
         for (int poly = 0; poly < 2; ++poly)
             EMU_LOGN_SWITCH(E.logN, moddown_fused<LG>(E, acc + (poly * T + L) * N, contrib + poly * L * N, (int)L,
                                                       W + E.H.fold_inv[level], W + E.H.fold_inv_s[level]));
-        for (int poly = 0; poly < 2; ++poly)
+        // forward row phase of the contributions with the combine as its epilogue (outputs over
+        // the accumulators' Q limbs when an automorphism follows)
+        const bool gal = galois != 0;
+        for (size_t qi = 0; qi < L; ++qi) {
+            const ntt::NttEpiJob ja{contrib + qi * N, acc + qi * N, a + qi * N, (gal ? acc : a) + qi * N,
+                                    (uint64_t)a_add, 0, (int)qi, ntt::kEpiCombine};
+            const ntt::NttEpiJob jb{contrib + (L + qi) * N, acc + (T + qi) * N, b + qi * N,
+                                    (gal ? acc + T * N : b) + qi * N, (uint64_t)b_add, 0, (int)qi, ntt::kEpiCombine};
+            EMU_LOGN_SWITCH(E.logN, rows_epi<LG>(E, ja));
+            EMU_LOGN_SWITCH(E.logN, rows_epi<LG>(E, jb));
+        }
+        if (gal)
             for (size_t qi = 0; qi < L; ++qi)
-                EMU_LOGN_SWITCH(E.logN, phase_one<LG>(E, contrib + (poly * L + qi) * N, (int)qi, true, false));
+                for (uint32_t i = 0; i < N; ++i) {
+                    const uint32_t s = automorphism_src(i, galois, E.logN);
+                    b[qi * N + i] = acc[(T + qi) * N + s];
+                    a[qi * N + i] = acc[qi * N + s];
+                }
+        return;
     } else {
         for (int poly = 0; poly < 2; ++poly)
             for (size_t pi = 0; pi < K; ++pi) ntt_one(E, acc + (poly * T + L + pi) * N, (int)(nq + pi), false);
@@ -358,6 +405,43 @@ void emu_keyswitch(void* h, size_t level, const uint64_t* key_term, const uint64
                 b[qi * N + i] = tb[qi * N + s];
                 a[qi * N + i] = ta[qi * N + s];
             }
+    }
+}
+
+// The device rescale sequence (wg_batch_kernels.cuh RescaleJobs) on one polynomial at level lv:
+// x holds lv + 1 limbs; afterwards its first lv limbs are the rescaled polynomial.
+void emu_rescale(void* h, size_t lv, uint64_t* x) {
+    const Emu& E = *static_cast<Emu*>(h);
+    const size_t N = E.H.N;
+    const uint64_t* rc = E.H.words.data() + E.H.rescale[lv];
+    std::vector<uint64_t> rem(lv * N);
+    uint64_t* dl = x + lv * N;
+    if (g_fused) {
+        EMU_LOGN_SWITCH(E.logN, phase_one<LG>(E, dl, (int)lv, false, false));
+        EMU_LOGN_SWITCH(E.logN, rescale_fused<LG>(E, dl, rem.data(), (int)lv, rc));
+        for (size_t q = 0; q < lv; ++q) {
+            const ntt::NttEpiJob j{rem.data() + q * N, nullptr, x + q * N, x + q * N, rc[lv + q], rc[2 * lv + q],
+                                   (int)q, ntt::kEpiRescale};
+            EMU_LOGN_SWITCH(E.logN, rows_epi<LG>(E, j));
+        }
+        return;
+    }
+    ntt_one(E, dl, (int)lv, false);
+    const Modulus& mp = E.H.mods[lv];
+    for (size_t q = 0; q < lv; ++q) {
+        const Modulus& mq = E.H.mods[q];
+        uint64_t* r = rem.data() + q * N;
+        for (size_t k = 0; k < N; ++k) {  // kb_rescale_prep
+            uint64_t shift = dl[k] + (mp.q >> 1);
+            if (shift >= mp.q) shift -= mp.q;
+            r[k] = sub_mod(reduce_shoup(shift, mq.q, rc[q]), rc[3 * lv + q], mq.q);
+        }
+        ntt_one(E, r, (int)q, true);
+        for (size_t k = 0; k < N; ++k) {  // kb_rescale_finish
+            uint64_t v = x[q * N + k];
+            if (v >= mq.q) v -= mq.q;
+            x[q * N + k] = mul_shoup(sub_mod(v, r[k], mq.q), rc[lv + q], rc[2 * lv + q], mq.q);
+        }
     }
 }
 

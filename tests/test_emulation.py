@@ -32,6 +32,7 @@ def emu(tmp_path_factory):
     E.emu_ntt.argtypes = [C.c_void_p, u64p, C.c_size_t, C.c_size_t, C.c_int, C.c_int]
     E.emu_set_ntt_geometry.argtypes = [C.c_int]
     E.emu_set_keyswitch_fusion.argtypes = [C.c_int]
+    E.emu_rescale.argtypes = [C.c_void_p, C.c_size_t, u64p]
     E.emu_keyswitch.argtypes = [C.c_void_p, C.c_size_t, u64p, u64p, C.c_size_t, u64p, u64p, C.c_int, C.c_int,
                                 C.c_uint64]
     return E
@@ -40,9 +41,10 @@ def emu(tmp_path_factory):
 @pytest.mark.parametrize("fused", [0, 1])
 @pytest.mark.parametrize("prm", SMALL)
 def test_emulated_kernels_match_oracle(oracle_mod, emu, prm, fused):
-    """NTT and key switch (rotation, relinearisation) at three levels; fused = 1 runs the key
-    switch as the device does by default: ModUp and ModDown inside the NTT column phases
-    (wg_ksfuse.cuh), the row phases as separate passes."""
+    """NTT, key switch (rotation, relinearisation) and rescale at three levels; fused = 1 runs
+    them as the device does by default: ModUp, ModDown and the rescale remainders inside the NTT
+    column phases (wg_ksfuse.cuh), the combine and the rescale finish as the epilogue of the last
+    row phase."""
     O = oracle_mod
     N = 1 << prm["logN"]
     p, q = O.find_primes(prm["p_bits"], prm["q_bits"], N)
@@ -77,6 +79,11 @@ def test_emulated_kernels_match_oracle(oracle_mod, emu, prm, fused):
             e0, e1 = b.copy(), a.copy()
             emu.emu_keyswitch(h, level, c2, rl, L - 1, e0, e1, 1, 1, 0)
             assert (e0 == r0).all() and (e1 == r1).all()
+            if level > 0:
+                (os0,) = o.rescale(level, [r0])
+                xs = r0.copy()
+                emu.emu_rescale(h, level, xs)
+                assert (xs[: level * N] == os0).all()
     finally:
         emu.emu_set_keyswitch_fusion(0)
         emu.emu_destroy(h)

@@ -235,11 +235,11 @@ def test_walsh15_batched_ops(wg, oracle_mod, count, nrot):
                                        plain=True)
     assert (_host(wg, pxb) == gb).all() and (_host(wg, pxa) == ga).all()
     # ModUp / ModDown as separate launches instead of inside the NTT column phases: same residues
-    ctx.set_keyswitch_fusion(False)
+    ctx.set_ntt_fusion(False)
     uxb, uxa = _dev(wg, xb), _dev(wg, xa)
     ctx.batch_mul_relin_rescale_rotate(levels, [sl(uxb, i) for i in range(count)], [sl(uxa, i) for i in range(count)],
                                        [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots)
-    ctx.set_keyswitch_fusion(True)
+    ctx.set_ntt_fusion(True)
     assert (_host(wg, uxb) == gb).all() and (_host(wg, uxa) == ga).all()
     # the graph-captured plan over its own buffers: same residues, replayable
     gxb, gxa = _dev(wg, xb), _dev(wg, xa)
