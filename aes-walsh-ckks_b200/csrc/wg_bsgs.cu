@@ -393,6 +393,9 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
 
     JobTable t;
     // 1. hoist
+    const bool fused = c.ntt_fusion;
+    int max_src = 1;
+    for (size_t j = 0; j < B; ++j) max_src = std::max(max_src, c.modup[level][j].src_count);
     std::vector<NttJob> intt_a, ntt_dig;
     std::vector<ModUpJob> modup;
     for (size_t ci = 0; ci < count; ++ci) {
@@ -442,6 +445,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     }
     // 4. giants >= 1: single ModDown of inner a, then QP key switch from that key term
     std::vector<NttJob> intt_pg, ntt_cs, intt_kt, ntt_dig2;
+    std::vector<NttEpiJob> cs_epi, cf_epi;
     std::vector<ModDownJob> md_single;
     std::vector<SubJob> kt_sub;
     std::vector<ModUpJob> modup2;
@@ -458,8 +462,13 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
             }
             md_single.push_back({in_a + L * N, cs, c.fold_inv[level], c.fold_inv_s[level], (int)L, 0});
             for (size_t qi = 0; qi < L; ++qi) {
-                ntt_cs.push_back({cs + qi * N, cs + qi * N, (int)qi, 0});
-                kt_sub.push_back({in_a + qi * N, cs + qi * N, in_a + qi * N, (int)qi, 0});
+                if (fused) {
+                    // key term = inner a - ModDown: the subtraction as the row phase's epilogue
+                    cs_epi.push_back({cs + qi * N, in_a + qi * N, nullptr, in_a + qi * N, 0, 0, (int)qi, kEpiCombine});
+                } else {
+                    ntt_cs.push_back({cs + qi * N, cs + qi * N, (int)qi, 0});
+                    kt_sub.push_back({in_a + qi * N, cs + qi * N, in_a + qi * N, (int)qi, 0});
+                }
             }
             uint64_t* cf2 = coeff2 + (ci * ng + gk) * L * N;
             uint64_t* dg2 = digits2 + (ci * ng + gk) * B * T * N;
@@ -496,6 +505,10 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
             md_pair.push_back({o + L * N, cf, c.fold_inv[level], c.fold_inv_s[level], (int)L, 0});
             uint64_t* dst = poly ? b[ci] : a[ci];  // out holds a at offset 0, b at T*N
             for (size_t qi = 0; qi < L; ++qi) {
+                if (fused) {
+                    cf_epi.push_back({cf + qi * N, o + qi * N, nullptr, dst + qi * N, 0, 0, (int)qi, kEpiCombine});
+                    continue;
+                }
                 ntt_cf.push_back({cf + qi * N, cf + qi * N, (int)qi, 0});
                 final_sub.push_back({o + qi * N, cf + qi * N, dst + qi * N, (int)qi, 0});
             }
@@ -539,15 +552,24 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     const ModDownJob* j_mdp = t.add(md_pair);
     const NttJob* j_ntt_cf = t.add(ntt_cf);
     const SubJob* j_final = t.add(final_sub);
+    const NttEpiJob* j_cs_epi = t.add(cs_epi);
+    const NttEpiJob* j_cf_epi = t.add(cf_epi);
     rescale_jobs.plan(t);
     t.upload(c, s);
     // 1.
-    ntt_jobs(c, t.at(j_intt_a), (int)intt_a.size(), false, s);
-    {
-        Probe probe(kClsModUp, 8.0 * N * (double)(count * B * T), s);
-        kb_modup<<<grid_for(c, modup.size()), kT, 0, s>>>(t.at(j_modup), (int)modup.size(), c.d_mod, N);
+    if (fused) {
+        // inverse row phase, [inverse columns, ModUp, forward columns], forward row phase
+        ntt_jobs_phase(c, t.at(j_intt_a), (int)intt_a.size(), false, false, s);
+        modup_ntt_jobs(c, t.at(j_modup), (int)modup.size(), max_src, 8.0 * N * (double)(count * B * T), s);
+        ntt_jobs_phase(c, t.at(j_ntt_dig), (int)ntt_dig.size(), true, false, s);
+    } else {
+        ntt_jobs(c, t.at(j_intt_a), (int)intt_a.size(), false, s);
+        {
+            Probe probe(kClsModUp, 8.0 * N * (double)(count * B * T), s);
+            kb_modup<<<grid_for(c, modup.size()), kT, 0, s>>>(t.at(j_modup), (int)modup.size(), c.d_mod, N);
+        }
+        ntt_jobs(c, t.at(j_ntt_dig), (int)ntt_dig.size(), true, s);
     }
-    ntt_jobs(c, t.at(j_ntt_dig), (int)ntt_dig.size(), true, s);
     // 2.
     if (!baby_jobs.empty()) {
         double bytes = 0;
@@ -564,7 +586,17 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
                                                                c.d_mod, (int)nq, (int)L, (int)T, (int)ns, (int)ng, N);
     }
     // 4.
-    if (!md_single.empty()) {
+    if (!md_single.empty() && fused) {
+        ntt_jobs_phase(c, t.at(j_intt_pg), (int)intt_pg.size(), false, false, s);
+        moddown_ntt_jobs(c, t.at(j_mds), (int)md_single.size(), 8.0 * N * (K + L) * md_single.size(), s, false);
+        ntt_rows_epilogue_jobs(c, t.at(j_cs_epi), (int)cs_epi.size(), 8.0 * N * cs_epi.size(), s);
+        ntt_jobs_phase(c, t.at(j_intt_kt), (int)intt_kt.size(), false, false, s);
+        modup_ntt_jobs(c, t.at(j_modup2), (int)modup2.size(), max_src, 8.0 * N * (double)(md_single.size() * B * T),
+                       s);
+        ntt_jobs_phase(c, t.at(j_ntt_dig2), (int)ntt_dig2.size(), true, false, s);
+        Probe probe(kClsKeyMac, 8.0 * N * mac2.size() * (3.0 * B + 2.0), s);
+        kb_mac<<<grid_for(c, mac2.size()), kT, 0, s>>>(t.at(j_mac2), (int)mac2.size(), c.d_mod, (int)nq, N);
+    } else if (!md_single.empty()) {
         ntt_jobs(c, t.at(j_intt_pg), (int)intt_pg.size(), false, s);
         {
             Probe probe(kClsModDown, 8.0 * N * (K + L) * md_single.size(), s);
@@ -592,16 +624,22 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
                                                                c.d_mod, (int)nq, (int)L, (int)T, c.logN);
     }
     // 6.
-    ntt_jobs(c, t.at(j_intt_po), (int)intt_po.size(), false, s);
-    {
-        Probe probe(kClsModDown, 8.0 * N * (K + L) * md_pair.size(), s);
-        kb_moddown<<<grid_for(c, md_pair.size()), kT, 0, s>>>(t.at(j_mdp), (int)md_pair.size(), c.d_mod, (int)nq,
-                                                              (int)K, N);
-    }
-    ntt_jobs(c, t.at(j_ntt_cf), (int)ntt_cf.size(), true, s);
-    {
-        Probe probe(kClsElementwise, 8.0 * N * 3.0 * final_sub.size(), s);
-        kb_sub<<<grid_for(c, final_sub.size()), kT, 0, s>>>(t.at(j_final), (int)final_sub.size(), c.d_mod);
+    if (fused) {
+        ntt_jobs_phase(c, t.at(j_intt_po), (int)intt_po.size(), false, false, s);
+        moddown_ntt_jobs(c, t.at(j_mdp), (int)md_pair.size(), 8.0 * N * (K + L) * md_pair.size(), s);
+        ntt_rows_epilogue_jobs(c, t.at(j_cf_epi), (int)cf_epi.size(), 8.0 * N * cf_epi.size(), s);
+    } else {
+        ntt_jobs(c, t.at(j_intt_po), (int)intt_po.size(), false, s);
+        {
+            Probe probe(kClsModDown, 8.0 * N * (K + L) * md_pair.size(), s);
+            kb_moddown<<<grid_for(c, md_pair.size()), kT, 0, s>>>(t.at(j_mdp), (int)md_pair.size(), c.d_mod,
+                                                                  (int)nq, (int)K, N);
+        }
+        ntt_jobs(c, t.at(j_ntt_cf), (int)ntt_cf.size(), true, s);
+        {
+            Probe probe(kClsElementwise, 8.0 * N * 3.0 * final_sub.size(), s);
+            kb_sub<<<grid_for(c, final_sub.size()), kT, 0, s>>>(t.at(j_final), (int)final_sub.size(), c.d_mod);
+        }
     }
     rescale_jobs.run(c, t, s);
     check_cuda(cudaGetLastError(), "linear transform launch");
@@ -642,7 +680,11 @@ void rotate_many_batch(Context& c, size_t level, size_t count, const uint64_t* c
     uint64_t* arena = c.batch_buffers(s).arena(c, count * per_ct, s);
     auto modq = [&](size_t limb) { return (int)(limb < L ? limb : nq + (limb - L)); };
 
+    const bool fused = c.ntt_fusion;
+    int max_src = 1;
+    for (size_t j = 0; j < B; ++j) max_src = std::max(max_src, c.modup[level][j].src_count);
     std::vector<NttJob> intt_a, ntt_dig, intt_p, ntt_c;
+    std::vector<NttEpiJob> c_epi;
     std::vector<ModUpJob> modup;
     std::vector<MacJob> mac;
     std::vector<ModDownJob> md;
@@ -685,12 +727,19 @@ void rotate_many_batch(Context& c, size_t level, size_t count, const uint64_t* c
                 }
                 md.push_back({acc + (poly * T + L) * N, cr + poly * L * N, c.fold_inv[level], c.fold_inv_s[level],
                               (int)L, 0});
-                for (size_t qi = 0; qi < L; ++qi)
-                    ntt_c.push_back({cr + (poly * L + qi) * N, cr + (poly * L + qi) * N, (int)qi, 0});
+                if (!fused)
+                    for (size_t qi = 0; qi < L; ++qi)
+                        ntt_c.push_back({cr + (poly * L + qi) * N, cr + (poly * L + qi) * N, (int)qi, 0});
             }
             for (size_t qi = 0; qi < L; ++qi) {
                 // combine in place of the accumulators, then gather into the output slot
-                comb.push_back({acc, cr, b, a, acc + T * N, acc, (int)L, (int)K, (int)qi, 1, 0, 0});
+                if (fused) {
+                    c_epi.push_back({cr + qi * N, acc + qi * N, nullptr, acc + qi * N, 0, 0, (int)qi, kEpiCombine});
+                    c_epi.push_back({cr + (L + qi) * N, acc + (T + qi) * N, b + qi * N, acc + (T + qi) * N, 1, 0,
+                                     (int)qi, kEpiCombine});
+                } else {
+                    comb.push_back({acc, cr, b, a, acc + T * N, acc, (int)L, (int)K, (int)qi, 1, 0, 0});
+                }
                 gath.push_back({acc + T * N + qi * N, acc + qi * N, ob + qi * N, oa + qi * N, gal[r]});
             }
         }
@@ -707,29 +756,46 @@ void rotate_many_batch(Context& c, size_t level, size_t count, const uint64_t* c
     const NttJob* j7 = t.add(ntt_c);
     const CombineJob* j8 = t.add(comb);
     const GatherJob* j9 = t.add(gath);
+    const NttEpiJob* j10 = t.add(c_epi);
     t.upload(c, s);
-    ntt_jobs(c, t.at(j1), (int)intt_a.size(), false, s);
-    {
-        double bytes = 0;
-        for (size_t j = 0; j < B; ++j) bytes += 8.0 * N * (c.modup[level][j].src_count + c.modup[level][j].dst_count);
-        Probe probe(kClsModUp, bytes * count, s);
-        kb_modup<<<grid_for(c, modup.size()), kT, 0, s>>>(t.at(j2), (int)modup.size(), c.d_mod, N);
+    double modup_bytes = 0;
+    for (size_t j = 0; j < B; ++j) modup_bytes += 8.0 * N * (c.modup[level][j].src_count + c.modup[level][j].dst_count);
+    modup_bytes *= count;
+    if (fused) {
+        ntt_jobs_phase(c, t.at(j1), (int)intt_a.size(), false, false, s);
+        modup_ntt_jobs(c, t.at(j2), (int)modup.size(), max_src, modup_bytes, s);
+        ntt_jobs_phase(c, t.at(j3), (int)ntt_dig.size(), true, false, s);
+    } else {
+        ntt_jobs(c, t.at(j1), (int)intt_a.size(), false, s);
+        {
+            Probe probe(kClsModUp, modup_bytes, s);
+            kb_modup<<<grid_for(c, modup.size()), kT, 0, s>>>(t.at(j2), (int)modup.size(), c.d_mod, N);
+        }
+        ntt_jobs(c, t.at(j3), (int)ntt_dig.size(), true, s);
     }
-    ntt_jobs(c, t.at(j3), (int)ntt_dig.size(), true, s);
     if (!mac.empty()) {
         {
             Probe probe(kClsKeyMac, 8.0 * N * mac.size() * (3.0 * B + 2.0), s);
             kb_mac<<<grid_for(c, mac.size()), kT, 0, s>>>(t.at(j4), (int)mac.size(), c.d_mod, (int)nq, N);
         }
-        ntt_jobs(c, t.at(j5), (int)intt_p.size(), false, s);
-        {
-            Probe probe(kClsModDown, 8.0 * N * (K + L) * md.size(), s);
-            kb_moddown<<<grid_for(c, md.size()), kT, 0, s>>>(t.at(j6), (int)md.size(), c.d_mod, (int)nq, (int)K, N);
+        if (fused) {
+            ntt_jobs_phase(c, t.at(j5), (int)intt_p.size(), false, false, s);
+            moddown_ntt_jobs(c, t.at(j6), (int)md.size(), 8.0 * N * (K + L) * md.size(), s);
+            ntt_rows_epilogue_jobs(c, t.at(j10), (int)c_epi.size(), 8.0 * N * c_epi.size(), s);
+            Probe probe(kClsCombine, 8.0 * N * 4.0 * gath.size(), s);
+            kb_gather<<<grid_for(c, gath.size()), kT, 0, s>>>(t.at(j9), (int)gath.size(), c.logN);
+        } else {
+            ntt_jobs(c, t.at(j5), (int)intt_p.size(), false, s);
+            {
+                Probe probe(kClsModDown, 8.0 * N * (K + L) * md.size(), s);
+                kb_moddown<<<grid_for(c, md.size()), kT, 0, s>>>(t.at(j6), (int)md.size(), c.d_mod, (int)nq, (int)K,
+                                                                 N);
+            }
+            ntt_jobs(c, t.at(j7), (int)ntt_c.size(), true, s);
+            Probe probe(kClsCombine, 8.0 * N * L * 12.0 * (mac.size() / T), s);
+            kb_combine<<<grid_for(c, comb.size()), kT, 0, s>>>(t.at(j8), (int)comb.size(), c.d_mod, N);
+            kb_gather<<<grid_for(c, gath.size()), kT, 0, s>>>(t.at(j9), (int)gath.size(), c.logN);
         }
-        ntt_jobs(c, t.at(j7), (int)ntt_c.size(), true, s);
-        Probe probe(kClsCombine, 8.0 * N * L * 12.0 * (mac.size() / T), s);
-        kb_combine<<<grid_for(c, comb.size()), kT, 0, s>>>(t.at(j8), (int)comb.size(), c.d_mod, N);
-        kb_gather<<<grid_for(c, gath.size()), kT, 0, s>>>(t.at(j9), (int)gath.size(), c.logN);
     }
     check_cuda(cudaGetLastError(), "rotate_many launch");
 }

@@ -205,6 +205,10 @@ void Context::trim(cudaStream_t s) {
     chunk_cache.clear();
     chunk_cache_total -= chunk_cache_bytes;
     chunk_cache_bytes = 0;
+    // the stream-ordered pool keeps freed blocks up to its release threshold: hand them back
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
 }
 
 Context::~Context() {

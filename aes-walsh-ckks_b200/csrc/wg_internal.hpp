@@ -199,8 +199,9 @@ struct Context {
     void* take_chunk(size_t bytes, cudaStream_t s, size_t* got);
     void give_chunk(void* p, size_t bytes, cudaStream_t s);
     // Give back what the context holds for stream s beyond its tables and keys: the stream's
-    // batched scratch arena and staging ring, its single-operation workspace, and every cached
-    // chunk (waiting for their last users first).  The next call on s allocates again.
+    // batched scratch arena and staging ring, its single-operation workspace, every cached
+    // chunk (waiting for their last users first) and the stream-ordered pool's unused reserve.
+    // The next call on s allocates again.
     void trim(cudaStream_t s);
 
     ~Context();
@@ -319,7 +320,10 @@ void rescale_ntt_jobs(const Context& c, const RescaleNttJob* d_jobs, int njobs, 
 // max_src: the largest source-limb count of the jobs (shared-memory size).
 void modup_ntt_jobs(const Context& c, const ModUpNttJob* d_jobs, int njobs, int max_src, double bytes,
                     cudaStream_t s);
-void moddown_ntt_jobs(const Context& c, const ModDownNttJob* d_jobs, int njobs, double bytes, cudaStream_t s);
+// fma_alpha: the alpha estimate rounded as fused multiply-adds (the key switch's pair ModDown)
+// or as multiplies then adds (the single-polynomial ModDown of the QP linear transform).
+void moddown_ntt_jobs(const Context& c, const ModDownNttJob* d_jobs, int njobs, double bytes, cudaStream_t s,
+                      bool fma_alpha = true);
 
 // NTT over `polys` polynomials of `limbs` limbs each, `poly_stride` words apart.
 void ntt_forward(const Context& c, uint64_t* data, int limbs, int polys, size_t poly_stride,

@@ -52,8 +52,8 @@ constexpr size_t fused_smem(int tiles) {
     return 8 * (size_t)Geom<LOGN>::PAD * (size_t)(tiles + 1);
 }
 
-// Block (tile, job): one digit's column tile.
-template <int LOGN>
+// Block (tile, job): one digit's column tile.  W >= every job's digit width.
+template <int LOGN, int W>
 __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
     k_modup_ntt(const ModUpNttJob* __restrict__ jobs, int njobs, const Modulus* __restrict__ mods,
                 const TwPair* __restrict__ tw_base) {
@@ -67,6 +67,11 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
     const int tile = blockIdx.x, t = threadIdx.x;
     uint64_t* work = smem + (size_t)n * G::PAD;
 
+    // every source tile in flight at once, each awaited just before its inverse column phase
+    for (int i = 0; i < n; ++i) {
+        load_tile_async<LOGN>(smem + (size_t)i * G::PAD, job.src + (size_t)(first + i) * G::N, tile, t);
+        cp_async_commit();
+    }
     double alpha[G::E];
 #pragma unroll
     for (int k = 0; k < G::E; ++k) alpha[k] = 0.0;
@@ -74,7 +79,7 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
         const int mi = first + i;
         const Modulus m = mods[mi];
         uint64_t* sm = smem + (size_t)i * G::PAD;
-        load_tile<LOGN>(sm, job.src + (size_t)mi * G::N, tile, t);
+        cp_async_wait_upto(n - 1 - i);
         __syncthreads();
         inverse_cols<LOGN>(sm, tile, t, m, tw_base + (size_t)mi * 2 * G::N + G::N);
         modup_scale<LOGN>(sm, t, d, i, m.q, alpha);
@@ -85,15 +90,16 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
     for (int dst = 0; dst < nd; ++dst) {
         const int mi = __ldg(d.dst_mod + dst);
         const uint64_t q = mods[mi].q;
-        modup_value<LOGN>(work, smem, t, d, dst, q, hps);
+        modup_value<LOGN, W>(work, smem, t, d, dst, q, hps);
         __syncthreads();
         forward_cols<LOGN>(work, tile, t, q, tw_base + (size_t)mi * 2 * G::N);
         store_tile<LOGN>(work, job.digit + (size_t)__ldg(d.dst_limb + dst) * G::N, tile, t);
     }
 }
 
-// Block (tile, job): one accumulator polynomial's column tile.
-template <int LOGN>
+// Block (tile, job): one accumulator polynomial's column tile.  FMA: the alpha sum's rounding
+// (moddown_hps); KW >= K.
+template <int LOGN, bool FMA, int KW>
 __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
     k_moddown_ntt(const ModDownNttJob* __restrict__ jobs, int njobs, const Modulus* __restrict__ mods, int nq, int K,
                   const TwPair* __restrict__ tw_base) {
@@ -107,17 +113,21 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
     const Modulus* pmods = mods + nq;
 
     for (int pi = 0; pi < K; ++pi) {
+        load_tile_async<LOGN>(smem + (size_t)pi * G::PAD, job.src_p + (size_t)pi * G::N, tile, t);
+        cp_async_commit();
+    }
+    for (int pi = 0; pi < K; ++pi) {
         const Modulus m = pmods[pi];
         uint64_t* sm = smem + (size_t)pi * G::PAD;
-        load_tile<LOGN>(sm, job.src_p + (size_t)pi * G::N, tile, t);
+        cp_async_wait_upto(K - 1 - pi);
         __syncthreads();
         inverse_cols<LOGN>(sm, tile, t, m, tw_base + (size_t)(nq + pi) * 2 * G::N + G::N);
     }
     uint32_t hps[G::E];
-    moddown_hps<LOGN>(smem, t, pmods, K, hps);
+    moddown_hps<LOGN, KW, FMA>(smem, t, pmods, K, hps);
     for (int qi = 0; qi < job.L; ++qi) {
         const uint64_t q = mods[qi].q;
-        moddown_value<LOGN>(work, smem, t, pmods, K, q, job.inv + (size_t)qi * K, job.inv_s + (size_t)qi * K, hps);
+        moddown_value<LOGN, KW>(work, smem, t, K, q, job.inv + (size_t)qi * K, job.inv_s + (size_t)qi * K, hps);
         __syncthreads();
         forward_cols<LOGN>(work, tile, t, q, tw_base + (size_t)qi * 2 * G::N);
         store_tile<LOGN>(work, job.out + (size_t)qi * G::N, tile, t);
@@ -158,32 +168,60 @@ void launch_rescale(const Context& c, const RescaleNttJob* jobs, int njobs, cuda
                                                                       reinterpret_cast<const TwPair*>(c.d_tw));
 }
 
-template <int LOGN>
-void launch_modup(const Context& c, const ModUpNttJob* jobs, int njobs, int max_src, cudaStream_t s) {
+template <int LOGN, int W>
+void launch_modup_w(const Context& c, const ModUpNttJob* jobs, int njobs, int max_src, cudaStream_t s) {
     using G = Geom<LOGN>;
     static const bool opted = [] {
-        cudaFuncSetAttribute(k_modup_ntt<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)fused_smem<LOGN>(kMaxDigitWidth));
+        cudaFuncSetAttribute(k_modup_ntt<LOGN, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)fused_smem<LOGN>(W));
         return true;
     }();
     (void)opted;
     const dim3 grid(G::TILES, njobs < 65535 ? njobs : 65535, (njobs + 65534) / 65535);
-    k_modup_ntt<LOGN><<<grid, G::THREADS, fused_smem<LOGN>(max_src), s>>>(jobs, njobs, c.d_mod,
-                                                                           reinterpret_cast<const TwPair*>(c.d_tw));
+    k_modup_ntt<LOGN, W><<<grid, G::THREADS, fused_smem<LOGN>(max_src), s>>>(jobs, njobs, c.d_mod,
+                                                                              reinterpret_cast<const TwPair*>(c.d_tw));
 }
 
 template <int LOGN>
-void launch_moddown(const Context& c, const ModDownNttJob* jobs, int njobs, cudaStream_t s) {
+void launch_modup(const Context& c, const ModUpNttJob* jobs, int njobs, int max_src, cudaStream_t s) {
+    if (max_src <= 4)
+        launch_modup_w<LOGN, 4>(c, jobs, njobs, max_src, s);
+    else if (max_src <= 8)
+        launch_modup_w<LOGN, 8>(c, jobs, njobs, max_src, s);
+    else
+        launch_modup_w<LOGN, kMaxDigitWidth>(c, jobs, njobs, max_src, s);
+}
+
+template <int LOGN, bool FMA, int KW>
+void launch_moddown_k(const Context& c, const ModDownNttJob* jobs, int njobs, cudaStream_t s) {
     using G = Geom<LOGN>;
     static const bool opted = [] {
-        cudaFuncSetAttribute(k_moddown_ntt<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)fused_smem<LOGN>(kMaxPLimbs));
+        cudaFuncSetAttribute(k_moddown_ntt<LOGN, FMA, KW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)fused_smem<LOGN>(KW));
         return true;
     }();
     (void)opted;
     const dim3 grid(G::TILES, njobs < 65535 ? njobs : 65535, (njobs + 65534) / 65535);
-    k_moddown_ntt<LOGN><<<grid, G::THREADS, fused_smem<LOGN>((int)c.np), s>>>(
+    k_moddown_ntt<LOGN, FMA, KW><<<grid, G::THREADS, fused_smem<LOGN>((int)c.np), s>>>(
         jobs, njobs, c.d_mod, (int)c.nq, (int)c.np, reinterpret_cast<const TwPair*>(c.d_tw));
+}
+
+template <int LOGN, bool FMA>
+void launch_moddown_f(const Context& c, const ModDownNttJob* jobs, int njobs, cudaStream_t s) {
+    if (c.np <= 4)
+        launch_moddown_k<LOGN, FMA, 4>(c, jobs, njobs, s);
+    else if (c.np <= 8)
+        launch_moddown_k<LOGN, FMA, 8>(c, jobs, njobs, s);
+    else
+        launch_moddown_k<LOGN, FMA, kMaxPLimbs>(c, jobs, njobs, s);
+}
+
+template <int LOGN>
+void launch_moddown(const Context& c, const ModDownNttJob* jobs, int njobs, bool fma, cudaStream_t s) {
+    if (fma)
+        launch_moddown_f<LOGN, true>(c, jobs, njobs, s);
+    else
+        launch_moddown_f<LOGN, false>(c, jobs, njobs, s);
 }
 
 }  // namespace
@@ -222,18 +260,19 @@ void rescale_ntt_jobs(const Context& c, const RescaleNttJob* d_jobs, int njobs, 
     check_cuda(cudaGetLastError(), "fused rescale launch");
 }
 
-void moddown_ntt_jobs(const Context& c, const ModDownNttJob* d_jobs, int njobs, double bytes, cudaStream_t s) {
+void moddown_ntt_jobs(const Context& c, const ModDownNttJob* d_jobs, int njobs, double bytes, cudaStream_t s,
+                      bool fma_alpha) {
     if (njobs <= 0) return;
     if (c.np < 1 || c.np > (size_t)kMaxPLimbs) fail(kInvalid, "fused moddown: P limb count out of range");
     Probe probe(kClsModDown, bytes, s);
     switch (c.logN) {
-        case 10: launch_moddown<10>(c, d_jobs, njobs, s); break;
-        case 11: launch_moddown<11>(c, d_jobs, njobs, s); break;
-        case 12: launch_moddown<12>(c, d_jobs, njobs, s); break;
-        case 13: launch_moddown<13>(c, d_jobs, njobs, s); break;
-        case 14: launch_moddown<14>(c, d_jobs, njobs, s); break;
-        case 15: launch_moddown<15>(c, d_jobs, njobs, s); break;
-        case 16: launch_moddown<16>(c, d_jobs, njobs, s); break;
+        case 10: launch_moddown<10>(c, d_jobs, njobs, fma_alpha, s); break;
+        case 11: launch_moddown<11>(c, d_jobs, njobs, fma_alpha, s); break;
+        case 12: launch_moddown<12>(c, d_jobs, njobs, fma_alpha, s); break;
+        case 13: launch_moddown<13>(c, d_jobs, njobs, fma_alpha, s); break;
+        case 14: launch_moddown<14>(c, d_jobs, njobs, fma_alpha, s); break;
+        case 15: launch_moddown<15>(c, d_jobs, njobs, fma_alpha, s); break;
+        case 16: launch_moddown<16>(c, d_jobs, njobs, fma_alpha, s); break;
         default: fail(kInvalid, "fused moddown: ring degree must be 2^10 .. 2^16");
     }
     check_cuda(cudaGetLastError(), "fused moddown launch");

@@ -68,6 +68,41 @@ WG_HD void load_tile(uint64_t* sm, const uint64_t* __restrict__ limb, int tile, 
     }
 }
 
+#if defined(__CUDACC__)
+// The same load as an asynchronous copy (cp.async, 8 bytes per element) that lands in shared
+// memory without passing through registers, so a CTA can have all its source tiles in flight at
+// once; completion is awaited per commit group (cp_async_wait_upto) before a barrier.
+template <int LOGN>
+__device__ __forceinline__ void load_tile_async(uint64_t* sm, const uint64_t* __restrict__ limb, int tile, int t) {
+    using G = Geom<LOGN>;
+#pragma unroll
+    for (int k = 0; k < G::E; ++k) {
+        const int e = t + k * G::THREADS;
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(sm + ntt::pad16(e));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(limb + col_offset<LOGN>(tile, e))
+                     : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int P>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(P) : "memory");
+}
+// wait until at most `pending` of this thread's commit groups are still in flight
+__device__ __forceinline__ void cp_async_wait_upto(int pending) {
+    switch (pending) {
+        case 0: cp_async_wait<0>(); break;
+        case 1: cp_async_wait<1>(); break;
+        case 2: cp_async_wait<2>(); break;
+        case 3: cp_async_wait<3>(); break;
+        case 4: cp_async_wait<4>(); break;
+        case 5: cp_async_wait<5>(); break;
+        case 6: cp_async_wait<6>(); break;
+        default: cp_async_wait<7>(); break;
+    }
+}
+#endif
+
 // Store thread t's elements of the tile to one limb (no reduction: the forward transform's row
 // phase continues from these words).
 template <int LOGN>
@@ -100,7 +135,8 @@ WG_HD void scale_n_inv(uint64_t* sm, int t, const Modulus& m) {
 
 // ModUp, source limb i of the digit (coefficients in tile sm_i, canonical): scale by
 // qhat_inv_i in place and add the FP64 estimate term to thread t's alpha sums, in the order of
-// modup_coeff_w.
+// modup_coeff_w.  (modup_coeff_w first reduces its input below q; the inverse transform's
+// N^-1 step already leaves it canonical, so that reduction is the identity here.)
 template <int LOGN, class Desc>
 WG_HD void modup_scale(uint64_t* sm_i, int t, const Desc& d, int i, uint64_t qi, double* alpha) {
     using G = Geom<LOGN>;
@@ -109,7 +145,7 @@ WG_HD void modup_scale(uint64_t* sm_i, int t, const Desc& d, int i, uint64_t qi,
 #pragma unroll
     for (int k = 0; k < G::E; ++k) {
         uint64_t& v = sm_i[ntt::pad16(t + k * G::THREADS)];
-        const uint64_t s = mul_shoup(red4q(v, qi), w, ws, qi);
+        const uint64_t s = mul_shoup(v, w, ws, qi);
         v = s;
         alpha[k] = dadd(alpha[k], dmul(u2d(s), inv));
     }
@@ -121,8 +157,9 @@ WG_HD uint32_t hps_count(double alpha, int n) {
 }
 
 // ModUp destination dst of the digit: thread t's coefficients into the work tile.
-// src_tiles holds the n scaled source tiles (stride PAD).
-template <int LOGN, class Desc>
+// src_tiles holds the n scaled source tiles (stride PAD); W >= n bounds the digit width so the
+// dst row of constants stays in registers.
+template <int LOGN, int W, class Desc>
 WG_HD void modup_value(uint64_t* work, const uint64_t* src_tiles, int t, const Desc& d, int dst, uint64_t m,
                        const uint32_t* hps) {
     using G = Geom<LOGN>;
@@ -130,47 +167,67 @@ WG_HD void modup_value(uint64_t* work, const uint64_t* src_tiles, int t, const D
     const uint64_t* row = d.qhat + (size_t)dst * n;
     const uint64_t* row_s = d.qhat_s + (size_t)dst * n;
     const uint64_t* corr = d.corr + (size_t)dst * (n + 1);
+    uint64_t w[W], ws[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+        w[i] = i < n ? WG_LDG(row + i) : 0;
+        ws[i] = i < n ? WG_LDG(row_s + i) : 0;
+    }
 #pragma unroll
     for (int k = 0; k < G::E; ++k) {
         const int pe = ntt::pad16(t + k * G::THREADS);
         uint64_t acc = 0;
-        for (int i = 0; i < n; ++i)
-            acc = add_mod(acc, mul_shoup(src_tiles[(size_t)i * G::PAD + pe], WG_LDG(row + i), WG_LDG(row_s + i), m), m);
+#pragma unroll
+        for (int i = 0; i < W; ++i)
+            if (i < n) acc = add_mod(acc, mul_shoup(src_tiles[(size_t)i * G::PAD + pe], w[i], ws[i], m), m);
         work[pe] = sub_mod(acc, WG_LDG(corr + hps[k]), m);
     }
 }
 
-// ModDown: FP64 estimate of thread t's coefficients over the K P tiles (canonical), in the
-// order of moddown_all_limbs_k (fused multiply-add, as the pair ModDown is compiled).
-template <int LOGN>
+// ModDown: FP64 estimate of thread t's coefficients over the K P tiles, in the order of
+// moddown_all_limbs_k; FMA: rounded as a fused multiply-add (the pair ModDown's compiled form)
+// or as a multiply then an add (the single-polynomial ModDown's).  The tiles hold canonical
+// residues (the inverse transform's N^-1 step), so moddown_all_limbs_k's reduction of its input
+// below p is the identity here and is left out.  KW >= K keeps the constants in registers.
+template <int LOGN, int KW, bool FMA = true>
 WG_HD void moddown_hps(const uint64_t* p_tiles, int t, const Modulus* __restrict__ pmods, int K, uint32_t* hps) {
     using G = Geom<LOGN>;
+    double inv[KW];
+#pragma unroll
+    for (int pi = 0; pi < KW; ++pi) inv[pi] = pi < K ? pmods[pi].inv_q : 0.0;
 #pragma unroll
     for (int k = 0; k < G::E; ++k) {
         const int pe = ntt::pad16(t + k * G::THREADS);
         double alpha = 0.0;
-        for (int pi = 0; pi < K; ++pi) {
-            const uint64_t s = red4q(p_tiles[(size_t)pi * G::PAD + pe], pmods[pi].q);
-            alpha = dfma(u2d(s), pmods[pi].inv_q, alpha);
-        }
+#pragma unroll
+        for (int pi = 0; pi < KW; ++pi)
+            if (pi < K) {
+                const uint64_t s = p_tiles[(size_t)pi * G::PAD + pe];
+                alpha = FMA ? dfma(u2d(s), inv[pi], alpha) : dadd(alpha, dmul(u2d(s), inv[pi]));
+            }
         hps[k] = hps_count(alpha, K);
     }
 }
 
-// ModDown contribution for Q limb qi: thread t's coefficients into the work tile.
-template <int LOGN>
-WG_HD void moddown_value(uint64_t* work, const uint64_t* p_tiles, int t, const Modulus* __restrict__ pmods, int K,
-                         uint64_t q, const uint64_t* __restrict__ iv, const uint64_t* __restrict__ ivs,
-                         const uint32_t* hps) {
+// ModDown contribution for Q limb qi: thread t's coefficients into the work tile (canonical P
+// residues as for moddown_hps; KW >= K).
+template <int LOGN, int KW>
+WG_HD void moddown_value(uint64_t* work, const uint64_t* p_tiles, int t, int K, uint64_t q,
+                         const uint64_t* __restrict__ iv, const uint64_t* __restrict__ ivs, const uint32_t* hps) {
     using G = Geom<LOGN>;
+    uint64_t w[KW], ws[KW];
+#pragma unroll
+    for (int pi = 0; pi < KW; ++pi) {
+        w[pi] = pi < K ? WG_LDG(iv + pi) : 0;
+        ws[pi] = pi < K ? WG_LDG(ivs + pi) : 0;
+    }
 #pragma unroll
     for (int k = 0; k < G::E; ++k) {
         const int pe = ntt::pad16(t + k * G::THREADS);
         uint64_t acc = 0;
-        for (int pi = 0; pi < K; ++pi) {
-            const uint64_t s = red4q(p_tiles[(size_t)pi * G::PAD + pe], pmods[pi].q);
-            acc = add_mod(acc, mul_shoup(s, WG_LDG(iv + pi), WG_LDG(ivs + pi), q), q);
-        }
+#pragma unroll
+        for (int pi = 0; pi < KW; ++pi)
+            if (pi < K) acc = add_mod(acc, mul_shoup(p_tiles[(size_t)pi * G::PAD + pe], w[pi], ws[pi], q), q);
         work[pe] = sub_mod(acc, (uint64_t)hps[k], q);
     }
 }

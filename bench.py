@@ -1161,18 +1161,31 @@ def evaluation_capacity(run, stream, torch):
 
 
 def evaluation_bytes(run, stream, torch):
-    """Device bytes one evaluation of the run's context keeps after it ends (its stream's
-    scratch plus the reusable chunks it handed back), measured from a trimmed context: the
-    admission estimate of the served mix.  The context is trimmed again afterwards."""
+    """Peak device bytes one evaluation of the run's context takes beyond its keys and plans:
+    from a trimmed context, the largest drop of free device memory seen by a 2 ms poll during
+    one evaluation, plus a quarter for what the poll misses; the admission estimate of the
+    served mix.  The context is trimmed again afterwards."""
     run.ctx.trim(stream)
     torch.cuda.synchronize()
     free0 = torch.cuda.mem_get_info()[0]
+    low = [free0]
+    done = threading.Event()
+
+    def poll():
+        while not done.is_set():
+            low[0] = min(low[0], torch.cuda.mem_get_info()[0])
+            time.sleep(0.002)
+
+    th = threading.Thread(target=poll, daemon=True)
+    th.start()
     run.step(stream)
     torch.cuda.synchronize()
-    held = max(0, free0 - torch.cuda.mem_get_info()[0])
+    done.set()
+    th.join()
+    low[0] = min(low[0], torch.cuda.mem_get_info()[0])
     run.ctx.trim(stream)
     torch.cuda.synchronize()
-    return held
+    return int(1.25 * max(0, free0 - low[0]))
 
 
 # ------------------------------------------------------------------------------------------
