@@ -71,7 +71,7 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
     std::vector<GatherJob> gather;
     std::vector<NttEpiJob> contrib_epi;
     KsPlan p{};
-    p.fused = c.ntt_fusion;
+    p.fused = c.fuse(2 * n);  // the ModDown launch has two jobs per switch
     // MAC groups: consecutive switches with the same key, level and digit layout (up to
     // kMacGroup), one job per QP limb; [group_begin, it) is the open group
     size_t group_begin = 0;
@@ -298,7 +298,7 @@ static void plan_pipeline(const Context& c, PipelinePlan& P, size_t count, const
     uint64_t* ksbase = rembase + rem_words;
     std::vector<KsItem> relin_items(count), rot_items;
     std::vector<TensorJob> tensor;
-    RescaleJobs& rs = P.rescale.emplace(c);
+    RescaleJobs& rs = P.rescale.emplace();
     uint64_t* c2p = c2base;
     uint64_t* remp = rembase;
     for (size_t i = 0; i < count; ++i) {
@@ -318,7 +318,7 @@ static void plan_pipeline(const Context& c, PipelinePlan& P, size_t count, const
         ri.galois = 0;
         c2p += L * N;
         for (int poly = 0; poly < 2; ++poly) {
-            rs.add(c, poly ? xa[i] : xb[i], lv, remp);
+            rs.add(poly ? xa[i] : xb[i], lv, remp);
             remp += lv * N;
         }
         if (galois[i]) {
@@ -339,7 +339,7 @@ static void plan_pipeline(const Context& c, PipelinePlan& P, size_t count, const
     }
     P.jt = P.t.add(tensor);
     P.nt = (int)tensor.size();
-    rs.plan(P.t);
+    rs.plan(c, P.t);
     P.p1 = plan_keyswitch(c, relin_items.data(), count, ksbase, P.t);
     P.p2 = plan_keyswitch(c, rot_items.data(), rot_items.size(), ksbase, P.t);
     P.rotate = !rot_items.empty();

@@ -199,13 +199,18 @@ dim3 grid_for(const Context& c, size_t njobs) {
 // The launches of one batched rescale (ckks_rescale, src/ckks/operations/arith/ckks_rescale.cpp:
 // 68-148) over polynomials of any levels: add() records a polynomial x at level lv with lv
 // remainder limbs of scratch, plan() puts the job tables into a JobTable, run() launches.
-// With Context::ntt_fusion: the inverse row phase of the dropped limbs, one fused launch
-// (inverse column phase, rounded remainders, forward column phase; k_rescale_ntt) and the
-// forward row phase with the finish step as its epilogue (k_ntt_rows_epi): 3 launches.
+// Fused (Context::fuse over the polynomials): the inverse row phase of the dropped limbs, one
+// fused launch (inverse column phase, rounded remainders, forward column phase; k_rescale_ntt)
+// and the forward row phase with the finish step as its epilogue (k_ntt_rows_epi): 3 launches.
 // Without: inverse NTT, kb_rescale_prep, forward NTT, kb_rescale_finish: 6 launches.  Same words.
 struct RescaleJobs {
-    bool fused;
-    size_t N;
+    struct Poly {
+        uint64_t* x;
+        size_t lv;
+        uint64_t* rem;
+    };
+    std::vector<Poly> polys;
+    bool fused = false;
     std::vector<NttJob> drop, rem_ntt;
     std::vector<RescalePrepJob> prep;
     std::vector<RescaleFinishJob> fin;
@@ -218,28 +223,34 @@ struct RescaleJobs {
     const RescaleNttJob* jc = nullptr;
     const NttEpiJob* je = nullptr;
 
-    explicit RescaleJobs(const Context& c) : fused(c.ntt_fusion), N(c.N) {}
-    bool empty() const { return drop.empty(); }
-    void add(const Context& c, uint64_t* x, size_t lv, uint64_t* rem) {
-        const uint64_t* rc = c.rs_host.data() + c.rs_host_off[lv];
-        uint64_t* dl = x + lv * N;
-        drop.push_back({dl, dl, (int)lv, 0});
-        if (fused) {
-            cols.push_back({dl, rem, c.rs_one_s[lv], (int)lv, 0});
-            for (size_t q = 0; q < lv; ++q)
-                rows.push_back({rem + q * N, nullptr, x + q * N, x + q * N, rc[lv + q], rc[2 * lv + q], (int)q,
-                                kEpiRescale});
-        } else {
-            for (size_t q = 0; q < lv; ++q) {
-                prep.push_back({dl, rem + q * N, rc[q], rc[3 * lv + q], (int)lv, (int)q});
-                rem_ntt.push_back({rem + q * N, rem + q * N, (int)q, 0});
-                fin.push_back({x + q * N, rem + q * N, rc[lv + q], rc[2 * lv + q], (int)q, 0});
+    bool empty() const { return polys.empty(); }
+    void add(uint64_t* x, size_t lv, uint64_t* rem) { polys.push_back({x, lv, rem}); }
+    // builds the jobs (fused when the batch fills the device: Context::fuse) into t
+    void plan(const Context& c, JobTable& t) {
+        const size_t N = c.N;
+        fused = c.fuse(polys.size());
+        for (const Poly& pl : polys) {
+            const size_t lv = pl.lv;
+            uint64_t* x = pl.x;
+            uint64_t* rem = pl.rem;
+            const uint64_t* rc = c.rs_host.data() + c.rs_host_off[lv];
+            uint64_t* dl = x + lv * N;
+            drop.push_back({dl, dl, (int)lv, 0});
+            if (fused) {
+                cols.push_back({dl, rem, c.rs_one_s[lv], (int)lv, 0});
+                for (size_t q = 0; q < lv; ++q)
+                    rows.push_back({rem + q * N, nullptr, x + q * N, x + q * N, rc[lv + q], rc[2 * lv + q], (int)q,
+                                    kEpiRescale});
+            } else {
+                for (size_t q = 0; q < lv; ++q) {
+                    prep.push_back({dl, rem + q * N, rc[q], rc[3 * lv + q], (int)lv, (int)q});
+                    rem_ntt.push_back({rem + q * N, rem + q * N, (int)q, 0});
+                    fin.push_back({x + q * N, rem + q * N, rc[lv + q], rc[2 * lv + q], (int)q, 0});
+                }
             }
+            prep_bytes += 8.0 * N * (1.0 + lv);
+            fin_bytes += 8.0 * N * 3.0 * lv;
         }
-        prep_bytes += 8.0 * N * (1.0 + lv);
-        fin_bytes += 8.0 * N * 3.0 * lv;
-    }
-    void plan(JobTable& t) {
         jd = t.add(drop);
         if (fused) {
             jc = t.add(cols);
@@ -252,6 +263,7 @@ struct RescaleJobs {
     }
     void run(const Context& c, const JobTable& t, cudaStream_t s) const {
         if (drop.empty()) return;
+        const size_t N = c.N;
         if (fused) {
             ntt_jobs_phase(c, t.at(jd), (int)drop.size(), false, false, s);
             rescale_ntt_jobs(c, t.at(jc), (int)cols.size(), prep_bytes, s);

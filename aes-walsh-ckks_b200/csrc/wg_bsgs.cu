@@ -393,7 +393,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
 
     JobTable t;
     // 1. hoist
-    const bool fused = c.ntt_fusion;
+    const bool fused = c.fuse(2 * count);  // the pair ModDown launch: two jobs per ciphertext
     int max_src = 1;
     for (size_t j = 0; j < B; ++j) max_src = std::max(max_src, c.modup[level][j].src_count);
     std::vector<NttJob> intt_a, ntt_dig;
@@ -514,12 +514,12 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
             }
         }
     }
-    RescaleJobs rescale_jobs(c);
+    RescaleJobs rescale_jobs;
     if (st.rescale) {
         if (level == 0) fail(kInvalid, "ckks_rescale: invalid level");
         for (size_t ci = 0; ci < count; ++ci)
             for (int poly = 0; poly < 2; ++poly)
-                rescale_jobs.add(c, poly ? a[ci] : b[ci], level, rem + (ci * 2 + poly) * level * N);
+                rescale_jobs.add(poly ? a[ci] : b[ci], level, rem + (ci * 2 + poly) * level * N);
     }
 
     // Baby slot 0 holds (a, b) with zero P limbs: copy Q limbs, clear P limbs.
@@ -554,7 +554,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     const SubJob* j_final = t.add(final_sub);
     const NttEpiJob* j_cs_epi = t.add(cs_epi);
     const NttEpiJob* j_cf_epi = t.add(cf_epi);
-    rescale_jobs.plan(t);
+    rescale_jobs.plan(c, t);
     t.upload(c, s);
     // 1.
     if (fused) {
@@ -680,7 +680,7 @@ void rotate_many_batch(Context& c, size_t level, size_t count, const uint64_t* c
     uint64_t* arena = c.batch_buffers(s).arena(c, count * per_ct, s);
     auto modq = [&](size_t limb) { return (int)(limb < L ? limb : nq + (limb - L)); };
 
-    const bool fused = c.ntt_fusion;
+    const bool fused = c.fuse(count * B);  // the ModUp launch: one job per digit
     int max_src = 1;
     for (size_t j = 0; j < B; ++j) max_src = std::max(max_src, c.modup[level][j].src_count);
     std::vector<NttJob> intt_a, ntt_dig, intt_p, ntt_c;

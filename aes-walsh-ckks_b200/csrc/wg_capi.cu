@@ -348,8 +348,11 @@ int wg_ctx_trim(wg_context* ctx, void* stream) {
     return guard([&] { C(ctx).trim(S(stream)); });
 }
 
-int wg_set_ntt_fusion(wg_context* ctx, int fused) {
-    return guard([&] { C(ctx).ntt_fusion = fused != 0; });
+int wg_set_ntt_fusion(wg_context* ctx, int mode) {
+    return guard([&] {
+        if (mode < 0 || mode > 2) wg::fail(wg::kInvalid, "ntt fusion: mode must be 0, 1 or 2");
+        C(ctx).ntt_fusion = mode;
+    });
 }
 
 int wg_keyswitch(wg_context* ctx, size_t level, const uint64_t* key_term, int kind, int64_t rotation, uint64_t* b,

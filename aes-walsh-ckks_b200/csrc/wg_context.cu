@@ -372,6 +372,10 @@ Context* create_context(uint64_t N, const uint64_t* q, size_t nq, const uint64_t
         c->rs_inv_p_s[d] = T + H.rescale[d] + 2 * d;
         c->rs_half[d] = T + H.rescale[d] + 3 * d;
     }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+        c->sm_count = sms;
+    cudaGetLastError();
     ntt_autotune(*c);
     return c.release();
 }

@@ -232,14 +232,14 @@ public:
         const size_t N = c_.N, lv = x.level;
         if (lv == 0) throw std::invalid_argument("ckks_rescale: invalid level");
         uint64_t* r = scratch(count_ * x.np * lv);
-        RescaleJobs rj(c_);
+        RescaleJobs rj;
         for (size_t i = 0; i < count_; ++i)
             for (int k = 0; k < x.np; ++k) {
-                rj.add(c_, x.p[i][k], lv, r);
+                rj.add(x.p[i][k], lv, r);
                 r += lv * N;
             }
         JobTable t;
-        rj.plan(t);
+        rj.plan(c_, t);
         t.upload(c_, s_);
         rj.run(c_, t, s_);
         x.scale = x.scale / static_cast<long double>(c_.q[lv]);

@@ -142,10 +142,19 @@ struct Context {
     Modulus* d_mod = nullptr;
     uint64_t* d_tw = nullptr;        // [mod][2][N] (w, Shoup w) pairs: forward, inverse (ntt::TwPair)
     int ntt_variant[2][2] = {{0, 0}, {0, 0}};  // NTT geometry per [direction][phase: rows, columns]
-    // key switches and rescales run their base changes fused with the adjacent NTT column
-    // phases and their final element-wise steps in the last row phase's epilogue
-    // (wg_ksfuse.cu, k_ntt_rows_epi); false: the separate launches (same words)
-    bool ntt_fusion = true;
+    // Key switches and rescales can run their base changes fused with the adjacent NTT column
+    // phases and their final element-wise steps in the last row phase's epilogue (wg_ksfuse.cu,
+    // k_ntt_rows_epi).  0: always the separate launches; 1: fused when the launch fills the
+    // device (fuse()); 2: always fused.  The words are the same in every mode.
+    int ntt_fusion = 1;
+    int sm_count = 148;  // multiprocessors of the device
+    // Whether a step over `jobs` jobs runs fused: the fused kernels give one CTA of 128 threads
+    // per (job, 1024-coefficient column tile) and hold several source tiles in shared memory, so
+    // they only pay when the launch fills the device at least twice; smaller calls (a single
+    // ciphertext) keep the separate, wider launches.
+    bool fuse(size_t jobs) const {
+        return ntt_fusion == 2 || (ntt_fusion == 1 && jobs * (N >= 1024 ? N / 1024 : 1) >= 2 * (size_t)sm_count);
+    }
     NttTuning tuning{};
     // ModUp descriptors, host copies holding device pointers: [level][part]
     std::vector<std::vector<ModUpDesc>> modup;

@@ -671,11 +671,11 @@ class Context:
         the tuned choice."""
         _check(lib().wg_ntt_set_geometry(self.h, int(direction), int(phase), int(geometry)))
 
-    def set_ntt_fusion(self, fused):
-        """Batched key switches and rescales with their base changes fused into the NTT column
-        phases and their last element-wise steps into the row-phase epilogue (default), or as
-        separate launches; the words are the same."""
-        _check(lib().wg_set_ntt_fusion(self.h, int(bool(fused))))
+    def set_ntt_fusion(self, mode):
+        """Key switches and rescales with their base changes fused into the NTT column phases
+        and their last element-wise steps into the row-phase epilogue: 0 never, 1 when the
+        launch fills the device (default; True maps here), 2 always; the words are the same."""
+        _check(lib().wg_set_ntt_fusion(self.h, int(mode)))
 
     def keyswitch(self, level, key_term, kind, b, a, b_add=True, a_add=False, rotation=0, stream=None):
         _check(lib().wg_keyswitch(self.h, level, _ptr(key_term), kind, int(rotation), _ptr(b), _ptr(a),

@@ -160,8 +160,11 @@ int wg_ntt_set_geometry(wg_context* ctx, int direction, int phase, int geometry)
  * epilogue of the last forward row phase.  ckks_hybrid_key_switch_inplace
  * (src/ckks/operations/keyswitch/ckks_keyswitch.cpp:1330-1641) and ckks_rescale
  * (src/ckks/operations/arith/ckks_rescale.cpp:68-148) compute the same words step by step.
- * fused = 0 selects the separate launches, for comparison; the words are identical. */
-int wg_set_ntt_fusion(wg_context* ctx, int fused);
+ * mode 1 (the default) fuses a step when its launch fills the device at least twice (the fused
+ * kernels run one 128-thread block per job and 1024-coefficient column tile), so a single
+ * ciphertext keeps the wider separate launches; mode 2 always fuses, mode 0 never.  The words
+ * are identical in every mode. */
+int wg_set_ntt_fusion(wg_context* ctx, int mode);
 
 /* Hybrid key switch of key_term at `level` with the installed key (kind, rotation):
  * b = (b_add ? b + ks_b : ks_b), a = (a_add ? a + ks_a : ks_a).  key_term may alias a.
@@ -196,7 +199,8 @@ int wg_relin(wg_context* ctx, size_t level, uint64_t* c0, uint64_t* c1, const ui
              void* stream);
 
 /* Rescale `npolys` polynomials (poly_stride words apart) from `level` to level-1; the first
- * level*N words of each polynomial hold the result.
+ * level*N words of each polynomial hold the result, and the dropped limb's words are left as
+ * scratch (here and in every batched entry point that rescales).
  * Replaces ckks_rescale, src/ckks/operations/arith/ckks_rescale.cpp:68-148. */
 int wg_rescale(wg_context* ctx, size_t level, uint64_t* polys, size_t npolys,
                size_t poly_stride, void* stream);
@@ -212,7 +216,8 @@ int wg_sub(wg_context* ctx, size_t level, uint64_t* x, const uint64_t* y, size_t
 /* Batched multiply + relinearize + rescale + rotate over `count` ciphertexts at arbitrary
  * levels: for ciphertext i, (xb[i], xa[i]) <- rotate(rescale(relin(x_i * y_i)), rots[i]).
  * Pointer arrays are host arrays of device pointers; each x buffer must hold
- * (levels[i]+1)*N words per polynomial and receives levels[i]*N words.  The workload the
+ * (levels[i]+1)*N words per polynomial and receives levels[i]*N words (limb levels[i] is left as
+ * scratch).  The workload the
  * reference runs as ckks_mul_inplace, ckks_relin_hybrid_inplace, ckks_rescale,
  * ckks_rotate_inplace per ciphertext with OpenMP over ciphertexts.  Every stage is one launch
  * over all ciphertexts, limbs and digits (job tables uploaded once per call). */

@@ -96,13 +96,18 @@ def _oracle_setup(O, wg, prm, rotations, seed=5):
     return N, o, ctx, keys, conj, relin
 
 
+@pytest.mark.parametrize("fusion", [1, 2])
 @pytest.mark.parametrize("prm", SMALL)
-def test_small_sets_against_oracle(wg, oracle_mod, prm):
+def test_small_sets_against_oracle(wg, oracle_mod, prm, fusion):
+    """Every operation on one ciphertext at several levels against the oracle; fusion 1 (the
+    default) runs single ciphertexts through the separate launches, 2 forces the fused
+    key-switch and rescale kernels."""
     import torch
 
     O = oracle_mod
     rots = (1, 3, -2)
     N, o, ctx, keys, conj, relin = _oracle_setup(O, wg, prm, rots)
+    ctx.set_ntt_fusion(fusion)
     L = o.nq
     x = o.uniform(L, 11)
     d = _dev(wg, x)
@@ -228,19 +233,25 @@ def test_walsh15_batched_ops(wg, oracle_mod, count, nrot):
     ctx.batch_mul_relin_rescale_rotate(levels, [sl(dxb, i) for i in range(count)], [sl(dxa, i) for i in range(count)],
                                        [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots)
     gb, ga = _host(wg, dxb), _host(wg, dxa)
+    # the live limbs of every result (levels[i] limbs after the rescale): the dropped limb is
+    # scratch that each path leaves in its own intermediate form
+    live = np.zeros(count * stride, dtype=bool)
+    for i in range(count):
+        live[i * stride:i * stride + int(levels[i]) * N] = True
+    same = lambda x, y: (_host(wg, x)[live] == y[live]).all()
     # the plain per-operation path gives the same residues
     pxb, pxa = _dev(wg, xb), _dev(wg, xa)
     ctx.batch_mul_relin_rescale_rotate(levels, [sl(pxb, i) for i in range(count)], [sl(pxa, i) for i in range(count)],
                                        [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots,
                                        plain=True)
-    assert (_host(wg, pxb) == gb).all() and (_host(wg, pxa) == ga).all()
-    # ModUp / ModDown as separate launches instead of inside the NTT column phases: same residues
+    assert same(pxb, gb) and same(pxa, ga)
+    # the base changes and final steps as separate launches instead of inside the NTT phases
     ctx.set_ntt_fusion(False)
     uxb, uxa = _dev(wg, xb), _dev(wg, xa)
     ctx.batch_mul_relin_rescale_rotate(levels, [sl(uxb, i) for i in range(count)], [sl(uxa, i) for i in range(count)],
                                        [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots)
     ctx.set_ntt_fusion(True)
-    assert (_host(wg, uxb) == gb).all() and (_host(wg, uxa) == ga).all()
+    assert same(uxb, gb) and same(uxa, ga)
     # the graph-captured plan over its own buffers: same residues, replayable
     gxb, gxa = _dev(wg, xb), _dev(wg, xa)
     plan = wg.BatchPlan(ctx, levels, [sl(gxb, i) for i in range(count)], [sl(gxa, i) for i in range(count)],
@@ -250,7 +261,7 @@ def test_walsh15_batched_ops(wg, oracle_mod, count, nrot):
         gxb.copy_(_dev(wg, xb))
         gxa.copy_(_dev(wg, xa))
         plan.launch()
-        assert (_host(wg, gxb) == gb).all() and (_host(wg, gxa) == ga).all()
+        assert same(gxb, gb) and same(gxa, ga)
     assert wg.launch_count() - n0 >= 2 * 20
     plan.close()
     ob, oa = xb.copy(), xa.copy()
