@@ -581,7 +581,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     }
     // 3.
     {
-        Probe probe(kClsElementwise, 8.0 * N * (double)(st.nterms * T + count * (ns + ng) * 2 * T), s);
+        Probe probe(kClsGiant, 8.0 * N * (double)(st.nterms * T + count * (ns + ng) * 2 * T), s);
         kb_giant<<<grid_for(c, giant_jobs.size()), kT, 0, s>>>(t.at(j_giant), (int)giant_jobs.size(), t.at(j_terms),
                                                                c.d_mod, (int)nq, (int)L, (int)T, (int)ns, (int)ng, N);
     }

@@ -247,7 +247,9 @@ enum KernelClass : int {
     kClsModDown = 3,   // folded HPS ModDown
     kClsCombine = 4,   // combine / automorphism gathers
     kClsElementwise = 5,  // tensor, add/sub, rescale steps
-    kClsCount = 6
+    kClsWalsh = 6,     // Walsh S-box products and sums
+    kClsGiant = 7,     // BSGS giant-step sums
+    kClsCount = 8
 };
 // Per-class launch counters: snapshot, and credit of the kernels a graph replay runs.
 void probe_counts(uint64_t* out);

@@ -302,7 +302,7 @@ public:
         JobTable t;
         const SumJob* j = t.add(jobs);
         t.upload(c_, s_);
-        Probe probe(kClsElementwise, 8.0 * c_.N * jobs.size() * 5.0, s_);
+        Probe probe(kClsWalsh, 8.0 * c_.N * jobs.size() * 5.0, s_);
         kb_sum<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
         check_cuda(cudaGetLastError(), "walsh parity sums");
     }
@@ -435,7 +435,7 @@ private:
         JobTable t;
         const LinJob* j = t.add(jobs);
         t.upload(c_, s_);
-        Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 17.0, s_);
+        Probe probe(kClsWalsh, 8.0 * N * jobs.size() * 17.0, s_);
         kb_lin_pair<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), cf, c_.d_mod);
         check_cuda(cudaGetLastError(), "walsh linear combination");
         return out;
@@ -573,7 +573,7 @@ private:
         const WalshCoefs* cfd = t.add(cf);
         const WalshJob* j = t.add(jobs);
         t.upload(c_, s_);
-        Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 66.0, s_);
+        Probe probe(kClsWalsh, 8.0 * N * jobs.size() * 66.0, s_);
         kb_walsh_products<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), t.at(cfd), c_.d_mod);
         check_cuda(cudaGetLastError(), "walsh products");
         return {acc, raw};

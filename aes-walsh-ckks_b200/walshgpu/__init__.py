@@ -187,7 +187,8 @@ def _u64(a) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
 
 
-KCLASS = {"ntt": 0, "modup": 1, "keymac": 2, "moddown": 3, "combine": 4, "elementwise": 5}
+KCLASS = {"ntt": 0, "modup": 1, "keymac": 2, "moddown": 3, "combine": 4, "elementwise": 5, "walsh": 6,
+          "giant": 7}
 
 
 def launch_count(kernel_class=-1) -> int:

@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--xboot-aes-steps", type=int, default=2, help="timed XBOOT AES-CTR evaluations (after one warm-up)")
     ap.add_argument("--no-keygen", action="store_true", help="skip the device key generation section")
     ap.add_argument("--serve-requests", type=int, default=32)
-    ap.add_argument("--serve-mix-requests", type=int, default=20)
+    ap.add_argument("--serve-mix-requests", type=int, default=10)
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not sample nvidia-smi clocks (for runs under a profiler, which wants the GPU to itself)")
     ap.add_argument("--no-aes", action="store_true",
@@ -984,6 +984,12 @@ def serve_bench(wg, torch, aes, requests, seed, capacity_blocks, workers=2, wind
             "workers": workers, "batch_window_ms": window_ms, "requests": requests, "blocks": int(sum(sizes)),
             "arrival_rate_per_s": rate, "offered_blocks_per_s": rate * float(np.mean(sizes)),
             "wall_s": wall, "blocks_per_s": sum(sizes) / wall,
+            # blocks_per_s counts the final drain (the last requests' latency after the last
+            # arrival); a server that keeps up shows flat latencies from the first quarter of the
+            # stream to the last
+            "arrival_span_s": float(np.sum(gaps)), "drain_s": wall - float(np.sum(gaps)),
+            "latency_first_last_quarter_ms": [float(lat[: max(1, requests // 4)].mean()),
+                                              float(lat[-max(1, requests // 4):].mean())],
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "mean": float(lat.mean()), "max": float(lat.max())},
             "queue_ms": {"p50": float(np.percentile(queue, 50)), "p99": float(np.percentile(queue, 99))},
@@ -1071,7 +1077,8 @@ def serve_mix_bench(wg, torch, aes, xruns, requests, seed, caps, eval_bytes, bud
     """Config 5's mixed stream over all five AES parameter sets: requests cycle through walsh15
     (log-uniform 2..1024 blocks, even), xboot15-full (1..16384), xboot15-sparse-1024 (1..1024),
     xboot14-full (1..8192) and xboot14-sparse-1024 (1..1024), arriving as one seeded Poisson
-    stream whose offered work is `load` x the device at each set's measured full-slot capacity.
+    stream whose offered work is `load` x the device in evaluation time (each request counted as
+    one full evaluation of its set at the measured full-slot capacity).
     One continuous-batching server per set on the same device, keys resident, all admitted
     through one shared device-memory budget (budget_frac of the device memory left free once
     every set's keys, plans and request buffers are resident; each evaluation holds its measured
@@ -1087,7 +1094,11 @@ def serve_mix_bench(wg, torch, aes, xruns, requests, seed, caps, eval_bytes, bud
         top = MIX_MAX_BLOCKS[kd] // (2 if kd == "walsh15" else 1)
         n = int(round(np.exp(rng.uniform(0.0, np.log(top)))))
         sizes.append(2 * n if kd == "walsh15" else n)
-    work = [n / caps[kd] for kd, n in zip(kinds, sizes)]
+    # offered work in device time: a request can cost a whole evaluation of its set, whatever its
+    # size (an XBOOT evaluation takes as long with 10 blocks as with 16384), so the arrival rate
+    # is set from the sets' full-evaluation times rather than from blocks
+    eval_s = {kd: MIX_MAX_BLOCKS[kd] / caps[kd] for kd in MIX_SETS}
+    work = [eval_s[kd] for kd in kinds]
     mk = lambda n: [(torch.empty(n, dtype=torch.int64, device="cuda"), torch.empty(n, dtype=torch.int64, device="cuda"))
                     for _ in range(128)]
     # every request's output buffers first, then the budget: the device memory left over
@@ -1127,10 +1138,12 @@ def serve_mix_bench(wg, torch, aes, xruns, requests, seed, caps, eval_bytes, bud
     offered = sum(sizes) / (sum(gaps) or 1.0)
     out = {"workload": f"{requests} requests cycling walsh15, xboot15-full, xboot15-sparse-1024, xboot14-full and "
                        f"xboot14-sparse-1024 (log-uniform sizes up to each set's slots), one Poisson stream at {load} "
-                       f"x the device's full-slot capacity; one server per set on the device, one shared "
+                       f"x the device in evaluation time (each request counted as one full evaluation of its set); "
+                       f"one server per set on the device, one shared "
                        f"device-memory budget of {budget_bytes / 2**30:.1f} GiB, walsh15 streams at the highest "
                        f"priority",
            "budget_gib": budget_bytes / 2**30, "evaluation_gib": {k: v / 2**30 for k, v in eval_bytes.items()},
+           "evaluation_s": eval_s,
            "batch_window_ms": window_ms, "arrival_rate_per_s": rate, "wall_s": wall,
            "blocks_per_s": sum(sizes) / wall, "offered_blocks_per_s": offered}
     for kd in MIX_SETS:

@@ -634,14 +634,18 @@ int wg_sequence_mul_relin_rescale_rotate(wg_context* ctx, size_t count, const si
 
 /* Instrumentation (no counterpart in the reference, which has only one wall-clock span
  * around the AES evaluation, bench/aes_bench.cpp:264-271).  Kernel classes:
- * 0 NTT phases, 1 ModUp, 2 key inner product, 3 ModDown, 4 combine/automorphism,
- * 5 elementwise (tensor, add/sub, rescale steps). */
+ * 0 NTT phases (the row phases with an epilogue included), 1 ModUp (fused or not), 2 key inner
+ * product (BSGS baby steps included), 3 ModDown (fused or not), 4 combine/automorphism,
+ * 5 elementwise (tensor, add/sub, rescale steps), 6 Walsh S-box products and sums,
+ * 7 BSGS giant-step sums. */
 #define WG_KCLASS_NTT 0
 #define WG_KCLASS_MODUP 1
 #define WG_KCLASS_KEYMAC 2
 #define WG_KCLASS_MODDOWN 3
 #define WG_KCLASS_COMBINE 4
 #define WG_KCLASS_ELEMENTWISE 5
+#define WG_KCLASS_WALSH 6
+#define WG_KCLASS_GIANT 7
 /* Kernel launches issued so far for a class (kernel_class < 0: all classes). */
 uint64_t wg_launch_count(int kernel_class);
 /* Bracket each following launch of `kernel_class` (up to max_launches) with CUDA events on
