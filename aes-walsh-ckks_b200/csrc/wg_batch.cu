@@ -50,6 +50,7 @@ struct KsPlan {
     int n_gather;
     const NttEpiJob* contrib_epi;  // fused: forward row phase of the contributions + combine
     int n_contrib_epi;
+    double contrib_epi_bytes;
     double mac_bytes, modup_bytes, moddown_bytes, combine_bytes;
     bool fused;   // ModUp / ModDown fused with the NTT column phases (Context::ntt_fusion)
     int max_src;  // widest digit (fused ModUp shared memory)
@@ -189,6 +190,7 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
     p.n_gather = (int)gather.size();
     p.contrib_epi = t.add(contrib_epi);
     p.n_contrib_epi = (int)contrib_epi.size();
+    p.contrib_epi_bytes = ntt_epilogue_bytes(contrib_epi, N);
     return p;
 }
 
@@ -206,7 +208,7 @@ static void run_keyswitch(const Context& c, const KsPlan& p, const JobTable& t, 
         }
         ntt_jobs_phase(c, t.at(p.intt_p), p.n_intt_p, false, false, s);
         moddown_ntt_jobs(c, t.at(p.moddown), p.n_moddown, p.moddown_bytes, s);
-        ntt_rows_epilogue_jobs(c, t.at(p.contrib_epi), p.n_contrib_epi, 8.0 * N * p.n_contrib_epi, s);
+        ntt_rows_epilogue_jobs(c, t.at(p.contrib_epi), p.n_contrib_epi, p.contrib_epi_bytes, s);
         if (p.n_gather) {
             Probe probe(kClsCombine, 8.0 * N * 4.0 * p.n_gather, s);
             kb_gather<<<grid_for(c, p.n_gather), kT, 0, s>>>(t.at(p.gather), p.n_gather, c.logN);

@@ -267,7 +267,7 @@ struct RescaleJobs {
         if (fused) {
             ntt_jobs_phase(c, t.at(jd), (int)drop.size(), false, false, s);
             rescale_ntt_jobs(c, t.at(jc), (int)cols.size(), prep_bytes, s);
-            ntt_rows_epilogue_jobs(c, t.at(je), (int)rows.size(), 8.0 * N * rows.size(), s);
+            ntt_rows_epilogue_jobs(c, t.at(je), (int)rows.size(), ntt_epilogue_bytes(rows, N), s);
         } else {
             ntt_jobs(c, t.at(jd), (int)drop.size(), false, s);
             {

@@ -449,7 +449,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     std::vector<ModDownJob> md_single;
     std::vector<SubJob> kt_sub;
     std::vector<ModUpJob> modup2;
-    std::vector<MacJob> mac2;
+    std::vector<MacGroupJob> mac2;
     for (size_t ci = 0; ci < count; ++ci)
         for (size_t gk = 0; gk < ng; ++gk) {
             if (giants[gk] == 0) continue;
@@ -481,10 +481,37 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
                     if (l < s0 || l >= s1)
                         ntt_dig2.push_back({dg2 + j * T * N + l * N, dg2 + j * T * N + l * N, modq(l), 0});
             }
-            for (size_t i = 0; i < T; ++i)
-                mac2.push_back({key.d_data, in_a, dg2, acc, T * N, (int)L, (int)K, (int)B, (int)c.alpha,
-                                (int)key.key_level, (int)i});
         }
+    // the giant's key inner products, up to kMacGroup ciphertexts per job so each key word is
+    // loaded once for all of them
+    double mac2_bytes = 0.0;
+    for (size_t gk = 0; gk < ng; ++gk) {
+        if (giants[gk] == 0) continue;
+        const KeyEntry& key = rot_key(giants[gk] * st.baby);
+        for (size_t c0 = 0; c0 < count; c0 += kMacGroup) {
+            const size_t n = std::min<size_t>(kMacGroup, count - c0);
+            for (size_t i = 0; i < T; ++i) {
+                MacGroupJob jb{};
+                jb.key = key.d_data;
+                jb.part_stride = T * N;
+                jb.L = (int)L;
+                jb.K = (int)K;
+                jb.parts = (int)B;
+                jb.alpha = (int)c.alpha;
+                jb.key_level = (int)key.key_level;
+                jb.i = (int)i;
+                jb.n = (int)n;
+                for (size_t k = 0; k < n; ++k) {
+                    const size_t slot = (c0 + k) * ng + gk;
+                    jb.key_term[k] = inner + slot * slotw;
+                    jb.digits[k] = digits2 + slot * B * T * N;
+                    jb.acc[k] = sw + slot * slotw;
+                }
+                mac2.push_back(jb);
+            }
+            mac2_bytes += 8.0 * N * T * (2.0 * B + (double)n * (B + 2.0));
+        }
+    }
     // 5. accumulation
     std::vector<GiantInfo> ginfo;
     for (size_t gk = 0; gk < ng; ++gk)
@@ -545,7 +572,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     const NttJob* j_intt_kt = t.add(intt_kt);
     const ModUpJob* j_modup2 = t.add(modup2);
     const NttJob* j_ntt_dig2 = t.add(ntt_dig2);
-    const MacJob* j_mac2 = t.add(mac2);
+    const MacGroupJob* j_mac2 = t.add(mac2);
     const GiantInfo* j_ginfo = t.add(ginfo);
     const AccumJob* j_accum = t.add(accum);
     const NttJob* j_intt_po = t.add(intt_po);
@@ -589,13 +616,13 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     if (!md_single.empty() && fused) {
         ntt_jobs_phase(c, t.at(j_intt_pg), (int)intt_pg.size(), false, false, s);
         moddown_ntt_jobs(c, t.at(j_mds), (int)md_single.size(), 8.0 * N * (K + L) * md_single.size(), s, false);
-        ntt_rows_epilogue_jobs(c, t.at(j_cs_epi), (int)cs_epi.size(), 8.0 * N * cs_epi.size(), s);
+        ntt_rows_epilogue_jobs(c, t.at(j_cs_epi), (int)cs_epi.size(), ntt_epilogue_bytes(cs_epi, N), s);
         ntt_jobs_phase(c, t.at(j_intt_kt), (int)intt_kt.size(), false, false, s);
         modup_ntt_jobs(c, t.at(j_modup2), (int)modup2.size(), max_src, 8.0 * N * (double)(md_single.size() * B * T),
                        s);
         ntt_jobs_phase(c, t.at(j_ntt_dig2), (int)ntt_dig2.size(), true, false, s);
-        Probe probe(kClsKeyMac, 8.0 * N * mac2.size() * (3.0 * B + 2.0), s);
-        kb_mac<<<grid_for(c, mac2.size()), kT, 0, s>>>(t.at(j_mac2), (int)mac2.size(), c.d_mod, (int)nq, N);
+        Probe probe(kClsKeyMac, mac2_bytes, s);
+        kb_mac_group<<<grid_for(c, mac2.size()), kT, 0, s>>>(t.at(j_mac2), (int)mac2.size(), c.d_mod, (int)nq, N);
     } else if (!md_single.empty()) {
         ntt_jobs(c, t.at(j_intt_pg), (int)intt_pg.size(), false, s);
         {
@@ -614,8 +641,8 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
             kb_modup<<<grid_for(c, modup2.size()), kT, 0, s>>>(t.at(j_modup2), (int)modup2.size(), c.d_mod, N);
         }
         ntt_jobs(c, t.at(j_ntt_dig2), (int)ntt_dig2.size(), true, s);
-        Probe probe(kClsKeyMac, 8.0 * N * mac2.size() * (3.0 * B + 2.0), s);
-        kb_mac<<<grid_for(c, mac2.size()), kT, 0, s>>>(t.at(j_mac2), (int)mac2.size(), c.d_mod, (int)nq, N);
+        Probe probe(kClsKeyMac, mac2_bytes, s);
+        kb_mac_group<<<grid_for(c, mac2.size()), kT, 0, s>>>(t.at(j_mac2), (int)mac2.size(), c.d_mod, (int)nq, N);
     }
     // 5.
     {
@@ -627,7 +654,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     if (fused) {
         ntt_jobs_phase(c, t.at(j_intt_po), (int)intt_po.size(), false, false, s);
         moddown_ntt_jobs(c, t.at(j_mdp), (int)md_pair.size(), 8.0 * N * (K + L) * md_pair.size(), s);
-        ntt_rows_epilogue_jobs(c, t.at(j_cf_epi), (int)cf_epi.size(), 8.0 * N * cf_epi.size(), s);
+        ntt_rows_epilogue_jobs(c, t.at(j_cf_epi), (int)cf_epi.size(), ntt_epilogue_bytes(cf_epi, N), s);
     } else {
         ntt_jobs(c, t.at(j_intt_po), (int)intt_po.size(), false, s);
         {
@@ -781,7 +808,7 @@ void rotate_many_batch(Context& c, size_t level, size_t count, const uint64_t* c
         if (fused) {
             ntt_jobs_phase(c, t.at(j5), (int)intt_p.size(), false, false, s);
             moddown_ntt_jobs(c, t.at(j6), (int)md.size(), 8.0 * N * (K + L) * md.size(), s);
-            ntt_rows_epilogue_jobs(c, t.at(j10), (int)c_epi.size(), 8.0 * N * c_epi.size(), s);
+            ntt_rows_epilogue_jobs(c, t.at(j10), (int)c_epi.size(), ntt_epilogue_bytes(c_epi, N), s);
             Probe probe(kClsCombine, 8.0 * N * 4.0 * gath.size(), s);
             kb_gather<<<grid_for(c, gath.size()), kT, 0, s>>>(t.at(j9), (int)gath.size(), c.logN);
         } else {

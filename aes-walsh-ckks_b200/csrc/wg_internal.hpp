@@ -326,6 +326,14 @@ using ntt::NttEpiJob;
 using ntt::kEpiRescale;
 using ntt::kEpiCombine;
 void ntt_rows_epilogue_jobs(const Context& c, const NttEpiJob* d_jobs, int njobs, double bytes, cudaStream_t s);
+// Algorithmic bytes of such jobs: the phase's share of its transform (8 N B per limb, as every
+// NTT phase is booked) plus the words the epilogue reads (acc, in) and writes (out).
+inline double ntt_epilogue_bytes(const std::vector<NttEpiJob>& jobs, size_t N) {
+    double words = 0.0;
+    for (const NttEpiJob& j : jobs)
+        words += 2.0 + (j.kind == kEpiCombine ? 1.0 : 0.0) + ((j.kind == kEpiRescale || j.c0) ? 1.0 : 0.0);
+    return 8.0 * (double)N * words;
+}
 void rescale_ntt_jobs(const Context& c, const RescaleNttJob* d_jobs, int njobs, double bytes, cudaStream_t s);
 
 // max_src: the largest source-limb count of the jobs (shared-memory size).

@@ -339,8 +339,7 @@ void ntt_jobs_phase(const Context& c, const NttJob* d_jobs, int njobs, bool forw
 
 void ntt_rows_epilogue_jobs(const Context& c, const NttEpiJob* d_jobs, int njobs, double bytes, cudaStream_t s) {
     if (njobs <= 0) return;
-    // booked as NTT work at the caller's bytes (the phase's own 8 N B per limb); the epilogue's
-    // reads replace the separate element-wise launch
+    // booked as NTT work: the phase's share plus the epilogue's words (ntt_epilogue_bytes)
     Probe probe(kClsNtt, bytes, s);
     const int v = c.ntt_variant[0][0];
     switch (c.logN) {
