@@ -230,8 +230,10 @@ def test_walsh15_batched_ops(wg, oracle_mod, count, nrot):
     ya = np.concatenate([o.uniform(L, 4000 + i) for i in range(count)])
     dxb, dxa, dyb, dya = (_dev(wg, v) for v in (xb, xa, yb, ya))
     sl = lambda t, i: t[i * stride:(i + 1) * stride]
+    n0 = wg.launch_count()
     ctx.batch_mul_relin_rescale_rotate(levels, [sl(dxb, i) for i in range(count)], [sl(dxa, i) for i in range(count)],
                                        [sl(dyb, i) for i in range(count)], [sl(dya, i) for i in range(count)], ct_rots)
+    batch_launches = wg.launch_count() - n0
     gb, ga = _host(wg, dxb), _host(wg, dxa)
     # the live limbs of every result (levels[i] limbs after the rescale): the dropped limb is
     # scratch that each path leaves in its own intermediate form
@@ -262,7 +264,8 @@ def test_walsh15_batched_ops(wg, oracle_mod, count, nrot):
         gxa.copy_(_dev(wg, xa))
         plan.launch()
         assert same(gxb, gb) and same(gxa, ga)
-    assert wg.launch_count() - n0 >= 2 * 20
+    # a replay runs (and counts) the kernels of one batched call: one launch per stage
+    assert wg.launch_count() - n0 == 2 * batch_launches and batch_launches < 40
     plan.close()
     ob, oa = xb.copy(), xa.copy()
     o.batched_ops(levels, ob, oa, yb, ya, relin, [keys[r] for r in ct_rots], ct_rots, stride, 8)
