@@ -140,8 +140,26 @@ __global__ void __launch_bounds__(Phase<LOGN, FWD, COLS, EB, STAGED>::THREADS, m
 }
 
 // The forward row phase of one job-table limb with an element-wise epilogue (NttEpiJob): the
-// same rounds and final reduction as k_ntt_phase<LOGN, true, false, ...>, then
-// ntt_epilogue(v) in place of the store.
+// same rounds and final reduction as k_ntt_phase<LOGN, true, false, ...>, then the epilogue in
+// place of the store.  The epilogue's operands (acc, in: the tile's contiguous words) are
+// copied into shared memory with cp.async when the block starts, so their loads overlap the
+// rounds instead of stalling the final step; out may alias acc or in, since each word is read
+// and written by this block only.
+template <int LOGN, int EB, bool STAGED>
+constexpr size_t rows_epi_smem() {
+    using P = Phase<LOGN, true, false, EB, STAGED>;
+    return smem_bytes<LOGN, true, false, EB, STAGED>() + 2 * 8 * (size_t)P::TILE;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
+
 template <int LOGN, int EB, bool STAGED>
 __global__ void __launch_bounds__(Phase<LOGN, true, false, EB, STAGED>::THREADS, min_blocks<EB>())
     k_ntt_rows_epi(const NttEpiJob* __restrict__ jobs, int njobs, const Modulus* __restrict__ mods,
@@ -152,6 +170,8 @@ __global__ void __launch_bounds__(Phase<LOGN, true, false, EB, STAGED>::THREADS,
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* sm = smem;
     TwPair* tw_s = reinterpret_cast<TwPair*>(smem + P::TILE + P::TILE / 16);
+    uint64_t* acc_s = smem + smem_bytes<LOGN, true, false, EB, STAGED>() / 8;
+    uint64_t* in_s = acc_s + P::TILE;
     const int j = blockIdx.y + 65535 * blockIdx.z;
     if (j >= njobs) return;
     const NttEpiJob job = jobs[j];
@@ -160,6 +180,26 @@ __global__ void __launch_bounds__(Phase<LOGN, true, false, EB, STAGED>::THREADS,
     const TwPair* tw = tw_base + (size_t)mi * 2 * N;
     const int tile = blockIdx.x;
     const int t = threadIdx.x;
+    // the row tile is P::TILE contiguous words at tile * TILE: 16-byte copies when the operand
+    // limbs are 16-byte aligned (they start on a word; tile * TILE keeps any 16-byte alignment),
+    // 8-byte copies otherwise
+    const size_t base = (size_t)tile * P::TILE;
+    const bool need_acc = job.kind == kEpiCombine;
+    const bool need_in = job.kind == kEpiRescale || job.c0 != 0;
+    const uintptr_t align = (need_acc ? reinterpret_cast<uintptr_t>(job.acc) : 0) |
+                            (need_in ? reinterpret_cast<uintptr_t>(job.in) : 0);
+    if ((align & 15) == 0) {
+        for (int c = t; c < P::TILE / 2; c += P::THREADS) {
+            if (need_acc) cp_async16(acc_s + 2 * c, job.acc + base + 2 * c);
+            if (need_in) cp_async16(in_s + 2 * c, job.in + base + 2 * c);
+        }
+    } else {
+        for (int e = t; e < P::TILE; e += P::THREADS) {
+            if (need_acc) cp_async8(acc_s + e, job.acc + base + e);
+            if (need_in) cp_async8(in_s + e, job.in + base + e);
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
 #pragma unroll
     for (int k = 0; k < E; ++k) {
         const int e = t + k * P::THREADS;
@@ -187,19 +227,22 @@ __global__ void __launch_bounds__(Phase<LOGN, true, false, EB, STAGED>::THREADS,
     else
         ntt_rounds<LOGN, true, false, EB, STAGED, false>(std::make_integer_sequence<int, P::ROUNDS>{}, sm, sub, o,
                                                         tile, m.q, twr);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    const uint64_t q = m.q;
 #pragma unroll
     for (int k = 0; k < E; ++k) {
         const int e = t + k * P::THREADS;
         const uint64_t raw = sm[pad16(e)];
-        const uint64_t v = lazy ? reduce64(raw, m) : red4q(raw, m.q);
-        ntt_epilogue(job, tile_offset<LOGN, true, false, EB, STAGED>(tile, e), v, m.q);
+        const uint64_t v = lazy ? reduce64(raw, m) : red4q(raw, q);
+        job.out[base + e] = epilogue_value(job, need_acc ? acc_s[e] : 0, need_in ? in_s[e] : 0, v, q);
     }
 }
 
 template <int LOGN, int EB, bool STAGED>
 void launch_rows_epi(const Context& c, const NttEpiJob* jobs, int njobs, cudaStream_t s) {
     using P = Phase<LOGN, true, false, EB, STAGED>;
-    constexpr size_t sm = smem_bytes<LOGN, true, false, EB, STAGED>();
+    constexpr size_t sm = rows_epi_smem<LOGN, EB, STAGED>();
     static const bool opted = [] {
         cudaFuncSetAttribute(k_ntt_rows_epi<LOGN, EB, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         return true;

@@ -219,15 +219,22 @@ struct NttEpiJob {
     int kind;
 };
 
-WG_HD void ntt_epilogue(const NttEpiJob& j, size_t off, uint64_t v, uint64_t q) {
+// The epilogue's word for the finished canonical word v and the operands acc, in (each used
+// only where the kind needs it).
+WG_HD uint64_t epilogue_value(const NttEpiJob& j, uint64_t acc, uint64_t in, uint64_t v, uint64_t q) {
     if (j.kind == kEpiRescale) {
-        uint64_t x = j.in[off];
-        if (x >= q) x -= q;
-        j.out[off] = mul_shoup(sub_mod(x, v, q), j.c0, j.c1, q);
-    } else {
-        const uint64_t d = sub_mod(j.acc[off], v, q);
-        j.out[off] = j.c0 ? add_mod(j.in[off], d, q) : d;
+        if (in >= q) in -= q;
+        return mul_shoup(sub_mod(in, v, q), j.c0, j.c1, q);
     }
+    const uint64_t d = sub_mod(acc, v, q);
+    return j.c0 ? add_mod(in, d, q) : d;
+}
+
+// The epilogue at word off of the job's limbs, operands read from their arrays.
+WG_HD void ntt_epilogue(const NttEpiJob& j, size_t off, uint64_t v, uint64_t q) {
+    const uint64_t acc = j.kind == kEpiCombine ? j.acc[off] : 0;
+    const uint64_t in = (j.kind == kEpiRescale || j.c0) ? j.in[off] : 0;
+    j.out[off] = epilogue_value(j, acc, in, v, q);
 }
 
 // Global offset (within one limb) of tile element e.

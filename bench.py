@@ -789,10 +789,16 @@ def xboot_bench(wg, torch, stream, timed, local, steps, with_cpu):
     step()
     l0 = wg.launch_count()
     ms = timed(step, steps)
+    launches = (wg.launch_count() - l0) / steps
+    ctx.set_ntt_fusion(0)  # the same layer with the separate launches around the NTTs
+    step()
+    unfused_ms = timed(step, steps)
+    ctx.set_ntt_fusion(1)
     res = {"workload": "XBOOT S-box, one SubBytes layer: 16 instances of 8 bits at level 5 of the xboot15 chain "
                        "(255 monomials from 247 multiply+relin+rescale per instance, 8 integer combinations)",
            "ms_per_layer": ms, "sboxes_per_s": count / (ms / 1000.0),
-           "launches_per_layer": (wg.launch_count() - l0) / steps, "output_level": level - 3}
+           "launches_per_layer": launches, "output_level": level - 3,
+           "unfused_ms_per_layer": unfused_ms, "fused_speedup": unfused_ms / ms}
     if with_cpu:
         try:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
