@@ -46,7 +46,9 @@ __device__ __forceinline__ void forward_cols(uint64_t* sm, int tile, int t, uint
         col_rounds<LOGN, true, false>(std::make_integer_sequence<int, Geom<LOGN>::ROUNDS>{}, sm, tile, t, q, tw);
 }
 
-// Shared memory: the source tiles, then the work tile (PAD words each).
+// Shared memory: the source tiles, then the work tile (PAD words each).  Resident blocks per SM
+// (the launch bounds) follow from it: up to 4 source tiles of 8.5 KiB leave room for 5 blocks,
+// the rescale's single tile for 6 (register-limited).
 template <int LOGN>
 constexpr size_t fused_smem(int tiles) {
     return 8 * (size_t)Geom<LOGN>::PAD * (size_t)(tiles + 1);
@@ -54,7 +56,7 @@ constexpr size_t fused_smem(int tiles) {
 
 // Block (tile, job): one digit's column tile.  W >= every job's digit width.
 template <int LOGN, int W>
-__global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
+__global__ void __launch_bounds__(Geom<LOGN>::THREADS, W <= 4 ? 5 : 4)
     k_modup_ntt(const ModUpNttJob* __restrict__ jobs, int njobs, const Modulus* __restrict__ mods,
                 const TwPair* __restrict__ tw_base) {
     using G = Geom<LOGN>;
@@ -100,7 +102,7 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
 // Block (tile, job): one accumulator polynomial's column tile.  FMA: the alpha sum's rounding
 // (moddown_hps); KW >= K.
 template <int LOGN, bool FMA, int KW>
-__global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
+__global__ void __launch_bounds__(Geom<LOGN>::THREADS, KW <= 4 ? 5 : 4)
     k_moddown_ntt(const ModDownNttJob* __restrict__ jobs, int njobs, const Modulus* __restrict__ mods, int nq, int K,
                   const TwPair* __restrict__ tw_base) {
     using G = Geom<LOGN>;
@@ -136,7 +138,7 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
 
 // Block (tile, job): one polynomial's column tile of a rescale.
 template <int LOGN>
-__global__ void __launch_bounds__(Geom<LOGN>::THREADS, 4)
+__global__ void __launch_bounds__(Geom<LOGN>::THREADS, 6)
     k_rescale_ntt(const RescaleNttJob* __restrict__ jobs, int njobs, const Modulus* __restrict__ mods,
                   const TwPair* __restrict__ tw_base) {
     using G = Geom<LOGN>;
