@@ -12,7 +12,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from params import SMALL
+from params import SMALL, WALSH15
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "aes-walsh-ckks_b200", "csrc")
@@ -86,6 +86,40 @@ def test_emulated_kernels_match_oracle(oracle_mod, emu, prm, fused):
                 assert (xs[: level * N] == os0).all()
     finally:
         emu.emu_set_keyswitch_fusion(0)
+        emu.emu_destroy(h)
+
+
+def test_emulated_fused_steps_walsh15(oracle_mod, emu):
+    """The fused key switch and rescale at the walsh15 shapes (N = 2^15: 16-column tiles of the
+    7-bit column phase; 13 Q limbs, 4 P limbs, digits of 5, 5 and 3) with the row-phase
+    geometry the device autotuner picks there (8 residues per thread, twiddles from the table):
+    a rotation at the top level and at level 0, and a rescale, against the oracle."""
+    O = oracle_mod
+    prm = WALSH15
+    N = 1 << prm["logN"]
+    p, q = O.find_primes(prm["p_bits"], prm["q_bits"], N)
+    o = O.OracleCtx(N, q, p, prm["dnum"])
+    h = emu.emu_create(N, q, len(q), p, len(p), prm["dnum"])
+    emu.emu_set_keyswitch_fusion(1)
+    emu.emu_set_ntt_geometry(1)
+    try:
+        L = len(q)
+        s = o.ternary(256, 3)
+        rk = o.rotation_key(s, 512, 11)
+        for level in (L - 1, 0):
+            b, a = o.uniform(level + 1, 20 + level), o.uniform(level + 1, 40 + level)
+            ob, oa = o.rotate(level, b, a, rk, 512)
+            eb, ea = b.copy(), a.copy()
+            emu.emu_keyswitch(h, level, a.copy(), rk, L - 1, eb, ea, 1, 0, o.galois(512))
+            assert (eb == ob).all() and (ea == oa).all(), level
+        x = o.uniform(L, 7)
+        (ref,) = o.rescale(L - 1, [x])
+        xs = x.copy()
+        emu.emu_rescale(h, L - 1, xs)
+        assert (xs[: (L - 1) * N] == ref).all()
+    finally:
+        emu.emu_set_keyswitch_fusion(0)
+        emu.emu_set_ntt_geometry(0)
         emu.emu_destroy(h)
 
 
