@@ -384,7 +384,10 @@ void ntt_rows_epilogue_jobs(const Context& c, const NttEpiJob* d_jobs, int njobs
     if (njobs <= 0) return;
     // booked as NTT work: the phase's share plus the epilogue's words (ntt_epilogue_bytes)
     Probe probe(kClsNtt, bytes, s);
-    const int v = c.ntt_variant[0][0];
+    // 8 residues per thread with twiddles from the table whatever the tuner chose for the plain
+    // row phase: the prefetched operands take 32 KiB of shared memory, which leaves 4 blocks per
+    // SM only in this geometry
+    const int v = 1;
     switch (c.logN) {
         case 10: rows_epi_variant<10>(c, v, d_jobs, njobs, s); break;
         case 11: rows_epi_variant<11>(c, v, d_jobs, njobs, s); break;
@@ -407,10 +410,10 @@ void ntt_phase_geometry(const Context& c, bool forward, bool cols, int variant, 
 }
 
 // Time every geometry of every (direction, phase) the way the batched circuits launch the
-// transform: one job-table launch over a scratch batch larger than the L2 cache (160 MB of
-// limbs) cycling over the context's moduli, so lazy and full-reduction moduli are both
-// represented; best of three launches after one warm-up.  A geometry replaces the default
-// (8 residues per thread, staged twiddles) only when it is at least 2 % faster, so timing noise
+// transform: job-table launches of 64 limbs over a scratch batch larger than the L2 cache (160 MB
+// of limbs) cycling over the context's moduli, so lazy and full-reduction moduli are both
+// represented; best of three passes after one warm-up.  A geometry replaces the default
+// (8 residues per thread, staged twiddles) only when it is at least 5 % faster, so timing noise
 // does not flip the choice.  Phases are timed on their own: each is one full pass over the
 // batch whatever the other phase does, and every geometry computes the same words, so the
 // choices combine freely.
@@ -427,6 +430,7 @@ void ntt_autotune(Context& c) {
     }
     const size_t N = c.N;
     const int kTuneLimbs = (int)((size_t{160} << 20) / (8 * N));
+    const int kTuneBatch = 64;
     const int nm = (int)(c.nq + c.np);
     check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
     uint64_t* buf = nullptr;
@@ -463,8 +467,11 @@ void ntt_autotune(Context& c) {
                     float t_best = 1e30f;
                     for (int rep = 0; rep < 4; ++rep) {
                         check_cuda(cudaEventRecord(e0, s), "ntt autotune: record");
-                        phase_dispatch(c, d == 0, p == 1, v, nullptr, 0, 0, 0, LimbMap{0, 0, 0}, d_jobs, kTuneLimbs,
-                                       s);
+                        // launches of kTuneBatch limbs, the size of a batched key switch's NTT
+                        // launch, so block tails and occupancy weigh as they do in the circuits
+                        for (int l0 = 0; l0 < kTuneLimbs; l0 += kTuneBatch)
+                            phase_dispatch(c, d == 0, p == 1, v, nullptr, 0, 0, 0, LimbMap{0, 0, 0}, d_jobs + l0,
+                                           std::min(kTuneBatch, kTuneLimbs - l0), s);
                         check_cuda(cudaEventRecord(e1, s), "ntt autotune: record");
                         check_cuda(cudaEventSynchronize(e1), "ntt autotune: wait");
                         float ms = 0;
@@ -475,7 +482,7 @@ void ntt_autotune(Context& c) {
                 }
                 int best_v = 0;
                 for (int v = 1; v < kNttGeometries; ++v)
-                    if (tn.ms[d][p][v] < 0.98f * tn.ms[d][p][0] && tn.ms[d][p][v] < tn.ms[d][p][best_v]) best_v = v;
+                    if (tn.ms[d][p][v] < 0.95f * tn.ms[d][p][0] && tn.ms[d][p][v] < tn.ms[d][p][best_v]) best_v = v;
                 tn.chosen[d][p] = best_v;
             }
         tn.limbs = kTuneLimbs;
