@@ -414,15 +414,23 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     std::vector<CtRef> ct_refs;
     for (size_t ci = 0; ci < count; ++ci) ct_refs.push_back({a[ci], b[ci]});
     const bool baby0 = !babies.empty() && babies[0] == 0;
+    // limb-outer, baby-step-inner: the blocks of consecutive jobs read the same hoisted digit
+    // limbs (one ciphertext group's, limb i) with different keys, so the digits come from HBM
+    // once per stage instead of once per baby step
+    std::vector<const KeyEntry*> baby_keys(ns, nullptr);
+    std::vector<uint64_t> baby_ginv(ns, 0);
     for (size_t k = 0; k < ns; ++k) {
         if (babies[k] == 0) continue;
-        const KeyEntry& key = rot_key(babies[k]);
-        const uint64_t ginv = host::powmod(galois_of(babies[k]), N - 1, 2 * N);
-        for (size_t c0 = 0; c0 < count; c0 += kGiantBatch)
-            for (size_t i = 0; i < T; ++i)
-                baby_jobs.push_back({key.d_data, ginv, (int)key.key_level, (int)i, (int)k, (int)c0,
-                                     (int)std::min<size_t>(kGiantBatch, count - c0), 0});
+        baby_keys[k] = &rot_key(babies[k]);
+        baby_ginv[k] = host::powmod(galois_of(babies[k]), N - 1, 2 * N);
     }
+    for (size_t i = 0; i < T; ++i)
+        for (size_t c0 = 0; c0 < count; c0 += kGiantBatch)
+            for (size_t k = 0; k < ns; ++k) {
+                if (!baby_keys[k]) continue;
+                baby_jobs.push_back({baby_keys[k]->d_data, baby_ginv[k], (int)baby_keys[k]->key_level, (int)i, (int)k,
+                                     (int)c0, (int)std::min<size_t>(kGiantBatch, count - c0), 0});
+            }
     // 3. giant sums
     std::vector<TermRef> terms;
     std::vector<GiantJob> giant_jobs;
