@@ -38,8 +38,13 @@ def emu(tmp_path_factory):
     return E
 
 
+# one digit per Q limb: the key inner products run over 8 parts, past the point where the
+# 128-bit product sums are folded (Acc128, every 4 terms)
+MANY_DIGITS = dict(logN=10, q_bits=[40, 45, 45, 45, 50, 50, 50, 50], p_bits=[55], dnum=8, h=64)
+
+
 @pytest.mark.parametrize("fused", [0, 1])
-@pytest.mark.parametrize("prm", SMALL)
+@pytest.mark.parametrize("prm", SMALL + [MANY_DIGITS])
 def test_emulated_kernels_match_oracle(oracle_mod, emu, prm, fused):
     """NTT, key switch (rotation, relinearisation) and rescale at three levels; fused = 1 runs
     them as the device does by default: ModUp, ModDown and the rescale remainders inside the NTT
