@@ -96,10 +96,9 @@ __global__ void __launch_bounds__(kT) kb_mac(const MacJob* jobs, int n, const Mo
               j->acc, N, j->i, coeff);
 }
 
-// acc_{a,b}[i] = sum_parts REDC(digit_part[i] * key_part_{a,b}[i]) for every switch of the group:
-// the canonical residue of the reference's mont_mul / add_mod chain (mac_accumulate,
-// wg_keyswitch.cuh), formed as one 128-bit sum per output and reduced once (Acc128).
-__global__ void __launch_bounds__(kT, 2) kb_mac_group(const MacGroupJob* jobs, int n, const Modulus* mods, int nq,
+// acc_{a,b}[i] = sum_parts REDC(digit_part[i] * key_part_{a,b}[i]) for every switch of the group,
+// parts accumulated in order as in mac_accumulate (wg_keyswitch.cuh).
+__global__ void __launch_bounds__(kT) kb_mac_group(const MacGroupJob* jobs, int n, const Modulus* mods, int nq,
                                                    size_t N) {
     const MacGroupJob* j = job_of(jobs, n);
     if (!j) return;
@@ -111,33 +110,27 @@ __global__ void __launch_bounds__(kT, 2) kb_mac_group(const MacGroupJob* jobs, i
     const size_t key_limbs = (size_t)j->key_level + 1 + K;
     const size_t klimb = is_p ? (size_t)j->key_level + 1 + (i - L) : (size_t)i;
     const size_t at = (size_t)i * N + coeff;
-    // 128-bit sums of the products, folded every kAccTerms parts and reduced once (Acc128)
-    Acc128 acc_a[kMacGroup], acc_b[kMacGroup];
+    uint64_t acc_a[kMacGroup], acc_b[kMacGroup];
 #pragma unroll
-    for (int c = 0; c < kMacGroup; ++c) acc_a[c] = acc_b[c] = Acc128{0, 0};
+    for (int c = 0; c < kMacGroup; ++c) acc_a[c] = acc_b[c] = 0;
     for (int p = 0; p < j->parts; ++p) {
         const int s0 = p * j->alpha, s1 = s0 + j->alpha < L ? s0 + j->alpha : L;
         const bool own = !is_p && i >= s0 && i < s1;
         const uint64_t ka = j->key[(((size_t)p * 2 + 0) * key_limbs + klimb) * N + coeff];
         const uint64_t kb = j->key[(((size_t)p * 2 + 1) * key_limbs + klimb) * N + coeff];
-        const bool fold = p > 0 && p % kAccTerms == 0;
 #pragma unroll
         for (int c = 0; c < kMacGroup; ++c) {
             if (c >= j->n) break;
             const uint64_t d = own ? j->key_term[c][at] : j->digits[c][p * j->part_stride + at];
-            if (fold) {
-                acc_fold(acc_a[c], m);
-                acc_fold(acc_b[c], m);
-            }
-            acc_mul(acc_a[c], d, ka);
-            acc_mul(acc_b[c], d, kb);
+            acc_a[c] = add_mod(acc_a[c], mont_mul(d, ka, q, qninv), q);
+            acc_b[c] = add_mod(acc_b[c], mont_mul(d, kb, q, qninv), q);
         }
     }
 #pragma unroll
     for (int c = 0; c < kMacGroup; ++c) {
         if (c >= j->n) break;
-        j->acc[c][at] = redc128(acc_a[c], q, qninv);
-        j->acc[c][(size_t)T * N + at] = redc128(acc_b[c], q, qninv);
+        j->acc[c][at] = acc_a[c];
+        j->acc[c][(size_t)T * N + at] = acc_b[c];
     }
 }
 

@@ -120,7 +120,7 @@ struct AccumJob {
     int ngiants, i, pad0, pad1;
 };
 
-__global__ void __launch_bounds__(kT, 2) kb_baby(const BabyJob* jobs, int n, const CtRef* __restrict__ cts,
+__global__ void __launch_bounds__(kT) kb_baby(const BabyJob* jobs, int n, const CtRef* __restrict__ cts,
                                               const uint64_t* __restrict__ digits, uint64_t* __restrict__ babies,
                                               const Modulus* mods, int nq, int L, int K, int parts, int alpha,
                                               int nslots, int logN) {
@@ -137,28 +137,24 @@ __global__ void __launch_bounds__(kT, 2) kb_baby(const BabyJob* jobs, int n, con
     const size_t klimb = is_p ? (size_t)j->key_level + 1 + (i - L) : (size_t)i;
     const size_t part_stride = (size_t)T * N;
     const size_t limb = (size_t)i * N + x;
-    // the key products as 128-bit sums reduced once (Acc128); the b accumulator starts from the
-    // ciphertext's b limb (Q limbs), added to the reduced sum at the end
-    Acc128 acc_a[kGiantBatch], acc_b[kGiantBatch];
+    uint64_t acc_a[kGiantBatch], acc_b[kGiantBatch];
 #pragma unroll
-    for (int c = 0; c < kGiantBatch; ++c) acc_a[c] = acc_b[c] = Acc128{0, 0};
+    for (int c = 0; c < kGiantBatch; ++c) {
+        acc_a[c] = 0;
+        acc_b[c] = (c < j->nc && !is_p) ? cts[j->c0 + c].b[limb] : 0;
+    }
     for (int p = 0; p < parts; ++p) {
         const int s0 = p * alpha, s1 = s0 + alpha < L ? s0 + alpha : L;
         const bool own = !is_p && i >= s0 && i < s1;  // source limb: the key term itself
         const uint64_t ka = j->key[(((size_t)p * 2 + 0) * key_limbs + klimb) * N + x];
         const uint64_t kb = j->key[(((size_t)p * 2 + 1) * key_limbs + klimb) * N + x];
-        const bool fold = p > 0 && p % kAccTerms == 0;
 #pragma unroll
         for (int c = 0; c < kGiantBatch; ++c) {
             if (c >= j->nc) break;
             const int ci = j->c0 + c;
             const uint64_t d = own ? cts[ci].a[limb] : digits[((size_t)ci * parts + p) * part_stride + limb];
-            if (fold) {
-                acc_fold(acc_a[c], m);
-                acc_fold(acc_b[c], m);
-            }
-            acc_mul(acc_a[c], d, ka);
-            acc_mul(acc_b[c], d, kb);
+            acc_a[c] = add_mod(acc_a[c], mont_mul(d, ka, q, qninv), q);
+            acc_b[c] = add_mod(acc_b[c], mont_mul(d, kb, q, qninv), q);
         }
     }
     const uint32_t dst = automorphism_src(x, j->galois_inv, logN);
@@ -167,15 +163,14 @@ __global__ void __launch_bounds__(kT, 2) kb_baby(const BabyJob* jobs, int n, con
     for (int c = 0; c < kGiantBatch; ++c) {
         if (c >= j->nc) break;
         uint64_t* o = babies + ((size_t)(j->c0 + c) * nslots + j->slot) * slot_words + (size_t)i * N;
-        const uint64_t b0 = is_p ? 0 : cts[j->c0 + c].b[limb];
-        o[dst] = redc128(acc_a[c], q, qninv);
-        o[(size_t)T * N + dst] = add_mod(b0, redc128(acc_b[c], q, qninv), q);
+        o[dst] = acc_a[c];
+        o[(size_t)T * N + dst] = acc_b[c];
     }
 }
 
 // Giant-step inner sums: inner[c][g] = sum over the terms (g, slot) of diag x baby[c][slot], in
-// QP: the canonical residue of the sum of the Montgomery products (mont_mul then add_mod term by
-// term in the reference), formed as one 128-bit sum per output and reduced once (Acc128).
+// QP.  Montgomery products and modular additions of canonical residues, so the order of the
+// terms does not change the canonical sums.
 __global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, const TermRef* __restrict__ term_table,
                                                const Modulus* mods, int nq, int L, int T, int nslots, int ngiants,
                                                size_t N) {
@@ -187,14 +182,9 @@ __global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, cons
     const uint64_t q = m.q, qninv = m.qninv;
     const size_t limb = (size_t)i * N + x;
     const size_t slot_words = 2 * (size_t)T * N;
-    // 128-bit sums of the products, folded every kAccTerms terms and reduced once (Acc128)
-    Acc128 acc_a[kGiantGroup], acc_b[kGiantGroup];
-    int cnt[kGiantGroup];
+    uint64_t acc_a[kGiantGroup], acc_b[kGiantGroup];
 #pragma unroll
-    for (int g = 0; g < kGiantGroup; ++g) {
-        acc_a[g] = acc_b[g] = Acc128{0, 0};
-        cnt[g] = 0;
-    }
+    for (int g = 0; g < kGiantGroup; ++g) acc_a[g] = acc_b[g] = 0;
     const uint64_t* babies = j->babies + (size_t)j->c * nslots * slot_words;
     int slot = -1;
     uint64_t ba = 0, bb = 0;
@@ -207,20 +197,15 @@ __global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, cons
             bb = bs[(size_t)T * N + limb];
         }
         const uint64_t d = tr.diag[limb];
+        const uint64_t pa = mont_mul(ba, d, q, qninv), pb = mont_mul(bb, d, q, qninv);
         // tr.g is the same for every thread of the block (one job per block), so this is a
         // uniform branch to the one accumulator pair the term adds to; the accumulators keep
         // constant indices and stay in registers
         switch (tr.g) {
 #define WG_GIANT_ADD(G)                          \
     case G:                                      \
-        if (cnt[G] == kAccTerms) {               \
-            acc_fold(acc_a[G], m);               \
-            acc_fold(acc_b[G], m);               \
-            cnt[G] = 0;                          \
-        }                                        \
-        acc_mul(acc_a[G], ba, d);                \
-        acc_mul(acc_b[G], bb, d);                \
-        ++cnt[G];                                \
+        acc_a[G] = add_mod(acc_a[G], pa, q);     \
+        acc_b[G] = add_mod(acc_b[G], pb, q);     \
         break;
             WG_GIANT_ADD(0)
             WG_GIANT_ADD(1)
@@ -240,8 +225,8 @@ __global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, cons
     for (int g = 0; g < kGiantGroup; ++g) {
         if (g >= j->ng) break;
         uint64_t* o = j->inner + ((size_t)j->c * ngiants + j->g0 + g) * slot_words;
-        o[limb] = redc128(acc_a[g], q, qninv);
-        o[(size_t)T * N + limb] = redc128(acc_b[g], q, qninv);
+        o[limb] = acc_a[g];
+        o[(size_t)T * N + limb] = acc_b[g];
     }
 }
 

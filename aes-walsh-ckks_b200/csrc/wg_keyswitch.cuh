@@ -170,8 +170,6 @@ WG_HD void mac_accumulate(const Modulus& m, int L, int K, int parts, int alpha, 
     const uint64_t q = m.q, qninv = m.qninv;
     const size_t key_limbs = (size_t)key_level + 1 + K;
     const size_t klimb = is_p ? (size_t)key_level + 1 + (i - L) : (size_t)i;
-    // the products as 128-bit sums reduced once (Acc128, wg_arith.cuh): the same canonical sums
-    Acc128 sa{0, 0}, sb{0, 0};
 #pragma unroll 4
     for (int j = 0; j < parts; ++j) {
         const int s0 = j * alpha, s1 = s0 + alpha < L ? s0 + alpha : L;
@@ -179,15 +177,9 @@ WG_HD void mac_accumulate(const Modulus& m, int L, int K, int parts, int alpha, 
                                                          : digits[j * part_stride + (size_t)i * N + coeff];
         const uint64_t ka = key[(((size_t)j * 2 + 0) * key_limbs + klimb) * N + coeff];
         const uint64_t kb = key[(((size_t)j * 2 + 1) * key_limbs + klimb) * N + coeff];
-        if (j > 0 && j % kAccTerms == 0) {
-            acc_fold(sa, m);
-            acc_fold(sb, m);
-        }
-        acc_mul(sa, d, ka);
-        acc_mul(sb, d, kb);
+        acc_a = add_mod(acc_a, mont_mul(d, ka, q, qninv), q);
+        acc_b = add_mod(acc_b, mont_mul(d, kb, q, qninv), q);
     }
-    acc_a = add_mod(acc_a, redc128(sa, q, qninv), q);
-    acc_b = add_mod(acc_b, redc128(sb, q, qninv), q);
 }
 
 // Key inner product for QP limb i at one coefficient:
