@@ -348,9 +348,22 @@ public:
         CtBatch out = alloc(x.level, 2);
         out.scale = x.scale;
         std::vector<KsItem> items(count_);
+        // X -> X^(2N-1) of every limb of every ciphertext in one launch
+        std::vector<GatherJob> gather;
+        gather.reserve(count_ * L);
+        for (size_t i = 0; i < count_; ++i)
+            for (size_t l = 0; l < L; ++l)
+                gather.push_back({x.p[i][0] + l * N, x.p[i][1] + l * N, perm.p[i][0] + l * N, perm.p[i][1] + l * N,
+                                  2 * N - 1});
+        {
+            JobTable t;
+            const GatherJob* j = t.add(gather);
+            t.upload(c_, s_);
+            Probe probe(kClsCombine, 8.0 * N * 4.0 * gather.size(), s_);
+            kb_gather<<<grid_for(c_, gather.size()), kT, 0, s_>>>(t.at(j), (int)gather.size(), c_.logN);
+            check_cuda(cudaGetLastError(), "conjugation automorphism");
+        }
         for (size_t i = 0; i < count_; ++i) {
-            for (int poly = 0; poly < 2; ++poly)
-                automorphism(c_, x.p[i][poly], perm.p[i][poly], (int)L, 1, 0, 2 * N - 1, s_);
             KsItem& it = items[i];
             it.level = x.level;
             it.key_term = perm.p[i][1];
