@@ -75,11 +75,11 @@ def test_tuning_report(wg, oracle_mod):
         for ph in range(2):
             g = t["chosen"][d][ph]
             assert 0 <= g < 4
-            # the default geometry is replaced only by a fastest one at least 2 % faster
+            # the default geometry is replaced only by a fastest one at least 5 % faster
             if g == 0:
-                assert (ms[d, ph, 1:] >= 0.98 * ms[d, ph, 0]).all()
+                assert (ms[d, ph, 1:] >= 0.95 * ms[d, ph, 0]).all()
             else:
-                assert ms[d, ph, g] < 0.98 * ms[d, ph, 0] and ms[d, ph, g] == ms[d, ph, 1:].min()
+                assert ms[d, ph, g] < 0.95 * ms[d, ph, 0] and ms[d, ph, g] == ms[d, ph, 1:].min()
     print("NTT tuning (N = 2^15, ms per phase over", t["limbs"], "limbs): chosen", t["chosen"])
     for d, dn in enumerate(("forward", "inverse")):
         for ph, pn in enumerate(("rows", "columns")):
