@@ -63,16 +63,15 @@ WG_HD void modup_coeff_w(const Desc& d, const Modulus* __restrict__ mods, const 
     uint64_t hps = round_half_up(alpha);
     if (hps > (uint64_t)n) hps = (uint64_t)n;
     for (int t = 0; t < d.dst_count; ++t) {
-        const Modulus& mt = mods[WG_LDG(d.dst_mod + t)];
+        const uint64_t m = mods[WG_LDG(d.dst_mod + t)].q;
         const uint64_t* row = d.qhat + (size_t)t * n;
-        // the canonical sum of the reference's Shoup products (mod the target), formed as one
-        // 128-bit sum of the plain products (each below 2^124, at most 16) and one reduction
-        Acc128 acc{0, 0};
+        const uint64_t* row_s = d.qhat_s + (size_t)t * n;
+        uint64_t acc = 0;
 #pragma unroll
         for (int i = 0; i < W; ++i)
-            if (i < n) acc_mul(acc, scaled[i], WG_LDG(row + i));
+            if (i < n) acc = add_mod(acc, mul_shoup(scaled[i], WG_LDG(row + i), WG_LDG(row_s + i), m), m);
         const uint64_t corr = WG_LDG(d.corr + (size_t)t * (n + 1) + hps);
-        digit[(size_t)WG_LDG(d.dst_limb + t) * N + coeff] = sub_mod(reduce128(acc.hi, acc.lo, mt), corr, mt.q);
+        digit[(size_t)WG_LDG(d.dst_limb + t) * N + coeff] = sub_mod(acc, corr, m);
     }
 }
 
@@ -129,15 +128,15 @@ WG_HD void moddown_all_limbs_k(const Modulus* __restrict__ mods, int nq, int L, 
     if (hps > (uint64_t)K) hps = (uint64_t)K;
     for (int qi = 0; qi < L; ++qi) {
         const Modulus& mq = mods[qi];
+        const uint64_t q = mq.q;
         const uint64_t* iv = inv + (size_t)qi * K;
-        // the canonical sum of the reference's Shoup products (s[pi] need not be reduced mod q
-        // first: its residue class is all that counts), as one 128-bit sum of the plain
-        // products (each below 2^124, at most 16) and one reduction
-        Acc128 acc{0, 0};
+        const uint64_t* ivs = inv_s + (size_t)qi * K;
+        uint64_t acc = 0;
+        // s[pi] mod q need not be formed: the Shoup product is canonical for any 64-bit input
 #pragma unroll
         for (int pi = 0; pi < KW; ++pi)
-            if (pi < K) acc_mul(acc, s[pi], WG_LDG(iv + pi));
-        out[(size_t)qi * N + coeff] = sub_mod(reduce128(acc.hi, acc.lo, mq), hps, mq.q);
+            if (pi < K) acc = add_mod(acc, mul_shoup(s[pi], WG_LDG(iv + pi), WG_LDG(ivs + pi), q), q);
+        out[(size_t)qi * N + coeff] = sub_mod(acc, hps, q);
     }
 }
 

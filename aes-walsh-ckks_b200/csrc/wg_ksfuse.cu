@@ -91,10 +91,10 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, W <= 4 ? 5 : 4)
     for (int k = 0; k < G::E; ++k) hps[k] = hps_count(alpha[k], n);
     for (int dst = 0; dst < nd; ++dst) {
         const int mi = __ldg(d.dst_mod + dst);
-        const Modulus m = mods[mi];
-        modup_value<LOGN, W>(work, smem, t, d, dst, m, hps);
+        const uint64_t q = mods[mi].q;
+        modup_value<LOGN, W>(work, smem, t, d, dst, q, hps);
         __syncthreads();
-        forward_cols<LOGN>(work, tile, t, m.q, tw_base + (size_t)mi * 2 * G::N);
+        forward_cols<LOGN>(work, tile, t, q, tw_base + (size_t)mi * 2 * G::N);
         store_tile<LOGN>(work, job.digit + (size_t)__ldg(d.dst_limb + dst) * G::N, tile, t);
     }
 }
@@ -128,10 +128,10 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, KW <= 4 ? 5 : 4)
     uint32_t hps[G::E];
     moddown_hps<LOGN, KW, FMA>(smem, t, pmods, K, hps);
     for (int qi = 0; qi < job.L; ++qi) {
-        const Modulus mq = mods[qi];
-        moddown_value<LOGN, KW>(work, smem, t, K, mq, job.inv + (size_t)qi * K, hps);
+        const uint64_t q = mods[qi].q;
+        moddown_value<LOGN, KW>(work, smem, t, K, q, job.inv + (size_t)qi * K, job.inv_s + (size_t)qi * K, hps);
         __syncthreads();
-        forward_cols<LOGN>(work, tile, t, mq.q, tw_base + (size_t)qi * 2 * G::N);
+        forward_cols<LOGN>(work, tile, t, q, tw_base + (size_t)qi * 2 * G::N);
         store_tile<LOGN>(work, job.out + (size_t)qi * G::N, tile, t);
     }
 }

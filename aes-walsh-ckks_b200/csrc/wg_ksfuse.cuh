@@ -158,27 +158,29 @@ WG_HD uint32_t hps_count(double alpha, int n) {
 
 // ModUp destination dst of the digit: thread t's coefficients into the work tile.
 // src_tiles holds the n scaled source tiles (stride PAD); W >= n bounds the digit width so the
-// dst row of constants stays in registers.  modup_coeff_w adds canonical Shoup products mod the
-// target modulus; the canonical residue of that sum is formed here from the 128-bit sum of the
-// plain products (each below 2^124, at most 16 of them) with one reduction.
+// dst row of constants stays in registers.
 template <int LOGN, int W, class Desc>
-WG_HD void modup_value(uint64_t* work, const uint64_t* src_tiles, int t, const Desc& d, int dst, const Modulus& m,
+WG_HD void modup_value(uint64_t* work, const uint64_t* src_tiles, int t, const Desc& d, int dst, uint64_t m,
                        const uint32_t* hps) {
     using G = Geom<LOGN>;
     const int n = d.src_count;
     const uint64_t* row = d.qhat + (size_t)dst * n;
+    const uint64_t* row_s = d.qhat_s + (size_t)dst * n;
     const uint64_t* corr = d.corr + (size_t)dst * (n + 1);
-    uint64_t w[W];
+    uint64_t w[W], ws[W];
 #pragma unroll
-    for (int i = 0; i < W; ++i) w[i] = i < n ? WG_LDG(row + i) : 0;
+    for (int i = 0; i < W; ++i) {
+        w[i] = i < n ? WG_LDG(row + i) : 0;
+        ws[i] = i < n ? WG_LDG(row_s + i) : 0;
+    }
 #pragma unroll
     for (int k = 0; k < G::E; ++k) {
         const int pe = ntt::pad16(t + k * G::THREADS);
-        Acc128 acc{0, 0};
+        uint64_t acc = 0;
 #pragma unroll
         for (int i = 0; i < W; ++i)
-            if (i < n) acc_mul(acc, src_tiles[(size_t)i * G::PAD + pe], w[i]);
-        work[pe] = sub_mod(reduce128(acc.hi, acc.lo, m), WG_LDG(corr + hps[k]), m.q);
+            if (i < n) acc = add_mod(acc, mul_shoup(src_tiles[(size_t)i * G::PAD + pe], w[i], ws[i], m), m);
+        work[pe] = sub_mod(acc, WG_LDG(corr + hps[k]), m);
     }
 }
 
@@ -208,24 +210,25 @@ WG_HD void moddown_hps(const uint64_t* p_tiles, int t, const Modulus* __restrict
 }
 
 // ModDown contribution for Q limb qi: thread t's coefficients into the work tile (canonical P
-// residues as for moddown_hps; KW >= K).  The canonical sum of moddown_all_limbs_k's Shoup
-// products, formed from the 128-bit sum of the plain products (each below 2^124, at most 16)
-// with one reduction.
+// residues as for moddown_hps; KW >= K).
 template <int LOGN, int KW>
-WG_HD void moddown_value(uint64_t* work, const uint64_t* p_tiles, int t, int K, const Modulus& mq,
-                         const uint64_t* __restrict__ iv, const uint32_t* hps) {
+WG_HD void moddown_value(uint64_t* work, const uint64_t* p_tiles, int t, int K, uint64_t q,
+                         const uint64_t* __restrict__ iv, const uint64_t* __restrict__ ivs, const uint32_t* hps) {
     using G = Geom<LOGN>;
-    uint64_t w[KW];
+    uint64_t w[KW], ws[KW];
 #pragma unroll
-    for (int pi = 0; pi < KW; ++pi) w[pi] = pi < K ? WG_LDG(iv + pi) : 0;
+    for (int pi = 0; pi < KW; ++pi) {
+        w[pi] = pi < K ? WG_LDG(iv + pi) : 0;
+        ws[pi] = pi < K ? WG_LDG(ivs + pi) : 0;
+    }
 #pragma unroll
     for (int k = 0; k < G::E; ++k) {
         const int pe = ntt::pad16(t + k * G::THREADS);
-        Acc128 acc{0, 0};
+        uint64_t acc = 0;
 #pragma unroll
         for (int pi = 0; pi < KW; ++pi)
-            if (pi < K) acc_mul(acc, p_tiles[(size_t)pi * G::PAD + pe], w[pi]);
-        work[pe] = sub_mod(reduce128(acc.hi, acc.lo, mq), (uint64_t)hps[k], mq.q);
+            if (pi < K) acc = add_mod(acc, mul_shoup(p_tiles[(size_t)pi * G::PAD + pe], w[pi], ws[pi], q), q);
+        work[pe] = sub_mod(acc, (uint64_t)hps[k], q);
     }
 }
 

@@ -177,7 +177,7 @@ void modup_fused(const Emu& E, const HostModUp& d, const uint64_t* src, uint64_t
         for (int dst = 0; dst < d.dst_count; ++dst) {
             const int mi = d.dst_mod[dst];
             for (int t = 0; t < G::THREADS; ++t)
-                ksf::modup_value<LOGN, 16>(work, smem.data(), t, d, dst, E.H.mods[mi], hps.data() + (size_t)t * G::E);
+                ksf::modup_value<LOGN, 16>(work, smem.data(), t, d, dst, E.H.mods[mi].q, hps.data() + (size_t)t * G::E);
             forward_cols<LOGN>(E, work, tile, mi);
             for (int t = 0; t < G::THREADS; ++t)
                 ksf::store_tile<LOGN>(work, digit + (size_t)d.dst_limb[dst] * G::N, tile, t);
@@ -205,8 +205,8 @@ void moddown_fused(const Emu& E, const uint64_t* src_p, uint64_t* out, int L, co
             ksf::moddown_hps<LOGN, 16>(smem.data(), t, pmods, K, hps.data() + (size_t)t * G::E);
         for (int qi = 0; qi < L; ++qi) {
             for (int t = 0; t < G::THREADS; ++t)
-                ksf::moddown_value<LOGN, 16>(work, smem.data(), t, K, E.H.mods[qi], inv + (size_t)qi * K,
-                                             hps.data() + (size_t)t * G::E);
+                ksf::moddown_value<LOGN, 16>(work, smem.data(), t, K, E.H.mods[qi].q, inv + (size_t)qi * K,
+                                             inv_s + (size_t)qi * K, hps.data() + (size_t)t * G::E);
             forward_cols<LOGN>(E, work, tile, qi);
             for (int t = 0; t < G::THREADS; ++t) ksf::store_tile<LOGN>(work, out + (size_t)qi * G::N, tile, t);
         }
