@@ -154,35 +154,6 @@ WG_HD uint64_t mont_mul(uint64_t normal, uint64_t mont, uint64_t q, uint64_t qni
     return u >= q ? u - q : u;
 }
 
-// A sum of Montgomery products kept as one 128-bit integer and reduced once: for canonical
-// factors (below q < 2^62) each product is below q^2, so up to 4 of them on top of a canonical
-// residue stay below q 2^64, the range in which the Montgomery reduction (mont_mul's second
-// half) returns x R^-1 mod q canonically.  acc_fold brings the sum back to a canonical residue of
-// the same class when more terms follow.  Since mont_mul and add_mod return canonical residues,
-// redc128 of the sum equals the chain of mont_mul / add_mod over the same terms in any order.
-struct Acc128 {
-    uint64_t lo, hi;
-};
-WG_HD void acc_mul(Acc128& a, uint64_t x, uint64_t y) {
-    const uint64_t lo = x * y;
-    const uint64_t hi = umulhi(x, y);
-    a.lo += lo;
-    a.hi += hi + (a.lo < lo ? 1ull : 0ull);
-}
-WG_HD uint64_t redc128(const Acc128& a, uint64_t q, uint64_t qninv) {
-    const uint64_t m = a.lo * qninv;
-    const uint64_t mq_lo = m * q;
-    const uint64_t mq_hi = umulhi(m, q);
-    const uint64_t lo = a.lo + mq_lo;
-    const uint64_t u = a.hi + mq_hi + (lo < a.lo ? 1ull : 0ull);
-    return u >= q ? u - q : u;
-}
-constexpr int kAccTerms = 4;  // products between folds
-WG_HD void acc_fold(Acc128& a, const Modulus& m) {
-    a.lo = reduce128(a.hi, a.lo, m);
-    a.hi = 0;
-}
-
 // reduce_mod_4q, add_mod_q, sub_mod_q (modarith.hpp:43-81).
 WG_HD uint64_t red4q(uint64_t x, uint64_t q) {
     const uint64_t two_q = q << 1;

@@ -38,8 +38,7 @@ def emu(tmp_path_factory):
     return E
 
 
-# one digit per Q limb: the key inner products run over 8 parts, past the point where the
-# 128-bit product sums are folded (Acc128, every 4 terms)
+# one digit per Q limb: the key inner products and ModUp run over 8 parts of one limb each
 MANY_DIGITS = dict(logN=10, q_bits=[40, 45, 45, 45, 50, 50, 50, 50], p_bits=[55], dnum=8, h=64)
 
 
