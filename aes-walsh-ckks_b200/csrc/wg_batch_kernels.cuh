@@ -3,7 +3,6 @@
 // Block (x, y + 65535 z) runs tile x (256 coefficients) of job y of a device job table.
 #pragma once
 #include <algorithm>
-#include <cmath>
 
 #include "wg_batch.hpp"
 #include "wg_internal.hpp"
@@ -263,15 +262,7 @@ struct RescaleJobs {
             uint64_t* dl = x + lv * N;
             drop.push_back({dl, dl, (int)lv, 0});
             if (fused) {
-                // a launch of few polynomials splits each one's remainder limbs over several
-                // blocks (each repeats the dropped limb's inverse column phase), so it runs at
-                // least about three waves of the 6 resident blocks per SM
-                const double per_poly = (double)(N >= 1024 ? N / 1024 : 1);
-                const double want = 3.0 * 6.0 * c.sm_count / ((double)polys.size() * per_poly);
-                const size_t parts = std::max<size_t>(1, std::min<size_t>(lv / 2, (size_t)std::ceil(want)));
-                for (size_t k = 0; k < parts; ++k)
-                    cols.push_back({dl, rem, c.rs_one_s[lv], (int)lv, (int)(k * lv / parts),
-                                    (int)((k + 1) * lv / parts), 0});
+                cols.push_back({dl, rem, c.rs_one_s[lv], (int)lv, 0});
                 for (size_t q = 0; q < lv; ++q)
                     rows.push_back({rem + q * N, nullptr, x + q * N, x + q * N, rc[lv + q], rc[2 * lv + q], (int)q,
                                     kEpiRescale});

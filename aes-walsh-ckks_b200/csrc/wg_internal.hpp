@@ -319,7 +319,6 @@ struct RescaleNttJob {
     uint64_t* rem;
     const uint64_t* rc;
     int lv;
-    int q0, q1;  // the remainders of limbs [q0, q1) (a polynomial's lv limbs may span several jobs)
     int pad;
 };
 // The forward row phase of job-table limbs with an element-wise epilogue (NttEpiJob, wg_ntt.cuh).

@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, 6)
     load_tile<LOGN>(drop, job.drop, tile, t);
     __syncthreads();
     inverse_cols<LOGN>(drop, tile, t, mp, tw_base + (size_t)lv * 2 * G::N + G::N);
-    for (int qi = job.q0; qi < job.q1; ++qi) {
+    for (int qi = 0; qi < lv; ++qi) {
         const uint64_t q = mods[qi].q;
         rescale_value<LOGN>(work, drop, t, mp.q, q, __ldg(job.rc + qi), __ldg(job.rc + 3 * lv + qi));
         __syncthreads();
