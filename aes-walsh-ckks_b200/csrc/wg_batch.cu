@@ -170,7 +170,6 @@ static KsPlan plan_keyswitch(const Context& c, const KsItem* items, size_t n, ui
         p.combine_bytes += 8.0 * N * L * (x.b_add + x.a_add + 6.0) + (gal ? 8.0 * N * L * 4.0 : 0.0);
     }
     close_group(n);
-    if (p.fused) split_moddown_jobs(c, moddown);
     p.intt_in = t.add(intt_in);
     p.n_intt_in = (int)intt_in.size();
     p.modup = t.add(modup);

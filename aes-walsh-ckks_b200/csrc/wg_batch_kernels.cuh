@@ -196,31 +196,6 @@ dim3 grid_for(const Context& c, size_t njobs) {
     return dim3((unsigned)(c.N / kT), (unsigned)std::min<size_t>(njobs, 65535), (unsigned)((njobs + 65534) / 65535));
 }
 
-// A fused ModDown launch runs one block per (job, column tile), each producing every Q limb of
-// its job, so few jobs leave most of the device idle in the last wave.  When the launch would
-// run fewer than three waves, each job's Q limbs are split over two blocks (both repeat the P
-// limbs' inverse column phase); the words are the same.
-inline void split_moddown_jobs(const Context& c, std::vector<ModDownJob>& md) {
-    const double tiles = (double)(c.N >= 1024 ? c.N / 1024 : 1);
-    const double resident = (c.np <= 4 ? 5.0 : 4.0) * c.sm_count;  // k_moddown_ntt's blocks per SM
-    if ((double)md.size() * tiles >= 3.0 * resident) return;
-    std::vector<ModDownJob> out;
-    out.reserve(2 * md.size());
-    for (const ModDownJob& j : md) {
-        if (j.L - j.q0 < 4) {
-            out.push_back(j);
-            continue;
-        }
-        const int mid = j.q0 + (j.L - j.q0) / 2;
-        ModDownJob lo = j, hi = j;
-        lo.L = mid;
-        hi.q0 = mid;
-        out.push_back(lo);
-        out.push_back(hi);
-    }
-    md.swap(out);
-}
-
 // The launches of one batched rescale (ckks_rescale, src/ckks/operations/arith/ckks_rescale.cpp:
 // 68-148) over polynomials of any levels: add() records a polynomial x at level lv with lv
 // remainder limbs of scratch, plan() puts the job tables into a JobTable, run() launches.

@@ -574,12 +574,6 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     const TermRef* j_terms = t.add(terms);
     const GiantJob* j_giant = t.add(giant_jobs);
     const NttJob* j_intt_pg = t.add(intt_pg);
-    // ModDown jobs before any split (algorithmic bytes count each output once)
-    const size_t n_single = md_single.size(), n_pair = md_pair.size();
-    if (fused) {
-        split_moddown_jobs(c, md_single);
-        split_moddown_jobs(c, md_pair);
-    }
     const ModDownJob* j_mds = t.add(md_single);
     const NttJob* j_ntt_cs = t.add(ntt_cs);
     const SubJob* j_kt_sub = t.add(kt_sub);
@@ -629,10 +623,10 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     // 4.
     if (!md_single.empty() && fused) {
         ntt_jobs_phase(c, t.at(j_intt_pg), (int)intt_pg.size(), false, false, s);
-        moddown_ntt_jobs(c, t.at(j_mds), (int)md_single.size(), 8.0 * N * (K + L) * n_single, s, false);
+        moddown_ntt_jobs(c, t.at(j_mds), (int)md_single.size(), 8.0 * N * (K + L) * md_single.size(), s, false);
         ntt_rows_epilogue_jobs(c, t.at(j_cs_epi), (int)cs_epi.size(), ntt_epilogue_bytes(cs_epi, N), s);
         ntt_jobs_phase(c, t.at(j_intt_kt), (int)intt_kt.size(), false, false, s);
-        modup_ntt_jobs(c, t.at(j_modup2), (int)modup2.size(), max_src, 8.0 * N * (double)(n_single * B * T),
+        modup_ntt_jobs(c, t.at(j_modup2), (int)modup2.size(), max_src, 8.0 * N * (double)(md_single.size() * B * T),
                        s);
         ntt_jobs_phase(c, t.at(j_ntt_dig2), (int)ntt_dig2.size(), true, false, s);
         Probe probe(kClsKeyMac, mac2_bytes, s);
@@ -667,7 +661,7 @@ void lt_stage_apply(Context& c, const LtStage& st, size_t count, uint64_t* const
     // 6.
     if (fused) {
         ntt_jobs_phase(c, t.at(j_intt_po), (int)intt_po.size(), false, false, s);
-        moddown_ntt_jobs(c, t.at(j_mdp), (int)md_pair.size(), 8.0 * N * (K + L) * n_pair, s);
+        moddown_ntt_jobs(c, t.at(j_mdp), (int)md_pair.size(), 8.0 * N * (K + L) * md_pair.size(), s);
         ntt_rows_epilogue_jobs(c, t.at(j_cf_epi), (int)cf_epi.size(), ntt_epilogue_bytes(cf_epi, N), s);
     } else {
         ntt_jobs(c, t.at(j_intt_po), (int)intt_po.size(), false, s);
@@ -793,8 +787,6 @@ void rotate_many_batch(Context& c, size_t level, size_t count, const uint64_t* c
     const NttJob* j3 = t.add(ntt_dig);
     const MacJob* j4 = t.add(mac);
     const NttJob* j5 = t.add(intt_p);
-    const size_t n_md = md.size();
-    if (fused) split_moddown_jobs(c, md);
     const ModDownJob* j6 = t.add(md);
     const NttJob* j7 = t.add(ntt_c);
     const CombineJob* j8 = t.add(comb);
@@ -823,7 +815,7 @@ void rotate_many_batch(Context& c, size_t level, size_t count, const uint64_t* c
         }
         if (fused) {
             ntt_jobs_phase(c, t.at(j5), (int)intt_p.size(), false, false, s);
-            moddown_ntt_jobs(c, t.at(j6), (int)md.size(), 8.0 * N * (K + L) * n_md, s);
+            moddown_ntt_jobs(c, t.at(j6), (int)md.size(), 8.0 * N * (K + L) * md.size(), s);
             ntt_rows_epilogue_jobs(c, t.at(j10), (int)c_epi.size(), ntt_epilogue_bytes(c_epi, N), s);
             Probe probe(kClsCombine, 8.0 * N * 4.0 * gath.size(), s);
             kb_gather<<<grid_for(c, gath.size()), kT, 0, s>>>(t.at(j9), (int)gath.size(), c.logN);

@@ -307,8 +307,8 @@ struct ModDownNttJob {
     uint64_t* out;
     const uint64_t* inv;  // folded P^-1 table of the level, [qi][pi]
     const uint64_t* inv_s;
-    int L;   // Q limbs [q0, L) are produced
-    int q0;  // 0 except for fused jobs split over blocks (split_moddown_jobs)
+    int L;
+    int pad;
 };
 // Rescale of one polynomial at level lv (ckks_rescale): drop holds its last limb after the
 // inverse row phase; the kernel finishes that inverse transform, forms the rounded remainder

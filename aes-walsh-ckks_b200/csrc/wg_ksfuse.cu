@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(Geom<LOGN>::THREADS, KW <= 4 ? 5 : 4)
     }
     uint32_t hps[G::E];
     moddown_hps<LOGN, KW, FMA>(smem, t, pmods, K, hps);
-    for (int qi = job.q0; qi < job.L; ++qi) {
+    for (int qi = 0; qi < job.L; ++qi) {
         const uint64_t q = mods[qi].q;
         moddown_value<LOGN, KW>(work, smem, t, K, q, job.inv + (size_t)qi * K, job.inv_s + (size_t)qi * K, hps);
         __syncthreads();
