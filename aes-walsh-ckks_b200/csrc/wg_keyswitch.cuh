@@ -86,27 +86,6 @@ WG_HD void modup_coeff(const Desc& d, const Modulus* __restrict__ mods, const ui
         modup_coeff_w<kMaxDigitWidth>(d, mods, src, digit, N, coeff);
 }
 
-// Folded ModDown contribution of one coefficient for Q limb qi:
-//   (sum_j [x_j mod q] * inv_j) - round(sum_j x_j / p_j)   (mod q)
-WG_HD uint64_t moddown_coeff(const Modulus& mq, const Modulus* __restrict__ pmods, int K,
-                             const uint64_t* __restrict__ src_p, size_t N, size_t coeff,
-                             const uint64_t* __restrict__ inv, const uint64_t* __restrict__ inv_s) {
-    const uint64_t q = mq.q;
-    uint64_t acc = 0;
-    double alpha = 0.0;
-    for (int pi = 0; pi < K; ++pi) {
-        const uint64_t s = red4q(src_p[(size_t)pi * N + coeff], pmods[pi].q);
-        alpha = dfma(u2d(s), pmods[pi].inv_q, alpha);
-        // the reference reduces s mod q first (barrett_reduce_u64); the Shoup product is the
-        // canonical residue of s * inv for any 64-bit s, so the reduction cannot change it
-        const uint64_t term = mul_shoup(s, WG_LDG(inv + pi), WG_LDG(inv_s + pi), q);
-        acc = add_mod(acc, term, q);
-    }
-    uint64_t hps = round_half_up(alpha);
-    if (hps > (uint64_t)K) hps = (uint64_t)K;
-    return sub_mod(acc, hps, q);
-}
-
 // moddown_all_limbs for at most KW P limbs (the P residues stay in registers).
 template <bool FUSED, int KW>
 WG_HD void moddown_all_limbs_k(const Modulus* __restrict__ mods, int nq, int L, int K,
@@ -140,9 +119,12 @@ WG_HD void moddown_all_limbs_k(const Modulus* __restrict__ mods, int nq, int L, 
     }
 }
 
-// Folded ModDown of one coefficient for Q limbs [0, L): the P residues are read and the FP64
-// alpha estimate formed once, then each limb gets its Shoup dot product (same arithmetic as
-// moddown_coeff, which recomputes both per limb).  out[qi * N + coeff] = contribution.
+// Folded ModDown of one coefficient for Q limbs [0, L):
+//   contribution_qi = (sum_j [x_j mod q_i] inv_ij) - round(sum_j x_j / p_j)   (mod q_i)
+// The P residues are read and the FP64 alpha estimate formed once, then each limb gets its Shoup
+// dot product (the reference reduces x_j mod q_i first with barrett_reduce_u64; the Shoup product
+// is the canonical residue of x_j inv_ij for any 64-bit x_j, so that reduction cannot change a
+// word).  out[qi * N + coeff] = contribution.
 // FUSED selects how the alpha sum is rounded: the reference's pair ModDown
 // (ckks_keyswitch.cpp:521-607) is compiled into an FMA, its single-polynomial ModDown
 // (ckks_keyswitch.cpp:609-673, used by the QP linear transform) into a multiply and an add.
