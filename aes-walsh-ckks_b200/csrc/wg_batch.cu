@@ -4,7 +4,8 @@
 // Each stage reads a table of small jobs (pointers, modulus index, constants) from device
 // memory; block (x, y + 65535 z) runs tile x of job y.  All tables of a call are built on the
 // host, staged in pinned memory and uploaded with one copy, so a batched key switch over 64
-// ciphertexts is 9 launches (13 with the NTT steps unfused) instead of 9-13 per ciphertext.
+// ciphertexts is 7-8 launches (12-13 with the NTT steps unfused) instead of that many per
+// ciphertext.
 // Arithmetic is shared with the single-ciphertext path (wg_keyswitch.cuh, wg_arith.cuh), so
 // results are identical.
 #include <algorithm>
