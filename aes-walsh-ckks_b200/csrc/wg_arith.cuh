@@ -143,14 +143,14 @@ WG_HD uint64_t barrett_u64(uint64_t a, uint64_t q, uint64_t mu_hi) {
 }
 
 // ckks_montgomery_mul_normal_by_montgomery (modarith.hpp:116-130).
+// qninv = -q^-1 mod 2^64, so m q = -t_lo (mod 2^64): the low words of t + m q sum to 0, with a
+// carry exactly when t_lo != 0, and the low product m q need not be formed.
 WG_HD uint64_t mont_mul(uint64_t normal, uint64_t mont, uint64_t q, uint64_t qninv) {
     const uint64_t t_lo = normal * mont;
     const uint64_t t_hi = umulhi(normal, mont);
     const uint64_t m = t_lo * qninv;
-    const uint64_t mq_lo = m * q;
     const uint64_t mq_hi = umulhi(m, q);
-    const uint64_t lo = t_lo + mq_lo;
-    uint64_t u = t_hi + mq_hi + (lo < t_lo ? 1ull : 0ull);
+    uint64_t u = t_hi + mq_hi + (t_lo != 0 ? 1ull : 0ull);
     return u >= q ? u - q : u;
 }
 

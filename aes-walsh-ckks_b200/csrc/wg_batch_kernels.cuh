@@ -96,12 +96,11 @@ __global__ void __launch_bounds__(kT) kb_mac(const MacJob* jobs, int n, const Mo
               j->acc, N, j->i, coeff);
 }
 
-// acc_{a,b}[i] = sum_parts REDC(digit_part[i] * key_part_{a,b}[i]) for every switch of the group,
-// parts accumulated in order as in mac_accumulate (wg_keyswitch.cuh).
-__global__ void __launch_bounds__(kT) kb_mac_group(const MacGroupJob* jobs, int n, const Modulus* mods, int nq,
-                                                   size_t N) {
-    const MacGroupJob* j = job_of(jobs, n);
-    if (!j) return;
+// acc_{a,b}[i] = sum_parts REDC(digit_part[i] * key_part_{a,b}[i]) for the NC switches of a group,
+// parts accumulated in order as in mac_accumulate (wg_keyswitch.cuh).  NC is a compile-time
+// count so that every digit load of a part is unconditional and all of them are in flight at once.
+template <int NC>
+__device__ __forceinline__ void mac_group(const MacGroupJob* j, const Modulus* mods, int nq, size_t N) {
     const size_t coeff = (size_t)blockIdx.x * kT + threadIdx.x;
     const int i = j->i, L = j->L, K = j->K, T = L + K;
     const bool is_p = i >= L;
@@ -110,27 +109,44 @@ __global__ void __launch_bounds__(kT) kb_mac_group(const MacGroupJob* jobs, int 
     const size_t key_limbs = (size_t)j->key_level + 1 + K;
     const size_t klimb = is_p ? (size_t)j->key_level + 1 + (i - L) : (size_t)i;
     const size_t at = (size_t)i * N + coeff;
-    uint64_t acc_a[kMacGroup], acc_b[kMacGroup];
+    uint64_t acc_a[NC], acc_b[NC];
 #pragma unroll
-    for (int c = 0; c < kMacGroup; ++c) acc_a[c] = acc_b[c] = 0;
+    for (int c = 0; c < NC; ++c) acc_a[c] = acc_b[c] = 0;
     for (int p = 0; p < j->parts; ++p) {
         const int s0 = p * j->alpha, s1 = s0 + j->alpha < L ? s0 + j->alpha : L;
         const bool own = !is_p && i >= s0 && i < s1;
         const uint64_t ka = j->key[(((size_t)p * 2 + 0) * key_limbs + klimb) * N + coeff];
         const uint64_t kb = j->key[(((size_t)p * 2 + 1) * key_limbs + klimb) * N + coeff];
+        uint64_t d[NC];
 #pragma unroll
-        for (int c = 0; c < kMacGroup; ++c) {
-            if (c >= j->n) break;
-            const uint64_t d = own ? j->key_term[c][at] : j->digits[c][p * j->part_stride + at];
-            acc_a[c] = add_mod(acc_a[c], mont_mul(d, ka, q, qninv), q);
-            acc_b[c] = add_mod(acc_b[c], mont_mul(d, kb, q, qninv), q);
+        for (int c = 0; c < NC; ++c) d[c] = own ? j->key_term[c][at] : j->digits[c][p * j->part_stride + at];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            acc_a[c] = add_mod(acc_a[c], mont_mul(d[c], ka, q, qninv), q);
+            acc_b[c] = add_mod(acc_b[c], mont_mul(d[c], kb, q, qninv), q);
         }
     }
 #pragma unroll
-    for (int c = 0; c < kMacGroup; ++c) {
-        if (c >= j->n) break;
+    for (int c = 0; c < NC; ++c) {
         j->acc[c][at] = acc_a[c];
         j->acc[c][(size_t)T * N + at] = acc_b[c];
+    }
+}
+
+__global__ void __launch_bounds__(kT, 3) kb_mac_group(const MacGroupJob* jobs, int n, const Modulus* mods, int nq,
+                                                      size_t N) {
+    const MacGroupJob* j = job_of(jobs, n);
+    if (!j) return;
+    static_assert(kMacGroup == 8, "one case per group size");
+    switch (j->n) {  // the same for every thread of the block
+        case 1: mac_group<1>(j, mods, nq, N); break;
+        case 2: mac_group<2>(j, mods, nq, N); break;
+        case 3: mac_group<3>(j, mods, nq, N); break;
+        case 4: mac_group<4>(j, mods, nq, N); break;
+        case 5: mac_group<5>(j, mods, nq, N); break;
+        case 6: mac_group<6>(j, mods, nq, N); break;
+        case 7: mac_group<7>(j, mods, nq, N); break;
+        default: mac_group<8>(j, mods, nq, N); break;
     }
 }
 

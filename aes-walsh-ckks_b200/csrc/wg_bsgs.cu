@@ -120,12 +120,13 @@ struct AccumJob {
     int ngiants, i, pad0, pad1;
 };
 
-__global__ void __launch_bounds__(kT) kb_baby(const BabyJob* jobs, int n, const CtRef* __restrict__ cts,
-                                              const uint64_t* __restrict__ digits, uint64_t* __restrict__ babies,
-                                              const Modulus* mods, int nq, int L, int K, int parts, int alpha,
-                                              int nslots, int logN) {
-    const BabyJob* j = job_of(jobs, n);
-    if (!j) return;
+// NC (the ciphertexts of the job) is a compile-time count so that every digit load of a part is
+// unconditional and all of them are in flight at once.
+template <int NC>
+__device__ __forceinline__ void baby_step(const BabyJob* j, const CtRef* __restrict__ cts,
+                                          const uint64_t* __restrict__ digits, uint64_t* __restrict__ babies,
+                                          const Modulus* mods, int nq, int L, int K, int parts, int alpha,
+                                          int nslots, int logN) {
     const size_t N = size_t{1} << logN;
     const uint32_t x = blockIdx.x * kT + threadIdx.x;
     const int i = j->i;
@@ -137,35 +138,57 @@ __global__ void __launch_bounds__(kT) kb_baby(const BabyJob* jobs, int n, const 
     const size_t klimb = is_p ? (size_t)j->key_level + 1 + (i - L) : (size_t)i;
     const size_t part_stride = (size_t)T * N;
     const size_t limb = (size_t)i * N + x;
-    uint64_t acc_a[kGiantBatch], acc_b[kGiantBatch];
+    const CtRef* ct = cts + j->c0;
+    uint64_t acc_a[NC], acc_b[NC];
 #pragma unroll
-    for (int c = 0; c < kGiantBatch; ++c) {
+    for (int c = 0; c < NC; ++c) {
         acc_a[c] = 0;
-        acc_b[c] = (c < j->nc && !is_p) ? cts[j->c0 + c].b[limb] : 0;
+        acc_b[c] = is_p ? 0 : ct[c].b[limb];
     }
     for (int p = 0; p < parts; ++p) {
         const int s0 = p * alpha, s1 = s0 + alpha < L ? s0 + alpha : L;
         const bool own = !is_p && i >= s0 && i < s1;  // source limb: the key term itself
         const uint64_t ka = j->key[(((size_t)p * 2 + 0) * key_limbs + klimb) * N + x];
         const uint64_t kb = j->key[(((size_t)p * 2 + 1) * key_limbs + klimb) * N + x];
+        uint64_t d[NC];
 #pragma unroll
-        for (int c = 0; c < kGiantBatch; ++c) {
-            if (c >= j->nc) break;
-            const int ci = j->c0 + c;
-            const uint64_t d = own ? cts[ci].a[limb] : digits[((size_t)ci * parts + p) * part_stride + limb];
-            acc_a[c] = add_mod(acc_a[c], mont_mul(d, ka, q, qninv), q);
-            acc_b[c] = add_mod(acc_b[c], mont_mul(d, kb, q, qninv), q);
+        for (int c = 0; c < NC; ++c)
+            d[c] = own ? ct[c].a[limb] : digits[((size_t)(j->c0 + c) * parts + p) * part_stride + limb];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            acc_a[c] = add_mod(acc_a[c], mont_mul(d[c], ka, q, qninv), q);
+            acc_b[c] = add_mod(acc_b[c], mont_mul(d[c], kb, q, qninv), q);
         }
     }
     const uint32_t dst = automorphism_src(x, j->galois_inv, logN);
     const size_t slot_words = 2 * (size_t)T * N;
 #pragma unroll
-    for (int c = 0; c < kGiantBatch; ++c) {
-        if (c >= j->nc) break;
+    for (int c = 0; c < NC; ++c) {
         uint64_t* o = babies + ((size_t)(j->c0 + c) * nslots + j->slot) * slot_words + (size_t)i * N;
         o[dst] = acc_a[c];
         o[(size_t)T * N + dst] = acc_b[c];
     }
+}
+
+__global__ void __launch_bounds__(kT, 3) kb_baby(const BabyJob* jobs, int n, const CtRef* __restrict__ cts,
+                                                 const uint64_t* __restrict__ digits, uint64_t* __restrict__ babies,
+                                                 const Modulus* mods, int nq, int L, int K, int parts, int alpha,
+                                                 int nslots, int logN) {
+    const BabyJob* j = job_of(jobs, n);
+    if (!j) return;
+    static_assert(kGiantBatch == 8, "one case per batch size");
+#define WG_BABY(NC) baby_step<NC>(j, cts, digits, babies, mods, nq, L, K, parts, alpha, nslots, logN)
+    switch (j->nc) {  // the same for every thread of the block
+        case 1: WG_BABY(1); break;
+        case 2: WG_BABY(2); break;
+        case 3: WG_BABY(3); break;
+        case 4: WG_BABY(4); break;
+        case 5: WG_BABY(5); break;
+        case 6: WG_BABY(6); break;
+        case 7: WG_BABY(7); break;
+        default: WG_BABY(8); break;
+    }
+#undef WG_BABY
 }
 
 // Giant-step inner sums: inner[c][g] = sum over the terms (g, slot) of diag x baby[c][slot], in
