@@ -353,7 +353,7 @@ static void launch_pipeline(const Context& c, const PipelinePlan& P, cudaStream_
     const JobTable& t = P.t;
     {
         Probe probe(kClsElementwise, P.tb, s);
-        kb_tensor<<<grid_for(c, P.nt), kT, 0, s>>>(t.at(P.jt), P.nt, c.d_mod);
+        kb_tensor<<<grid_wide(c, P.nt), kT, 0, s>>>(t.at(P.jt), P.nt, c.d_mod);
     }
     run_keyswitch(c, P.p1, t, s);
     P.rescale->run(c, t, s);

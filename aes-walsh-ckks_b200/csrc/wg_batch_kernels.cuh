@@ -75,6 +75,16 @@ struct RescaleFinishJob {
     int mod, pad;
 };
 
+// The elementwise kernels take kWide words per thread, kT x kWide coefficients per block (N is at
+// least 1024): a thread's loads all go out before its arithmetic, and a block outlives its read of
+// the job table by more than one word.  Word r of a thread is wide_index(r), so each of the kWide
+// loads of a warp is coalesced.  These kernels (kb_tensor here; kb_scalar, kb_lincomb, kb_pmul,
+// kb_copy and kb_add in wg_ctops.cuh) are launched with grid_wide only.
+constexpr int kWide = 4;
+__device__ __forceinline__ size_t wide_index(int r) {
+    return ((size_t)blockIdx.x * kWide + r) * kT + threadIdx.x;
+}
+
 template <class J>
 __device__ __forceinline__ const J* job_of(const J* jobs, int n) {
     const int j = blockIdx.y + 65535 * blockIdx.z;
@@ -178,13 +188,21 @@ __global__ void __launch_bounds__(kT) kb_gather(const GatherJob* jobs, int n, in
 __global__ void __launch_bounds__(kT) kb_tensor(const TensorJob* jobs, int n, const Modulus* mods) {
     const TensorJob* j = job_of(jobs, n);
     if (!j) return;
-    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
     const Modulus m = mods[j->mod];
-    const uint64_t xa = j->a1[k], xb = j->b1[k], ya = j->a2[k], yb = j->b2[k];
-    j->c2[k] = barrett_mul(xa, ya, m);
-    const uint64_t tmp = barrett_mul(xb, ya, m);
-    j->b1[k] = barrett_mul(xb, yb, m);
-    j->a1[k] = add_mod(barrett_mul(xa, yb, m), tmp, m.q);
+    uint64_t xa[kWide], xb[kWide], ya[kWide], yb[kWide];
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) {
+        const size_t k = wide_index(r);
+        xa[r] = j->a1[k], xb[r] = j->b1[k], ya[r] = j->a2[k], yb[r] = j->b2[k];
+    }
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) {
+        const size_t k = wide_index(r);
+        j->c2[k] = barrett_mul(xa[r], ya[r], m);
+        const uint64_t tmp = barrett_mul(xb[r], ya[r], m);
+        j->b1[k] = barrett_mul(xb[r], yb[r], m);
+        j->a1[k] = add_mod(barrett_mul(xa[r], yb[r], m), tmp, m.q);
+    }
 }
 
 // Same two steps as k_rescale_prep / k_rescale_finish in wg_ops.cu.
@@ -210,6 +228,11 @@ __global__ void __launch_bounds__(kT) kb_rescale_finish(const RescaleFinishJob* 
 
 dim3 grid_for(const Context& c, size_t njobs) {
     return dim3((unsigned)(c.N / kT), (unsigned)std::min<size_t>(njobs, 65535), (unsigned)((njobs + 65534) / 65535));
+}
+// The grid of the kWide-words-per-thread kernels.
+dim3 grid_wide(const Context& c, size_t njobs) {
+    return dim3((unsigned)(c.N / (kT * kWide)), (unsigned)std::min<size_t>(njobs, 65535),
+                (unsigned)((njobs + 65534) / 65535));
 }
 
 // The launches of one batched rescale (ckks_rescale, src/ckks/operations/arith/ckks_rescale.cpp:

@@ -191,12 +191,43 @@ __global__ void __launch_bounds__(kT, 3) kb_baby(const BabyJob* jobs, int n, con
 #undef WG_BABY
 }
 
+// Adds one term's products to the accumulator pair of its giant step.  g is the same for every
+// thread of the block (one job per block), so this is a uniform branch to that pair; the
+// accumulators keep constant indices and stay in registers.
+__device__ __forceinline__ void giant_add(int g, uint64_t pa, uint64_t pb, uint64_t q, uint64_t* acc_a,
+                                          uint64_t* acc_b) {
+    static_assert(kGiantGroup == 8, "one case per giant step of a group");
+    switch (g) {
+#define WG_GIANT_ADD(G)                          \
+    case G:                                      \
+        acc_a[G] = add_mod(acc_a[G], pa, q);     \
+        acc_b[G] = add_mod(acc_b[G], pb, q);     \
+        break;
+        WG_GIANT_ADD(0)
+        WG_GIANT_ADD(1)
+        WG_GIANT_ADD(2)
+        WG_GIANT_ADD(3)
+        WG_GIANT_ADD(4)
+        WG_GIANT_ADD(5)
+        WG_GIANT_ADD(6)
+        WG_GIANT_ADD(7)
+#undef WG_GIANT_ADD
+        default:
+            break;
+    }
+}
+
 // Giant-step inner sums: inner[c][g] = sum over the terms (g, slot) of diag x baby[c][slot], in
 // QP.  Montgomery products and modular additions of canonical residues, so the order of the
 // terms does not change the canonical sums.
-__global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, const TermRef* __restrict__ term_table,
-                                               const Modulus* mods, int nq, int L, int T, int nslots, int ngiants,
-                                               size_t N) {
+// The terms go kGiantUnroll at a time: their table entries, then all their diagonal and baby-step
+// words, then the products, so each warp has that many HBM loads in flight rather than one
+// dependent chain per term (a baby-step word shared by consecutive terms is read again from L1).
+constexpr int kGiantUnroll = 4;
+
+__global__ void __launch_bounds__(kT, 3) kb_giant(const GiantJob* jobs, int n, const TermRef* __restrict__ term_table,
+                                                  const Modulus* mods, int nq, int L, int T, int nslots, int ngiants,
+                                                  size_t N) {
     const GiantJob* j = job_of(jobs, n);
     if (!j) return;
     const size_t x = (size_t)blockIdx.x * kT + threadIdx.x;
@@ -208,42 +239,32 @@ __global__ void __launch_bounds__(kT) kb_giant(const GiantJob* jobs, int n, cons
     uint64_t acc_a[kGiantGroup], acc_b[kGiantGroup];
 #pragma unroll
     for (int g = 0; g < kGiantGroup; ++g) acc_a[g] = acc_b[g] = 0;
-    const uint64_t* babies = j->babies + (size_t)j->c * nslots * slot_words;
-    int slot = -1;
-    uint64_t ba = 0, bb = 0;
-    for (int t = 0; t < j->nterms; ++t) {
-        const TermRef tr = term_table[j->term0 + t];
-        if (tr.slot != slot) {
-            slot = tr.slot;
-            const uint64_t* bs = babies + (size_t)slot * slot_words;
-            ba = bs[limb];
-            bb = bs[(size_t)T * N + limb];
+    const uint64_t* babies = j->babies + (size_t)j->c * nslots * slot_words + limb;
+    const TermRef* terms = term_table + j->term0;
+    const int nterms = j->nterms;
+    int t = 0;
+    for (; t + kGiantUnroll <= nterms; t += kGiantUnroll) {
+        TermRef tr[kGiantUnroll];
+        uint64_t d[kGiantUnroll], ba[kGiantUnroll], bb[kGiantUnroll];
+#pragma unroll
+        for (int u = 0; u < kGiantUnroll; ++u) tr[u] = terms[t + u];
+#pragma unroll
+        for (int u = 0; u < kGiantUnroll; ++u) {
+            const uint64_t* bs = babies + (size_t)tr[u].slot * slot_words;
+            d[u] = tr[u].diag[limb];
+            ba[u] = bs[0];
+            bb[u] = bs[(size_t)T * N];
         }
-        const uint64_t d = tr.diag[limb];
-        const uint64_t pa = mont_mul(ba, d, q, qninv), pb = mont_mul(bb, d, q, qninv);
-        // tr.g is the same for every thread of the block (one job per block), so this is a
-        // uniform branch to the one accumulator pair the term adds to; the accumulators keep
-        // constant indices and stay in registers
-        switch (tr.g) {
-#define WG_GIANT_ADD(G)                          \
-    case G:                                      \
-        acc_a[G] = add_mod(acc_a[G], pa, q);     \
-        acc_b[G] = add_mod(acc_b[G], pb, q);     \
-        break;
-            WG_GIANT_ADD(0)
-            WG_GIANT_ADD(1)
-            WG_GIANT_ADD(2)
-            WG_GIANT_ADD(3)
-            WG_GIANT_ADD(4)
-            WG_GIANT_ADD(5)
-            WG_GIANT_ADD(6)
-            WG_GIANT_ADD(7)
-#undef WG_GIANT_ADD
-            default:
-                break;
-        }
+#pragma unroll
+        for (int u = 0; u < kGiantUnroll; ++u)
+            giant_add(tr[u].g, mont_mul(ba[u], d[u], q, qninv), mont_mul(bb[u], d[u], q, qninv), q, acc_a, acc_b);
     }
-    static_assert(kGiantGroup == 8, "one case per giant step of a group");
+    for (; t < nterms; ++t) {
+        const TermRef tr = terms[t];
+        const uint64_t* bs = babies + (size_t)tr.slot * slot_words;
+        const uint64_t d = tr.diag[limb];
+        giant_add(tr.g, mont_mul(bs[0], d, q, qninv), mont_mul(bs[(size_t)T * N], d, q, qninv), q, acc_a, acc_b);
+    }
 #pragma unroll
     for (int g = 0; g < kGiantGroup; ++g) {
         if (g >= j->ng) break;

@@ -35,14 +35,24 @@ struct ScalarJob {
 __global__ void __launch_bounds__(kT) kb_scalar(const ScalarJob* jobs, int n, const Modulus* mods) {
     const ScalarJob* j = job_of(jobs, n);
     if (!j) return;
-    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
-    const uint64_t q = mods[j->mod].q;
-    if (j->op == kScalarMul)
-        j->x[k] = mul_shoup(j->x[k], j->s, j->s_shoup, q);
-    else if (j->op == kScalarMulAdd)
-        j->x[k] = add_mod(j->x[k], mul_shoup(j->y[k], j->s, j->s_shoup, q), q);
-    else
-        j->x[k] = add_mod(j->x[k], j->s, q);
+    const uint64_t q = mods[j->mod].q, s = j->s, ss = j->s_shoup;
+    uint64_t x[kWide], y[kWide];
+    if (j->op == kScalarMul) {
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) x[r] = j->x[wide_index(r)];
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) j->x[wide_index(r)] = mul_shoup(x[r], s, ss, q);
+    } else if (j->op == kScalarMulAdd) {
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) x[r] = j->x[wide_index(r)], y[r] = j->y[wide_index(r)];
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) j->x[wide_index(r)] = add_mod(x[r], mul_shoup(y[r], s, ss, q), q);
+    } else {
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) x[r] = j->x[wide_index(r)];
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) j->x[wide_index(r)] = add_mod(x[r], s, q);
+    }
 }
 
 constexpr int kMaxLincombTerms = 16;
@@ -61,11 +71,23 @@ struct LincombJob {
 __global__ void __launch_bounds__(kT) kb_lincomb(const LincombJob* jobs, int n, const Modulus* mods) {
     const LincombJob* j = job_of(jobs, n);
     if (!j) return;
-    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
     const uint64_t q = mods[j->mod].q;
-    uint64_t acc = add_mod(j->accumulate ? j->out[k] : 0, j->add, q);
-    for (int t = 0; t < j->n; ++t) acc = add_mod(acc, mul_shoup(j->src[t][k], j->c[t], j->cs[t], q), q);
-    j->out[k] = acc;
+    uint64_t acc[kWide];
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) acc[r] = j->accumulate ? j->out[wide_index(r)] : 0;
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) acc[r] = add_mod(acc[r], j->add, q);
+    for (int t = 0; t < j->n; ++t) {
+        const uint64_t* src = j->src[t];
+        const uint64_t c = j->c[t], cs = j->cs[t];
+        uint64_t v[kWide];
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) v[r] = src[wide_index(r)];
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) acc[r] = add_mod(acc[r], mul_shoup(v[r], c, cs, q), q);
+    }
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) j->out[wide_index(r)] = acc[r];
 }
 
 struct PmulJob {
@@ -78,8 +100,12 @@ struct PmulJob {
 __global__ void __launch_bounds__(kT) kb_pmul(const PmulJob* jobs, int n, const Modulus* mods) {
     const PmulJob* j = job_of(jobs, n);
     if (!j) return;
-    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
-    j->x[k] = barrett_mul(j->x[k], j->p[k], mods[j->mod]);
+    const Modulus m = mods[j->mod];
+    uint64_t x[kWide], p[kWide];
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) x[r] = j->x[wide_index(r)], p[r] = j->p[wide_index(r)];
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) j->x[wide_index(r)] = barrett_mul(x[r], p[r], m);
 }
 
 struct CopyJob {
@@ -90,8 +116,11 @@ struct CopyJob {
 __global__ void __launch_bounds__(kT) kb_copy(const CopyJob* jobs, int n) {
     const CopyJob* j = job_of(jobs, n);
     if (!j) return;
-    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
-    j->dst[k] = j->src[k];
+    uint64_t v[kWide];
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) v[r] = j->src[wide_index(r)];
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) j->dst[wide_index(r)] = v[r];
 }
 
 struct AddJob {
@@ -104,9 +133,17 @@ struct AddJob {
 __global__ void __launch_bounds__(kT) kb_add(const AddJob* jobs, int n, const Modulus* mods) {
     const AddJob* j = job_of(jobs, n);
     if (!j) return;
-    const size_t k = (size_t)blockIdx.x * kT + threadIdx.x;
     const uint64_t q = mods[j->mod].q;
-    j->x[k] = j->sub ? sub_mod(j->x[k], j->y[k], q) : add_mod(j->x[k], j->y[k], q);
+    uint64_t x[kWide], y[kWide];
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) x[r] = j->x[wide_index(r)], y[r] = j->y[wide_index(r)];
+    if (j->sub) {
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) j->x[wide_index(r)] = sub_mod(x[r], y[r], q);
+    } else {
+#pragma unroll
+        for (int r = 0; r < kWide; ++r) j->x[wide_index(r)] = add_mod(x[r], y[r], q);
+    }
 }
 
 // A batch of ciphertexts with common metadata.  Polynomial k of ciphertext i lives at p[i][k]
@@ -172,7 +209,7 @@ public:
         const CopyJob* j = t.add(jobs);
         t.upload(c_, s_);
         Probe probe(kClsElementwise, 16.0 * N * jobs.size(), s_);
-        kb_copy<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size());
+        kb_copy<<<grid_wide(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size());
         check_cuda(cudaGetLastError(), "batched copy");
         return y;
     }
@@ -202,7 +239,7 @@ public:
         const TensorJob* j = t.add(jobs);
         t.upload(c_, s_);
         Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 7.0, s_);
-        kb_tensor<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        kb_tensor<<<grid_wide(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
         check_cuda(cudaGetLastError(), "evalpoly tensor");
     }
 
@@ -264,7 +301,7 @@ public:
         const AddJob* j = t.add(jobs);
         t.upload(c_, s_);
         Probe probe(kClsElementwise, 8.0 * c_.N * jobs.size() * 3.0, s_);
-        kb_add<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        kb_add<<<grid_wide(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
         check_cuda(cudaGetLastError(), "batched add");
     }
 
@@ -288,7 +325,7 @@ public:
         const ScalarJob* j = t.add(jobs);
         t.upload(c_, s_);
         Probe probe(kClsElementwise, 8.0 * N * jobs.size() * (op == kScalarMulAdd ? 3.0 : 2.0), s_);
-        kb_scalar<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        kb_scalar<<<grid_wide(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
         check_cuda(cudaGetLastError(), "evalpoly scalar");
     }
 
@@ -334,7 +371,7 @@ public:
             double words = 0;
             for (const auto& jb : jobs) words += jb.n + 1 + jb.accumulate;
             Probe probe(kClsElementwise, 8.0 * N * words, s_);
-            kb_lincomb<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+            kb_lincomb<<<grid_wide(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
             check_cuda(cudaGetLastError(), "linear combination");
         }
         return out;
@@ -514,7 +551,7 @@ public:
         const PmulJob* j = t.add(jobs);
         t.upload(c_, s_);
         Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 3.0, s_);
-        kb_pmul<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        kb_pmul<<<grid_wide(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
         check_cuda(cudaGetLastError(), "plaintext multiply");
     }
 
@@ -529,7 +566,7 @@ public:
         const PmulJob* j = t.add(jobs);
         t.upload(c_, s_);
         Probe probe(kClsElementwise, 8.0 * N * jobs.size() * 3.0, s_);
-        kb_pmul<<<grid_for(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
+        kb_pmul<<<grid_wide(c_, jobs.size()), kT, 0, s_>>>(t.at(j), (int)jobs.size(), c_.d_mod);
         check_cuda(cudaGetLastError(), "evalpoly plaintext multiply");
     }
 

@@ -239,7 +239,9 @@ namespace {
 constexpr size_t kStateBits = 128;
 constexpr size_t kAesRounds = 10;
 
-template <class Job, class Kernel>
+// One launch of `kernel` over a job table.  wide: the kernel takes kWide words per thread
+// (kb_scalar, kb_pmul, kb_add: grid_wide); otherwise one word per thread (grid_for).
+template <bool wide = false, class Job, class Kernel>
 void launch_jobs(Context& c, const std::vector<Job>& jobs, Kernel kernel, double bytes_per_job, const char* what,
                  cudaStream_t s) {
     if (jobs.empty()) return;
@@ -247,7 +249,8 @@ void launch_jobs(Context& c, const std::vector<Job>& jobs, Kernel kernel, double
     const Job* j = t.add(jobs);
     t.upload(c, s);
     Probe probe(kClsElementwise, bytes_per_job * (double)jobs.size(), s);
-    kernel<<<grid_for(c, jobs.size()), kT, 0, s>>>(t.at(j), (int)jobs.size(), c.d_mod);
+    const dim3 grid = wide ? grid_wide(c, jobs.size()) : grid_for(c, jobs.size());
+    kernel<<<grid, kT, 0, s>>>(t.at(j), (int)jobs.size(), c.d_mod);
     check_cuda(cudaGetLastError(), what);
 }
 
@@ -334,7 +337,7 @@ public:
                     one.push_back({x.b + l * N, nullptr, scaled_integer_mod(1, ks, c_.q[l]), 0, (int)l, kScalarAdd});
         }
         launch_jobs(c_, copy, kb_linear, 16.0 * N, "ckks_aes initial copy", s_);
-        launch_jobs(c_, one, kb_scalar, 16.0 * N, "ckks_aes initial constant", s_);
+        launch_jobs<true>(c_, one, kb_scalar, 16.0 * N, "ckks_aes initial constant", s_);
         if (varying.empty()) return;
         const size_t nv = varying.size();
         // sign selectors at scale q_L (level L) and the bit planes at the parameter scale (level L - 1)
@@ -362,7 +365,7 @@ public:
             for (int poly = 0; poly < 2; ++poly)
                 for (size_t l = 0; l <= L; ++l) mul.push_back({(poly ? x.a : x.b) + l * N, signs[k] + l * N, (int)l, 0});
         }
-        launch_jobs(c_, mul, kb_pmul, 24.0 * N, "ckks_aes sign selector", s_);
+        launch_jobs<true>(c_, mul, kb_pmul, 24.0 * N, "ckks_aes sign selector", s_);
         v.np = 2;
         v.level = L;
         v.cap = L + 1;
@@ -375,7 +378,7 @@ public:
                       static_cast<long double>(c_.q[L]);
             for (size_t l = 0; l < L; ++l) add.push_back({x.b + l * N, bits[k] + l * N, (int)l, 0});
         }
-        launch_jobs(c_, add, kb_add, 24.0 * N, "ckks_aes public bits", s_);
+        launch_jobs<true>(c_, add, kb_add, 24.0 * N, "ckks_aes public bits", s_);
     }
 
     // sub_bytes_inplace (ckks_aes_ctr.cpp:474-509): the 16 byte positions as S-box instances
@@ -530,7 +533,7 @@ public:
         std::vector<AddJob> add;
         for (size_t bit = 0; bit < kStateBits; ++bit)
             for (size_t l = 0; l < L; ++l) add.push_back({st_[bit].b + l * N, pts[bit] + l * N, (int)l, 0});
-        launch_jobs(c_, add, kb_add, 24.0 * N, "ckks_aes message bits", s_);
+        launch_jobs<true>(c_, add, kb_add, 24.0 * N, "ckks_aes message bits", s_);
     }
 
     void copy_out(uint64_t* const* out_b, uint64_t* const* out_a, size_t* out_level, double* out_scale) {
