@@ -454,6 +454,14 @@ static Modulus emu_modulus(uint64_t q) {
     return m;
 }
 
+// mont_mul (the Montgomery product of the key inner products) on n pairs: out[i] = x[i] y[i] 2^-64
+// mod q for odd q, qninv = -q^-1 mod 2^64 by Newton iteration.
+void emu_mont_mul(uint64_t q, const uint64_t* x, const uint64_t* y, size_t n, uint64_t* out) {
+    uint64_t inv = q;  // q q = 1 (mod 8): three correct bits, doubled by each step
+    for (int k = 0; k < 5; ++k) inv *= 2 - q * inv;
+    for (size_t i = 0; i < n; ++i) out[i] = mont_mul(x[i], y[i], q, 0 - inv);
+}
+
 // reduce128 on n values (hi[i], lo[i]) modulo q
 void emu_reduce128(uint64_t q, const uint64_t* hi, const uint64_t* lo, size_t n, uint64_t* out) {
     const Modulus m = emu_modulus(q);

@@ -186,6 +186,34 @@ def test_reduce128_canonical(emu, q):
     assert [int(x) for x in out] == [v % q for v in vals]
 
 
+@pytest.mark.parametrize("q", WIDE_MODULI)
+def test_mont_mul_exact(emu, q):
+    """The Montgomery product is x y 2^-64 mod q, canonical, for x < 2q and y < q: random pairs and
+    the pairs whose 128-bit product has a zero low word (x and y multiples of 2^32 or of higher
+    powers of two, zero), where the carry out of the low words is the edge of the formula."""
+    emu.emu_mont_mul.argtypes = [C.c_uint64, u64p, u64p, C.c_size_t, u64p]
+    rng = np.random.default_rng(q % 999983)
+    xs = [int(v) for v in rng.integers(0, 2 * q, 4000, dtype=np.uint64)]
+    ys = [int(v) for v in rng.integers(0, q, 4000, dtype=np.uint64)]
+    bits = q.bit_length() - 1
+    for a in range(1, bits):
+        for b in (64 - a, 65 - a, 70 - a):
+            if 0 < b < bits:
+                for ka, kb in ((1, 1), (3, 5), ((q >> a) - 1, (q >> b) - 1)):
+                    if ka > 0 and kb > 0:
+                        xs.append((ka << a) % (2 * q))
+                        ys.append((kb << b) % q)
+    xs += [0, 0, q - 1, 2 * q - 1, q, 1]
+    ys += [0, q - 1, q - 1, q - 1, 1, 0]
+    x = np.array(xs, dtype=np.uint64)
+    y = np.array(ys, dtype=np.uint64)
+    out = np.zeros(len(xs), dtype=np.uint64)
+    emu.emu_mont_mul(q, x, y, len(xs), out)
+    rinv = pow(1 << 64, -1, q)
+    assert any((a * b) % (1 << 64) == 0 and a * b for a, b in zip(xs, ys))
+    assert [int(v) for v in out] == [(a * b * rinv) % q for a, b in zip(xs, ys)]
+
+
 def _walsh_model(q, lb, la, hb, ha, pt, coefs, c0):
     """The reference's sequence on exact integers: canonical low combinations (sums of added
     multiples), imaginary half times the encoded i, tensor products, products summed by mask."""
